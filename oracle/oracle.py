@@ -1,0 +1,462 @@
+"""CPU oracle for the ISDF hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, as the checker.  The product package (``mp_isdf_b200``) never
+imports it and has no CPU fallback.
+
+It restates the reference (mikovtun/mp_isdf) algorithm for the path:
+
+* AO values / gradients and axis features: the C++ restatement in
+  ``oracle/isdf_oracle.cpp`` (``cpp/src/ao_eval.cpp:205-250``,
+  ``cpp/include/anchor_select_impl.hpp:51-79``);
+* cartesian -> real-spherical matrices: derived here by least squares against
+  real spherical harmonics built from scipy's associated Legendre functions
+  (independently of the product's closed-form derivation); libcint's
+  ``CINTc2s_bra_sph`` is not vendored, so its convention is restated as: p in
+  (x, y, z) order scaled by sqrt(3/4pi), s by 1/sqrt(4pi)
+  (``cpp/src/ao_eval.cpp:132-138``), l >= 2 as r^l Y_lm, m = -l..l, unit-sphere
+  normalised, without the Condon-Shortley phase;
+* qrcp_dense: explicit weighted pair matrix + LAPACK ``dgeqp3`` via scipy
+  (``cpp/src/anchor_select_qrcp.cpp:248-307``);
+* rand_sketch quadrature: U/V from ``std::mt19937_64`` +
+  ``std::normal_distribution`` (C++), ``dgeqp3`` of the sketch, tail / rank
+  logic (``cpp/src/anchor_select_randomized_id.cpp:92-374``);
+* multi-axis scaling (``cpp/src/anchor_select.cpp:426-480``);
+* the fit ``_physical_pair_refit`` and the pair-space error functions
+  (``python/isdf.py:154-191, 238-263``), literally for small grids and in
+  Gram form for large ones;
+* the FP64 nuclear gradient of E = sum_g w_g rho_ISDF(g)^2 assembled from AO
+  values and their dx/dy/dz derivatives.
+
+Parity pinning: see tests/test_oracle.py (known answers of the reference's
+own tests).  The reference itself cannot be built here, and PySCF is absent,
+so AO values are pinned by orthonormality and derivative consistency only.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from math import factorial, pi, sqrt
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libisdf_oracle.so"
+LMAX = 6
+
+_lib = None
+
+
+def build(force=False):
+    """Compile the C++ restatement (g++ -O2 -fopenmp)."""
+    src = HERE / "isdf_oracle.cpp"
+    if LIB_PATH.exists() and not force and LIB_PATH.stat().st_mtime >= src.stat().st_mtime:
+        return LIB_PATH
+    import subprocess
+    tmp = LIB_PATH.with_suffix(".so.tmp")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared",
+                           str(src), "-o", str(tmp)])
+    os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        P = ctypes.c_void_p
+        L.oracle_ctx_create.restype = P
+        L.oracle_ctx_create.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P,
+                                        ctypes.c_longlong, P, ctypes.c_int]
+        L.oracle_ctx_destroy.argtypes = [P]
+        L.oracle_ctx_nao.argtypes = [P]
+        L.oracle_ctx_nao.restype = ctypes.c_int
+        L.oracle_ao_atoms.argtypes = [P, P]
+        L.oracle_eval_ao.argtypes = [P, P, ctypes.c_longlong, ctypes.c_int, P]
+        L.oracle_axis_features.argtypes = [P, P, ctypes.c_longlong, P, ctypes.c_int, P, P]
+        L.oracle_axis_norms_hypot.argtypes = [P, P, P, ctypes.c_longlong, P, ctypes.c_int, P]
+        L.oracle_axis_norms_hypot.restype = ctypes.c_int
+        L.oracle_axis_norms_sq.argtypes = [P, P, P, ctypes.c_longlong, P, ctypes.c_int, P]
+        L.oracle_sketch_factors.argtypes = [ctypes.c_longlong, ctypes.c_longlong,
+                                            ctypes.c_uint64, P, P]
+        L.oracle_sketch.argtypes = [P, P, P, ctypes.c_longlong, P, ctypes.c_int, P, P, P,
+                                    ctypes.c_longlong, P]
+        L.oracle_grid_gram.argtypes = [P, P, ctypes.c_longlong, P, ctypes.c_longlong, P, P]
+        L.oracle_fit_apply.argtypes = [ctypes.c_longlong, ctypes.c_longlong] + [P] * 9
+        L.oracle_last_error.restype = ctypes.c_char_p
+        L.oracle_num_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+# ---------------------------------------------------------------------------
+# cartesian -> spherical
+# ---------------------------------------------------------------------------
+def cart_powers(l):
+    """libcint cartesian order (``cpp/src/ao_eval.cpp:30-44``)."""
+    out = []
+    for lx in range(l, -1, -1):
+        for lz in range(0, l - lx + 1):
+            out.append((lx, l - lx - lz, lz))
+    return out
+
+
+def real_harmonics(l, pts):
+    """Real unit-sphere-normalised Y_lm (m=-l..l), no Condon-Shortley phase."""
+    from scipy.special import lpmv
+    x, y, z = pts.T
+    theta = np.arccos(np.clip(z, -1, 1))
+    phi = np.arctan2(y, x)
+    out = []
+    for m in range(-l, l + 1):
+        am = abs(m)
+        norm = sqrt((2 * l + 1) / (4 * pi) * factorial(l - am) / factorial(l + am))
+        leg = lpmv(am, l, np.cos(theta)) * (-1) ** am      # drop the CS phase
+        if m == 0:
+            out.append(norm * leg)
+        elif m > 0:
+            out.append(sqrt(2) * norm * leg * np.cos(am * phi))
+        else:
+            out.append(sqrt(2) * norm * leg * np.sin(am * phi))
+    return np.array(out)
+
+
+def c2s_matrix(l):
+    """nsph x ncart matrix T with sum_c T[s,c] x^lx y^ly z^lz = r^l Y_ls."""
+    if l == 0:
+        return np.array([[1.0 / sqrt(4 * pi)]])
+    if l == 1:
+        return np.eye(3) * sqrt(3.0 / (4 * pi))
+    rng = np.random.default_rng(1000 + l)
+    pts = rng.normal(size=(8 * (l + 1) ** 2 + 64, 3))
+    pts /= np.linalg.norm(pts, axis=1)[:, None]
+    mono = np.array([pts[:, 0] ** a * pts[:, 1] ** b * pts[:, 2] ** c
+                     for a, b, c in cart_powers(l)])            # [ncart, npts]
+    target = real_harmonics(l, pts)                            # [nsph, npts]
+    t, *_ = np.linalg.lstsq(mono.T, target.T, rcond=None)
+    t = t.T
+    t[np.abs(t) < 1e-13] = 0.0
+    return t
+
+
+def c2s_table(lmax=LMAX):
+    return np.concatenate([c2s_matrix(l).ravel() for l in range(lmax + 1)])
+
+
+_C2S = None
+
+
+# ---------------------------------------------------------------------------
+# context
+# ---------------------------------------------------------------------------
+class OracleContext:
+    def __init__(self, atm, bas, env):
+        global _C2S
+        if _C2S is None:
+            _C2S = np.ascontiguousarray(c2s_table(LMAX))
+        self.atm = np.ascontiguousarray(atm, dtype=np.int32)
+        self.bas = np.ascontiguousarray(bas, dtype=np.int32)
+        self.env = np.ascontiguousarray(env, dtype=np.float64)
+        L = lib()
+        self.h = L.oracle_ctx_create(_p(self.atm), len(self.atm), _p(self.bas), len(self.bas),
+                                     _p(self.env), len(self.env), _p(_C2S), LMAX)
+        if not self.h:
+            raise ValueError(L.oracle_last_error().decode())
+        self.nao = L.oracle_ctx_nao(self.h)
+        self.natm = len(self.atm)
+        self.ao_atom = np.empty(self.nao, dtype=np.int32)
+        L.oracle_ao_atoms(self.h, _p(self.ao_atom))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_ctx_destroy(self.h)
+            self.h = None
+
+    def eval_ao(self, pts):
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        out = np.empty((len(pts), self.nao))
+        lib().oracle_eval_ao(self.h, _p(pts), len(pts), 0, _p(out))
+        return out
+
+    def eval_ao_gradient(self, pts):
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        out = np.empty((3, len(pts), self.nao))
+        lib().oracle_eval_ao(self.h, _p(pts), len(pts), 1, _p(out))
+        return out
+
+    def axis_features(self, pts, axes, scales=None):
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        ax = np.ascontiguousarray(axes, dtype=np.int32)
+        sc = None if scales is None else np.ascontiguousarray(scales, dtype=np.float64)
+        out = np.empty((len(pts), len(ax) * self.nao))
+        lib().oracle_axis_features(self.h, _p(pts), len(pts), _p(ax), len(ax),
+                                   None if sc is None else _p(sc), _p(out))
+        return out
+
+    def axis_norms(self, pts, w, axes, exact_order=True):
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        ax = np.ascontiguousarray(axes, dtype=np.int32)
+        out = np.zeros(len(ax))
+        if exact_order:
+            rc = lib().oracle_axis_norms_hypot(self.h, _p(pts), _p(w), len(pts), _p(ax),
+                                               len(ax), _p(out))
+            if rc < 0:
+                raise ValueError(lib().oracle_last_error().decode())
+            return out, bool(rc)
+        lib().oracle_axis_norms_sq(self.h, _p(pts), _p(w), len(pts), _p(ax), len(ax), _p(out))
+        return out, bool(np.any(w != 0))
+
+    def sketch(self, pts, w, axes, scales, u, v, ell):
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        ax = np.ascontiguousarray(axes, dtype=np.int32)
+        sc = np.ascontiguousarray(scales if scales is not None else np.ones(len(ax)))
+        y = np.empty((len(pts), ell))
+        lib().oracle_sketch(self.h, _p(pts), _p(w), len(pts), _p(ax), len(ax), _p(sc),
+                            _p(np.ascontiguousarray(u)), _p(np.ascontiguousarray(v)), ell, _p(y))
+        return y
+
+    def grid_gram(self, pts, anchor_ao):
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        a = np.ascontiguousarray(anchor_ao, dtype=np.float64)
+        G = np.empty((len(pts), len(a)))
+        q = np.empty(len(pts))
+        lib().oracle_grid_gram(self.h, _p(pts), len(pts), _p(a), len(a), _p(G), _p(q))
+        return G, q
+
+
+AXIS_CODES = {"ao": 0, "dx": 1, "dy": 2, "dz": 3}
+
+
+def sketch_factors(d, ell, seed):
+    u = np.empty(d * ell)
+    v = np.empty(d * ell)
+    lib().oracle_sketch_factors(d, ell, np.uint64(seed), _p(u), _p(v))
+    return u.reshape(d, ell), v.reshape(d, ell)
+
+
+# ---------------------------------------------------------------------------
+# selection (cpp/src/anchor_select.cpp:426-505)
+# ---------------------------------------------------------------------------
+def axis_scales(ctx, pts, w, axes, axis_weights=None, exact_order=True):
+    """Global Frobenius scales for >1 axes (``cpp/src/anchor_select.cpp:437-480``)."""
+    if len(axes) <= 1:
+        return None
+    norms, any_eligible = ctx.axis_norms(pts, w, axes, exact_order=exact_order)
+    if not any_eligible:
+        return np.array([])
+    if np.any(~(norms > 0)) or not np.all(np.isfinite(norms)):
+        raise ValueError("axis Frobenius norm must be finite and positive")
+    factors = np.ones(len(axes)) if not axis_weights else np.asarray(axis_weights, float)
+    return factors / norms
+
+
+def pair_matrix(features, w):
+    """A[:, g] = sqrt|w_g| f_g (x) f_g (``cpp/src/anchor_select_qrcp.cpp:253-267``)."""
+    outer = np.einsum("gi,gj->gij", features, features).reshape(len(features), -1)
+    return (outer * np.sqrt(np.abs(w))[:, None]).T
+
+
+def select_qrcp_dense(ctx, pts, w, axes, tolerance=1e-10, max_rank=0, scales=None):
+    """qrcp_dense via scipy/LAPACK dgeqp3 (``anchor_select_qrcp.cpp:178-307``)."""
+    from scipy.linalg import qr
+    w = np.asarray(w, float)
+    keep = np.flatnonzero(w != 0)
+    if len(keep) == 0:
+        return []
+    f = ctx.axis_features(pts[keep], axes, scales)
+    A = pair_matrix(f, w[keep])
+    m, n = A.shape
+    _, r, piv = qr(A, pivoting=True, mode="economic")
+    cap = min(m, n, max_rank if max_rank else min(m, n))
+    diag = np.abs(np.diag(r))
+    first = diag[0] if cap else 0.0
+    out = []
+    for i in range(cap):
+        if first == 0 or diag[i] <= tolerance * first:
+            break
+        out.append(int(keep[piv[i]]))
+    return out
+
+
+def select_rand_sketch(ctx, pts, w, axes, tolerance=1e-10, max_rank=0, sketch_size=128,
+                       oversampling=16, seed=7, scales=None, return_details=False):
+    """Quadrature Khatri-Rao sketch + dgeqp3 (``anchor_select_randomized_id.cpp``)."""
+    from scipy.linalg.lapack import dgeqp3
+    if oversampling == 0 or (not max_rank and sketch_size <= oversampling):
+        raise ValueError("invalid randomized ID grid, tolerance, batch, sketch or rank/oversampling")
+    w = np.asarray(w, float)
+    keep = np.flatnonzero(w != 0)
+    d = len(axes) * ctx.nao
+    ell = max_rank + oversampling if max_rank else sketch_size
+    n = len(keep)
+    if n == 0:
+        return ([], {}) if return_details else []
+    physical_rank = d * (d + 1) // 2
+    if max_rank > min(n, physical_rank):
+        raise ValueError("requested anchor_rank exceeds eligible candidates or physical pair rank")
+    u, v = sketch_factors(d, ell, seed)
+    y = ctx.sketch(pts[keep], w[keep], axes, scales, u, v, ell)   # [n, ell]
+    ymat = np.asfortranarray(y.T)                                  # ell x n column-major
+    qr_, jpvt, tau, work, info = dgeqp3(ymat)
+    if info != 0:
+        raise RuntimeError("dgeqp3 failed")
+    steps = min(ell, n)
+    energy = np.array([np.sum(qr_[i, i:] ** 2) for i in range(steps)])
+    diag = np.abs(np.diag(qr_)[:steps])
+    tails = np.zeros(steps + 1)
+    for i in range(steps - 1, -1, -1):
+        tails[i] = np.hypot(tails[i + 1], np.sqrt(energy[i]))
+    diag_max = diag.max() if steps else 0.0
+    norm = tails[0]
+    floor = np.finfo(float).eps * max(ell, n) * diag_max
+    numerical_rank = steps
+    for i in range(steps):
+        if diag[i] <= floor:
+            numerical_rank = i
+            break
+    cap = min(max_rank if max_rank else ell - oversampling, ell - oversampling, steps,
+              physical_rank, numerical_rank)
+    if max_rank and numerical_rank < max_rank:
+        raise ValueError("requested anchor_rank exceeds the numerical rank of the randomized sketch")
+    rank = max_rank if max_rank else cap
+    if not max_rank:
+        for i in range(cap + 1):
+            if tails[i] <= tolerance * norm:
+                rank = i
+                break
+    piv = [int(keep[jpvt[i] - 1]) for i in range(rank)]
+    if return_details:
+        return piv, dict(y=y, diag=diag, tails=tails, numerical_rank=numerical_rank,
+                         jpvt=jpvt - 1, u=u, v=v, keep=keep)
+    return piv
+
+
+# ---------------------------------------------------------------------------
+# fit and pair error (python/isdf.py)
+# ---------------------------------------------------------------------------
+def physical_pair_refit(anchor_pairs, anchor_weights, ao, batch_size=2048):
+    """``_physical_pair_refit`` (``python/isdf.py:238-263``) restated."""
+    u, s, vh = np.linalg.svd(anchor_pairs.T, full_matrices=False)
+    retained = s > (1e-12 * s[0] if len(s) else 0)
+    physical_transform = (vh[retained].T / s[retained]) @ u[:, retained].T
+    theta = np.empty((len(anchor_weights), len(ao)))
+    for first in range(0, len(ao), batch_size):
+        block = ao[first:first + batch_size]
+        pairs = (block[:, :, None] * block[:, None, :]).reshape(len(block), -1)
+        theta[:, first:first + len(block)] = (physical_transform @ pairs.T) / anchor_weights[:, None]
+    diag = {"retained_rank": int(np.count_nonzero(retained)),
+            "condition": float(s[0] / s[-1]) if len(s) and s[-1] > 0 else float("inf"),
+            "singular_values": s}
+    return theta, diag
+
+
+def pair_space_error_norms(pair_grid, pair_anchor, anchor_weights, theta, grid_weights,
+                           block_size=256):
+    """``pair_space_error_norms`` (``python/isdf.py:154-173``) restated."""
+    weighted_anchor = pair_anchor * anchor_weights[:, None]
+    residual_sq = exact_sq = 0.0
+    for first in range(0, len(grid_weights), block_size):
+        last = min(first + block_size, len(grid_weights))
+        exact = pair_grid[first:last]
+        rec = theta[:, first:last].T @ weighted_anchor
+        weight = np.abs(grid_weights[first:last])
+        residual_sq += np.einsum("g,gi,gi->", weight, exact - rec, exact - rec)
+        exact_sq += np.einsum("g,gi,gi->", weight, exact, exact)
+    absolute = np.sqrt(residual_sq)
+    relative = absolute / np.sqrt(exact_sq) if exact_sq else (0.0 if absolute == 0 else np.inf)
+    return {"l2": absolute, "relative": relative}
+
+
+def gram_fit(ctx, coords, weights, anchor_coords, anchor_weights):
+    """Theta and pair error in Gram form (large grids), FP64.
+
+    X_g = pinv((Phi_a Phi_a^T)o2) (G_g o G_g) equals pinv(C^T) p_g of the
+    literal SVD fit when the anchor pair matrix C has full rank; the cutoff
+    is applied to singular values of C (sqrt of eigenvalues of M).
+    """
+    phi_a = ctx.eval_ao(anchor_coords)
+    S = phi_a @ phi_a.T
+    M = S * S
+    lam, vec = np.linalg.eigh(M)
+    s = np.sqrt(np.clip(lam, 0, None))
+    keep = s > 1e-12 * s.max()
+    T = (vec[:, keep] / lam[keep]) @ vec[:, keep].T
+    G, q = ctx.grid_gram(coords, phi_a)
+    n, k = G.shape
+    theta = np.empty((k, n))
+    err2 = np.zeros(1)
+    ex2 = np.zeros(1)
+    w = np.ascontiguousarray(weights, float)
+    lib().oracle_fit_apply(n, k, _p(G), _p(q), _p(w), _p(np.ascontiguousarray(T)),
+                           _p(np.ascontiguousarray(M)),
+                           _p(np.ascontiguousarray(anchor_weights, float)), _p(theta),
+                           _p(err2), _p(ex2))
+    err2 = max(err2[0], 0.0)
+    return theta, {"l2": np.sqrt(err2), "relative": np.sqrt(err2 / ex2[0]) if ex2[0] else 0.0}
+
+
+# ---------------------------------------------------------------------------
+# nuclear-gradient reference (not in the reference project)
+# ---------------------------------------------------------------------------
+def isdf_energy(ctx, coords, weights, anchor_coords, anchor_weights, dm):
+    """E = sum_g w_g rho_ISDF(g)^2 with rho_ISDF(g) = sum_k Theta_kg w_k rho_a(k)."""
+    phi_a = ctx.eval_ao(anchor_coords)
+    M = (phi_a @ phi_a.T) ** 2
+    rho_a = np.einsum("ki,ij,kj->k", phi_a, dm, phi_a)
+    z = np.linalg.solve(M, rho_a)
+    G, _ = ctx.grid_gram(coords, phi_a)
+    rho = (G * G) @ z
+    return float(np.sum(weights * rho * rho))
+
+
+def isdf_energy_gradient(ctx, coords, weights, anchor_coords, anchor_weights, dm,
+                         chunk=65536):
+    """Analytic dE/dR[natm,3] from AO values and dx/dy/dz (d phi/dR_A = -grad_r phi)."""
+    natm = ctx.natm
+    own = ctx.ao_atom
+    phi_a = ctx.eval_ao(anchor_coords)              # [k, nao]
+    dphi_a = ctx.eval_ao_gradient(anchor_coords)    # [3, k, nao]
+    S = phi_a @ phi_a.T
+    M = S * S
+    rho_a = np.einsum("ki,ij,kj->k", phi_a, dm, phi_a)
+    z = np.linalg.solve(M, rho_a)
+    k, nao = phi_a.shape
+    grad = np.zeros((natm, 3))
+    B = np.zeros((k, nao))
+    v = np.zeros(k)
+    for s in range(0, len(coords), chunk):
+        pts = coords[s:s + chunk]
+        w = weights[s:s + chunk]
+        phi = ctx.eval_ao(pts)                      # [b, nao]
+        dphi = ctx.eval_ao_gradient(pts)            # [3, b, nao]
+        G = phi @ phi_a.T                           # [b, k]
+        h = G * G
+        rho = h @ z
+        u = 2 * w * rho
+        v += u @ h
+        alpha = 2 * u[:, None] * z[None, :] * G     # [b, k]
+        B += alpha.T @ phi
+        beta = alpha @ phi_a                        # [b, nao]
+        contrib = np.einsum("gm,cgm->cm", beta, dphi)   # [3, nao]
+        for c in range(3):
+            np.add.at(grad[:, c], own, -contrib[c])
+    # anchor-side terms: B (grid reduction) and the M / rho_a dependence
+    y = np.linalg.solve(M, v)
+    # d rho_a(k) = 2 phi_a(k)^T D dphi_a(k)
+    Dphi = phi_a @ dm                               # [k, nao]
+    anchor_coef = B + 2 * y[:, None] * Dphi         # coefficient of dphi_a[k, mu]
+    # -y^T dM z, dM_kl = 2 S_kl dS_kl, dS_kl = dphi_k.phi_l + phi_k.dphi_l
+    W = 2 * S * (y[:, None] * z[None, :])           # coefficient of dS_kl
+    anchor_coef -= (W + W.T) @ phi_a
+    contrib = np.einsum("km,ckm->cm", anchor_coef, dphi_a)
+    for c in range(3):
+        np.add.at(grad[:, c], own, -contrib[c])
+    return grad
