@@ -1,0 +1,169 @@
+/*
+ * C-ABI of the B200 ISDF hot-path library (libisdf_b200.so).
+ *
+ * Every entry point returns an int status (0 = ok, see isdf_status); no C++
+ * exception crosses the boundary.  isdf_last_error() returns the message of
+ * the calling thread's last failure.  Arrays are plain pointers with explicit
+ * sizes; "dev" pointers are CUDA device pointers, "host" pointers are host
+ * memory.  `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ * stream).  A context belongs to the device that was current when it was
+ * created; calls on distinct streams with distinct outputs may run
+ * concurrently.
+ *
+ * Each declaration names the interface of mikovtun/mp_isdf it replaces
+ * (file:line within that project).
+ */
+#ifndef ISDF_B200_H
+#define ISDF_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct isdf_ctx isdf_ctx;
+
+enum isdf_status {
+    ISDF_OK = 0,
+    ISDF_ERR_INVALID = 1,         /* std::invalid_argument -> ValueError */
+    ISDF_ERR_OVERFLOW = 2,        /* std::overflow_error */
+    ISDF_ERR_RUNTIME = 3,         /* std::runtime_error */
+    ISDF_ERR_CUDA = 4,            /* CUDA runtime failure */
+    ISDF_ERR_NOT_IMPLEMENTED = 5, /* NotImplementedError */
+    ISDF_ERR_LOGIC = 6            /* std::logic_error */
+};
+
+/* AxisType codes (cpp/include/enums.hpp:8-14). */
+enum isdf_axis { ISDF_AXIS_AO = 0, ISDF_AXIS_DX = 1, ISDF_AXIS_DY = 2, ISDF_AXIS_DZ = 3, ISDF_AXIS_OCC = 4 };
+
+/* LocalAnchorSelectionAlgorithm codes (cpp/include/enums.hpp:23-30). */
+enum isdf_algorithm {
+    ISDF_QRCP_DENSE = 0,             /* QRColumnPivoting */
+    ISDF_QRCP_ONLINE = 1,            /* OnlineQRColumnPivoting */
+    ISDF_RAND_SKETCH_QUADRATURE = 2, /* RandomizedQuadratureKhatriRao */
+    ISDF_CVT = 3,                    /* CentroidalVoronoi (not on this path) */
+    ISDF_RAND_SKETCH_DENSITY = 4,    /* RandomizedAODensityKhatriRao (not on this path) */
+    ISDF_RAND_SKETCH_DENSITY_NORM = 5
+};
+
+enum isdf_precision { ISDF_FP64 = 0, ISDF_MIXED = 1 };
+
+/* Human-readable name of a status code. */
+const char* isdf_status_string(int status);
+/* Message of the calling thread's last failure ("" if none). */
+const char* isdf_last_error(void);
+/* 1 when a CUDA device is usable, else 0 (never fails). */
+int isdf_cuda_available(void);
+
+/* ---- context --------------------------------------------------------------
+ * Replaces LibcintContext(atm, bas, env) (cpp/src/ao_eval.cpp:78-158,
+ * cpp/src/ao_eval_pybind.cpp:33-46): copies the libcint ATM[natm,6],
+ * BAS[nbas,8] int32 tables and ENV[nenv] and uploads the shell table to the
+ * current device. */
+int isdf_ctx_create(const int32_t* atm_host, int32_t natm, const int32_t* bas_host, int32_t nbas,
+                    const double* env_host, int64_t nenv, isdf_ctx** out);
+int isdf_ctx_destroy(isdf_ctx* ctx);
+/* LibcintContext.nao (cpp/src/ao_eval_pybind.cpp:91) and atom count. */
+int isdf_ctx_info(const isdf_ctx* ctx, int64_t* nao, int32_t* natm, int32_t* nshell);
+/* Atom owning each AO (nao int32), for nuclear derivatives. */
+int isdf_ctx_ao_atoms(const isdf_ctx* ctx, int32_t* out_host);
+
+/* ---- AO evaluation --------------------------------------------------------
+ * Replaces LibcintContext::eval_ao / eval_ao_gradient (cpp/src/ao_eval.cpp:164-310).
+ * xyz_dev[ng,3] bohr.  values_dev (ng x nao, row-major) and/or
+ * grad_dev (3 x ng x nao, component-major) may be NULL when not wanted.
+ * dtype: 0 = float64, 1 = float32 outputs. */
+int isdf_eval_ao(isdf_ctx* ctx, const double* xyz_dev, int64_t ng, int32_t dtype,
+                 void* values_dev, void* grad_dev, void* stream);
+/* Host-buffer form of the same call (copies in, evaluates, copies out). */
+int isdf_eval_ao_host(isdf_ctx* ctx, const double* xyz_host, int64_t ng, double* values_host,
+                      double* grad_host);
+
+/* ---- axis features ----------------------------------------------------------
+ * Replaces AnchorSelection::evaluate_axis (cpp/include/anchor_select_impl.hpp:11-81,
+ * cpp/src/anchor_select_pybind.cpp:211-222): concatenated unscaled axis
+ * blocks, out (ng x naxes*nao) row-major. */
+int isdf_evaluate_axis(isdf_ctx* ctx, const double* xyz_dev, int64_t ng, const int32_t* axes_host,
+                       int32_t naxes, double* out_dev, void* stream);
+int isdf_evaluate_axis_host(isdf_ctx* ctx, const double* xyz_host, int64_t ng,
+                            const int32_t* axes_host, int32_t naxes, double* out_host);
+
+/* ---- anchor selection ------------------------------------------------------
+ * Replaces AnchorSelection::select (cpp/src/anchor_select.cpp:79-173,
+ * cpp/src/anchor_select_pybind.cpp:162-210) for QRColumnPivoting,
+ * OnlineQRColumnPivoting and RandomizedQuadratureKhatriRao.  Pivots are
+ * original grid indices in pivot order. */
+typedef struct isdf_select_args {
+    int32_t algorithm;           /* enum isdf_algorithm */
+    int32_t naxes;
+    const int32_t* axes;         /* host, naxes AxisType codes */
+    const double* axis_weights;  /* host, naxes factors, or NULL */
+    double tolerance;            /* default 1e-10 */
+    int64_t max_rank;            /* 0 = tolerance only */
+    int64_t batch_size;          /* default 128 (validated; results are batch invariant) */
+    int64_t sketch_size;         /* default 128 */
+    int64_t oversampling;        /* default 16 */
+    uint64_t seed;               /* default 7 */
+    int32_t precision;           /* enum isdf_precision (rand_sketch only) */
+    int32_t debug;               /* print a summary line on stderr */
+} isdf_select_args;
+
+typedef struct isdf_select_info {
+    int64_t n_kept;              /* nonzero-weight points */
+    int64_t sketch_rows;         /* rand_sketch: ell */
+    int64_t numerical_rank;      /* rand_sketch */
+    int64_t verifications;       /* exact recomputations (pair QR: winners; mixed sketch: candidates) */
+    int64_t reselections;
+    double relative_residual;    /* sketch tail / pair-QR last |R_jj| / |R_00| */
+} isdf_select_info;
+
+void isdf_select_args_default(isdf_select_args* args);
+/* pivots_host must hold at least `capacity` entries; *npivots receives the count. */
+int isdf_select(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz_dev,
+                const double* w_dev, int64_t ng, int64_t* pivots_host, int64_t capacity,
+                int64_t* npivots, isdf_select_info* info, void* stream);
+int isdf_select_host(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz_host,
+                     const double* w_host, int64_t ng, int64_t* pivots_host, int64_t capacity,
+                     int64_t* npivots, isdf_select_info* info);
+
+/* ---- interpolation-vector fit + pair-space error ---------------------------
+ * Replaces _physical_pair_refit and the pair-space error functions
+ * (python/isdf.py:238-263, 154-191).  anchors_host: k original grid indices.
+ * theta_dev receives Theta (k x n_kept, row-major, leading dimension n_kept);
+ * it must hold k*ng doubles.  want_error != 0 also evaluates the pair-space
+ * error with FP64 AO values. */
+typedef struct isdf_fit_info {
+    int64_t n_kept;
+    int64_t retained_rank;
+    double condition;
+    double max_abs_physical_coefficient;
+    double pair_l2;              /* sqrt(sum |w| |p - rec|^2) */
+    double pair_relative;
+    double theta_w[64];          /* sum_g Theta[a,g] w_g (first 64 anchors) */
+} isdf_fit_info;
+
+int isdf_fit(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t ng,
+             const int64_t* anchors_host, int64_t k, int32_t precision, int32_t want_error,
+             double* theta_dev, isdf_fit_info* info, void* stream);
+int isdf_fit_host(isdf_ctx* ctx, const double* xyz_host, const double* w_host, int64_t ng,
+                  const int64_t* anchors_host, int64_t k, int32_t precision, int32_t want_error,
+                  double* theta_host, isdf_fit_info* info);
+/* Pair-space error of a given Theta (k x n_kept, leading dimension n_kept),
+ * recomputed with FP64 AO values. */
+int isdf_pair_error(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t ng,
+                    const int64_t* anchors_host, int64_t k, const double* theta_dev,
+                    double* l2, double* relative, void* stream);
+/* Pair-space error reduction from Gram terms (device arrays): q[n] = |p_g|,
+ * H[n,k] = C p_g, X[n,k] = Theta_g * w_anchor, M[k,k] = C C^T, w[n].
+ * out_host = {l2, relative}.  Same reduction as isdf_fit's error
+ * (python/isdf.py:154-173). */
+int isdf_pair_error_terms(int64_t n, int64_t k, const double* q_dev, const double* H_dev,
+                          const double* X_dev, const double* M_dev, const double* w_dev,
+                          double* out_host, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ISDF_B200_H */

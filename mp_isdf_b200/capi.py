@@ -1,0 +1,243 @@
+"""ctypes binding of the C-ABI in ``include/isdf_b200.h`` (libisdf_b200.so).
+
+Device-pointer entry points take torch CUDA tensors; the stream is torch's
+current stream on the tensor's device.  Host-buffer entry points take numpy
+arrays.  There is no CPU implementation behind any of these calls: without a
+CUDA device they raise.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libisdf_b200.so"
+
+P = ctypes.c_void_p
+I32 = ctypes.c_int32
+I64 = ctypes.c_int64
+F64 = ctypes.c_double
+
+SYMBOLS = [
+    "isdf_status_string", "isdf_last_error", "isdf_cuda_available",
+    "isdf_ctx_create", "isdf_ctx_destroy", "isdf_ctx_info", "isdf_ctx_ao_atoms",
+    "isdf_eval_ao", "isdf_eval_ao_host", "isdf_evaluate_axis", "isdf_evaluate_axis_host",
+    "isdf_select_args_default", "isdf_select", "isdf_select_host",
+    "isdf_fit", "isdf_fit_host", "isdf_pair_error", "isdf_pair_error_terms",
+]
+
+ALGORITHMS = {"qrcp_dense": 0, "qrcp_online": 1, "rand_sketch": 2}
+AXES = {"ao": 0, "dx": 1, "dy": 2, "dz": 3, "occ": 4}
+
+
+class SelectArgs(ctypes.Structure):
+    _fields_ = [("algorithm", I32), ("naxes", I32), ("axes", P), ("axis_weights", P),
+                ("tolerance", F64), ("max_rank", I64), ("batch_size", I64),
+                ("sketch_size", I64), ("oversampling", I64), ("seed", ctypes.c_uint64),
+                ("precision", I32), ("debug", I32)]
+
+
+class SelectInfo(ctypes.Structure):
+    _fields_ = [("n_kept", I64), ("sketch_rows", I64), ("numerical_rank", I64),
+                ("verifications", I64), ("reselections", I64), ("relative_residual", F64)]
+
+
+class FitInfo(ctypes.Structure):
+    _fields_ = [("n_kept", I64), ("retained_rank", I64), ("condition", F64),
+                ("max_abs_physical_coefficient", F64), ("pair_l2", F64),
+                ("pair_relative", F64), ("theta_w", F64 * 64)]
+
+
+class IsdfError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing; run `python -m mp_isdf_b200.build`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        L.isdf_status_string.restype = ctypes.c_char_p
+        L.isdf_last_error.restype = ctypes.c_char_p
+        L.isdf_ctx_create.argtypes = [P, I32, P, I32, P, I64, ctypes.POINTER(P)]
+        L.isdf_ctx_destroy.argtypes = [P]
+        L.isdf_ctx_info.argtypes = [P, ctypes.POINTER(I64), ctypes.POINTER(I32), ctypes.POINTER(I32)]
+        L.isdf_ctx_ao_atoms.argtypes = [P, P]
+        L.isdf_eval_ao.argtypes = [P, P, I64, I32, P, P, P]
+        L.isdf_eval_ao_host.argtypes = [P, P, I64, P, P]
+        L.isdf_evaluate_axis.argtypes = [P, P, I64, P, I32, P, P]
+        L.isdf_evaluate_axis_host.argtypes = [P, P, I64, P, I32, P]
+        L.isdf_select_args_default.argtypes = [ctypes.POINTER(SelectArgs)]
+        L.isdf_select.argtypes = [P, ctypes.POINTER(SelectArgs), P, P, I64, P, I64,
+                                  ctypes.POINTER(I64), ctypes.POINTER(SelectInfo), P]
+        L.isdf_select_host.argtypes = [P, ctypes.POINTER(SelectArgs), P, P, I64, P, I64,
+                                       ctypes.POINTER(I64), ctypes.POINTER(SelectInfo)]
+        L.isdf_fit.argtypes = [P, P, P, I64, P, I64, I32, I32, P, ctypes.POINTER(FitInfo), P]
+        L.isdf_fit_host.argtypes = [P, P, P, I64, P, I64, I32, I32, P, ctypes.POINTER(FitInfo)]
+        L.isdf_pair_error.argtypes = [P, P, P, I64, P, I64, P, ctypes.POINTER(F64),
+                                      ctypes.POINTER(F64), P]
+        L.isdf_pair_error_terms.argtypes = [I64, I64, P, P, P, P, P, P, P]
+        _lib = L
+    return _lib
+
+
+def check(status: int):
+    if status != 0:
+        raise IsdfError(status, lib().isdf_last_error().decode())
+
+
+def _np(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _ptr(a):
+    """Data pointer of a numpy array or torch tensor (None -> NULL)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(P)
+    return P(a.data_ptr())
+
+
+def _stream(t):
+    import torch
+    return P(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+class Context:
+    """Device context over libcint-layout tables (C-ABI ``isdf_ctx``)."""
+
+    def __init__(self, atm, bas, env):
+        self._atm = _np(atm, np.int32)
+        self._bas = _np(bas, np.int32)
+        self._env = _np(env, np.float64)
+        h = P()
+        check(lib().isdf_ctx_create(_ptr(self._atm), len(self._atm), _ptr(self._bas),
+                                    len(self._bas), _ptr(self._env), len(self._env),
+                                    ctypes.byref(h)))
+        self.h = h
+        nao, natm, nsh = I64(), I32(), I32()
+        check(lib().isdf_ctx_info(self.h, ctypes.byref(nao), ctypes.byref(natm), ctypes.byref(nsh)))
+        self.nao, self.natm, self.nshell = nao.value, natm.value, nsh.value
+        self.ao_atoms = np.empty(self.nao, dtype=np.int32)
+        check(lib().isdf_ctx_ao_atoms(self.h, _ptr(self.ao_atoms)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().isdf_ctx_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    # ---- device tensors ------------------------------------------------------
+    def eval_ao(self, xyz, values=None, grad=None, dtype=None):
+        """xyz: CUDA float64 tensor [ng,3]; fills/returns values [ng,nao] and/or grad [3,ng,nao]."""
+        import torch
+        ng = xyz.shape[0]
+        dt = dtype or (values.dtype if values is not None else torch.float64)
+        code = 0 if dt == torch.float64 else 1
+        check(lib().isdf_eval_ao(self.h, _ptr(xyz), ng, code, _ptr(values), _ptr(grad),
+                                 _stream(xyz)))
+        return values, grad
+
+    def select(self, xyz, w, algorithm="rand_sketch", axes=("ao",), axis_weights=None,
+               tolerance=1e-10, max_rank=0, batch_size=128, sketch_size=128, oversampling=16,
+               seed=7, precision="fp64", debug=False):
+        """Anchor selection on device-resident points/weights; returns (pivots, info)."""
+        args, keep = make_select_args(algorithm, axes, axis_weights, tolerance, max_rank,
+                                      batch_size, sketch_size, oversampling, seed, precision, debug)
+        ng = xyz.shape[0]
+        piv = np.empty(max(ng, 1), dtype=np.int64)
+        n = I64()
+        info = SelectInfo()
+        check(lib().isdf_select(self.h, ctypes.byref(args), _ptr(xyz), _ptr(w), ng, _ptr(piv),
+                                len(piv), ctypes.byref(n), ctypes.byref(info), _stream(xyz)))
+        del keep
+        return piv[:n.value].copy(), info
+
+    def fit(self, xyz, w, anchors, theta, precision="fp64", want_error=True):
+        """Theta into the CUDA float64 tensor `theta` (capacity k*ng); returns FitInfo."""
+        a = _np(anchors, np.int64)
+        info = FitInfo()
+        check(lib().isdf_fit(self.h, _ptr(xyz), _ptr(w), xyz.shape[0], _ptr(a), len(a),
+                             1 if precision == "mixed" else 0, int(want_error), _ptr(theta),
+                             ctypes.byref(info), _stream(xyz)))
+        return info
+
+    def pair_error(self, xyz, w, anchors, theta):
+        a = _np(anchors, np.int64)
+        l2, rel = F64(), F64()
+        check(lib().isdf_pair_error(self.h, _ptr(xyz), _ptr(w), xyz.shape[0], _ptr(a), len(a),
+                                    _ptr(theta), ctypes.byref(l2), ctypes.byref(rel),
+                                    _stream(xyz)))
+        return l2.value, rel.value
+
+    # ---- host arrays -----------------------------------------------------------
+    def eval_ao_host(self, xyz, gradient=False):
+        xyz = _np(xyz, np.float64).reshape(-1, 3)
+        out = np.empty((3, len(xyz), self.nao) if gradient else (len(xyz), self.nao))
+        check(lib().isdf_eval_ao_host(self.h, _ptr(xyz), len(xyz),
+                                      None if gradient else _ptr(out),
+                                      _ptr(out) if gradient else None))
+        return out
+
+    def select_host(self, xyz, w, **kw):
+        args, keep = make_select_args(**kw)
+        xyz = _np(xyz, np.float64).reshape(-1, 3)
+        w = _np(w, np.float64)
+        piv = np.empty(max(len(xyz), 1), dtype=np.int64)
+        n = I64()
+        info = SelectInfo()
+        check(lib().isdf_select_host(self.h, ctypes.byref(args), _ptr(xyz), _ptr(w), len(xyz),
+                                     _ptr(piv), len(piv), ctypes.byref(n), ctypes.byref(info)))
+        del keep
+        return piv[:n.value].copy(), info
+
+    def fit_host(self, xyz, w, anchors, precision="fp64"):
+        xyz = _np(xyz, np.float64).reshape(-1, 3)
+        w = _np(w, np.float64)
+        a = _np(anchors, np.int64)
+        theta = np.empty(max(1, len(a) * len(xyz)))
+        info = FitInfo()
+        check(lib().isdf_fit_host(self.h, _ptr(xyz), _ptr(w), len(xyz), _ptr(a), len(a),
+                                  1 if precision == "mixed" else 0, 1, _ptr(theta),
+                                  ctypes.byref(info)))
+        return theta[:len(a) * info.n_kept].reshape(len(a), info.n_kept), info
+
+
+def make_select_args(algorithm="rand_sketch", axes=("ao",), axis_weights=None, tolerance=1e-10,
+                     max_rank=0, batch_size=128, sketch_size=128, oversampling=16, seed=7,
+                     precision="fp64", debug=False):
+    args = SelectArgs()
+    lib().isdf_select_args_default(ctypes.byref(args))
+    ax = np.array([AXES[a] if isinstance(a, str) else int(a) for a in axes], dtype=np.int32)
+    aw = None if axis_weights is None else _np(axis_weights, np.float64)
+    args.algorithm = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
+    args.naxes = len(ax)
+    args.axes = _ptr(ax)
+    args.axis_weights = _ptr(aw) if aw is not None else None
+    args.tolerance = tolerance
+    args.max_rank = max_rank
+    args.batch_size = batch_size
+    args.sketch_size = sketch_size
+    args.oversampling = oversampling
+    args.seed = seed
+    args.precision = 1 if precision == "mixed" else 0
+    args.debug = int(debug)
+    return args, (ax, aw)
+
+
+def pair_error_terms(q, H, X, M, w):
+    """{l2, relative} from device tensors (see isdf_pair_error_terms)."""
+    n, k = H.shape
+    out = np.zeros(2)
+    check(lib().isdf_pair_error_terms(n, k, _ptr(q), _ptr(H), _ptr(X), _ptr(M), _ptr(w),
+                                      _ptr(out), _stream(q)))
+    return {"l2": out[0], "relative": out[1]}

@@ -1,0 +1,407 @@
+// extern "C" boundary of libisdf_b200.so (declared in include/isdf_b200.h).
+#include "../../include/isdf_b200.h"
+#include "isdf_fit.h"
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+
+struct isdf_ctx {
+    std::unique_ptr<isdf::Context> c;
+    cudaStream_t stream = nullptr;   // private stream of the host-buffer entry points
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return ISDF_OK;
+    } catch (const isdf::Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return ISDF_ERR_RUNTIME;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return ISDF_ERR_RUNTIME;
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        ISDF_CUDA(cudaGetDevice(&prev));
+        if (prev != dev) ISDF_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (cudaGetDevice(&cur) == cudaSuccess && prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+isdf::Context& ctx_of(isdf_ctx* ctx) {
+    if (!ctx || !ctx->c) isdf::fail(isdf::kInvalid, "null isdf context");
+    return *ctx->c;
+}
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+template <class T>
+void upload(isdf::DeviceBuffer<T>& d, const T* h, size_t n, cudaStream_t s) {
+    d.reset(n, s);
+    if (n) ISDF_CUDA(cudaMemcpyAsync(d.get(), h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+isdf::SelectOptions options_of(const isdf_select_args* a) {
+    if (!a) isdf::fail(isdf::kInvalid, "null selection arguments");
+    isdf::SelectOptions o;
+    o.algorithm = a->algorithm;
+    if (a->naxes <= 0 || !a->axes) isdf::fail(isdf::kInvalid, "axis list must not be empty");
+    o.axes.assign(a->axes, a->axes + a->naxes);
+    if (a->axis_weights) o.axis_weights.assign(a->axis_weights, a->axis_weights + a->naxes);
+    o.tolerance = a->tolerance;
+    o.max_rank = a->max_rank;
+    o.batch_size = a->batch_size;
+    o.sketch_size = a->sketch_size;
+    o.oversampling = a->oversampling;
+    o.seed = a->seed;
+    o.precision = a->precision;
+    o.debug = a->debug != 0;
+    if (o.max_rank < 0 || o.batch_size < 0 || o.sketch_size < 0 || o.oversampling < 0)
+        isdf::fail(isdf::kInvalid, "sizes must be nonnegative");
+    return o;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* isdf_status_string(int status) {
+    switch (status) {
+    case ISDF_OK: return "ok";
+    case ISDF_ERR_INVALID: return "invalid argument";
+    case ISDF_ERR_OVERFLOW: return "overflow";
+    case ISDF_ERR_RUNTIME: return "runtime error";
+    case ISDF_ERR_CUDA: return "CUDA error";
+    case ISDF_ERR_NOT_IMPLEMENTED: return "not implemented";
+    case ISDF_ERR_LOGIC: return "logic error";
+    default: return "unknown status";
+    }
+}
+
+const char* isdf_last_error(void) { return g_last_error.c_str(); }
+
+int isdf_cuda_available(void) {
+    int n = 0;
+    return cudaGetDeviceCount(&n) == cudaSuccess && n > 0 ? 1 : 0;
+}
+
+int isdf_ctx_create(const int32_t* atm, int32_t natm, const int32_t* bas, int32_t nbas,
+                    const double* env, int64_t nenv, isdf_ctx** out) {
+    return guarded([&] {
+        if (!out) isdf::fail(isdf::kInvalid, "null output pointer");
+        *out = nullptr;
+        if ((natm && !atm) || (nbas && !bas) || !env)
+            isdf::fail(isdf::kInvalid, "expected atm[natm,6], bas[nbas,8], env[nenv]");
+        auto h = std::make_unique<isdf_ctx>();
+        h->c.reset(isdf::create_context(atm, natm, bas, nbas, env, nenv));
+        ISDF_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        *out = h.release();
+    });
+}
+
+int isdf_ctx_destroy(isdf_ctx* ctx) {
+    return guarded([&] {
+        if (!ctx) return;
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+    });
+}
+
+int isdf_ctx_info(const isdf_ctx* ctx, int64_t* nao, int32_t* natm, int32_t* nshell) {
+    return guarded([&] {
+        auto& c = ctx_of(const_cast<isdf_ctx*>(ctx));
+        if (nao) *nao = c.nao;
+        if (natm) *natm = c.natm;
+        if (nshell) *nshell = c.nshell;
+    });
+}
+
+int isdf_ctx_ao_atoms(const isdf_ctx* ctx, int32_t* out) {
+    return guarded([&] {
+        auto& c = ctx_of(const_cast<isdf_ctx*>(ctx));
+        std::memcpy(out, c.ao_atom.data(), c.ao_atom.size() * sizeof(int32_t));
+    });
+}
+
+int isdf_eval_ao(isdf_ctx* ctx, const double* xyz, int64_t ng, int32_t dtype, void* values,
+                 void* grad, void* stream) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        if (ng < 0) isdf::fail(isdf::kInvalid, "expected coords[ngrid,3] in Bohr");
+        if (dtype == 0)
+            isdf::eval_ao<double>(c, xyz, ng, static_cast<double*>(values), static_cast<double*>(grad),
+                                  c.nao, as_stream(stream));
+        else if (dtype == 1)
+            isdf::eval_ao<float>(c, xyz, ng, static_cast<float*>(values), static_cast<float*>(grad),
+                                 c.nao, as_stream(stream));
+        else
+            isdf::fail(isdf::kInvalid, "dtype must be 0 (float64) or 1 (float32)");
+    });
+}
+
+int isdf_eval_ao_host(isdf_ctx* ctx, const double* xyz, int64_t ng, double* values, double* grad) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        cudaStream_t s = ctx->stream;
+        if (ng < 0) isdf::fail(isdf::kInvalid, "expected coords[ngrid,3] in Bohr");
+        if (ng == 0 || c.nao == 0) return;
+        isdf::DeviceBuffer<double> dx, dv, dg2;
+        upload(dx, xyz, static_cast<size_t>(3 * ng), s);
+        const size_t nv = static_cast<size_t>(ng) * c.nao;
+        if (values) dv.reset(nv, s);
+        if (grad) dg2.reset(3 * nv, s);
+        isdf::eval_ao<double>(c, dx.get(), ng, values ? dv.get() : nullptr, grad ? dg2.get() : nullptr,
+                              c.nao, s);
+        if (values) ISDF_CUDA(cudaMemcpyAsync(values, dv.get(), nv * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (grad) ISDF_CUDA(cudaMemcpyAsync(grad, dg2.get(), 3 * nv * sizeof(double), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int isdf_evaluate_axis(isdf_ctx* ctx, const double* xyz, int64_t ng, const int32_t* axes,
+                       int32_t naxes, double* out, void* stream) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        if (!axes) isdf::fail(isdf::kInvalid, "axis list must not be empty");
+        isdf::AxisSpec ax = isdf::make_axis_spec(c, axes, naxes);
+        isdf::eval_axis_features<double>(c, xyz, nullptr, ng, ax, out,
+                                         static_cast<int64_t>(naxes) * c.nao, nullptr, nullptr,
+                                         as_stream(stream));
+    });
+}
+
+int isdf_evaluate_axis_host(isdf_ctx* ctx, const double* xyz, int64_t ng, const int32_t* axes,
+                            int32_t naxes, double* out) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        cudaStream_t s = ctx->stream;
+        if (!axes) isdf::fail(isdf::kInvalid, "axis list must not be empty");
+        isdf::AxisSpec ax = isdf::make_axis_spec(c, axes, naxes);
+        if (ng <= 0) return;
+        const int64_t d = static_cast<int64_t>(naxes) * c.nao;
+        isdf::DeviceBuffer<double> dx, dout(static_cast<size_t>(ng * d), s);
+        upload(dx, xyz, static_cast<size_t>(3 * ng), s);
+        isdf::eval_axis_features<double>(c, dx.get(), nullptr, ng, ax, dout.get(), d, nullptr, nullptr, s);
+        ISDF_CUDA(cudaMemcpyAsync(out, dout.get(), ng * d * sizeof(double), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+void isdf_select_args_default(isdf_select_args* a) {
+    if (!a) return;
+    std::memset(a, 0, sizeof(*a));
+    a->algorithm = ISDF_QRCP_DENSE;
+    a->tolerance = 1e-10;
+    a->max_rank = 0;
+    a->batch_size = 128;
+    a->sketch_size = 128;
+    a->oversampling = 16;
+    a->seed = 7;
+    a->precision = ISDF_FP64;
+}
+
+int isdf_select(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz, const double* w,
+                int64_t ng, int64_t* pivots, int64_t capacity, int64_t* npivots,
+                isdf_select_info* info, void* stream) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        isdf::SelectOptions o = options_of(args);
+        if (npivots) *npivots = 0;
+        if (ng < 0) isdf::fail(isdf::kInvalid, "expected points[ngrid,3]");
+        const bool density = o.algorithm == ISDF_RAND_SKETCH_DENSITY || o.algorithm == ISDF_RAND_SKETCH_DENSITY_NORM;
+        if (density && (o.axes.size() != 1 || o.axes[0] != ISDF_AXIS_AO))
+            isdf::fail(isdf::kInvalid, "density Khatri-Rao sketches with non-AO axis features are NYI");
+        isdf::validate_axis_weights(o.axis_weights.empty() ? nullptr : o.axis_weights.data(),
+                                    static_cast<int>(o.axes.size()));
+        std::vector<int64_t> out;
+        cudaStream_t s = as_stream(stream);
+        if (info) std::memset(info, 0, sizeof(*info));
+        switch (o.algorithm) {
+        case ISDF_QRCP_DENSE:
+        case ISDF_QRCP_ONLINE: {
+            isdf::PairQrDiagnostics d;
+            out = isdf::select_pair_qr(c, xyz, w, ng, o, s, &d);
+            if (info) {
+                info->verifications = d.verifications;
+                info->reselections = d.reselections;
+                info->relative_residual = (d.first > 0 && !d.rdiag.empty()) ? d.rdiag.back() / d.first : 0.0;
+            }
+            if (o.debug)
+                std::fprintf(stderr,
+                             "[%s qrcp] rank=%lld max_initial_norm=%.6e relative_residual=%.6e "
+                             "candidate_checks=%lld candidate_reselections=%lld exact_scans=%lld\n",
+                             o.algorithm == ISDF_QRCP_ONLINE ? "online" : "dense",
+                             static_cast<long long>(out.size()), d.first,
+                             info ? info->relative_residual : 0.0,
+                             static_cast<long long>(d.verifications),
+                             static_cast<long long>(d.reselections), static_cast<long long>(d.exact_scans));
+            break;
+        }
+        case ISDF_RAND_SKETCH_QUADRATURE: {
+            isdf::SketchDiagnostics d;
+            out = isdf::select_rand_sketch(c, xyz, w, ng, o, s, &d);
+            if (info) {
+                info->sketch_rows = d.ell;
+                info->numerical_rank = d.numerical_rank;
+                info->relative_residual = d.relative_tail;
+                info->verifications = d.reverified;
+            }
+            if (o.debug)
+                std::fprintf(stderr,
+                             "[rand_sketch:quadrature] rank=%lld sketch_size=%lld oversampling=%lld "
+                             "sketch_relative_frobenius=%.6e numerical_rank=%lld rank_cap=%lld "
+                             "seed=%llu precision=%s space=device\n",
+                             static_cast<long long>(d.rank), static_cast<long long>(d.ell),
+                             static_cast<long long>(o.oversampling), d.relative_tail,
+                             static_cast<long long>(d.numerical_rank), static_cast<long long>(d.cap),
+                             static_cast<unsigned long long>(o.seed), o.precision ? "mixed" : "fp64");
+            break;
+        }
+        case ISDF_CVT:
+        case ISDF_RAND_SKETCH_DENSITY:
+        case ISDF_RAND_SKETCH_DENSITY_NORM:
+            isdf::fail(isdf::kNotImplemented,
+                       "this anchor selection algorithm is outside the B200 hot path (NYI)");
+        default:
+            isdf::fail(isdf::kInvalid, "unknown anchor selection algorithm");
+        }
+        if (static_cast<int64_t>(out.size()) > capacity)
+            isdf::fail(isdf::kInvalid, "pivot buffer is too small");
+        if (!out.empty()) std::memcpy(pivots, out.data(), out.size() * sizeof(int64_t));
+        if (npivots) *npivots = static_cast<int64_t>(out.size());
+    });
+}
+
+int isdf_select_host(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz,
+                     const double* w, int64_t ng, int64_t* pivots, int64_t capacity,
+                     int64_t* npivots, isdf_select_info* info) {
+    int rc = guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        cudaStream_t s = ctx->stream;
+        isdf::DeviceBuffer<double> dx, dw;
+        upload(dx, xyz, static_cast<size_t>(3 * std::max<int64_t>(ng, 0)), s);
+        upload(dw, w, static_cast<size_t>(std::max<int64_t>(ng, 0)), s);
+        const int r = isdf_select(ctx, args, dx.get(), dw.get(), ng, pivots, capacity, npivots, info, s);
+        if (r != ISDF_OK) throw isdf::Error(r, g_last_error);
+    });
+    return rc;
+}
+
+namespace {
+
+void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, const int64_t* anchors,
+              int64_t k, int32_t precision, const double* theta_in, double* theta_out,
+              isdf_fit_info* info, double* l2, double* rel, cudaStream_t s) {
+    auto& c = ctx_of(ctx);
+    DeviceGuard dg(c.device);
+    if (ng < 0 || k < 0) isdf::fail(isdf::kInvalid, "sizes must be nonnegative");
+    if (precision != ISDF_FP64 && precision != ISDF_MIXED)
+        isdf::fail(isdf::kInvalid, "precision must be fp64 or mixed");
+    if (precision == ISDF_MIXED)
+        isdf::fail(isdf::kNotImplemented, "the mixed-precision fit is not available in this build");
+    isdf::KeptPoints kp = isdf::compact_points(xyz, w, ng, s);
+    isdf::DeviceBuffer<int64_t> didx;
+    upload(didx, anchors, static_cast<size_t>(k), s);
+    isdf::DeviceBuffer<double> apts(static_cast<size_t>(3 * std::max<int64_t>(k, 1)), s),
+        aw(std::max<int64_t>(k, 1), s);
+    isdf::gather_points(xyz, w, didx.get(), k, ng, apts.get(), aw.get(), s);
+    isdf::AnchorFactor f = isdf::factor_anchors(c, apts.get(), aw.get(), k, s);
+    const bool have = theta_in != nullptr;
+    double* theta = have ? const_cast<double*>(theta_in) : theta_out;
+    isdf::FitOutput o = isdf::fit_grid(c, xyz, w, kp, f, theta, kp.n, have, s);
+    const double el2 = std::sqrt(o.err2);
+    const double erel = o.exact2 ? el2 / std::sqrt(o.exact2) : (el2 == 0 ? 0.0 : INFINITY);
+    if (info) {
+        std::memset(info, 0, sizeof(*info));
+        info->n_kept = kp.n;
+        info->retained_rank = f.retained;
+        info->condition = f.condition;
+        info->max_abs_physical_coefficient = o.max_abs_coeff;
+        info->pair_l2 = el2;
+        info->pair_relative = erel;
+        for (int64_t a = 0; a < k && a < 64; ++a) info->theta_w[a] = o.theta_w[a];
+    }
+    if (l2) *l2 = el2;
+    if (rel) *rel = erel;
+}
+
+}  // namespace
+
+int isdf_fit(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, const int64_t* anchors,
+             int64_t k, int32_t precision, int32_t want_error, double* theta, isdf_fit_info* info,
+             void* stream) {
+    (void)want_error;
+    return guarded([&] {
+        fit_impl(ctx, xyz, w, ng, anchors, k, precision, nullptr, theta, info, nullptr, nullptr,
+                 as_stream(stream));
+    });
+}
+
+int isdf_fit_host(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng,
+                  const int64_t* anchors, int64_t k, int32_t precision, int32_t want_error,
+                  double* theta_host, isdf_fit_info* info) {
+    (void)want_error;
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        cudaStream_t s = ctx->stream;
+        isdf::DeviceBuffer<double> dx, dw, dt(static_cast<size_t>(std::max<int64_t>(1, k * ng)), s);
+        upload(dx, xyz, static_cast<size_t>(3 * std::max<int64_t>(ng, 0)), s);
+        upload(dw, w, static_cast<size_t>(std::max<int64_t>(ng, 0)), s);
+        isdf_fit_info local{};
+        fit_impl(ctx, dx.get(), dw.get(), ng, anchors, k, precision, nullptr, dt.get(), &local,
+                 nullptr, nullptr, s);
+        if (theta_host && k * local.n_kept)
+            ISDF_CUDA(cudaMemcpyAsync(theta_host, dt.get(), k * local.n_kept * sizeof(double),
+                                      cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        if (info) *info = local;
+    });
+}
+
+int isdf_pair_error(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng,
+                    const int64_t* anchors, int64_t k, const double* theta, double* l2,
+                    double* relative, void* stream) {
+    return guarded([&] {
+        if (!theta) isdf::fail(isdf::kInvalid, "theta is required");
+        fit_impl(ctx, xyz, w, ng, anchors, k, ISDF_FP64, theta, nullptr, nullptr, l2, relative,
+                 as_stream(stream));
+    });
+}
+
+int isdf_pair_error_terms(int64_t n, int64_t k, const double* q, const double* H, const double* X,
+                          const double* M, const double* w, double* out, void* stream) {
+    return guarded([&] {
+        if (n < 0 || k < 0 || !out) isdf::fail(isdf::kInvalid, "invalid pair error terms");
+        double acc[2] = {0, 0};
+        if (n > 0) isdf::pair_error_terms(n, k, q, H, X, M, w, acc, as_stream(stream));
+        const double a = std::sqrt(std::max(acc[0], 0.0));
+        out[0] = a;
+        out[1] = acc[1] ? a / std::sqrt(acc[1]) : (a == 0 ? 0.0 : INFINITY);
+    });
+}
+
+}  // extern "C"

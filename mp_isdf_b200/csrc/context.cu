@@ -1,0 +1,427 @@
+// Context construction (libcint ATM/BAS/ENV tables -> device shell table) and
+// the fused per-contracted-shell AO evaluator.
+//
+// Reference behaviour restated (mikovtun/mp_isdf):
+//   table validation and shell metadata  cpp/src/ao_eval.cpp:54-65, 94-121
+//   cartesian order x^l, x^(l-1)y, ...    cpp/src/ao_eval.cpp:30-44
+//   s/p spherical scaling                 cpp/src/ao_eval.cpp:132-138
+//   value / gradient formulas             cpp/src/ao_eval.cpp:207-249
+//   value layout [p*nao+ao], gradient layout [(axis*Ng+p)*nao+ao]
+//                                         cpp/include/ao_eval.hpp:83-99
+#include "isdf_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <memory>
+#include <type_traits>
+
+namespace isdf {
+
+// ------------------------------------------------------------------------------
+// cartesian -> real spherical transform
+// ------------------------------------------------------------------------------
+namespace {
+
+double fact(int n) { double r = 1; for (int i = 2; i <= n; ++i) r *= i; return r; }
+double binom(int n, int k) {
+    if (k < 0 || k > n) return 0.0;
+    return fact(n) / (fact(k) * fact(n - k));
+}
+
+// Index of the cartesian monomial (lx, ly, lz) in libcint order.
+int cart_index(int l, int lx, int ly, int lz) {
+    (void)ly;
+    int idx = 0;
+    for (int x = l; x > lx; --x) idx += l - x + 1;
+    return idx + lz;
+}
+
+}  // namespace
+
+// Rows m = -l..l of r^l Y_lm (unit-sphere normalised real harmonics without the
+// Condon-Shortley phase) expanded in cartesian monomials, from the closed-form
+// expansion of real regular solid harmonics (Helgaker, Jorgensen & Olsen,
+// "Molecular Electronic-Structure Theory", eqs. 6.4.47-6.4.50) times
+// sqrt((2l+1)/4pi).  l = 0 is 1/sqrt(4pi) and l = 1 keeps the (x, y, z)
+// order scaled by sqrt(3/4pi), as the reference does for libcint's s/p path.
+std::vector<double> c2s_matrix(int l) {
+    const int nc = (l + 1) * (l + 2) / 2, ns = 2 * l + 1;
+    std::vector<double> t(static_cast<size_t>(ns) * nc, 0.0);
+    const double pi = 3.14159265358979323846;
+    if (l == 0) { t[0] = 1.0 / std::sqrt(4 * pi); return t; }
+    if (l == 1) {
+        for (int i = 0; i < 3; ++i) t[i * 3 + i] = std::sqrt(3.0 / (4 * pi));
+        return t;
+    }
+    const double pref = std::sqrt((2 * l + 1) / (4 * pi));
+    for (int m = -l; m <= l; ++m) {
+        const int am = std::abs(m);
+        const double norm = 1.0 / (std::pow(2.0, am) * fact(l)) *
+                            std::sqrt(2.0 * fact(l + am) * fact(l - am) / (m == 0 ? 2.0 : 1.0));
+        const int wm = m < 0 ? 1 : 0;  // 2*v_m
+        for (int tt = 0; tt <= (l - am) / 2; ++tt)
+            for (int u = 0; u <= tt; ++u)
+                for (int w = wm; w <= am; w += 2) {   // w = 2v
+                    const int sgn_exp = tt + (w - wm) / 2;
+                    const double c = ((sgn_exp & 1) ? -1.0 : 1.0) * std::pow(0.25, tt) *
+                                     binom(l, tt) * binom(l - tt, am + tt) * binom(tt, u) *
+                                     binom(am, w);
+                    const int lx = 2 * tt + am - 2 * u - w;
+                    const int ly = 2 * u + w;
+                    const int lz = l - 2 * tt - am;
+                    if (lx < 0 || ly < 0 || lz < 0 || c == 0) continue;
+                    t[static_cast<size_t>(m + l) * nc + cart_index(l, lx, ly, lz)] += pref * norm * c;
+                }
+    }
+    return t;
+}
+
+// ------------------------------------------------------------------------------
+// constant tables
+// ------------------------------------------------------------------------------
+__host__ __device__ constexpr int c2s_offset(int l) {
+    int off = 0;
+    for (int i = 0; i < l; ++i) off += (2 * i + 1) * (i + 1) * (i + 2) / 2;
+    return off;
+}
+constexpr int kC2sSize = c2s_offset(kMaxL + 1);
+
+__constant__ double c_c2s[kC2sSize];
+__constant__ float c_c2sf[kC2sSize];
+
+namespace {
+
+void upload_c2s_once(int device) {
+    static bool done[64] = {false};
+    if (device < 64 && done[device]) return;
+    std::vector<double> all;
+    for (int l = 0; l <= kMaxL; ++l) {
+        auto t = c2s_matrix(l);
+        all.insert(all.end(), t.begin(), t.end());
+    }
+    std::vector<float> allf(all.begin(), all.end());
+    ISDF_CUDA(cudaMemcpyToSymbol(c_c2s, all.data(), all.size() * sizeof(double)));
+    ISDF_CUDA(cudaMemcpyToSymbol(c_c2sf, allf.data(), allf.size() * sizeof(float)));
+    if (device < 64) done[device] = true;
+}
+
+template <class T> __device__ __forceinline__ T c2s(int idx);
+template <> __device__ __forceinline__ double c2s<double>(int idx) { return c_c2s[idx]; }
+template <> __device__ __forceinline__ float c2s<float>(int idx) { return c_c2sf[idx]; }
+
+__device__ __forceinline__ double dexp(double x) { return exp(x); }
+__device__ __forceinline__ float dexp(float x) { return __expf(x); }
+
+}  // namespace
+
+Context::~Context() {
+    cudaFree(d_shells);
+    cudaFree(d_exp);
+    cudaFree(d_coef);
+    cudaFree(d_expf);
+    cudaFree(d_coeff);
+    cudaFree(d_ao_atom);
+}
+
+Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nbas,
+                        const double* env, int64_t nenv) {
+    require(natm >= 0 && nbas >= 0 && nenv >= 20, "invalid libcint ATM/BAS/ENV table sizes");
+    auto c = std::make_unique<Context>();
+    ISDF_CUDA(cudaGetDevice(&c->device));
+    c->natm = natm;
+    c->atm.assign(atm, atm + static_cast<size_t>(natm) * 6);
+    c->bas.assign(bas, bas + static_cast<size_t>(nbas) * 8);
+    c->env.assign(env, env + nenv);
+    auto range_ok = [&](int64_t off, int64_t len) {
+        return off >= 0 && len >= 0 && off <= nenv && len <= nenv - off;
+    };
+    std::vector<double> exps, coefs;
+    int64_t nao = 0;
+    for (int a = 0; a < natm; ++a) {
+        const int pc = atm[6 * a + 1];
+        require(range_ok(pc, 3), "libcint table contains an invalid ENV offset");
+        c->atom_xyz.insert(c->atom_xyz.end(), env + pc, env + pc + 3);
+    }
+    for (int i = 0; i < nbas; ++i) {
+        const int32_t* b = bas + 8 * i;
+        const int atom = b[0], l = b[1], np = b[2], nc = b[3];
+        require(atom >= 0 && atom < natm && l >= 0 && np > 0 && nc > 0 && np <= 64 && nc <= 64,
+                "invalid libcint basis shell");
+        if (l > kMaxL) fail(kNotImplemented, "angular momentum above l=6 is not supported");
+        require(range_ok(b[5], np) && range_ok(b[6], static_cast<int64_t>(np) * nc),
+                "libcint table contains an invalid ENV offset");
+        ShellDesc s{};
+        s.l = l; s.nprim = np; s.nctr = nc;
+        if (nao + static_cast<int64_t>(2 * l + 1) * nc > std::numeric_limits<int>::max())
+            fail(kOverflow, "AO or transformation index exceeds int range");
+        s.ao_off = static_cast<int>(nao);
+        s.prim_off = static_cast<int>(exps.size());
+        s.coef_off = static_cast<int>(coefs.size());
+        s.atom = atom;
+        const double* xyz = &c->atom_xyz[3 * atom];
+        s.x = xyz[0]; s.y = xyz[1]; s.z = xyz[2];
+        exps.insert(exps.end(), env + b[5], env + b[5] + np);
+        coefs.insert(coefs.end(), env + b[6], env + b[6] + static_cast<int64_t>(np) * nc);
+        c->shells.push_back(s);
+        for (int k = 0; k < (2 * l + 1) * nc; ++k) c->ao_atom.push_back(atom);
+        nao += static_cast<int64_t>(2 * l + 1) * nc;
+        c->lmax = std::max(c->lmax, l);
+    }
+    c->nao = static_cast<int>(nao);
+    c->nshell = static_cast<int>(c->shells.size());
+    upload_c2s_once(c->device);
+    auto up = [](auto*& dst, const auto& src) {
+        using V = std::remove_pointer_t<std::remove_reference_t<decltype(dst)>>;
+        if (src.empty()) return;
+        ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&dst), src.size() * sizeof(V)));
+        ISDF_CUDA(cudaMemcpy(dst, src.data(), src.size() * sizeof(V), cudaMemcpyHostToDevice));
+    };
+    std::vector<float> expf_(exps.begin(), exps.end()), coeff_(coefs.begin(), coefs.end());
+    up(c->d_shells, c->shells);
+    up(c->d_exp, exps);
+    up(c->d_coef, coefs);
+    up(c->d_expf, expf_);
+    up(c->d_coeff, coeff_);
+    up(c->d_ao_atom, c->ao_atom);
+    return c.release();
+}
+
+// ------------------------------------------------------------------------------
+// AO kernels
+// ------------------------------------------------------------------------------
+namespace {
+
+template <int L>
+struct Cart {
+    static constexpr int nc = (L + 1) * (L + 2) / 2;
+    // libcint order: for lx = L..0, for lz = 0..L-lx: ly = L-lx-lz
+    static __host__ __device__ constexpr int lx(int c) {
+        int x = L;
+        while (c >= L - x + 1) { c -= L - x + 1; --x; }
+        return x;
+    }
+    static __host__ __device__ constexpr int lz(int c) {
+        int x = L;
+        while (c >= L - x + 1) { c -= L - x + 1; --x; }
+        return c;
+    }
+    static __host__ __device__ constexpr int ly(int c) { return L - lx(c) - lz(c); }
+};
+
+// Per-thread evaluation of one contracted shell of angular momentum L at one
+// point; `sink.put<C>(ao, v)` receives component C (0 value, 1..3 gradient).
+template <class T, int L, bool GRAD, class Sink>
+__device__ __forceinline__ void eval_shell(const ShellDesc& b, double dxd, double dyd, double dzd,
+                                           const T* __restrict__ exps, const T* __restrict__ coefs,
+                                           Sink& sink) {
+    constexpr int NC = Cart<L>::nc;
+    constexpr int NS = 2 * L + 1;
+    constexpr int OFF = c2s_offset(L);
+    const T x = static_cast<T>(dxd), y = static_cast<T>(dyd), z = static_cast<T>(dzd);
+    const T r2 = static_cast<T>(dxd * dxd + dyd * dyd + dzd * dzd);
+    T px[L + 1], py[L + 1], pz[L + 1];
+    px[0] = py[0] = pz[0] = T(1);
+#pragma unroll
+    for (int i = 1; i <= L; ++i) { px[i] = px[i - 1] * x; py[i] = py[i - 1] * y; pz[i] = pz[i - 1] * z; }
+    T v[NS], vx[NS], vy[NS], vz[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) { v[s] = vx[s] = vy[s] = vz[s] = T(0); }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const int ax = Cart<L>::lx(c), ay = Cart<L>::ly(c), az = Cart<L>::lz(c);
+        const T m = px[ax] * py[ay] * pz[az];
+        T mx = T(0), my = T(0), mz = T(0);
+        if (GRAD) {
+            if (ax) mx = T(ax) * px[ax - 1] * py[ay] * pz[az];
+            if (ay) my = T(ay) * px[ax] * py[ay - 1] * pz[az];
+            if (az) mz = T(az) * px[ax] * py[ay] * pz[az - 1];
+        }
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const T t = c2s<T>(OFF + s * NC + c);
+            v[s] += t * m;
+            if (GRAD) { vx[s] += t * mx; vy[s] += t * my; vz[s] += t * mz; }
+        }
+    }
+    for (int g0 = 0; g0 < b.nctr; g0 += kMaxCtrGroup) {
+        const int ng = min(kMaxCtrGroup, b.nctr - g0);
+        T R[kMaxCtrGroup], Rp[kMaxCtrGroup];
+#pragma unroll
+        for (int j = 0; j < kMaxCtrGroup; ++j) { R[j] = T(0); Rp[j] = T(0); }
+        for (int p = 0; p < b.nprim; ++p) {
+            const T a = exps[b.prim_off + p];
+            const T arg = a * r2;
+            if (arg > T(kExpCut)) continue;
+            const T e = dexp(-arg);
+#pragma unroll
+            for (int j = 0; j < kMaxCtrGroup; ++j) {
+                if (j < ng) {
+                    const T cc = coefs[b.coef_off + (g0 + j) * b.nprim + p] * e;
+                    R[j] += cc;
+                    if (GRAD) Rp[j] -= a * cc;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kMaxCtrGroup; ++j) {
+            if (j < ng) {
+                const int ao0 = b.ao_off + (g0 + j) * NS;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    sink.template put<0>(ao0 + s, R[j] * v[s]);
+                    if (GRAD) {
+                        const T two_rp = T(2) * Rp[j] * v[s];
+                        sink.template put<1>(ao0 + s, R[j] * vx[s] + x * two_rp);
+                        sink.template put<2>(ao0 + s, R[j] * vy[s] + y * two_rp);
+                        sink.template put<3>(ao0 + s, R[j] * vz[s] + z * two_rp);
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <class T, bool GRAD, class Sink>
+__device__ __forceinline__ void eval_shell_dispatch(const ShellDesc& b, double dx, double dy,
+                                                    double dz, const T* exps, const T* coefs,
+                                                    Sink& sink) {
+    switch (b.l) {
+    case 0: eval_shell<T, 0, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
+    case 1: eval_shell<T, 1, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
+    case 2: eval_shell<T, 2, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
+    case 3: eval_shell<T, 3, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
+    case 4: eval_shell<T, 4, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
+    case 5: eval_shell<T, 5, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
+    default: eval_shell<T, 6, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
+    }
+}
+
+template <class T>
+struct RawSink {
+    T* val; T* grad; int64_t p, n, ld; bool want_val;
+    template <int C> __device__ __forceinline__ void put(int ao, T v) {
+        if (C == 0) { if (want_val) val[p * ld + ao] = v; }
+        else grad[((C - 1) * n + p) * ld + ao] = v;
+    }
+};
+
+template <class T>
+struct AxisSink {
+    T* out; int64_t p, ld; const AxisSpec* ax; const int* off; double sq[4]; bool count;
+    template <int C> __device__ __forceinline__ void put(int ao, T v) {
+        if (!((ax->need_mask >> C) & 1)) return;
+        if (count) sq[C] += static_cast<double>(v) * static_cast<double>(v);
+        for (int a = 0; a < ax->naxes; ++a)
+            if (ax->comp[a] == C) out[p * ld + off[a] + ao] = static_cast<T>(ax->scale[a] * static_cast<double>(v));
+    }
+};
+
+constexpr int kPtsPerBlock = 32;
+constexpr int kShellLanes = 4;
+
+template <class T, bool GRAD>
+__global__ void __launch_bounds__(kPtsPerBlock * kShellLanes)
+ao_raw_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restrict__ exps,
+              const T* __restrict__ coefs, const double* __restrict__ pts, int64_t n,
+              T* val, T* grad, int64_t ld, bool want_val) {
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * kPtsPerBlock + threadIdx.x;
+    if (p >= n) return;
+    const double px = pts[3 * p], py = pts[3 * p + 1], pz = pts[3 * p + 2];
+    RawSink<T> sink{val, grad, p, n, ld, want_val};
+    for (int sh = threadIdx.y; sh < nshell; sh += kShellLanes) {
+        const ShellDesc b = shells[sh];
+        eval_shell_dispatch<T, GRAD>(b, px - b.x, py - b.y, pz - b.z, exps, coefs, sink);
+    }
+}
+
+template <class T, bool GRAD>
+__global__ void __launch_bounds__(kPtsPerBlock * kShellLanes)
+ao_axis_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restrict__ exps,
+               const T* __restrict__ coefs, const double* __restrict__ pts,
+               const int64_t* __restrict__ index, int64_t n, AxisSpec ax, T* out, int64_t ld,
+               double* sumsq, const double* __restrict__ weights, int nao) {
+    __shared__ double red[kPtsPerBlock * kShellLanes][4];
+    __shared__ int off[16];
+    const int tid = threadIdx.y * kPtsPerBlock + threadIdx.x;
+    if (tid < ax.naxes) off[tid] = tid * nao;
+    __syncthreads();
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * kPtsPerBlock + threadIdx.x;
+    AxisSink<T> sink{out, p, ld, &ax, off, {0, 0, 0, 0}, false};
+    if (p < n) {
+        const int64_t gi = index ? index[p] : p;
+        const double px = pts[3 * gi], py = pts[3 * gi + 1], pz = pts[3 * gi + 2];
+        sink.count = sumsq != nullptr && (weights == nullptr || weights[gi] != 0.0);
+        for (int sh = threadIdx.y; sh < nshell; sh += kShellLanes) {
+            const ShellDesc b = shells[sh];
+            eval_shell_dispatch<T, GRAD>(b, px - b.x, py - b.y, pz - b.z, exps, coefs, sink);
+        }
+    }
+    if (sumsq) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) red[tid][c] = sink.sq[c];
+        __syncthreads();
+        for (int stride = kPtsPerBlock * kShellLanes / 2; stride > 0; stride >>= 1) {
+            if (tid < stride)
+                for (int c = 0; c < 4; ++c) red[tid][c] += red[tid + stride][c];
+            __syncthreads();
+        }
+        if (tid < 4 && ((ax.need_mask >> tid) & 1)) atomicAdd(&sumsq[tid], red[0][tid]);
+    }
+}
+
+template <class T> const T* exps_of(const Context& c);
+template <> const double* exps_of<double>(const Context& c) { return c.d_exp; }
+template <> const float* exps_of<float>(const Context& c) { return c.d_expf; }
+template <class T> const T* coefs_of(const Context& c);
+template <> const double* coefs_of<double>(const Context& c) { return c.d_coef; }
+template <> const float* coefs_of<float>(const Context& c) { return c.d_coeff; }
+
+}  // namespace
+
+template <class T>
+void eval_ao(const Context& c, const double* pts, int64_t n, T* out_val, T* out_grad,
+             int64_t ld, cudaStream_t s) {
+    if (n == 0 || c.nao == 0) return;
+    dim3 block(kPtsPerBlock, kShellLanes);
+    const int64_t nb = (n + kPtsPerBlock - 1) / kPtsPerBlock;
+    require(nb < (1ll << 31), "too many grid points for one launch");
+    if (out_grad)
+        ao_raw_kernel<T, true><<<static_cast<unsigned>(nb), block, 0, s>>>(
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, n, out_val, out_grad, ld,
+            out_val != nullptr);
+    else
+        ao_raw_kernel<T, false><<<static_cast<unsigned>(nb), block, 0, s>>>(
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, n, out_val, nullptr, ld, true);
+    ISDF_LAUNCH_CHECK();
+}
+
+template <class T>
+void eval_axis_features(const Context& c, const double* pts, const int64_t* index, int64_t n,
+                        const AxisSpec& ax, T* out, int64_t ld, double* sumsq,
+                        const double* weights, cudaStream_t s) {
+    if (n == 0 || c.nao == 0) return;
+    require(ax.naxes > 0 && ax.naxes <= 16, "between 1 and 16 axes are supported");
+    dim3 block(kPtsPerBlock, kShellLanes);
+    const int64_t nb = (n + kPtsPerBlock - 1) / kPtsPerBlock;
+    require(nb < (1ll << 31), "too many grid points for one launch");
+    const bool grad = (ax.need_mask & 0xE) != 0;
+    if (grad)
+        ao_axis_kernel<T, true><<<static_cast<unsigned>(nb), block, 0, s>>>(
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, index, n, ax, out, ld,
+            sumsq, weights, c.nao);
+    else
+        ao_axis_kernel<T, false><<<static_cast<unsigned>(nb), block, 0, s>>>(
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, index, n, ax, out, ld,
+            sumsq, weights, c.nao);
+    ISDF_LAUNCH_CHECK();
+}
+
+template void eval_ao<double>(const Context&, const double*, int64_t, double*, double*, int64_t, cudaStream_t);
+template void eval_ao<float>(const Context&, const double*, int64_t, float*, float*, int64_t, cudaStream_t);
+template void eval_axis_features<double>(const Context&, const double*, const int64_t*, int64_t,
+                                         const AxisSpec&, double*, int64_t, double*, const double*, cudaStream_t);
+template void eval_axis_features<float>(const Context&, const double*, const int64_t*, int64_t,
+                                        const AxisSpec&, float*, int64_t, double*, const double*, cudaStream_t);
+
+}  // namespace isdf

@@ -1,0 +1,363 @@
+// Interpolation-vector fit and pair-space error.
+//
+// Reference (mikovtun/mp_isdf python/isdf.py:238-263, _physical_pair_refit):
+//   C = anchor AO pairs (k x nao^2), U S V^T = svd(C^T), keep s > 1e-12 s_0,
+//   X = V S^-1 U^T p_g for every grid pair column p_g = phi_g (x) phi_g,
+//   Theta[:, g] = X / w_anchor.
+// Without forming any grid pair column: C p_g = (Phi_a phi_g)^2 =: h_g and
+// C C^T = (Phi_a Phi_a^T)^2 =: M (Hadamard squares), so
+//   X_g = V_r S_r^-2 V_r^T h_g = T h_g,
+// with V, S the SVD of C^T computed accurately from the R factor of an
+// explicit CGS2 QR of C^T (C^T = Q R, svd(R) = U_r S V^T).
+// Pair-space error (python/isdf.py:154-191), per grid point:
+//   |p_g - C^T X_g|^2 = q_g^2 - 2 X_g.h_g + X_g^T M X_g,  q_g = |phi_g|^2.
+#include "isdf_fit.h"
+#include "isdf_reduce.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+
+namespace isdf {
+namespace {
+
+__global__ void transpose_kernel(const double* __restrict__ a, int64_t rows, int64_t cols,
+                                 double* __restrict__ at) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= rows * cols) return;
+    const int64_t r = i / cols, c = i % cols;
+    at[c * rows + r] = a[i];
+}
+
+__global__ void hadamard_square_kernel(const double* __restrict__ a, int64_t n, double* __restrict__ b) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i] * a[i];
+}
+
+__global__ void gather_points_kernel(const double* __restrict__ pts, const double* __restrict__ w,
+                                     const int64_t* __restrict__ idx, int64_t n,
+                                     double* __restrict__ out_pts, double* __restrict__ out_w,
+                                     int64_t npts_total, int* __restrict__ bad) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t g = idx[i];
+    if (g < 0 || g >= npts_total) { atomicOr(bad, 1); return; }
+    out_pts[3 * i] = pts[3 * g];
+    out_pts[3 * i + 1] = pts[3 * g + 1];
+    out_pts[3 * i + 2] = pts[3 * g + 2];
+    if (out_w) out_w[i] = w[g];
+}
+
+// One-sided Jacobi SVD of the k x k column-major matrix A (overwritten by
+// U*S), accumulating the right singular vectors in V (column-major).  One CTA,
+// round-robin (circle method) pair ordering, warps own pairs.
+__global__ void __launch_bounds__(1024)
+jacobi_svd_kernel(double* A, double* V, int k, int max_sweeps, int* sweeps_out) {
+    const int kp = k + (k & 1);
+    const int lane = threadIdx.x % 32, wid = threadIdx.x / 32, nw = blockDim.x / 32;
+    for (int i = threadIdx.x; i < k * k; i += blockDim.x) V[i] = (i % k == i / k) ? 1.0 : 0.0;
+    __shared__ int rotated;
+    const double eps = 2.220446049250313e-16;
+    int sweep = 0;
+    for (; sweep < max_sweeps; ++sweep) {
+        if (threadIdx.x == 0) rotated = 0;
+        __syncthreads();
+        for (int round = 0; round < kp - 1; ++round) {
+            for (int pr = wid; pr < kp / 2; pr += nw) {
+                // circle method: player 0 fixed, others rotate
+                int a = pr == 0 ? 0 : 1 + (pr - 1 + round) % (kp - 1);
+                int b = 1 + (kp - 2 - pr + round) % (kp - 1);
+                if (pr == 0) b = 1 + (kp - 2 + round) % (kp - 1);
+                if (a >= k || b >= k || a == b) continue;
+                if (a > b) { int t = a; a = b; b = t; }
+                double alpha = 0, beta = 0, gamma = 0;
+                for (int r = lane; r < k; r += 32) {
+                    const double x = A[a * k + r], y = A[b * k + r];
+                    alpha += x * x; beta += y * y; gamma += x * y;
+                }
+                alpha = warp_sum(alpha); beta = warp_sum(beta); gamma = warp_sum(gamma);
+                alpha = __shfl_sync(0xffffffffu, alpha, 0);
+                beta = __shfl_sync(0xffffffffu, beta, 0);
+                gamma = __shfl_sync(0xffffffffu, gamma, 0);
+                if (gamma == 0.0 || fabs(gamma) <= eps * sqrt(alpha * beta)) continue;
+                const double zeta = (beta - alpha) / (2.0 * gamma);
+                const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+                for (int r = lane; r < k; r += 32) {
+                    const double x = A[a * k + r], y = A[b * k + r];
+                    A[a * k + r] = cs * x - sn * y;
+                    A[b * k + r] = sn * x + cs * y;
+                    const double vx = V[a * k + r], vy = V[b * k + r];
+                    V[a * k + r] = cs * vx - sn * vy;
+                    V[b * k + r] = sn * vx + cs * vy;
+                }
+                if (lane == 0) rotated = 1;
+            }
+            __syncthreads();
+        }
+        __syncthreads();
+        if (!rotated) break;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sweeps_out[0] = sweep;
+}
+
+// s[j] = |A[:, j]|
+__global__ void column_norms_kernel(const double* __restrict__ A, int k, double* __restrict__ s) {
+    const int j = blockIdx.x;
+    double acc = 0;
+    for (int r = threadIdx.x; r < k; r += 32) acc += A[j * k + r] * A[j * k + r];
+    acc = warp_sum(acc);
+    if (threadIdx.x == 0) s[j] = sqrt(acc);
+}
+
+// T[a][b] = sum_j V[a,j] V[b,j] / s_j^2 over retained j  (V column-major)
+__global__ void pinv_from_svd_kernel(const double* __restrict__ V, const double* __restrict__ s,
+                                     int k, double cutoff, double power, double* __restrict__ T) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k * k) return;
+    const int a = i / k, b = i % k;
+    double acc = 0;
+    for (int j = 0; j < k; ++j)
+        if (s[j] > cutoff) acc += V[j * k + a] * V[j * k + b] / pow(s[j], power);
+    T[i] = acc;
+}
+
+// Per point: Theta, pair-error terms, Theta.w and max |X|.
+template <bool HAVE_THETA>
+__global__ void fit_point_kernel(const double* __restrict__ H, const double* __restrict__ X,
+                                 const double* __restrict__ Y, const double* __restrict__ q,
+                                 const double* __restrict__ w, int64_t b, int k,
+                                 const double* __restrict__ wa, double* __restrict__ theta,
+                                 int64_t ldt, int64_t g0, double* __restrict__ acc) {
+    __shared__ double sh[8];
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    double e = 0, ex = 0, mx = 0;
+    if (g < b) {
+        const double* h = H + g * k;
+        const double* x = X + g * k;
+        const double* y = Y + g * k;
+        double xh = 0, xy = 0;
+        for (int a = 0; a < k; ++a) {
+            xh += x[a] * h[a];
+            xy += x[a] * y[a];
+            mx = fmax(mx, fabs(x[a]));
+            if (!HAVE_THETA) theta[a * ldt + g0 + g] = x[a] / wa[a];
+        }
+        const double aw = fabs(w[g]);
+        e = aw * (q[g] * q[g] - 2.0 * xh + xy);
+        ex = aw * q[g] * q[g];
+    }
+    e = block_sum<256>(e, sh);
+    ex = block_sum<256>(ex, sh);
+    double m = mx;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    __shared__ double msh[8];
+    if (threadIdx.x % 32 == 0) msh[threadIdx.x / 32] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 8; ++i) m = fmax(m, msh[i]);
+        atomicAdd(&acc[0], e);
+        atomicAdd(&acc[1], ex);
+        // non-negative doubles order like their bit patterns
+        atomicMax(reinterpret_cast<unsigned long long*>(&acc[2]),
+                  static_cast<unsigned long long>(__double_as_longlong(m)));
+    }
+}
+
+// tw[a] += sum_g Theta[a, g] w_g over the chunk (one block per anchor row)
+__global__ void theta_dot_w_kernel(const double* __restrict__ theta, int64_t ldt, int64_t g0,
+                                   int64_t b, const double* __restrict__ w, double* __restrict__ tw) {
+    __shared__ double sh[8];
+    const int a = blockIdx.y;
+    double acc = 0;
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < b;
+         g += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        acc += theta[a * ldt + g0 + g] * w[g];
+    acc = block_sum<256>(acc, sh);
+    if (threadIdx.x == 0) atomicAdd(&tw[a], acc);
+}
+
+// X[g][a] = Theta[a, g0+g] * wa[a]
+__global__ void theta_to_x_kernel(const double* __restrict__ theta, int64_t ldt, int64_t g0,
+                                  int64_t b, int k, const double* __restrict__ wa,
+                                  double* __restrict__ X) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= b * k) return;
+    const int64_t g = i / k;
+    const int a = static_cast<int>(i % k);
+    X[i] = theta[a * ldt + g0 + g] * wa[a];
+}
+
+unsigned blocks_for(int64_t n, int t = 256) { return static_cast<unsigned>((n + t - 1) / t); }
+
+}  // namespace
+
+AnchorFactor factor_anchors(const Context& c, const double* anchor_pts, const double* anchor_w,
+                            int64_t k, cudaStream_t s) {
+    AnchorFactor f;
+    f.k = k;
+    const int64_t nao = c.nao;
+    if (k == 0) return f;
+    require(k <= 4096, "more than 4096 anchors are not supported by the fit");
+    f.phi_a.reset(static_cast<size_t>(k * nao), s);
+    f.phi_aT.reset(static_cast<size_t>(k * nao), s);
+    f.M.reset(static_cast<size_t>(k * k), s);
+    f.T.reset(static_cast<size_t>(k * k), s);
+    f.wa.reset(k, s);
+    ISDF_CUDA(cudaMemcpyAsync(f.wa.get(), anchor_w, k * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    eval_ao<double>(c, anchor_pts, k, f.phi_a.get(), nullptr, nao, s);
+    transpose_kernel<<<blocks_for(k * nao), 256, 0, s>>>(f.phi_a.get(), k, nao, f.phi_aT.get());
+    ISDF_LAUNCH_CHECK();
+    DeviceBuffer<double> S(static_cast<size_t>(k * k), s);
+    gemm_f64(k, k, nao, f.phi_a.get(), nao, 0, f.phi_aT.get(), k, 0, S.get(), k, 0, 1, false, s);
+    hadamard_square_kernel<<<blocks_for(k * k), 256, 0, s>>>(S.get(), k * k, f.M.get());
+    ISDF_LAUNCH_CHECK();
+
+    // R factor of C^T (nao^2 x k) by CGS2, or the Gram matrix M when C^T is too large.
+    const int64_t m = nao * nao;
+    std::vector<double> R(static_cast<size_t>(k * k), 0.0);   // column-major
+    double power = 2.0;
+    DeviceBuffer<double> A(static_cast<size_t>(k * k), s), V(static_cast<size_t>(k * k), s);
+    if (m * k <= (int64_t(1) << 30)) {
+        DeviceBuffer<double> Q(static_cast<size_t>(m * k), s), a(m, s), r(m, s), t(k, s), nrm(1, s);
+        std::vector<double> ht(k);
+        for (int64_t j = 0; j < k; ++j) {
+            pair_vector(f.phi_a.get() + j * nao, nao, 1.0, a.get(), s);
+            const double* src = a.get();
+            for (int pass = 0; pass < 2; ++pass) {
+                t.zero(s);
+                nrm.zero(s);
+                rows_dot(Q.get(), static_cast<int>(j), m, src, t.get(), s);
+                rows_axpy(Q.get(), static_cast<int>(j), m, t.get(), src, r.get(), nrm.get(), s);
+                if (j) {
+                    ISDF_CUDA(cudaMemcpyAsync(ht.data(), t.get(), j * sizeof(double), cudaMemcpyDeviceToHost, s));
+                    ISDF_CUDA(cudaStreamSynchronize(s));
+                    for (int64_t i = 0; i < j; ++i) R[j * k + i] += ht[i];
+                }
+                src = r.get();
+            }
+            double n2 = 0;
+            ISDF_CUDA(cudaMemcpyAsync(&n2, nrm.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+            ISDF_CUDA(cudaStreamSynchronize(s));
+            const double rjj = std::sqrt(n2);
+            R[j * k + j] = rjj;
+            scale_copy(r.get(), rjj > 0 ? 1.0 / rjj : 0.0, m, Q.get() + j * m, s);
+        }
+        ISDF_CUDA(cudaMemcpyAsync(A.get(), R.data(), R.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        power = 2.0;   // T = V S^-2 V^T from the SVD of R
+    } else {
+        ISDF_CUDA(cudaMemcpyAsync(A.get(), f.M.get(), k * k * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        power = 1.0;   // singular values of M are s^2
+        f.gram_fallback = true;
+    }
+    DeviceBuffer<int> sweeps(1, s);
+    jacobi_svd_kernel<<<1, 1024, 0, s>>>(A.get(), V.get(), static_cast<int>(k), 60, sweeps.get());
+    ISDF_LAUNCH_CHECK();
+    DeviceBuffer<double> sv(k, s);
+    column_norms_kernel<<<static_cast<unsigned>(k), 32, 0, s>>>(A.get(), static_cast<int>(k), sv.get());
+    ISDF_LAUNCH_CHECK();
+    std::vector<double> hs(k);
+    ISDF_CUDA(cudaMemcpyAsync(hs.data(), sv.get(), k * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    if (f.gram_fallback)
+        for (auto& x : hs) x = std::sqrt(std::max(x, 0.0));
+    f.sv = hs;
+    std::sort(f.sv.begin(), f.sv.end(), std::greater<double>());
+    const double s0 = f.sv.empty() ? 0.0 : f.sv.front();
+    const double cutoff = 1e-12 * s0;
+    f.retained = 0;
+    for (double x : f.sv) f.retained += x > cutoff;
+    f.condition = (!f.sv.empty() && f.sv.back() > 0) ? s0 / f.sv.back() : std::numeric_limits<double>::infinity();
+    // singular values in A's column order (power 1 for the Gram fallback)
+    const double dev_cut = f.gram_fallback ? cutoff * cutoff : cutoff;
+    pinv_from_svd_kernel<<<blocks_for(k * k), 256, 0, s>>>(V.get(), sv.get(), static_cast<int>(k),
+                                                           dev_cut, power, f.T.get());
+    ISDF_LAUNCH_CHECK();
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    return f;
+}
+
+FitOutput fit_grid(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
+                   const AnchorFactor& f, double* theta, int64_t ldt, bool have_theta,
+                   cudaStream_t s) {
+    FitOutput out;
+    const int64_t n = kp.n, k = f.k, nao = c.nao;
+    out.theta_w.assign(k, 0.0);
+    if (n == 0 || k == 0) return out;
+    const int64_t chunk = std::max<int64_t>(256, std::min<int64_t>(n, (int64_t(1) << 26) / nao));
+    DeviceBuffer<double> phi(static_cast<size_t>(chunk * nao), s), q(chunk, s), G(chunk * k, s),
+        H(chunk * k, s), X(chunk * k, s), Y(chunk * k, s), cpts(chunk * 3, s), cw(chunk, s),
+        acc(3, s), tw(k, s);
+    DeviceBuffer<int> bad(1, s);
+    acc.zero(s);
+    tw.zero(s);
+    bad.zero(s);
+    for (int64_t g0 = 0; g0 < n; g0 += chunk) {
+        const int64_t b = std::min(chunk, n - g0);
+        gather_points_kernel<<<blocks_for(b), 256, 0, s>>>(pts, w, kp.index.get() + g0, b, cpts.get(),
+                                                           cw.get(), INT64_MAX, bad.get());
+        ISDF_LAUNCH_CHECK();
+        eval_ao<double>(c, cpts.get(), b, phi.get(), nullptr, nao, s);
+        row_dot(phi.get(), b, nao, nullptr, q.get(), s);
+        gemm_f64(b, k, nao, phi.get(), nao, 0, f.phi_aT.get(), k, 0, G.get(), k, 0, 1, false, s);
+        hadamard_square_kernel<<<blocks_for(b * k), 256, 0, s>>>(G.get(), b * k, H.get());
+        ISDF_LAUNCH_CHECK();
+        if (have_theta) {
+            theta_to_x_kernel<<<blocks_for(b * k), 256, 0, s>>>(theta, ldt, g0, b, static_cast<int>(k),
+                                                                f.wa.get(), X.get());
+            ISDF_LAUNCH_CHECK();
+        } else {
+            gemm_f64(b, k, k, H.get(), k, 0, f.T.get(), k, 0, X.get(), k, 0, 1, false, s);
+        }
+        gemm_f64(b, k, k, X.get(), k, 0, f.M.get(), k, 0, Y.get(), k, 0, 1, false, s);
+        if (have_theta)
+            fit_point_kernel<true><<<blocks_for(b), 256, 0, s>>>(H.get(), X.get(), Y.get(), q.get(), cw.get(), b,
+                                                                 static_cast<int>(k), f.wa.get(), theta, ldt, g0, acc.get());
+        else
+            fit_point_kernel<false><<<blocks_for(b), 256, 0, s>>>(H.get(), X.get(), Y.get(), q.get(), cw.get(), b,
+                                                                  static_cast<int>(k), f.wa.get(), theta, ldt, g0, acc.get());
+        ISDF_LAUNCH_CHECK();
+        dim3 tg(static_cast<unsigned>(std::min<int64_t>(64, (b + 255) / 256)), static_cast<unsigned>(k));
+        theta_dot_w_kernel<<<tg, 256, 0, s>>>(theta, ldt, g0, b, cw.get(), tw.get());
+        ISDF_LAUNCH_CHECK();
+    }
+    double h[3];
+    ISDF_CUDA(cudaMemcpyAsync(h, acc.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(out.theta_w.data(), tw.get(), k * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    out.err2 = std::max(h[0], 0.0);
+    out.exact2 = h[1];
+    out.max_abs_coeff = h[2];
+    out.n = n;
+    return out;
+}
+
+void gather_points(const double* pts, const double* w, const int64_t* idx, int64_t n,
+                   int64_t npts_total, double* out_pts, double* out_w, cudaStream_t s) {
+    if (n == 0) return;
+    DeviceBuffer<int> bad(1, s);
+    bad.zero(s);
+    gather_points_kernel<<<blocks_for(n), 256, 0, s>>>(pts, w, idx, n, out_pts, out_w, npts_total,
+                                                       bad.get());
+    ISDF_LAUNCH_CHECK();
+    int hb = 0;
+    ISDF_CUDA(cudaMemcpyAsync(&hb, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    if (hb) fail(kInvalid, "anchor index outside the grid");
+}
+
+void pair_error_terms(int64_t n, int64_t k, const double* q, const double* H, const double* X,
+                      const double* M, const double* w, double* out2, cudaStream_t s) {
+    DeviceBuffer<double> Y(std::max<int64_t>(1, n * k), s), acc(3, s);
+    acc.zero(s);
+    gemm_f64(n, k, k, X, k, 0, M, k, 0, Y.get(), k, 0, 1, false, s);
+    fit_point_kernel<true><<<blocks_for(n), 256, 0, s>>>(H, X, Y.get(), q, w, n, static_cast<int>(k),
+                                                         nullptr, nullptr, 0, 0, acc.get());
+    ISDF_LAUNCH_CHECK();
+    ISDF_CUDA(cudaMemcpyAsync(out2, acc.get(), 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace isdf

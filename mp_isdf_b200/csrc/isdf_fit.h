@@ -1,0 +1,43 @@
+// Internal declarations of the fit / pair-error stages.
+#pragma once
+
+#include "isdf_select.h"
+
+namespace isdf {
+
+struct AnchorFactor {
+    int64_t k = 0;
+    DeviceBuffer<double> phi_a, phi_aT;   // k x nao, nao x k
+    DeviceBuffer<double> M;               // (Phi_a Phi_a^T)^2, k x k
+    DeviceBuffer<double> T;               // pseudo-inverse of M (SVD cutoff 1e-12 on C)
+    DeviceBuffer<double> wa;              // anchor weights
+    std::vector<double> sv;               // singular values of C^T, descending
+    int retained = 0;
+    double condition = 0;
+    bool gram_fallback = false;           // SVD taken of M instead of R (very large C^T)
+};
+
+struct FitOutput {
+    int64_t n = 0;
+    double err2 = 0, exact2 = 0, max_abs_coeff = 0;
+    std::vector<double> theta_w;          // sum_g Theta[a, g] w_g
+};
+
+AnchorFactor factor_anchors(const Context& c, const double* anchor_pts, const double* anchor_w,
+                            int64_t k, cudaStream_t s);
+
+// Grid pass over the kept points: writes Theta[a*ldt + g] (unless have_theta,
+// in which case Theta is read) and accumulates the pair-space error terms.
+FitOutput fit_grid(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
+                   const AnchorFactor& f, double* theta, int64_t ldt, bool have_theta,
+                   cudaStream_t s);
+
+void gather_points(const double* pts, const double* w, const int64_t* idx, int64_t n,
+                   int64_t npts_total, double* out_pts, double* out_w, cudaStream_t s);
+
+// Pair-space error reduction from precomputed Gram terms (device pointers):
+// out2 = {sum |w| (q^2 - 2 x.h + x^T M x), sum |w| q^2}.
+void pair_error_terms(int64_t n, int64_t k, const double* q, const double* H, const double* X,
+                      const double* M, const double* w, double* out2, cudaStream_t s);
+
+}  // namespace isdf

@@ -1,0 +1,156 @@
+// Internal declarations of the B200 ISDF library (not part of the C-ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace isdf {
+
+constexpr int kMaxL = 6;          // highest angular momentum the AO kernels handle
+constexpr int kMaxCtrGroup = 4;   // contractions evaluated per exponential sweep
+constexpr double kExpCut = 100.0; // alpha*r^2 beyond which a primitive is skipped (<4e-44)
+
+// ---- errors -----------------------------------------------------------------
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+enum : int {
+    kOk = 0,
+    kInvalid = 1,        // -> ValueError (std::invalid_argument in the reference)
+    kOverflow = 2,       // -> OverflowError / RuntimeError family (std::overflow_error)
+    kRuntime = 3,        // -> RuntimeError
+    kCuda = 4,           // CUDA runtime failure
+    kNotImplemented = 5, // -> NotImplementedError
+    kLogic = 6,          // -> RuntimeError (std::logic_error)
+};
+[[noreturn]] inline void fail(int code, const std::string& msg) { throw Error(code, msg); }
+inline void require(bool ok, const std::string& msg) { if (!ok) fail(kInvalid, msg); }
+
+#define ISDF_CUDA(expr)                                                                  \
+    do {                                                                                 \
+        cudaError_t err__ = (expr);                                                      \
+        if (err__ != cudaSuccess)                                                        \
+            ::isdf::fail(::isdf::kCuda, std::string(#expr) + ": " + cudaGetErrorString(err__)); \
+    } while (0)
+#define ISDF_LAUNCH_CHECK() ISDF_CUDA(cudaGetLastError())
+
+// ---- device buffers ----------------------------------------------------------
+// Stream-ordered allocation from the device's default memory pool.
+template <class T>
+class DeviceBuffer {
+public:
+    DeviceBuffer() = default;
+    DeviceBuffer(size_t n, cudaStream_t s) { reset(n, s); }
+    ~DeviceBuffer() { release(); }
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), n_(o.n_), s_(o.s_) { o.p_ = nullptr; o.n_ = 0; }
+    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+        if (this != &o) { release(); p_ = o.p_; n_ = o.n_; s_ = o.s_; o.p_ = nullptr; o.n_ = 0; }
+        return *this;
+    }
+    void reset(size_t n, cudaStream_t s) {
+        release();
+        s_ = s;
+        n_ = n;
+        if (n) ISDF_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p_), n * sizeof(T), s));
+    }
+    void release() {
+        if (p_) cudaFreeAsync(p_, s_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    T* get() const { return p_; }
+    size_t size() const { return n_; }
+    void zero(cudaStream_t s) { if (n_) ISDF_CUDA(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s)); }
+
+private:
+    T* p_ = nullptr;
+    size_t n_ = 0;
+    cudaStream_t s_ = nullptr;
+};
+
+// ---- shell table ---------------------------------------------------------------
+struct ShellDesc {
+    int l, nprim, nctr, ao_off;
+    int prim_off;   // exponents at prim_off .. prim_off+nprim
+    int coef_off;   // coefficients [nctr][nprim] at coef_off
+    int atom, pad;
+    double x, y, z;
+};
+
+// Angular momentum group: a run of shells with equal l (kernels specialise on l).
+struct Context {
+    int device = 0;
+    int natm = 0;
+    int nao = 0;
+    int nshell = 0;
+    int lmax = 0;
+    std::vector<int32_t> atm, bas;
+    std::vector<double> env;
+    std::vector<ShellDesc> shells;        // host copy
+    std::vector<int32_t> ao_atom;         // atom of each AO
+    std::vector<double> atom_xyz;         // natm x 3
+    ShellDesc* d_shells = nullptr;
+    double* d_exp = nullptr;
+    double* d_coef = nullptr;
+    float* d_expf = nullptr;
+    float* d_coeff = nullptr;
+    int32_t* d_ao_atom = nullptr;
+    ~Context();
+};
+
+Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nbas,
+                        const double* env, int64_t nenv);
+
+// Real-spherical transform of one angular momentum: nsph x ncart, row-major.
+std::vector<double> c2s_matrix(int l);
+
+// ---- AO evaluation ---------------------------------------------------------------
+// Component codes used by the kernels: 0 value, 1 d/dx, 2 d/dy, 3 d/dz.
+enum AoOut : int { kAoValues = 1, kAoGrad = 2 };
+
+// Values [p*ld + ao] and/or gradients [(c*n + p)*ld + ao] (component-major as
+// in the reference).  `out_grad` may alias a separate buffer.
+template <class T>
+void eval_ao(const Context& c, const double* pts, int64_t n, T* out_val, T* out_grad,
+             int64_t ld, cudaStream_t s);
+
+// Concatenated axis features F[g*d + off_a + j] = scale_a * comp_a(g, j) over
+// the given points (gathered through `index` when non-null), with per-component
+// sums of squares accumulated into sumsq[4] (FP64) over points whose weight
+// (through `weights`, may be null) is nonzero.
+struct AxisSpec {
+    int naxes = 0;
+    int comp[16];      // component of each axis entry (0..3)
+    double scale[16];  // scale of each axis entry
+    int need_mask = 0; // bit c set if component c is needed
+};
+template <class T>
+void eval_axis_features(const Context& c, const double* pts, const int64_t* index, int64_t n,
+                        const AxisSpec& ax, T* out, int64_t ld, double* sumsq,
+                        const double* weights, cudaStream_t s);
+
+// ---- small dense kernels ---------------------------------------------------------
+void iota_i64(int64_t* out, int64_t n, cudaStream_t s);
+// out[g] = F[g,:] . x (warp per row); |F[g,:]|^2 when x is null.
+void row_dot(const double* F, int64_t n, int64_t d, const double* x, double* out, cudaStream_t s);
+// a[i*d + k] = scale * f[i] * f[k]   (explicit weighted pair vector)
+void pair_vector(const double* f, int64_t d, double scale, double* a, cudaStream_t s);
+// out[r] += Q[r,:] . x  for r < rows (Q row-major rows x m); out must be pre-zeroed
+void rows_dot(const double* Q, int rows, int64_t m, const double* x, double* out, cudaStream_t s);
+// y = x - Q^T t ; *norm2 += |y|^2 when norm2 is non-null (x and y may alias)
+void rows_axpy(const double* Q, int rows, int64_t m, const double* t, const double* x, double* y,
+               double* norm2, cudaStream_t s);
+void scale_copy(const double* x, double scale, int64_t m, double* y, cudaStream_t s);
+// C[z][m][n] (+)= A[z][m][k] B[z][k][n], FP64, row-major with explicit strides.
+void gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, int64_t strideA,
+              const double* B, int64_t ldb, int64_t strideB, double* C, int64_t ldc,
+              int64_t strideC, int batch, bool accumulate, cudaStream_t s);
+
+}  // namespace isdf

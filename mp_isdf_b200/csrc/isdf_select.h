@@ -1,0 +1,72 @@
+// Internal declarations of the anchor-selection stages.
+#pragma once
+
+#include "isdf_internal.h"
+
+namespace isdf {
+
+struct KeptPoints {
+    DeviceBuffer<int64_t> index;  // original indices of nonzero-weight points, ascending
+    int64_t n = 0;
+};
+
+// Flags non-finite weights (always) and non-finite coordinates of kept points,
+// and compacts the nonzero-weight points in their original order.
+KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStream_t s);
+
+struct SelectOptions {
+    int algorithm = 0;               // LocalAnchorSelectionAlgorithm code
+    std::vector<int32_t> axes;       // AxisType codes
+    std::vector<double> axis_weights;
+    double tolerance = 1e-10;
+    int64_t max_rank = 0;
+    int64_t batch_size = 128;
+    int64_t sketch_size = 128;
+    int64_t oversampling = 16;
+    uint64_t seed = 7;
+    int precision = 0;               // 0 FP64, 1 mixed
+    bool debug = false;
+};
+
+struct SketchDiagnostics {
+    int64_t ell = 0, numerical_rank = 0, cap = 0, rank = 0;
+    double relative_tail = 0;
+    int64_t reverified = 0;          // mixed path: candidates recomputed in FP64
+    std::vector<double> diag, tails;
+};
+
+struct PairQrDiagnostics {
+    int64_t rank = 0, verifications = 0, reselections = 0, exact_scans = 0;
+    double first = 0, last = 0, floor = 0;
+    std::vector<double> rdiag;       // |R_jj| of the selected pivots
+    std::vector<double> gap;         // relative gap to the runner-up at each step
+};
+
+struct SketchQR {
+    std::vector<int64_t> jpvt;       // 0-based pivot columns, per step
+    std::vector<double> diag;        // |R_jj|
+    std::vector<double> energy;      // sum of squares of row j of R
+};
+
+AxisSpec make_axis_spec(const Context& c, const int32_t* axes, int naxes);
+void validate_axis_weights(const double* axis_weights, int naxes);
+std::vector<double> axis_scales_from_sumsq(const AxisSpec& ax, const double* sumsq4,
+                                           const double* axis_weights, bool any_eligible);
+void sketch_factors(int64_t d, int64_t ell, uint64_t seed, std::vector<double>& u,
+                    std::vector<double>& v);
+
+// Full column-pivoted Householder QR of the ell x n sketch stored row-wise
+// (Yt[s*ldy + g]); modifies Yt.
+SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t s);
+
+std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, const double* w,
+                                        int64_t ng, const SelectOptions& o, cudaStream_t s,
+                                        SketchDiagnostics* diag = nullptr);
+
+// qrcp_dense / qrcp_online: greedy max-residual pivoting of the weighted
+// pair columns sqrt|w_g| f_g (x) f_g, computed without materialising them.
+std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const double* w,
+                                    int64_t ng, const SelectOptions& o, cudaStream_t s,
+                                    PairQrDiagnostics* diag = nullptr);
+
+}  // namespace isdf

@@ -1,0 +1,315 @@
+// Drop-in `mp_isdf` Python module over the C-ABI of libisdf_b200.so.
+//
+// Mirrors the reference module's names, argument meanings and error types
+// (mikovtun/mp_isdf cpp/src/ao_eval_pybind.cpp:70-120,
+// cpp/src/anchor_select_pybind.cpp:142-222, cpp/src/evaluation_space_pybind.hpp).
+// Every computation runs on the GPU; the `space` argument is validated as in
+// the reference and "host" only means the result is returned in host memory.
+#include "isdf_b200.h"
+
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace py = pybind11;
+
+namespace {
+
+using IntArray = py::array_t<int32_t, py::array::c_style | py::array::forcecast>;
+using FloatArray = py::array_t<double, py::array::c_style | py::array::forcecast>;
+
+enum class AxisType : int { AtomicOrbital = 0, AtomicOrbitalGradX, AtomicOrbitalGradY,
+                            AtomicOrbitalGradZ, OccupiedOrbital };
+enum class LocalAlgo : int { QRColumnPivoting = 0, OnlineQRColumnPivoting, RandomizedQuadratureKhatriRao,
+                             CentroidalVoronoi, RandomizedAODensityKhatriRao,
+                             RandomizedAODensityNormalizedKhatriRao };
+enum class DistAlgo : int { SVD = 0, RandomizedQRColumnPivoting };
+
+struct NotImplemented : std::runtime_error { using std::runtime_error::runtime_error; };
+
+void check(int status) {
+    if (status == ISDF_OK) return;
+    const std::string msg = isdf_last_error();
+    switch (status) {
+    case ISDF_ERR_INVALID: throw std::invalid_argument(msg);
+    case ISDF_ERR_OVERFLOW: throw std::overflow_error(msg);
+    case ISDF_ERR_NOT_IMPLEMENTED: throw NotImplemented(msg);
+    case ISDF_ERR_LOGIC: throw std::logic_error(msg);
+    default: throw std::runtime_error(msg);
+    }
+}
+
+void parse_space(const std::string& space) {
+    if (space == "auto" || space == "default" || space == "host" || space == "device") return;
+    throw std::invalid_argument("space must be 'auto', 'host', or 'device'");
+}
+
+FloatArray points_of(const FloatArray& coords, const char* what) {
+    if (coords.ndim() != 2 || coords.shape(1) != 3) throw std::invalid_argument(what);
+    return coords;
+}
+
+struct Context {
+    isdf_ctx* h = nullptr;
+    int64_t nao = 0;
+    int32_t natm = 0, nshell = 0;
+    Context(const IntArray& atm, const IntArray& bas, const FloatArray& env) {
+        if (atm.ndim() != 2 || atm.shape(1) != 6 || bas.ndim() != 2 || bas.shape(1) != 8 || env.ndim() != 1)
+            throw std::invalid_argument("expected atm[natm,6], bas[nbas,8], env[nenv]");
+        check(isdf_ctx_create(atm.data(), static_cast<int32_t>(atm.shape(0)), bas.data(),
+                              static_cast<int32_t>(bas.shape(0)), env.data(), env.shape(0), &h));
+        check(isdf_ctx_info(h, &nao, &natm, &nshell));
+    }
+    ~Context() { if (h) isdf_ctx_destroy(h); }
+    Context(const Context&) = delete;
+    Context& operator=(const Context&) = delete;
+
+    py::array_t<double> evaluate(const FloatArray& coords, bool gradient, const std::string& space) {
+        parse_space(space);
+        auto pts = points_of(coords, "expected coords[ngrid,3] in Bohr");
+        const py::ssize_t ng = pts.shape(0);
+        std::vector<py::ssize_t> shape = gradient ? std::vector<py::ssize_t>{3, ng, static_cast<py::ssize_t>(nao)}
+                                                  : std::vector<py::ssize_t>{ng, static_cast<py::ssize_t>(nao)};
+        py::array_t<double> out(shape);
+        double* o = out.mutable_data();
+        const double* p = pts.data();
+        int rc;
+        {
+            py::gil_scoped_release release;
+            rc = isdf_eval_ao_host(h, p, ng, gradient ? nullptr : o, gradient ? o : nullptr);
+        }
+        check(rc);
+        return out;
+    }
+
+    py::array_t<int32_t> ao_atoms() const {
+        py::array_t<int32_t> out(nao);
+        check(isdf_ctx_ao_atoms(h, out.mutable_data()));
+        return out;
+    }
+};
+
+std::vector<int32_t> read_axes(py::object axes) {
+    std::vector<int32_t> out;
+    if (py::isinstance<py::list>(axes) || py::isinstance<py::tuple>(axes)) {
+        for (auto a : axes) out.push_back(static_cast<int32_t>(a.cast<AxisType>()));
+    } else {
+        out.push_back(static_cast<int32_t>(axes.cast<AxisType>()));
+    }
+    return out;
+}
+
+void check_occupied(const std::vector<int32_t>& axes, py::object mo_coeff, std::size_t nocc, int64_t nao) {
+    bool occ = false;
+    for (auto a : axes) occ |= a == ISDF_AXIS_OCC;
+    if (!occ) return;
+    if (mo_coeff.is_none() || nocc == 0 || static_cast<int64_t>(nocc) > nao)
+        throw std::invalid_argument(
+            "OccupiedOrbital requires row-major (nao,nao) RHF mo_coeff and 1 <= nocc <= nao");
+    auto c = mo_coeff.cast<FloatArray>();
+    if (c.ndim() != 2 || c.shape(0) != nao || c.shape(1) != nao)
+        throw std::invalid_argument("mo_coeff must have shape (nao,nao)");
+    throw NotImplemented("the OccupiedOrbital axis is outside the B200 hot path (NYI)");
+}
+
+struct Selector {
+    std::shared_ptr<Context> ctx;
+    explicit Selector(std::shared_ptr<Context> c) : ctx(std::move(c)) {}
+
+    std::vector<int64_t> select(const FloatArray& points, const FloatArray& weights, py::object axes,
+                                double tolerance, std::size_t max_rank, LocalAlgo algorithm,
+                                py::object mo_coeff, std::size_t nocc, const std::string& space,
+                                std::size_t batch_size, bool debug, std::size_t sketch_size,
+                                std::size_t oversampling, std::uint64_t seed, bool audit,
+                                py::object cvt_weights, std::size_t cvt_max_iter, double cvt_tol,
+                                const std::vector<double>& axis_weights, py::object point_importance,
+                                double ao_screening_threshold, const std::string& precision) {
+        (void)audit; (void)cvt_max_iter; (void)cvt_tol; (void)ao_screening_threshold;
+        auto pts = points_of(points, "expected points[ngrid,3]");
+        if (weights.ndim() != 1 || weights.shape(0) != pts.shape(0))
+            throw std::invalid_argument("expected weights[ngrid]");
+        auto ax = read_axes(axes);
+        if (!cvt_weights.is_none() || !point_importance.is_none() ||
+            algorithm == LocalAlgo::CentroidalVoronoi ||
+            algorithm == LocalAlgo::RandomizedAODensityKhatriRao ||
+            algorithm == LocalAlgo::RandomizedAODensityNormalizedKhatriRao) {
+            if ((algorithm == LocalAlgo::RandomizedAODensityKhatriRao ||
+                 algorithm == LocalAlgo::RandomizedAODensityNormalizedKhatriRao) &&
+                (ax.size() != 1 || ax[0] != ISDF_AXIS_AO))
+                throw std::invalid_argument("density Khatri-Rao sketches with non-AO axis features are NYI");
+            throw NotImplemented("CVT and density sketches are outside the B200 hot path (NYI)");
+        }
+        check_occupied(ax, mo_coeff, nocc, ctx->nao);
+        parse_space(space);
+        if (!axis_weights.empty() && axis_weights.size() != ax.size())
+            throw std::invalid_argument("axis weights must match axes");
+        if (precision != "fp64" && precision != "mixed")
+            throw std::invalid_argument("precision must be 'fp64' or 'mixed'");
+        isdf_select_args a;
+        isdf_select_args_default(&a);
+        a.algorithm = static_cast<int32_t>(algorithm);
+        a.naxes = static_cast<int32_t>(ax.size());
+        a.axes = ax.data();
+        a.axis_weights = axis_weights.empty() ? nullptr : axis_weights.data();
+        a.tolerance = tolerance;
+        a.max_rank = static_cast<int64_t>(max_rank);
+        a.batch_size = static_cast<int64_t>(batch_size);
+        a.sketch_size = static_cast<int64_t>(sketch_size);
+        a.oversampling = static_cast<int64_t>(oversampling);
+        a.seed = seed;
+        a.precision = precision == "mixed" ? ISDF_MIXED : ISDF_FP64;
+        a.debug = debug;
+        const int64_t ng = pts.shape(0);
+        std::vector<int64_t> piv(static_cast<size_t>(std::max<int64_t>(ng, 1)));
+        int64_t np = 0;
+        isdf_select_info info{};
+        int rc;
+        {
+            py::gil_scoped_release release;
+            rc = isdf_select_host(ctx->h, &a, pts.data(), weights.data(), ng, piv.data(),
+                                  static_cast<int64_t>(piv.size()), &np, &info);
+        }
+        check(rc);
+        piv.resize(np);
+        return piv;
+    }
+
+    py::array_t<double> evaluate_axis(const FloatArray& points, py::object axes, py::object mo_coeff,
+                                      std::size_t nocc, const std::string& space) {
+        auto ax = read_axes(axes);
+        check_occupied(ax, mo_coeff, nocc, ctx->nao);
+        parse_space(space);
+        auto pts = points_of(points, "expected points[ngrid,3]");
+        const py::ssize_t ng = pts.shape(0);
+        py::array_t<double> out({ng, static_cast<py::ssize_t>(ax.size() * ctx->nao)});
+        int rc;
+        {
+            py::gil_scoped_release release;
+            rc = isdf_evaluate_axis_host(ctx->h, pts.data(), ng, ax.data(), static_cast<int32_t>(ax.size()),
+                                         out.mutable_data());
+        }
+        check(rc);
+        return out;
+    }
+};
+
+py::dict fit(const std::shared_ptr<Context>& ctx, const FloatArray& coords, const FloatArray& weights,
+             py::array_t<int64_t, py::array::c_style | py::array::forcecast> anchors,
+             const std::string& precision, bool pair_space_error) {
+    auto pts = points_of(coords, "expected coords[ngrid,3]");
+    if (weights.ndim() != 1 || weights.shape(0) != pts.shape(0))
+        throw std::invalid_argument("expected weights[ngrid]");
+    if (precision != "fp64" && precision != "mixed")
+        throw std::invalid_argument("precision must be 'fp64' or 'mixed'");
+    const int64_t ng = pts.shape(0), k = anchors.size();
+    std::vector<double> theta(static_cast<size_t>(std::max<int64_t>(1, k * ng)));
+    isdf_fit_info info{};
+    int rc;
+    {
+        py::gil_scoped_release release;
+        rc = isdf_fit_host(ctx->h, pts.data(), weights.data(), ng, anchors.data(), k,
+                           precision == "mixed" ? ISDF_MIXED : ISDF_FP64, pair_space_error, theta.data(), &info);
+    }
+    check(rc);
+    py::array_t<double> th({static_cast<py::ssize_t>(k), static_cast<py::ssize_t>(info.n_kept)});
+    std::memcpy(th.mutable_data(), theta.data(), sizeof(double) * k * info.n_kept);
+    py::dict d;
+    d["interp_vecs"] = th;
+    d["retained_rank"] = info.retained_rank;
+    d["condition"] = info.condition;
+    d["max_abs_physical_coefficient"] = info.max_abs_physical_coefficient;
+    d["pair_l2"] = info.pair_l2;
+    d["pair_relative"] = info.pair_relative;
+    std::vector<double> tw(info.theta_w, info.theta_w + std::min<int64_t>(k, 64));
+    d["theta_w"] = tw;
+    return d;
+}
+
+}  // namespace
+
+PYBIND11_MODULE(mp_isdf, m) {
+    m.doc() = "B200 (sm_100a) ISDF hot path: spherical AO values/gradients, anchor selection and fit";
+    m.attr("cuda_enabled") = true;
+    m.attr("backend") = "b200";
+    py::register_exception<NotImplemented>(m, "NotImplementedError", PyExc_NotImplementedError);
+
+    py::class_<Context, std::shared_ptr<Context>>(m, "LibcintContext",
+        "Own a private copy of libcint tables and cache the shell table on the B200.")
+        .def(py::init<const IntArray&, const IntArray&, const FloatArray&>(), py::arg("atm"),
+             py::arg("bas"), py::arg("env"))
+        .def_property_readonly("nao", [](const Context& c) { return c.nao; })
+        .def_property_readonly("natm", [](const Context& c) { return c.natm; })
+        .def_property_readonly("ao_atoms", &Context::ao_atoms)
+        .def("eval_ao", [](Context& c, const FloatArray& coords, const std::string& space) {
+            return c.evaluate(coords, false, space);
+        }, py::arg("coords"), py::arg("space") = "auto", "Return real spherical AOs with shape (ngrid, nao).")
+        .def("eval_ao_gradient", [](Context& c, const FloatArray& coords, const std::string& space) {
+            return c.evaluate(coords, true, space);
+        }, py::arg("coords"), py::arg("space") = "auto", "Return x,y,z AO gradients with shape (3, ngrid, nao).");
+
+    m.def("eval_ao", [](const IntArray& atm, const IntArray& bas, const FloatArray& env,
+                        const FloatArray& coords, const std::string& space) {
+        Context c(atm, bas, env);
+        return c.evaluate(coords, false, space);
+    }, py::arg("atm"), py::arg("bas"), py::arg("env"), py::arg("coords"), py::arg("space") = "auto");
+    m.def("eval_ao_gradient", [](const IntArray& atm, const IntArray& bas, const FloatArray& env,
+                                 const FloatArray& coords, const std::string& space) {
+        Context c(atm, bas, env);
+        return c.evaluate(coords, true, space);
+    }, py::arg("atm"), py::arg("bas"), py::arg("env"), py::arg("coords"), py::arg("space") = "auto");
+
+    py::enum_<AxisType>(m, "AxisType")
+        .value("AtomicOrbital", AxisType::AtomicOrbital)
+        .value("AtomicOrbitalGradX", AxisType::AtomicOrbitalGradX)
+        .value("AtomicOrbitalGradY", AxisType::AtomicOrbitalGradY)
+        .value("AtomicOrbitalGradZ", AxisType::AtomicOrbitalGradZ)
+        .value("OccupiedOrbital", AxisType::OccupiedOrbital);
+    py::enum_<LocalAlgo>(m, "LocalAnchorSelectionAlgorithm")
+        .value("QRColumnPivoting", LocalAlgo::QRColumnPivoting)
+        .value("OnlineQRColumnPivoting", LocalAlgo::OnlineQRColumnPivoting)
+        .value("RandomizedQuadratureKhatriRao", LocalAlgo::RandomizedQuadratureKhatriRao)
+        .value("CentroidalVoronoi", LocalAlgo::CentroidalVoronoi)
+        .value("RandomizedAODensityKhatriRao", LocalAlgo::RandomizedAODensityKhatriRao)
+        .value("RandomizedAODensityNormalizedKhatriRao", LocalAlgo::RandomizedAODensityNormalizedKhatriRao);
+    py::enum_<DistAlgo>(m, "DistributedAnchorSelectionAlgorithm")
+        .value("SVD", DistAlgo::SVD)
+        .value("RandomizedQRColumnPivoting", DistAlgo::RandomizedQRColumnPivoting);
+
+    py::class_<Selector>(m, "AnchorSelection")
+        .def(py::init<std::shared_ptr<Context>>(), py::arg("context"), py::keep_alive<1, 2>())
+        .def_property_readonly("nao", [](const Selector& s) { return s.ctx->nao; })
+        .def("select", &Selector::select, py::arg("points"), py::arg("weights"), py::arg("axes"),
+             py::arg("tolerance") = 1e-10, py::arg("max_rank") = 0,
+             py::arg("algorithm") = LocalAlgo::QRColumnPivoting, py::arg("mo_coeff") = py::none(),
+             py::arg("nocc") = 0, py::arg("space") = "auto", py::arg("batch_size") = 128,
+             py::arg("debug") = false, py::arg("sketch_size") = 128, py::arg("oversampling") = 16,
+             py::arg("seed") = 7, py::arg("audit") = false, py::arg("cvt_weights") = py::none(),
+             py::arg("cvt_max_iter") = 100, py::arg("cvt_tol") = 1e-5,
+             py::arg("axis_weights") = std::vector<double>{}, py::arg("point_importance") = py::none(),
+             py::arg("ao_screening_threshold") = 1e-24, py::arg("precision") = "fp64",
+             "Select original grid indices in pivot order (QRCP / online QRCP / quadrature sketch).")
+        .def("evaluate_axis", &Selector::evaluate_axis, py::arg("points"), py::arg("axes"),
+             py::arg("mo_coeff") = py::none(), py::arg("nocc") = 0, py::arg("space") = "auto",
+             "Evaluate concatenated axis functions (ngrid, naxes*nao).");
+
+    py::class_<Context>* unused = nullptr;
+    (void)unused;
+    struct Distributed { std::shared_ptr<Context> ctx; };
+    py::class_<Distributed>(m, "DistributedAnchorSelection")
+        .def(py::init([](std::shared_ptr<Context> c) { return Distributed{std::move(c)}; }),
+             py::arg("context"), py::keep_alive<1, 2>())
+        .def("select", [](const Distributed&, py::object, py::object, py::object, DistAlgo) {
+            throw std::logic_error("distributed SLATE SVD anchor selection is not implemented");
+        }, py::arg("points"), py::arg("weights"), py::arg("axes"), py::arg("algorithm") = DistAlgo::SVD);
+
+    m.def("fit", &fit, py::arg("context"), py::arg("coords"), py::arg("weights"),
+          py::arg("anchor_indices"), py::arg("precision") = "fp64", py::arg("pair_space_error") = true,
+          "Interpolation vectors Theta (k, n_nonzero_weight) for the given anchors, with the "
+          "pair-space error evaluated in FP64.");
+}

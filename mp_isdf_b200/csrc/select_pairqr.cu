@@ -1,0 +1,368 @@
+// qrcp_dense / qrcp_online anchor selection on the weighted AO-pair columns
+// a_g = sqrt|w_g| f_g (x) f_g without materialising the d^2 x n pair matrix.
+//
+// The greedy rule of column-pivoted QR (dgeqp3 for qrcp_dense,
+// cpp/src/anchor_select_qrcp.cpp:275-306; the multipass selector of
+// cpp/src/anchor_select_online_qr.cpp:200-358 for qrcp_online) selects at
+// each step the column with the largest residual norm after projection onto
+// the span of the previous pivots.  Here:
+//   * residual estimates e_g = K_gg - sum_i L_gi^2 use the pair Gram
+//     K_pg = sqrt|w_p w_g| (f_p . f_g)^2: one GEMV over the feature matrix per
+//     pivot, L_gj = (K_pg - sum_{i<j} R_ij L_gi) / R_jj;
+//   * the leading candidate is always re-verified exactly: its explicit pair
+//     vector is orthogonalised twice (CGS2) against the explicit orthonormal
+//     pivot basis, giving R[:, j] with Householder-level accuracy.  If the
+//     exact value loses the lead, the next candidate is verified (the online
+//     reference's reselection loop, online_qr.cpp:238-254);
+//   * a stop decided on an estimate is confirmed by an exact scan of every
+//     column whose estimate, within its rounding bound, could still exceed
+//     the threshold ("no optimistic estimate may terminate", online_qr.cpp:233).
+// Tie-breaking: qrcp_dense emulates dgeqp3's column swaps (first maximum in
+// the current column order); qrcp_online takes the first maximum in grid order.
+#include "isdf_reduce.cuh"
+#include "isdf_select.h"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+
+namespace isdf {
+namespace {
+
+constexpr int kNT = 256;
+
+__global__ void gather_weights_kernel(const double* __restrict__ w, const int64_t* __restrict__ idx,
+                                      int64_t n, double* __restrict__ sw) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g < n) sw[g] = sqrt(fabs(w[idx[g]]));
+}
+
+// F[:, a-block] *= scale[a]
+__global__ void scale_columns_kernel(double* F, int64_t n, int64_t d, int nao,
+                                     const double* __restrict__ scales) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n * d) return;
+    F[i] *= scales[(i % d) / nao];
+}
+
+__global__ void init_est_kernel(const double* __restrict__ sw, const double* __restrict__ nf,
+                                int64_t n, double* __restrict__ est, double* __restrict__ kdiag) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const double a = sw[g] * nf[g];
+    est[g] = a * a;
+    kdiag[g] = a * a;
+}
+
+// est argmax over unselected columns -> per-block keys (value = estimate of the
+// squared residual norm).
+__global__ void __launch_bounds__(kNT)
+argmax_kernel(const double* __restrict__ est, const char* __restrict__ selected,
+              const int64_t* __restrict__ pos, int64_t n, ArgKey* __restrict__ partial) {
+    __shared__ ArgKey sh[kNT / 32];
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * kNT + threadIdx.x;
+    ArgKey k = key_none();
+    if (g < n && !selected[g]) k = ArgKey{est[g], pos ? pos[g] : g, g};
+    k = block_best<kNT>(k, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = k;
+}
+
+__global__ void __launch_bounds__(1024)
+argmax_final_kernel(const ArgKey* __restrict__ partial, int nblocks, ArgKey* __restrict__ out) {
+    __shared__ ArgKey sh[32];
+    ArgKey k = key_none();
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+        if (key_better(partial[b], k)) k = partial[b];
+    k = block_best<1024>(k, sh);
+    if (threadIdx.x == 0) out[0] = k;
+}
+
+// L[g, j] = (sw_p sw_g D_g^2 - sum_{i<j} R_ij L_gi) / R_jj ; est_g -= L_gj^2
+__global__ void update_residual_kernel(const double* __restrict__ D, const double* __restrict__ sw,
+                                       double swp, int64_t n, double* __restrict__ L,
+                                       int64_t ldl, int j, const double* __restrict__ Rcol,
+                                       double rjj, double* __restrict__ est,
+                                       const char* __restrict__ selected) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    double v = swp * sw[g] * D[g] * D[g];
+    const double* lg = L + g * ldl;
+    for (int i = 0; i < j; ++i) v -= Rcol[i] * lg[i];
+    v /= rjj;
+    L[g * ldl + j] = v;
+    if (!selected[g]) est[g] = fmax(est[g] - v * v, 0.0);
+}
+
+}  // namespace
+
+namespace {
+
+struct PairQr {
+    const Context& c;
+    cudaStream_t s;
+    int64_t n = 0, d = 0, m = 0;
+    DeviceBuffer<double> F, sw, nf, est, kdiag, D, L, Q, a, r, tvec, scal, Rcol;
+    DeviceBuffer<char> selected;
+    DeviceBuffer<int64_t> pos;
+    DeviceBuffer<ArgKey> partial, best;
+    int64_t capL = 0;
+    int nblocks = 0;
+    std::vector<double> R;   // column-major, capL x capL (host)
+    PairQr(const Context& ctx, cudaStream_t st) : c(ctx), s(st) {}
+
+    ArgKey argmax(bool use_pos) {
+        argmax_kernel<<<nblocks, kNT, 0, s>>>(est.get(), selected.get(),
+                                              use_pos ? pos.get() : nullptr, n, partial.get());
+        ISDF_LAUNCH_CHECK();
+        argmax_final_kernel<<<1, 1024, 0, s>>>(partial.get(), nblocks, best.get());
+        ISDF_LAUNCH_CHECK();
+        ArgKey h;
+        ISDF_CUDA(cudaMemcpyAsync(&h, best.get(), sizeof(ArgKey), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        return h;
+    }
+
+    // Exact residual of column p against the j current basis vectors: leaves the
+    // residual in r, the CGS2 coefficients in coeff (host), returns |r|^2.
+    double exact_residual(int64_t p, int j, std::vector<double>& coeff) {
+        double swp = 0;
+        ISDF_CUDA(cudaMemcpyAsync(&swp, sw.get() + p, sizeof(double), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        pair_vector(F.get() + p * d, d, swp, a.get(), s);
+        coeff.assign(j, 0.0);
+        scal.zero(s);
+        if (j == 0) {
+            rows_axpy(Q.get(), 0, m, tvec.get(), a.get(), r.get(), scal.get(), s);
+        } else {
+            const double* src = a.get();
+            for (int pass = 0; pass < 2; ++pass) {
+                tvec.zero(s);
+                rows_dot(Q.get(), j, m, src, tvec.get(), s);
+                if (pass == 1) scal.zero(s);
+                rows_axpy(Q.get(), j, m, tvec.get(), src, r.get(), pass == 1 ? scal.get() : nullptr, s);
+                std::vector<double> t(j);
+                ISDF_CUDA(cudaMemcpyAsync(t.data(), tvec.get(), j * sizeof(double),
+                                          cudaMemcpyDeviceToHost, s));
+                ISDF_CUDA(cudaStreamSynchronize(s));
+                for (int i = 0; i < j; ++i) coeff[i] += t[i];
+                src = r.get();
+            }
+        }
+        double nr2 = 0;
+        ISDF_CUDA(cudaMemcpyAsync(&nr2, scal.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        return nr2;
+    }
+
+    void set_est(int64_t g, double v) {
+        ISDF_CUDA(cudaMemcpyAsync(est.get() + g, &v, sizeof(double), cudaMemcpyHostToDevice, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+    }
+
+    void grow(int64_t need) {
+        if (need <= capL) return;
+        const int64_t cap2 = std::max<int64_t>(need, std::max<int64_t>(8, 2 * capL));
+        DeviceBuffer<double> L2(static_cast<size_t>(n * cap2), s), Q2(static_cast<size_t>(cap2 * m), s);
+        if (capL) {
+            ISDF_CUDA(cudaMemcpy2DAsync(L2.get(), cap2 * sizeof(double), L.get(), capL * sizeof(double),
+                                        capL * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
+            ISDF_CUDA(cudaMemcpyAsync(Q2.get(), Q.get(), capL * m * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, s));
+        }
+        L = std::move(L2);
+        Q = std::move(Q2);
+        std::vector<double> R2(static_cast<size_t>(cap2 * cap2), 0.0);
+        for (int64_t jj = 0; jj < capL; ++jj)
+            for (int64_t ii = 0; ii < capL; ++ii) R2[jj * cap2 + ii] = R[jj * capL + ii];
+        R.swap(R2);
+        capL = cap2;
+        tvec.reset(capL, s);
+        Rcol.reset(capL, s);
+    }
+};
+
+__global__ void swap_positions_kernel(int64_t* pos, int64_t* col_at, int64_t p, int64_t j) {
+    const int64_t pp = pos[p];
+    const int64_t cj = col_at[j];
+    col_at[pp] = cj;
+    pos[cj] = pp;
+    col_at[j] = p;
+    pos[p] = j;
+}
+
+__global__ void mark_selected_kernel(char* selected, double* est, int64_t p) {
+    selected[p] = 1;
+    est[p] = 0.0;
+}
+
+// exact-scan candidates: unselected g with est_g + bound_g > thr2
+__global__ void flag_uncertain_kernel(const double* __restrict__ est, const double* __restrict__ kdiag,
+                                      const char* __restrict__ selected, int64_t n, double rel,
+                                      double thr2, char* __restrict__ flag) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    flag[g] = !selected[g] && est[g] + rel * kdiag[g] > thr2;
+}
+
+}  // namespace
+
+std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const double* w,
+                                    int64_t ng, const SelectOptions& o, cudaStream_t s,
+                                    PairQrDiagnostics* diag) {
+    const bool online = o.algorithm == 1;
+    if (!std::isfinite(o.tolerance) || o.tolerance < 0 || (online && o.batch_size <= 0))
+        fail(kInvalid, online ? "invalid online QR weights, tolerance or batch size"
+                              : "invalid weights, axis list, or tolerance");
+    validate_axis_weights(o.axis_weights.empty() ? nullptr : o.axis_weights.data(),
+                          static_cast<int>(o.axes.size()));
+    AxisSpec ax = make_axis_spec(c, o.axes.data(), static_cast<int>(o.axes.size()));
+    const int64_t d = static_cast<int64_t>(ax.naxes) * c.nao;
+    if (d > 46340)
+        fail(kOverflow, online ? "AO pair dimension is too large" : "pair-product matrix is too large");
+    KeptPoints kp = compact_points(pts, w, ng, s);
+    const int64_t n = kp.n;
+    if (n == 0) return {};
+
+    PairQr q(c, s);
+    q.n = n; q.d = d; q.m = d * d;
+    const int64_t m = q.m;
+    q.nblocks = static_cast<int>((n + kNT - 1) / kNT);
+    q.F.reset(static_cast<size_t>(n * d), s);
+    DeviceBuffer<double> sumsq(4, s);
+    sumsq.zero(s);
+    eval_axis_features<double>(c, pts, kp.index.get(), n, ax, q.F.get(), d,
+                               ax.naxes > 1 ? sumsq.get() : nullptr, nullptr, s);
+    if (ax.naxes > 1) {
+        double h[4];
+        ISDF_CUDA(cudaMemcpyAsync(h, sumsq.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        auto sc = axis_scales_from_sumsq(ax, h, o.axis_weights.empty() ? nullptr : o.axis_weights.data(), true);
+        DeviceBuffer<double> dsc(sc.size(), s);
+        ISDF_CUDA(cudaMemcpyAsync(dsc.get(), sc.data(), sc.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        scale_columns_kernel<<<static_cast<unsigned>((n * d + 255) / 256), 256, 0, s>>>(
+            q.F.get(), n, d, c.nao, dsc.get());
+        ISDF_LAUNCH_CHECK();
+        ISDF_CUDA(cudaStreamSynchronize(s));
+    }
+    const unsigned nb = static_cast<unsigned>((n + 255) / 256);
+    q.sw.reset(n, s); q.nf.reset(n, s); q.est.reset(n, s); q.kdiag.reset(n, s); q.D.reset(n, s);
+    q.selected.reset(n, s); q.selected.zero(s);
+    q.pos.reset(n, s);
+    DeviceBuffer<int64_t> col_at(n, s);
+    iota_i64(q.pos.get(), n, s);
+    iota_i64(col_at.get(), n, s);
+    q.partial.reset(q.nblocks, s);
+    q.best.reset(1, s);
+    q.a.reset(m, s); q.r.reset(m, s); q.scal.reset(1, s);
+    gather_weights_kernel<<<nb, 256, 0, s>>>(w, kp.index.get(), n, q.sw.get());
+    ISDF_LAUNCH_CHECK();
+    row_dot(q.F.get(), n, d, nullptr, q.nf.get(), s);
+    init_est_kernel<<<nb, 256, 0, s>>>(q.sw.get(), q.nf.get(), n, q.est.get(), q.kdiag.get());
+    ISDF_LAUNCH_CHECK();
+    {
+        std::vector<double> kd(n);
+        ISDF_CUDA(cudaMemcpyAsync(kd.data(), q.kdiag.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        double frob2 = 0;
+        for (double x : kd) {
+            if (!std::isfinite(x)) fail(kOverflow, online ? "non-finite online AO pair column"
+                                                          : "non-finite weighted pair product");
+            frob2 += x;
+        }
+        if (diag) diag->floor = 32 * std::numeric_limits<double>::epsilon() * std::sqrt(frob2);
+        q.grow(8);
+        const int64_t cap = std::min({m, n, o.max_rank ? o.max_rank : std::min(m, n)});
+        const double eps = std::numeric_limits<double>::epsilon();
+        const double floor = online ? 32 * eps * std::sqrt(frob2) : 0.0;
+        std::vector<int64_t> kept(n);
+        ISDF_CUDA(cudaMemcpyAsync(kept.data(), kp.index.get(), n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        std::vector<int64_t> result;
+        double first = -1;
+        std::vector<double> coeff;
+        int64_t verifications = 0, reselections = 0, exact_scans = 0;
+        DeviceBuffer<char> flags(n, s);
+        std::vector<char> hflags;
+        bool exact_mode = false;   // every estimate in `est` is exact (after a scan)
+        while (true) {
+            const int j = static_cast<int>(result.size());
+            if (j == cap) break;
+            ArgKey k = q.argmax(!online);
+            if (k.col < 0) break;
+            // verification loop
+            double exact2 = 0;
+            while (true) {
+                exact2 = q.exact_residual(k.col, j, coeff);
+                ++verifications;
+                q.set_est(k.col, exact2);
+                ArgKey k2 = q.argmax(!online);
+                if (k2.col == k.col) break;
+                ++reselections;
+                k = k2;
+            }
+            const double rjj = std::sqrt(exact2);
+            if (first < 0) first = rjj;   // R_00: the largest column norm
+            const double thr = std::max(o.tolerance * first, floor);
+            const bool stop = first == 0 || rjj <= thr || (online && rjj <= floor);
+            if (stop) {
+                if (exact_mode) break;
+                // confirm on exact values: scan every column that could still exceed thr
+                const double rel = 64.0 * eps * static_cast<double>(j + 1);
+                flag_uncertain_kernel<<<nb, 256, 0, s>>>(q.est.get(), q.kdiag.get(), q.selected.get(),
+                                                          n, rel, thr * thr, flags.get());
+                ISDF_LAUNCH_CHECK();
+                hflags.resize(n);
+                ISDF_CUDA(cudaMemcpyAsync(hflags.data(), flags.get(), n, cudaMemcpyDeviceToHost, s));
+                ISDF_CUDA(cudaStreamSynchronize(s));
+                ++exact_scans;
+                for (int64_t g = 0; g < n; ++g)
+                    if (hflags[g]) q.set_est(g, q.exact_residual(g, j, coeff));
+                exact_mode = true;
+                k = q.argmax(!online);
+                if (k.col < 0) break;
+                exact2 = q.exact_residual(k.col, j, coeff);
+                const double r2 = std::sqrt(exact2);
+                if (first == 0 || r2 <= thr) break;
+            }
+            // accept pivot k.col
+            const int64_t p = k.col;
+            const double rj = std::sqrt(exact2);
+            q.grow(j + 1);
+            for (int i = 0; i < j; ++i) q.R[static_cast<size_t>(j) * q.capL + i] = coeff[i];
+            q.R[static_cast<size_t>(j) * q.capL + j] = rj;
+            scale_copy(q.r.get(), 1.0 / rj, m, q.Q.get() + static_cast<int64_t>(j) * m, s);
+            mark_selected_kernel<<<1, 1, 0, s>>>(q.selected.get(), q.est.get(), p);
+            ISDF_LAUNCH_CHECK();
+            if (!online) {
+                swap_positions_kernel<<<1, 1, 0, s>>>(q.pos.get(), col_at.get(), p, j);
+                ISDF_LAUNCH_CHECK();
+            }
+            // new column of L and downdated estimates
+            row_dot(q.F.get(), n, d, q.F.get() + p * d, q.D.get(), s);
+            ISDF_CUDA(cudaMemcpyAsync(q.Rcol.get(), q.R.data() + static_cast<size_t>(j) * q.capL,
+                                      j * sizeof(double) + sizeof(double), cudaMemcpyHostToDevice, s));
+            double swp = 0;
+            ISDF_CUDA(cudaMemcpyAsync(&swp, q.sw.get() + p, sizeof(double), cudaMemcpyDeviceToHost, s));
+            ISDF_CUDA(cudaStreamSynchronize(s));
+            update_residual_kernel<<<nb, 256, 0, s>>>(q.D.get(), q.sw.get(), swp, n, q.L.get(), q.capL,
+                                                      j, q.Rcol.get(), rj, q.est.get(), q.selected.get());
+            ISDF_LAUNCH_CHECK();
+            exact_mode = false;   // downdated estimates carry rounding again
+            result.push_back(p);
+            if (diag) diag->rdiag.push_back(rj);
+        }
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        std::vector<int64_t> out;
+        for (auto p : result) out.push_back(kept[p]);
+        if (diag) {
+            diag->rank = static_cast<int64_t>(out.size());
+            diag->verifications = verifications;
+            diag->reselections = reselections;
+            diag->exact_scans = exact_scans;
+            diag->first = first;
+        }
+        return out;
+    }
+}
+
+}  // namespace isdf

@@ -1,0 +1,94 @@
+"""CPU-side checks of the C-ABI library and the drop-in module (no GPU compute)."""
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    text = (ROOT / "include" / "isdf_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(isdf_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    import ctypes
+    from mp_isdf_b200 import capi
+    lib = ctypes.CDLL(str(capi.LIB_PATH))
+    names = declared_functions()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(capi.SYMBOLS)
+
+
+def test_status_strings_and_cuda_probe():
+    from mp_isdf_b200 import capi
+    L = capi.lib()
+    assert L.isdf_status_string(0) == b"ok"
+    assert L.isdf_status_string(1) == b"invalid argument"
+    assert L.isdf_cuda_available() in (0, 1)
+
+
+def test_dropin_module_surface():
+    import mp_isdf
+    assert mp_isdf.cuda_enabled is True
+    for name in ("AtomicOrbital", "AtomicOrbitalGradX", "AtomicOrbitalGradY",
+                 "AtomicOrbitalGradZ", "OccupiedOrbital"):
+        assert hasattr(mp_isdf.AxisType, name)
+    for name in ("QRColumnPivoting", "OnlineQRColumnPivoting", "RandomizedQuadratureKhatriRao",
+                 "CentroidalVoronoi", "RandomizedAODensityKhatriRao",
+                 "RandomizedAODensityNormalizedKhatriRao"):
+        assert hasattr(mp_isdf.LocalAnchorSelectionAlgorithm, name)
+    assert hasattr(mp_isdf.DistributedAnchorSelectionAlgorithm, "SVD")
+    for name in ("LibcintContext", "AnchorSelection", "DistributedAnchorSelection",
+                 "eval_ao", "eval_ao_gradient", "fit"):
+        assert hasattr(mp_isdf, name)
+
+
+def test_context_without_gpu_fails_loudly(s_shells):
+    """No CPU fallback: without a CUDA device the context constructor raises."""
+    from mp_isdf_b200 import capi
+    if capi.lib().isdf_cuda_available():
+        pytest.skip("a CUDA device is present")
+    import mp_isdf
+    with pytest.raises(RuntimeError):
+        mp_isdf.LibcintContext(*s_shells)
+
+
+def test_c2s_closed_form_matches_oracle_least_squares():
+    """The product's closed-form solid-harmonic table (C++) and the oracle's
+    least-squares derivation agree; checked through a tiny host-only helper
+    compiled from the same source formula."""
+    import subprocess, tempfile
+    from oracle import oracle as O
+    src = ROOT / "mp_isdf_b200" / "csrc" / "context.cu"
+    text = src.read_text()
+    start = text.index("namespace {\n\ndouble fact")
+    end = text.index("// ------------------------------------------------------------------------------\n// constant tables")
+    snippet = "#include <cmath>\n#include <cstdio>\n#include <vector>\n#include <cstdlib>\n" \
+              "namespace isdf {\n" + text[start:end] + "}\nint main(){for(int l=0;l<=6;++l){auto t=isdf::c2s_matrix(l);" \
+              "for(double x: t) std::printf(\"%.17g\\n\", x);} }\n"
+    with tempfile.TemporaryDirectory() as d:
+        c = Path(d) / "c2s.cpp"
+        c.write_text(snippet)
+        exe = Path(d) / "c2s"
+        subprocess.check_call(["g++", "-O1", "-std=c++17", str(c), "-o", str(exe)])
+        vals = np.array([float(x) for x in subprocess.check_output([str(exe)]).split()])
+    ref = O.c2s_table(6)
+    np.testing.assert_allclose(vals, ref, atol=1e-12)
+
+
+def test_inputs_generator_shapes():
+    from mp_isdf_b200 import inputs
+    mol, pts, w, cfg = inputs.make_config("c1", level=0)
+    assert mol.nao == 96 and len(mol.symbols) == 12
+    assert pts.shape[1] == 3 and len(w) == len(pts)
+    assert np.all(np.isfinite(w)) and np.any(w == 0)
+    sym, xyz = inputs.water_cluster((4, 4, 4), seed=5)
+    assert len(sym) == 192
+    tables = inputs.build_tables(sym, xyz)
+    assert tables.nao == 1536

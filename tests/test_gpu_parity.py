@@ -1,0 +1,302 @@
+"""GPU parity of the B200 library against the CPU oracle, through the drop-in
+module and the C-ABI.  Tolerances: AO values/gradients rtol 1e-11, atol 1e-12
+(the reference's own test tolerance, python/test/test_ao_eval.py:207);
+pivots exact except where the oracle's top-two residual gap is below 1e-10
+relative; Theta rtol 1e-9 x cond^2 scale; pair error rtol 1e-9."""
+import numpy as np
+import pytest
+from scipy.linalg import qr
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mpi():
+    import mp_isdf
+    return mp_isdf
+
+
+@pytest.fixture(scope="module")
+def s_ctx(mpi, s_shells):
+    c = mpi.LibcintContext(*s_shells)
+    return c, mpi.AnchorSelection(c), O.OracleContext(*s_shells)
+
+
+@pytest.fixture(scope="module")
+def water(mpi, small_water):
+    mol, pts, w = small_water
+    c = mpi.LibcintContext(mol.atm, mol.bas, mol.env)
+    return mol, pts, w, c, mpi.AnchorSelection(c), O.OracleContext(mol.atm, mol.bas, mol.env)
+
+
+# ---------------------------------------------------------------------------
+# AO evaluation
+# ---------------------------------------------------------------------------
+def test_ao_values_gradients_match_oracle(water):
+    mol, pts, w, c, sel, oc = water
+    rng = np.random.default_rng(42)
+    p = np.vstack([mol.coords[:2], rng.normal(size=(37, 3)) * 2 + mol.coords[0], pts[::97]])
+    np.testing.assert_allclose(c.eval_ao(p), oc.eval_ao(p), rtol=1e-11, atol=1e-12)
+    np.testing.assert_allclose(c.eval_ao_gradient(p), oc.eval_ao_gradient(p), rtol=1e-11, atol=1e-12)
+    assert c.eval_ao(p).shape == (len(p), mol.nao)
+    assert c.eval_ao_gradient(p).shape == (3, len(p), mol.nao)
+
+
+def test_ao_empty_grid_and_owned_tables(mpi, small_water):
+    mol, _, _ = small_water
+    atm, bas, env = mol.atm.copy(), mol.bas.copy(), mol.env.copy()
+    c = mpi.LibcintContext(atm, bas, env)
+    assert c.nao == mol.nao
+    assert c.eval_ao(np.empty((0, 3))).shape == (0, mol.nao)
+    assert c.eval_ao_gradient(np.empty((0, 3))).shape == (3, 0, mol.nao)
+    p = np.random.default_rng(7).normal(size=(9, 3))
+    ref = c.eval_ao(p)
+    atm.fill(0); bas.fill(0); env.fill(0)   # the context owns private copies
+    for _ in range(2):
+        np.testing.assert_array_equal(c.eval_ao(p), ref)
+    with pytest.raises(ValueError):
+        c.eval_ao(p, space="invalid")
+    for space in ("auto", "host", "device"):
+        np.testing.assert_array_equal(c.eval_ao(p, space=space), ref)
+    np.testing.assert_array_equal(mpi.eval_ao(mol.atm, mol.bas, mol.env, p), ref)
+
+
+def test_ao_float32_and_device_tensor_path(small_water):
+    import torch
+    from mp_isdf_b200 import capi
+    mol, pts, w = small_water
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    oc = O.OracleContext(mol.atm, mol.bas, mol.env)
+    p = pts[::13]
+    xyz = torch.tensor(p, device="cuda")
+    v64 = torch.empty(len(p), mol.nao, dtype=torch.float64, device="cuda")
+    g64 = torch.empty(3, len(p), mol.nao, dtype=torch.float64, device="cuda")
+    ctx.eval_ao(xyz, v64, g64)
+    v32 = torch.empty(len(p), mol.nao, dtype=torch.float32, device="cuda")
+    g32 = torch.empty(3, len(p), mol.nao, dtype=torch.float32, device="cuda")
+    ctx.eval_ao(xyz, v32, g32)
+    torch.cuda.synchronize()
+    ref, gref = oc.eval_ao(p), oc.eval_ao_gradient(p)
+    np.testing.assert_allclose(v64.cpu().numpy(), ref, rtol=1e-11, atol=1e-12)
+    np.testing.assert_allclose(g64.cpu().numpy(), gref, rtol=1e-11, atol=1e-12)
+    # FP32 storage form: relative to each point's largest value
+    scale = np.abs(ref).max(axis=1, keepdims=True) + 1e-30
+    assert np.max(np.abs(v32.cpu().numpy() - ref) / scale) < 2e-6
+    gscale = np.abs(gref).max(axis=2, keepdims=True) + 1e-30
+    assert np.max(np.abs(g32.cpu().numpy() - gref) / gscale) < 4e-6
+
+
+def test_evaluate_axis_matches_oracle(water, mpi):
+    mol, pts, w, c, sel, oc = water
+    p = pts[::211]
+    axes = [mpi.AxisType.AtomicOrbitalGradZ, mpi.AxisType.AtomicOrbital,
+            mpi.AxisType.AtomicOrbitalGradZ, mpi.AxisType.AtomicOrbitalGradX]
+    np.testing.assert_allclose(sel.evaluate_axis(p, axes), oc.axis_features(p, [3, 0, 3, 1]),
+                               rtol=1e-11, atol=1e-12)
+    with pytest.raises(ValueError):
+        sel.evaluate_axis(p, mpi.AxisType.OccupiedOrbital)
+
+
+# ---------------------------------------------------------------------------
+# selection: known answers of the reference's tests
+# ---------------------------------------------------------------------------
+def test_three_s_shell_dense_and_online(s_ctx, mpi):
+    """python/test/test_online_anchor_select.py:44-101."""
+    c, sel, oc = s_ctx
+    points = np.random.default_rng(23).normal(size=(17, 3))
+    weights = np.linspace(0.5, 2, 17)
+    weights[2] = 0
+    weights[4] *= -1
+    mask = weights != 0
+    matrix = O.pair_matrix(oc.axis_features(points[mask], [0]), weights[mask])
+    expected = np.flatnonzero(mask)[qr(matrix, pivoting=True)[2]]
+    axis = mpi.AxisType.AtomicOrbital
+    online = mpi.LocalAnchorSelectionAlgorithm.OnlineQRColumnPivoting
+    dense = sel.select(points, weights, axis)
+    assert len(dense) == 6
+    np.testing.assert_array_equal(dense, expected[:6])
+    for space in ("host", "device"):
+        for batch in (1, 3, 17):
+            got = sel.select(points, weights, axis, algorithm=online, space=space, batch_size=batch)
+            np.testing.assert_array_equal(got, expected[:6])
+            np.testing.assert_array_equal(
+                sel.select(points, weights, axis, algorithm=online, batch_size=batch, max_rank=3),
+                expected[:3])
+    assert sel.select(points, weights, axis, algorithm=online, tolerance=1) == []
+    for cutoff in (0.1, 0.5):
+        assert (sel.select(points, weights, axis, algorithm=online, tolerance=cutoff, batch_size=2)
+                == sel.select(points, weights, axis, tolerance=cutoff))
+    assert sel.select(points, np.zeros_like(weights), axis, algorithm=online) == []
+    with pytest.raises(ValueError):
+        sel.select(points, weights, axis, algorithm=online, batch_size=0)
+
+
+def test_three_s_shell_rand_sketch(s_ctx, mpi):
+    """python/test/test_randomized_anchor_select.py:151-172, 283-307."""
+    c, sel, oc = s_ctx
+    points = np.random.default_rng(23).normal(size=(19, 3))
+    weights = np.linspace(.4, 1.5, 19)
+    weights[2] = 0
+    weights[4] = -1
+    algo = mpi.LocalAnchorSelectionAlgorithm.RandomizedQuadratureKhatriRao
+    axis = mpi.AxisType.AtomicOrbital
+
+    def select(**kw):
+        return sel.select(points, weights, axis, algorithm=algo, sketch_size=12, oversampling=3,
+                          seed=31, **kw)
+    ref = O.select_rand_sketch(oc, points, weights, [0], max_rank=3, sketch_size=12,
+                               oversampling=3, seed=31)
+    for batch in (1, 4, 19):
+        piv = select(batch_size=batch, max_rank=3)
+        assert piv == ref
+        assert len(piv) == 3 and 2 not in piv
+    assert len(select(batch_size=4)) == 6
+    assert select(tolerance=1, max_rank=0) == []
+    assert len(select(tolerance=1, max_rank=2)) == 2
+    assert len(select(tolerance=0, max_rank=2)) == 2
+    assert sel.select(points, weights, axis, algorithm=algo, sketch_size=2, oversampling=3,
+                      max_rank=3, seed=31) == ref
+    with pytest.raises(ValueError):
+        sel.select(points, weights, axis, algorithm=algo, sketch_size=12, oversampling=0)
+    with pytest.raises(ValueError):
+        select(batch_size=0)
+    assert sel.select(points, np.zeros_like(weights), axis, algorithm=algo, sketch_size=12,
+                      oversampling=3) == []
+    # signed weights enter as |w|
+    assert sel.select(points, np.abs(weights), axis, algorithm=algo, max_rank=3, oversampling=4,
+                      sketch_size=1, seed=31) == \
+        sel.select(points, weights, axis, algorithm=algo, max_rank=3, oversampling=4,
+                   sketch_size=1, seed=31)
+
+
+def _greedy_gaps(matrix, pivots_local):
+    """Relative gap between the best and runner-up residual norm at each step."""
+    gaps = []
+    for k in range(len(pivots_local)):
+        if k:
+            q = qr(matrix[:, pivots_local[:k]], mode="economic")[0]
+            res = matrix - q @ (q.T @ matrix)
+        else:
+            res = matrix
+        nrm = np.linalg.norm(res, axis=0)
+        nrm[pivots_local[:k]] = -1
+        top = np.sort(nrm)[::-1]
+        gaps.append((top[0] - top[1]) / top[0])
+    return np.array(gaps)
+
+
+@pytest.mark.parametrize("axes,weights_", [([0], None), ([0, 1, 3], [1.0, 0.5, 2.0])])
+def test_dense_pivots_match_lapack_small_water(water, mpi, axes, weights_):
+    mol, pts, w, c, sel, oc = water
+    pts_s, w_s = pts[::40], w[::40].copy()
+    w_s[5] = -abs(w_s[5])
+    scales = O.axis_scales(oc, pts_s, w_s, axes, weights_)
+    expected = O.select_qrcp_dense(oc, pts_s, w_s, axes, max_rank=12, scales=scales)
+    axt = [mpi.AxisType(a) for a in axes]
+    got = sel.select(pts_s, w_s, axt, max_rank=12, axis_weights=weights_ or [])
+    mask = w_s != 0
+    keep = np.flatnonzero(mask)
+    matrix = O.pair_matrix(oc.axis_features(pts_s[mask], axes, scales), w_s[mask])
+    gaps = _greedy_gaps(matrix, np.searchsorted(keep, expected))
+    for i, (a, b) in enumerate(zip(got, expected)):
+        if a != b:
+            assert gaps[i] <= 1e-10, (i, a, b, gaps[i])
+            break
+    online = sel.select(pts_s, w_s, axt, max_rank=12, axis_weights=weights_ or [],
+                        algorithm=mpi.LocalAnchorSelectionAlgorithm.OnlineQRColumnPivoting,
+                        batch_size=64)
+    assert online == got
+
+
+def test_rand_sketch_matches_oracle_small_water(water, mpi):
+    mol, pts, w, c, sel, oc = water
+    algo = mpi.LocalAnchorSelectionAlgorithm.RandomizedQuadratureKhatriRao
+    for axes, aw in (([0], None), ([0, 1, 2, 3], [1.0, 0.5, 0.5, 0.5])):
+        scales = O.axis_scales(oc, pts, w, axes, aw)
+        ref, det = O.select_rand_sketch(oc, pts, w, axes, max_rank=8, oversampling=4, seed=2,
+                                        scales=scales, return_details=True)
+        got = sel.select(pts, w, [mpi.AxisType(a) for a in axes], algorithm=algo, max_rank=8,
+                         oversampling=4, seed=2, axis_weights=aw or [])
+        assert got == ref, (got, ref)
+
+
+# ---------------------------------------------------------------------------
+# fit and pair error
+# ---------------------------------------------------------------------------
+def test_fit_matches_literal_refit_and_error(water, mpi):
+    mol, pts, w, c, sel, oc = water
+    pts_s, w_s = pts[::11], w[::11]
+    piv = sel.select(pts_s, w_s, mpi.AxisType.AtomicOrbital, max_rank=8)
+    res = mpi.fit(c, pts_s, w_s, np.array(piv))
+    keep = w_s != 0
+    ao = oc.eval_ao(pts_s[keep])
+    anchor_ao = oc.eval_ao(pts_s[piv])
+    pairs = (anchor_ao[:, :, None] * anchor_ao[:, None, :]).reshape(len(piv), -1)
+    theta, diag = O.physical_pair_refit(pairs, w_s[piv], ao)
+    cond = diag["condition"]
+    tol = max(1e-10, 1e-15 * cond ** 2)
+    th = res["interp_vecs"]
+    assert th.shape == theta.shape
+    np.testing.assert_allclose(th, theta, rtol=tol, atol=tol * np.abs(theta).max())
+    assert res["retained_rank"] == diag["retained_rank"]
+    np.testing.assert_allclose(res["condition"], cond, rtol=1e-6)
+    products = (ao[:, :, None] * ao[:, None, :]).reshape(len(ao), -1)
+    err = O.pair_space_error_norms(products, pairs, w_s[piv], theta, w_s[keep])
+    np.testing.assert_allclose(res["pair_l2"], err["l2"], rtol=1e-9)
+    np.testing.assert_allclose(res["pair_relative"], err["relative"], rtol=1e-9)
+    np.testing.assert_allclose(res["theta_w"], theta @ w_s[keep], rtol=1e-9,
+                               atol=1e-9 * np.abs(theta @ w_s[keep]).max())
+
+
+def test_pair_error_terms_known_answer():
+    """python/test/test_isdf.py:157-164 through the C-ABI reduction kernel."""
+    import torch
+    from mp_isdf_b200 import capi
+    exact = np.array([[1., 2.], [3., 4.]])
+    anchor = np.array([[1., 0.]])
+    theta = np.array([[1., 3.]])
+    aw = np.array([1.])
+    wg = np.array([2., -1.])
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+    q = t(np.linalg.norm(exact, axis=1))
+    H = t(exact @ anchor.T)
+    X = t((theta * aw[:, None]).T)
+    M = t(anchor @ anchor.T)
+    e = capi.pair_error_terms(q, H, X, M, t(wg))
+    np.testing.assert_allclose(e["l2"], np.sqrt(24.), rtol=1e-14)
+    np.testing.assert_allclose(e["relative"], np.sqrt(24. / 35.), rtol=1e-14)
+
+
+# ---------------------------------------------------------------------------
+# error paths
+# ---------------------------------------------------------------------------
+def test_error_paths(water, mpi):
+    mol, pts, w, c, sel, oc = water
+    axis = mpi.AxisType.AtomicOrbital
+    p, ww = pts[:50].copy(), w[:50].copy()
+    bad = ww.copy(); bad[3] = np.nan
+    with pytest.raises(ValueError):
+        sel.select(p, bad, axis)
+    badp = p.copy(); badp[np.flatnonzero(ww)[0], 1] = np.inf
+    with pytest.raises(ValueError):
+        sel.select(badp, ww, axis)
+    with pytest.raises(ValueError):
+        sel.select(p, ww, axis, space="invalid")
+    with pytest.raises(ValueError):
+        sel.select(p, ww, [axis, mpi.AxisType.AtomicOrbitalGradX], axis_weights=[1.0])
+    for f in ([0., 1.], [np.nan, 1.], [np.inf, 1.]):
+        with pytest.raises(ValueError):
+            sel.select(p, ww, [axis, mpi.AxisType.AtomicOrbitalGradX], axis_weights=f)
+    with pytest.raises(ValueError):
+        sel.select(p, ww, axis, algorithm=mpi.LocalAnchorSelectionAlgorithm.RandomizedQuadratureKhatriRao,
+                   max_rank=10 ** 6, oversampling=4)
+    with pytest.raises(ValueError):
+        sel.select(np.empty((0, 3)), np.empty(0), mpi.AxisType.OccupiedOrbital)
+    with pytest.raises(RuntimeError):
+        mpi.DistributedAnchorSelection(c).select(p, ww, axis)
+    with pytest.raises(NotImplementedError):
+        sel.select(p, ww, axis, algorithm=mpi.LocalAnchorSelectionAlgorithm.CentroidalVoronoi,
+                   max_rank=2)
+    assert sel.select(p, np.zeros(50), axis) == []
