@@ -1,0 +1,351 @@
+#!/usr/bin/env python3
+"""Anchor selection + interpolation-vector fit, seconds per water cluster.
+
+One step = rand_sketch (quadrature) anchor selection + Theta fit for one
+cluster, grid and weights resident in HBM (`value`), and the same through the
+host-buffer C-ABI entry points with host<->device copies inside the timed
+region (`e2e`).  Default workload: (H2O)64, synthetic cc-pVDZ-shaped basis
+(1536 AOs), level-3 stand-in grid (~2e6 points), axes ao,dx,dy,dz, rank 10.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                       [--config c5] [--precision fp64|mixed]
+Under torchrun (N > 1) every rank runs its own cluster (replicas, weak scaling);
+`value` is the max-over-ranks time divided by the number of clusters.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "anchor-select+fit s per cluster (mixed vs FP64 GPU) at fixed pair error; GB/s, TC util"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--config", default="c5")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(cfg_key):
+    from mp_isdf_b200 import inputs
+    mol, pts, w, cfg = inputs.make_config(cfg_key)
+    names, factors = inputs.parse_axes(cfg["axes"])
+    return mol, pts, w, cfg, names, factors
+
+
+def workload_desc(cfg_key, cfg, mol, pts, w, names, precision):
+    return {
+        "workload": f"{cfg_key} {cfg['name']}: synthetic cc-pVDZ-shaped basis ({mol.nao} AOs), "
+                    f"level-{cfg['level']} stand-in grid ({len(pts)} points, "
+                    f"{int(np.count_nonzero(w))} nonzero-weight), axes {cfg['axes']}, "
+                    f"rand_sketch quadrature rank {cfg['rank']} oversampling {cfg['oversampling']}, "
+                    f"{precision} form",
+        "nao": mol.nao, "grid_points": int(len(pts)), "axes": cfg["axes"],
+        "anchor_rank": cfg["rank"], "sketch_rows": cfg["rank"] + cfg["oversampling"],
+        "precision": precision, "l2_policy": "working set >> L2 (126 MB); 256 MB L2 flush before every timed step",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i - 5] for r in self.rows for i in range(5, 9)
+                          if r[i].lower() in ("active", "1")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# roofline bookkeeping
+# ---------------------------------------------------------------------------
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d["hbm_gbs"], d["bf16_tflops"], "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def algorithmic(family, cfg, mol, n_kept, naxes, ell, k):
+    """(bound, units per kernel family over one step, unit).  Bytes are the
+    minimal HBM traffic of the family's outputs/inputs; flops are 2*M*N*K."""
+    nao = mol.nao
+    d = naxes * nao
+    if family.startswith("ao_axis"):
+        s = 8 if family.endswith("f64") else 4
+        return "hbm", n_kept * d * s + n_kept * 24, "bytes"
+    if family.startswith("ao_eval"):
+        s = 8 if family.endswith("f64") else 4
+        return "hbm", (n_kept + k) * nao * s + n_kept * 24, "bytes"
+    if family == "gemm_f64":
+        # sketch projection (reads F once) + fit Gram (reads Phi once)
+        return "hbm", n_kept * d * 8 + n_kept * nao * 8, "bytes"
+    if family.startswith("sketch_tc") or family.startswith("fit_tc"):
+        return "tensor", 2.0 * n_kept * d * 2 * ell * 3, "flop"
+    if family.startswith("qrcp_sketch_update"):
+        return "hbm", sum(2 * (ell - j + 1) * n_kept * 8 for j in range(ell + 1)), "bytes"
+    if family == "sketch_combine":
+        return "hbm", n_kept * (naxes * 2 * ell + ell) * 8, "bytes"
+    if family == "fit_point":
+        return "hbm", n_kept * k * 8 * 4, "bytes"
+    return "hbm", 0, "bytes"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (oracle restatement, bounded sample)
+# ---------------------------------------------------------------------------
+def cpu_sample(mol, pts, w, names, factors, cfg, n_sample=4000, seed=0):
+    """Time the oracle's restatement of the same path on `n_sample` nonzero
+    points, scaled to the full kept-point count: axis norms, Khatri-Rao sketch,
+    dgeqp3 of the sketch, AO values + Gram fit.  Returns (seconds/cluster, cores, sample)."""
+    from oracle import oracle as O
+    axes = [O.AXIS_CODES[a] for a in names]
+    keep = np.flatnonzero(w != 0)
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(keep, size=min(n_sample, len(keep)), replace=False))
+    p, ww = pts[idx], w[idx]
+    ctx = O.OracleContext(mol.atm, mol.bas, mol.env)
+    ell = cfg["rank"] + cfg["oversampling"]
+    t0 = time.perf_counter()
+    scales = O.axis_scales(ctx, p, ww, axes, factors, exact_order=False) if len(axes) > 1 else None
+    piv = O.select_rand_sketch(ctx, p, ww, axes, max_rank=cfg["rank"],
+                               oversampling=cfg["oversampling"], seed=cfg.get("sketch_seed", 7),
+                               scales=scales)
+    O.gram_fit(ctx, p, ww, p[piv], ww[piv])
+    dt = time.perf_counter() - t0
+    scale = len(keep) / len(idx)
+    return dt * scale, O.lib().oracle_num_threads(), \
+        f"{len(idx)} of {len(keep)} nonzero-weight points (uniform random), time x{scale:.1f}"
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    mol, pts, w, cfg, names, factors = workload(args.config)
+    precision = args.precision or "fp64"
+    vals = []
+    cores = 1
+    sample = ""
+    for i in range(args.warmup + args.steps):
+        v, cores, sample = cpu_sample(mol, pts, w, names, factors, cfg, n_sample=3000, seed=i)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.mean(vals)
+    line = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": workload_desc(args.config, cfg, mol, pts, w, names, precision),
+        "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CMake build needs network FetchContent (Kokkos, LAPACK++, SLATE, "
+                "libcint, MAGMA); timed is the C++/OpenMP restatement of its algorithm in oracle/",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from mp_isdf_b200 import capi
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    mol, pts, w, cfg, names, factors = workload(args.config)
+    precision = args.precision or "fp64"
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    x = torch.tensor(pts, device=dev)
+    wt = torch.tensor(w, device=dev)
+    n = len(pts)
+    n_kept = int(np.count_nonzero(w))
+    k = cfg["rank"]
+    ell = k + cfg["oversampling"]
+    theta = torch.empty(k * n, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    sel_kw = dict(algorithm="rand_sketch", axes=names, axis_weights=factors, max_rank=k,
+                  oversampling=cfg["oversampling"], seed=cfg.get("sketch_seed", 7),
+                  precision=precision)
+
+    def step():
+        piv, _ = ctx.select(x, wt, **sel_kw)
+        info = ctx.fit(x, wt, piv, theta, precision=precision)
+        return piv, info
+
+    for _ in range(args.warmup):
+        piv, info = step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    capi.profile_enable(True)
+    capi.profile_read()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        piv, info = step()
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b) / 1e3)
+    clocks = sampler.stop()
+    capi.profile_enable(False)
+    prof = capi.profile_read()
+    total = sum(times)
+    if world > 1:
+        t = torch.tensor([total], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total = float(t.item())
+    per_cluster = total / args.steps / world
+    launches = sum(c for _, c in prof.values()) // max(args.steps, 1)
+
+    # e2e through the host-buffer C-ABI
+    e2e = None
+    if not args.no_e2e:
+        pts_h = np.ascontiguousarray(pts)
+        w_h = np.ascontiguousarray(w)
+        e2e_times = []
+        for i in range(max(1, min(3, args.steps)) + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            piv_h, _ = ctx.select_host(pts_h, w_h, **sel_kw)
+            th, finfo = ctx.fit_host(pts_h, w_h, piv_h, precision=precision)
+            dt = time.perf_counter() - t0
+            if i:
+                e2e_times.append(dt)
+        h2d = 2 * (pts_h.nbytes + w_h.nbytes)
+        d2h = th.nbytes + 8 * len(piv_h)
+        e2e = {"value": statistics.mean(e2e_times) / 1.0, "unit": "s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "path": "isdf_select_host + isdf_fit_host (pageable numpy buffers)"}
+
+    if rank != 0:
+        return
+    hbm, bf16, peak_kind = peaks()
+    fams = sorted(prof.items(), key=lambda kv: -kv[1][0])
+    roofline = None
+    kernels = {}
+    for name, (ms, cnt) in fams:
+        bound, units, unit = algorithmic(name, cfg, mol, n_kept, len(names), ell, k)
+        per_launch_ms = ms / cnt
+        kernels[name] = {"ms_per_step": ms / args.steps, "launches_per_step": cnt / args.steps,
+                         "share": ms / sum(v[0] for v in prof.values())}
+        if roofline is None and units:
+            achieved = units / (ms / args.steps / 1e3)
+            if bound == "hbm":
+                ach, pk, u = achieved / 1e9, hbm, "GB/s"
+            else:
+                ach, pk, u = achieved / 1e12, bf16, "TFLOP/s"
+            roofline = {"kernel": name, "bound": bound, "achieved": ach, "peak": pk, "unit": u,
+                        "frac": ach / pk, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json)",
+                        "traffic": None,
+                        "algorithmic_per_step": units, "per_launch_ms": per_launch_ms,
+                        "launches_per_step": cnt / args.steps}
+    cpu = None
+    if not args.no_cpu and world == 1:
+        v, cores, sample = cpu_sample(mol, pts, w, names, factors, cfg, n_sample=3000)
+        cpu = {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": sample}
+    line = {
+        "metric": METRIC, "value": per_cluster, "unit": "s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if precision == "fp64" else "bf16x3+f32+f64", "data": "synthetic",
+        "config": workload_desc(args.config, cfg, mol, pts, w, names, precision)
+        | {"parallelism": f"replicas x{world}"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+        "clocks": clocks, "kernels": kernels,
+        "result": {"anchors": [int(p) for p in piv], "pair_relative": info.pair_relative,
+                   "retained_rank": info.retained_rank, "condition": info.condition},
+        "step_times_s": times,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -162,6 +162,15 @@ int isdf_pair_error_terms(int64_t n, int64_t k, const double* q_dev, const doubl
                           const double* X_dev, const double* M_dev, const double* w_dev,
                           double* out_host, void* stream);
 
+/* ---- profiling ---------------------------------------------------------------
+ * No counterpart in the reference beyond its per-stage wall times
+ * (python/isdf.py:384-396): CUDA-event timing per kernel family, off by
+ * default.  isdf_profile_read synchronises the recorded events, returns up to
+ * `max` families sorted by total time (names: 48 bytes each) and clears the
+ * record. */
+int isdf_profile_enable(int32_t on);
+int isdf_profile_read(int32_t max, char* names, double* total_ms, int64_t* launches, int32_t* count);
+
 #ifdef __cplusplus
 }
 #endif

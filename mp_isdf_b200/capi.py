@@ -25,6 +25,7 @@ SYMBOLS = [
     "isdf_eval_ao", "isdf_eval_ao_host", "isdf_evaluate_axis", "isdf_evaluate_axis_host",
     "isdf_select_args_default", "isdf_select", "isdf_select_host",
     "isdf_fit", "isdf_fit_host", "isdf_pair_error", "isdf_pair_error_terms",
+    "isdf_profile_enable", "isdf_profile_read",
 ]
 
 ALGORITHMS = {"qrcp_dense": 0, "qrcp_online": 1, "rand_sketch": 2}
@@ -84,6 +85,8 @@ def lib():
         L.isdf_pair_error.argtypes = [P, P, P, I64, P, I64, P, ctypes.POINTER(F64),
                                       ctypes.POINTER(F64), P]
         L.isdf_pair_error_terms.argtypes = [I64, I64, P, P, P, P, P, P, P]
+        L.isdf_profile_enable.argtypes = [I32]
+        L.isdf_profile_read.argtypes = [I32, P, P, P, ctypes.POINTER(I32)]
         _lib = L
     return _lib
 
@@ -232,6 +235,24 @@ def make_select_args(algorithm="rand_sketch", axes=("ao",), axis_weights=None, t
     args.precision = 1 if precision == "mixed" else 0
     args.debug = int(debug)
     return args, (ax, aw)
+
+
+def profile_enable(on=True):
+    check(lib().isdf_profile_enable(1 if on else 0))
+
+
+def profile_read(max_entries=64):
+    """{family: (total_ms, launches)} since the last read, sorted by time."""
+    names = ctypes.create_string_buffer(48 * max_entries)
+    ms = np.zeros(max_entries)
+    cnt = np.zeros(max_entries, dtype=np.int64)
+    n = I32()
+    check(lib().isdf_profile_read(max_entries, names, _ptr(ms), _ptr(cnt), ctypes.byref(n)))
+    out = {}
+    for i in range(n.value):
+        name = names.raw[48 * i:48 * (i + 1)].split(b"\0", 1)[0].decode()
+        out[name] = (float(ms[i]), int(cnt[i]))
+    return out
 
 
 def pair_error_terms(q, H, X, M, w):

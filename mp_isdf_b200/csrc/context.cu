@@ -383,6 +383,7 @@ template <class T>
 void eval_ao(const Context& c, const double* pts, int64_t n, T* out_val, T* out_grad,
              int64_t ld, cudaStream_t s) {
     if (n == 0 || c.nao == 0) return;
+    ISDF_PROFILE(sizeof(T) == 8 ? "ao_eval_f64" : "ao_eval_f32", s);
     dim3 block(kPtsPerBlock, kShellLanes);
     const int64_t nb = (n + kPtsPerBlock - 1) / kPtsPerBlock;
     require(nb < (1ll << 31), "too many grid points for one launch");
@@ -402,6 +403,7 @@ void eval_axis_features(const Context& c, const double* pts, const int64_t* inde
                         const double* weights, cudaStream_t s) {
     if (n == 0 || c.nao == 0) return;
     require(ax.naxes > 0 && ax.naxes <= 16, "between 1 and 16 axes are supported");
+    ISDF_PROFILE(sizeof(T) == 8 ? "ao_axis_f64" : "ao_axis_f32", s);
     dim3 block(kPtsPerBlock, kShellLanes);
     const int64_t nb = (n + kPtsPerBlock - 1) / kPtsPerBlock;
     require(nb < (1ll << 31), "too many grid points for one launch");

@@ -312,6 +312,7 @@ FitOutput fit_grid(const Context& c, const double* pts, const double* w, const K
             gemm_f64(b, k, k, H.get(), k, 0, f.T.get(), k, 0, X.get(), k, 0, 1, false, s);
         }
         gemm_f64(b, k, k, X.get(), k, 0, f.M.get(), k, 0, Y.get(), k, 0, 1, false, s);
+        ISDF_PROFILE("fit_point", s);
         if (have_theta)
             fit_point_kernel<true><<<blocks_for(b), 256, 0, s>>>(H.get(), X.get(), Y.get(), q.get(), cw.get(), b,
                                                                  static_cast<int>(k), f.wa.get(), theta, ldt, g0, acc.get());

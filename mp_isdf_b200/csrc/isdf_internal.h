@@ -39,6 +39,26 @@ inline void require(bool ok, const std::string& msg) { if (!ok) fail(kInvalid, m
     } while (0)
 #define ISDF_LAUNCH_CHECK() ISDF_CUDA(cudaGetLastError())
 
+// ---- profiling -----------------------------------------------------------------
+// Scoped CUDA-event pair around the launches of one kernel family (no-op
+// unless enabled through isdf_profile_enable).
+bool profiling_enabled();
+class ProfileScope {
+public:
+    ProfileScope(const char* name, cudaStream_t s);
+    ~ProfileScope();
+    ProfileScope(const ProfileScope&) = delete;
+    ProfileScope& operator=(const ProfileScope&) = delete;
+
+private:
+    const char* name_;
+    cudaStream_t s_;
+    cudaEvent_t a_ = nullptr, b_ = nullptr;
+};
+#define ISDF_PROFILE_CAT2(a, b) a##b
+#define ISDF_PROFILE_CAT(a, b) ISDF_PROFILE_CAT2(a, b)
+#define ISDF_PROFILE(name, stream) ::isdf::ProfileScope ISDF_PROFILE_CAT(prof_, __LINE__)(name, stream)
+
 // ---- device buffers ----------------------------------------------------------
 // Stream-ordered allocation from the device's default memory pool.
 template <class T>

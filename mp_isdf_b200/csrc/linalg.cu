@@ -146,6 +146,7 @@ void iota_i64(int64_t* out, int64_t n, cudaStream_t s) {
 
 void row_dot(const double* F, int64_t n, int64_t d, const double* x, double* out, cudaStream_t s) {
     if (n <= 0) return;
+    ISDF_PROFILE("row_dot_f64", s);
     row_dot_kernel<<<static_cast<unsigned>((n * 32 + 255) / 256), 256, 0, s>>>(F, n, d, x, out);
     ISDF_LAUNCH_CHECK();
 }
@@ -184,6 +185,7 @@ void gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, int
     dim3 grid(static_cast<unsigned>((M + BM - 1) / BM), static_cast<unsigned>((N + BN - 1) / BN),
               batch);
     require(grid.x < (1u << 31) && grid.y < 65536, "GEMM shape exceeds the launch limits");
+    ISDF_PROFILE("gemm_f64", s);
     gemm_f64_kernel<<<grid, 256, 0, s>>>(M, N, K, A, lda, strideA, B, ldb, strideB, C, ldc,
                                          strideC, accumulate);
     ISDF_LAUNCH_CHECK();

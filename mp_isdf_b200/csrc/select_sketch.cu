@@ -203,6 +203,7 @@ void sketch_fp64(const Context& c, const double* pts, const KeptPoints& kp, cons
     }
     DeviceBuffer<int> bad(1, s);
     bad.zero(s);
+    ISDF_PROFILE("sketch_combine", s);
     combine_sketch_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(
         P.get(), naxes, ell, naxes > 1 ? dscales.get() : nullptr, w, kp.index.get(), n, Yt, ldy,
         bad.get());
@@ -346,9 +347,13 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
     QrState st{Yt, ldy, m, n, pos.get(), col_at.get(), selected.get(), v.get(), tau.get(),
                diag.get(), energy.get(), jpvt.get(), partial.get()};
     for (int64_t j = 0; j <= steps; ++j) {
-        qr_update_kernel<<<nblocks, kQrThreads, 0, s>>>(st, j);
-        ISDF_LAUNCH_CHECK();
+        {
+            ISDF_PROFILE("qrcp_sketch_update", s);
+            qr_update_kernel<<<nblocks, kQrThreads, 0, s>>>(st, j);
+            ISDF_LAUNCH_CHECK();
+        }
         if (j < steps) {
+            ISDF_PROFILE("qrcp_sketch_pivot", s);
             qr_pivot_kernel<<<1, 1024, 0, s>>>(st, j, nblocks);
             ISDF_LAUNCH_CHECK();
         }

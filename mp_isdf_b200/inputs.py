@@ -225,7 +225,7 @@ def _radial(n: int, xi: float):
     return r, w_cheb * r ** 2 * drdx
 
 
-def becke_grid(symbols, coords, level=3, neighbours=8, chunk=262144,
+def becke_grid(symbols, coords, level=3, neighbours=8, chunk=32768,
                zero_below=1e-14):
     """Atom-centred grid; returns (coords[Ng,3], weights[Ng]) in bohr.
 
@@ -253,7 +253,8 @@ def becke_grid(symbols, coords, level=3, neighbours=8, chunk=262144,
     tree = cKDTree(coords)
     rab = np.linalg.norm(coords[:, None] - coords[None], axis=-1)
     out = np.empty_like(wts)
-    for s in range(0, len(pts), chunk):
+
+    def partition(s):
         p = pts[s:s + chunk]
         own = owner[s:s + chunk]
         _, nb = tree.query(p, k=k)
@@ -273,6 +274,11 @@ def becke_grid(symbols, coords, level=3, neighbours=8, chunk=262144,
         cell = s_ab.prod(axis=2)                                         # [b,k]
         mine = cell[nb == own[:, None]].reshape(len(p))
         out[s:s + chunk] = wts[s:s + chunk] * mine / cell.sum(axis=1)
+
+    import concurrent.futures as cf
+    import os
+    with cf.ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
+        list(ex.map(partition, range(0, len(pts), chunk)))
     out[np.abs(out) < zero_below] = 0.0
     return pts, out
 
