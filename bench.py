@@ -42,12 +42,21 @@ def parse():
     ap.add_argument("--precision", choices=("fp64", "mixed"), default=None)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--max-points", type=int, default=0,
+                    help="keep every k-th grid point so that at most this many remain "
+                         "(small cases for profiling; 0 = full grid)")
     return ap.parse_args()
+
+
+MAX_POINTS = 0
 
 
 def workload(cfg_key):
     from mp_isdf_b200 import inputs
     mol, pts, w, cfg = inputs.make_config(cfg_key)
+    if MAX_POINTS and len(pts) > MAX_POINTS:
+        stride = -(-len(pts) // MAX_POINTS)
+        pts, w = pts[::stride].copy(), w[::stride].copy()
     names, factors = inputs.parse_axes(cfg["axes"])
     return mol, pts, w, cfg, names, factors
 
@@ -214,7 +223,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     mol, pts, w, cfg, names, factors = workload(args.config)
-    precision = args.precision or "fp64"
+    forms = [args.precision] if args.precision else ["mixed", "fp64"]
     ctx = capi.Context(mol.atm, mol.bas, mol.env)
     x = torch.tensor(pts, device=dev)
     wt = torch.tensor(w, device=dev)
@@ -224,47 +233,59 @@ def run_ours(args, rank, world, local_rank):
     ell = k + cfg["oversampling"]
     theta = torch.empty(k * n, dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    sel_kw = dict(algorithm="rand_sketch", axes=names, axis_weights=factors, max_rank=k,
-                  oversampling=cfg["oversampling"], seed=cfg.get("sketch_seed", 7),
-                  precision=precision)
 
-    def step():
-        piv, _ = ctx.select(x, wt, **sel_kw)
-        info = ctx.fit(x, wt, piv, theta, precision=precision)
-        return piv, info
+    def sel_kw(precision):
+        return dict(algorithm="rand_sketch", axes=names, axis_weights=factors, max_rank=k,
+                    oversampling=cfg["oversampling"], seed=cfg.get("sketch_seed", 7),
+                    precision=precision)
 
-    for _ in range(args.warmup):
-        piv, info = step()
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    capi.profile_enable(True)
-    capi.profile_read()
-    sampler = ClockSampler(local_rank)
-    sampler.start()
-    times = []
-    for _ in range(args.steps):
-        flush.zero_()
+    def step(precision):
+        piv, sinfo = ctx.select(x, wt, **sel_kw(precision))
+        finfo = ctx.fit(x, wt, piv, theta, precision=precision, want_error=False)
+        return piv, sinfo, finfo
+
+    results = {}
+    for precision in forms:
+        for _ in range(args.warmup):
+            step(precision)
         torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        piv, info = step()
-        b.record()
+        if world > 1:
+            torch.distributed.barrier()
+        capi.profile_enable(True)
+        capi.profile_read()
+        sampler = ClockSampler(local_rank)
+        sampler.start()
+        times = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            piv, sinfo, finfo = step(precision)
+            b.record()
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b) / 1e3)
+        clocks = sampler.stop()
+        capi.profile_enable(False)
+        prof = capi.profile_read()
+        total = sum(times)
+        if world > 1:
+            t = torch.tensor([total], device=dev, dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            total = float(t.item())
+        # pair-space error of this form's Theta, evaluated with FP64 AO values (untimed)
+        einfo = ctx.fit(x, wt, piv, theta, precision=precision, want_error=True)
         torch.cuda.synchronize()
-        times.append(a.elapsed_time(b) / 1e3)
-    clocks = sampler.stop()
-    capi.profile_enable(False)
-    prof = capi.profile_read()
-    total = sum(times)
-    if world > 1:
-        t = torch.tensor([total], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total = float(t.item())
-    per_cluster = total / args.steps / world
-    launches = sum(c for _, c in prof.values()) // max(args.steps, 1)
+        results[precision] = dict(total=total, times=times, prof=prof, clocks=clocks,
+                                  piv=[int(p) for p in piv], sinfo=sinfo, einfo=einfo)
 
-    # e2e through the host-buffer C-ABI
+    head = forms[0]
+    res = results[head]
+    per_cluster = res["total"] / args.steps / world
+    launches = sum(c for _, c in res["prof"].values()) // max(args.steps, 1)
+
+    # e2e through the host-buffer C-ABI (headline form)
     e2e = None
     if not args.no_e2e:
         pts_h = np.ascontiguousarray(pts)
@@ -273,61 +294,87 @@ def run_ours(args, rank, world, local_rank):
         for i in range(max(1, min(3, args.steps)) + 1):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            piv_h, _ = ctx.select_host(pts_h, w_h, **sel_kw)
-            th, finfo = ctx.fit_host(pts_h, w_h, piv_h, precision=precision)
+            piv_h, _ = ctx.select_host(pts_h, w_h, **sel_kw(head))
+            th, _ = ctx.fit_host(pts_h, w_h, piv_h, precision=head)
             dt = time.perf_counter() - t0
             if i:
                 e2e_times.append(dt)
         h2d = 2 * (pts_h.nbytes + w_h.nbytes)
         d2h = th.nbytes + 8 * len(piv_h)
-        e2e = {"value": statistics.mean(e2e_times) / 1.0, "unit": "s",
+        e2e = {"value": statistics.mean(e2e_times) / world, "unit": "s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "path": "isdf_select_host + isdf_fit_host (pageable numpy buffers)"}
 
     if rank != 0:
         return
     hbm, bf16, peak_kind = peaks()
-    fams = sorted(prof.items(), key=lambda kv: -kv[1][0])
+    fams = sorted(res["prof"].items(), key=lambda kv: -kv[1][0])
+    tot_ms = sum(v[0] for v in res["prof"].values())
     roofline = None
     kernels = {}
+    nao_pad = -(-mol.nao // 32) * 32
     for name, (ms, cnt) in fams:
-        bound, units, unit = algorithmic(name, cfg, mol, n_kept, len(names), ell, k)
-        per_launch_ms = ms / cnt
         kernels[name] = {"ms_per_step": ms / args.steps, "launches_per_step": cnt / args.steps,
-                         "share": ms / sum(v[0] for v in prof.values())}
-        if roofline is None and units:
+                         "share": ms / tot_ms}
+        if roofline is not None:
+            continue
+        if name == "project_tc_grad":
+            nt = 16 if 2 * ell <= 16 else 32 if 2 * ell <= 32 else 64
+            units = 2.0 * n_kept * len(names) * nao_pad * nt * 3
+            useful = 2.0 * n_kept * len(names) * mol.nao * 2 * ell
+            ach = units / (ms / args.steps / 1e3) / 1e12
+            roofline = {"kernel": name, "bound": "tensor", "achieved": ach, "peak": bf16,
+                        "unit": "TFLOP/s", "frac": ach / bf16,
+                        "peak_source": f"{peak_kind} bf16 dense (MEASURED_PEAKS.json)",
+                        "traffic": None, "algorithmic_per_step": units,
+                        "useful_flop_per_step": useful,
+                        "flop_model": "3 split-BF16 products x 2*n*(naxes*nao_pad32)*N_tile",
+                        "per_launch_ms": ms / cnt, "launches_per_step": cnt / args.steps}
+        else:
+            bound, units, unit = algorithmic(name, cfg, mol, n_kept, len(names), ell, k)
+            if not units:
+                continue
             achieved = units / (ms / args.steps / 1e3)
-            if bound == "hbm":
-                ach, pk, u = achieved / 1e9, hbm, "GB/s"
-            else:
-                ach, pk, u = achieved / 1e12, bf16, "TFLOP/s"
+            ach, pk, u = (achieved / 1e9, hbm, "GB/s") if bound == "hbm" else (achieved / 1e12, bf16, "TFLOP/s")
             roofline = {"kernel": name, "bound": bound, "achieved": ach, "peak": pk, "unit": u,
                         "frac": ach / pk, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json)",
-                        "traffic": None,
-                        "algorithmic_per_step": units, "per_launch_ms": per_launch_ms,
-                        "launches_per_step": cnt / args.steps}
+                        "traffic": None, "algorithmic_per_step": units,
+                        "per_launch_ms": ms / cnt, "launches_per_step": cnt / args.steps}
     cpu = None
     if not args.no_cpu and world == 1:
         v, cores, sample = cpu_sample(mol, pts, w, names, factors, cfg, n_sample=3000)
         cpu = {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": sample}
+    forms_out = {}
+    for p, r in results.items():
+        forms_out[p] = {"s_per_cluster": r["total"] / args.steps / world,
+                        "step_times_s": r["times"], "anchors": r["piv"],
+                        "pair_relative": r["einfo"].pair_relative, "pair_l2": r["einfo"].pair_l2,
+                        "sketch_columns_reverified": r["sinfo"].verifications,
+                        "clocks": r["clocks"]}
+    extra = {}
+    if "mixed" in results and "fp64" in results:
+        m, f = results["mixed"], results["fp64"]
+        extra = {"speedup_mixed_vs_fp64": f["total"] / m["total"],
+                 "anchors_identical": m["piv"] == f["piv"],
+                 "pair_relative_rel_diff": abs(m["einfo"].pair_relative - f["einfo"].pair_relative)
+                 / f["einfo"].pair_relative}
     line = {
         "metric": METRIC, "value": per_cluster, "unit": "s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["total"] / args.steps * 1e3,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if precision == "fp64" else "bf16x3+f32+f64", "data": "synthetic",
-        "config": workload_desc(args.config, cfg, mol, pts, w, names, precision)
+        "dtype": "f64" if head == "fp64" else "bf16x3+f32+f64", "data": "synthetic",
+        "config": workload_desc(args.config, cfg, mol, pts, w, names, head)
         | {"parallelism": f"replicas x{world}"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-        "clocks": clocks, "kernels": kernels,
-        "result": {"anchors": [int(p) for p in piv], "pair_relative": info.pair_relative,
-                   "retained_rank": info.retained_rank, "condition": info.condition},
-        "step_times_s": times,
+        "clocks": res["clocks"], "kernels": kernels, "forms": forms_out, **extra,
     }
     print(json.dumps(line), flush=True)
 
 
 def main():
     args = parse()
+    global MAX_POINTS
+    MAX_POINTS = args.max_points
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

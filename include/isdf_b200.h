@@ -141,6 +141,8 @@ typedef struct isdf_fit_info {
     double pair_l2;              /* sqrt(sum |w| |p - rec|^2) */
     double pair_relative;
     double theta_w[64];          /* sum_g Theta[a,g] w_g (first 64 anchors) */
+    int64_t fit_path;            /* 0 FP64; 1 mixed; 2 mixed requested, bound too loose -> FP64 */
+    double mixed_bound;          /* a-posteriori bound on the mixed fit's relative pair-error change */
 } isdf_fit_info;
 
 int isdf_fit(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t ng,
@@ -161,6 +163,32 @@ int isdf_pair_error(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, i
 int isdf_pair_error_terms(int64_t n, int64_t k, const double* q_dev, const double* H_dev,
                           const double* X_dev, const double* M_dev, const double* w_dev,
                           double* out_host, void* stream);
+
+/* ---- nuclear-gradient adjoint (no counterpart in the reference, which has no
+ * nuclear derivatives: python/isdf.py:7-8) ------------------------------------
+ * E = sum_g w_g rho_ISDF(g)^2, rho_ISDF(g) = sum_k Theta_kg w_k rho_a(k),
+ * rho_a(k) = phi(a_k)^T D phi(a_k), with grid, anchors (original grid
+ * indices) and weights held fixed; grad_host receives dE/dR (natm x 3, bohr).
+ * dm_host: AO density matrix (nao x nao, row-major).  AO values/gradients are
+ * recomputed per grid chunk (FP64). */
+int isdf_energy_gradient(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t ng,
+                         const int64_t* anchors_host, int64_t k, const double* dm_host,
+                         double* energy, double* grad_host, void* stream);
+/* Moves the atoms of a context (natm x 3, bohr; the basis functions follow). */
+int isdf_ctx_set_coords(isdf_ctx* ctx, const double* coords_host);
+
+/* ---- axis-feature projection -------------------------------------------------
+ * The contraction at the core of the Khatri-Rao sketch
+ * (cpp/src/anchor_select_randomized_id.cpp:299-309, the f_g . u_s and
+ * f_g . v_s sums) and of the fit Gram (python/isdf.py:251-256), exposed on
+ * its own: out[g][a][j] = sum_mu comp_a(g, mu) * W[a*nao + mu][j] for the
+ * unscaled axis blocks, W_host row-major [naxes*nao][nout].  precision
+ * ISDF_FP64: FP64 AO values and FP64 products; ISDF_MIXED: FP32 AO values
+ * evaluated in shared memory and split-BF16 tensor-core products (requires
+ * naxes <= 4, nout <= 64).  out_dev: ng x naxes x nout float64. */
+int isdf_project_axes(isdf_ctx* ctx, const double* xyz_dev, int64_t ng, const int32_t* axes_host,
+                      int32_t naxes, const double* W_host, int32_t nout, int32_t precision,
+                      double* out_dev, void* stream);
 
 /* ---- profiling ---------------------------------------------------------------
  * No counterpart in the reference beyond its per-stage wall times

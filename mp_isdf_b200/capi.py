@@ -25,7 +25,8 @@ SYMBOLS = [
     "isdf_eval_ao", "isdf_eval_ao_host", "isdf_evaluate_axis", "isdf_evaluate_axis_host",
     "isdf_select_args_default", "isdf_select", "isdf_select_host",
     "isdf_fit", "isdf_fit_host", "isdf_pair_error", "isdf_pair_error_terms",
-    "isdf_profile_enable", "isdf_profile_read",
+    "isdf_profile_enable", "isdf_profile_read", "isdf_project_axes",
+    "isdf_energy_gradient", "isdf_ctx_set_coords",
 ]
 
 ALGORITHMS = {"qrcp_dense": 0, "qrcp_online": 1, "rand_sketch": 2}
@@ -47,7 +48,8 @@ class SelectInfo(ctypes.Structure):
 class FitInfo(ctypes.Structure):
     _fields_ = [("n_kept", I64), ("retained_rank", I64), ("condition", F64),
                 ("max_abs_physical_coefficient", F64), ("pair_l2", F64),
-                ("pair_relative", F64), ("theta_w", F64 * 64)]
+                ("pair_relative", F64), ("theta_w", F64 * 64), ("fit_path", I64),
+                ("mixed_bound", F64)]
 
 
 class IsdfError(RuntimeError):
@@ -85,6 +87,9 @@ def lib():
         L.isdf_pair_error.argtypes = [P, P, P, I64, P, I64, P, ctypes.POINTER(F64),
                                       ctypes.POINTER(F64), P]
         L.isdf_pair_error_terms.argtypes = [I64, I64, P, P, P, P, P, P, P]
+        L.isdf_project_axes.argtypes = [P, P, I64, P, I32, P, I32, I32, P, P]
+        L.isdf_energy_gradient.argtypes = [P, P, P, I64, P, I64, P, ctypes.POINTER(F64), P, P]
+        L.isdf_ctx_set_coords.argtypes = [P, P]
         L.isdf_profile_enable.argtypes = [I32]
         L.isdf_profile_read.argtypes = [I32, P, P, P, ctypes.POINTER(I32)]
         _lib = L
@@ -181,6 +186,33 @@ class Context:
                                     _ptr(theta), ctypes.byref(l2), ctypes.byref(rel),
                                     _stream(xyz)))
         return l2.value, rel.value
+
+    def project_axes(self, xyz, axes, W, precision="fp64"):
+        """out[g][a][j] = sum_mu comp_a(g, mu) W[a*nao+mu][j] (CUDA float64 tensor)."""
+        import torch
+        ax = np.array([AXES[a] if isinstance(a, str) else int(a) for a in axes], dtype=np.int32)
+        W = _np(W, np.float64)
+        nout = W.shape[1]
+        out = torch.empty(xyz.shape[0], len(ax), nout, dtype=torch.float64, device=xyz.device)
+        check(lib().isdf_project_axes(self.h, _ptr(xyz), xyz.shape[0], _ptr(ax), len(ax), _ptr(W),
+                                      nout, 1 if precision == "mixed" else 0, _ptr(out),
+                                      _stream(xyz)))
+        return out
+
+    def set_coords(self, coords):
+        """Move the atoms (natm x 3, bohr)."""
+        c = _np(coords, np.float64).reshape(self.natm, 3)
+        check(lib().isdf_ctx_set_coords(self.h, _ptr(c)))
+
+    def energy_gradient(self, xyz, w, anchors, dm):
+        """(E, dE/dR[natm,3]) of E = sum_g w_g rho_ISDF(g)^2 on device tensors."""
+        a = _np(anchors, np.int64)
+        d = _np(dm, np.float64)
+        e = F64()
+        g = np.zeros((self.natm, 3))
+        check(lib().isdf_energy_gradient(self.h, _ptr(xyz), _ptr(w), xyz.shape[0], _ptr(a), len(a),
+                                         _ptr(d), ctypes.byref(e), _ptr(g), _stream(xyz)))
+        return e.value, g
 
     # ---- host arrays -----------------------------------------------------------
     def eval_ao_host(self, xyz, gradient=False):

@@ -1,0 +1,234 @@
+// Nuclear gradient of the ISDF density functional (not in the reference).
+//
+//   E = sum_g w_g rho(g)^2,   rho(g) = sum_k Theta_kg w_k rho_a(k) = h_g . z,
+//   h_g = (Phi_a phi_g)^2,  z = M^+ rho_a,  M = (Phi_a Phi_a^T)^2,
+//   rho_a(k) = phi(a_k)^T D phi(a_k),
+// with grid points, anchors and weights fixed and d phi_mu / d R_A = -grad_r phi_mu
+// for AOs mu on atom A (the AO gradient formula of cpp/src/ao_eval.cpp:240-244).
+// With u_g = 2 w_g rho_g and alpha_gk = 2 u_g z_k G_gk (G = Phi_g Phi_a^T):
+//   grid terms    dE/dR_A -= sum_g sum_{mu in A} (alpha_g Phi_a)_mu grad phi_mu(g)
+//   anchor terms  dE/dR_A -= sum_k sum_{mu in A} c_k,mu grad phi_mu(a_k),
+//                 c = alpha^T Phi_g + 2 y o (Phi_a D) - (W + W^T) Phi_a,
+//                 y = M^+ v, v = sum_g u_g h_g, W = 2 S o (y z^T), S = Phi_a Phi_a^T.
+// The grid is processed in chunks: AO values and gradients are recomputed per
+// chunk (never stored for the whole grid) and reduced on the fly.
+#include "isdf_adjoint.h"
+#include "isdf_reduce.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace isdf {
+namespace {
+
+unsigned nblk(int64_t n) { return static_cast<unsigned>((n + 255) / 256); }
+
+// per point: h = G^2, rho = h.z, u = 2 w rho; E += w rho^2; v += u h;
+// alpha[g][k] = 2 u z_k G_gk (row-major) and alphaT[k][g] (for B += alpha^T Phi)
+__global__ void __launch_bounds__(256)
+adjoint_point_kernel(const double* __restrict__ G, const double* __restrict__ w, int64_t b, int k,
+                     const double* __restrict__ z, double* __restrict__ alpha,
+                     double* __restrict__ alphaT, double* __restrict__ v, double* __restrict__ energy) {
+    __shared__ double sh[8];
+    __shared__ double vs[64];
+    for (int i = threadIdx.x; i < k && i < 64; i += blockDim.x) vs[i] = 0.0;
+    __syncthreads();
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    double e = 0;
+    if (g < b) {
+        const double* Gg = G + g * k;
+        double rho = 0;
+        for (int a = 0; a < k; ++a) rho += Gg[a] * Gg[a] * z[a];
+        const double u = 2.0 * w[g] * rho;
+        e = w[g] * rho * rho;
+        for (int a = 0; a < k; ++a) {
+            const double al = 2.0 * u * z[a] * Gg[a];
+            alpha[g * k + a] = al;
+            alphaT[a * b + g] = al;
+            if (a < 64) atomicAdd(&vs[a], u * Gg[a] * Gg[a]);
+            else atomicAdd(&v[a], u * Gg[a] * Gg[a]);
+        }
+    }
+    e = block_sum<256>(e, sh);
+    if (threadIdx.x == 0) atomicAdd(energy, e);
+    for (int i = threadIdx.x; i < k && i < 64; i += blockDim.x) atomicAdd(&v[i], vs[i]);
+}
+
+// acc[c][mu] += sum_g beta[g][mu] * grad[c][g][mu] over the chunk
+__global__ void __launch_bounds__(256)
+column_dot_kernel(const double* __restrict__ beta, const double* __restrict__ grad, int64_t b,
+                  int nao, double* __restrict__ acc) {
+    const int mu = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (mu >= nao) return;
+    const double* gr = grad + static_cast<int64_t>(c) * b * nao;
+    double s = 0;
+    for (int64_t g = 0; g < b; ++g) s += beta[g * nao + mu] * gr[g * nao + mu];
+    acc[c * nao + mu] += s;
+}
+
+__global__ void gather_kernel(const double* __restrict__ pts, const double* __restrict__ w,
+                              const int64_t* __restrict__ idx, int64_t n, double* __restrict__ op,
+                              double* __restrict__ ow) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t g = idx[i];
+    op[3 * i] = pts[3 * g]; op[3 * i + 1] = pts[3 * g + 1]; op[3 * i + 2] = pts[3 * g + 2];
+    ow[i] = w[g];
+}
+
+// Small anchor-side algebra, one block: see the header comment.
+__global__ void anchor_terms_kernel(int k, int nao, const double* __restrict__ phia,
+                                    const double* __restrict__ S, const double* __restrict__ T,
+                                    const double* __restrict__ DphiT, const double* __restrict__ z,
+                                    const double* __restrict__ v, double* __restrict__ y,
+                                    double* __restrict__ W) {
+    // y = T v
+    for (int a = threadIdx.x; a < k; a += blockDim.x) {
+        double s = 0;
+        for (int b = 0; b < k; ++b) s += T[a * k + b] * v[b];
+        y[a] = s;
+    }
+    __syncthreads();
+    // W = 2 S o (y z^T) + its transpose (symmetrised coefficient of dS)
+    for (int i = threadIdx.x; i < k * k; i += blockDim.x) {
+        const int a = i / k, b = i % k;
+        W[i] = 2.0 * S[i] * (y[a] * z[b] + y[b] * z[a]);
+    }
+    (void)phia; (void)DphiT; (void)nao;
+}
+
+// coef[k][mu] = B[k][mu] + 2 y_k (Phi_a D)[k][mu] - (W Phi_a)[k][mu]
+__global__ void anchor_coef_kernel(int k, int nao, const double* __restrict__ B,
+                                   const double* __restrict__ PhiD, const double* __restrict__ WPhi,
+                                   const double* __restrict__ y, double* __restrict__ coef) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k * nao) return;
+    const int a = i / nao;
+    coef[i] = B[i] + 2.0 * y[a] * PhiD[i] - WPhi[i];
+}
+
+// acc[c][mu] += sum_k coef[k][mu] dphi_a[c][k][mu]
+__global__ void anchor_contrib_kernel(int k, int nao, const double* __restrict__ coef,
+                                      const double* __restrict__ dphia, double* __restrict__ acc) {
+    const int mu = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (mu >= nao) return;
+    double s = 0;
+    for (int a = 0; a < k; ++a) s += coef[a * nao + mu] * dphia[(static_cast<int64_t>(c) * k + a) * nao + mu];
+    acc[c * nao + mu] += s;
+}
+
+// rho_a(k) = (Phi_a D)[k] . Phi_a[k]
+__global__ void rho_anchor_kernel(int k, int nao, const double* __restrict__ PhiD,
+                                  const double* __restrict__ phia, double* __restrict__ rho) {
+    const int a = blockIdx.x;
+    double s = 0;
+    for (int mu = threadIdx.x; mu < nao; mu += 32) s += PhiD[a * nao + mu] * phia[a * nao + mu];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) rho[a] = s;
+}
+
+__global__ void matvec_kernel(int k, const double* __restrict__ T, const double* __restrict__ x,
+                              double* __restrict__ y) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= k) return;
+    double s = 0;
+    for (int b = 0; b < k; ++b) s += T[a * k + b] * x[b];
+    y[a] = s;
+}
+
+}  // namespace
+
+void set_atom_coords(Context& c, const double* coords) {
+    for (int a = 0; a < c.natm; ++a)
+        for (int x = 0; x < 3; ++x) {
+            if (!std::isfinite(coords[3 * a + x])) fail(kInvalid, "atom coordinates must be finite");
+            c.atom_xyz[3 * a + x] = coords[3 * a + x];
+        }
+    for (auto& sh : c.shells) {
+        sh.x = c.atom_xyz[3 * sh.atom];
+        sh.y = c.atom_xyz[3 * sh.atom + 1];
+        sh.z = c.atom_xyz[3 * sh.atom + 2];
+    }
+    if (!c.shells.empty())
+        ISDF_CUDA(cudaMemcpy(c.d_shells, c.shells.data(), c.shells.size() * sizeof(ShellDesc),
+                             cudaMemcpyHostToDevice));
+}
+
+AdjointResult energy_gradient(const Context& c, const double* pts, const double* w,
+                              const KeptPoints& kp, const AnchorFactor& f, const double* dm,
+                              cudaStream_t s) {
+    AdjointResult r;
+    const int64_t n = kp.n, k = f.k, nao = c.nao;
+    r.grad.assign(static_cast<size_t>(c.natm) * 3, 0.0);
+    if (k == 0 || n == 0) return r;
+    require(k <= 4096, "too many anchors for the adjoint");
+    // anchor-side quantities
+    DeviceBuffer<double> dphia(static_cast<size_t>(3 * k * nao), s), Dd(static_cast<size_t>(nao * nao), s),
+        PhiD(static_cast<size_t>(k * nao), s), S(static_cast<size_t>(k * k), s), rhoa(k, s), z(k, s),
+        v(k, s), y(k, s), W(static_cast<size_t>(k * k), s), B(static_cast<size_t>(k * nao), s),
+        WPhi(static_cast<size_t>(k * nao), s), coef(static_cast<size_t>(k * nao), s),
+        acc(static_cast<size_t>(3 * nao), s), energy(1, s);
+    ISDF_CUDA(cudaMemcpyAsync(Dd.get(), dm, nao * nao * sizeof(double), cudaMemcpyHostToDevice, s));
+    v.zero(s); B.zero(s); acc.zero(s); energy.zero(s);
+    {
+        // anchor AO gradients (anchor coordinates gathered by the caller into f)
+        eval_ao<double>(c, f.anchor_pts.get(), k, nullptr, dphia.get(), nao, s);
+    }
+    gemm_f64(k, nao, nao, f.phi_a.get(), nao, 0, Dd.get(), nao, 0, PhiD.get(), nao, 0, 1, false, s);
+    rho_anchor_kernel<<<static_cast<unsigned>(k), 32, 0, s>>>(static_cast<int>(k), static_cast<int>(nao),
+                                                                PhiD.get(), f.phi_a.get(), rhoa.get());
+    ISDF_LAUNCH_CHECK();
+    matvec_kernel<<<nblk(k), 256, 0, s>>>(static_cast<int>(k), f.T.get(), rhoa.get(), z.get());
+    ISDF_LAUNCH_CHECK();
+    gemm_f64(k, k, nao, f.phi_a.get(), nao, 0, f.phi_aT.get(), k, 0, S.get(), k, 0, 1, false, s);
+
+    // grid pass in chunks: AO values + gradients recomputed per chunk
+    const int64_t chunk = std::max<int64_t>(256, std::min<int64_t>(n, (int64_t(1) << 25) / nao));
+    DeviceBuffer<double> cp(static_cast<size_t>(3 * chunk), s), cw(chunk, s),
+        phi(static_cast<size_t>(chunk * nao), s), dphi(static_cast<size_t>(3 * chunk * nao), s),
+        G(static_cast<size_t>(chunk * k), s), alpha(static_cast<size_t>(chunk * k), s),
+        alphaT(static_cast<size_t>(chunk * k), s), beta(static_cast<size_t>(chunk * nao), s);
+    for (int64_t g0 = 0; g0 < n; g0 += chunk) {
+        const int64_t b = std::min(chunk, n - g0);
+        ISDF_PROFILE("adjoint_grid", s);
+        gather_kernel<<<nblk(b), 256, 0, s>>>(pts, w, kp.index.get() + g0, b, cp.get(), cw.get());
+        ISDF_LAUNCH_CHECK();
+        eval_ao<double>(c, cp.get(), b, phi.get(), dphi.get(), nao, s);
+        gemm_f64(b, k, nao, phi.get(), nao, 0, f.phi_aT.get(), k, 0, G.get(), k, 0, 1, false, s);
+        adjoint_point_kernel<<<nblk(b), 256, 0, s>>>(G.get(), cw.get(), b, static_cast<int>(k), z.get(),
+                                                     alpha.get(), alphaT.get(), v.get(), energy.get());
+        ISDF_LAUNCH_CHECK();
+        // B += alpha^T Phi_chunk ; beta = alpha Phi_a
+        gemm_f64(k, nao, b, alphaT.get(), b, 0, phi.get(), nao, 0, B.get(), nao, 0, 1, true, s);
+        gemm_f64(b, nao, k, alpha.get(), k, 0, f.phi_a.get(), nao, 0, beta.get(), nao, 0, 1, false, s);
+        dim3 cg(static_cast<unsigned>((nao + 255) / 256), 3);
+        column_dot_kernel<<<cg, 256, 0, s>>>(beta.get(), dphi.get(), b, static_cast<int>(nao), acc.get());
+        ISDF_LAUNCH_CHECK();
+    }
+    // anchor terms
+    anchor_terms_kernel<<<1, 256, 0, s>>>(static_cast<int>(k), static_cast<int>(nao), f.phi_a.get(), S.get(),
+                                          f.T.get(), PhiD.get(), z.get(), v.get(), y.get(), W.get());
+    ISDF_LAUNCH_CHECK();
+    gemm_f64(k, nao, k, W.get(), k, 0, f.phi_a.get(), nao, 0, WPhi.get(), nao, 0, 1, false, s);
+    anchor_coef_kernel<<<nblk(k * nao), 256, 0, s>>>(static_cast<int>(k), static_cast<int>(nao), B.get(),
+                                                     PhiD.get(), WPhi.get(), y.get(), coef.get());
+    ISDF_LAUNCH_CHECK();
+    dim3 cg(static_cast<unsigned>((nao + 255) / 256), 3);
+    anchor_contrib_kernel<<<cg, 256, 0, s>>>(static_cast<int>(k), static_cast<int>(nao), coef.get(),
+                                             dphia.get(), acc.get());
+    ISDF_LAUNCH_CHECK();
+    std::vector<double> hacc(3 * nao);
+    ISDF_CUDA(cudaMemcpyAsync(hacc.data(), acc.get(), hacc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(&r.energy, energy.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    // d phi / d R_A = -grad_r phi for AOs on atom A
+    for (int64_t mu = 0; mu < nao; ++mu) {
+        const int a = c.ao_atom[mu];
+        for (int cc = 0; cc < 3; ++cc) r.grad[a * 3 + cc] -= hacc[cc * nao + mu];
+    }
+    return r;
+}
+
+}  // namespace isdf

@@ -1,6 +1,8 @@
 // extern "C" boundary of libisdf_b200.so (declared in include/isdf_b200.h).
 #include "../../include/isdf_b200.h"
+#include "isdf_adjoint.h"
 #include "isdf_fit.h"
+#include "isdf_project.h"
 
 #include <cstdio>
 #include <cstring>
@@ -314,14 +316,12 @@ namespace {
 
 void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, const int64_t* anchors,
               int64_t k, int32_t precision, const double* theta_in, double* theta_out,
-              isdf_fit_info* info, double* l2, double* rel, cudaStream_t s) {
+              isdf_fit_info* info, double* l2, double* rel, cudaStream_t s, bool want_error = true) {
     auto& c = ctx_of(ctx);
     DeviceGuard dg(c.device);
     if (ng < 0 || k < 0) isdf::fail(isdf::kInvalid, "sizes must be nonnegative");
     if (precision != ISDF_FP64 && precision != ISDF_MIXED)
         isdf::fail(isdf::kInvalid, "precision must be fp64 or mixed");
-    if (precision == ISDF_MIXED)
-        isdf::fail(isdf::kNotImplemented, "the mixed-precision fit is not available in this build");
     isdf::KeptPoints kp = isdf::compact_points(xyz, w, ng, s);
     isdf::DeviceBuffer<int64_t> didx;
     upload(didx, anchors, static_cast<size_t>(k), s);
@@ -331,7 +331,26 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
     isdf::AnchorFactor f = isdf::factor_anchors(c, apts.get(), aw.get(), k, s);
     const bool have = theta_in != nullptr;
     double* theta = have ? const_cast<double*>(theta_in) : theta_out;
-    isdf::FitOutput o = isdf::fit_grid(c, xyz, w, kp, f, theta, kp.n, have, s);
+    isdf::FitOutput o;
+    if (!have && precision == ISDF_MIXED && isdf::fit_mixed_supported(k)) {
+        o = isdf::fit_grid_mixed(c, xyz, w, kp, f, theta, kp.n, s);
+        o.path = 1;
+        if (!(o.mixed_bound <= isdf::kMixedFitTolerance)) {
+            // the anchors' conditioning can amplify the BF16x3 Gram error past
+            // the tolerance: recompute Theta with FP64 AO values
+            const double bound = o.mixed_bound;
+            o = isdf::fit_grid(c, xyz, w, kp, f, theta, kp.n, false, s);
+            o.mixed_bound = bound;
+            o.path = 2;
+        } else if (want_error) {
+            // pair-space error of the mixed Theta, evaluated with FP64 AO values
+            isdf::FitOutput e = isdf::fit_grid(c, xyz, w, kp, f, theta, kp.n, true, s);
+            o.err2 = e.err2;
+            o.exact2 = e.exact2;
+        }
+    } else {
+        o = isdf::fit_grid(c, xyz, w, kp, f, theta, kp.n, have, s);
+    }
     const double el2 = std::sqrt(o.err2);
     const double erel = o.exact2 ? el2 / std::sqrt(o.exact2) : (el2 == 0 ? 0.0 : INFINITY);
     if (info) {
@@ -342,6 +361,8 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
         info->max_abs_physical_coefficient = o.max_abs_coeff;
         info->pair_l2 = el2;
         info->pair_relative = erel;
+        info->fit_path = o.path;
+        info->mixed_bound = o.mixed_bound;
         for (int64_t a = 0; a < k && a < 64; ++a) info->theta_w[a] = o.theta_w[a];
     }
     if (l2) *l2 = el2;
@@ -353,17 +374,15 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
 int isdf_fit(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, const int64_t* anchors,
              int64_t k, int32_t precision, int32_t want_error, double* theta, isdf_fit_info* info,
              void* stream) {
-    (void)want_error;
     return guarded([&] {
         fit_impl(ctx, xyz, w, ng, anchors, k, precision, nullptr, theta, info, nullptr, nullptr,
-                 as_stream(stream));
+                 as_stream(stream), want_error != 0);
     });
 }
 
 int isdf_fit_host(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng,
                   const int64_t* anchors, int64_t k, int32_t precision, int32_t want_error,
                   double* theta_host, isdf_fit_info* info) {
-    (void)want_error;
     return guarded([&] {
         auto& c = ctx_of(ctx);
         DeviceGuard dg(c.device);
@@ -373,7 +392,7 @@ int isdf_fit_host(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng,
         upload(dw, w, static_cast<size_t>(std::max<int64_t>(ng, 0)), s);
         isdf_fit_info local{};
         fit_impl(ctx, dx.get(), dw.get(), ng, anchors, k, precision, nullptr, dt.get(), &local,
-                 nullptr, nullptr, s);
+                 nullptr, nullptr, s, want_error != 0);
         if (theta_host && k * local.n_kept)
             ISDF_CUDA(cudaMemcpyAsync(theta_host, dt.get(), k * local.n_kept * sizeof(double),
                                       cudaMemcpyDeviceToHost, s));
@@ -389,6 +408,77 @@ int isdf_pair_error(isdf_ctx* ctx, const double* xyz, const double* w, int64_t n
         if (!theta) isdf::fail(isdf::kInvalid, "theta is required");
         fit_impl(ctx, xyz, w, ng, anchors, k, ISDF_FP64, theta, nullptr, nullptr, l2, relative,
                  as_stream(stream));
+    });
+}
+
+int isdf_energy_gradient(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng,
+                         const int64_t* anchors, int64_t k, const double* dm, double* energy,
+                         double* grad, void* stream) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        cudaStream_t s = as_stream(stream);
+        if (ng < 0 || k <= 0 || !anchors || !dm) isdf::fail(isdf::kInvalid, "invalid adjoint arguments");
+        isdf::KeptPoints kp = isdf::compact_points(xyz, w, ng, s);
+        isdf::DeviceBuffer<int64_t> didx;
+        upload(didx, anchors, static_cast<size_t>(k), s);
+        isdf::DeviceBuffer<double> apts(static_cast<size_t>(3 * k), s), aw(k, s);
+        isdf::gather_points(xyz, w, didx.get(), k, ng, apts.get(), aw.get(), s);
+        isdf::AnchorFactor f = isdf::factor_anchors(c, apts.get(), aw.get(), k, s);
+        isdf::AdjointResult r = isdf::energy_gradient(c, xyz, w, kp, f, dm, s);
+        if (energy) *energy = r.energy;
+        if (grad) std::memcpy(grad, r.grad.data(), r.grad.size() * sizeof(double));
+    });
+}
+
+int isdf_ctx_set_coords(isdf_ctx* ctx, const double* coords) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        if (!coords) isdf::fail(isdf::kInvalid, "null coordinates");
+        ISDF_CUDA(cudaDeviceSynchronize());
+        isdf::set_atom_coords(c, coords);
+    });
+}
+
+int isdf_project_axes(isdf_ctx* ctx, const double* xyz, int64_t ng, const int32_t* axes,
+                      int32_t naxes, const double* W, int32_t nout, int32_t precision, double* out,
+                      void* stream) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        cudaStream_t s = as_stream(stream);
+        if (!axes || !W || nout <= 0 || ng < 0) isdf::fail(isdf::kInvalid, "invalid projection arguments");
+        isdf::AxisSpec ax = isdf::make_axis_spec(c, axes, naxes);
+        const int64_t d = static_cast<int64_t>(naxes) * c.nao;
+        if (ng == 0) return;
+        if (precision == ISDF_MIXED) {
+            if (!isdf::project_tc_supported(naxes, nout))
+                isdf::fail(isdf::kNotImplemented, "tensor-core projection needs naxes <= 4 and nout <= 64");
+            std::vector<double> hw(W, W + d * nout);
+            std::vector<int> comps(ax.comp, ax.comp + naxes);
+            isdf::ProjectPlan plan = isdf::make_project_plan(c, comps, hw, nout, s);
+            isdf::DeviceBuffer<float> P(static_cast<size_t>(ng * naxes * nout), s);
+            isdf::DeviceBuffer<int> err(1, s);
+            err.zero(s);
+            isdf::project_tc(c, plan, xyz, nullptr, ng, nullptr, P.get(), naxes * nout, nullptr,
+                             nullptr, err.get(), s);
+            isdf::widen_f32(P.get(), ng * naxes * nout, out, s);
+            int herr = 0;
+            ISDF_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+            ISDF_CUDA(cudaStreamSynchronize(s));
+            if (herr) isdf::fail(isdf::kRuntime, "tensor-core projection timed out");
+        } else if (precision == ISDF_FP64) {
+            isdf::DeviceBuffer<double> F(static_cast<size_t>(ng * d), s), dW(static_cast<size_t>(d * nout), s);
+            ISDF_CUDA(cudaMemcpyAsync(dW.get(), W, d * nout * sizeof(double), cudaMemcpyHostToDevice, s));
+            isdf::eval_axis_features<double>(c, xyz, nullptr, ng, ax, F.get(), d, nullptr, nullptr, s);
+            isdf::gemm_f64(ng, nout, c.nao, F.get(), d, c.nao, dW.get(), nout,
+                           static_cast<int64_t>(c.nao) * nout, out, static_cast<int64_t>(naxes) * nout,
+                           nout, naxes, false, s);
+            ISDF_CUDA(cudaStreamSynchronize(s));
+        } else {
+            isdf::fail(isdf::kInvalid, "precision must be fp64 or mixed");
+        }
     });
 }
 

@@ -8,6 +8,7 @@
 //   value / gradient formulas             cpp/src/ao_eval.cpp:207-249
 //   value layout [p*nao+ao], gradient layout [(axis*Ng+p)*nao+ao]
 //                                         cpp/include/ao_eval.hpp:83-99
+#include "ao_device.cuh"
 #include "isdf_internal.h"
 
 #include <algorithm>
@@ -77,44 +78,6 @@ std::vector<double> c2s_matrix(int l) {
     return t;
 }
 
-// ------------------------------------------------------------------------------
-// constant tables
-// ------------------------------------------------------------------------------
-__host__ __device__ constexpr int c2s_offset(int l) {
-    int off = 0;
-    for (int i = 0; i < l; ++i) off += (2 * i + 1) * (i + 1) * (i + 2) / 2;
-    return off;
-}
-constexpr int kC2sSize = c2s_offset(kMaxL + 1);
-
-__constant__ double c_c2s[kC2sSize];
-__constant__ float c_c2sf[kC2sSize];
-
-namespace {
-
-void upload_c2s_once(int device) {
-    static bool done[64] = {false};
-    if (device < 64 && done[device]) return;
-    std::vector<double> all;
-    for (int l = 0; l <= kMaxL; ++l) {
-        auto t = c2s_matrix(l);
-        all.insert(all.end(), t.begin(), t.end());
-    }
-    std::vector<float> allf(all.begin(), all.end());
-    ISDF_CUDA(cudaMemcpyToSymbol(c_c2s, all.data(), all.size() * sizeof(double)));
-    ISDF_CUDA(cudaMemcpyToSymbol(c_c2sf, allf.data(), allf.size() * sizeof(float)));
-    if (device < 64) done[device] = true;
-}
-
-template <class T> __device__ __forceinline__ T c2s(int idx);
-template <> __device__ __forceinline__ double c2s<double>(int idx) { return c_c2s[idx]; }
-template <> __device__ __forceinline__ float c2s<float>(int idx) { return c_c2sf[idx]; }
-
-__device__ __forceinline__ double dexp(double x) { return exp(x); }
-__device__ __forceinline__ float dexp(float x) { return __expf(x); }
-
-}  // namespace
-
 Context::~Context() {
     cudaFree(d_shells);
     cudaFree(d_exp);
@@ -122,6 +85,8 @@ Context::~Context() {
     cudaFree(d_expf);
     cudaFree(d_coeff);
     cudaFree(d_ao_atom);
+    cudaFree(d_c2s);
+    cudaFree(d_c2sf);
 }
 
 Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nbas,
@@ -170,7 +135,18 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
     }
     c->nao = static_cast<int>(nao);
     c->nshell = static_cast<int>(c->shells.size());
-    upload_c2s_once(c->device);
+    {
+        std::vector<double> all;
+        for (int l = 0; l <= kMaxL; ++l) {
+            auto t = c2s_matrix(l);
+            all.insert(all.end(), t.begin(), t.end());
+        }
+        std::vector<float> allf(all.begin(), all.end());
+        ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c->d_c2s), all.size() * sizeof(double)));
+        ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c->d_c2sf), allf.size() * sizeof(float)));
+        ISDF_CUDA(cudaMemcpy(c->d_c2s, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
+        ISDF_CUDA(cudaMemcpy(c->d_c2sf, allf.data(), allf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
     auto up = [](auto*& dst, const auto& src) {
         using V = std::remove_pointer_t<std::remove_reference_t<decltype(dst)>>;
         if (src.empty()) return;
@@ -192,114 +168,10 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
 // ------------------------------------------------------------------------------
 namespace {
 
-template <int L>
-struct Cart {
-    static constexpr int nc = (L + 1) * (L + 2) / 2;
-    // libcint order: for lx = L..0, for lz = 0..L-lx: ly = L-lx-lz
-    static __host__ __device__ constexpr int lx(int c) {
-        int x = L;
-        while (c >= L - x + 1) { c -= L - x + 1; --x; }
-        return x;
-    }
-    static __host__ __device__ constexpr int lz(int c) {
-        int x = L;
-        while (c >= L - x + 1) { c -= L - x + 1; --x; }
-        return c;
-    }
-    static __host__ __device__ constexpr int ly(int c) { return L - lx(c) - lz(c); }
-};
-
-// Per-thread evaluation of one contracted shell of angular momentum L at one
-// point; `sink.put<C>(ao, v)` receives component C (0 value, 1..3 gradient).
-template <class T, int L, bool GRAD, class Sink>
-__device__ __forceinline__ void eval_shell(const ShellDesc& b, double dxd, double dyd, double dzd,
-                                           const T* __restrict__ exps, const T* __restrict__ coefs,
-                                           Sink& sink) {
-    constexpr int NC = Cart<L>::nc;
-    constexpr int NS = 2 * L + 1;
-    constexpr int OFF = c2s_offset(L);
-    const T x = static_cast<T>(dxd), y = static_cast<T>(dyd), z = static_cast<T>(dzd);
-    const T r2 = static_cast<T>(dxd * dxd + dyd * dyd + dzd * dzd);
-    T px[L + 1], py[L + 1], pz[L + 1];
-    px[0] = py[0] = pz[0] = T(1);
-#pragma unroll
-    for (int i = 1; i <= L; ++i) { px[i] = px[i - 1] * x; py[i] = py[i - 1] * y; pz[i] = pz[i - 1] * z; }
-    T v[NS], vx[NS], vy[NS], vz[NS];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) { v[s] = vx[s] = vy[s] = vz[s] = T(0); }
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-        const int ax = Cart<L>::lx(c), ay = Cart<L>::ly(c), az = Cart<L>::lz(c);
-        const T m = px[ax] * py[ay] * pz[az];
-        T mx = T(0), my = T(0), mz = T(0);
-        if (GRAD) {
-            if (ax) mx = T(ax) * px[ax - 1] * py[ay] * pz[az];
-            if (ay) my = T(ay) * px[ax] * py[ay - 1] * pz[az];
-            if (az) mz = T(az) * px[ax] * py[ay] * pz[az - 1];
-        }
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const T t = c2s<T>(OFF + s * NC + c);
-            v[s] += t * m;
-            if (GRAD) { vx[s] += t * mx; vy[s] += t * my; vz[s] += t * mz; }
-        }
-    }
-    for (int g0 = 0; g0 < b.nctr; g0 += kMaxCtrGroup) {
-        const int ng = min(kMaxCtrGroup, b.nctr - g0);
-        T R[kMaxCtrGroup], Rp[kMaxCtrGroup];
-#pragma unroll
-        for (int j = 0; j < kMaxCtrGroup; ++j) { R[j] = T(0); Rp[j] = T(0); }
-        for (int p = 0; p < b.nprim; ++p) {
-            const T a = exps[b.prim_off + p];
-            const T arg = a * r2;
-            if (arg > T(kExpCut)) continue;
-            const T e = dexp(-arg);
-#pragma unroll
-            for (int j = 0; j < kMaxCtrGroup; ++j) {
-                if (j < ng) {
-                    const T cc = coefs[b.coef_off + (g0 + j) * b.nprim + p] * e;
-                    R[j] += cc;
-                    if (GRAD) Rp[j] -= a * cc;
-                }
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < kMaxCtrGroup; ++j) {
-            if (j < ng) {
-                const int ao0 = b.ao_off + (g0 + j) * NS;
-#pragma unroll
-                for (int s = 0; s < NS; ++s) {
-                    sink.template put<0>(ao0 + s, R[j] * v[s]);
-                    if (GRAD) {
-                        const T two_rp = T(2) * Rp[j] * v[s];
-                        sink.template put<1>(ao0 + s, R[j] * vx[s] + x * two_rp);
-                        sink.template put<2>(ao0 + s, R[j] * vy[s] + y * two_rp);
-                        sink.template put<3>(ao0 + s, R[j] * vz[s] + z * two_rp);
-                    }
-                }
-            }
-        }
-    }
-}
-
-template <class T, bool GRAD, class Sink>
-__device__ __forceinline__ void eval_shell_dispatch(const ShellDesc& b, double dx, double dy,
-                                                    double dz, const T* exps, const T* coefs,
-                                                    Sink& sink) {
-    switch (b.l) {
-    case 0: eval_shell<T, 0, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
-    case 1: eval_shell<T, 1, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
-    case 2: eval_shell<T, 2, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
-    case 3: eval_shell<T, 3, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
-    case 4: eval_shell<T, 4, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
-    case 5: eval_shell<T, 5, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
-    default: eval_shell<T, 6, GRAD>(b, dx, dy, dz, exps, coefs, sink); break;
-    }
-}
-
 template <class T>
 struct RawSink {
     T* val; T* grad; int64_t p, n, ld; bool want_val;
+    __device__ __forceinline__ bool wants(int, int) const { return true; }
     template <int C> __device__ __forceinline__ void put(int ao, T v) {
         if (C == 0) { if (want_val) val[p * ld + ao] = v; }
         else grad[((C - 1) * n + p) * ld + ao] = v;
@@ -309,6 +181,7 @@ struct RawSink {
 template <class T>
 struct AxisSink {
     T* out; int64_t p, ld; const AxisSpec* ax; const int* off; double sq[4]; bool count;
+    __device__ __forceinline__ bool wants(int, int) const { return true; }
     template <int C> __device__ __forceinline__ void put(int ao, T v) {
         if (!((ax->need_mask >> C) & 1)) return;
         if (count) sq[C] += static_cast<double>(v) * static_cast<double>(v);
@@ -323,22 +196,22 @@ constexpr int kShellLanes = 4;
 template <class T, bool GRAD>
 __global__ void __launch_bounds__(kPtsPerBlock * kShellLanes)
 ao_raw_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restrict__ exps,
-              const T* __restrict__ coefs, const double* __restrict__ pts, int64_t n,
-              T* val, T* grad, int64_t ld, bool want_val) {
+              const T* __restrict__ coefs, const T* __restrict__ c2s, const double* __restrict__ pts,
+              int64_t n, T* val, T* grad, int64_t ld, bool want_val) {
     const int64_t p = static_cast<int64_t>(blockIdx.x) * kPtsPerBlock + threadIdx.x;
     if (p >= n) return;
     const double px = pts[3 * p], py = pts[3 * p + 1], pz = pts[3 * p + 2];
     RawSink<T> sink{val, grad, p, n, ld, want_val};
     for (int sh = threadIdx.y; sh < nshell; sh += kShellLanes) {
         const ShellDesc b = shells[sh];
-        eval_shell_dispatch<T, GRAD>(b, px - b.x, py - b.y, pz - b.z, exps, coefs, sink);
+        eval_shell_any<T, GRAD>(b, px - b.x, py - b.y, pz - b.z, exps, coefs, c2s, sink);
     }
 }
 
 template <class T, bool GRAD>
 __global__ void __launch_bounds__(kPtsPerBlock * kShellLanes)
 ao_axis_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restrict__ exps,
-               const T* __restrict__ coefs, const double* __restrict__ pts,
+               const T* __restrict__ coefs, const T* __restrict__ c2s, const double* __restrict__ pts,
                const int64_t* __restrict__ index, int64_t n, AxisSpec ax, T* out, int64_t ld,
                double* sumsq, const double* __restrict__ weights, int nao) {
     __shared__ double red[kPtsPerBlock * kShellLanes][4];
@@ -354,7 +227,7 @@ ao_axis_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __rest
         sink.count = sumsq != nullptr && (weights == nullptr || weights[gi] != 0.0);
         for (int sh = threadIdx.y; sh < nshell; sh += kShellLanes) {
             const ShellDesc b = shells[sh];
-            eval_shell_dispatch<T, GRAD>(b, px - b.x, py - b.y, pz - b.z, exps, coefs, sink);
+            eval_shell_any<T, GRAD>(b, px - b.x, py - b.y, pz - b.z, exps, coefs, c2s, sink);
         }
     }
     if (sumsq) {
@@ -376,6 +249,9 @@ template <> const float* exps_of<float>(const Context& c) { return c.d_expf; }
 template <class T> const T* coefs_of(const Context& c);
 template <> const double* coefs_of<double>(const Context& c) { return c.d_coef; }
 template <> const float* coefs_of<float>(const Context& c) { return c.d_coeff; }
+template <class T> const T* c2s_of(const Context& c);
+template <> const double* c2s_of<double>(const Context& c) { return c.d_c2s; }
+template <> const float* c2s_of<float>(const Context& c) { return c.d_c2sf; }
 
 }  // namespace
 
@@ -389,11 +265,12 @@ void eval_ao(const Context& c, const double* pts, int64_t n, T* out_val, T* out_
     require(nb < (1ll << 31), "too many grid points for one launch");
     if (out_grad)
         ao_raw_kernel<T, true><<<static_cast<unsigned>(nb), block, 0, s>>>(
-            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, n, out_val, out_grad, ld,
-            out_val != nullptr);
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), c2s_of<T>(c), pts, n, out_val,
+            out_grad, ld, out_val != nullptr);
     else
         ao_raw_kernel<T, false><<<static_cast<unsigned>(nb), block, 0, s>>>(
-            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, n, out_val, nullptr, ld, true);
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), c2s_of<T>(c), pts, n, out_val,
+            nullptr, ld, true);
     ISDF_LAUNCH_CHECK();
 }
 
@@ -410,12 +287,12 @@ void eval_axis_features(const Context& c, const double* pts, const int64_t* inde
     const bool grad = (ax.need_mask & 0xE) != 0;
     if (grad)
         ao_axis_kernel<T, true><<<static_cast<unsigned>(nb), block, 0, s>>>(
-            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, index, n, ax, out, ld,
-            sumsq, weights, c.nao);
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), c2s_of<T>(c), pts, index, n, ax,
+            out, ld, sumsq, weights, c.nao);
     else
         ao_axis_kernel<T, false><<<static_cast<unsigned>(nb), block, 0, s>>>(
-            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, index, n, ax, out, ld,
-            sumsq, weights, c.nao);
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), c2s_of<T>(c), pts, index, n, ax,
+            out, ld, sumsq, weights, c.nao);
     ISDF_LAUNCH_CHECK();
 }
 

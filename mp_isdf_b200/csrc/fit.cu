@@ -12,11 +12,13 @@
 // Pair-space error (python/isdf.py:154-191), per grid point:
 //   |p_g - C^T X_g|^2 = q_g^2 - 2 X_g.h_g + X_g^T M X_g,  q_g = |phi_g|^2.
 #include "isdf_fit.h"
+#include "isdf_project.h"
 #include "isdf_reduce.cuh"
 
 #include <algorithm>
 #include <cmath>
 #include <limits>
+#include <string>
 
 namespace isdf {
 namespace {
@@ -207,6 +209,9 @@ AnchorFactor factor_anchors(const Context& c, const double* anchor_pts, const do
     f.T.reset(static_cast<size_t>(k * k), s);
     f.wa.reset(k, s);
     ISDF_CUDA(cudaMemcpyAsync(f.wa.get(), anchor_w, k * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    f.anchor_pts.reset(static_cast<size_t>(3 * k), s);
+    ISDF_CUDA(cudaMemcpyAsync(f.anchor_pts.get(), anchor_pts, 3 * k * sizeof(double),
+                              cudaMemcpyDeviceToDevice, s));
     eval_ao<double>(c, anchor_pts, k, f.phi_a.get(), nullptr, nao, s);
     transpose_kernel<<<blocks_for(k * nao), 256, 0, s>>>(f.phi_a.get(), k, nao, f.phi_aT.get());
     ISDF_LAUNCH_CHECK();
@@ -332,6 +337,147 @@ FitOutput fit_grid(const Context& c, const double* pts, const double* w, const K
     out.exact2 = h[1];
     out.max_abs_coeff = h[2];
     out.n = n;
+    return out;
+}
+
+namespace {
+
+// Mixed-precision fit epilogue: G (FP32, from the tensor-core projection) ->
+// h = G o G, X = T h, Theta = X / w_anchor in FP64; also Theta.w, max |X|, and
+// the terms of an a-posteriori bound on how far the pair error of this Theta
+// can lie from the FP64 fit's:  excess <= lambda_max(T) * sum_g |w_g| |dh_g|^2,
+// |dG_ga| <= kFitGramBound |phi_g| |phi_a|  (dh = 2 G dG + dG^2).
+constexpr double kFitGramBound = 2e-5;
+
+__global__ void __launch_bounds__(256)
+fit_mixed_kernel(const float* __restrict__ G, const float* __restrict__ psq, int64_t n, int k,
+                 const double* __restrict__ T, const double* __restrict__ M,
+                 const double* __restrict__ anorm, const double* __restrict__ wa,
+                 const double* __restrict__ w, const int64_t* __restrict__ index,
+                 double* __restrict__ theta, int64_t ldt, double* __restrict__ tw,
+                 double* __restrict__ acc) {
+    extern __shared__ double sm[];
+    double* Ts = sm;                // k*k
+    double* Ms = sm + k * k;        // k*k
+    double* tws = sm + 2 * k * k;   // k partial sums
+    __shared__ double red[8];
+    for (int i = threadIdx.x; i < k * k; i += blockDim.x) { Ts[i] = T[i]; Ms[i] = M[i]; }
+    for (int i = threadIdx.x; i < k; i += blockDim.x) tws[i] = 0.0;
+    __syncthreads();
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    double mx = 0, dh2 = 0, e2 = 0, q2 = 0;
+    if (g < n) {
+        double h[64], x[64];
+        const double qg = static_cast<double>(psq[g * 4]);   // |phi_g|^2
+        const double fn = sqrt(qg);
+        const double aw = fabs(w[index[g]]);
+        for (int a = 0; a < k; ++a) {
+            const double gv = static_cast<double>(G[g * k + a]);
+            h[a] = gv * gv;
+            const double dG = kFitGramBound * fn * anorm[a];
+            const double dh = 2.0 * fabs(gv) * dG + dG * dG;
+            dh2 += dh * dh;
+        }
+        const double wg = w[index[g]];
+        double xh = 0;
+        for (int a = 0; a < k; ++a) {
+            double xa = 0;
+            for (int b = 0; b < k; ++b) xa += Ts[a * k + b] * h[b];
+            x[a] = xa;
+            xh += xa * h[a];
+            mx = fmax(mx, fabs(xa));
+            const double th = xa / wa[a];
+            theta[a * ldt + g] = th;
+            atomicAdd(&tws[a], th * wg);
+        }
+        double xmx = 0;
+        for (int a = 0; a < k; ++a) {
+            double t = 0;
+            for (int b = 0; b < k; ++b) t += Ms[a * k + b] * x[b];
+            xmx += x[a] * t;
+        }
+        dh2 *= aw;
+        e2 = aw * (qg * qg - 2.0 * xh + xmx);
+        q2 = aw * qg * qg;
+    }
+    dh2 = block_sum<256>(dh2, red);
+    e2 = block_sum<256>(e2, red);
+    q2 = block_sum<256>(q2, red);
+    if (threadIdx.x == 0) {
+        atomicAdd(&acc[3], dh2);
+        atomicAdd(&acc[4], e2);
+        atomicAdd(&acc[5], q2);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    if (threadIdx.x % 32 == 0)
+        atomicMax(reinterpret_cast<unsigned long long*>(&acc[2]),
+                  static_cast<unsigned long long>(__double_as_longlong(mx)));
+    __syncthreads();
+    for (int i = threadIdx.x; i < k; i += blockDim.x) atomicAdd(&tw[i], tws[i]);
+}
+
+__global__ void row_norms_kernel(const double* __restrict__ a, int rows, int cols, double* __restrict__ out) {
+    const int r = blockIdx.x;
+    double s = 0;
+    for (int c = threadIdx.x; c < cols; c += 32) s += a[static_cast<int64_t>(r) * cols + c] * a[static_cast<int64_t>(r) * cols + c];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) out[r] = sqrt(s);
+}
+
+}  // namespace
+
+bool fit_mixed_supported(int64_t k) { return k >= 1 && k <= 64 && project_tc_supported(1, static_cast<int>(k)); }
+
+FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
+                         const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s) {
+    FitOutput out;
+    const int64_t n = kp.n, k = f.k, nao = c.nao;
+    out.theta_w.assign(k, 0.0);
+    if (n == 0 || k == 0) return out;
+    std::vector<double> phi(static_cast<size_t>(k * nao)), W(static_cast<size_t>(k * nao));
+    ISDF_CUDA(cudaMemcpyAsync(phi.data(), f.phi_a.get(), phi.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    for (int64_t a = 0; a < k; ++a)
+        for (int64_t mu = 0; mu < nao; ++mu) W[mu * k + a] = phi[a * nao + mu];
+    ProjectPlan plan = make_project_plan(c, {0}, W, static_cast<int>(k), s);
+    DeviceBuffer<float> G(static_cast<size_t>(n * k), s), psq(static_cast<size_t>(n * 4), s);
+    DeviceBuffer<int> err(1, s);
+    DeviceBuffer<double> acc(6, s), tw(k, s), anorm(k, s);
+    err.zero(s);
+    acc.zero(s);
+    tw.zero(s);
+    psq.zero(s);
+    row_norms_kernel<<<static_cast<unsigned>(k), 32, 0, s>>>(f.phi_a.get(), static_cast<int>(k),
+                                                            static_cast<int>(nao), anorm.get());
+    ISDF_LAUNCH_CHECK();
+    project_tc(c, plan, pts, kp.index.get(), n, nullptr, G.get(), k, nullptr, psq.get(), err.get(), s);
+    {
+        ISDF_PROFILE("fit_mixed", s);
+        const size_t smem = static_cast<size_t>(2 * k * k + k) * sizeof(double);
+        fit_mixed_kernel<<<blocks_for(n), 256, smem, s>>>(G.get(), psq.get(), n, static_cast<int>(k),
+                                                          f.T.get(), f.M.get(), anorm.get(), f.wa.get(),
+                                                          w, kp.index.get(), theta, ldt, tw.get(),
+                                                          acc.get());
+        ISDF_LAUNCH_CHECK();
+    }
+    double h[6];
+    int herr = 0;
+    ISDF_CUDA(cudaMemcpyAsync(h, acc.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(out.theta_w.data(), tw.get(), k * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    if (herr) fail(kRuntime, "tensor-core fit pipeline timed out (error flags " + std::to_string(herr) + ")");
+    // lambda_max(T) = 1 / s_min^2 over the retained singular values of C^T
+    double smin = 0;
+    for (double x : f.sv)
+        if (x > 1e-12 * (f.sv.empty() ? 0.0 : f.sv.front())) smin = x;
+    const double lam = smin > 0 ? 1.0 / (smin * smin) : std::numeric_limits<double>::infinity();
+    out.mixed_bound = (h[4] > 0) ? lam * h[3] / (2.0 * h[4]) : std::numeric_limits<double>::infinity();
+    out.max_abs_coeff = h[2];
+    out.n = n;
+    out.err2 = std::numeric_limits<double>::quiet_NaN();
+    out.exact2 = std::numeric_limits<double>::quiet_NaN();
     return out;
 }
 

@@ -11,6 +11,7 @@ struct AnchorFactor {
     DeviceBuffer<double> M;               // (Phi_a Phi_a^T)^2, k x k
     DeviceBuffer<double> T;               // pseudo-inverse of M (SVD cutoff 1e-12 on C)
     DeviceBuffer<double> wa;              // anchor weights
+    DeviceBuffer<double> anchor_pts;      // anchor coordinates, k x 3
     std::vector<double> sv;               // singular values of C^T, descending
     int retained = 0;
     double condition = 0;
@@ -21,7 +22,13 @@ struct FitOutput {
     int64_t n = 0;
     double err2 = 0, exact2 = 0, max_abs_coeff = 0;
     std::vector<double> theta_w;          // sum_g Theta[a, g] w_g
+    double mixed_bound = 0;               // bound on |rel. pair-error change| vs FP64 (mixed fit)
+    int path = 0;                         // 0 FP64, 1 mixed, 2 mixed bound too loose -> FP64
 };
+
+// Largest relative pair-error deviation from the FP64 fit that the mixed fit
+// accepts (10x below the 1e-8 target); beyond it the fit is redone in FP64.
+constexpr double kMixedFitTolerance = 1e-9;
 
 AnchorFactor factor_anchors(const Context& c, const double* anchor_pts, const double* anchor_w,
                             int64_t k, cudaStream_t s);
@@ -31,6 +38,13 @@ AnchorFactor factor_anchors(const Context& c, const double* anchor_pts, const do
 FitOutput fit_grid(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
                    const AnchorFactor& f, double* theta, int64_t ldt, bool have_theta,
                    cudaStream_t s);
+
+// Mixed precision: G from the fused FP32-AO / split-BF16 tensor-core projection,
+// then h, X = T h and Theta in FP64.  The pair-space error is not evaluated
+// here (see fit_grid with have_theta).
+bool fit_mixed_supported(int64_t k);
+FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
+                         const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s);
 
 void gather_points(const double* pts, const double* w, const int64_t* idx, int64_t n,
                    int64_t npts_total, double* out_pts, double* out_w, cudaStream_t s);

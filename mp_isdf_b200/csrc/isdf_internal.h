@@ -122,6 +122,8 @@ struct Context {
     float* d_expf = nullptr;
     float* d_coeff = nullptr;
     int32_t* d_ao_atom = nullptr;
+    double* d_c2s = nullptr;              // cartesian->spherical tables, l = 0..kMaxL
+    float* d_c2sf = nullptr;
     ~Context();
 };
 
@@ -158,6 +160,7 @@ void eval_axis_features(const Context& c, const double* pts, const int64_t* inde
 
 // ---- small dense kernels ---------------------------------------------------------
 void iota_i64(int64_t* out, int64_t n, cudaStream_t s);
+void widen_f32(const float* x, int64_t n, double* y, cudaStream_t s);
 // out[g] = F[g,:] . x (warp per row); |F[g,:]|^2 when x is null.
 void row_dot(const double* F, int64_t n, int64_t d, const double* x, double* out, cudaStream_t s);
 // a[i*d + k] = scale * f[i] * f[k]   (explicit weighted pair vector)

@@ -1,0 +1,48 @@
+// Fused AO-evaluation + tensor-core projection (see project_tc.cu).
+#pragma once
+
+#include "isdf_internal.h"
+
+namespace isdf {
+
+struct ProjectArgs {
+    const ShellDesc* shells;
+    const float* expf_;
+    const float* coeff_;
+    const float* c2sf;
+    float* point_sq;           // [n][4] per-point sums of squares per component, or null
+    int nao;
+    const double* pts;
+    const int64_t* index;      // kept-point gather (may be null)
+    const double* weights;     // for the sums of squares (may be null)
+    int64_t n;
+    int nchunks;
+    const int* chunk_shell_begin;
+    const int* chunk_shell_end;
+    const uint8_t* wimg;       // per chunk: nax x (hi, lo) BF16 tiles
+    int comp_mask;
+    int axis_comp[4];
+    float* out;                // out[g*ld_out + a*nout + j]
+    int64_t ld_out;
+    int nout;
+    double* sumsq;             // [4] or null
+    int* error;                // bit flags of bounded waits that gave up
+};
+
+struct ProjectPlan {
+    int nax = 0, nout = 0, nt = 0, nchunks = 0, comp_mask = 0;
+    int axis_comp[4] = {0, 0, 0, 0};
+    bool grad = false;
+    DeviceBuffer<uint16_t> wimg;
+    DeviceBuffer<int> chunk_begin, chunk_end;
+};
+
+// W is row-major [nax*nao][nout] in FP64; it is split into BF16 hi + lo.
+ProjectPlan make_project_plan(const Context& c, const std::vector<int>& axis_comp,
+                              const std::vector<double>& W, int nout, cudaStream_t s);
+bool project_tc_supported(int nax, int nout);
+void project_tc(const Context& c, const ProjectPlan& plan, const double* pts, const int64_t* index,
+                int64_t n, const double* weights, float* out, int64_t ld_out, double* sumsq,
+                float* point_sq, int* error, cudaStream_t s);
+
+}  // namespace isdf

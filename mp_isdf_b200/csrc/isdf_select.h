@@ -46,6 +46,22 @@ struct SketchQR {
     std::vector<int64_t> jpvt;       // 0-based pivot columns, per step
     std::vector<double> diag;        // |R_jj|
     std::vector<double> energy;      // sum of squares of row j of R
+    int64_t reverified = 0;          // columns recomputed exactly (verified mode)
+};
+
+// Everything needed to recompute a sketch column exactly in FP64 (device
+// pointers): used by the verified QR of a mixed-precision sketch.
+struct ExactSketchSource {
+    const Context* ctx = nullptr;
+    int naxes = 0;
+    int comp[16] = {};
+    const double* scales = nullptr;  // naxes
+    const double* WT = nullptr;      // (2 ell) x d, row-major
+    const double* pts = nullptr;
+    const int64_t* index = nullptr;  // kept-point gather
+    const double* w = nullptr;
+    int64_t ell = 0;
+    double* delta = nullptr;         // per-column absolute error bounds (0 = exact)
 };
 
 AxisSpec make_axis_spec(const Context& c, const int32_t* axes, int naxes);
@@ -56,8 +72,21 @@ void sketch_factors(int64_t d, int64_t ell, uint64_t seed, std::vector<double>& 
                     std::vector<double>& v);
 
 // Full column-pivoted Householder QR of the ell x n sketch stored row-wise
-// (Yt[s*ldy + g]); modifies Yt.
-SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t s);
+// (Yt[s*ldy + g]); modifies Yt.  With `exact`, columns whose error interval
+// reaches the best candidate are recomputed in FP64 before each pivot choice.
+SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t s,
+                     const ExactSketchSource* exact = nullptr);
+
+struct MixedSketch {
+    DeviceBuffer<double> scales, WT, delta;
+    ExactSketchSource source;
+};
+// Fills Yt with the mixed-precision sketch of the kept points and returns the
+// FP64 recomputation source (scales, W^T, error bounds) for the verified QR.
+MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& kp, const double* w,
+                         const AxisSpec& ax, const double* axis_weights, int64_t ell,
+                         const std::vector<double>& u, const std::vector<double>& v, double* Yt,
+                         int64_t ldy, cudaStream_t s);
 
 std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, const double* w,
                                         int64_t ng, const SelectOptions& o, cudaStream_t s,

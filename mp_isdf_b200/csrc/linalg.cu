@@ -138,6 +138,19 @@ __global__ void iota_kernel(int64_t* out, int64_t n) {
 
 }  // namespace
 
+namespace {
+__global__ void widen_kernel(const float* __restrict__ x, int64_t n, double* __restrict__ y) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = static_cast<double>(x[i]);
+}
+}  // namespace
+
+void widen_f32(const float* x, int64_t n, double* y, cudaStream_t s) {
+    if (n <= 0) return;
+    widen_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(x, n, y);
+    ISDF_LAUNCH_CHECK();
+}
+
 void iota_i64(int64_t* out, int64_t n, cudaStream_t s) {
     if (n <= 0) return;
     iota_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(out, n);

@@ -11,6 +11,7 @@
 //   Y[s,g] = sqrt|w_g|/sqrt(ell) (f_g.u_s)(f_g.v_s)   :297-309
 //   dgeqp3 of Y, row energies -> tails, numerical rank, exact-rank / tolerance
 //   rank selection                          cpp/src/anchor_select_randomized_id.cpp:320-374
+#include "isdf_project.h"
 #include "isdf_select.h"
 #include "isdf_reduce.cuh"
 
@@ -215,157 +216,123 @@ void sketch_fp64(const Context& c, const double* pts, const KeptPoints& kp, cons
 }
 
 // ------------------------------------------------------------------------------
-// column-pivoted Householder QR of the (ell x n) sketch, dgeqp3 pivot rule:
-// at step j the column with the largest trailing norm wins, ties broken by the
-// smallest current (swapped) column position.
+// mixed-precision sketch: fused FP32 AO evaluation + split-BF16 tensor-core
+// projection, FP64 combination with per-column error bounds
 // ------------------------------------------------------------------------------
 namespace {
 
-constexpr int kQrThreads = 256;
+// Relative accuracy of a split-BF16 (hi*hi + hi*lo + lo*hi) dot product of
+// FP32 features with FP64 weights, with a 10x margin over its ~2^-16
+// representation error: |d(f.u)| <= kSplitBf16Bound * |f| * |u_scale|.
+constexpr double kSplitBf16Bound = 1.5e-4;
 
-struct QrState {
-    double* Yt; int64_t ldy; int64_t m; int64_t n;
-    int64_t* pos;        // current position of each column
-    int64_t* col_at;     // column at each position (inverse of pos)
-    char* selected;
-    double* v;           // current reflector (m)
-    double* tau;         // per step
-    double* diag;        // |R_jj| per step
-    double* energy;      // row energies of R per step
-    int64_t* jpvt;       // pivot columns per step
-    ArgKey* partial;     // per block
-};
-
-// Apply reflector j-1 (if j > 0) to every unselected column, accumulate the
-// final row-(j-1) energy and produce per-block argmax keys of the rows j..m-1
-// norms.
-__global__ void __launch_bounds__(kQrThreads) qr_update_kernel(QrState st, int64_t j) {
-    const int64_t g = static_cast<int64_t>(blockIdx.x) * kQrThreads + threadIdx.x;
-    __shared__ ArgKey ksh[kQrThreads / 32];
-    ArgKey key = key_none();
-    double e = 0.0;
-    if (g < st.n && !st.selected[g]) {
-        double* col = st.Yt + g;
-        const int64_t ld = st.ldy;
-        if (j > 0) {
-            const double t = st.tau[j - 1];
-            if (t != 0.0) {
-                double dot = 0;
-                for (int64_t i = j - 1; i < st.m; ++i) dot += st.v[i] * col[i * ld];
-                dot *= t;
-                for (int64_t i = j - 1; i < st.m; ++i) col[i * ld] -= st.v[i] * dot;
-            }
-            const double r = col[(j - 1) * ld];
-            e = r * r;
+// Yt[s][g] = sw/sqrt(ell) L_s R_s from the FP32 per-axis partials, and the
+// absolute error bound of the column's norm:
+//   delta_g = k * sw/sqrt(ell) * |f_g| * sqrt(sum_s (|L_s| + |R_s| + k|f_g|)^2)
+__global__ void combine_mixed_kernel(const float* __restrict__ P, const float* __restrict__ psq,
+                                     int naxes, const int* __restrict__ comp, int64_t ell,
+                                     const double* __restrict__ scales, const double* __restrict__ w,
+                                     const int64_t* __restrict__ index, int64_t n,
+                                     double* __restrict__ Yt, int64_t ldy, double* __restrict__ delta,
+                                     int* __restrict__ bad) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const double sw = sqrt(fabs(w[index[g]])) / sqrt(static_cast<double>(ell));
+    const float* pg = P + g * naxes * 2 * ell;
+    double f2 = 0;
+    for (int a = 0; a < naxes; ++a) {
+        const double sc = scales ? scales[a] : 1.0;
+        f2 += sc * sc * static_cast<double>(psq[g * 4 + comp[a]]);
+    }
+    const double fn = sqrt(f2);
+    const double k = kSplitBf16Bound;
+    double bound2 = 0;
+    bool ok = true;
+    for (int64_t s = 0; s < ell; ++s) {
+        double left = 0, right = 0;
+        for (int a = 0; a < naxes; ++a) {
+            const double sc = scales ? scales[a] : 1.0;
+            left += sc * static_cast<double>(pg[a * 2 * ell + s]);
+            right += sc * static_cast<double>(pg[a * 2 * ell + ell + s]);
         }
-        if (j < st.m) {
-            double nrm = 0;
-            for (int64_t i = j; i < st.m; ++i) { const double x = col[i * ld]; nrm += x * x; }
-            key = ArgKey{nrm, st.pos[g], g};
-        }
+        const double y = sw * left * right;
+        ok = ok && isfinite(y);
+        Yt[s * ldy + g] = y;
+        const double e = fabs(left) + fabs(right) + k * fn;
+        bound2 += e * e;
     }
-    // block reductions
-    __shared__ double esh[kQrThreads / 32];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
-    if (threadIdx.x % 32 == 0) esh[threadIdx.x / 32] = e;
-    ArgKey best = block_best<kQrThreads>(key, ksh);
-    if (threadIdx.x == 0) {
-        double et = 0;
-        for (int i = 0; i < kQrThreads / 32; ++i) et += esh[i];
-        if (j > 0 && et != 0.0) atomicAdd(&st.energy[j - 1], et);
-        st.partial[blockIdx.x] = best;
-    }
-}
-
-// Reduce the block keys, record the pivot, swap positions, build reflector j.
-__global__ void __launch_bounds__(1024) qr_pivot_kernel(QrState st, int64_t j, int nblocks) {
-    __shared__ ArgKey ksh[32];
-    ArgKey k = key_none();
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-        if (key_better(st.partial[b], k)) k = st.partial[b];
-    k = block_best<1024>(k, ksh);
-    __shared__ int64_t piv;
-    __shared__ double sh_scale;
-    if (threadIdx.x == 0) piv = k.col;
-    __syncthreads();
-    if (piv < 0) return;   // every column already pivoted (cannot happen for j < min(m, n))
-    if (threadIdx.x == 0) {
-        const int64_t p = piv;
-        st.jpvt[j] = p;
-        st.selected[p] = 1;
-        // dgeqp3 swaps the pivot column into position j
-        const int64_t pp = st.pos[p];
-        const int64_t cj = st.col_at[j];
-        st.col_at[pp] = cj;
-        st.pos[cj] = pp;
-        st.col_at[j] = p;
-        st.pos[p] = j;
-        const double* col = st.Yt + p;
-        const double alpha = col[j * st.ldy];
-        double xnorm = 0;
-        for (int64_t i = j + 1; i < st.m; ++i) xnorm = hypot(xnorm, col[i * st.ldy]);
-        double beta, tau, scale;
-        if (xnorm == 0.0) {
-            beta = alpha; tau = 0.0; scale = 0.0;
-        } else {
-            beta = -copysign(hypot(alpha, xnorm), alpha);
-            tau = (beta - alpha) / beta;
-            scale = 1.0 / (alpha - beta);
-        }
-        st.tau[j] = tau;
-        st.diag[j] = fabs(beta);
-        atomicAdd(&st.energy[j], beta * beta);
-        sh_scale = scale;
-    }
-    __syncthreads();
-    const int64_t p = piv;
-    for (int64_t i = threadIdx.x; i < st.m; i += blockDim.x) {
-        double vi;
-        if (i < j) vi = 0.0;
-        else if (i == j) vi = 1.0;
-        else vi = st.Yt[i * st.ldy + p] * sh_scale;
-        st.v[i] = vi;
-    }
+    delta[g] = k * sw * fn * sqrt(bound2);
+    if (!ok) atomicOr(bad, 1);
 }
 
 }  // namespace
 
-SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t s) {
-    SketchQR out;
-    const int64_t steps = std::min(m, n);
-    if (steps == 0) return out;
-    const int nblocks = static_cast<int>((n + kQrThreads - 1) / kQrThreads);
-    DeviceBuffer<int64_t> pos(n, s), col_at(n, s), jpvt(steps, s);
-    DeviceBuffer<char> selected(n, s);
-    DeviceBuffer<double> v(m, s), tau(steps, s), diag(steps, s), energy(steps, s);
-    DeviceBuffer<ArgKey> partial(nblocks, s);
-    selected.zero(s);
-    energy.zero(s);
-    iota_i64(pos.get(), n, s);
-    iota_i64(col_at.get(), n, s);
-    QrState st{Yt, ldy, m, n, pos.get(), col_at.get(), selected.get(), v.get(), tau.get(),
-               diag.get(), energy.get(), jpvt.get(), partial.get()};
-    for (int64_t j = 0; j <= steps; ++j) {
-        {
-            ISDF_PROFILE("qrcp_sketch_update", s);
-            qr_update_kernel<<<nblocks, kQrThreads, 0, s>>>(st, j);
-            ISDF_LAUNCH_CHECK();
+MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& kp, const double* w,
+                         const AxisSpec& ax, const double* axis_weights, int64_t ell,
+                         const std::vector<double>& u, const std::vector<double>& v, double* Yt,
+                         int64_t ldy, cudaStream_t s) {
+    MixedSketch ms;
+    const int nao = c.nao;
+    const int naxes = ax.naxes;
+    const int64_t d = static_cast<int64_t>(naxes) * nao;
+    const int64_t n = kp.n;
+    const int nout = static_cast<int>(2 * ell);
+    std::vector<double> hw(static_cast<size_t>(d * nout)), hwt(static_cast<size_t>(d * nout));
+    for (int64_t j = 0; j < d; ++j)
+        for (int64_t t = 0; t < ell; ++t) {
+            hw[j * nout + t] = u[j * ell + t];
+            hw[j * nout + ell + t] = v[j * ell + t];
+            hwt[t * d + j] = u[j * ell + t];
+            hwt[(ell + t) * d + j] = v[j * ell + t];
         }
-        if (j < steps) {
-            ISDF_PROFILE("qrcp_sketch_pivot", s);
-            qr_pivot_kernel<<<1, 1024, 0, s>>>(st, j, nblocks);
-            ISDF_LAUNCH_CHECK();
-        }
-    }
-    out.jpvt.resize(steps);
-    out.diag.resize(steps);
-    out.energy.resize(steps);
-    ISDF_CUDA(cudaMemcpyAsync(out.jpvt.data(), jpvt.get(), steps * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    ISDF_CUDA(cudaMemcpyAsync(out.diag.data(), diag.get(), steps * sizeof(double), cudaMemcpyDeviceToHost, s));
-    ISDF_CUDA(cudaMemcpyAsync(out.energy.data(), energy.get(), steps * sizeof(double), cudaMemcpyDeviceToHost, s));
+    std::vector<int> comps(ax.comp, ax.comp + naxes);
+    ProjectPlan plan = make_project_plan(c, comps, hw, nout, s);
+    DeviceBuffer<float> P(static_cast<size_t>(n * naxes * nout), s), psq(static_cast<size_t>(n * 4), s);
+    DeviceBuffer<double> sumsq(4, s);
+    DeviceBuffer<int> err(1, s), dcomp(naxes, s);
+    psq.zero(s);
+    sumsq.zero(s);
+    err.zero(s);
+    project_tc(c, plan, pts, kp.index.get(), n, w, P.get(), naxes * nout, sumsq.get(), psq.get(),
+               err.get(), s);
+    double h[4] = {0, 0, 0, 0};
+    int herr = 0;
+    ISDF_CUDA(cudaMemcpyAsync(h, sumsq.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaStreamSynchronize(s));
-    return out;
+    if (herr) fail(kRuntime, "tensor-core sketch pipeline timed out (error flags " + std::to_string(herr) + ")");
+    std::vector<double> sc(naxes, 1.0);
+    if (naxes > 1) sc = axis_scales_from_sumsq(ax, h, axis_weights, n > 0);
+    ms.scales.reset(naxes, s);
+    ms.WT.reset(hwt.size(), s);
+    ms.delta.reset(n, s);
+    ISDF_CUDA(cudaMemcpyAsync(ms.scales.get(), sc.data(), naxes * sizeof(double), cudaMemcpyHostToDevice, s));
+    ISDF_CUDA(cudaMemcpyAsync(ms.WT.get(), hwt.data(), hwt.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    ISDF_CUDA(cudaMemcpyAsync(dcomp.get(), comps.data(), naxes * sizeof(int), cudaMemcpyHostToDevice, s));
+    DeviceBuffer<int> bad(1, s);
+    bad.zero(s);
+    {
+        ISDF_PROFILE("sketch_combine", s);
+        combine_mixed_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(
+            P.get(), psq.get(), naxes, dcomp.get(), ell, naxes > 1 ? ms.scales.get() : nullptr, w,
+            kp.index.get(), n, Yt, ldy, ms.delta.get(), bad.get());
+        ISDF_LAUNCH_CHECK();
+    }
+    int hbad = 0;
+    ISDF_CUDA(cudaMemcpyAsync(&hbad, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));   // host staging vectors go out of scope
+    if (hbad) fail(kOverflow, "non-finite randomized ID sketch");
+    ms.source.ctx = &c;
+    ms.source.naxes = naxes;
+    for (int a = 0; a < naxes; ++a) ms.source.comp[a] = comps[a];
+    ms.source.scales = ms.scales.get();
+    ms.source.WT = ms.WT.get();
+    ms.source.pts = pts;
+    ms.source.index = kp.index.get();
+    ms.source.w = w;
+    ms.source.ell = ell;
+    ms.source.delta = ms.delta.get();
+    return ms;
 }
 
 // ------------------------------------------------------------------------------
@@ -401,10 +368,16 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
     sketch_factors(d, ell, o.seed, u, v);
     const int64_t ldy = n;
     DeviceBuffer<double> Yt(static_cast<size_t>(ell * n), s);
-    const int64_t chunk = std::max<int64_t>(1024, std::min<int64_t>(n, (int64_t(1) << 28) / d));
-    sketch_fp64(c, pts, kp, w, ax, o.axis_weights.empty() ? nullptr : o.axis_weights.data(), ell,
-                u, v, Yt.get(), ldy, chunk, s);
-    SketchQR qr = qrcp_sketch(Yt.get(), ldy, ell, n, s);
+    const double* aw = o.axis_weights.empty() ? nullptr : o.axis_weights.data();
+    SketchQR qr;
+    if (o.precision == 1 && project_tc_supported(ax.naxes, static_cast<int>(2 * ell)) && ell <= 64) {
+        MixedSketch ms = sketch_mixed(c, pts, kp, w, ax, aw, ell, u, v, Yt.get(), ldy, s);
+        qr = qrcp_sketch(Yt.get(), ldy, ell, n, s, &ms.source);
+    } else {
+        const int64_t chunk = std::max<int64_t>(1024, std::min<int64_t>(n, (int64_t(1) << 28) / d));
+        sketch_fp64(c, pts, kp, w, ax, aw, ell, u, v, Yt.get(), ldy, chunk, s);
+        qr = qrcp_sketch(Yt.get(), ldy, ell, n, s);
+    }
     const int64_t steps = std::min(ell, n);
     std::vector<double> tails(steps + 1, 0.0);
     double diag_max = 0;
@@ -445,6 +418,7 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
         diag_out->rank = rank;
         diag_out->relative_tail = norm ? tails[rank] / norm : 0.0;
         diag_out->diag = qr.diag;
+        diag_out->reverified = qr.reverified;
         diag_out->tails = tails;
     }
     return selected;

@@ -1,0 +1,348 @@
+#!/usr/bin/env python3
+"""ISDF hot-path driver on the B200: grid -> anchor selection -> Theta fit.
+
+Mirrors the selection-to-fit slice of mikovtun/mp_isdf ``python/isdf.py``
+(``build_isdf`` :287-672 and the CLI :825-1004) over the drop-in ``mp_isdf``
+module of this repository.  PySCF is not required: molecules are either
+synthetic water clusters (``--molecule water:4x4x4[:seed]``, the seeded
+cc-pVDZ-shaped basis of ``mp_isdf_b200.inputs``) or libcint tables loaded from
+an ``.npz`` file with arrays atm, bas, env (and optionally coords, weights).
+The Coulomb metric, J/K and derivative targets are outside this path
+(``--no-metric`` is implied).
+
+Example:
+  python python/isdf.py --molecule water:2x2x1 --level 2 --axes ao \
+      --anchor-algorithm qrcp_dense --anchor-rank 8 --pair-space-error
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, os.environ.get("ISDF_BUILD_DIR", str(ROOT / "mp_isdf_b200")))
+import mp_isdf  # noqa: E402
+
+from mp_isdf_b200 import inputs  # noqa: E402
+
+KHATRIRAO_SKETCH_TECHNIQUES = ("quadrature", "density", "density_col_norm")
+DENSITY_SKETCHES = ("density", "density_col_norm")
+SKETCH_ALGORITHMS = ("rand_sketch",)
+AXES = {
+    "ao": mp_isdf.AxisType.AtomicOrbital,
+    "dx": mp_isdf.AxisType.AtomicOrbitalGradX,
+    "dy": mp_isdf.AxisType.AtomicOrbitalGradY,
+    "dz": mp_isdf.AxisType.AtomicOrbitalGradZ,
+    "occ": mp_isdf.AxisType.OccupiedOrbital,
+}
+
+
+def pair_space_error_norms(pair_grid, pair_anchor, anchor_weights, theta, grid_weights,
+                           block_size=256):
+    """Absolute and relative |w|-weighted L2 error of explicit pair columns
+    (``python/isdf.py:154-173``); for small grids."""
+    weighted_anchor = pair_anchor * anchor_weights[:, None]
+    residual_sq = exact_sq = 0.0
+    for first in range(0, len(grid_weights), block_size):
+        last = min(first + block_size, len(grid_weights))
+        exact = pair_grid[first:last]
+        rec = theta[:, first:last].T @ weighted_anchor
+        weight = np.abs(grid_weights[first:last])
+        residual_sq += np.einsum("g,gi,gi->", weight, exact - rec, exact - rec, optimize=True)
+        exact_sq += np.einsum("g,gi,gi->", weight, exact, exact, optimize=True)
+    absolute = np.sqrt(residual_sq)
+    relative = absolute / np.sqrt(exact_sq) if exact_sq else (0.0 if absolute == 0 else np.inf)
+    return {"l2": absolute, "relative": relative}
+
+
+class Molecule:
+    """Minimal stand-in for the PySCF molecule: libcint tables + helpers."""
+
+    def __init__(self, atm, bas, env, coords=None, symbols=None):
+        self._atm, self._bas, self._env = atm, bas, env
+        self.coords = coords
+        self.symbols = symbols
+
+    @classmethod
+    def from_spec(cls, spec: str):
+        if spec.startswith("water:"):
+            parts = spec.split(":")
+            lat = tuple(int(v) for v in parts[1].split("x"))
+            seed = int(parts[2]) if len(parts) > 2 else 0
+            sym, xyz = inputs.water_cluster(lat, seed=seed)
+            t = inputs.build_tables(sym, xyz)
+            return cls(t.atm, t.bas, t.env, t.coords, t.symbols)
+        d = np.load(spec)
+        return cls(d["atm"], d["bas"], d["env"])
+
+
+def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), axis_weights=None,
+               space="auto", anchor_algorithm="qrcp_dense", sketch="quadrature",
+               anchor_batch_size=128, fit_batch_size=2048, anchor_sketch_size=128,
+               anchor_oversampling=16, anchor_seed=7, selection_only=False, debug=False,
+               pair_space_error=False, report_timings=False, report_dimensions=False, grid=None,
+               precision="fp64"):
+    """Selection-to-fit slice of ``build_isdf`` (``python/isdf.py:287-672``).
+
+    `grid` is an optional (coords, weights) pair; otherwise a Becke-partitioned
+    atom-centred grid of the requested level is generated for the synthetic
+    waters.  `precision` selects the FP64 or mixed (FP32 AO / split-BF16
+    tensor-core / FP64 QR and solve) form on the B200.
+    """
+    started = time.perf_counter()
+    last = started
+    timings = {}
+
+    def record(stage):
+        nonlocal last
+        now = time.perf_counter()
+        timings[stage] = now - last
+        last = now
+        if report_timings and not debug:
+            print(f"  {stage:18s} {timings[stage]:10.6f} s  (elapsed {last - started:.6f} s)", flush=True)
+
+    if isinstance(axes, str):
+        axes = (axes,)
+    try:
+        axis_types = [AXES[a] if isinstance(a, str) else a for a in axes]
+    except KeyError as exc:
+        raise ValueError(f"unknown axis: {exc.args[0]!r}; choose from {list(AXES)}") from exc
+    if axis_weights is not None:
+        axis_weights = tuple(float(w) for w in axis_weights)
+        if len(axis_weights) != len(axis_types) or not all(np.isfinite(w) and w > 0 for w in axis_weights):
+            raise ValueError("axis_weights must contain one finite positive factor per axis")
+    sketch_algorithm = anchor_algorithm == "rand_sketch"
+    if sketch_algorithm:
+        if sketch not in KHATRIRAO_SKETCH_TECHNIQUES:
+            raise ValueError(f"sketch must be one of {KHATRIRAO_SKETCH_TECHNIQUES} for rand_sketch")
+        if sketch in DENSITY_SKETCHES:
+            raise NotImplementedError("density Khatri--Rao sketches are outside the B200 hot path (NYI)")
+    elif sketch != "quadrature":
+        raise ValueError("non-default sketch requires anchor_algorithm='rand_sketch'")
+    if anchor_algorithm not in ("qrcp_dense", "qrcp_online", *SKETCH_ALGORITHMS):
+        if anchor_algorithm in ("cvt", "rbrp", "rbrp_id"):
+            raise NotImplementedError(f"{anchor_algorithm} is outside the B200 hot path (NYI)")
+        raise ValueError(f"unknown anchor algorithm: {anchor_algorithm!r}")
+    if not isinstance(anchor_batch_size, (int, np.integer)) or anchor_batch_size <= 0:
+        raise ValueError("anchor_batch_size must be a positive integer")
+    if not isinstance(fit_batch_size, (int, np.integer)) or fit_batch_size <= 0:
+        raise ValueError("fit_batch_size must be a positive integer")
+    if anchor_rank != 0 and anchor_tol is not None:
+        raise ValueError("anchor_rank and anchor_tol are mutually exclusive")
+    if anchor_tol is None:
+        anchor_tol = 1e-10
+    if not np.isfinite(anchor_tol) or anchor_tol < 0:
+        raise ValueError("anchor_tol must be finite and nonnegative")
+    if (not isinstance(anchor_sketch_size, (int, np.integer)) or
+            not isinstance(anchor_oversampling, (int, np.integer)) or
+            anchor_oversampling < 1 or anchor_sketch_size < 1 or
+            (sketch_algorithm and anchor_rank == 0 and anchor_sketch_size <= anchor_oversampling)):
+        raise ValueError("randomized anchor sketch_size must exceed oversampling when anchor_rank=0")
+    if not isinstance(anchor_seed, (int, np.integer)) or not 0 <= anchor_seed < 2 ** 64:
+        raise ValueError("anchor_seed must be an unsigned 64-bit integer")
+    if selection_only and pair_space_error:
+        raise ValueError("pair_space_error requires fitting; disable selection_only")
+    if mp_isdf.AxisType.OccupiedOrbital in axis_types:
+        raise NotImplementedError("the occupied-orbital axis needs an RHF and is outside this path")
+
+    if grid is None:
+        if mol.symbols is None:
+            raise ValueError("a grid is required for molecules loaded from tables")
+        all_coords, all_weights = inputs.becke_grid(mol.symbols, mol.coords, level=level)
+    else:
+        all_coords, all_weights = grid
+    all_coords = np.ascontiguousarray(all_coords, dtype=np.float64)
+    all_weights = np.ascontiguousarray(all_weights, dtype=np.float64)
+    keep = all_weights != 0
+    if not np.any(keep):
+        raise ValueError("grid has no nonzero weights")
+    record("grid")
+
+    context = mp_isdf.LibcintContext(mol._atm, mol._bas, mol._env)
+    selector = mp_isdf.AnchorSelection(context)
+    record("context")
+    nao = context.nao
+    axis_width = nao * len(axis_types)
+    pair_rank_ceiling = axis_width * (axis_width + 1) // 2
+    if report_dimensions:
+        dims = (f"[ISDF dimensions] AOs={nao} axis_features={axis_width} "
+                f"symmetric_pair_rank_ceiling={pair_rank_ceiling} "
+                f"grid_points={len(all_coords)} nonzero_weight_points={int(np.count_nonzero(keep))}")
+        if sketch_algorithm:
+            ell = anchor_rank + anchor_oversampling if anchor_rank > 0 else anchor_sketch_size
+            cap = min(ell - anchor_oversampling, pair_rank_ceiling, int(np.count_nonzero(keep)))
+            dims += (f" sketch_rows={ell} oversampling={anchor_oversampling}"
+                     f" sketch_rank_cap={cap} sketch_matrix={ell}x{int(np.count_nonzero(keep))}"
+                     f" sketch_storage={ell * int(np.count_nonzero(keep)) * 8 / 2**20:.1f}MiB")
+            if anchor_rank > 0:
+                dims += f" requested_rank={anchor_rank} (anchor_sketch_size ignored)"
+        print(dims, flush=True)
+    algo = {"qrcp_dense": mp_isdf.LocalAnchorSelectionAlgorithm.QRColumnPivoting,
+            "qrcp_online": mp_isdf.LocalAnchorSelectionAlgorithm.OnlineQRColumnPivoting,
+            "rand_sketch": mp_isdf.LocalAnchorSelectionAlgorithm.RandomizedQuadratureKhatriRao}[anchor_algorithm]
+    anchor_indices = np.asarray(selector.select(
+        all_coords, all_weights, axis_types, tolerance=anchor_tol, max_rank=anchor_rank,
+        algorithm=algo, space=space, batch_size=anchor_batch_size, debug=debug,
+        sketch_size=anchor_sketch_size, oversampling=anchor_oversampling, seed=anchor_seed,
+        axis_weights=list(axis_weights) if axis_weights is not None else [],
+        precision=precision), dtype=np.intp)
+    if len(anchor_indices) == 0:
+        raise ValueError("anchor selection found no anchors; adjust settings or grid")
+    record("anchor_selection")
+    if selection_only:
+        return {"anchor_indices": anchor_indices, "anchor_coords": all_coords[anchor_indices],
+                "anchor_weights": all_weights[anchor_indices], "coordinates": all_coords[keep],
+                "weights": all_weights[keep], "interp_vecs": None, "pair_space_errors": None,
+                "fit_diagnostics": None, "elapsed": last - started, "timings": timings}
+
+    coords = all_coords[keep]
+    weights = all_weights[keep]
+    anchor_coords = all_coords[anchor_indices]
+    anchor_weights = all_weights[anchor_indices]
+    anchor_ao = context.eval_ao(anchor_coords, space=space)
+    record("ao_evaluation")
+    fit = mp_isdf.fit(context, all_coords, all_weights, anchor_indices, precision=precision,
+                      pair_space_error=pair_space_error)
+    interp_vecs = fit["interp_vecs"]
+    fit_diagnostics = {key: fit[key] for key in ("retained_rank", "condition",
+                                                 "max_abs_physical_coefficient")}
+    record("isdf_fit")
+    pair_space_errors = None
+    if pair_space_error:
+        pair_space_errors = {"scalar": {"l2": fit["pair_l2"], "relative": fit["pair_relative"]}}
+        record("pair_space_check")
+    # Overlap reconstruction (python/isdf.py:665-671); without int1e_ovlp the
+    # reference overlap is the grid quadrature Phi^T diag(w) Phi (small systems).
+    overlap_approx = np.einsum("ku,kv,k->uv", anchor_ao, anchor_ao,
+                               anchor_weights * np.asarray(fit["theta_w"][:len(anchor_weights)]),
+                               optimize=True) if len(anchor_weights) <= 64 else None
+    overlap_relative_error = None
+    if overlap_approx is not None and nao <= 400 and len(coords) <= 400000:
+        ao = context.eval_ao(coords, space=space)
+        overlap = ao.T @ (weights[:, None] * ao)
+        overlap_relative_error = (np.linalg.norm(overlap_approx - overlap) /
+                                  max(np.linalg.norm(overlap), 1e-30))
+    record("overlap_check")
+    return {"anchor_indices": anchor_indices, "fit_diagnostics": fit_diagnostics,
+            "anchor_coords": anchor_coords, "anchor_weights": anchor_weights,
+            "coordinates": coords, "weights": weights, "interp_vecs": interp_vecs,
+            "overlap_reconstruction": overlap_approx,
+            "overlap_relative_error": overlap_relative_error,
+            "pair_space_errors": pair_space_errors, "X1": anchor_ao,
+            "elapsed": last - started, "timings": timings}
+
+
+def main(argv=None):
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    parser.add_argument("--molecule", default="water:1x1x1",
+                        help="water:AxBxC[:seed] synthetic cluster, or an .npz with atm/bas/env")
+    parser.add_argument("--basis", default="synthetic-cc-pvdz",
+                        help="basis label (only the synthetic cc-pVDZ-shaped basis is available)")
+    parser.add_argument("--level", type=int, default=0)
+    parser.add_argument("--anchor-rank", type=int, default=0)
+    parser.add_argument("--anchor-tol", type=float, default=None)
+    parser.add_argument("--anchor-algorithm", choices=("qrcp_dense", "qrcp_online", *SKETCH_ALGORITHMS,
+                                                       "cvt", "rbrp", "rbrp_id"), default="qrcp_dense")
+    parser.add_argument("--sketch", choices=KHATRIRAO_SKETCH_TECHNIQUES, default=None)
+    parser.add_argument("--anchor-batch-size", type=int, default=128)
+    parser.add_argument("--fit-batch-size", type=int, default=2048)
+    parser.add_argument("--anchor-sketch-size", type=int, default=128)
+    parser.add_argument("--anchor-oversampling", type=int, default=16)
+    parser.add_argument("--anchor-seed", type=int, default=7)
+    parser.add_argument("--axes", default="ao")
+    parser.add_argument("--space", choices=("auto", "host", "device"), default="auto")
+    parser.add_argument("--pair-space-error", action="store_true")
+    parser.add_argument("--no-metric", action="store_true",
+                        help="accepted for compatibility; the metric is outside this path")
+    parser.add_argument("--debug", action="store_true")
+    parser.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
+    parser.add_argument("--grid-file", default=None, help=".npz with coords and weights")
+    parser.add_argument("--json", default=None, help="write a JSON record of the run")
+    args = parser.parse_args(argv)
+    if args.anchor_rank < 0:
+        parser.error("--anchor-rank must be nonnegative")
+    if args.anchor_algorithm not in SKETCH_ALGORITHMS and args.sketch is not None:
+        parser.error("--sketch requires --anchor-algorithm rand_sketch")
+    if args.anchor_batch_size <= 0:
+        parser.error("--anchor-batch-size must be positive")
+    if args.fit_batch_size <= 0:
+        parser.error("--fit-batch-size must be positive")
+    if args.anchor_sketch_size < 1 or args.anchor_oversampling < 1 or (
+            args.anchor_algorithm in SKETCH_ALGORITHMS and args.anchor_rank == 0 and
+            args.anchor_sketch_size <= args.anchor_oversampling):
+        parser.error("randomized sketch size must exceed oversampling when --anchor-rank=0")
+    if not 0 <= args.anchor_seed < 2 ** 64:
+        parser.error("--anchor-seed must be an unsigned 64-bit integer")
+    if args.anchor_rank != 0 and args.anchor_tol is not None:
+        parser.error("--anchor-rank and --anchor-tol are mutually exclusive")
+    if args.anchor_tol is not None and (not np.isfinite(args.anchor_tol) or args.anchor_tol < 0):
+        parser.error("--anchor-tol must be finite and nonnegative")
+    if args.level < 0:
+        parser.error("--level must be nonnegative")
+    axes, axis_weights = [], []
+    for entry in args.axes.split(","):
+        fields = entry.strip().lower().split(":")
+        if len(fields) > 2 or fields[0] not in AXES:
+            parser.error(f"invalid --axes entry: {entry!r}")
+        try:
+            factor = float(fields[1]) if len(fields) == 2 else 1.0
+        except ValueError:
+            parser.error(f"invalid --axes factor: {entry!r}")
+        if not np.isfinite(factor) or factor <= 0:
+            parser.error(f"--axes factor must be finite and positive: {entry!r}")
+        axes.append(fields[0])
+        axis_weights.append(factor)
+    mol = Molecule.from_spec(args.molecule)
+    grid = None
+    if args.grid_file:
+        g = np.load(args.grid_file)
+        grid = (g["coords"], g["weights"])
+    result = build_isdf(mol, level=args.level, anchor_rank=args.anchor_rank,
+                        anchor_tol=args.anchor_tol, axes=axes, axis_weights=axis_weights,
+                        space=args.space, anchor_algorithm=args.anchor_algorithm,
+                        sketch=args.sketch or "quadrature",
+                        anchor_batch_size=args.anchor_batch_size,
+                        fit_batch_size=args.fit_batch_size,
+                        anchor_sketch_size=args.anchor_sketch_size,
+                        anchor_oversampling=args.anchor_oversampling, anchor_seed=args.anchor_seed,
+                        pair_space_error=args.pair_space_error, report_timings=not args.debug,
+                        debug=args.debug, report_dimensions=True, grid=grid,
+                        precision=args.precision)
+    print(f"Grid points: {len(result['coordinates'])}; AOs: {result['X1'].shape[1]}; "
+          f"anchors: {len(result['anchor_indices'])}")
+    if args.anchor_rank and len(result["anchor_indices"]) == args.anchor_rank:
+        print(f"Anchor count equals --anchor-rank {args.anchor_rank}; use --anchor-rank 0 "
+              "for tolerance-only selection or a larger value for a higher cap.")
+    if result["overlap_relative_error"] is not None:
+        print(f"Overlap reconstruction relative error: {result['overlap_relative_error']:.3e}")
+    if result["pair_space_errors"] is not None:
+        for label, error in result["pair_space_errors"].items():
+            print(f"Pair-space {label} grid L2 error: {error['l2']:.3e}; "
+                  f"relative error: {error['relative']:.3e}")
+    if not args.debug:
+        print(f"ISDF build time: {result['elapsed']:.6f} s")
+    else:
+        print("Timing report:")
+        for stage, seconds in result["timings"].items():
+            frac = 100 * seconds / result["elapsed"] if result["elapsed"] else 0.0
+            print(f"  {stage:22s} {seconds:10.6f} s  ({frac:5.1f}% of build)")
+        print(f"  ISDF build total       {result['elapsed']:10.6f} s")
+    if args.json:
+        rec = {"anchor_indices": [int(i) for i in result["anchor_indices"]],
+               "timings": result["timings"], "elapsed": result["elapsed"],
+               "pair_space_errors": result["pair_space_errors"],
+               "fit_diagnostics": {k: float(v) for k, v in result["fit_diagnostics"].items()},
+               "precision": args.precision, "axes": args.axes}
+        Path(args.json).write_text(json.dumps(rec, indent=1))
+    return result
+
+
+if __name__ == "__main__":
+    main()

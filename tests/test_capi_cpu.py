@@ -68,7 +68,7 @@ def test_c2s_closed_form_matches_oracle_least_squares():
     src = ROOT / "mp_isdf_b200" / "csrc" / "context.cu"
     text = src.read_text()
     start = text.index("namespace {\n\ndouble fact")
-    end = text.index("// ------------------------------------------------------------------------------\n// constant tables")
+    end = text.index("Context::~Context()")
     snippet = "#include <cmath>\n#include <cstdio>\n#include <vector>\n#include <cstdlib>\n" \
               "namespace isdf {\n" + text[start:end] + "}\nint main(){for(int l=0;l<=6;++l){auto t=isdf::c2s_matrix(l);" \
               "for(double x: t) std::printf(\"%.17g\\n\", x);} }\n"

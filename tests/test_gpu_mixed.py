@@ -1,0 +1,130 @@
+"""Mixed-precision form (FP32 AO values, split-BF16 tcgen05 projections, FP64
+QRCP with exact re-verification of near-tie columns, FP64 solve) against the
+FP64 form and the oracle.  Criteria: anchors identical to the FP64 path's;
+pair-space error of the mixed Theta (evaluated with FP64 AO values) within
+1e-8 relative of the FP64 fit's; Theta within 1e-4 relative."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mpi():
+    import mp_isdf
+    return mp_isdf
+
+
+@pytest.fixture(scope="module")
+def c1(mpi):
+    from mp_isdf_b200 import inputs
+    mol, pts, w, cfg = inputs.make_config("c1")
+    c = mpi.LibcintContext(mol.atm, mol.bas, mol.env)
+    return mol, pts, w, c, mpi.AnchorSelection(c)
+
+
+@pytest.mark.parametrize("axes,aw,rank,ovs", [
+    ([0], None, 8, 4),
+    ([0, 1, 2, 3], [1.0, 0.5, 0.5, 0.5], 8, 4),
+    ([0, 1, 2, 3], None, 10, 16),
+    ([0, 3], [1.0, 2.0], 6, 10),
+])
+def test_mixed_sketch_pivots_equal_fp64_small(mpi, small_water, axes, aw, rank, ovs):
+    mol, pts, w = small_water
+    c = mpi.LibcintContext(mol.atm, mol.bas, mol.env)
+    sel = mpi.AnchorSelection(c)
+    algo = mpi.LocalAnchorSelectionAlgorithm.RandomizedQuadratureKhatriRao
+    axt = [mpi.AxisType(a) for a in axes]
+    kw = dict(algorithm=algo, max_rank=rank, oversampling=ovs, seed=2, axis_weights=aw or [])
+    fp64 = sel.select(pts, w, axt, precision="fp64", **kw)
+    mixed = sel.select(pts, w, axt, precision="mixed", **kw)
+    assert mixed == fp64
+    oc = O.OracleContext(mol.atm, mol.bas, mol.env)
+    scales = O.axis_scales(oc, pts, w, axes, aw)
+    ref = O.select_rand_sketch(oc, pts, w, axes, max_rank=rank, oversampling=ovs, seed=2,
+                               scales=scales)
+    assert mixed == ref
+
+
+def test_mixed_sketch_and_fit_c1(mpi, c1):
+    mol, pts, w, c, sel = c1
+    algo = mpi.LocalAnchorSelectionAlgorithm.RandomizedQuadratureKhatriRao
+    for axes in ([mpi.AxisType.AtomicOrbital],
+                 [mpi.AxisType.AtomicOrbital, mpi.AxisType.AtomicOrbitalGradX,
+                  mpi.AxisType.AtomicOrbitalGradY, mpi.AxisType.AtomicOrbitalGradZ]):
+        kw = dict(algorithm=algo, max_rank=8, oversampling=16, seed=7)
+        fp64 = sel.select(pts, w, axes, precision="fp64", **kw)
+        mixed = sel.select(pts, w, axes, precision="mixed", **kw)
+        assert mixed == fp64
+    piv = np.array(fp64)
+    f64 = mpi.fit(c, pts, w, piv, precision="fp64")
+    mx = mpi.fit(c, pts, w, piv, precision="mixed")
+    th64, thm = f64["interp_vecs"], mx["interp_vecs"]
+    assert thm.shape == th64.shape
+    rel = np.abs(thm - th64).max() / np.abs(th64).max()
+    cond = f64["condition"]
+    info = (f"theta rel {rel:.3e} cond(C) {cond:.3e} pair {f64['pair_relative']:.12e} "
+            f"{mx['pair_relative']:.12e} path {mx['fit_path']} bound {mx['mixed_bound']:.3e}")
+    print(info)
+    # Theta errors are amplified by cond(C)^2 (the solve with (Phi_a Phi_a^T)^2);
+    # the pair error is stationary in Theta and is the acceptance criterion.
+    assert rel < 1e-5 * max(1.0, cond) ** 2, info
+    assert abs(mx["pair_relative"] - f64["pair_relative"]) <= 1e-8 * f64["pair_relative"], info
+    assert abs(mx["pair_l2"] - f64["pair_l2"]) <= 1e-8 * f64["pair_l2"], info
+
+
+def test_tensor_core_projection_accuracy(small_water):
+    """Split-BF16 tcgen05 projection of FP32 AO features vs the FP64 path and
+    the oracle: error bounded by 1.5e-4 * |f_g| * |w_j| per entry (the bound
+    the verified QR relies on), typically ~1e-5 of it."""
+    import torch
+    from mp_isdf_b200 import capi
+    mol, pts, w = small_water
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    oc = O.OracleContext(mol.atm, mol.bas, mol.env)
+    p = pts[::3]
+    x = torch.tensor(p, device="cuda")
+    rng = np.random.default_rng(0)
+    for axes, nout in ((("ao",), 10), (("ao", "dx", "dy", "dz"), 52), (("dz", "ao"), 24)):
+        d = len(axes) * mol.nao
+        W = rng.normal(size=(d, nout))
+        p64 = ctx.project_axes(x, axes, W, "fp64").cpu().numpy()
+        pm = ctx.project_axes(x, axes, W, "mixed").cpu().numpy()
+        codes = [O.AXIS_CODES[a] for a in axes]
+        f = oc.axis_features(p, codes)
+        nao = mol.nao
+        ref = np.stack([f[:, a * nao:(a + 1) * nao] @ W[a * nao:(a + 1) * nao] for a in range(len(axes))],
+                       axis=1)
+        np.testing.assert_allclose(p64, ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max())
+        fn = np.stack([np.linalg.norm(f[:, a * nao:(a + 1) * nao], axis=1) for a in range(len(axes))], axis=1)
+        wn = np.stack([np.linalg.norm(W[a * nao:(a + 1) * nao], axis=0) for a in range(len(axes))])
+        bound = fn[:, :, None] * wn[None, :, :] + 1e-300
+        ratio = np.abs(pm - ref) / bound
+        print(axes, "max err/(|f||w|) =", ratio.max(), "median", np.median(ratio))
+        assert ratio.max() < 1.5e-4, ratio.max()
+
+
+def test_mixed_dense_device_api(small_water):
+    """C-ABI device path with torch tensors, mixed precision."""
+    import torch
+    from mp_isdf_b200 import capi
+    mol, pts, w = small_water
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    x = torch.tensor(pts, device="cuda")
+    wt = torch.tensor(w, device="cuda")
+    p64, i64 = ctx.select(x, wt, axes=("ao", "dx", "dy", "dz"), max_rank=8, oversampling=16,
+                          precision="fp64")
+    pm, im = ctx.select(x, wt, axes=("ao", "dx", "dy", "dz"), max_rank=8, oversampling=16,
+                        precision="mixed")
+    np.testing.assert_array_equal(pm, p64)
+    assert im.verifications >= 1          # the winner of every step is recomputed exactly
+    theta = torch.empty(len(pm) * len(pts), dtype=torch.float64, device="cuda")
+    info = ctx.fit(x, wt, pm, theta, precision="mixed", want_error=True)
+    theta64 = torch.empty_like(theta)
+    info64 = ctx.fit(x, wt, pm, theta64, precision="fp64")
+    torch.cuda.synchronize()
+    print("small water mixed fit path", info.fit_path, "bound", info.mixed_bound)
+    assert info.fit_path in (1, 2)
+    assert abs(info.pair_relative - info64.pair_relative) <= 1e-8 * info64.pair_relative
