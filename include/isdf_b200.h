@@ -164,6 +164,19 @@ int isdf_pair_error_terms(int64_t n, int64_t k, const double* q_dev, const doubl
                           const double* X_dev, const double* M_dev, const double* w_dev,
                           double* out_host, void* stream);
 
+/* Same reduction as isdf_pair_error_terms, for callers that cannot allocate
+ * device memory on the call path (a fixed device-memory budget, their own
+ * pool or arena, no cudaFree synchronisation allowed).  No counterpart in the
+ * reference.  It allocates nothing: its scratch is a fixed 16 KB device array
+ * inside the library that every GPU loading the library keeps until exit.
+ * Limits: k <= 64 anchors (larger k returns ISDF_ERR_INVALID); any n.  All
+ * calls share that array, so calls whose GPU work overlaps race; serialise
+ * them.  The first call on a device looks up the array's address once for
+ * that device; make it before any stream capture. */
+int isdf_pair_error_terms_noalloc(int64_t n, int64_t k, const double* q_dev, const double* H_dev,
+                                  const double* X_dev, const double* M_dev, const double* w_dev,
+                                  double* out_host, void* stream);
+
 /* ---- nuclear-gradient adjoint (no counterpart in the reference, which has no
  * nuclear derivatives: python/isdf.py:7-8) ------------------------------------
  * E = sum_g w_g rho_ISDF(g)^2, rho_ISDF(g) = sum_k Theta_kg w_k rho_a(k),

@@ -26,7 +26,7 @@ SYMBOLS = [
     "isdf_select_args_default", "isdf_select", "isdf_select_host",
     "isdf_fit", "isdf_fit_host", "isdf_pair_error", "isdf_pair_error_terms",
     "isdf_profile_enable", "isdf_profile_read", "isdf_project_axes",
-    "isdf_energy_gradient", "isdf_ctx_set_coords",
+    "isdf_energy_gradient", "isdf_ctx_set_coords", "isdf_pair_error_terms_noalloc",
 ]
 
 ALGORITHMS = {"qrcp_dense": 0, "qrcp_online": 1, "rand_sketch": 2}
@@ -87,6 +87,7 @@ def lib():
         L.isdf_pair_error.argtypes = [P, P, P, I64, P, I64, P, ctypes.POINTER(F64),
                                       ctypes.POINTER(F64), P]
         L.isdf_pair_error_terms.argtypes = [I64, I64, P, P, P, P, P, P, P]
+        L.isdf_pair_error_terms_noalloc.argtypes = [I64, I64, P, P, P, P, P, P, P]
         L.isdf_project_axes.argtypes = [P, P, I64, P, I32, P, I32, I32, P, P]
         L.isdf_energy_gradient.argtypes = [P, P, P, I64, P, I64, P, ctypes.POINTER(F64), P, P]
         L.isdf_ctx_set_coords.argtypes = [P, P]

@@ -82,6 +82,10 @@ isdf::SelectOptions options_of(const isdf_select_args* a) {
 
 }  // namespace
 
+namespace isdf {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace isdf
+
 extern "C" {
 
 const char* isdf_status_string(int status) {

@@ -29,6 +29,8 @@ enum : int {
     kLogic = 6,          // -> RuntimeError (std::logic_error)
 };
 [[noreturn]] inline void fail(int code, const std::string& msg) { throw Error(code, msg); }
+// Message returned by isdf_last_error() on the calling thread.
+void set_last_error(const std::string& msg);
 inline void require(bool ok, const std::string& msg) { if (!ok) fail(kInvalid, msg); }
 
 #define ISDF_CUDA(expr)                                                                  \
