@@ -3,77 +3,86 @@
 // Restates cpp/src/ao_eval.cpp:207-249 (mikovtun/mp_isdf): radial sum over
 // primitives, its derivative with respect to r^2, cartesian monomials in
 // libcint order (cpp/src/ao_eval.cpp:30-44) contracted with the cartesian ->
-// spherical table, gradient = R * d(poly) + 2 x R' * poly.
+// spherical coefficients, gradient = R * d(poly) + 2 x R' * poly.  The
+// coefficients are compile-time constants (c2s_table.h): the unrolled code
+// multiplies only by the nonzero ones.
 #pragma once
 
+#include "c2s_table.h"
 #include "isdf_internal.h"
+
+#include <type_traits>
 
 namespace isdf {
 
-__host__ __device__ constexpr int c2s_table_offset(int l) {
-    int off = 0;
-    for (int i = 0; i < l; ++i) off += (2 * i + 1) * (i + 1) * (i + 2) / 2;
-    return off;
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+    if constexpr (B < E) {
+        f(std::integral_constant<int, B>{});
+        static_for<B + 1, E>(f);
+    }
 }
-constexpr int kC2sTableSize = c2s_table_offset(kMaxL + 1);
-
-template <int L>
-struct CartOrder {
-    static constexpr int nc = (L + 1) * (L + 2) / 2;
-    static __host__ __device__ constexpr int lx(int c) {
-        int x = L;
-        while (c >= L - x + 1) { c -= L - x + 1; --x; }
-        return x;
-    }
-    static __host__ __device__ constexpr int lz(int c) {
-        int x = L;
-        while (c >= L - x + 1) { c -= L - x + 1; --x; }
-        return c;
-    }
-};
 
 __device__ __forceinline__ double ao_exp(double x) { return exp(x); }
 __device__ __forceinline__ float ao_exp(float x) { return __expf(x); }
 
+// Spherical polynomial values (and cartesian derivatives) of angular
+// momentum L at the offset (x, y, z).
+template <class T, int L, bool GRAD>
+struct SphPoly {
+    static constexpr int NS = 2 * L + 1;
+    T v[NS], vx[GRAD ? NS : 1], vy[GRAD ? NS : 1], vz[GRAD ? NS : 1];
+    __device__ __forceinline__ SphPoly(T x, T y, T z) {
+        constexpr int NC = (L + 1) * (L + 2) / 2;
+        T px[L + 1], py[L + 1], pz[L + 1];
+        px[0] = py[0] = pz[0] = T(1);
+#pragma unroll
+        for (int i = 1; i <= L; ++i) { px[i] = px[i - 1] * x; py[i] = py[i - 1] * y; pz[i] = pz[i - 1] * z; }
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            v[s] = T(0);
+            if constexpr (GRAD) { vx[s] = T(0); vy[s] = T(0); vz[s] = T(0); }
+        }
+        static_for<0, NC>([&](auto ci) {
+            constexpr int c = decltype(ci)::value;
+            constexpr int ax = c2s_detail::cart_lx(L, c), az = c2s_detail::cart_lz(L, c);
+            constexpr int ay = L - ax - az;
+            const T m = px[ax] * py[ay] * pz[az];
+            [[maybe_unused]] T mx = T(0), my = T(0), mz = T(0);
+            if constexpr (GRAD) {
+                if constexpr (ax > 0) mx = T(ax) * px[ax > 0 ? ax - 1 : 0] * py[ay] * pz[az];
+                if constexpr (ay > 0) my = T(ay) * px[ax] * py[ay > 0 ? ay - 1 : 0] * pz[az];
+                if constexpr (az > 0) mz = T(az) * px[ax] * py[ay] * pz[az > 0 ? az - 1 : 0];
+            }
+            static_for<0, NS>([&](auto si) {
+                constexpr int s = decltype(si)::value;
+                constexpr double t = C2s<L, s, c>::value;
+                if constexpr (t != 0.0) {
+                    v[s] += T(t) * m;
+                    if constexpr (GRAD) {
+                        if constexpr (ax > 0) vx[s] += T(t) * mx;
+                        if constexpr (ay > 0) vy[s] += T(t) * my;
+                        if constexpr (az > 0) vz[s] += T(t) * mz;
+                    }
+                }
+            });
+        });
+    }
+};
+
 // `sink.put<C>(ao, v)` receives component C (0 value, 1..3 d/dx, d/dy, d/dz)
-// of AO index `ao`; `sink.wants(ao_first, ao_last)` may skip whole
-// contraction groups.
+// of AO index `ao` for the contractions [ctr0, ctr1) of shell b.
 template <class T, int L, bool GRAD, class Sink>
 __device__ __forceinline__ void eval_shell_t(const ShellDesc& b, double dxd, double dyd, double dzd,
                                              const T* __restrict__ exps, const T* __restrict__ coefs,
-                                             const T* __restrict__ c2s, Sink& sink) {
-    constexpr int NC = CartOrder<L>::nc;
+                                             Sink& sink, int ctr0 = 0, int ctr1 = 1 << 30) {
     constexpr int NS = 2 * L + 1;
-    constexpr int OFF = c2s_table_offset(L);
     const T x = static_cast<T>(dxd), y = static_cast<T>(dyd), z = static_cast<T>(dzd);
     const T r2 = static_cast<T>(dxd * dxd + dyd * dyd + dzd * dzd);
-    T px[L + 1], py[L + 1], pz[L + 1];
-    px[0] = py[0] = pz[0] = T(1);
-#pragma unroll
-    for (int i = 1; i <= L; ++i) { px[i] = px[i - 1] * x; py[i] = py[i - 1] * y; pz[i] = pz[i - 1] * z; }
-    T v[NS], vx[NS], vy[NS], vz[NS];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) { v[s] = vx[s] = vy[s] = vz[s] = T(0); }
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-        const int ax = CartOrder<L>::lx(c), az = CartOrder<L>::lz(c), ay = L - ax - az;
-        const T m = px[ax] * py[ay] * pz[az];
-        T mx = T(0), my = T(0), mz = T(0);
-        if (GRAD) {
-            if (ax) mx = T(ax) * px[ax - 1] * py[ay] * pz[az];
-            if (ay) my = T(ay) * px[ax] * py[ay - 1] * pz[az];
-            if (az) mz = T(az) * px[ax] * py[ay] * pz[az - 1];
-        }
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const T t = c2s[OFF + s * NC + c];
-            v[s] += t * m;
-            if (GRAD) { vx[s] += t * mx; vy[s] += t * my; vz[s] += t * mz; }
-        }
-    }
-    for (int g0 = 0; g0 < b.nctr; g0 += kMaxCtrGroup) {
-        const int ng = min(kMaxCtrGroup, b.nctr - g0);
-        if (!sink.wants(b.ao_off + g0 * NS, b.ao_off + (g0 + ng) * NS)) continue;
+    const SphPoly<T, L, GRAD> poly(x, y, z);
+    const int cend = min(b.nctr, ctr1);
+    for (int g0 = ctr0; g0 < cend; g0 += kMaxCtrGroup) {
+        const int ng = min(kMaxCtrGroup, cend - g0);
         T R[kMaxCtrGroup], Rp[kMaxCtrGroup];
 #pragma unroll
         for (int j = 0; j < kMaxCtrGroup; ++j) { R[j] = T(0); Rp[j] = T(0); }
@@ -87,7 +96,7 @@ __device__ __forceinline__ void eval_shell_t(const ShellDesc& b, double dxd, dou
                 if (j < ng) {
                     const T cc = coefs[b.coef_off + (g0 + j) * b.nprim + p] * e;
                     R[j] += cc;
-                    if (GRAD) Rp[j] -= a * cc;
+                    if constexpr (GRAD) Rp[j] -= a * cc;
                 }
         }
 #pragma unroll
@@ -96,30 +105,32 @@ __device__ __forceinline__ void eval_shell_t(const ShellDesc& b, double dxd, dou
                 const int ao0 = b.ao_off + (g0 + j) * NS;
 #pragma unroll
                 for (int s = 0; s < NS; ++s) {
-                    sink.template put<0>(ao0 + s, R[j] * v[s]);
-                    if (GRAD) {
-                        const T two_rp = T(2) * Rp[j] * v[s];
-                        sink.template put<1>(ao0 + s, R[j] * vx[s] + x * two_rp);
-                        sink.template put<2>(ao0 + s, R[j] * vy[s] + y * two_rp);
-                        sink.template put<3>(ao0 + s, R[j] * vz[s] + z * two_rp);
+                    sink.template put<0>(ao0 + s, R[j] * poly.v[s]);
+                    if constexpr (GRAD) {
+                        const T two_rp = T(2) * Rp[j] * poly.v[s];
+                        sink.template put<1>(ao0 + s, R[j] * poly.vx[s] + x * two_rp);
+                        sink.template put<2>(ao0 + s, R[j] * poly.vy[s] + y * two_rp);
+                        sink.template put<3>(ao0 + s, R[j] * poly.vz[s] + z * two_rp);
                     }
                 }
             }
     }
 }
 
-template <class T, bool GRAD, class Sink>
+// Runtime dispatch on l up to LMAX (at least the context's largest angular
+// momentum; shells above LMAX are not evaluated).
+template <class T, bool GRAD, int LMAX = kMaxL, class Sink>
 __device__ __forceinline__ void eval_shell_any(const ShellDesc& b, double dx, double dy, double dz,
-                                               const T* exps, const T* coefs, const T* c2s,
-                                               Sink& sink) {
+                                               const T* exps, const T* coefs, Sink& sink,
+                                               int ctr0 = 0, int ctr1 = 1 << 30) {
     switch (b.l) {
-    case 0: eval_shell_t<T, 0, GRAD>(b, dx, dy, dz, exps, coefs, c2s, sink); break;
-    case 1: eval_shell_t<T, 1, GRAD>(b, dx, dy, dz, exps, coefs, c2s, sink); break;
-    case 2: eval_shell_t<T, 2, GRAD>(b, dx, dy, dz, exps, coefs, c2s, sink); break;
-    case 3: eval_shell_t<T, 3, GRAD>(b, dx, dy, dz, exps, coefs, c2s, sink); break;
-    case 4: eval_shell_t<T, 4, GRAD>(b, dx, dy, dz, exps, coefs, c2s, sink); break;
-    case 5: eval_shell_t<T, 5, GRAD>(b, dx, dy, dz, exps, coefs, c2s, sink); break;
-    default: eval_shell_t<T, 6, GRAD>(b, dx, dy, dz, exps, coefs, c2s, sink); break;
+    case 0: eval_shell_t<T, 0, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
+    case 1: if constexpr (LMAX >= 1) eval_shell_t<T, 1, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
+    case 2: if constexpr (LMAX >= 2) eval_shell_t<T, 2, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
+    case 3: if constexpr (LMAX >= 3) eval_shell_t<T, 3, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
+    case 4: if constexpr (LMAX >= 4) eval_shell_t<T, 4, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
+    case 5: if constexpr (LMAX >= 5) eval_shell_t<T, 5, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
+    default: if constexpr (LMAX >= 6) eval_shell_t<T, 6, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
     }
 }
 

@@ -19,65 +19,6 @@
 
 namespace isdf {
 
-// ------------------------------------------------------------------------------
-// cartesian -> real spherical transform
-// ------------------------------------------------------------------------------
-namespace {
-
-double fact(int n) { double r = 1; for (int i = 2; i <= n; ++i) r *= i; return r; }
-double binom(int n, int k) {
-    if (k < 0 || k > n) return 0.0;
-    return fact(n) / (fact(k) * fact(n - k));
-}
-
-// Index of the cartesian monomial (lx, ly, lz) in libcint order.
-int cart_index(int l, int lx, int ly, int lz) {
-    (void)ly;
-    int idx = 0;
-    for (int x = l; x > lx; --x) idx += l - x + 1;
-    return idx + lz;
-}
-
-}  // namespace
-
-// Rows m = -l..l of r^l Y_lm (unit-sphere normalised real harmonics without the
-// Condon-Shortley phase) expanded in cartesian monomials, from the closed-form
-// expansion of real regular solid harmonics (Helgaker, Jorgensen & Olsen,
-// "Molecular Electronic-Structure Theory", eqs. 6.4.47-6.4.50) times
-// sqrt((2l+1)/4pi).  l = 0 is 1/sqrt(4pi) and l = 1 keeps the (x, y, z)
-// order scaled by sqrt(3/4pi), as the reference does for libcint's s/p path.
-std::vector<double> c2s_matrix(int l) {
-    const int nc = (l + 1) * (l + 2) / 2, ns = 2 * l + 1;
-    std::vector<double> t(static_cast<size_t>(ns) * nc, 0.0);
-    const double pi = 3.14159265358979323846;
-    if (l == 0) { t[0] = 1.0 / std::sqrt(4 * pi); return t; }
-    if (l == 1) {
-        for (int i = 0; i < 3; ++i) t[i * 3 + i] = std::sqrt(3.0 / (4 * pi));
-        return t;
-    }
-    const double pref = std::sqrt((2 * l + 1) / (4 * pi));
-    for (int m = -l; m <= l; ++m) {
-        const int am = std::abs(m);
-        const double norm = 1.0 / (std::pow(2.0, am) * fact(l)) *
-                            std::sqrt(2.0 * fact(l + am) * fact(l - am) / (m == 0 ? 2.0 : 1.0));
-        const int wm = m < 0 ? 1 : 0;  // 2*v_m
-        for (int tt = 0; tt <= (l - am) / 2; ++tt)
-            for (int u = 0; u <= tt; ++u)
-                for (int w = wm; w <= am; w += 2) {   // w = 2v
-                    const int sgn_exp = tt + (w - wm) / 2;
-                    const double c = ((sgn_exp & 1) ? -1.0 : 1.0) * std::pow(0.25, tt) *
-                                     binom(l, tt) * binom(l - tt, am + tt) * binom(tt, u) *
-                                     binom(am, w);
-                    const int lx = 2 * tt + am - 2 * u - w;
-                    const int ly = 2 * u + w;
-                    const int lz = l - 2 * tt - am;
-                    if (lx < 0 || ly < 0 || lz < 0 || c == 0) continue;
-                    t[static_cast<size_t>(m + l) * nc + cart_index(l, lx, ly, lz)] += pref * norm * c;
-                }
-    }
-    return t;
-}
-
 Context::~Context() {
     cudaFree(d_shells);
     cudaFree(d_exp);
@@ -85,8 +26,6 @@ Context::~Context() {
     cudaFree(d_expf);
     cudaFree(d_coeff);
     cudaFree(d_ao_atom);
-    cudaFree(d_c2s);
-    cudaFree(d_c2sf);
 }
 
 Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nbas,
@@ -124,6 +63,7 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
         s.prim_off = static_cast<int>(exps.size());
         s.coef_off = static_cast<int>(coefs.size());
         s.atom = atom;
+        s.amin = static_cast<float>(*std::min_element(env + b[5], env + b[5] + np));
         const double* xyz = &c->atom_xyz[3 * atom];
         s.x = xyz[0]; s.y = xyz[1]; s.z = xyz[2];
         exps.insert(exps.end(), env + b[5], env + b[5] + np);
@@ -135,18 +75,6 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
     }
     c->nao = static_cast<int>(nao);
     c->nshell = static_cast<int>(c->shells.size());
-    {
-        std::vector<double> all;
-        for (int l = 0; l <= kMaxL; ++l) {
-            auto t = c2s_matrix(l);
-            all.insert(all.end(), t.begin(), t.end());
-        }
-        std::vector<float> allf(all.begin(), all.end());
-        ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c->d_c2s), all.size() * sizeof(double)));
-        ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c->d_c2sf), allf.size() * sizeof(float)));
-        ISDF_CUDA(cudaMemcpy(c->d_c2s, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
-        ISDF_CUDA(cudaMemcpy(c->d_c2sf, allf.data(), allf.size() * sizeof(float), cudaMemcpyHostToDevice));
-    }
     auto up = [](auto*& dst, const auto& src) {
         using V = std::remove_pointer_t<std::remove_reference_t<decltype(dst)>>;
         if (src.empty()) return;
@@ -171,7 +99,6 @@ namespace {
 template <class T>
 struct RawSink {
     T* val; T* grad; int64_t p, n, ld; bool want_val;
-    __device__ __forceinline__ bool wants(int, int) const { return true; }
     template <int C> __device__ __forceinline__ void put(int ao, T v) {
         if (C == 0) { if (want_val) val[p * ld + ao] = v; }
         else grad[((C - 1) * n + p) * ld + ao] = v;
@@ -181,7 +108,6 @@ struct RawSink {
 template <class T>
 struct AxisSink {
     T* out; int64_t p, ld; const AxisSpec* ax; const int* off; double sq[4]; bool count;
-    __device__ __forceinline__ bool wants(int, int) const { return true; }
     template <int C> __device__ __forceinline__ void put(int ao, T v) {
         if (!((ax->need_mask >> C) & 1)) return;
         if (count) sq[C] += static_cast<double>(v) * static_cast<double>(v);
@@ -196,7 +122,7 @@ constexpr int kShellLanes = 4;
 template <class T, bool GRAD>
 __global__ void __launch_bounds__(kPtsPerBlock * kShellLanes)
 ao_raw_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restrict__ exps,
-              const T* __restrict__ coefs, const T* __restrict__ c2s, const double* __restrict__ pts,
+              const T* __restrict__ coefs, const double* __restrict__ pts,
               int64_t n, T* val, T* grad, int64_t ld, bool want_val) {
     const int64_t p = static_cast<int64_t>(blockIdx.x) * kPtsPerBlock + threadIdx.x;
     if (p >= n) return;
@@ -204,14 +130,14 @@ ao_raw_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restr
     RawSink<T> sink{val, grad, p, n, ld, want_val};
     for (int sh = threadIdx.y; sh < nshell; sh += kShellLanes) {
         const ShellDesc b = shells[sh];
-        eval_shell_any<T, GRAD>(b, px - b.x, py - b.y, pz - b.z, exps, coefs, c2s, sink);
+        eval_shell_any<T, GRAD>(b, px - b.x, py - b.y, pz - b.z, exps, coefs, sink);
     }
 }
 
 template <class T, bool GRAD>
 __global__ void __launch_bounds__(kPtsPerBlock * kShellLanes)
 ao_axis_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restrict__ exps,
-               const T* __restrict__ coefs, const T* __restrict__ c2s, const double* __restrict__ pts,
+               const T* __restrict__ coefs, const double* __restrict__ pts,
                const int64_t* __restrict__ index, int64_t n, AxisSpec ax, T* out, int64_t ld,
                double* sumsq, const double* __restrict__ weights, int nao) {
     __shared__ double red[kPtsPerBlock * kShellLanes][4];
@@ -227,7 +153,7 @@ ao_axis_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __rest
         sink.count = sumsq != nullptr && (weights == nullptr || weights[gi] != 0.0);
         for (int sh = threadIdx.y; sh < nshell; sh += kShellLanes) {
             const ShellDesc b = shells[sh];
-            eval_shell_any<T, GRAD>(b, px - b.x, py - b.y, pz - b.z, exps, coefs, c2s, sink);
+            eval_shell_any<T, GRAD>(b, px - b.x, py - b.y, pz - b.z, exps, coefs, sink);
         }
     }
     if (sumsq) {
@@ -249,9 +175,6 @@ template <> const float* exps_of<float>(const Context& c) { return c.d_expf; }
 template <class T> const T* coefs_of(const Context& c);
 template <> const double* coefs_of<double>(const Context& c) { return c.d_coef; }
 template <> const float* coefs_of<float>(const Context& c) { return c.d_coeff; }
-template <class T> const T* c2s_of(const Context& c);
-template <> const double* c2s_of<double>(const Context& c) { return c.d_c2s; }
-template <> const float* c2s_of<float>(const Context& c) { return c.d_c2sf; }
 
 }  // namespace
 
@@ -265,11 +188,11 @@ void eval_ao(const Context& c, const double* pts, int64_t n, T* out_val, T* out_
     require(nb < (1ll << 31), "too many grid points for one launch");
     if (out_grad)
         ao_raw_kernel<T, true><<<static_cast<unsigned>(nb), block, 0, s>>>(
-            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), c2s_of<T>(c), pts, n, out_val,
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, n, out_val,
             out_grad, ld, out_val != nullptr);
     else
         ao_raw_kernel<T, false><<<static_cast<unsigned>(nb), block, 0, s>>>(
-            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), c2s_of<T>(c), pts, n, out_val,
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, n, out_val,
             nullptr, ld, true);
     ISDF_LAUNCH_CHECK();
 }
@@ -287,11 +210,11 @@ void eval_axis_features(const Context& c, const double* pts, const int64_t* inde
     const bool grad = (ax.need_mask & 0xE) != 0;
     if (grad)
         ao_axis_kernel<T, true><<<static_cast<unsigned>(nb), block, 0, s>>>(
-            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), c2s_of<T>(c), pts, index, n, ax,
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, index, n, ax,
             out, ld, sumsq, weights, c.nao);
     else
         ao_axis_kernel<T, false><<<static_cast<unsigned>(nb), block, 0, s>>>(
-            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), c2s_of<T>(c), pts, index, n, ax,
+            c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, index, n, ax,
             out, ld, sumsq, weights, c.nao);
     ISDF_LAUNCH_CHECK();
 }

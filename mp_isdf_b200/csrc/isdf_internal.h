@@ -102,7 +102,8 @@ struct ShellDesc {
     int l, nprim, nctr, ao_off;
     int prim_off;   // exponents at prim_off .. prim_off+nprim
     int coef_off;   // coefficients [nctr][nprim] at coef_off
-    int atom, pad;
+    int atom;
+    float amin;     // smallest exponent: the shell is exactly zero where amin r^2 > kExpCut
     double x, y, z;
 };
 
@@ -124,8 +125,6 @@ struct Context {
     float* d_expf = nullptr;
     float* d_coeff = nullptr;
     int32_t* d_ao_atom = nullptr;
-    double* d_c2s = nullptr;              // cartesian->spherical tables, l = 0..kMaxL
-    float* d_c2sf = nullptr;
     ~Context();
 };
 
@@ -133,7 +132,6 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
                         const double* env, int64_t nenv);
 
 // Real-spherical transform of one angular momentum: nsph x ncart, row-major.
-std::vector<double> c2s_matrix(int l);
 
 // ---- AO evaluation ---------------------------------------------------------------
 // Component codes used by the kernels: 0 value, 1 d/dx, 2 d/dy, 3 d/dz.

@@ -9,7 +9,6 @@ struct ProjectArgs {
     const ShellDesc* shells;
     const float* expf_;
     const float* coeff_;
-    const float* c2sf;
     float* point_sq;           // [n][4] per-point sums of squares per component, or null
     int nao;
     const double* pts;
@@ -17,8 +16,9 @@ struct ProjectArgs {
     const double* weights;     // for the sums of squares (may be null)
     int64_t n;
     int nchunks;
-    const int* chunk_shell_begin;
-    const int* chunk_shell_end;
+    const int4* pieces;        // (shell, first contraction, contractions, first slot in chunk)
+    const int* chunk_piece_begin;  // pieces of chunk c: [begin[c], begin[c+1])
+    const int* chunk_fill;     // slots of chunk c in use; the rest are zero
     const uint8_t* wimg;       // per chunk: nax x (hi, lo) BF16 tiles
     int comp_mask;
     int axis_comp[4];
@@ -30,11 +30,12 @@ struct ProjectArgs {
 };
 
 struct ProjectPlan {
-    int nax = 0, nout = 0, nt = 0, nchunks = 0, comp_mask = 0;
+    int nax = 0, nout = 0, nt = 0, nchunks = 0, comp_mask = 0, lmax = 0;
     int axis_comp[4] = {0, 0, 0, 0};
     bool grad = false;
     DeviceBuffer<uint16_t> wimg;
-    DeviceBuffer<int> chunk_begin, chunk_end;
+    DeviceBuffer<int4> pieces;
+    DeviceBuffer<int> piece_begin, fill;
 };
 
 // W is row-major [nax*nao][nout] in FP64; it is split into BF16 hi + lo.

@@ -30,6 +30,13 @@ __device__ __forceinline__ ArgKey warp_best(ArgKey k) {
     return k;
 }
 
+// Result valid in every lane.
+__device__ __forceinline__ double warp_allsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // Result valid in thread 0.  `sh` needs NT/32 entries.
 template <int NT>
 __device__ __forceinline__ ArgKey block_best(ArgKey k, ArgKey* sh) {

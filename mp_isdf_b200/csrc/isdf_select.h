@@ -82,6 +82,10 @@ struct MixedSketch {
     ExactSketchSource source;
 };
 // Fills Yt with the mixed-precision sketch of the kept points and returns the
+// Largest basis the FP64 re-verification of sketch columns holds in shared
+// memory (four components of one point, FP64).
+constexpr int kMaxVerifiedNao = 6144;
+
 // FP64 recomputation source (scales, W^T, error bounds) for the verified QR.
 MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& kp, const double* w,
                          const AxisSpec& ax, const double* axis_weights, int64_t ell,

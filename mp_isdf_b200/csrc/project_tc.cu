@@ -2,7 +2,7 @@
 //
 // For a tile of 128 grid points (one UMMA M=128 tile) the CTA evaluates the
 // needed AO components (value and/or d/dx, d/dy, d/dz) in FP32, one K-chunk of
-// 32 AOs at a time, splits them into BF16 hi + lo parts and multiplies them on
+// 32 AO slots at a time, splits them into BF16 hi + lo parts and multiplies them on
 // the tensor cores with a pre-split BF16 hi + lo weight matrix:
 //     P[g][a][n] = sum_mu comp_a(g, mu) W_a[mu][n]
 //                ~ A_hi B_hi + A_hi B_lo + A_lo B_hi   (FP32 accumulate in TMEM)
@@ -10,12 +10,18 @@
 // is written to HBM.  Used for
 //   * the Khatri-Rao sketch projections f_g . [u_s v_s] (all selected axes);
 //   * the fit Gram G[g][k] = phi_g . phi_a(k) (AO values only).
-// The per-component sums of squares of the FP32 values are accumulated in FP64
-// for the multi-axis Frobenius scales.
+// K-chunks hold whole contraction groups ("pieces") padded to 32 slots, so a
+// producer thread evaluates each (point, piece) once, writes its values at
+// fixed slots and needs no range checks.  A piece whose every primitive is
+// beyond the exponent cutoff at a point is exactly zero there and skipped.
+// The per-component sums of squares of the FP32 values are accumulated (FP32
+// per piece, FP64 across pieces) for the multi-axis Frobenius scales and the
+// error bounds.
 //
-// Warp roles (320 threads): warps 0-7 evaluate AOs (thread = point, two shell
-// lanes), convert to the UMMA operand layout and, warps 0-3, run the TMEM
-// epilogue; warp 8 issues the MMAs; warp 9 streams W chunks by bulk copy.
+// Warp roles: 4*PPT producer warps evaluate AOs (thread = point x piece lane),
+// convert to the UMMA operand layout and, warps 0-3, run the TMEM epilogue;
+// one warp issues the MMAs; one warp streams W chunks by bulk copy.  The FP32
+// staging buffer lets chunk c+1 be evaluated while the MMAs of chunk c run.
 #include "ao_device.cuh"
 #include "isdf_project.h"
 #include "isdf_reduce.cuh"
@@ -31,30 +37,21 @@ namespace isdf {
 namespace {
 
 constexpr int kRows = 128;            // points per tile (UMMA M)
-constexpr int kChunk = 32;            // AOs per K-chunk
-constexpr int kProducers = 256;       // 8 warps
-constexpr int kThreads = kProducers + 64;
+constexpr int kChunk = 32;            // AO slots per K-chunk
 constexpr uint32_t kTileA = kRows * kChunk * 2;       // bytes of one BF16 A tile (8 KB)
 constexpr uint32_t kLboA = (kRows / 8) * 128;          // K-adjacent core matrices
 constexpr uint32_t kSboA = 128;                        // M-adjacent core matrices
 
-// Writes component values of AO column k (0..31 within the chunk) of point p
-// into the FP32 staging buffer stage[comp][k][p].
+// Writes the component values of one piece into the FP32 staging buffer
+// stage[comp][slot][point]; slot = ao + base.
 struct StageSink {
-    float* stage;        // [ncomp][kChunk][kRows]
-    int p, ao_lo, ao_hi, ao0;  // AOs in [ao_lo, ao_hi) belong to this chunk; ao0 = chunk start
-    int comp_slot[4];    // slot of each component in the staging buffer, -1 if unused
-    bool count;
-    double sq[4];
-    __device__ __forceinline__ bool wants(int first, int last) const {
-        return last > ao_lo && first < ao_hi;
-    }
+    float* stage;
+    int p, base;
+    float sq[4];
     template <int C>
     __device__ __forceinline__ void put(int ao, float v) {
-        const int slot = comp_slot[C];
-        if (slot < 0 || ao < ao_lo || ao >= ao_hi) return;
-        stage[(slot * kChunk + (ao - ao0)) * kRows + p] = v;
-        if (count) sq[C] += static_cast<double>(v) * static_cast<double>(v);
+        stage[(C * kChunk + ao + base) * kRows + p] = v;
+        sq[C] += v * v;
     }
 };
 
@@ -83,9 +80,17 @@ __device__ __forceinline__ void named_bar_sync(int id, int count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-template <int NAX, int NT, bool GRAD>
-__global__ void __launch_bounds__(kThreads, 1)
+template <int PPT>
+struct Roles {
+    static constexpr int kProducers = kRows * PPT;
+    static constexpr int kThreads = kProducers + 64;
+};
+
+template <int NAX, int NT, bool GRAD, int LMAX, int PPT>
+__global__ void __launch_bounds__(Roles<PPT>::kThreads, 1)
 project_tc_kernel(ProjectArgs args) {
+    constexpr int kProducers = Roles<PPT>::kProducers;
+    constexpr int kThreads = Roles<PPT>::kThreads;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // layout: [A: NAX x (hi, lo) tiles][B: 2 stages x NAX x (hi, lo)][stage FP32][barriers]
     constexpr uint32_t kTileB = NT * kChunk * 2;
@@ -108,6 +113,7 @@ project_tc_kernel(ProjectArgs args) {
 
     const int tid = threadIdx.x;
     const int warp = tid / 32, lane = tid % 32;
+    constexpr int kMmaWarp = kProducers / 32;
     constexpr uint32_t kTmemCols = (NAX * NT <= 32) ? 32 : (NAX * NT <= 64) ? 64
                                    : (NAX * NT <= 128) ? 128 : (NAX * NT <= 256) ? 256 : 512;
     static_assert(NAX * NT <= 512, "accumulators exceed TMEM");
@@ -140,16 +146,10 @@ project_tc_kernel(ProjectArgs args) {
         *abort_flag = 1;
     };
 
-    if (warp < 8) {
+    if (warp < kMmaWarp) {
         // ------------------------------ producers ------------------------------
         const int p = tid & (kRows - 1);
-        const int half = tid >> 7;
-        int comp_slot[4] = {-1, -1, -1, -1};
-        {
-            int s = 0;
-            for (int c = 0; c < 4; ++c)
-                if ((args.comp_mask >> c) & 1) comp_slot[c] = s++;
-        }
+        const int lanegrp = tid / kRows;     // piece lane of this thread
         uint32_t q = 0;   // chunk sequence number of this CTA
         uint32_t t = 0;   // tile sequence number of this CTA
         for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++t) {
@@ -164,27 +164,37 @@ project_tc_kernel(ProjectArgs args) {
             }
             float psq[4] = {0.f, 0.f, 0.f, 0.f};
             for (int c = 0; c < nchunks; ++c, ++q) {
-                // 1. evaluate this chunk's AOs into the FP32 staging buffer
-                StageSink sink{sStage, p, c * kChunk, min((c + 1) * kChunk, args.nao), c * kChunk,
-                               {comp_slot[0], comp_slot[1], comp_slot[2], comp_slot[3]},
-                               count || args.point_sq != nullptr, {0, 0, 0, 0}};
-                if (half == 0) {
-                    for (int s = 0; s < kNComp; ++s)
-                        for (int k = 0; k < kChunk; ++k) sStage[(s * kChunk + k) * kRows + p] = 0.f;
-                }
-                named_bar_sync(1, kProducers);
+                // 1. evaluate this chunk's pieces into the FP32 staging buffer
+                const int pe = args.chunk_piece_begin[c + 1];
+                for (int k = (valid ? args.chunk_fill[c] : 0) + lanegrp; k < kChunk; k += PPT)
+#pragma unroll
+                    for (int cc = 0; cc < kNComp; ++cc) sStage[(cc * kChunk + k) * kRows + p] = 0.f;
+                double csq[4] = {0, 0, 0, 0};
                 if (valid) {
-                    for (int sh = args.chunk_shell_begin[c] + half; sh < args.chunk_shell_end[c]; sh += 2) {
-                        const ShellDesc b = args.shells[sh];
+                    for (int pi = args.chunk_piece_begin[c] + lanegrp; pi < pe; pi += PPT) {
+                        const int4 pc = args.pieces[pi];
+                        const ShellDesc b = args.shells[pc.x];
+                        const int ns = 2 * b.l + 1;
                         const double dx = px - b.x, dy = py - b.y, dz = pz - b.z;
-                        eval_shell_any<float, GRAD>(b, dx, dy, dz, args.expf_, args.coeff_,
-                                                    args.c2sf, sink);
+                        const float r2 = static_cast<float>(dx * dx + dy * dy + dz * dz);
+                        if (b.amin * r2 > static_cast<float>(kExpCut)) {
+                            // every primitive is cut off: the piece is exactly zero here
+                            for (int k = pc.w; k < pc.w + pc.z * ns; ++k)
+#pragma unroll
+                                for (int cc = 0; cc < kNComp; ++cc) sStage[(cc * kChunk + k) * kRows + p] = 0.f;
+                            continue;
+                        }
+                        StageSink sink{sStage, p, pc.w - (b.ao_off + pc.y * ns), {0.f, 0.f, 0.f, 0.f}};
+                        eval_shell_any<float, GRAD, LMAX>(b, dx, dy, dz, args.expf_, args.coeff_, sink,
+                                                          pc.y, pc.y + pc.z);
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc) csq[cc] += sink.sq[cc];
                     }
                 }
 #pragma unroll
                 for (int cc = 0; cc < 4; ++cc) {
-                    if (count) sq[cc] += sink.sq[cc];
-                    psq[cc] += static_cast<float>(sink.sq[cc]);
+                    if (count) sq[cc] += csq[cc];
+                    psq[cc] += static_cast<float>(csq[cc]);
                 }
                 named_bar_sync(1, kProducers);
                 // 2. wait until the MMAs of the previous chunk released the A tiles
@@ -195,7 +205,7 @@ project_tc_kernel(ProjectArgs args) {
                     const int rest = u / kRows;
                     const int kg = rest % (kChunk / 8);
                     const int a = rest / (kChunk / 8);
-                    const int slot = comp_slot[args.axis_comp[a]];
+                    const int slot = GRAD ? args.axis_comp[a] : 0;
                     float x[8];
 #pragma unroll
                     for (int i = 0; i < 8; ++i) x[i] = sStage[(slot * kChunk + kg * 8 + i) * kRows + row];
@@ -212,7 +222,7 @@ project_tc_kernel(ProjectArgs args) {
                 named_bar_sync(1, kProducers);
                 if (*prod_abort) break;
             }
-            // per-point sums of squares of each component (two shell lanes add up)
+            // per-point sums of squares of each component (the piece lanes add up)
             if (args.point_sq && valid)
                 for (int cc = 0; cc < 4; ++cc)
                     if ((args.comp_mask >> cc) & 1) atomicAdd(&args.point_sq[g * 4 + cc], psq[cc]);
@@ -242,7 +252,7 @@ project_tc_kernel(ProjectArgs args) {
             named_bar_sync(1, kProducers);
             if (*prod_abort) break;
         }
-    } else if (warp == 8) {
+    } else if (warp == kMmaWarp) {
         // ------------------------------ MMA issuer ------------------------------
         if (lane == 0) {
             constexpr uint32_t idesc = tc::idesc_bf16_f32(kRows, NT);
@@ -307,7 +317,7 @@ project_tc_kernel(ProjectArgs args) {
     __syncthreads();
     if (args.sumsq && tid < 4 && ((args.comp_mask >> tid) & 1)) {
         double v = 0;
-        for (int w = 0; w < 8; ++w) v += red[w][tid];
+        for (int w = 0; w < kMmaWarp; ++w) v += red[w][tid];
         atomicAdd(&args.sumsq[tid], v);
     }
     tc::tc_fence_after();
@@ -321,21 +331,31 @@ size_t smem_bytes() {
     return NAX * 2 * kTileA + 2 * NAX * 2 * kTileB + kNComp * kChunk * kRows * 4 + 256 + 1024;
 }
 
-template <int NAX, int NT, bool GRAD>
+template <int NAX, int NT, bool GRAD, int LMAX, int PPT>
 void launch(const ProjectArgs& a, int nsm, cudaStream_t s) {
     const size_t smem = smem_bytes<NAX, NT, GRAD>();
-    auto kern = project_tc_kernel<NAX, NT, GRAD>;
+    auto kern = project_tc_kernel<NAX, NT, GRAD, LMAX, PPT>;
     ISDF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(smem)));
     const int64_t ntiles = (a.n + kRows - 1) / kRows;
     const int grid = static_cast<int>(std::min<int64_t>(ntiles, nsm));
-    kern<<<grid, kThreads, smem, s>>>(a);
+    kern<<<grid, Roles<PPT>::kThreads, smem, s>>>(a);
     ISDF_LAUNCH_CHECK();
+}
+
+// Specialisation on the basis' largest angular momentum: small l leaves room
+// for four piece lanes (16 producer warps) within the register file.
+template <int NAX, int NT, bool GRAD>
+void launch_l(const ProjectArgs& a, int lmax, int nsm, cudaStream_t s) {
+    if (lmax <= 2) launch<NAX, NT, GRAD, 2, 4>(a, nsm, s);
+    else if (lmax <= 4) launch<NAX, NT, GRAD, 4, 2>(a, nsm, s);
+    else launch<NAX, NT, GRAD, kMaxL, 2>(a, nsm, s);
 }
 
 }  // namespace
 
-// Host-side preparation of the chunk plan and of the BF16 hi/lo weight image.
+// Host-side preparation of the shell-aligned chunk plan and of the BF16 hi/lo
+// weight image.
 ProjectPlan make_project_plan(const Context& c, const std::vector<int>& axis_comp,
                               const std::vector<double>& W, int nout, cudaStream_t s) {
     ProjectPlan pl;
@@ -351,49 +371,68 @@ ProjectPlan make_project_plan(const Context& c, const std::vector<int>& axis_com
         pl.comp_mask |= 1 << axis_comp[a];
         if (axis_comp[a] > 0) pl.grad = true;
     }
-    pl.nchunks = (nao + kChunk - 1) / kChunk;
-    // shells overlapping each chunk
-    std::vector<int> sb(pl.nchunks), se(pl.nchunks);
-    for (int ch = 0; ch < pl.nchunks; ++ch) {
-        const int lo = ch * kChunk, hi = std::min(nao, lo + kChunk);
-        int b = -1, e = -1;
-        for (int i = 0; i < c.nshell; ++i) {
-            const auto& sh = c.shells[i];
-            const int s0 = sh.ao_off, s1 = sh.ao_off + (2 * sh.l + 1) * sh.nctr;
-            if (s1 > lo && s0 < hi) { if (b < 0) b = i; e = i + 1; }
+    pl.lmax = c.lmax;
+    // pieces: runs of whole contractions of one shell; a chunk takes pieces in
+    // shell order until the next contraction no longer fits in its 32 slots
+    std::vector<int4> pieces;
+    std::vector<int> piece_begin{0}, fill;
+    std::vector<int> chunk_of_ao(nao, -1), slot_of_ao(nao, -1);
+    int used = 0;
+    auto close_chunk = [&]() {
+        fill.push_back(used);
+        piece_begin.push_back(static_cast<int>(pieces.size()));
+        used = 0;
+    };
+    for (int i = 0; i < c.nshell; ++i) {
+        const auto& sh = c.shells[i];
+        const int ns = 2 * sh.l + 1;
+        for (int j = 0; j < sh.nctr;) {
+            const int room = (kChunk - used) / ns;
+            if (room == 0) { close_chunk(); continue; }
+            const int take = std::min(room, sh.nctr - j);
+            pieces.push_back(make_int4(i, j, take, used));
+            for (int u = 0; u < take * ns; ++u) {
+                chunk_of_ao[sh.ao_off + j * ns + u] = static_cast<int>(fill.size());
+                slot_of_ao[sh.ao_off + j * ns + u] = used + u;
+            }
+            used += take * ns;
+            j += take;
         }
-        sb[ch] = b < 0 ? 0 : b;
-        se[ch] = e < 0 ? 0 : e;
     }
+    if (used > 0 || fill.empty()) close_chunk();
+    pl.nchunks = static_cast<int>(fill.size());
     // W image: per chunk, per axis, (hi, lo) tiles of NT rows x 32 K in the
     // interleaved K-major layout.  W is row-major [nax*nao][nout].
     const uint32_t tileB = pl.nt * kChunk * 2;
     const size_t stage = static_cast<size_t>(nax) * 2 * tileB;
     std::vector<uint16_t> img(stage / 2 * pl.nchunks, 0);
     const uint32_t lbo = (pl.nt / 8) * 128;
-    for (int ch = 0; ch < pl.nchunks; ++ch)
-        for (int a = 0; a < nax; ++a)
-            for (int nrow = 0; nrow < nout; ++nrow)
-                for (int k = 0; k < kChunk; ++k) {
-                    const int mu = ch * kChunk + k;
-                    if (mu >= nao) continue;
-                    const double wv = W[(static_cast<size_t>(a) * nao + mu) * nout + nrow];
-                    const float f = static_cast<float>(wv);
-                    const __nv_bfloat16 hb = __float2bfloat16_rn(f);
-                    const float hf = __bfloat162float(hb);
-                    const __nv_bfloat16 lb = __float2bfloat16_rn(static_cast<float>(wv - hf));
-                    const uint32_t off = tc::interleaved_offset(nrow, k, lbo, 128);
-                    const size_t base = (ch * stage + (a * 2) * tileB + off) / 2;
-                    img[base] = __bfloat16_as_ushort(hb);
-                    img[base + tileB / 2] = __bfloat16_as_ushort(lb);
-                }
+    for (int a = 0; a < nax; ++a)
+        for (int mu = 0; mu < nao; ++mu) {
+            const int ch = chunk_of_ao[mu], k = slot_of_ao[mu];
+            for (int nrow = 0; nrow < nout; ++nrow) {
+                const double wv = W[(static_cast<size_t>(a) * nao + mu) * nout + nrow];
+                const float f = static_cast<float>(wv);
+                const __nv_bfloat16 hb = __float2bfloat16_rn(f);
+                const float hf = __bfloat162float(hb);
+                const __nv_bfloat16 lb = __float2bfloat16_rn(static_cast<float>(wv - hf));
+                const uint32_t off = tc::interleaved_offset(nrow, k, lbo, 128);
+                const size_t base = (ch * stage + (a * 2) * tileB + off) / 2;
+                img[base] = __bfloat16_as_ushort(hb);
+                img[base + tileB / 2] = __bfloat16_as_ushort(lb);
+            }
+        }
     pl.wimg.reset(img.size(), s);
     ISDF_CUDA(cudaMemcpyAsync(pl.wimg.get(), img.data(), img.size() * 2, cudaMemcpyHostToDevice, s));
-    pl.chunk_begin.reset(pl.nchunks, s);
-    pl.chunk_end.reset(pl.nchunks, s);
-    ISDF_CUDA(cudaMemcpyAsync(pl.chunk_begin.get(), sb.data(), sb.size() * 4, cudaMemcpyHostToDevice, s));
-    ISDF_CUDA(cudaMemcpyAsync(pl.chunk_end.get(), se.data(), se.size() * 4, cudaMemcpyHostToDevice, s));
-    ISDF_CUDA(cudaStreamSynchronize(s));   // host image is a temporary
+    pl.pieces.reset(pieces.size(), s);
+    pl.piece_begin.reset(piece_begin.size(), s);
+    pl.fill.reset(fill.size(), s);
+    ISDF_CUDA(cudaMemcpyAsync(pl.pieces.get(), pieces.data(), pieces.size() * sizeof(int4),
+                              cudaMemcpyHostToDevice, s));
+    ISDF_CUDA(cudaMemcpyAsync(pl.piece_begin.get(), piece_begin.data(), piece_begin.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, s));
+    ISDF_CUDA(cudaMemcpyAsync(pl.fill.get(), fill.data(), fill.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));   // host images are temporaries
     return pl;
 }
 
@@ -411,7 +450,6 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     a.shells = c.d_shells;
     a.expf_ = c.d_expf;
     a.coeff_ = c.d_coeff;
-    a.c2sf = c.d_c2sf;
     a.point_sq = point_sq;
     a.nao = c.nao;
     a.pts = pts;
@@ -419,8 +457,9 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     a.weights = weights;
     a.n = n;
     a.nchunks = pl.nchunks;
-    a.chunk_shell_begin = pl.chunk_begin.get();
-    a.chunk_shell_end = pl.chunk_end.get();
+    a.pieces = pl.pieces.get();
+    a.chunk_piece_begin = pl.piece_begin.get();
+    a.chunk_fill = pl.fill.get();
     a.wimg = reinterpret_cast<const uint8_t*>(pl.wimg.get());
     a.comp_mask = pl.comp_mask;
     for (int i = 0; i < pl.nax; ++i) a.axis_comp[i] = pl.axis_comp[i];
@@ -434,7 +473,7 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     ISDF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     ISDF_PROFILE(pl.grad ? "project_tc_grad" : "project_tc_val", s);
 #define ISDF_TC_CASE(NAX, NT, G) \
-    if (pl.nax == NAX && pl.nt == NT && pl.grad == G) { launch<NAX, NT, G>(a, nsm, s); return; }
+    if (pl.nax == NAX && pl.nt == NT && pl.grad == G) { launch_l<NAX, NT, G>(a, pl.lmax, nsm, s); return; }
     ISDF_TC_CASE(1, 16, false) ISDF_TC_CASE(1, 32, false) ISDF_TC_CASE(1, 64, false)
     ISDF_TC_CASE(1, 16, true) ISDF_TC_CASE(1, 32, true) ISDF_TC_CASE(1, 64, true)
     ISDF_TC_CASE(2, 64, true) ISDF_TC_CASE(3, 64, true) ISDF_TC_CASE(4, 64, true)

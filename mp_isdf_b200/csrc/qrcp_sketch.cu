@@ -182,17 +182,14 @@ __global__ void __launch_bounds__(1024) qr_pivot_kernel(QrState st, int64_t j, i
 }
 
 // ---- exact FP64 sketch columns -----------------------------------------------------
-struct FeatSink {
-    double* feat; const int* comp; const double* scale; int naxes; int nao;
-    __device__ __forceinline__ bool wants(int, int) const { return true; }
-    template <int C> __device__ __forceinline__ void put(int ao, double v) {
-        for (int a = 0; a < naxes; ++a)
-            if (comp[a] == C) feat[a * nao + ao] = scale[a] * v;
-    }
+// Component-major AO values of one point: feat[C*nao + ao].
+struct CompSink {
+    double* feat; int nao;
+    template <int C> __device__ __forceinline__ void put(int ao, double v) { feat[C * nao + ao] = v; }
 };
 
 struct ExactArgs {
-    const ShellDesc* shells; int nshell; const double* exps; const double* coefs; const double* c2s;
+    const ShellDesc* shells; int nshell; const double* exps; const double* coefs;
     int nao; int naxes; int comp[16]; int grad;
     const double* scales;       // naxes (device)
     const double* WT;           // (2 ell) x d, row-major
@@ -200,59 +197,82 @@ struct ExactArgs {
     int64_t ell;
 };
 
+template <bool GRAD, int LMAX>
 __global__ void __launch_bounds__(256)
 exact_columns_kernel(ExactArgs ea, QrState st, const int64_t* cand, int64_t j) {
-    extern __shared__ double feat[];          // d doubles, then 2*ell doubles
-    __shared__ int comp_s[16];
-    __shared__ double scale_s[16];
+    constexpr int kNComp = GRAD ? 4 : 1;
+    extern __shared__ double feat[];   // kNComp*nao AO values, 2*ell projections, m sketch rows
     const int64_t g = cand[blockIdx.x];
     const int64_t gi = ea.index[g];
-    const int d = ea.naxes * ea.nao;
-    double* lr = feat + d;
-    if (threadIdx.x < ea.naxes) { comp_s[threadIdx.x] = ea.comp[threadIdx.x]; scale_s[threadIdx.x] = ea.scales[threadIdx.x]; }
-    for (int i = threadIdx.x; i < d; i += blockDim.x) feat[i] = 0.0;
-    __syncthreads();
+    const int nao = ea.nao;
+    const int64_t d = static_cast<int64_t>(ea.naxes) * nao;
+    double* lr = feat + kNComp * nao;
     const double px = ea.pts[3 * gi], py = ea.pts[3 * gi + 1], pz = ea.pts[3 * gi + 2];
-    FeatSink sink{feat, comp_s, scale_s, ea.naxes, ea.nao};
+    CompSink sink{feat, nao};
     for (int sh = threadIdx.x; sh < ea.nshell; sh += blockDim.x) {
         const ShellDesc b = ea.shells[sh];
-        if (ea.grad)
-            eval_shell_any<double, true>(b, px - b.x, py - b.y, pz - b.z, ea.exps, ea.coefs, ea.c2s, sink);
-        else
-            eval_shell_any<double, false>(b, px - b.x, py - b.y, pz - b.z, ea.exps, ea.coefs, ea.c2s, sink);
+        eval_shell_any<double, GRAD, LMAX>(b, px - b.x, py - b.y, pz - b.z, ea.exps, ea.coefs, sink);
     }
     __syncthreads();
     const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+    // projections lr[s2] = sum_a scale_a comp_a(g) . WT[s2][a]
     for (int64_t s2 = warp; s2 < 2 * ea.ell; s2 += blockDim.x / 32) {
         const double* wt = ea.WT + s2 * d;
         double acc = 0;
-        for (int i = lane; i < d; i += 32) acc += feat[i] * wt[i];
+        for (int a = 0; a < ea.naxes; ++a) {
+            const double* f = feat + (GRAD ? ea.comp[a] : 0) * nao;
+            const double* wa = wt + static_cast<int64_t>(a) * nao;
+            double pa = 0;
+            for (int i = lane; i < nao; i += 32) pa += f[i] * wa[i];
+            acc += ea.scales[a] * pa;
+        }
         acc = warp_sum(acc);
         if (lane == 0) lr[s2] = acc;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    // apply the j previous reflectors to the sketch column (warp 0, lanes over rows)
+    if (warp == 0) {
         const int64_t m = st.m;
+        double* y = lr + 2 * ea.ell;
         const double sw = sqrt(fabs(ea.w[gi])) / sqrt(static_cast<double>(ea.ell));
-        double y[128];
-        for (int64_t s = 0; s < m; ++s) y[s] = sw * lr[s] * lr[ea.ell + s];
+        for (int64_t s = lane; s < m; s += 32) y[s] = sw * lr[s] * lr[ea.ell + s];
+        __syncwarp();
         for (int64_t i = 0; i < j; ++i) {
             const double t = st.tau[i];
             if (t == 0.0) continue;
             const double* v = st.vhist + i * m;
             double dot = 0;
-            for (int64_t r = i; r < m; ++r) dot += v[r] * y[r];
-            dot *= t;
-            for (int64_t r = i; r < m; ++r) y[r] -= v[r] * dot;
+            for (int64_t r = i + lane; r < m; r += 32) dot += v[r] * y[r];
+            dot = warp_allsum(dot) * t;
+            for (int64_t r = i + lane; r < m; r += 32) y[r] -= v[r] * dot;
+            __syncwarp();
         }
         double nrm = 0;
-        for (int64_t s = 0; s < m; ++s) {
+        for (int64_t s = lane; s < m; s += 32) {
             st.Yt[s * st.ldy + g] = y[s];
             if (s >= j) nrm += y[s] * y[s];
         }
-        st.est[g] = nrm;
-        st.delta[g] = 0.0;
+        nrm = warp_sum(nrm);
+        if (lane == 0) {
+            st.est[g] = nrm;
+            st.delta[g] = 0.0;
+        }
     }
+}
+
+using ExactKernel = void (*)(ExactArgs, QrState, const int64_t*, int64_t);
+
+// Specialisation on the basis' largest angular momentum keeps the FP64
+// evaluation within registers.
+ExactKernel pick_exact_kernel(bool grad, int lmax) {
+    if (grad) {
+        if (lmax <= 2) return exact_columns_kernel<true, 2>;
+        if (lmax <= 4) return exact_columns_kernel<true, 4>;
+        return exact_columns_kernel<true, kMaxL>;
+    }
+    if (lmax <= 2) return exact_columns_kernel<false, 2>;
+    if (lmax <= 4) return exact_columns_kernel<false, 4>;
+    return exact_columns_kernel<false, kMaxL>;
 }
 
 }  // namespace
@@ -279,6 +299,7 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
                diag.get(), energy.get(), jpvt.get(), partial.get(), nullptr, nullptr, nullptr};
     ExactArgs ea{};
     size_t exact_smem = 0;
+    ExactKernel exact_kernel = nullptr;
     if (exact) {
         est.reset(n, s);
         lbp.reset(nblocks, s);
@@ -290,12 +311,13 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
         st.lb_partial = lbp.get();
         const Context& c = *exact->ctx;
         ea.shells = c.d_shells; ea.nshell = c.nshell; ea.exps = c.d_exp; ea.coefs = c.d_coef;
-        ea.c2s = c.d_c2s; ea.nao = c.nao; ea.naxes = exact->naxes; ea.grad = 0;
+        ea.nao = c.nao; ea.naxes = exact->naxes; ea.grad = 0;
         for (int a = 0; a < exact->naxes; ++a) { ea.comp[a] = exact->comp[a]; ea.grad |= exact->comp[a] > 0; }
         ea.scales = exact->scales; ea.WT = exact->WT; ea.pts = exact->pts; ea.index = exact->index;
         ea.w = exact->w; ea.ell = exact->ell;
-        exact_smem = (static_cast<size_t>(exact->naxes) * c.nao + 2 * exact->ell) * sizeof(double);
-        ISDF_CUDA(cudaFuncSetAttribute(exact_columns_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        exact_smem = (static_cast<size_t>(ea.grad ? 4 : 1) * c.nao + 2 * exact->ell + m) * sizeof(double);
+        exact_kernel = pick_exact_kernel(ea.grad != 0, c.lmax);
+        ISDF_CUDA(cudaFuncSetAttribute(exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(exact_smem)));
     }
     int64_t reverified = 0;
@@ -318,7 +340,7 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
             ISDF_CUDA(cudaStreamSynchronize(s));
             if (hc > 0) {
                 require(hc < (int64_t(1) << 31), "too many sketch candidates");
-                exact_columns_kernel<<<static_cast<unsigned>(hc), 256, exact_smem, s>>>(ea, st, cand.get(), j);
+                exact_kernel<<<static_cast<unsigned>(hc), 256, exact_smem, s>>>(ea, st, cand.get(), j);
                 ISDF_LAUNCH_CHECK();
                 reverified += hc;
             }

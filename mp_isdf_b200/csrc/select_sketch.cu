@@ -370,7 +370,10 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
     DeviceBuffer<double> Yt(static_cast<size_t>(ell * n), s);
     const double* aw = o.axis_weights.empty() ? nullptr : o.axis_weights.data();
     SketchQR qr;
-    if (o.precision == 1 && project_tc_supported(ax.naxes, static_cast<int>(2 * ell)) && ell <= 64) {
+    // the mixed form needs the tensor-core shape and room for one point's AO
+    // components in shared memory for the FP64 re-verification of candidates
+    if (o.precision == 1 && project_tc_supported(ax.naxes, static_cast<int>(2 * ell)) && ell <= 64 &&
+        c.nao <= kMaxVerifiedNao) {
         MixedSketch ms = sketch_mixed(c, pts, kp, w, ax, aw, ell, u, v, Yt.get(), ldy, s);
         qr = qrcp_sketch(Yt.get(), ldy, ell, n, s, &ms.source);
     } else {

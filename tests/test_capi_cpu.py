@@ -59,19 +59,16 @@ def test_context_without_gpu_fails_loudly(s_shells):
         mp_isdf.LibcintContext(*s_shells)
 
 
-def test_c2s_closed_form_matches_oracle_least_squares():
-    """The product's closed-form solid-harmonic table (C++) and the oracle's
-    least-squares derivation agree; checked through a tiny host-only helper
-    compiled from the same source formula."""
+def test_c2s_compile_time_table_matches_oracle_least_squares():
+    """The product's compile-time solid-harmonic table (c2s_table.h, the
+    coefficients the device AO code multiplies by) and the oracle's
+    least-squares derivation agree; the header is compiled host-only."""
     import subprocess, tempfile
     from oracle import oracle as O
-    src = ROOT / "mp_isdf_b200" / "csrc" / "context.cu"
-    text = src.read_text()
-    start = text.index("namespace {\n\ndouble fact")
-    end = text.index("Context::~Context()")
-    snippet = "#include <cmath>\n#include <cstdio>\n#include <vector>\n#include <cstdlib>\n" \
-              "namespace isdf {\n" + text[start:end] + "}\nint main(){for(int l=0;l<=6;++l){auto t=isdf::c2s_matrix(l);" \
-              "for(double x: t) std::printf(\"%.17g\\n\", x);} }\n"
+    hdr = ROOT / "mp_isdf_b200" / "csrc" / "c2s_table.h"
+    snippet = (f'#include "{hdr}"\n#include <cstdio>\n'
+               "int main(){for(int l=0;l<=6;++l)for(int s=0;s<2*l+1;++s)"
+               "for(int c=0;c<(l+1)*(l+2)/2;++c)std::printf(\"%.17g\\n\", isdf::c2s_coef(l,s,c));}\n")
     with tempfile.TemporaryDirectory() as d:
         c = Path(d) / "c2s.cpp"
         c.write_text(snippet)
