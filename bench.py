@@ -268,7 +268,11 @@ def run_ours(args, rank, world, local_rank):
             times.append(a.elapsed_time(b) / 1e3)
         clocks = sampler.stop()
         capi.profile_enable(False)
-        prof = capi.profile_read()
+        prof_all = capi.profile_read()
+        # "phase:" scopes time host+device phases of the call on the stream;
+        # the rest are kernel families
+        prof = {k: v for k, v in prof_all.items() if not k.startswith("phase:")}
+        phases = {k[6:]: v for k, v in prof_all.items() if k.startswith("phase:")}
         total = sum(times)
         if world > 1:
             t = torch.tensor([total], device=dev, dtype=torch.float64)
@@ -277,7 +281,7 @@ def run_ours(args, rank, world, local_rank):
         # pair-space error of this form's Theta, evaluated with FP64 AO values (untimed)
         einfo = ctx.fit(x, wt, piv, theta, precision=precision, want_error=True)
         torch.cuda.synchronize()
-        results[precision] = dict(total=total, times=times, prof=prof, clocks=clocks,
+        results[precision] = dict(total=total, times=times, prof=prof, phases=phases, clocks=clocks,
                                   piv=[int(p) for p in piv], sinfo=sinfo, einfo=einfo)
 
     head = forms[0]
@@ -288,14 +292,16 @@ def run_ours(args, rank, world, local_rank):
     # e2e through the host-buffer C-ABI (headline form)
     e2e = None
     if not args.no_e2e:
-        pts_h = np.ascontiguousarray(pts)
-        w_h = np.ascontiguousarray(w)
+        # pinned host buffers: inputs copied in by each call, Theta copied out
+        pts_h = torch.from_numpy(np.ascontiguousarray(pts)).pin_memory().numpy()
+        w_h = torch.from_numpy(np.ascontiguousarray(w)).pin_memory().numpy()
+        th_h = torch.empty(k * n, dtype=torch.float64).pin_memory().numpy()
         e2e_times = []
         for i in range(max(1, min(3, args.steps)) + 1):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             piv_h, _ = ctx.select_host(pts_h, w_h, **sel_kw(head))
-            th, _ = ctx.fit_host(pts_h, w_h, piv_h, precision=head)
+            th, _ = ctx.fit_host(pts_h, w_h, piv_h, precision=head, want_error=False, out=th_h)
             dt = time.perf_counter() - t0
             if i:
                 e2e_times.append(dt)
@@ -303,7 +309,7 @@ def run_ours(args, rank, world, local_rank):
         d2h = th.nbytes + 8 * len(piv_h)
         e2e = {"value": statistics.mean(e2e_times) / world, "unit": "s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "isdf_select_host + isdf_fit_host (pageable numpy buffers)"}
+               "path": "isdf_select_host + isdf_fit_host (pinned host buffers, wall clock)"}
 
     if rank != 0:
         return
@@ -350,6 +356,7 @@ def run_ours(args, rank, world, local_rank):
                         "step_times_s": r["times"], "anchors": r["piv"],
                         "pair_relative": r["einfo"].pair_relative, "pair_l2": r["einfo"].pair_l2,
                         "sketch_columns_reverified": r["sinfo"].verifications,
+                        "phases_ms_per_step": {k: v[0] / args.steps for k, v in r["phases"].items()},
                         "clocks": r["clocks"]}
     extra = {}
     if "mixed" in results and "fp64" in results:

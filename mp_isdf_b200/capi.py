@@ -236,14 +236,21 @@ class Context:
         del keep
         return piv[:n.value].copy(), info
 
-    def fit_host(self, xyz, w, anchors, precision="fp64"):
+    def fit_host(self, xyz, w, anchors, precision="fp64", want_error=True, out=None):
+        """Theta (k x n_kept) from host buffers.  `out` may supply the float64
+        host buffer (capacity k*ng, e.g. pinned memory) that Theta lands in."""
         xyz = _np(xyz, np.float64).reshape(-1, 3)
         w = _np(w, np.float64)
         a = _np(anchors, np.int64)
-        theta = np.empty(max(1, len(a) * len(xyz)))
+        if out is None:
+            theta = np.empty(max(1, len(a) * len(xyz)))
+        else:
+            theta = out
+            if theta.dtype != np.float64 or not theta.flags.c_contiguous or theta.size < len(a) * len(xyz):
+                raise ValueError("out must be a contiguous float64 buffer of at least k*ng entries")
         info = FitInfo()
         check(lib().isdf_fit_host(self.h, _ptr(xyz), _ptr(w), len(xyz), _ptr(a), len(a),
-                                  1 if precision == "mixed" else 0, 1, _ptr(theta),
+                                  1 if precision == "mixed" else 0, int(want_error), _ptr(theta),
                                   ctypes.byref(info)))
         return theta[:len(a) * info.n_kept].reshape(len(a), info.n_kept), info
 

@@ -326,13 +326,22 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
     if (ng < 0 || k < 0) isdf::fail(isdf::kInvalid, "sizes must be nonnegative");
     if (precision != ISDF_FP64 && precision != ISDF_MIXED)
         isdf::fail(isdf::kInvalid, "precision must be fp64 or mixed");
-    isdf::KeptPoints kp = isdf::compact_points(xyz, w, ng, s);
+    ISDF_PROFILE("phase:fit", s);
+    isdf::KeptPoints kp;
+    {
+        ISDF_PROFILE("phase:compact", s);
+        kp = isdf::compact_points(xyz, w, ng, s);
+    }
     isdf::DeviceBuffer<int64_t> didx;
     upload(didx, anchors, static_cast<size_t>(k), s);
     isdf::DeviceBuffer<double> apts(static_cast<size_t>(3 * std::max<int64_t>(k, 1)), s),
         aw(std::max<int64_t>(k, 1), s);
     isdf::gather_points(xyz, w, didx.get(), k, ng, apts.get(), aw.get(), s);
-    isdf::AnchorFactor f = isdf::factor_anchors(c, apts.get(), aw.get(), k, s);
+    isdf::AnchorFactor f;
+    {
+        ISDF_PROFILE("phase:factor_anchors", s);
+        f = isdf::factor_anchors(c, apts.get(), aw.get(), k, s);
+    }
     const bool have = theta_in != nullptr;
     double* theta = have ? const_cast<double*>(theta_in) : theta_out;
     isdf::FitOutput o;
@@ -428,7 +437,11 @@ int isdf_energy_gradient(isdf_ctx* ctx, const double* xyz, const double* w, int6
         upload(didx, anchors, static_cast<size_t>(k), s);
         isdf::DeviceBuffer<double> apts(static_cast<size_t>(3 * k), s), aw(k, s);
         isdf::gather_points(xyz, w, didx.get(), k, ng, apts.get(), aw.get(), s);
-        isdf::AnchorFactor f = isdf::factor_anchors(c, apts.get(), aw.get(), k, s);
+        isdf::AnchorFactor f;
+    {
+        ISDF_PROFILE("phase:factor_anchors", s);
+        f = isdf::factor_anchors(c, apts.get(), aw.get(), k, s);
+    }
         isdf::AdjointResult r = isdf::energy_gradient(c, xyz, w, kp, f, dm, s);
         if (energy) *energy = r.energy;
         if (grad) std::memcpy(grad, r.grad.data(), r.grad.size() * sizeof(double));

@@ -440,7 +440,11 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
     ISDF_CUDA(cudaStreamSynchronize(s));
     for (int64_t a = 0; a < k; ++a)
         for (int64_t mu = 0; mu < nao; ++mu) W[mu * k + a] = phi[a * nao + mu];
-    ProjectPlan plan = make_project_plan(c, {0}, W, static_cast<int>(k), s);
+    ProjectPlan plan;
+    {
+        ISDF_PROFILE("phase:fit_plan", s);
+        plan = make_project_plan(c, {0}, W, static_cast<int>(k), s);
+    }
     DeviceBuffer<float> G(static_cast<size_t>(n * k), s), psq(static_cast<size_t>(n * 4), s);
     DeviceBuffer<int> err(1, s);
     DeviceBuffer<double> acc(6, s), tw(k, s), anorm(k, s);

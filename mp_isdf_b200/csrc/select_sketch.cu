@@ -22,6 +22,7 @@
 #include <cmath>
 #include <limits>
 #include <random>
+#include <thread>
 
 namespace isdf {
 
@@ -122,14 +123,17 @@ void validate_axis_weights(const double* axis_weights, int naxes) {
 void sketch_factors(int64_t d, int64_t ell, uint64_t seed, std::vector<double>& u,
                     std::vector<double>& v) {
     // Two independent streams; fill order i = a*ell + s.
-    std::mt19937_64 gen_u(seed), gen_v(seed ^ 0x9e3779b97f4a7c15ULL);
-    std::normal_distribution<double> normal_u(0, 1), normal_v(0, 1);
+    // The streams are independent, so each fills its matrix on its own thread.
     u.resize(static_cast<size_t>(d * ell));
     v.resize(static_cast<size_t>(d * ell));
-    for (int64_t i = 0; i < d * ell; ++i) {
-        u[i] = normal_u(gen_u);
-        v[i] = normal_v(gen_v);
-    }
+    auto fill = [d, ell](uint64_t sd, std::vector<double>& out) {
+        std::mt19937_64 gen(sd);
+        std::normal_distribution<double> normal(0, 1);
+        for (int64_t i = 0; i < d * ell; ++i) out[i] = normal(gen);
+    };
+    std::thread tv(fill, seed ^ 0x9e3779b97f4a7c15ULL, std::ref(v));
+    fill(seed, u);
+    tv.join();
 }
 
 namespace {
@@ -286,7 +290,11 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
             hwt[(ell + t) * d + j] = v[j * ell + t];
         }
     std::vector<int> comps(ax.comp, ax.comp + naxes);
-    ProjectPlan plan = make_project_plan(c, comps, hw, nout, s);
+    ProjectPlan plan;
+    {
+        ISDF_PROFILE("phase:sketch_plan", s);
+        plan = make_project_plan(c, comps, hw, nout, s);
+    }
     DeviceBuffer<float> P(static_cast<size_t>(n * naxes * nout), s), psq(static_cast<size_t>(n * 4), s);
     DeviceBuffer<double> sumsq(4, s);
     DeviceBuffer<int> err(1, s), dcomp(naxes, s);
@@ -349,7 +357,12 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
     if (o.max_rank > std::numeric_limits<int64_t>::max() - o.oversampling)
         fail(kOverflow, "randomized ID rank + oversampling overflows size_t");
     const int64_t requested = o.max_rank ? o.max_rank + o.oversampling : o.sketch_size;
-    KeptPoints kp = compact_points(pts, w, ng, s);
+    ISDF_PROFILE("phase:select", s);
+    KeptPoints kp;
+    {
+        ISDF_PROFILE("phase:compact", s);
+        kp = compact_points(pts, w, ng, s);
+    }
     const int64_t n = kp.n;
     if (n == 0) return {};
     const int64_t physical_rank = d * (d + 1) / 2;
@@ -365,7 +378,10 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
     if (o.max_rank > std::min(n, physical_rank))
         fail(kInvalid, "requested anchor_rank exceeds eligible candidates or physical pair rank");
     std::vector<double> u, v;
-    sketch_factors(d, ell, o.seed, u, v);
+    {
+        ISDF_PROFILE("phase:sketch_factors", s);
+        sketch_factors(d, ell, o.seed, u, v);
+    }
     const int64_t ldy = n;
     DeviceBuffer<double> Yt(static_cast<size_t>(ell * n), s);
     const double* aw = o.axis_weights.empty() ? nullptr : o.axis_weights.data();
@@ -375,6 +391,7 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
     if (o.precision == 1 && project_tc_supported(ax.naxes, static_cast<int>(2 * ell)) && ell <= 64 &&
         c.nao <= kMaxVerifiedNao) {
         MixedSketch ms = sketch_mixed(c, pts, kp, w, ax, aw, ell, u, v, Yt.get(), ldy, s);
+        ISDF_PROFILE("phase:qrcp", s);
         qr = qrcp_sketch(Yt.get(), ldy, ell, n, s, &ms.source);
     } else {
         const int64_t chunk = std::max<int64_t>(1024, std::min<int64_t>(n, (int64_t(1) << 28) / d));
@@ -404,16 +421,15 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
     if (!o.max_rank)
         for (int64_t i = 0; i <= cap; ++i)
             if (tails[i] <= o.tolerance * norm) { rank = i; break; }
-    std::vector<int64_t> kept_host(n);
-    ISDF_CUDA(cudaMemcpyAsync(kept_host.data(), kp.index.get(), n * sizeof(int64_t),
-                              cudaMemcpyDeviceToHost, s));
-    ISDF_CUDA(cudaStreamSynchronize(s));
-    std::vector<int64_t> selected;
+    // original grid ids of the pivots (a gather of `rank` entries of the kept index)
+    std::vector<int64_t> selected(rank);
     for (int64_t i = 0; i < rank; ++i) {
         const int64_t pv = qr.jpvt[i];
         if (pv < 0 || pv >= n) fail(kRuntime, "randomized ID QRCP returned invalid pivot");
-        selected.push_back(kept_host[pv]);
+        ISDF_CUDA(cudaMemcpyAsync(&selected[i], kp.index.get() + pv, sizeof(int64_t),
+                                  cudaMemcpyDeviceToHost, s));
     }
+    ISDF_CUDA(cudaStreamSynchronize(s));
     if (diag_out) {
         diag_out->ell = ell;
         diag_out->numerical_rank = numerical_rank;
