@@ -71,14 +71,13 @@ struct SphPoly {
 };
 
 // `sink.put<C>(ao, v)` receives component C (0 value, 1..3 d/dx, d/dy, d/dz)
-// of AO index `ao` for the contractions [ctr0, ctr1) of shell b.
+// of AO index `ao` for the contractions [ctr0, ctr1) of shell b, given the
+// offset (x, y, z) from the shell centre and r2 = |offset|^2.
 template <class T, int L, bool GRAD, class Sink>
-__device__ __forceinline__ void eval_shell_t(const ShellDesc& b, double dxd, double dyd, double dzd,
-                                             const T* __restrict__ exps, const T* __restrict__ coefs,
-                                             Sink& sink, int ctr0 = 0, int ctr1 = 1 << 30) {
+__device__ __forceinline__ void eval_shell_core(const ShellDesc& b, T x, T y, T z, T r2,
+                                                const T* __restrict__ exps, const T* __restrict__ coefs,
+                                                Sink& sink, int ctr0, int ctr1) {
     constexpr int NS = 2 * L + 1;
-    const T x = static_cast<T>(dxd), y = static_cast<T>(dyd), z = static_cast<T>(dzd);
-    const T r2 = static_cast<T>(dxd * dxd + dyd * dyd + dzd * dzd);
     const SphPoly<T, L, GRAD> poly(x, y, z);
     const int cend = min(b.nctr, ctr1);
     for (int g0 = ctr0; g0 < cend; g0 += kMaxCtrGroup) {
@@ -118,20 +117,29 @@ __device__ __forceinline__ void eval_shell_t(const ShellDesc& b, double dxd, dou
 }
 
 // Runtime dispatch on l up to LMAX (at least the context's largest angular
-// momentum; shells above LMAX are not evaluated).
+// momentum; shells above LMAX are not evaluated), offset and r2 in T.
+template <class T, bool GRAD, int LMAX = kMaxL, class Sink>
+__device__ __forceinline__ void eval_shell_rel(const ShellDesc& b, T x, T y, T z, T r2, const T* exps,
+                                               const T* coefs, Sink& sink, int ctr0 = 0,
+                                               int ctr1 = 1 << 30) {
+    switch (b.l) {
+    case 0: eval_shell_core<T, 0, GRAD>(b, x, y, z, r2, exps, coefs, sink, ctr0, ctr1); break;
+    case 1: if constexpr (LMAX >= 1) eval_shell_core<T, 1, GRAD>(b, x, y, z, r2, exps, coefs, sink, ctr0, ctr1); break;
+    case 2: if constexpr (LMAX >= 2) eval_shell_core<T, 2, GRAD>(b, x, y, z, r2, exps, coefs, sink, ctr0, ctr1); break;
+    case 3: if constexpr (LMAX >= 3) eval_shell_core<T, 3, GRAD>(b, x, y, z, r2, exps, coefs, sink, ctr0, ctr1); break;
+    case 4: if constexpr (LMAX >= 4) eval_shell_core<T, 4, GRAD>(b, x, y, z, r2, exps, coefs, sink, ctr0, ctr1); break;
+    case 5: if constexpr (LMAX >= 5) eval_shell_core<T, 5, GRAD>(b, x, y, z, r2, exps, coefs, sink, ctr0, ctr1); break;
+    default: if constexpr (LMAX >= 6) eval_shell_core<T, 6, GRAD>(b, x, y, z, r2, exps, coefs, sink, ctr0, ctr1); break;
+    }
+}
+
+// Same, from FP64 offsets: r2 is formed in FP64 and rounded once to T.
 template <class T, bool GRAD, int LMAX = kMaxL, class Sink>
 __device__ __forceinline__ void eval_shell_any(const ShellDesc& b, double dx, double dy, double dz,
                                                const T* exps, const T* coefs, Sink& sink,
                                                int ctr0 = 0, int ctr1 = 1 << 30) {
-    switch (b.l) {
-    case 0: eval_shell_t<T, 0, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
-    case 1: if constexpr (LMAX >= 1) eval_shell_t<T, 1, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
-    case 2: if constexpr (LMAX >= 2) eval_shell_t<T, 2, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
-    case 3: if constexpr (LMAX >= 3) eval_shell_t<T, 3, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
-    case 4: if constexpr (LMAX >= 4) eval_shell_t<T, 4, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
-    case 5: if constexpr (LMAX >= 5) eval_shell_t<T, 5, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
-    default: if constexpr (LMAX >= 6) eval_shell_t<T, 6, GRAD>(b, dx, dy, dz, exps, coefs, sink, ctr0, ctr1); break;
-    }
+    eval_shell_rel<T, GRAD, LMAX>(b, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
+                                  static_cast<T>(dx * dx + dy * dy + dz * dz), exps, coefs, sink, ctr0, ctr1);
 }
 
 }  // namespace isdf

@@ -472,13 +472,16 @@ int isdf_project_axes(isdf_ctx* ctx, const double* xyz, int64_t ng, const int32_
         if (precision == ISDF_MIXED) {
             if (!isdf::project_tc_supported(naxes, nout))
                 isdf::fail(isdf::kNotImplemented, "tensor-core projection needs naxes <= 4 and nout <= 64");
-            std::vector<double> hw(W, W + d * nout);
             std::vector<int> comps(ax.comp, ax.comp + naxes);
-            isdf::ProjectPlan plan = isdf::make_project_plan(c, comps, hw, nout, s);
+            isdf::DeviceBuffer<double> dW(static_cast<size_t>(d * nout), s);
+            ISDF_CUDA(cudaMemcpyAsync(dW.get(), W, d * nout * sizeof(double), cudaMemcpyHostToDevice, s));
+            // W row-major [a*nao + mu][j]
+            const isdf::WSource src{dW.get(), static_cast<int64_t>(c.nao) * nout, nout, 1, nout, 0};
+            isdf::ProjectPlan plan = isdf::make_project_plan(c, comps, nout, &src, 1, s);
             isdf::DeviceBuffer<float> P(static_cast<size_t>(ng * naxes * nout), s);
             isdf::DeviceBuffer<int> err(1, s);
             err.zero(s);
-            isdf::project_tc(c, plan, xyz, nullptr, ng, nullptr, P.get(), naxes * nout, nullptr,
+            isdf::project_tc(c, plan, xyz, nullptr, ng, nullptr, P.get(), naxes * nout, 1, nullptr,
                              nullptr, err.get(), s);
             isdf::widen_f32(P.get(), ng * naxes * nout, out, s);
             int herr = 0;

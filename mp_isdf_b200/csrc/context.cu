@@ -26,6 +26,12 @@ Context::~Context() {
     cudaFree(d_expf);
     cudaFree(d_coeff);
     cudaFree(d_ao_atom);
+    cudaFree(d_pieces);
+    cudaFree(d_shell_hi);
+    cudaFree(d_shell_lo);
+    cudaFree(d_piece_begin);
+    cudaFree(d_fill);
+    cudaFree(d_ao_slot);
 }
 
 Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nbas,
@@ -33,6 +39,15 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
     require(natm >= 0 && nbas >= 0 && nenv >= 20, "invalid libcint ATM/BAS/ENV table sizes");
     auto c = std::make_unique<Context>();
     ISDF_CUDA(cudaGetDevice(&c->device));
+    {
+        // Scratch buffers come from this process's default stream-ordered pool;
+        // keep freed blocks cached across calls instead of returning them to
+        // the driver at every synchronisation (the pool's default).
+        cudaMemPool_t pool;
+        ISDF_CUDA(cudaDeviceGetDefaultMemPool(&pool, c->device));
+        uint64_t keep = std::numeric_limits<uint64_t>::max();
+        ISDF_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     c->natm = natm;
     c->atm.assign(atm, atm + static_cast<size_t>(natm) * 6);
     c->bas.assign(bas, bas + static_cast<size_t>(nbas) * 8);
@@ -88,6 +103,18 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
     up(c->d_expf, expf_);
     up(c->d_coeff, coeff_);
     up(c->d_ao_atom, c->ao_atom);
+    {
+        std::vector<float4> hi, lo;
+        for (const auto& sh : c->shells) {
+            const float xh = static_cast<float>(sh.x), yh = static_cast<float>(sh.y), zh = static_cast<float>(sh.z);
+            hi.push_back(make_float4(xh, yh, zh, sh.amin));
+            lo.push_back(make_float4(static_cast<float>(sh.x - xh), static_cast<float>(sh.y - yh),
+                                     static_cast<float>(sh.z - zh), 0.f));
+        }
+        up(c->d_shell_hi, hi);
+        up(c->d_shell_lo, lo);
+    }
+    build_chunk_layout(*c);
     return c.release();
 }
 

@@ -435,15 +435,12 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
     const int64_t n = kp.n, k = f.k, nao = c.nao;
     out.theta_w.assign(k, 0.0);
     if (n == 0 || k == 0) return out;
-    std::vector<double> phi(static_cast<size_t>(k * nao)), W(static_cast<size_t>(k * nao));
-    ISDF_CUDA(cudaMemcpyAsync(phi.data(), f.phi_a.get(), phi.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-    ISDF_CUDA(cudaStreamSynchronize(s));
-    for (int64_t a = 0; a < k; ++a)
-        for (int64_t mu = 0; mu < nao; ++mu) W[mu * k + a] = phi[a * nao + mu];
     ProjectPlan plan;
     {
         ISDF_PROFILE("phase:fit_plan", s);
-        plan = make_project_plan(c, {0}, W, static_cast<int>(k), s);
+        // W[mu][a] = phi_a[a*nao + mu]
+        const WSource src{f.phi_a.get(), 0, 1, nao, static_cast<int>(k), 0};
+        plan = make_project_plan(c, {0}, static_cast<int>(k), &src, 1, s);
     }
     DeviceBuffer<float> G(static_cast<size_t>(n * k), s), psq(static_cast<size_t>(n * 4), s);
     DeviceBuffer<int> err(1, s);
@@ -455,7 +452,7 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
     row_norms_kernel<<<static_cast<unsigned>(k), 32, 0, s>>>(f.phi_a.get(), static_cast<int>(k),
                                                             static_cast<int>(nao), anorm.get());
     ISDF_LAUNCH_CHECK();
-    project_tc(c, plan, pts, kp.index.get(), n, nullptr, G.get(), k, nullptr, psq.get(), err.get(), s);
+    project_tc(c, plan, pts, kp.index.get(), n, nullptr, G.get(), k, 1, nullptr, psq.get(), err.get(), s);
     {
         ISDF_PROFILE("fit_mixed", s);
         const size_t smem = static_cast<size_t>(2 * k * k + k) * sizeof(double);

@@ -125,8 +125,22 @@ struct Context {
     float* d_expf = nullptr;
     float* d_coeff = nullptr;
     int32_t* d_ao_atom = nullptr;
+    // shell centres as FP32 hi + lo pairs (x = hi + lo to ~2^-48 relative) and
+    // the smallest exponent: (x_hi, y_hi, z_hi, amin), (x_lo, y_lo, z_lo, 0)
+    float4* d_shell_hi = nullptr;
+    float4* d_shell_lo = nullptr;
+    // K-chunk layout of the tensor-core projection (built with the context):
+    // chunks of 32 AO slots holding whole contraction groups ("pieces").
+    int nchunks = 0;
+    int4* d_pieces = nullptr;             // (shell, first contraction, contractions, first slot)
+    int* d_piece_begin = nullptr;         // nchunks + 1
+    int* d_fill = nullptr;                // used slots per chunk
+    int2* d_ao_slot = nullptr;            // (chunk, slot) of each AO
     ~Context();
 };
+
+// Fills the context's K-chunk layout (defined with the projection kernel).
+void build_chunk_layout(Context& c);
 
 Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nbas,
                         const double* env, int64_t nenv);

@@ -7,6 +7,8 @@ namespace isdf {
 
 struct ProjectArgs {
     const ShellDesc* shells;
+    const float4* shell_hi;    // (x_hi, y_hi, z_hi, amin) per shell
+    const float4* shell_lo;    // (x_lo, y_lo, z_lo, 0) per shell
     const float* expf_;
     const float* coeff_;
     float* point_sq;           // [n][4] per-point sums of squares per component, or null
@@ -22,8 +24,8 @@ struct ProjectArgs {
     const uint8_t* wimg;       // per chunk: nax x (hi, lo) BF16 tiles
     int comp_mask;
     int axis_comp[4];
-    float* out;                // out[g*ld_out + a*nout + j]
-    int64_t ld_out;
+    float* out;                // out[g*ld_out + (a*nout + j)*col_stride]
+    int64_t ld_out, col_stride;
     int nout;
     double* sumsq;             // [4] or null
     int* error;                // bit flags of bounded waits that gave up
@@ -34,16 +36,23 @@ struct ProjectPlan {
     int axis_comp[4] = {0, 0, 0, 0};
     bool grad = false;
     DeviceBuffer<uint16_t> wimg;
-    DeviceBuffer<int4> pieces;
-    DeviceBuffer<int> piece_begin, fill;
 };
 
-// W is row-major [nax*nao][nout] in FP64; it is split into BF16 hi + lo.
-ProjectPlan make_project_plan(const Context& c, const std::vector<int>& axis_comp,
-                              const std::vector<double>& W, int nout, cudaStream_t s);
+// Device FP64 weights feeding output columns [col0, col0 + ncols) of the
+// projection: W_a[mu][col0 + j] = p[a*s_axis + mu*s_ao + j*s_col].
+struct WSource {
+    const double* p;
+    int64_t s_axis, s_ao, s_col;
+    int ncols, col0;
+};
+
+// Builds the BF16 hi + lo weight image on the device from the sources.
+ProjectPlan make_project_plan(const Context& c, const std::vector<int>& axis_comp, int nout,
+                              const WSource* src, int nsrc, cudaStream_t s);
 bool project_tc_supported(int nax, int nout);
 void project_tc(const Context& c, const ProjectPlan& plan, const double* pts, const int64_t* index,
-                int64_t n, const double* weights, float* out, int64_t ld_out, double* sumsq,
+                int64_t n, const double* weights, float* out, int64_t ld_out, int64_t col_stride,
+                double* sumsq,
                 float* point_sq, int* error, cudaStream_t s);
 
 }  // namespace isdf

@@ -31,6 +31,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
+#include <vector>
 
 namespace isdf {
 
@@ -55,25 +57,24 @@ struct StageSink {
     }
 };
 
-__device__ __forceinline__ uint32_t pack_bf16(float lo_elem, float hi_elem) {
-    const uint32_t a = __bfloat16_as_ushort(__float2bfloat16_rn(lo_elem));
-    const uint32_t b = __bfloat16_as_ushort(__float2bfloat16_rn(hi_elem));
-    return a | (b << 16);
+__device__ __forceinline__ uint32_t bf162_bits(__nv_bfloat162 v) {
+    uint32_t u;
+    memcpy(&u, &v, sizeof(u));
+    return u;
 }
 
-// hi = bf16(x), lo = bf16(x - hi) for 8 values, packed for two 16-byte stores.
+// hi = bf16(x), lo = bf16(x - hi) (round to nearest) for 8 values, packed for
+// two 16-byte stores; pairs are converted with one packed instruction each.
 __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
-    float h[8], l[8];
+    uint32_t h[4], l[4];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const __nv_bfloat16 hb = __float2bfloat16_rn(x[i]);
-        h[i] = __bfloat162float(hb);
-        l[i] = x[i] - h[i];
+    for (int i = 0; i < 4; ++i) {
+        h[i] = bf162_bits(__floats2bfloat162_rn(x[2 * i], x[2 * i + 1]));
+        const float h0 = __uint_as_float(h[i] << 16), h1 = __uint_as_float(h[i] & 0xffff0000u);
+        l[i] = bf162_bits(__floats2bfloat162_rn(x[2 * i] - h0, x[2 * i + 1] - h1));
     }
-    hi = make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]),
-                    pack_bf16(h[6], h[7]));
-    lo = make_uint4(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]), pack_bf16(l[4], l[5]),
-                    pack_bf16(l[6], l[7]));
+    hi = make_uint4(h[0], h[1], h[2], h[3]);
+    lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
 __device__ __forceinline__ void named_bar_sync(int id, int count) {
@@ -155,11 +156,15 @@ project_tc_kernel(ProjectArgs args) {
         for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++t) {
             const int64_t g = tile * kRows + p;
             const bool valid = g < n;
-            double px = 0, py = 0, pz = 0;
+            // point as FP32 hi + lo: offsets from a shell centre are formed in FP32
+            // to about one rounding of the offset itself
+            float pxh = 0.f, pyh = 0.f, pzh = 0.f, pxl = 0.f, pyl = 0.f, pzl = 0.f;
             bool count = false;
             if (valid) {
                 const int64_t gi = args.index ? args.index[g] : g;
-                px = args.pts[3 * gi]; py = args.pts[3 * gi + 1]; pz = args.pts[3 * gi + 2];
+                const double px = args.pts[3 * gi], py = args.pts[3 * gi + 1], pz = args.pts[3 * gi + 2];
+                pxh = static_cast<float>(px); pyh = static_cast<float>(py); pzh = static_cast<float>(pz);
+                pxl = static_cast<float>(px - pxh); pyl = static_cast<float>(py - pyh); pzl = static_cast<float>(pz - pzh);
                 count = args.sumsq && (args.weights == nullptr || args.weights[gi] != 0.0);
             }
             float psq[4] = {0.f, 0.f, 0.f, 0.f};
@@ -169,15 +174,19 @@ project_tc_kernel(ProjectArgs args) {
                 for (int k = (valid ? args.chunk_fill[c] : 0) + lanegrp; k < kChunk; k += PPT)
 #pragma unroll
                     for (int cc = 0; cc < kNComp; ++cc) sStage[(cc * kChunk + k) * kRows + p] = 0.f;
-                double csq[4] = {0, 0, 0, 0};
+                float csq[4] = {0.f, 0.f, 0.f, 0.f};
                 if (valid) {
                     for (int pi = args.chunk_piece_begin[c] + lanegrp; pi < pe; pi += PPT) {
                         const int4 pc = args.pieces[pi];
+                        const float4 ch = args.shell_hi[pc.x], cl = args.shell_lo[pc.x];
                         const ShellDesc b = args.shells[pc.x];
                         const int ns = 2 * b.l + 1;
-                        const double dx = px - b.x, dy = py - b.y, dz = pz - b.z;
-                        const float r2 = static_cast<float>(dx * dx + dy * dy + dz * dz);
-                        if (b.amin * r2 > static_cast<float>(kExpCut)) {
+                        const float dx = (pxh - ch.x) + (pxl - cl.x);
+                        const float dy = (pyh - ch.y) + (pyl - cl.y);
+                        const float dz = (pzh - ch.z) + (pzl - cl.z);
+                        const float r2 = dx * dx + dy * dy + dz * dz;
+                        // the same r2 decides the screening and every primitive's cutoff
+                        if (ch.w * r2 > static_cast<float>(kExpCut)) {
                             // every primitive is cut off: the piece is exactly zero here
                             for (int k = pc.w; k < pc.w + pc.z * ns; ++k)
 #pragma unroll
@@ -185,7 +194,7 @@ project_tc_kernel(ProjectArgs args) {
                             continue;
                         }
                         StageSink sink{sStage, p, pc.w - (b.ao_off + pc.y * ns), {0.f, 0.f, 0.f, 0.f}};
-                        eval_shell_any<float, GRAD, LMAX>(b, dx, dy, dz, args.expf_, args.coeff_, sink,
+                        eval_shell_rel<float, GRAD, LMAX>(b, dx, dy, dz, r2, args.expf_, args.coeff_, sink,
                                                           pc.y, pc.y + pc.z);
 #pragma unroll
                         for (int cc = 0; cc < 4; ++cc) csq[cc] += sink.sq[cc];
@@ -194,7 +203,7 @@ project_tc_kernel(ProjectArgs args) {
 #pragma unroll
                 for (int cc = 0; cc < 4; ++cc) {
                     if (count) sq[cc] += csq[cc];
-                    psq[cc] += static_cast<float>(csq[cc]);
+                    psq[cc] += csq[cc];
                 }
                 named_bar_sync(1, kProducers);
                 // 2. wait until the MMAs of the previous chunk released the A tiles
@@ -239,10 +248,11 @@ project_tc_kernel(ProjectArgs args) {
                                           static_cast<uint32_t>(a * NT + c0), r);
                         tc::tmem_ld_wait();
                         if (gg < n) {
-                            float* out = args.out + gg * args.ld_out + a * args.nout;
+                            const int64_t cs = args.col_stride;
+                            float* out = args.out + gg * args.ld_out + (a * args.nout + c0) * cs;
 #pragma unroll
                             for (int i = 0; i < 16; ++i)
-                                if (c0 + i < args.nout) out[c0 + i] = __uint_as_float(r[i]);
+                                if (c0 + i < args.nout) out[i * cs] = __uint_as_float(r[i]);
                         }
                     }
                 }
@@ -354,29 +364,14 @@ void launch_l(const ProjectArgs& a, int lmax, int nsm, cudaStream_t s) {
 
 }  // namespace
 
-// Host-side preparation of the shell-aligned chunk plan and of the BF16 hi/lo
-// weight image.
-ProjectPlan make_project_plan(const Context& c, const std::vector<int>& axis_comp,
-                              const std::vector<double>& W, int nout, cudaStream_t s) {
-    ProjectPlan pl;
+// K-chunk layout of a basis: pieces are runs of whole contractions of one
+// shell; a chunk takes pieces in shell order until the next contraction no
+// longer fits in its 32 slots.
+void build_chunk_layout(Context& c) {
     const int nao = c.nao;
-    const int nax = static_cast<int>(axis_comp.size());
-    pl.nax = nax;
-    pl.nout = nout;
-    pl.nt = nout <= 16 ? 16 : nout <= 32 ? 32 : nout <= 64 ? 64 : 128;
-    pl.grad = false;
-    pl.comp_mask = 0;
-    for (int a = 0; a < nax; ++a) {
-        pl.axis_comp[a] = axis_comp[a];
-        pl.comp_mask |= 1 << axis_comp[a];
-        if (axis_comp[a] > 0) pl.grad = true;
-    }
-    pl.lmax = c.lmax;
-    // pieces: runs of whole contractions of one shell; a chunk takes pieces in
-    // shell order until the next contraction no longer fits in its 32 slots
     std::vector<int4> pieces;
     std::vector<int> piece_begin{0}, fill;
-    std::vector<int> chunk_of_ao(nao, -1), slot_of_ao(nao, -1);
+    std::vector<int2> ao_slot(std::max(nao, 1), make_int2(0, 0));
     int used = 0;
     auto close_chunk = [&]() {
         fill.push_back(used);
@@ -391,48 +386,82 @@ ProjectPlan make_project_plan(const Context& c, const std::vector<int>& axis_com
             if (room == 0) { close_chunk(); continue; }
             const int take = std::min(room, sh.nctr - j);
             pieces.push_back(make_int4(i, j, take, used));
-            for (int u = 0; u < take * ns; ++u) {
-                chunk_of_ao[sh.ao_off + j * ns + u] = static_cast<int>(fill.size());
-                slot_of_ao[sh.ao_off + j * ns + u] = used + u;
-            }
+            for (int u = 0; u < take * ns; ++u)
+                ao_slot[sh.ao_off + j * ns + u] = make_int2(static_cast<int>(fill.size()), used + u);
             used += take * ns;
             j += take;
         }
     }
     if (used > 0 || fill.empty()) close_chunk();
-    pl.nchunks = static_cast<int>(fill.size());
-    // W image: per chunk, per axis, (hi, lo) tiles of NT rows x 32 K in the
-    // interleaved K-major layout.  W is row-major [nax*nao][nout].
-    const uint32_t tileB = pl.nt * kChunk * 2;
+    if (pieces.empty()) pieces.push_back(make_int4(0, 0, 0, 0));
+    c.nchunks = static_cast<int>(fill.size());
+    auto up = [](auto*& dst, const auto& src) {
+        using V = std::remove_pointer_t<std::remove_reference_t<decltype(dst)>>;
+        ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&dst), src.size() * sizeof(V)));
+        ISDF_CUDA(cudaMemcpy(dst, src.data(), src.size() * sizeof(V), cudaMemcpyHostToDevice));
+    };
+    up(c.d_pieces, pieces);
+    up(c.d_piece_begin, piece_begin);
+    up(c.d_fill, fill);
+    up(c.d_ao_slot, ao_slot);
+}
+
+namespace {
+
+// One thread per (axis, AO, source column): FP64 weight -> BF16 hi + lo at the
+// AO's (chunk, slot) in the interleaved K-major B tiles of its axis.
+__global__ void w_image_kernel(WSource src, int nax, int nao, const int2* __restrict__ ao_slot,
+                               int nt, uint16_t* __restrict__ img) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t total = static_cast<int64_t>(nax) * nao * src.ncols;
+    if (i >= total) return;
+    const int j = static_cast<int>(i % src.ncols);
+    const int mu = static_cast<int>((i / src.ncols) % nao);
+    const int a = static_cast<int>(i / (static_cast<int64_t>(src.ncols) * nao));
+    const double wv = src.p[a * src.s_axis + mu * src.s_ao + j * src.s_col];
+    const __nv_bfloat16 hb = __float2bfloat16_rn(static_cast<float>(wv));
+    const __nv_bfloat16 lb = __float2bfloat16_rn(static_cast<float>(wv - static_cast<double>(__bfloat162float(hb))));
+    const uint32_t tileB = static_cast<uint32_t>(nt) * kChunk * 2;
     const size_t stage = static_cast<size_t>(nax) * 2 * tileB;
-    std::vector<uint16_t> img(stage / 2 * pl.nchunks, 0);
-    const uint32_t lbo = (pl.nt / 8) * 128;
-    for (int a = 0; a < nax; ++a)
-        for (int mu = 0; mu < nao; ++mu) {
-            const int ch = chunk_of_ao[mu], k = slot_of_ao[mu];
-            for (int nrow = 0; nrow < nout; ++nrow) {
-                const double wv = W[(static_cast<size_t>(a) * nao + mu) * nout + nrow];
-                const float f = static_cast<float>(wv);
-                const __nv_bfloat16 hb = __float2bfloat16_rn(f);
-                const float hf = __bfloat162float(hb);
-                const __nv_bfloat16 lb = __float2bfloat16_rn(static_cast<float>(wv - hf));
-                const uint32_t off = tc::interleaved_offset(nrow, k, lbo, 128);
-                const size_t base = (ch * stage + (a * 2) * tileB + off) / 2;
-                img[base] = __bfloat16_as_ushort(hb);
-                img[base + tileB / 2] = __bfloat16_as_ushort(lb);
-            }
-        }
-    pl.wimg.reset(img.size(), s);
-    ISDF_CUDA(cudaMemcpyAsync(pl.wimg.get(), img.data(), img.size() * 2, cudaMemcpyHostToDevice, s));
-    pl.pieces.reset(pieces.size(), s);
-    pl.piece_begin.reset(piece_begin.size(), s);
-    pl.fill.reset(fill.size(), s);
-    ISDF_CUDA(cudaMemcpyAsync(pl.pieces.get(), pieces.data(), pieces.size() * sizeof(int4),
-                              cudaMemcpyHostToDevice, s));
-    ISDF_CUDA(cudaMemcpyAsync(pl.piece_begin.get(), piece_begin.data(), piece_begin.size() * sizeof(int),
-                              cudaMemcpyHostToDevice, s));
-    ISDF_CUDA(cudaMemcpyAsync(pl.fill.get(), fill.data(), fill.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-    ISDF_CUDA(cudaStreamSynchronize(s));   // host images are temporaries
+    const int2 cs = ao_slot[mu];
+    const uint32_t off = tc::interleaved_offset(src.col0 + j, cs.y, (nt / 8) * 128, 128);
+    const size_t base = (cs.x * stage + (a * 2) * tileB + off) / 2;
+    img[base] = __bfloat16_as_ushort(hb);
+    img[base + tileB / 2] = __bfloat16_as_ushort(lb);
+}
+
+}  // namespace
+
+// The split BF16 weight image, built on the device: per chunk, per axis,
+// (hi, lo) tiles of NT rows x 32 K in the interleaved K-major layout.
+ProjectPlan make_project_plan(const Context& c, const std::vector<int>& axis_comp, int nout,
+                              const WSource* src, int nsrc, cudaStream_t s) {
+    ProjectPlan pl;
+    const int nax = static_cast<int>(axis_comp.size());
+    pl.nax = nax;
+    pl.nout = nout;
+    pl.nt = nout <= 16 ? 16 : nout <= 32 ? 32 : 64;
+    pl.grad = false;
+    pl.comp_mask = 0;
+    pl.lmax = c.lmax;
+    pl.nchunks = c.nchunks;
+    for (int a = 0; a < nax; ++a) {
+        pl.axis_comp[a] = axis_comp[a];
+        pl.comp_mask |= 1 << axis_comp[a];
+        if (axis_comp[a] > 0) pl.grad = true;
+    }
+    const size_t stage = static_cast<size_t>(nax) * 2 * pl.nt * kChunk * 2;
+    pl.wimg.reset(stage / 2 * pl.nchunks, s);
+    ISDF_CUDA(cudaMemsetAsync(pl.wimg.get(), 0, stage * pl.nchunks, s));
+    for (int i = 0; i < nsrc; ++i) {
+        require(src[i].col0 >= 0 && src[i].ncols >= 0 && src[i].col0 + src[i].ncols <= nout,
+                "projection weight columns out of range");
+        const int64_t total = static_cast<int64_t>(nax) * c.nao * src[i].ncols;
+        if (total == 0) continue;
+        w_image_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
+            src[i], nax, c.nao, c.d_ao_slot, pl.nt, pl.wimg.get());
+        ISDF_LAUNCH_CHECK();
+    }
     return pl;
 }
 
@@ -443,11 +472,14 @@ bool project_tc_supported(int nax, int nout) {
 }
 
 void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, const int64_t* index,
-                int64_t n, const double* weights, float* out, int64_t ld_out, double* sumsq,
+                int64_t n, const double* weights, float* out, int64_t ld_out, int64_t col_stride,
+                double* sumsq,
                 float* point_sq, int* error, cudaStream_t s) {
     if (n == 0) return;
     ProjectArgs a{};
     a.shells = c.d_shells;
+    a.shell_hi = c.d_shell_hi;
+    a.shell_lo = c.d_shell_lo;
     a.expf_ = c.d_expf;
     a.coeff_ = c.d_coeff;
     a.point_sq = point_sq;
@@ -457,14 +489,15 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     a.weights = weights;
     a.n = n;
     a.nchunks = pl.nchunks;
-    a.pieces = pl.pieces.get();
-    a.chunk_piece_begin = pl.piece_begin.get();
-    a.chunk_fill = pl.fill.get();
+    a.pieces = c.d_pieces;
+    a.chunk_piece_begin = c.d_piece_begin;
+    a.chunk_fill = c.d_fill;
     a.wimg = reinterpret_cast<const uint8_t*>(pl.wimg.get());
     a.comp_mask = pl.comp_mask;
     for (int i = 0; i < pl.nax; ++i) a.axis_comp[i] = pl.axis_comp[i];
     a.out = out;
     a.ld_out = ld_out;
+    a.col_stride = col_stride;
     a.nout = pl.nout;
     a.sumsq = sumsq;
     a.error = error;

@@ -26,6 +26,7 @@ namespace isdf {
 namespace {
 
 constexpr int kQrThreads = 256;
+constexpr int kExactBlocks = 148;   // fixed grid of the candidate re-verification
 
 struct QrState {
     double* Yt; int64_t ldy; int64_t m; int64_t n;
@@ -197,12 +198,11 @@ struct ExactArgs {
     int64_t ell;
 };
 
+// FP64 recomputation of sketch column g (block-wide; feat holds kNComp*nao
+// AO values, 2*ell projections and m sketch rows).
 template <bool GRAD, int LMAX>
-__global__ void __launch_bounds__(256)
-exact_columns_kernel(ExactArgs ea, QrState st, const int64_t* cand, int64_t j) {
+__device__ void exact_column(const ExactArgs& ea, const QrState& st, int64_t g, int64_t j, double* feat) {
     constexpr int kNComp = GRAD ? 4 : 1;
-    extern __shared__ double feat[];   // kNComp*nao AO values, 2*ell projections, m sketch rows
-    const int64_t g = cand[blockIdx.x];
     const int64_t gi = ea.index[g];
     const int nao = ea.nao;
     const int64_t d = static_cast<int64_t>(ea.naxes) * nao;
@@ -260,7 +260,22 @@ exact_columns_kernel(ExactArgs ea, QrState st, const int64_t* cand, int64_t j) {
     }
 }
 
-using ExactKernel = void (*)(ExactArgs, QrState, const int64_t*, int64_t);
+// Re-verifies the candidates cand[0 .. *count) chosen on the device this step;
+// the grid is fixed, so the host needs no count before the launch.
+template <bool GRAD, int LMAX>
+__global__ void __launch_bounds__(256)
+exact_columns_kernel(ExactArgs ea, QrState st, const int64_t* cand, const int64_t* count, int64_t j,
+                     unsigned long long* total) {
+    extern __shared__ double feat[];
+    const int64_t nc = *count;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(total, static_cast<unsigned long long>(nc));
+    for (int64_t ci = blockIdx.x; ci < nc; ci += gridDim.x) {
+        exact_column<GRAD, LMAX>(ea, st, cand[ci], j, feat);
+        __syncthreads();   // feat is reused by the next candidate
+    }
+}
+
+using ExactKernel = void (*)(ExactArgs, QrState, const int64_t*, const int64_t*, int64_t, unsigned long long*);
 
 // Specialisation on the basis' largest angular momentum keeps the FP64
 // evaluation within registers.
@@ -320,7 +335,8 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
         ISDF_CUDA(cudaFuncSetAttribute(exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(exact_smem)));
     }
-    int64_t reverified = 0;
+    DeviceBuffer<unsigned long long> reverified_d(1, s);
+    reverified_d.zero(s);
     for (int64_t j = 0; j <= steps; ++j) {
         {
             ISDF_PROFILE("qrcp_sketch_update", s);
@@ -335,15 +351,9 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
             candidates_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(st, lb.get(), cand.get(),
                                                                                       count.get());
             ISDF_LAUNCH_CHECK();
-            int64_t hc = 0;
-            ISDF_CUDA(cudaMemcpyAsync(&hc, count.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-            ISDF_CUDA(cudaStreamSynchronize(s));
-            if (hc > 0) {
-                require(hc < (int64_t(1) << 31), "too many sketch candidates");
-                exact_kernel<<<static_cast<unsigned>(hc), 256, exact_smem, s>>>(ea, st, cand.get(), j);
-                ISDF_LAUNCH_CHECK();
-                reverified += hc;
-            }
+            exact_kernel<<<kExactBlocks, 256, exact_smem, s>>>(ea, st, cand.get(), count.get(), j,
+                                                                reverified_d.get());
+            ISDF_LAUNCH_CHECK();
             est_argmax_kernel<<<nblocks, kQrThreads, 0, s>>>(st);
             ISDF_LAUNCH_CHECK();
         }
@@ -359,8 +369,11 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
     ISDF_CUDA(cudaMemcpyAsync(out.jpvt.data(), jpvt.get(), steps * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaMemcpyAsync(out.diag.data(), diag.get(), steps * sizeof(double), cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaMemcpyAsync(out.energy.data(), energy.get(), steps * sizeof(double), cudaMemcpyDeviceToHost, s));
+    unsigned long long reverified = 0;
+    if (exact)
+        ISDF_CUDA(cudaMemcpyAsync(&reverified, reverified_d.get(), sizeof(reverified), cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaStreamSynchronize(s));
-    out.reverified = reverified;
+    out.reverified = static_cast<int64_t>(reverified);
     return out;
 }
 

@@ -242,7 +242,7 @@ __global__ void combine_mixed_kernel(const float* __restrict__ P, const float* _
     const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (g >= n) return;
     const double sw = sqrt(fabs(w[index[g]])) / sqrt(static_cast<double>(ell));
-    const float* pg = P + g * naxes * 2 * ell;
+    const float* pg = P + g;   // column-major, leading dimension n
     double f2 = 0;
     for (int a = 0; a < naxes; ++a) {
         const double sc = scales ? scales[a] : 1.0;
@@ -256,8 +256,8 @@ __global__ void combine_mixed_kernel(const float* __restrict__ P, const float* _
         double left = 0, right = 0;
         for (int a = 0; a < naxes; ++a) {
             const double sc = scales ? scales[a] : 1.0;
-            left += sc * static_cast<double>(pg[a * 2 * ell + s]);
-            right += sc * static_cast<double>(pg[a * 2 * ell + ell + s]);
+            left += sc * static_cast<double>(pg[(a * 2 * ell + s) * n]);
+            right += sc * static_cast<double>(pg[(a * 2 * ell + ell + s) * n]);
         }
         const double y = sw * left * right;
         ok = ok && isfinite(y);
@@ -267,6 +267,16 @@ __global__ void combine_mixed_kernel(const float* __restrict__ P, const float* _
     }
     delta[g] = k * sw * fn * sqrt(bound2);
     if (!ok) atomicOr(bad, 1);
+}
+
+// WT[t*d + j] = u[j*ell + t] (t < ell), v[j*ell + t - ell] (t >= ell): the
+// projection weights row-major for the FP64 re-verification.
+__global__ void factors_transpose_kernel(const double* __restrict__ u, const double* __restrict__ v,
+                                         int64_t d, int64_t ell, double* __restrict__ WT) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= d * 2 * ell) return;
+    const int64_t t = i / d, j = i % d;
+    WT[i] = t < ell ? u[j * ell + t] : v[j * ell + t - ell];
 }
 
 }  // namespace
@@ -281,19 +291,22 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     const int64_t d = static_cast<int64_t>(naxes) * nao;
     const int64_t n = kp.n;
     const int nout = static_cast<int>(2 * ell);
-    std::vector<double> hw(static_cast<size_t>(d * nout)), hwt(static_cast<size_t>(d * nout));
-    for (int64_t j = 0; j < d; ++j)
-        for (int64_t t = 0; t < ell; ++t) {
-            hw[j * nout + t] = u[j * ell + t];
-            hw[j * nout + ell + t] = v[j * ell + t];
-            hwt[t * d + j] = u[j * ell + t];
-            hwt[(ell + t) * d + j] = v[j * ell + t];
-        }
     std::vector<int> comps(ax.comp, ax.comp + naxes);
     ProjectPlan plan;
+    DeviceBuffer<double> du(static_cast<size_t>(d * ell), s), dv(static_cast<size_t>(d * ell), s);
+    ms.WT.reset(static_cast<size_t>(d * nout), s);
     {
         ISDF_PROFILE("phase:sketch_plan", s);
-        plan = make_project_plan(c, comps, hw, nout, s);
+        ISDF_CUDA(cudaMemcpyAsync(du.get(), u.data(), u.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        ISDF_CUDA(cudaMemcpyAsync(dv.get(), v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        // feature j = a*nao + mu feeds column s of u (left) and ell + s of v (right)
+        const WSource srcs[2] = {{du.get(), static_cast<int64_t>(nao) * ell, ell, 1, static_cast<int>(ell), 0},
+                                 {dv.get(), static_cast<int64_t>(nao) * ell, ell, 1, static_cast<int>(ell),
+                                  static_cast<int>(ell)}};
+        plan = make_project_plan(c, comps, nout, srcs, 2, s);
+        factors_transpose_kernel<<<static_cast<unsigned>((d * nout + 255) / 256), 256, 0, s>>>(
+            du.get(), dv.get(), d, ell, ms.WT.get());
+        ISDF_LAUNCH_CHECK();
     }
     DeviceBuffer<float> P(static_cast<size_t>(n * naxes * nout), s), psq(static_cast<size_t>(n * 4), s);
     DeviceBuffer<double> sumsq(4, s);
@@ -301,7 +314,8 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     psq.zero(s);
     sumsq.zero(s);
     err.zero(s);
-    project_tc(c, plan, pts, kp.index.get(), n, w, P.get(), naxes * nout, sumsq.get(), psq.get(),
+    // column-major projections P[a*nout + j][g] (coalesced for the combine pass)
+    project_tc(c, plan, pts, kp.index.get(), n, w, P.get(), 1, n, sumsq.get(), psq.get(),
                err.get(), s);
     double h[4] = {0, 0, 0, 0};
     int herr = 0;
@@ -312,10 +326,8 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     std::vector<double> sc(naxes, 1.0);
     if (naxes > 1) sc = axis_scales_from_sumsq(ax, h, axis_weights, n > 0);
     ms.scales.reset(naxes, s);
-    ms.WT.reset(hwt.size(), s);
     ms.delta.reset(n, s);
     ISDF_CUDA(cudaMemcpyAsync(ms.scales.get(), sc.data(), naxes * sizeof(double), cudaMemcpyHostToDevice, s));
-    ISDF_CUDA(cudaMemcpyAsync(ms.WT.get(), hwt.data(), hwt.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     ISDF_CUDA(cudaMemcpyAsync(dcomp.get(), comps.data(), naxes * sizeof(int), cudaMemcpyHostToDevice, s));
     DeviceBuffer<int> bad(1, s);
     bad.zero(s);
