@@ -136,6 +136,24 @@ def peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+def k_chunks(mol):
+    """K-chunks of 32 AO slots of the fused kernel: whole contractions of one
+    shell, packed in shell order (the library's chunk layout rule)."""
+    chunks, used = 0, 0
+    for b in mol.bas:
+        ns, nctr = 2 * int(b[1]) + 1, int(b[3])
+        j = 0
+        while j < nctr:
+            room = (32 - used) // ns
+            if room == 0:
+                chunks, used = chunks + 1, 0
+                continue
+            take = min(room, nctr - j)
+            used += take * ns
+            j += take
+    return chunks + (1 if used or not chunks else 0)
+
+
 def algorithmic(family, cfg, mol, n_kept, naxes, ell, k):
     """(bound, units per kernel family over one step, unit).  Bytes are the
     minimal HBM traffic of the family's outputs/inputs; flops are 2*M*N*K."""
@@ -156,6 +174,9 @@ def algorithmic(family, cfg, mol, n_kept, naxes, ell, k):
         return "hbm", sum(2 * (ell - j + 1) * n_kept * 8 for j in range(ell + 1)), "bytes"
     if family == "sketch_combine":
         return "hbm", n_kept * (naxes * 2 * ell + ell) * 8, "bytes"
+    if family == "gram_tiles":
+        # stored split-BF16 AO tiles read once, G written once
+        return "hbm", -(-n_kept // 128) * k_chunks(mol) * 16384 + n_kept * k * 4, "bytes"
     if family == "fit_point":
         return "hbm", n_kept * k * 8 * 4, "bytes"
     return "hbm", 0, "bytes"
@@ -240,9 +261,8 @@ def run_ours(args, rank, world, local_rank):
                     precision=precision)
 
     def step(precision):
-        piv, sinfo = ctx.select(x, wt, **sel_kw(precision))
-        finfo = ctx.fit(x, wt, piv, theta, precision=precision, want_error=False)
-        return piv, sinfo, finfo
+        # selection + fit in one library call (isdf_select_fit)
+        return ctx.select_fit(x, wt, theta, want_error=False, **sel_kw(precision))
 
     results = {}
     for precision in forms:
@@ -279,7 +299,9 @@ def run_ours(args, rank, world, local_rank):
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             total = float(t.item())
         # pair-space error of this form's Theta, evaluated with FP64 AO values (untimed)
-        einfo = ctx.fit(x, wt, piv, theta, precision=precision, want_error=True)
+        pl2, prel = ctx.pair_error(x, wt, piv, theta)
+        einfo = {"pair_l2": pl2, "pair_relative": prel, "fit_path": finfo.fit_path,
+                 "mixed_bound": finfo.mixed_bound}
         torch.cuda.synchronize()
         results[precision] = dict(total=total, times=times, prof=prof, phases=phases, clocks=clocks,
                                   piv=[int(p) for p in piv], sinfo=sinfo, einfo=einfo)
@@ -300,8 +322,7 @@ def run_ours(args, rank, world, local_rank):
         for i in range(max(1, min(3, args.steps)) + 1):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            piv_h, _ = ctx.select_host(pts_h, w_h, **sel_kw(head))
-            th, _ = ctx.fit_host(pts_h, w_h, piv_h, precision=head, want_error=False, out=th_h)
+            piv_h, th, _, _ = ctx.select_fit_host(pts_h, w_h, want_error=False, out=th_h, **sel_kw(head))
             dt = time.perf_counter() - t0
             if i:
                 e2e_times.append(dt)
@@ -309,7 +330,7 @@ def run_ours(args, rank, world, local_rank):
         d2h = th.nbytes + 8 * len(piv_h)
         e2e = {"value": statistics.mean(e2e_times) / world, "unit": "s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "isdf_select_host + isdf_fit_host (pinned host buffers, wall clock)"}
+               "path": "isdf_select_fit_host (pinned host buffers, wall clock)"}
 
     if rank != 0:
         return
@@ -318,7 +339,7 @@ def run_ours(args, rank, world, local_rank):
     tot_ms = sum(v[0] for v in res["prof"].values())
     roofline = None
     kernels = {}
-    nao_pad = -(-mol.nao // 32) * 32
+    nao_pad = k_chunks(mol) * 32   # K slots of the fused kernel
     for name, (ms, cnt) in fams:
         kernels[name] = {"ms_per_step": ms / args.steps, "launches_per_step": cnt / args.steps,
                          "share": ms / tot_ms}
@@ -334,7 +355,7 @@ def run_ours(args, rank, world, local_rank):
                         "peak_source": f"{peak_kind} bf16 dense (MEASURED_PEAKS.json)",
                         "traffic": None, "algorithmic_per_step": units,
                         "useful_flop_per_step": useful,
-                        "flop_model": "3 split-BF16 products x 2*n*(naxes*nao_pad32)*N_tile",
+                        "flop_model": "3 split-BF16 products x 2*n*(naxes*K_slots)*N_tile",
                         "per_launch_ms": ms / cnt, "launches_per_step": cnt / args.steps}
         else:
             bound, units, unit = algorithmic(name, cfg, mol, n_kept, len(names), ell, k)
@@ -354,7 +375,8 @@ def run_ours(args, rank, world, local_rank):
     for p, r in results.items():
         forms_out[p] = {"s_per_cluster": r["total"] / args.steps / world,
                         "step_times_s": r["times"], "anchors": r["piv"],
-                        "pair_relative": r["einfo"].pair_relative, "pair_l2": r["einfo"].pair_l2,
+                        "pair_relative": r["einfo"]["pair_relative"], "pair_l2": r["einfo"]["pair_l2"],
+                        "fit_path": r["einfo"]["fit_path"], "mixed_fit_bound": r["einfo"]["mixed_bound"],
                         "sketch_columns_reverified": r["sinfo"].verifications,
                         "phases_ms_per_step": {k: v[0] / args.steps for k, v in r["phases"].items()},
                         "clocks": r["clocks"]}
@@ -363,8 +385,8 @@ def run_ours(args, rank, world, local_rank):
         m, f = results["mixed"], results["fp64"]
         extra = {"speedup_mixed_vs_fp64": f["total"] / m["total"],
                  "anchors_identical": m["piv"] == f["piv"],
-                 "pair_relative_rel_diff": abs(m["einfo"].pair_relative - f["einfo"].pair_relative)
-                 / f["einfo"].pair_relative}
+                 "pair_relative_rel_diff": abs(m["einfo"]["pair_relative"] - f["einfo"]["pair_relative"])
+                 / f["einfo"]["pair_relative"]}
     line = {
         "metric": METRIC, "value": per_cluster, "unit": "s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["total"] / args.steps * 1e3,

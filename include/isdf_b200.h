@@ -151,6 +151,22 @@ int isdf_fit(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t 
 int isdf_fit_host(isdf_ctx* ctx, const double* xyz_host, const double* w_host, int64_t ng,
                   const int64_t* anchors_host, int64_t k, int32_t precision, int32_t want_error,
                   double* theta_host, isdf_fit_info* info);
+/* Anchor selection followed by the fit on the same points in one call: the
+ * path of build_isdf from selector.select to _physical_pair_refit
+ * (python/isdf.py:591-652).  Same results as isdf_select then isdf_fit with
+ * args->precision; in the mixed rand_sketch form the split-BF16 AO value
+ * tiles of the sketch pass stay in HBM and the fit contracts them instead of
+ * evaluating the AOs again (the reference likewise evaluates Phi once and
+ * hands it to the fit).  theta_dev needs capacity k * ng (k <= capacity). */
+int isdf_select_fit(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz_dev,
+                    const double* w_dev, int64_t ng, int64_t* pivots_host, int64_t capacity,
+                    int64_t* npivots, isdf_select_info* select_info, int32_t want_error,
+                    double* theta_dev, isdf_fit_info* fit_info, void* stream);
+/* Host-buffer twin; theta_host needs capacity npivots * ng. */
+int isdf_select_fit_host(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz_host,
+                         const double* w_host, int64_t ng, int64_t* pivots_host, int64_t capacity,
+                         int64_t* npivots, isdf_select_info* select_info, int32_t want_error,
+                         double* theta_host, isdf_fit_info* fit_info);
 /* Pair-space error of a given Theta (k x n_kept, leading dimension n_kept),
  * recomputed with FP64 AO values. */
 int isdf_pair_error(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t ng,

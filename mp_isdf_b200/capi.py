@@ -27,6 +27,7 @@ SYMBOLS = [
     "isdf_fit", "isdf_fit_host", "isdf_pair_error", "isdf_pair_error_terms",
     "isdf_profile_enable", "isdf_profile_read", "isdf_project_axes",
     "isdf_energy_gradient", "isdf_ctx_set_coords", "isdf_pair_error_terms_noalloc",
+    "isdf_select_fit", "isdf_select_fit_host",
 ]
 
 ALGORITHMS = {"qrcp_dense": 0, "qrcp_online": 1, "rand_sketch": 2}
@@ -84,6 +85,12 @@ def lib():
                                        ctypes.POINTER(I64), ctypes.POINTER(SelectInfo)]
         L.isdf_fit.argtypes = [P, P, P, I64, P, I64, I32, I32, P, ctypes.POINTER(FitInfo), P]
         L.isdf_fit_host.argtypes = [P, P, P, I64, P, I64, I32, I32, P, ctypes.POINTER(FitInfo)]
+        L.isdf_select_fit.argtypes = [P, ctypes.POINTER(SelectArgs), P, P, I64, P, I64,
+                                      ctypes.POINTER(I64), ctypes.POINTER(SelectInfo), I32, P,
+                                      ctypes.POINTER(FitInfo), P]
+        L.isdf_select_fit_host.argtypes = [P, ctypes.POINTER(SelectArgs), P, P, I64, P, I64,
+                                           ctypes.POINTER(I64), ctypes.POINTER(SelectInfo), I32, P,
+                                           ctypes.POINTER(FitInfo)]
         L.isdf_pair_error.argtypes = [P, P, P, I64, P, I64, P, ctypes.POINTER(F64),
                                       ctypes.POINTER(F64), P]
         L.isdf_pair_error_terms.argtypes = [I64, I64, P, P, P, P, P, P, P]
@@ -180,6 +187,22 @@ class Context:
                              ctypes.byref(info), _stream(xyz)))
         return info
 
+    def select_fit(self, xyz, w, theta, want_error=True, **kw):
+        """Selection then fit on the same device points in one call (keyword
+        arguments as select()); Theta into `theta` (capacity max_rank * ng).
+        Returns (pivots, select info, fit info)."""
+        args, keep = make_select_args(**kw)
+        ng = xyz.shape[0]
+        cap = max(1, min(ng, theta.numel() // max(ng, 1)))
+        piv = np.empty(cap, dtype=np.int64)
+        n = I64()
+        sinfo, finfo = SelectInfo(), FitInfo()
+        check(lib().isdf_select_fit(self.h, ctypes.byref(args), _ptr(xyz), _ptr(w), ng, _ptr(piv),
+                                    len(piv), ctypes.byref(n), ctypes.byref(sinfo), int(want_error),
+                                    _ptr(theta), ctypes.byref(finfo), _stream(xyz)))
+        del keep
+        return piv[:n.value].copy(), sinfo, finfo
+
     def pair_error(self, xyz, w, anchors, theta):
         a = _np(anchors, np.int64)
         l2, rel = F64(), F64()
@@ -235,6 +258,29 @@ class Context:
                                      _ptr(piv), len(piv), ctypes.byref(n), ctypes.byref(info)))
         del keep
         return piv[:n.value].copy(), info
+
+    def select_fit_host(self, xyz, w, want_error=True, out=None, **kw):
+        """Selection then fit from host buffers in one call.  Returns (pivots,
+        Theta [k, n_kept], select info, fit info); `out` may supply the float64
+        host buffer for Theta (capacity ng * ng, or max_rank * ng when max_rank
+        is given)."""
+        args, keep = make_select_args(**kw)
+        xyz = _np(xyz, np.float64).reshape(-1, 3)
+        w = _np(w, np.float64)
+        ng = len(xyz)
+        cap = max(1, kw.get("max_rank") or ng)
+        theta = out if out is not None else np.empty(max(1, cap * ng))
+        if theta.dtype != np.float64 or not theta.flags.c_contiguous or theta.size < min(cap, ng) * ng:
+            raise ValueError("out must be a contiguous float64 buffer of at least max_rank*ng entries")
+        piv = np.empty(cap, dtype=np.int64)
+        n = I64()
+        sinfo, finfo = SelectInfo(), FitInfo()
+        check(lib().isdf_select_fit_host(self.h, ctypes.byref(args), _ptr(xyz), _ptr(w), ng, _ptr(piv),
+                                         len(piv), ctypes.byref(n), ctypes.byref(sinfo), int(want_error),
+                                         _ptr(theta), ctypes.byref(finfo)))
+        del keep
+        k = n.value
+        return piv[:k].copy(), theta[:k * finfo.n_kept].reshape(k, finfo.n_kept), sinfo, finfo
 
     def fit_host(self, xyz, w, anchors, precision="fp64", want_error=True, out=None):
         """Theta (k x n_kept) from host buffers.  `out` may supply the float64

@@ -227,72 +227,82 @@ void isdf_select_args_default(isdf_select_args* a) {
     a->precision = ISDF_FP64;
 }
 
+namespace {
+
+std::vector<int64_t> select_impl(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz,
+                                 const double* w, int64_t ng, isdf_select_info* info, cudaStream_t s,
+                                 isdf::RetainedAo* keep) {
+    auto& c = ctx_of(ctx);
+    DeviceGuard dg(c.device);
+    isdf::SelectOptions o = options_of(args);
+    if (ng < 0) isdf::fail(isdf::kInvalid, "expected points[ngrid,3]");
+    const bool density = o.algorithm == ISDF_RAND_SKETCH_DENSITY || o.algorithm == ISDF_RAND_SKETCH_DENSITY_NORM;
+    if (density && (o.axes.size() != 1 || o.axes[0] != ISDF_AXIS_AO))
+        isdf::fail(isdf::kInvalid, "density Khatri-Rao sketches with non-AO axis features are NYI");
+    isdf::validate_axis_weights(o.axis_weights.empty() ? nullptr : o.axis_weights.data(),
+                                static_cast<int>(o.axes.size()));
+    std::vector<int64_t> out;
+    if (info) std::memset(info, 0, sizeof(*info));
+    switch (o.algorithm) {
+    case ISDF_QRCP_DENSE:
+    case ISDF_QRCP_ONLINE: {
+        isdf::PairQrDiagnostics d;
+        out = isdf::select_pair_qr(c, xyz, w, ng, o, s, &d);
+        if (info) {
+            info->verifications = d.verifications;
+            info->reselections = d.reselections;
+            info->relative_residual = (d.first > 0 && !d.rdiag.empty()) ? d.rdiag.back() / d.first : 0.0;
+        }
+        if (o.debug)
+            std::fprintf(stderr,
+                         "[%s qrcp] rank=%lld max_initial_norm=%.6e relative_residual=%.6e "
+                         "candidate_checks=%lld candidate_reselections=%lld exact_scans=%lld\n",
+                         o.algorithm == ISDF_QRCP_ONLINE ? "online" : "dense",
+                         static_cast<long long>(out.size()), d.first,
+                         info ? info->relative_residual : 0.0,
+                         static_cast<long long>(d.verifications),
+                         static_cast<long long>(d.reselections), static_cast<long long>(d.exact_scans));
+        break;
+    }
+    case ISDF_RAND_SKETCH_QUADRATURE: {
+        isdf::SketchDiagnostics d;
+        out = isdf::select_rand_sketch(c, xyz, w, ng, o, s, &d, keep);
+        if (info) {
+            info->sketch_rows = d.ell;
+            info->numerical_rank = d.numerical_rank;
+            info->relative_residual = d.relative_tail;
+            info->verifications = d.reverified;
+        }
+        if (o.debug)
+            std::fprintf(stderr,
+                         "[rand_sketch:quadrature] rank=%lld sketch_size=%lld oversampling=%lld "
+                         "sketch_relative_frobenius=%.6e numerical_rank=%lld rank_cap=%lld "
+                         "seed=%llu precision=%s space=device\n",
+                         static_cast<long long>(d.rank), static_cast<long long>(d.ell),
+                         static_cast<long long>(o.oversampling), d.relative_tail,
+                         static_cast<long long>(d.numerical_rank), static_cast<long long>(d.cap),
+                         static_cast<unsigned long long>(o.seed), o.precision ? "mixed" : "fp64");
+        break;
+    }
+    case ISDF_CVT:
+    case ISDF_RAND_SKETCH_DENSITY:
+    case ISDF_RAND_SKETCH_DENSITY_NORM:
+        isdf::fail(isdf::kNotImplemented,
+                   "this anchor selection algorithm is outside the B200 hot path (NYI)");
+    default:
+        isdf::fail(isdf::kInvalid, "unknown anchor selection algorithm");
+    }
+    return out;
+}
+
+}  // namespace
+
 int isdf_select(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz, const double* w,
                 int64_t ng, int64_t* pivots, int64_t capacity, int64_t* npivots,
                 isdf_select_info* info, void* stream) {
     return guarded([&] {
-        auto& c = ctx_of(ctx);
-        DeviceGuard dg(c.device);
-        isdf::SelectOptions o = options_of(args);
         if (npivots) *npivots = 0;
-        if (ng < 0) isdf::fail(isdf::kInvalid, "expected points[ngrid,3]");
-        const bool density = o.algorithm == ISDF_RAND_SKETCH_DENSITY || o.algorithm == ISDF_RAND_SKETCH_DENSITY_NORM;
-        if (density && (o.axes.size() != 1 || o.axes[0] != ISDF_AXIS_AO))
-            isdf::fail(isdf::kInvalid, "density Khatri-Rao sketches with non-AO axis features are NYI");
-        isdf::validate_axis_weights(o.axis_weights.empty() ? nullptr : o.axis_weights.data(),
-                                    static_cast<int>(o.axes.size()));
-        std::vector<int64_t> out;
-        cudaStream_t s = as_stream(stream);
-        if (info) std::memset(info, 0, sizeof(*info));
-        switch (o.algorithm) {
-        case ISDF_QRCP_DENSE:
-        case ISDF_QRCP_ONLINE: {
-            isdf::PairQrDiagnostics d;
-            out = isdf::select_pair_qr(c, xyz, w, ng, o, s, &d);
-            if (info) {
-                info->verifications = d.verifications;
-                info->reselections = d.reselections;
-                info->relative_residual = (d.first > 0 && !d.rdiag.empty()) ? d.rdiag.back() / d.first : 0.0;
-            }
-            if (o.debug)
-                std::fprintf(stderr,
-                             "[%s qrcp] rank=%lld max_initial_norm=%.6e relative_residual=%.6e "
-                             "candidate_checks=%lld candidate_reselections=%lld exact_scans=%lld\n",
-                             o.algorithm == ISDF_QRCP_ONLINE ? "online" : "dense",
-                             static_cast<long long>(out.size()), d.first,
-                             info ? info->relative_residual : 0.0,
-                             static_cast<long long>(d.verifications),
-                             static_cast<long long>(d.reselections), static_cast<long long>(d.exact_scans));
-            break;
-        }
-        case ISDF_RAND_SKETCH_QUADRATURE: {
-            isdf::SketchDiagnostics d;
-            out = isdf::select_rand_sketch(c, xyz, w, ng, o, s, &d);
-            if (info) {
-                info->sketch_rows = d.ell;
-                info->numerical_rank = d.numerical_rank;
-                info->relative_residual = d.relative_tail;
-                info->verifications = d.reverified;
-            }
-            if (o.debug)
-                std::fprintf(stderr,
-                             "[rand_sketch:quadrature] rank=%lld sketch_size=%lld oversampling=%lld "
-                             "sketch_relative_frobenius=%.6e numerical_rank=%lld rank_cap=%lld "
-                             "seed=%llu precision=%s space=device\n",
-                             static_cast<long long>(d.rank), static_cast<long long>(d.ell),
-                             static_cast<long long>(o.oversampling), d.relative_tail,
-                             static_cast<long long>(d.numerical_rank), static_cast<long long>(d.cap),
-                             static_cast<unsigned long long>(o.seed), o.precision ? "mixed" : "fp64");
-            break;
-        }
-        case ISDF_CVT:
-        case ISDF_RAND_SKETCH_DENSITY:
-        case ISDF_RAND_SKETCH_DENSITY_NORM:
-            isdf::fail(isdf::kNotImplemented,
-                       "this anchor selection algorithm is outside the B200 hot path (NYI)");
-        default:
-            isdf::fail(isdf::kInvalid, "unknown anchor selection algorithm");
-        }
+        std::vector<int64_t> out = select_impl(ctx, args, xyz, w, ng, info, as_stream(stream), nullptr);
         if (static_cast<int64_t>(out.size()) > capacity)
             isdf::fail(isdf::kInvalid, "pivot buffer is too small");
         if (!out.empty()) std::memcpy(pivots, out.data(), out.size() * sizeof(int64_t));
@@ -320,18 +330,22 @@ namespace {
 
 void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, const int64_t* anchors,
               int64_t k, int32_t precision, const double* theta_in, double* theta_out,
-              isdf_fit_info* info, double* l2, double* rel, cudaStream_t s, bool want_error = true) {
+              isdf_fit_info* info, double* l2, double* rel, cudaStream_t s, bool want_error = true,
+              const isdf::RetainedAo* ra = nullptr) {
     auto& c = ctx_of(ctx);
     DeviceGuard dg(c.device);
     if (ng < 0 || k < 0) isdf::fail(isdf::kInvalid, "sizes must be nonnegative");
     if (precision != ISDF_FP64 && precision != ISDF_MIXED)
         isdf::fail(isdf::kInvalid, "precision must be fp64 or mixed");
     ISDF_PROFILE("phase:fit", s);
-    isdf::KeptPoints kp;
-    {
+    // the kept points (and AO tiles) of a preceding mixed selection on these points
+    const bool reuse = ra && ra->valid;
+    isdf::KeptPoints kp_own;
+    if (!reuse) {
         ISDF_PROFILE("phase:compact", s);
-        kp = isdf::compact_points(xyz, w, ng, s);
+        kp_own = isdf::compact_points(xyz, w, ng, s);
     }
+    const isdf::KeptPoints& kp = reuse ? ra->kp : kp_own;
     isdf::DeviceBuffer<int64_t> didx;
     upload(didx, anchors, static_cast<size_t>(k), s);
     isdf::DeviceBuffer<double> apts(static_cast<size_t>(3 * std::max<int64_t>(k, 1)), s),
@@ -346,7 +360,8 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
     double* theta = have ? const_cast<double*>(theta_in) : theta_out;
     isdf::FitOutput o;
     if (!have && precision == ISDF_MIXED && isdf::fit_mixed_supported(k)) {
-        o = isdf::fit_grid_mixed(c, xyz, w, kp, f, theta, kp.n, s);
+        o = isdf::fit_grid_mixed(c, xyz, w, kp, f, theta, kp.n, s, reuse ? ra->tiles.get() : nullptr,
+                                 reuse ? ra->psq.get() : nullptr);
         o.path = 1;
         if (!(o.mixed_bound <= isdf::kMixedFitTolerance)) {
             // the anchors' conditioning can amplify the BF16x3 Gram error past
@@ -411,6 +426,57 @@ int isdf_fit_host(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng,
                                       cudaMemcpyDeviceToHost, s));
         ISDF_CUDA(cudaStreamSynchronize(s));
         if (info) *info = local;
+    });
+}
+
+int isdf_select_fit(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz, const double* w,
+                    int64_t ng, int64_t* pivots, int64_t capacity, int64_t* npivots,
+                    isdf_select_info* select_info, int32_t want_error, double* theta,
+                    isdf_fit_info* fit_info, void* stream) {
+    return guarded([&] {
+        if (npivots) *npivots = 0;
+        if (!args) isdf::fail(isdf::kInvalid, "selection arguments are required");
+        cudaStream_t s = as_stream(stream);
+        isdf::RetainedAo keep;
+        std::vector<int64_t> out = select_impl(ctx, args, xyz, w, ng, select_info, s, &keep);
+        if (static_cast<int64_t>(out.size()) > capacity)
+            isdf::fail(isdf::kInvalid, "pivot buffer is too small");
+        if (!out.empty()) std::memcpy(pivots, out.data(), out.size() * sizeof(int64_t));
+        if (npivots) *npivots = static_cast<int64_t>(out.size());
+        fit_impl(ctx, xyz, w, ng, out.data(), static_cast<int64_t>(out.size()), args->precision, nullptr,
+                 theta, fit_info, nullptr, nullptr, s, want_error != 0, &keep);
+    });
+}
+
+int isdf_select_fit_host(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz,
+                         const double* w, int64_t ng, int64_t* pivots, int64_t capacity,
+                         int64_t* npivots, isdf_select_info* select_info, int32_t want_error,
+                         double* theta_host, isdf_fit_info* fit_info) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        cudaStream_t s = ctx->stream;
+        if (npivots) *npivots = 0;
+        if (!args) isdf::fail(isdf::kInvalid, "selection arguments are required");
+        isdf::DeviceBuffer<double> dx, dw;
+        upload(dx, xyz, static_cast<size_t>(3 * std::max<int64_t>(ng, 0)), s);
+        upload(dw, w, static_cast<size_t>(std::max<int64_t>(ng, 0)), s);
+        isdf::RetainedAo keep;
+        std::vector<int64_t> out = select_impl(ctx, args, dx.get(), dw.get(), ng, select_info, s, &keep);
+        if (static_cast<int64_t>(out.size()) > capacity)
+            isdf::fail(isdf::kInvalid, "pivot buffer is too small");
+        if (!out.empty()) std::memcpy(pivots, out.data(), out.size() * sizeof(int64_t));
+        const int64_t np = static_cast<int64_t>(out.size());
+        isdf::DeviceBuffer<double> dt(static_cast<size_t>(std::max<int64_t>(1, np * ng)), s);
+        isdf_fit_info local{};
+        fit_impl(ctx, dx.get(), dw.get(), ng, out.data(), np, args->precision, nullptr, dt.get(), &local,
+                 nullptr, nullptr, s, want_error != 0, &keep);
+        if (theta_host && np * local.n_kept)
+            ISDF_CUDA(cudaMemcpyAsync(theta_host, dt.get(), np * local.n_kept * sizeof(double),
+                                      cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        if (npivots) *npivots = np;
+        if (fit_info) *fit_info = local;
     });
 }
 

@@ -430,7 +430,8 @@ __global__ void row_norms_kernel(const double* __restrict__ a, int rows, int col
 bool fit_mixed_supported(int64_t k) { return k >= 1 && k <= 64 && project_tc_supported(1, static_cast<int>(k)); }
 
 FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
-                         const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s) {
+                         const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s,
+                         const uint8_t* ao_tiles, const float* ao_psq) {
     FitOutput out;
     const int64_t n = kp.n, k = f.k, nao = c.nao;
     out.theta_w.assign(k, 0.0);
@@ -442,21 +443,29 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
         const WSource src{f.phi_a.get(), 0, 1, nao, static_cast<int>(k), 0};
         plan = make_project_plan(c, {0}, static_cast<int>(k), &src, 1, s);
     }
-    DeviceBuffer<float> G(static_cast<size_t>(n * k), s), psq(static_cast<size_t>(n * 4), s);
+    DeviceBuffer<float> G(static_cast<size_t>(n * k), s), psq;
     DeviceBuffer<int> err(1, s);
     DeviceBuffer<double> acc(6, s), tw(k, s), anorm(k, s);
     err.zero(s);
     acc.zero(s);
     tw.zero(s);
-    psq.zero(s);
     row_norms_kernel<<<static_cast<unsigned>(k), 32, 0, s>>>(f.phi_a.get(), static_cast<int>(k),
                                                             static_cast<int>(nao), anorm.get());
     ISDF_LAUNCH_CHECK();
-    project_tc(c, plan, pts, kp.index.get(), n, nullptr, G.get(), k, 1, nullptr, psq.get(), err.get(), s);
+    const float* point_sq = ao_psq;
+    if (ao_tiles) {
+        // AO values of these points already sit in HBM as split-BF16 tiles
+        gram_from_tiles(c, plan, ao_tiles, n, G.get(), k, err.get(), s);
+    } else {
+        psq.reset(static_cast<size_t>(n * 4), s);
+        psq.zero(s);
+        project_tc(c, plan, pts, kp.index.get(), n, nullptr, G.get(), k, 1, nullptr, psq.get(), err.get(), s);
+        point_sq = psq.get();
+    }
     {
         ISDF_PROFILE("fit_mixed", s);
         const size_t smem = static_cast<size_t>(2 * k * k + k) * sizeof(double);
-        fit_mixed_kernel<<<blocks_for(n), 256, smem, s>>>(G.get(), psq.get(), n, static_cast<int>(k),
+        fit_mixed_kernel<<<blocks_for(n), 256, smem, s>>>(G.get(), point_sq, n, static_cast<int>(k),
                                                           f.T.get(), f.M.get(), anorm.get(), f.wa.get(),
                                                           w, kp.index.get(), theta, ldt, tw.get(),
                                                           acc.get());

@@ -41,10 +41,13 @@ FitOutput fit_grid(const Context& c, const double* pts, const double* w, const K
 
 // Mixed precision: G from the fused FP32-AO / split-BF16 tensor-core projection,
 // then h, X = T h and Theta in FP64.  The pair-space error is not evaluated
-// here (see fit_grid with have_theta).
+// here (see fit_grid with have_theta).  With `ao_tiles` (the AO value tiles a
+// mixed sketch of the same kept points left in HBM) and their per-point sums
+// of squares `ao_psq`, G comes from a GEMM over the tiles instead.
 bool fit_mixed_supported(int64_t k);
 FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
-                         const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s);
+                         const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s,
+                         const uint8_t* ao_tiles = nullptr, const float* ao_psq = nullptr);
 
 void gather_points(const double* pts, const double* w, const int64_t* idx, int64_t n,
                    int64_t npts_total, double* out_pts, double* out_w, cudaStream_t s);

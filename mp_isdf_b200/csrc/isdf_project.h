@@ -29,6 +29,8 @@ struct ProjectArgs {
     int nout;
     double* sumsq;             // [4] or null
     int* error;                // bit flags of bounded waits that gave up
+    uint8_t* a_store;          // null, or [tile][chunk] (hi, lo) A tiles of axis entry store_axis
+    int store_axis;
 };
 
 struct ProjectPlan {
@@ -53,6 +55,17 @@ bool project_tc_supported(int nax, int nout);
 void project_tc(const Context& c, const ProjectPlan& plan, const double* pts, const int64_t* index,
                 int64_t n, const double* weights, float* out, int64_t ld_out, int64_t col_stride,
                 double* sumsq,
-                float* point_sq, int* error, cudaStream_t s);
+                float* point_sq, int* error, cudaStream_t s, uint8_t* a_store = nullptr,
+                int store_axis = 0);
+
+// G[g*ld_out + j] from A tiles stored by project_tc (a_store) over n points and
+// a one-axis value plan: the same split-BF16 products as project_tc.
+void gram_from_tiles(const Context& c, const ProjectPlan& pl, const uint8_t* a_tiles, int64_t n,
+                     float* out, int64_t ld_out, int* error, cudaStream_t s);
+
+// Bytes of the stored A tiles of one axis entry over n points.
+inline size_t stored_tile_bytes(const Context& c, int64_t n) {
+    return static_cast<size_t>((n + 127) / 128) * c.nchunks * 2 * 128 * 32 * 2;
+}
 
 }  // namespace isdf

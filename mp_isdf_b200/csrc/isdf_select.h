@@ -81,20 +81,33 @@ struct MixedSketch {
     DeviceBuffer<double> scales, WT, delta;
     ExactSketchSource source;
 };
-// Fills Yt with the mixed-precision sketch of the kept points and returns the
+
 // Largest basis the FP64 re-verification of sketch columns holds in shared
 // memory (four components of one point, FP64).
 constexpr int kMaxVerifiedNao = 6144;
 
+// AO data of a mixed-precision rand_sketch selection kept for the fit that
+// follows it on the same points: the split-BF16 AO value tiles of the fused
+// projection and the per-point sums of squares, over the kept points.
+struct RetainedAo {
+    KeptPoints kp;
+    DeviceBuffer<uint8_t> tiles;   // [tile][K-chunk] (hi, lo) A tiles of the AO values
+    DeviceBuffer<float> psq;       // [n][4] per-point sums of squares (component 0 = values)
+    bool valid = false;
+};
+
+// Fills Yt with the mixed-precision sketch of the kept points and returns the
 // FP64 recomputation source (scales, W^T, error bounds) for the verified QR.
+// With `keep`, the AO value tiles and sums of squares stay in `keep` when an
+// axis entry is the plain AO value and the tiles fit in free device memory.
 MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& kp, const double* w,
                          const AxisSpec& ax, const double* axis_weights, int64_t ell,
                          const std::vector<double>& u, const std::vector<double>& v, double* Yt,
-                         int64_t ldy, cudaStream_t s);
+                         int64_t ldy, cudaStream_t s, RetainedAo* keep = nullptr);
 
 std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, const double* w,
                                         int64_t ng, const SelectOptions& o, cudaStream_t s,
-                                        SketchDiagnostics* diag = nullptr);
+                                        SketchDiagnostics* diag = nullptr, RetainedAo* keep = nullptr);
 
 // qrcp_dense / qrcp_online: greedy max-residual pivoting of the weighted
 // pair columns sqrt|w_g| f_g (x) f_g, computed without materialising them.

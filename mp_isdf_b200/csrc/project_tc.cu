@@ -205,6 +205,8 @@ project_tc_kernel(ProjectArgs args) {
                     if (count) sq[cc] += csq[cc];
                     psq[cc] += csq[cc];
                 }
+                // the previous chunk's tile store must have read A before it is rewritten
+                if (args.a_store && tid == 0) tc::bulk_wait_read_all();
                 named_bar_sync(1, kProducers);
                 // 2. wait until the MMAs of the previous chunk released the A tiles
                 if (q > 0 && !tc::mbar_wait(a_empty, (q - 1) & 1)) fail_wait(0);
@@ -230,6 +232,12 @@ project_tc_kernel(ProjectArgs args) {
                 if (tid == 0) *prod_abort = *abort_flag;
                 named_bar_sync(1, kProducers);
                 if (*prod_abort) break;
+                // keep the (hi, lo) tiles of one axis entry in HBM for a later GEMM
+                if (args.a_store && tid == 0) {
+                    tc::bulk_s2g(args.a_store + (static_cast<size_t>(tile) * nchunks + c) * 2 * kTileA,
+                                 sA + args.store_axis * 2 * kTileA, 2 * kTileA);
+                    tc::bulk_commit();
+                }
             }
             // per-point sums of squares of each component (the piece lanes add up)
             if (args.point_sq && valid)
@@ -315,6 +323,7 @@ project_tc_kernel(ProjectArgs args) {
         __syncwarp();
     }
 
+    if (args.a_store && tid == 0) tc::bulk_wait_all();
     // sums of squares (FP64) over the producers
     if (args.sumsq) {
 #pragma unroll
@@ -474,7 +483,7 @@ bool project_tc_supported(int nax, int nout) {
 void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, const int64_t* index,
                 int64_t n, const double* weights, float* out, int64_t ld_out, int64_t col_stride,
                 double* sumsq,
-                float* point_sq, int* error, cudaStream_t s) {
+                float* point_sq, int* error, cudaStream_t s, uint8_t* a_store, int store_axis) {
     if (n == 0) return;
     ProjectArgs a{};
     a.shells = c.d_shells;
@@ -498,6 +507,9 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     a.out = out;
     a.ld_out = ld_out;
     a.col_stride = col_stride;
+    a.a_store = a_store;
+    a.store_axis = store_axis;
+    require(a_store == nullptr || (store_axis >= 0 && store_axis < pl.nax), "invalid stored axis entry");
     a.nout = pl.nout;
     a.sumsq = sumsq;
     a.error = error;

@@ -284,7 +284,7 @@ __global__ void factors_transpose_kernel(const double* __restrict__ u, const dou
 MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& kp, const double* w,
                          const AxisSpec& ax, const double* axis_weights, int64_t ell,
                          const std::vector<double>& u, const std::vector<double>& v, double* Yt,
-                         int64_t ldy, cudaStream_t s) {
+                         int64_t ldy, cudaStream_t s, RetainedAo* keep) {
     MixedSketch ms;
     const int nao = c.nao;
     const int naxes = ax.naxes;
@@ -314,9 +314,21 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     psq.zero(s);
     sumsq.zero(s);
     err.zero(s);
+    // the AO value tiles of the first plain-AO axis entry can stay in HBM for the fit
+    int store_axis = -1;
+    for (int a = 0; a < naxes && store_axis < 0; ++a)
+        if (comps[a] == 0) store_axis = a;
+    if (keep && store_axis >= 0) {
+        size_t free_b = 0, total_b = 0;
+        ISDF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t bytes = stored_tile_bytes(c, n);
+        if (bytes <= free_b / 2) keep->tiles.reset(bytes, s);
+        else store_axis = -1;
+    }
     // column-major projections P[a*nout + j][g] (coalesced for the combine pass)
     project_tc(c, plan, pts, kp.index.get(), n, w, P.get(), 1, n, sumsq.get(), psq.get(),
-               err.get(), s);
+               err.get(), s, keep && store_axis >= 0 ? keep->tiles.get() : nullptr,
+               std::max(store_axis, 0));
     double h[4] = {0, 0, 0, 0};
     int herr = 0;
     ISDF_CUDA(cudaMemcpyAsync(h, sumsq.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -352,6 +364,10 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     ms.source.w = w;
     ms.source.ell = ell;
     ms.source.delta = ms.delta.get();
+    if (keep && store_axis >= 0) {
+        keep->psq = std::move(psq);
+        keep->valid = true;
+    }
     return ms;
 }
 
@@ -360,7 +376,7 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
 // ------------------------------------------------------------------------------
 std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, const double* w,
                                         int64_t ng, const SelectOptions& o, cudaStream_t s,
-                                        SketchDiagnostics* diag_out) {
+                                        SketchDiagnostics* diag_out, RetainedAo* keep) {
     if (!std::isfinite(o.tolerance) || o.tolerance < 0 || o.batch_size <= 0 ||
         o.oversampling <= 0 || (!o.max_rank && o.sketch_size <= o.oversampling))
         fail(kInvalid, "invalid randomized ID grid, tolerance, batch, sketch or rank/oversampling");
@@ -402,7 +418,7 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
     // components in shared memory for the FP64 re-verification of candidates
     if (o.precision == 1 && project_tc_supported(ax.naxes, static_cast<int>(2 * ell)) && ell <= 64 &&
         c.nao <= kMaxVerifiedNao) {
-        MixedSketch ms = sketch_mixed(c, pts, kp, w, ax, aw, ell, u, v, Yt.get(), ldy, s);
+        MixedSketch ms = sketch_mixed(c, pts, kp, w, ax, aw, ell, u, v, Yt.get(), ldy, s, keep);
         ISDF_PROFILE("phase:qrcp", s);
         qr = qrcp_sketch(Yt.get(), ldy, ell, n, s, &ms.source);
     } else {
@@ -452,6 +468,7 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
         diag_out->reverified = qr.reverified;
         diag_out->tails = tails;
     }
+    if (keep && keep->valid) keep->kp = std::move(kp);
     return selected;
 }
 

@@ -144,6 +144,22 @@ __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src, uint32
         : "memory");
 }
 
+// Shared -> global bulk copy in the current bulk group (16-byte aligned, size
+// % 16 == 0); the writing threads fence their shared-memory stores to the
+// async proxy and synchronise before the issuing thread starts it.
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src_smem, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                 "r"(smem_addr(src_smem)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Wait until the committed bulk stores have finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read_all() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// Wait until the committed bulk stores have completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // Byte offset of element (row, k) of a K-major bf16 operand tile in the
 // interleaved layout with K-adjacent core matrices `lbo` apart and M-adjacent
 // ones `sbo` apart.

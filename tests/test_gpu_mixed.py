@@ -128,3 +128,58 @@ def test_mixed_dense_device_api(small_water):
     print("small water mixed fit path", info.fit_path, "bound", info.mixed_bound)
     assert info.fit_path in (1, 2)
     assert abs(info.pair_relative - info64.pair_relative) <= 1e-8 * info64.pair_relative
+
+
+@pytest.mark.parametrize("axes", [("ao",), ("ao", "dx", "dy", "dz"), ("dx", "ao"), ("dz",)])
+def test_select_fit_matches_select_then_fit(small_water, axes):
+    """isdf_select_fit (selection and fit in one call; in the mixed form the fit
+    contracts the AO value tiles the sketch left in HBM) against isdf_select
+    followed by isdf_fit on the same device points: identical anchors, the
+    same fit path, Theta and the error bound to FP32-evaluation level, and the
+    pair-space error within 1e-8 relative of the FP64 fit's."""
+    import torch
+    from mp_isdf_b200 import capi
+    mol, pts, w = small_water
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    x = torch.tensor(pts, device="cuda")
+    wt = torch.tensor(w, device="cuda")
+    kw = dict(axes=axes, max_rank=8, oversampling=16, seed=3)
+    for precision in ("mixed", "fp64"):
+        piv, _ = ctx.select(x, wt, precision=precision, **kw)
+        theta = torch.zeros(len(piv) * len(pts), dtype=torch.float64, device="cuda")
+        info = ctx.fit(x, wt, piv, theta, precision=precision, want_error=True)
+        theta2 = torch.zeros(8 * len(pts), dtype=torch.float64, device="cuda")
+        piv2, sinfo, info2 = ctx.select_fit(x, wt, theta2, want_error=True, precision=precision, **kw)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(piv2, piv)
+        assert info2.n_kept == info.n_kept and info2.fit_path == info.fit_path
+        n = len(piv) * info.n_kept
+        t1, t2 = theta[:n].cpu().numpy(), theta2[:n].cpu().numpy()
+        rel = np.abs(t1 - t2).max() / np.abs(t1).max()
+        print(axes, precision, "path", info.fit_path, "bound", info.mixed_bound, info2.mixed_bound,
+              "theta rel", rel)
+        # FP64 fits differ only by the order of atomic reductions, amplified by
+        # cond(C)^2 in the solve; mixed fits also by FP32 AO rounding
+        scale = max(1.0, info.condition) ** 2
+        assert rel <= (1e-12 * scale if info.fit_path != 1 else 1e-5 * scale), rel
+        if precision == "mixed":
+            assert abs(info2.mixed_bound - info.mixed_bound) <= 1e-3 * info.mixed_bound
+        assert abs(info2.pair_relative - info.pair_relative) <= 1e-8 * info.pair_relative
+
+
+def test_select_fit_host_buffers(small_water):
+    """Host-buffer twin of the fused call returns what the device call does."""
+    import torch
+    from mp_isdf_b200 import capi
+    mol, pts, w = small_water
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    kw = dict(axes=("ao", "dx", "dy", "dz"), max_rank=6, oversampling=10, seed=5, precision="mixed")
+    piv_h, th_h, si, fi = ctx.select_fit_host(pts, w, want_error=False, **kw)
+    x = torch.tensor(pts, device="cuda")
+    wt = torch.tensor(w, device="cuda")
+    theta = torch.zeros(6 * len(pts), dtype=torch.float64, device="cuda")
+    piv_d, _, fd = ctx.select_fit(x, wt, theta, want_error=False, **kw)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(piv_h, piv_d)
+    th_d = theta[:len(piv_d) * fd.n_kept].cpu().numpy().reshape(len(piv_d), fd.n_kept)
+    np.testing.assert_array_equal(th_h, th_d)
