@@ -363,10 +363,10 @@ void launch(const ProjectArgs& a, int nsm, cudaStream_t s) {
 }
 
 // Specialisation on the basis' largest angular momentum: small l leaves room
-// for four piece lanes (16 producer warps) within the register file.
+// for six piece lanes (24 producer warps) within the register file.
 template <int NAX, int NT, bool GRAD>
 void launch_l(const ProjectArgs& a, int lmax, int nsm, cudaStream_t s) {
-    if (lmax <= 2) launch<NAX, NT, GRAD, 2, 4>(a, nsm, s);
+    if (lmax <= 2) launch<NAX, NT, GRAD, 2, 6>(a, nsm, s);
     else if (lmax <= 4) launch<NAX, NT, GRAD, 4, 2>(a, nsm, s);
     else launch<NAX, NT, GRAD, kMaxL, 2>(a, nsm, s);
 }

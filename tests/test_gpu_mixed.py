@@ -182,4 +182,7 @@ def test_select_fit_host_buffers(small_water):
     torch.cuda.synchronize()
     np.testing.assert_array_equal(piv_h, piv_d)
     th_d = theta[:len(piv_d) * fd.n_kept].cpu().numpy().reshape(len(piv_d), fd.n_kept)
-    np.testing.assert_array_equal(th_h, th_d)
+    assert fi.fit_path == fd.fit_path and fi.n_kept == fd.n_kept
+    # equal up to the order of atomic FP64 reductions, amplified by cond(C)^2
+    rel = np.abs(th_h - th_d).max() / np.abs(th_d).max()
+    assert rel <= 1e-12 * max(1.0, fd.condition) ** 2, rel
