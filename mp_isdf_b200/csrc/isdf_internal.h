@@ -133,7 +133,8 @@ struct Context {
     // chunks of 32 AO slots holding whole contraction groups ("pieces").
     int nchunks = 0;
     int4* d_pieces = nullptr;             // (shell, first contraction, contractions, first slot)
-    int* d_piece_begin = nullptr;         // nchunks + 1
+    int piece_lanes = 0;                  // producer lanes per point the layout is balanced for
+    int* d_piece_begin = nullptr;         // lane j of chunk c: [begin[c*lanes + j], begin[c*lanes + j + 1])
     int* d_fill = nullptr;                // used slots per chunk
     int2* d_ao_slot = nullptr;            // (chunk, slot) of each AO
     ~Context();
@@ -141,6 +142,8 @@ struct Context {
 
 // Fills the context's K-chunk layout (defined with the projection kernel).
 void build_chunk_layout(Context& c);
+// Producer lanes per point of the projection kernel for a basis' largest l.
+inline int piece_lanes_for_lmax(int lmax) { return lmax <= 2 ? 6 : 2; }
 
 Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nbas,
                         const double* env, int64_t nenv);

@@ -19,7 +19,7 @@ struct ProjectArgs {
     int64_t n;
     int nchunks;
     const int4* pieces;        // (shell, first contraction, contractions, first slot in chunk)
-    const int* chunk_piece_begin;  // pieces of chunk c: [begin[c], begin[c+1])
+    const int* lane_begin;     // pieces of lane j in chunk c: [lane_begin[c*PPT+j], lane_begin[c*PPT+j+1])
     const int* chunk_fill;     // slots of chunk c in use; the rest are zero
     const uint8_t* wimg;       // per chunk: nax x (hi, lo) BF16 tiles
     int comp_mask;

@@ -170,13 +170,13 @@ project_tc_kernel(ProjectArgs args) {
             float psq[4] = {0.f, 0.f, 0.f, 0.f};
             for (int c = 0; c < nchunks; ++c, ++q) {
                 // 1. evaluate this chunk's pieces into the FP32 staging buffer
-                const int pe = args.chunk_piece_begin[c + 1];
+                const int pb = args.lane_begin[c * PPT + lanegrp], pe = args.lane_begin[c * PPT + lanegrp + 1];
                 for (int k = (valid ? args.chunk_fill[c] : 0) + lanegrp; k < kChunk; k += PPT)
 #pragma unroll
                     for (int cc = 0; cc < kNComp; ++cc) sStage[(cc * kChunk + k) * kRows + p] = 0.f;
                 float csq[4] = {0.f, 0.f, 0.f, 0.f};
                 if (valid) {
-                    for (int pi = args.chunk_piece_begin[c] + lanegrp; pi < pe; pi += PPT) {
+                    for (int pi = pb; pi < pe; ++pi) {
                         const int4 pc = args.pieces[pi];
                         const float4 ch = args.shell_hi[pc.x], cl = args.shell_lo[pc.x];
                         const ShellDesc b = args.shells[pc.x];
@@ -366,6 +366,7 @@ void launch(const ProjectArgs& a, int nsm, cudaStream_t s) {
 // for six piece lanes (24 producer warps) within the register file.
 template <int NAX, int NT, bool GRAD>
 void launch_l(const ProjectArgs& a, int lmax, int nsm, cudaStream_t s) {
+    // lane counts as in piece_lanes_for_lmax()
     if (lmax <= 2) launch<NAX, NT, GRAD, 2, 6>(a, nsm, s);
     else if (lmax <= 4) launch<NAX, NT, GRAD, 4, 2>(a, nsm, s);
     else launch<NAX, NT, GRAD, kMaxL, 2>(a, nsm, s);
@@ -378,13 +379,16 @@ void launch_l(const ProjectArgs& a, int lmax, int nsm, cudaStream_t s) {
 // longer fits in its 32 slots.
 void build_chunk_layout(Context& c) {
     const int nao = c.nao;
-    std::vector<int4> pieces;
-    std::vector<int> piece_begin{0}, fill;
+    const int lanes = piece_lanes_for_lmax(c.lmax);
+    std::vector<std::vector<int4>> chunks;     // pieces of each chunk, in shell order
+    std::vector<int> fill;
     std::vector<int2> ao_slot(std::max(nao, 1), make_int2(0, 0));
+    std::vector<int4> cur;
     int used = 0;
     auto close_chunk = [&]() {
+        chunks.push_back(cur);
         fill.push_back(used);
-        piece_begin.push_back(static_cast<int>(pieces.size()));
+        cur.clear();
         used = 0;
     };
     for (int i = 0; i < c.nshell; ++i) {
@@ -394,23 +398,49 @@ void build_chunk_layout(Context& c) {
             const int room = (kChunk - used) / ns;
             if (room == 0) { close_chunk(); continue; }
             const int take = std::min(room, sh.nctr - j);
-            pieces.push_back(make_int4(i, j, take, used));
+            cur.push_back(make_int4(i, j, take, used));
             for (int u = 0; u < take * ns; ++u)
-                ao_slot[sh.ao_off + j * ns + u] = make_int2(static_cast<int>(fill.size()), used + u);
+                ao_slot[sh.ao_off + j * ns + u] = make_int2(static_cast<int>(chunks.size()), used + u);
             used += take * ns;
             j += take;
         }
     }
-    if (used > 0 || fill.empty()) close_chunk();
+    if (used > 0 || chunks.empty()) close_chunk();
+    // balance each chunk's pieces over the producer lanes (longest first onto
+    // the least-loaded lane) with an estimate of their evaluation cost
+    auto cost = [&](const int4& p) {
+        const auto& sh = c.shells[p.x];
+        return 6 + sh.nprim * (2 + p.z) + p.z * (2 * sh.l + 1) * 3;
+    };
+    std::vector<int4> pieces;
+    std::vector<int> lane_begin;
+    for (auto& ch : chunks) {
+        std::vector<int> order(ch.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = static_cast<int>(i);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(ch[a]) > cost(ch[b]); });
+        std::vector<std::vector<int4>> per_lane(lanes);
+        std::vector<int> load(lanes, 0);
+        for (int i : order) {
+            const int l = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+            per_lane[l].push_back(ch[i]);
+            load[l] += cost(ch[i]);
+        }
+        for (int l = 0; l < lanes; ++l) {
+            lane_begin.push_back(static_cast<int>(pieces.size()));
+            pieces.insert(pieces.end(), per_lane[l].begin(), per_lane[l].end());
+        }
+    }
+    lane_begin.push_back(static_cast<int>(pieces.size()));
     if (pieces.empty()) pieces.push_back(make_int4(0, 0, 0, 0));
     c.nchunks = static_cast<int>(fill.size());
+    c.piece_lanes = lanes;
     auto up = [](auto*& dst, const auto& src) {
         using V = std::remove_pointer_t<std::remove_reference_t<decltype(dst)>>;
         ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&dst), src.size() * sizeof(V)));
         ISDF_CUDA(cudaMemcpy(dst, src.data(), src.size() * sizeof(V), cudaMemcpyHostToDevice));
     };
     up(c.d_pieces, pieces);
-    up(c.d_piece_begin, piece_begin);
+    up(c.d_piece_begin, lane_begin);
     up(c.d_fill, fill);
     up(c.d_ao_slot, ao_slot);
 }
@@ -499,7 +529,8 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     a.n = n;
     a.nchunks = pl.nchunks;
     a.pieces = c.d_pieces;
-    a.chunk_piece_begin = c.d_piece_begin;
+    a.lane_begin = c.d_piece_begin;
+    require(c.piece_lanes == piece_lanes_for_lmax(pl.lmax), "chunk layout built for other producer lanes");
     a.chunk_fill = c.d_fill;
     a.wimg = reinterpret_cast<const uint8_t*>(pl.wimg.get());
     a.comp_mask = pl.comp_mask;
