@@ -87,29 +87,47 @@ struct Roles {
     static constexpr int kThreads = kProducers + 64;
 };
 
+// Shared-memory plan of one instantiation: A tiles, 1 or 2 W stages (2 when
+// they fit), two FP32 staging buffers and the barriers.
+template <int NAX, int NT, bool GRAD>
+struct Smem {
+    static constexpr uint32_t kTileB = NT * kChunk * 2;
+    static constexpr uint32_t kABytes = NAX * 2 * kTileA;
+    static constexpr uint32_t kBStage = NAX * 2 * kTileB;
+    static constexpr int kNComp = GRAD ? 4 : 1;
+    static constexpr uint32_t kStage = kNComp * kChunk * kRows * 4;
+    static constexpr uint32_t kBarBytes = 256;
+    static constexpr uint32_t kLimit = 232448;   // opt-in shared memory per block
+    static constexpr int kBStages =
+        (kABytes + 2 * kBStage + 2 * kStage + kBarBytes + 1024 <= kLimit) ? 2 : 1;
+    static constexpr size_t kBytes = kABytes + kBStages * kBStage + 2 * kStage + kBarBytes + 1024;
+    static_assert(kABytes + kBStage + 2 * kStage + kBarBytes + 1024 <= kLimit, "shared memory plan too large");
+};
+
 template <int NAX, int NT, bool GRAD, int LMAX, int PPT>
 __global__ void __launch_bounds__(Roles<PPT>::kThreads, 1)
 project_tc_kernel(ProjectArgs args) {
+    using SM = Smem<NAX, NT, GRAD>;
     constexpr int kProducers = Roles<PPT>::kProducers;
     constexpr int kThreads = Roles<PPT>::kThreads;
+    constexpr uint32_t kTileB = SM::kTileB;
+    constexpr uint32_t kBStage = SM::kBStage;
+    constexpr int kBStages = SM::kBStages;
+    constexpr int kNComp = SM::kNComp;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    // layout: [A: NAX x (hi, lo) tiles][B: 2 stages x NAX x (hi, lo)][stage FP32][barriers]
-    constexpr uint32_t kTileB = NT * kChunk * 2;
-    constexpr uint32_t kABytes = NAX * 2 * kTileA;
-    constexpr uint32_t kBStage = NAX * 2 * kTileB;
-    constexpr int kNComp = GRAD ? 4 : 1;
+    // layout: [A: NAX x (hi, lo) tiles][B: kBStages x NAX x (hi, lo)][2 x FP32 staging][barriers]
     uint8_t* sA = smem_raw;
-    uint8_t* sB = sA + kABytes;
-    float* sStage = reinterpret_cast<float*>(sB + 2 * kBStage);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sStage + kNComp * kChunk * kRows);
+    uint8_t* sB = sA + SM::kABytes;
+    float* sStage0 = reinterpret_cast<float*>(sB + kBStages * kBStage);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(sStage0) + 2 * SM::kStage);
     uint64_t* a_full = bars + 0;
     uint64_t* a_empty = bars + 1;
-    uint64_t* b_full = bars + 2;     // [2]
-    uint64_t* b_empty = bars + 4;    // [2]
+    uint64_t* b_full = bars + 2;     // [kBStages]
+    uint64_t* b_empty = bars + 4;    // [kBStages]
     uint64_t* acc_full = bars + 6;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 7);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 8);
-    volatile int* prod_abort = reinterpret_cast<volatile int*>(bars + 9);
+    volatile int* prod_abort = reinterpret_cast<volatile int*>(bars + 9);   // [2]
     __shared__ double red[kThreads / 32][4];
 
     const int tid = threadIdx.x;
@@ -121,14 +139,16 @@ project_tc_kernel(ProjectArgs args) {
 
     if (tid == 0) {
         tc::mbar_init(a_full, kProducers);
-        tc::mbar_init(a_empty, 1);
-        tc::mbar_init(&b_full[0], 1);
-        tc::mbar_init(&b_full[1], 1);
-        tc::mbar_init(&b_empty[0], 1);
-        tc::mbar_init(&b_empty[1], 1);
+        // released by the MMAs' commit and, when tiles are stored, by the store's read
+        tc::mbar_init(a_empty, args.a_store ? 2 : 1);
+        for (int i = 0; i < kBStages; ++i) {
+            tc::mbar_init(&b_full[i], 1);
+            tc::mbar_init(&b_empty[i], 1);
+        }
         tc::mbar_init(acc_full, 1);
         *abort_flag = 0;
-        *prod_abort = 0;
+        prod_abort[0] = 0;
+        prod_abort[1] = 0;
         tc::mbar_init_fence();
     }
     if (warp == 0) tc::tmem_alloc(tmem_slot, kTmemCols);
@@ -149,11 +169,15 @@ project_tc_kernel(ProjectArgs args) {
 
     if (warp < kMmaWarp) {
         // ------------------------------ producers ------------------------------
+        // Chunk q is evaluated into staging buffer q & 1; one barrier per chunk
+        // separates evaluation from conversion, and the next chunk's evaluation
+        // (other buffer) needs no barrier against this chunk's conversion.
         const int p = tid & (kRows - 1);
         const int lanegrp = tid / kRows;     // piece lane of this thread
         uint32_t q = 0;   // chunk sequence number of this CTA
         uint32_t t = 0;   // tile sequence number of this CTA
-        for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++t) {
+        bool stop = false;
+        for (int64_t tile = blockIdx.x; tile < ntiles && !stop; tile += gridDim.x, ++t) {
             const int64_t g = tile * kRows + p;
             const bool valid = g < n;
             // point as FP32 hi + lo: offsets from a shell centre are formed in FP32
@@ -169,6 +193,7 @@ project_tc_kernel(ProjectArgs args) {
             }
             float psq[4] = {0.f, 0.f, 0.f, 0.f};
             for (int c = 0; c < nchunks; ++c, ++q) {
+                float* sStage = sStage0 + (q & 1) * (SM::kStage / 4);
                 // 1. evaluate this chunk's pieces into the FP32 staging buffer
                 const int pb = args.lane_begin[c * PPT + lanegrp], pe = args.lane_begin[c * PPT + lanegrp + 1];
                 for (int k = (valid ? args.chunk_fill[c] : 0) + lanegrp; k < kChunk; k += PPT)
@@ -205,10 +230,12 @@ project_tc_kernel(ProjectArgs args) {
                     if (count) sq[cc] += csq[cc];
                     psq[cc] += csq[cc];
                 }
-                // the previous chunk's tile store must have read A before it is rewritten
-                if (args.a_store && tid == 0) tc::bulk_wait_read_all();
+                // uniform abort decision: one producer samples the flag before the
+                // barrier (alternating slots, so a late reader sees its chunk's value)
+                if (tid == 0) prod_abort[q & 1] = *abort_flag;
                 named_bar_sync(1, kProducers);
-                // 2. wait until the MMAs of the previous chunk released the A tiles
+                if (prod_abort[q & 1]) { stop = true; break; }
+                // 2. wait until the previous chunk's MMAs (and tile store) released A
                 if (q > 0 && !tc::mbar_wait(a_empty, (q - 1) & 1)) fail_wait(0);
                 // 3. convert staging -> BF16 hi/lo A tiles (UMMA interleaved K-major)
                 for (int u = tid; u < kRows * NAX * (kChunk / 8); u += kProducers) {
@@ -228,22 +255,15 @@ project_tc_kernel(ProjectArgs args) {
                 }
                 tc::fence_proxy_async_smem();
                 tc::mbar_arrive(a_full);
-                // uniform abort decision: one producer samples the flag before the barrier
-                if (tid == 0) *prod_abort = *abort_flag;
-                named_bar_sync(1, kProducers);
-                if (*prod_abort) break;
-                // keep the (hi, lo) tiles of one axis entry in HBM for a later GEMM
-                if (args.a_store && tid == 0) {
-                    tc::bulk_s2g(args.a_store + (static_cast<size_t>(tile) * nchunks + c) * 2 * kTileA,
-                                 sA + args.store_axis * 2 * kTileA, 2 * kTileA);
-                    tc::bulk_commit();
-                }
             }
+            if (stop) break;
             // per-point sums of squares of each component (the piece lanes add up)
             if (args.point_sq && valid)
                 for (int cc = 0; cc < 4; ++cc)
                     if ((args.comp_mask >> cc) & 1) atomicAdd(&args.point_sq[g * 4 + cc], psq[cc]);
-            // 4. epilogue (warps 0-3: TMEM lane quarter = warp)
+            // 4. epilogue (warps 0-3: TMEM lane quarter = warp).  The next tile's
+            // first MMA waits for every producer's arrival, so it cannot
+            // overwrite the accumulators before they are read here.
             if (warp < 4) {
                 if (!tc::mbar_wait(acc_full, t & 1)) fail_wait(1);
                 tc::tc_fence_after();
@@ -266,9 +286,6 @@ project_tc_kernel(ProjectArgs args) {
                 }
                 tc::tc_fence_before();
             }
-            if (tid == 0) *prod_abort = *abort_flag;
-            named_bar_sync(1, kProducers);
-            if (*prod_abort) break;
         }
     } else if (warp == kMmaWarp) {
         // ------------------------------ MMA issuer ------------------------------
@@ -276,11 +293,12 @@ project_tc_kernel(ProjectArgs args) {
             constexpr uint32_t idesc = tc::idesc_bf16_f32(kRows, NT);
             constexpr uint32_t kLboB = (NT / 8) * 128;
             uint32_t q = 0;
-            for (int64_t tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x) {
+            bool ok = true;
+            for (int64_t tile = blockIdx.x; tile < ntiles && ok && !*abort_flag; tile += gridDim.x) {
                 for (int c = 0; c < nchunks; ++c, ++q) {
-                    const int s = q & 1;
-                    if (!tc::mbar_wait(&b_full[s], (q >> 1) & 1)) { fail_wait(2); break; }
-                    if (!tc::mbar_wait(a_full, q & 1)) { fail_wait(3); break; }
+                    const int s = q % kBStages;
+                    if (!tc::mbar_wait(&b_full[s], (q / kBStages) & 1)) { fail_wait(2); ok = false; break; }
+                    if (!tc::mbar_wait(a_full, q & 1)) { fail_wait(3); ok = false; break; }
                     tc::tc_fence_after();
                     for (int a = 0; a < NAX; ++a) {
                         const uint32_t d = tmem_base + static_cast<uint32_t>(a * NT);
@@ -301,9 +319,19 @@ project_tc_kernel(ProjectArgs args) {
                     }
                     tc::mma_commit(a_empty);
                     tc::mma_commit(&b_empty[s]);
+                    if (args.a_store) {
+                        // keep the (hi, lo) tiles of one axis entry in HBM for a later
+                        // GEMM; A is released once the copy has read it
+                        tc::bulk_s2g(args.a_store + (static_cast<size_t>(tile) * nchunks + c) * 2 * kTileA,
+                                     sA + args.store_axis * 2 * kTileA, 2 * kTileA);
+                        tc::bulk_commit();
+                        tc::bulk_wait_read_all();
+                        tc::mbar_arrive(a_empty);
+                    }
                 }
-                tc::mma_commit(acc_full);
+                if (ok) tc::mma_commit(acc_full);
             }
+            if (args.a_store) tc::bulk_wait_all();
         }
         __syncwarp();
     } else {
@@ -312,8 +340,9 @@ project_tc_kernel(ProjectArgs args) {
             uint32_t q = 0;
             for (int64_t tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x) {
                 for (int c = 0; c < nchunks; ++c, ++q) {
-                    const int s = q & 1;
-                    if (q >= 2 && !tc::mbar_wait(&b_empty[s], ((q >> 1) - 1) & 1)) { fail_wait(4); break; }
+                    const int s = q % kBStages;
+                    if (q >= static_cast<uint32_t>(kBStages) &&
+                        !tc::mbar_wait(&b_empty[s], ((q / kBStages) - 1) & 1)) { fail_wait(4); break; }
                     tc::mbar_arrive_expect_tx(&b_full[s], kBStage);
                     tc::bulk_g2s(sB + s * kBStage, args.wimg + static_cast<size_t>(c) * kBStage, kBStage,
                                  &b_full[s]);
@@ -323,7 +352,6 @@ project_tc_kernel(ProjectArgs args) {
         __syncwarp();
     }
 
-    if (args.a_store && tid == 0) tc::bulk_wait_all();
     // sums of squares (FP64) over the producers
     if (args.sumsq) {
 #pragma unroll
@@ -343,16 +371,9 @@ project_tc_kernel(ProjectArgs args) {
     if (warp == 0) tc::tmem_dealloc(tmem_base, kTmemCols);
 }
 
-template <int NAX, int NT, bool GRAD>
-size_t smem_bytes() {
-    constexpr uint32_t kTileB = NT * kChunk * 2;
-    constexpr int kNComp = GRAD ? 4 : 1;
-    return NAX * 2 * kTileA + 2 * NAX * 2 * kTileB + kNComp * kChunk * kRows * 4 + 256 + 1024;
-}
-
 template <int NAX, int NT, bool GRAD, int LMAX, int PPT>
 void launch(const ProjectArgs& a, int nsm, cudaStream_t s) {
-    const size_t smem = smem_bytes<NAX, NT, GRAD>();
+    const size_t smem = Smem<NAX, NT, GRAD>::kBytes;
     auto kern = project_tc_kernel<NAX, NT, GRAD, LMAX, PPT>;
     ISDF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(smem)));
