@@ -276,6 +276,7 @@ def run_ours(args, rank, world, local_rank):
         sampler = ClockSampler(local_rank)
         sampler.start()
         times = []
+        prof_all, step_phases = {}, []
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -286,9 +287,16 @@ def run_ours(args, rank, world, local_rank):
             b.record()
             torch.cuda.synchronize()
             times.append(a.elapsed_time(b) / 1e3)
+            # per-step profile (read after the timed region)
+            p = capi.profile_read()
+            step_phases.append({nm[6:]: round(v[0], 3) for nm, v in p.items() if nm.startswith("phase:")})
+            for name, (ms, cnt) in p.items():
+                acc = prof_all.setdefault(name, [0.0, 0])
+                acc[0] += ms
+                acc[1] += cnt
         clocks = sampler.stop()
         capi.profile_enable(False)
-        prof_all = capi.profile_read()
+        prof_all = {k: tuple(v) for k, v in prof_all.items()}
         # "phase:" scopes time host+device phases of the call on the stream;
         # the rest are kernel families
         prof = {k: v for k, v in prof_all.items() if not k.startswith("phase:")}
@@ -303,7 +311,8 @@ def run_ours(args, rank, world, local_rank):
         einfo = {"pair_l2": pl2, "pair_relative": prel, "fit_path": finfo.fit_path,
                  "mixed_bound": finfo.mixed_bound}
         torch.cuda.synchronize()
-        results[precision] = dict(total=total, times=times, prof=prof, phases=phases, clocks=clocks,
+        results[precision] = dict(total=total, times=times, prof=prof, phases=phases, step_phases=step_phases,
+                                  clocks=clocks,
                                   piv=[int(p) for p in piv], sinfo=sinfo, einfo=einfo)
 
     head = forms[0]
@@ -379,6 +388,7 @@ def run_ours(args, rank, world, local_rank):
                         "fit_path": r["einfo"]["fit_path"], "mixed_fit_bound": r["einfo"]["mixed_bound"],
                         "sketch_columns_reverified": r["sinfo"].verifications,
                         "phases_ms_per_step": {k: v[0] / args.steps for k, v in r["phases"].items()},
+                        "phases_ms_each_step": r["step_phases"],
                         "clocks": r["clocks"]}
     extra = {}
     if "mixed" in results and "fp64" in results:

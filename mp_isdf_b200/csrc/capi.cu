@@ -360,7 +360,7 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
     double* theta = have ? const_cast<double*>(theta_in) : theta_out;
     isdf::FitOutput o;
     if (!have && precision == ISDF_MIXED && isdf::fit_mixed_supported(k)) {
-        o = isdf::fit_grid_mixed(c, xyz, w, kp, f, theta, kp.n, s, reuse ? ra->tiles.get() : nullptr,
+        o = isdf::fit_grid_mixed(c, xyz, w, kp, f, theta, kp.n, s, reuse ? ra->tiles : nullptr,
                                  reuse ? ra->psq.get() : nullptr);
         o.path = 1;
         if (!(o.mixed_bound <= isdf::kMixedFitTolerance)) {
@@ -437,6 +437,7 @@ int isdf_select_fit(isdf_ctx* ctx, const isdf_select_args* args, const double* x
         if (npivots) *npivots = 0;
         if (!args) isdf::fail(isdf::kInvalid, "selection arguments are required");
         cudaStream_t s = as_stream(stream);
+        std::lock_guard<std::mutex> lock(ctx_of(ctx).ws_mu);   // workspace held to the end of the fit
         isdf::RetainedAo keep;
         std::vector<int64_t> out = select_impl(ctx, args, xyz, w, ng, select_info, s, &keep);
         if (static_cast<int64_t>(out.size()) > capacity)
@@ -461,6 +462,7 @@ int isdf_select_fit_host(isdf_ctx* ctx, const isdf_select_args* args, const doub
         isdf::DeviceBuffer<double> dx, dw;
         upload(dx, xyz, static_cast<size_t>(3 * std::max<int64_t>(ng, 0)), s);
         upload(dw, w, static_cast<size_t>(std::max<int64_t>(ng, 0)), s);
+        std::lock_guard<std::mutex> lock(c.ws_mu);   // workspace held to the end of the fit
         isdf::RetainedAo keep;
         std::vector<int64_t> out = select_impl(ctx, args, dx.get(), dw.get(), ng, select_info, s, &keep);
         if (static_cast<int64_t>(out.size()) > capacity)

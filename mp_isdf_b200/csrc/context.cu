@@ -32,6 +32,18 @@ Context::~Context() {
     cudaFree(d_piece_begin);
     cudaFree(d_fill);
     cudaFree(d_ao_slot);
+    cudaFree(ws);
+}
+
+uint8_t* Context::workspace(size_t bytes) const {
+    if (bytes > ws_bytes) {
+        if (ws) ISDF_CUDA(cudaFree(ws));   // waits for the device
+        ws = nullptr;
+        ws_bytes = 0;
+        ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&ws), bytes));
+        ws_bytes = bytes;
+    }
+    return ws;
 }
 
 Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nbas,

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -137,6 +138,15 @@ struct Context {
     int* d_piece_begin = nullptr;         // lane j of chunk c: [begin[c*lanes + j], begin[c*lanes + j + 1])
     int* d_fill = nullptr;                // used slots per chunk
     int2* d_ao_slot = nullptr;            // (chunk, slot) of each AO
+    // Grow-only device workspace of the fused selection + fit (the stored AO
+    // tiles and the sketch projections), kept across calls so that repeated
+    // calls allocate nothing large; a call holds ws_mu while it uses it.
+    mutable std::mutex ws_mu;
+    mutable uint8_t* ws = nullptr;
+    mutable size_t ws_bytes = 0;
+    // At least `bytes` of workspace (the caller holds ws_mu; growing waits for
+    // the device and invalidates earlier pointers).
+    uint8_t* workspace(size_t bytes) const;
     ~Context();
 };
 

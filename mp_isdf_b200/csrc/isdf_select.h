@@ -89,9 +89,11 @@ constexpr int kMaxVerifiedNao = 6144;
 // AO data of a mixed-precision rand_sketch selection kept for the fit that
 // follows it on the same points: the split-BF16 AO value tiles of the fused
 // projection and the per-point sums of squares, over the kept points.
+// The tiles and the projections live in the context's workspace: the caller
+// holds ctx.ws_mu from the selection to the end of the fit.
 struct RetainedAo {
     KeptPoints kp;
-    DeviceBuffer<uint8_t> tiles;   // [tile][K-chunk] (hi, lo) A tiles of the AO values
+    const uint8_t* tiles = nullptr;  // [tile][K-chunk] (hi, lo) A tiles of the AO values
     DeviceBuffer<float> psq;       // [n][4] per-point sums of squares (component 0 = values)
     bool valid = false;
 };

@@ -262,8 +262,8 @@ __device__ void exact_column(const ExactArgs& ea, const QrState& st, int64_t g, 
 
 // Re-verifies the candidates cand[0 .. *count) chosen on the device this step;
 // the grid is fixed, so the host needs no count before the launch.
-template <bool GRAD, int LMAX>
-__global__ void __launch_bounds__(256)
+template <bool GRAD, int LMAX, int NTHR>
+__global__ void __launch_bounds__(NTHR)
 exact_columns_kernel(ExactArgs ea, QrState st, const int64_t* cand, const int64_t* count, int64_t j,
                      unsigned long long* total) {
     extern __shared__ double feat[];
@@ -275,19 +275,24 @@ exact_columns_kernel(ExactArgs ea, QrState st, const int64_t* cand, const int64_
     }
 }
 
-using ExactKernel = void (*)(ExactArgs, QrState, const int64_t*, const int64_t*, int64_t, unsigned long long*);
+using ExactKernelFn = void (*)(ExactArgs, QrState, const int64_t*, const int64_t*, int64_t, unsigned long long*);
+struct ExactKernel {
+    ExactKernelFn fn = nullptr;
+    int threads = 0;
+};
 
 // Specialisation on the basis' largest angular momentum keeps the FP64
-// evaluation within registers.
+// evaluation within registers; small l leaves room for about one shell per
+// thread of a 1024-thread block.
 ExactKernel pick_exact_kernel(bool grad, int lmax) {
     if (grad) {
-        if (lmax <= 2) return exact_columns_kernel<true, 2>;
-        if (lmax <= 4) return exact_columns_kernel<true, 4>;
-        return exact_columns_kernel<true, kMaxL>;
+        if (lmax <= 2) return {exact_columns_kernel<true, 2, 1024>, 1024};
+        if (lmax <= 4) return {exact_columns_kernel<true, 4, 256>, 256};
+        return {exact_columns_kernel<true, kMaxL, 256>, 256};
     }
-    if (lmax <= 2) return exact_columns_kernel<false, 2>;
-    if (lmax <= 4) return exact_columns_kernel<false, 4>;
-    return exact_columns_kernel<false, kMaxL>;
+    if (lmax <= 2) return {exact_columns_kernel<false, 2, 1024>, 1024};
+    if (lmax <= 4) return {exact_columns_kernel<false, 4, 256>, 256};
+    return {exact_columns_kernel<false, kMaxL, 256>, 256};
 }
 
 }  // namespace
@@ -314,7 +319,7 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
                diag.get(), energy.get(), jpvt.get(), partial.get(), nullptr, nullptr, nullptr};
     ExactArgs ea{};
     size_t exact_smem = 0;
-    ExactKernel exact_kernel = nullptr;
+    ExactKernel exact_kernel;
     if (exact) {
         est.reset(n, s);
         lbp.reset(nblocks, s);
@@ -332,7 +337,7 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
         ea.w = exact->w; ea.ell = exact->ell;
         exact_smem = (static_cast<size_t>(ea.grad ? 4 : 1) * c.nao + 2 * exact->ell + m) * sizeof(double);
         exact_kernel = pick_exact_kernel(ea.grad != 0, c.lmax);
-        ISDF_CUDA(cudaFuncSetAttribute(exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        ISDF_CUDA(cudaFuncSetAttribute(exact_kernel.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(exact_smem)));
     }
     DeviceBuffer<unsigned long long> reverified_d(1, s);
@@ -351,7 +356,7 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
             candidates_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(st, lb.get(), cand.get(),
                                                                                       count.get());
             ISDF_LAUNCH_CHECK();
-            exact_kernel<<<kExactBlocks, 256, exact_smem, s>>>(ea, st, cand.get(), count.get(), j,
+            exact_kernel.fn<<<kExactBlocks, exact_kernel.threads, exact_smem, s>>>(ea, st, cand.get(), count.get(), j,
                                                                 reverified_d.get());
             ISDF_LAUNCH_CHECK();
             est_argmax_kernel<<<nblocks, kQrThreads, 0, s>>>(st);

@@ -308,7 +308,8 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
             du.get(), dv.get(), d, ell, ms.WT.get());
         ISDF_LAUNCH_CHECK();
     }
-    DeviceBuffer<float> P(static_cast<size_t>(n * naxes * nout), s), psq(static_cast<size_t>(n * 4), s);
+    DeviceBuffer<float> P_own, psq(static_cast<size_t>(n * 4), s);
+    float* P = nullptr;
     DeviceBuffer<double> sumsq(4, s);
     DeviceBuffer<int> err(1, s), dcomp(naxes, s);
     psq.zero(s);
@@ -318,17 +319,29 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     int store_axis = -1;
     for (int a = 0; a < naxes && store_axis < 0; ++a)
         if (comps[a] == 0) store_axis = a;
-    if (keep && store_axis >= 0) {
-        size_t free_b = 0, total_b = 0;
-        ISDF_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        const size_t bytes = stored_tile_bytes(c, n);
-        if (bytes <= free_b / 2) keep->tiles.reset(bytes, s);
-        else store_axis = -1;
+    const size_t p_bytes = (static_cast<size_t>(n) * naxes * nout * sizeof(float) + 255) / 256 * 256;
+    uint8_t* tiles = nullptr;
+    if (keep) {
+        // tiles (when they fit in free memory) and projections in the workspace
+        size_t tile_bytes = store_axis >= 0 ? stored_tile_bytes(c, n) : 0;
+        if (tile_bytes + p_bytes > c.ws_bytes && tile_bytes > 0) {
+            size_t free_b = 0, total_b = 0;
+            ISDF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            if (tile_bytes + p_bytes - c.ws_bytes > free_b / 2) {
+                tile_bytes = 0;
+                store_axis = -1;
+            }
+        }
+        uint8_t* base = c.workspace(tile_bytes + p_bytes);
+        if (store_axis >= 0) tiles = base;
+        P = reinterpret_cast<float*>(base + tile_bytes);
+    } else {
+        P_own.reset(static_cast<size_t>(n) * naxes * nout, s);
+        P = P_own.get();
     }
     // column-major projections P[a*nout + j][g] (coalesced for the combine pass)
-    project_tc(c, plan, pts, kp.index.get(), n, w, P.get(), 1, n, sumsq.get(), psq.get(),
-               err.get(), s, keep && store_axis >= 0 ? keep->tiles.get() : nullptr,
-               std::max(store_axis, 0));
+    project_tc(c, plan, pts, kp.index.get(), n, w, P, 1, n, sumsq.get(), psq.get(),
+               err.get(), s, tiles, std::max(store_axis, 0));
     double h[4] = {0, 0, 0, 0};
     int herr = 0;
     ISDF_CUDA(cudaMemcpyAsync(h, sumsq.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -346,7 +359,7 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     {
         ISDF_PROFILE("sketch_combine", s);
         combine_mixed_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(
-            P.get(), psq.get(), naxes, dcomp.get(), ell, naxes > 1 ? ms.scales.get() : nullptr, w,
+            P, psq.get(), naxes, dcomp.get(), ell, naxes > 1 ? ms.scales.get() : nullptr, w,
             kp.index.get(), n, Yt, ldy, ms.delta.get(), bad.get());
         ISDF_LAUNCH_CHECK();
     }
@@ -365,6 +378,7 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     ms.source.ell = ell;
     ms.source.delta = ms.delta.get();
     if (keep && store_axis >= 0) {
+        keep->tiles = tiles;
         keep->psq = std::move(psq);
         keep->valid = true;
     }
