@@ -62,14 +62,18 @@ def workload(cfg_key):
 
 
 def workload_desc(cfg_key, cfg, mol, pts, w, names, precision):
+    if cfg["algorithm"] == "rand_sketch":
+        algo = f"rand_sketch quadrature rank {cfg['rank']} oversampling {cfg['oversampling']}"
+    else:
+        algo = f"{cfg['algorithm']} rank {cfg['rank']}"
     return {
         "workload": f"{cfg_key} {cfg['name']}: synthetic cc-pVDZ-shaped basis ({mol.nao} AOs), "
                     f"level-{cfg['level']} stand-in grid ({len(pts)} points, "
-                    f"{int(np.count_nonzero(w))} nonzero-weight), axes {cfg['axes']}, "
-                    f"rand_sketch quadrature rank {cfg['rank']} oversampling {cfg['oversampling']}, "
+                    f"{int(np.count_nonzero(w))} nonzero-weight), axes {cfg['axes']}, {algo}, "
                     f"{precision} form",
-        "nao": mol.nao, "grid_points": int(len(pts)), "axes": cfg["axes"],
-        "anchor_rank": cfg["rank"], "sketch_rows": cfg["rank"] + cfg["oversampling"],
+        "nao": mol.nao, "grid_points": int(len(pts)), "axes": cfg["axes"], "algorithm": cfg["algorithm"],
+        "anchor_rank": cfg["rank"],
+        "sketch_rows": cfg["rank"] + cfg["oversampling"] if cfg["algorithm"] == "rand_sketch" else None,
         "precision": precision, "l2_policy": "working set >> L2 (126 MB); 256 MB L2 flush before every timed step",
     }
 
@@ -196,6 +200,23 @@ def algorithmic(family, cfg, mol, n_kept, naxes, ell, k):
 # ---------------------------------------------------------------------------
 # CPU baseline (oracle restatement, bounded sample)
 # ---------------------------------------------------------------------------
+def selection_kwargs(cfg, names, factors, precision):
+    """isdf_select arguments of a config (algorithm, axes, rank, sketch)."""
+    return dict(algorithm=cfg["algorithm"], axes=names, axis_weights=factors, max_rank=cfg["rank"],
+                oversampling=cfg.get("oversampling", 16), seed=cfg.get("sketch_seed", 7),
+                batch_size=cfg.get("online_batch", 128), precision=precision)
+
+
+def cpu_sample_size(cfg, mol, names):
+    """Sample size of the CPU restatement run and whether it fits the host:
+    dense pair QR materialises d^2 x n doubles as the reference does."""
+    if cfg["algorithm"] == "rand_sketch":
+        return 3000, True
+    d2 = (len(names) * mol.nao) ** 2
+    n = 1000
+    return n, d2 * n * 8 <= 2e9
+
+
 def cpu_sample(mol, pts, w, names, factors, cfg, n_sample=4000, seed=0):
     """Time the oracle's restatement of the same path on `n_sample` nonzero
     points, scaled to the full kept-point count: axis norms, Khatri-Rao sketch,
@@ -207,17 +228,25 @@ def cpu_sample(mol, pts, w, names, factors, cfg, n_sample=4000, seed=0):
     idx = np.sort(rng.choice(keep, size=min(n_sample, len(keep)), replace=False))
     p, ww = pts[idx], w[idx]
     ctx = O.OracleContext(mol.atm, mol.bas, mol.env)
-    ell = cfg["rank"] + cfg["oversampling"]
     t0 = time.perf_counter()
     scales = O.axis_scales(ctx, p, ww, axes, factors, exact_order=False) if len(axes) > 1 else None
-    piv = O.select_rand_sketch(ctx, p, ww, axes, max_rank=cfg["rank"],
-                               oversampling=cfg["oversampling"], seed=cfg.get("sketch_seed", 7),
-                               scales=scales)
+    if cfg["algorithm"] == "rand_sketch":
+        piv = O.select_rand_sketch(ctx, p, ww, axes, max_rank=cfg["rank"],
+                                   oversampling=cfg["oversampling"], seed=cfg.get("sketch_seed", 7),
+                                   scales=scales)
+        scale = len(keep) / len(idx)
+        how = "linear in points"
+    else:
+        # dgeqp3 of the explicit d^2 x n pair matrix, as the reference: its
+        # cost grows as n * min(d^2, n)
+        piv = O.select_qrcp_dense(ctx, p, ww, axes, max_rank=cfg["rank"], scales=scales)
+        d2 = (len(axes) * mol.nao) ** 2
+        scale = len(keep) / len(idx) * min(d2, len(keep)) / min(d2, len(idx))
+        how = "scaled by n*min(d^2, n)"
     O.gram_fit(ctx, p, ww, p[piv], ww[piv])
     dt = time.perf_counter() - t0
-    scale = len(keep) / len(idx)
     return dt * scale, O.lib().oracle_num_threads(), \
-        f"{len(idx)} of {len(keep)} nonzero-weight points (uniform random), time x{scale:.1f}"
+        f"{len(idx)} of {len(keep)} nonzero-weight points (uniform random), time x{scale:.1f} ({how})"
 
 
 # ---------------------------------------------------------------------------
@@ -229,8 +258,13 @@ def run_reference(args, rank, world):
     vals = []
     cores = 1
     sample = ""
+    n_sample, feasible = cpu_sample_size(cfg, mol, names)
+    if not feasible:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's qrcp on this config "
+                          "materialises a d^2 x n pair matrix that exceeds host memory"}), flush=True)
+        return
     for i in range(args.warmup + args.steps):
-        v, cores, sample = cpu_sample(mol, pts, w, names, factors, cfg, n_sample=3000, seed=i)
+        v, cores, sample = cpu_sample(mol, pts, w, names, factors, cfg, n_sample=n_sample, seed=i)
         if i >= args.warmup:
             vals.append(v)
     value = statistics.mean(vals)
@@ -262,14 +296,12 @@ def run_ours(args, rank, world, local_rank):
     n = len(pts)
     n_kept = int(np.count_nonzero(w))
     k = cfg["rank"]
-    ell = k + cfg["oversampling"]
+    ell = k + cfg.get("oversampling", 16)
     theta = torch.empty(k * n, dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def sel_kw(precision):
-        return dict(algorithm="rand_sketch", axes=names, axis_weights=factors, max_rank=k,
-                    oversampling=cfg["oversampling"], seed=cfg.get("sketch_seed", 7),
-                    precision=precision)
+        return selection_kwargs(cfg, names, factors, precision)
 
     def step(precision):
         # selection + fit in one library call (isdf_select_fit)
@@ -399,8 +431,13 @@ def run_ours(args, rank, world, local_rank):
     roofline = dict(rl, kernel=top, peak_source=f"{peak_kind} (MEASURED_PEAKS.json)") if rl else None
     cpu = None
     if not args.no_cpu and world == 1:
-        v, cores, sample = cpu_sample(mol, pts, w, names, factors, cfg, n_sample=3000)
-        cpu = {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": sample}
+        n_sample, feasible = cpu_sample_size(cfg, mol, names)
+        if feasible:
+            v, cores, sample = cpu_sample(mol, pts, w, names, factors, cfg, n_sample=n_sample)
+            cpu = {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": sample}
+        else:
+            cpu = {"value": None, "unit": "s", "cores": None, "kind": "port",
+                   "sample": "infeasible: the reference's explicit d^2 x n pair matrix does not fit host memory"}
     forms_out = {}
     for p, r in results.items():
         forms_out[p] = {"s_per_cluster": r["total"] / args.steps / world,

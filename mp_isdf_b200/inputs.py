@@ -292,6 +292,9 @@ CONFIGS = {
     "c2": dict(name="(H2O)16", lattice=(4, 2, 2), seed=1, level=3,
                axes="ao:1,dx:0.5,dy:0.5,dz:0.5", algorithm="rand_sketch", rank=8,
                oversampling=4, sketch_seed=2, online_batch=65536),
+    "c2o": dict(name="(H2O)16", lattice=(4, 2, 2), seed=1, level=3,
+                axes="ao:1,dx:0.5,dy:0.5,dz:0.5", algorithm="qrcp_online", rank=8,
+                online_batch=65536),
     "c3": dict(name="(H2O)32", lattice=(4, 4, 2), seed=3, level=3, axes="ao",
                algorithm="rand_sketch", rank=10, oversampling=16, sketch_seed=7),
     "c4": dict(name="(H2O)8", lattice=(2, 2, 2), seed=4, level=3, axes="ao",
