@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--precision", choices=("fp64", "mixed"), default=None)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--max-points", type=int, default=0,
                     help="keep every k-th grid point so that at most this many remain "
                          "(small cases for profiling; 0 = full grid)")
@@ -200,6 +201,35 @@ def algorithmic(family, cfg, mol, n_kept, naxes, ell, k):
 # ---------------------------------------------------------------------------
 # CPU baseline (oracle restatement, bounded sample)
 # ---------------------------------------------------------------------------
+def time_adjoint(ctx, mol, x, wt, anchors, cfg, steps=3):
+    """Nuclear gradient of E = sum_g w_g rho_ISDF(g)^2 for the config's seeded
+    density (tr(DS) = electrons, S by grid quadrature), timed with CUDA events."""
+    import torch
+    from mp_isdf_b200 import inputs
+    nao = mol.nao
+    S = torch.zeros(nao, nao, dtype=torch.float64, device=x.device)
+    for i in range(0, x.shape[0], 65536):
+        xb = x[i:i + 65536].contiguous()
+        phi = torch.empty(xb.shape[0], nao, dtype=torch.float64, device=x.device)
+        ctx.eval_ao(xb, phi)
+        S += phi.T @ (phi * wt[i:i + 65536, None])
+    dm = inputs.random_density(mol, S.cpu().numpy(), cfg["electrons"], cfg["seed"])
+    ctx.energy_gradient(x, wt, anchors, dm)
+    times = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        e, g = ctx.energy_gradient(x, wt, anchors, dm)
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b) / 1e3)
+    return {"s": statistics.mean(times), "step_times_s": times, "energy": e,
+            "grad_norm": float(np.linalg.norm(g)), "form": "FP64, fused grid pass: AO values and gradients recomputed per 128-point tile, never stored",
+            "electrons": cfg["electrons"]}
+
+
 def selection_kwargs(cfg, names, factors, precision):
     """isdf_select arguments of a config (algorithm, axes, rank, sketch)."""
     return dict(algorithm=cfg["algorithm"], axes=names, axis_weights=factors, max_rank=cfg["rank"],
@@ -384,6 +414,10 @@ def run_ours(args, rank, world, local_rank):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "path": "isdf_select_fit_host (pinned host buffers, wall clock)"}
 
+    adjoint = None
+    if cfg.get("electrons") and not args.no_adjoint:
+        adjoint = time_adjoint(ctx, mol, x, wt, results[head]["piv"], cfg)
+
     if rank != 0:
         return
     hbm, bf16, peak_kind = peaks()
@@ -464,6 +498,7 @@ def run_ours(args, rank, world, local_rank):
         | {"parallelism": f"replicas x{world}"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": res["clocks"], "kernels": kernels, "forms": forms_out, **extra,
+        "adjoint": adjoint,
     }
     print(json.dumps(line), flush=True)
 

@@ -10,8 +10,15 @@
 //   anchor terms  dE/dR_A -= sum_k sum_{mu in A} c_k,mu grad phi_mu(a_k),
 //                 c = alpha^T Phi_g + 2 y o (Phi_a D) - (W + W^T) Phi_a,
 //                 y = M^+ v, v = sum_g u_g h_g, W = 2 S o (y z^T), S = Phi_a Phi_a^T.
-// The grid is processed in chunks: AO values and gradients are recomputed per
-// chunk (never stored for the whole grid) and reduced on the fly.
+// The grid pass is one fused kernel (adjoint_grid_kernel): per tile of 128
+// points it evaluates the FP64 AO values (sweep 1: G, rho, u, alpha, E, v),
+// then values and gradients again (sweep 2) and folds both the grid terms and
+// the alpha^T Phi_g part of the anchor coefficients,
+//   sum_g phi_mu(g) sum_k alpha_gk grad phi_mu(a_k),
+// straight into per-atom sums; Phi and grad Phi never reach HBM.  Bases or
+// anchor counts beyond its limits take a chunked path (AO chunks in HBM and
+// GEMMs).
+#include "ao_device.cuh"
 #include "isdf_adjoint.h"
 #include "isdf_reduce.cuh"
 
@@ -138,6 +145,175 @@ __global__ void matvec_kernel(int k, const double* __restrict__ T, const double*
     y[a] = s;
 }
 
+// ---- fused grid pass -----------------------------------------------------------
+constexpr int kAdjPts = 128;      // points per tile
+constexpr int kAdjLanes = 2;      // shell lanes per point
+constexpr int kAdjMaxAtoms = 1024;
+
+struct AdjGridArgs {
+    const ShellDesc* shells;
+    int nshell, nao, natm;
+    const double* exps;
+    const double* coefs;
+    const double* pts;
+    const double* w;
+    const int64_t* index;      // kept points
+    int64_t n;
+    const double* phia;        // [KMAX][nao], rows >= k zero
+    const double* dphia;       // [3][KMAX][nao], rows >= k zero
+    const double* z;           // [KMAX], zero padded
+    double* gacc;              // [natm][3] += sum_g sum_{mu in atom} (beta grad phi + phi t)
+    double* v;                 // [KMAX] += sum_g u_g G_gk^2
+    double* energy;            // += sum_g w_g rho_g^2
+};
+
+// sweep 1: G[a] += phi_mu(g) Phi_a[a][mu]
+template <int KMAX>
+struct GramSink {
+    const double* phia;
+    int nao;
+    double G[KMAX];
+    template <int C>
+    __device__ __forceinline__ void put(int ao, double v) {
+        if constexpr (C == 0) {
+#pragma unroll
+            for (int a = 0; a < KMAX; ++a) G[a] += v * __ldg(phia + a * nao + ao);
+        }
+    }
+};
+
+// sweep 2: per AO, beta = alpha . Phi_a[:, mu] and t = alpha . grad phi_mu(a_:);
+// acc += beta grad phi_mu(g) + phi_mu(g) t
+template <int KMAX>
+struct GradSink {
+    const double* phia;
+    const double* dphia;
+    int nao;
+    double al[KMAX];
+    double beta, acc[3];
+    template <int C>
+    __device__ __forceinline__ void put(int ao, double v) {
+        if constexpr (C == 0) {
+            double b = 0, t0 = 0, t1 = 0, t2 = 0;
+#pragma unroll
+            for (int a = 0; a < KMAX; ++a) {
+                b += al[a] * __ldg(phia + a * nao + ao);
+                t0 += al[a] * __ldg(dphia + (0 * KMAX + a) * nao + ao);
+                t1 += al[a] * __ldg(dphia + (1 * KMAX + a) * nao + ao);
+                t2 += al[a] * __ldg(dphia + (2 * KMAX + a) * nao + ao);
+            }
+            beta = b;
+            acc[0] += v * t0;
+            acc[1] += v * t1;
+            acc[2] += v * t2;
+        } else {
+            acc[C - 1] += beta * v;
+        }
+    }
+};
+
+template <int LMAX, int KMAX>
+__global__ void __launch_bounds__(kAdjPts * kAdjLanes, 1) adjoint_grid_kernel(AdjGridArgs args) {
+    extern __shared__ double adj_smem[];
+    double* Gs = adj_smem;                                   // [lanes][pts][KMAX]
+    double* As = Gs + kAdjLanes * kAdjPts * KMAX;            // [pts][KMAX]
+    double* grad_s = As + kAdjPts * KMAX;                    // [natm][3]
+    double* v_s = grad_s + 3 * args.natm;                    // [KMAX]
+    double* e_s = v_s + KMAX;                                // [1]
+    const int tid = threadIdx.x, lane = tid % 32;
+    const int p = tid % kAdjPts, sl = tid / kAdjPts;         // point, shell lane (warp-uniform)
+    for (int i = tid; i < 3 * args.natm + KMAX + 1; i += blockDim.x) grad_s[i] = 0.0;
+    __syncthreads();
+    const int64_t ntiles = (args.n + kAdjPts - 1) / kAdjPts;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t g = tile * kAdjPts + p;
+        const bool valid = g < args.n;
+        double px = 0, py = 0, pz = 0, wg = 0;
+        if (valid) {
+            const int64_t gi = args.index[g];
+            px = args.pts[3 * gi]; py = args.pts[3 * gi + 1]; pz = args.pts[3 * gi + 2];
+            wg = args.w[gi];
+        }
+        // sweep 1: G = Phi_a phi_g, partial over this lane's shells
+        GramSink<KMAX> gs{args.phia, args.nao, {}};
+#pragma unroll
+        for (int a = 0; a < KMAX; ++a) gs.G[a] = 0.0;
+        if (valid)
+            for (int sh = sl; sh < args.nshell; sh += kAdjLanes) {
+                const ShellDesc b = args.shells[sh];
+                eval_shell_any<double, false, LMAX>(b, px - b.x, py - b.y, pz - b.z, args.exps, args.coefs, gs);
+            }
+#pragma unroll
+        for (int a = 0; a < KMAX; ++a) Gs[(sl * kAdjPts + p) * KMAX + a] = gs.G[a];
+        __syncthreads();
+        if (sl == 0) {
+            double G[KMAX], rho = 0;
+#pragma unroll
+            for (int a = 0; a < KMAX; ++a) {
+                G[a] = 0;
+                for (int l = 0; l < kAdjLanes; ++l) G[a] += Gs[(l * kAdjPts + p) * KMAX + a];
+                rho += G[a] * G[a] * args.z[a];
+            }
+            const double u = 2.0 * wg * rho;
+            double e = wg * rho * rho;
+#pragma unroll
+            for (int a = 0; a < KMAX; ++a) {
+                As[p * KMAX + a] = 2.0 * u * args.z[a] * G[a];
+                const double va = warp_allsum(u * G[a] * G[a]);
+                if (lane == 0) atomicAdd(&v_s[a], va);
+            }
+            e = warp_allsum(e);
+            if (lane == 0) atomicAdd(e_s, e);
+        }
+        __syncthreads();
+        // sweep 2: values and gradients; per shell, the warp's 32 points are
+        // reduced before one shared-memory add per component
+        GradSink<KMAX> gr{args.phia, args.dphia, args.nao, {}, 0.0, {0.0, 0.0, 0.0}};
+#pragma unroll
+        for (int a = 0; a < KMAX; ++a) gr.al[a] = As[p * KMAX + a];
+        for (int sh = sl; sh < args.nshell; sh += kAdjLanes) {
+            const ShellDesc b = args.shells[sh];
+            gr.acc[0] = gr.acc[1] = gr.acc[2] = 0.0;
+            if (valid)
+                eval_shell_any<double, true, LMAX>(b, px - b.x, py - b.y, pz - b.z, args.exps, args.coefs, gr);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const double r = warp_allsum(gr.acc[c]);
+                if (lane == 0) atomicAdd(&grad_s[3 * b.atom + c], r);
+            }
+        }
+        __syncthreads();   // Gs and As are rewritten by the next tile
+    }
+    for (int i = tid; i < 3 * args.natm; i += blockDim.x) atomicAdd(&args.gacc[i], grad_s[i]);
+    for (int i = tid; i < KMAX; i += blockDim.x) atomicAdd(&args.v[i], v_s[i]);
+    if (tid == 0) atomicAdd(args.energy, *e_s);
+}
+
+template <int LMAX, int KMAX>
+void launch_adjoint_grid(const AdjGridArgs& a, cudaStream_t s) {
+    const size_t smem = (static_cast<size_t>(kAdjLanes + 1) * kAdjPts * KMAX + 3 * a.natm + KMAX + 1) * sizeof(double);
+    auto kern = adjoint_grid_kernel<LMAX, KMAX>;
+    ISDF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    int dev = 0, nsm = 148;
+    ISDF_CUDA(cudaGetDevice(&dev));
+    ISDF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t ntiles = (a.n + kAdjPts - 1) / kAdjPts;
+    kern<<<static_cast<unsigned>(std::min<int64_t>(ntiles, nsm)), kAdjPts * kAdjLanes, smem, s>>>(a);
+    ISDF_LAUNCH_CHECK();
+}
+
+// rows [0, k) of a [rows_in][nao] matrix into a zero-padded [kmax][nao] one, per component
+__global__ void pad_rows_kernel(const double* __restrict__ src, int ncomp, int k, int kmax, int nao,
+                                double* __restrict__ dst) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t total = static_cast<int64_t>(ncomp) * kmax * nao;
+    if (i >= total) return;
+    const int mu = static_cast<int>(i % nao);
+    const int a = static_cast<int>((i / nao) % kmax);
+    const int c = static_cast<int>(i / (static_cast<int64_t>(nao) * kmax));
+    dst[i] = a < k ? src[(static_cast<int64_t>(c) * k + a) * nao + mu] : 0.0;
+}
+
 }  // namespace
 
 void set_atom_coords(Context& c, const double* coords) {
@@ -154,6 +330,7 @@ void set_atom_coords(Context& c, const double* coords) {
     if (!c.shells.empty())
         ISDF_CUDA(cudaMemcpy(c.d_shells, c.shells.data(), c.shells.size() * sizeof(ShellDesc),
                              cudaMemcpyHostToDevice));
+    upload_shell_centres(c);
 }
 
 AdjointResult energy_gradient(const Context& c, const double* pts, const double* w,
@@ -184,13 +361,44 @@ AdjointResult energy_gradient(const Context& c, const double* pts, const double*
     ISDF_LAUNCH_CHECK();
     gemm_f64(k, k, nao, f.phi_a.get(), nao, 0, f.phi_aT.get(), k, 0, S.get(), k, 0, 1, false, s);
 
-    // grid pass in chunks: AO values + gradients recomputed per chunk
-    const int64_t chunk = std::max<int64_t>(256, std::min<int64_t>(n, (int64_t(1) << 25) / nao));
+    const int kmax = k <= 8 ? 8 : k <= 16 ? 16 : 32;
+    const size_t fused_smem =
+        (static_cast<size_t>(kAdjLanes + 1) * kAdjPts * kmax + 3 * c.natm + kmax + 1) * sizeof(double);
+    const bool fused = k <= 32 && c.natm <= kAdjMaxAtoms && fused_smem <= 200 * 1024;
+    DeviceBuffer<double> gacc(static_cast<size_t>(3 * c.natm), s);
+    gacc.zero(s);
+    if (fused) {
+        ISDF_PROFILE("adjoint_grid", s);
+        DeviceBuffer<double> phia_pad(static_cast<size_t>(kmax * nao), s),
+            dphia_pad(static_cast<size_t>(3 * kmax * nao), s), z_pad(kmax, s);
+        pad_rows_kernel<<<nblk(kmax * nao), 256, 0, s>>>(f.phi_a.get(), 1, static_cast<int>(k), kmax,
+                                                          static_cast<int>(nao), phia_pad.get());
+        ISDF_LAUNCH_CHECK();
+        pad_rows_kernel<<<nblk(3 * kmax * nao), 256, 0, s>>>(dphia.get(), 3, static_cast<int>(k), kmax,
+                                                              static_cast<int>(nao), dphia_pad.get());
+        ISDF_LAUNCH_CHECK();
+        pad_rows_kernel<<<1, 256, 0, s>>>(z.get(), 1, static_cast<int>(k), kmax, 1, z_pad.get());
+        ISDF_LAUNCH_CHECK();
+        AdjGridArgs a{c.d_shells, c.nshell, static_cast<int>(nao), c.natm, c.d_exp, c.d_coef, pts, w,
+                      kp.index.get(), n, phia_pad.get(), dphia_pad.get(), z_pad.get(), gacc.get(), v.get(),
+                      energy.get()};
+        if (c.lmax <= 2) {
+            if (kmax == 8) launch_adjoint_grid<2, 8>(a, s);
+            else if (kmax == 16) launch_adjoint_grid<2, 16>(a, s);
+            else launch_adjoint_grid<2, 32>(a, s);
+        } else {
+            if (kmax == 8) launch_adjoint_grid<kMaxL, 8>(a, s);
+            else if (kmax == 16) launch_adjoint_grid<kMaxL, 16>(a, s);
+            else launch_adjoint_grid<kMaxL, 32>(a, s);
+        }
+    }
+    // otherwise the grid pass in chunks: AO values + gradients recomputed per chunk
+    const int64_t chunk = fused ? 1 : std::max<int64_t>(256, std::min<int64_t>(n, (int64_t(1) << 25) / nao));
     DeviceBuffer<double> cp(static_cast<size_t>(3 * chunk), s), cw(chunk, s),
         phi(static_cast<size_t>(chunk * nao), s), dphi(static_cast<size_t>(3 * chunk * nao), s),
         G(static_cast<size_t>(chunk * k), s), alpha(static_cast<size_t>(chunk * k), s),
         alphaT(static_cast<size_t>(chunk * k), s), beta(static_cast<size_t>(chunk * nao), s);
-    for (int64_t g0 = 0; g0 < n; g0 += chunk) {
+    for (int64_t g0 = 0; !fused && g0 < n; g0 += chunk) {
         const int64_t b = std::min(chunk, n - g0);
         ISDF_PROFILE("adjoint_grid", s);
         gather_kernel<<<nblk(b), 256, 0, s>>>(pts, w, kp.index.get() + g0, b, cp.get(), cw.get());
@@ -219,8 +427,9 @@ AdjointResult energy_gradient(const Context& c, const double* pts, const double*
     anchor_contrib_kernel<<<cg, 256, 0, s>>>(static_cast<int>(k), static_cast<int>(nao), coef.get(),
                                              dphia.get(), acc.get());
     ISDF_LAUNCH_CHECK();
-    std::vector<double> hacc(3 * nao);
+    std::vector<double> hacc(3 * nao), hg(3 * c.natm);
     ISDF_CUDA(cudaMemcpyAsync(hacc.data(), acc.get(), hacc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(hg.data(), gacc.get(), hg.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaMemcpyAsync(&r.energy, energy.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaStreamSynchronize(s));
     // d phi / d R_A = -grad_r phi for AOs on atom A
@@ -228,6 +437,7 @@ AdjointResult energy_gradient(const Context& c, const double* pts, const double*
         const int a = c.ao_atom[mu];
         for (int cc = 0; cc < 3; ++cc) r.grad[a * 3 + cc] -= hacc[cc * nao + mu];
     }
+    for (int i = 0; i < 3 * c.natm; ++i) r.grad[i] -= hg[i];   // fused grid pass (per atom)
     return r;
 }
 

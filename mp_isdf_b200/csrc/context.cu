@@ -35,6 +35,19 @@ Context::~Context() {
     cudaFree(ws);
 }
 
+void upload_shell_centres(Context& c) {
+    if (c.shells.empty()) return;
+    std::vector<float4> hi, lo;
+    for (const auto& sh : c.shells) {
+        const float xh = static_cast<float>(sh.x), yh = static_cast<float>(sh.y), zh = static_cast<float>(sh.z);
+        hi.push_back(make_float4(xh, yh, zh, sh.amin));
+        lo.push_back(make_float4(static_cast<float>(sh.x - xh), static_cast<float>(sh.y - yh),
+                                 static_cast<float>(sh.z - zh), 0.f));
+    }
+    ISDF_CUDA(cudaMemcpy(c.d_shell_hi, hi.data(), hi.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    ISDF_CUDA(cudaMemcpy(c.d_shell_lo, lo.data(), lo.size() * sizeof(float4), cudaMemcpyHostToDevice));
+}
+
 uint8_t* Context::workspace(size_t bytes) const {
     if (bytes > ws_bytes) {
         if (ws) ISDF_CUDA(cudaFree(ws));   // waits for the device
@@ -115,16 +128,10 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
     up(c->d_expf, expf_);
     up(c->d_coeff, coeff_);
     up(c->d_ao_atom, c->ao_atom);
-    {
-        std::vector<float4> hi, lo;
-        for (const auto& sh : c->shells) {
-            const float xh = static_cast<float>(sh.x), yh = static_cast<float>(sh.y), zh = static_cast<float>(sh.z);
-            hi.push_back(make_float4(xh, yh, zh, sh.amin));
-            lo.push_back(make_float4(static_cast<float>(sh.x - xh), static_cast<float>(sh.y - yh),
-                                     static_cast<float>(sh.z - zh), 0.f));
-        }
-        up(c->d_shell_hi, hi);
-        up(c->d_shell_lo, lo);
+    if (!c->shells.empty()) {
+        ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c->d_shell_hi), c->shells.size() * sizeof(float4)));
+        ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c->d_shell_lo), c->shells.size() * sizeof(float4)));
+        upload_shell_centres(*c);
     }
     build_chunk_layout(*c);
     return c.release();

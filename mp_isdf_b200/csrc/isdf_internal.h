@@ -150,6 +150,8 @@ struct Context {
     ~Context();
 };
 
+// Copies the shells' centres (FP32 hi + lo) and smallest exponents to the device.
+void upload_shell_centres(Context& c);
 // Fills the context's K-chunk layout (defined with the projection kernel).
 void build_chunk_layout(Context& c);
 // Producer lanes per point of the projection kernel for a basis' largest l.

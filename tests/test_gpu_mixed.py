@@ -186,3 +186,21 @@ def test_select_fit_host_buffers(small_water):
     # equal up to the order of atomic FP64 reductions, amplified by cond(C)^2
     rel = np.abs(th_h - th_d).max() / np.abs(th_d).max()
     assert rel <= 1e-12 * max(1.0, fd.condition) ** 2, rel
+
+
+def test_mixed_projection_follows_moved_atoms(small_water):
+    """After isdf_ctx_set_coords the tensor-core path evaluates AOs at the new
+    centres: mixed and FP64 projections agree to the split-BF16 bound."""
+    import torch
+    from mp_isdf_b200 import capi
+    mol, pts, w = small_water
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    moved = mol.coords + np.random.default_rng(1).normal(scale=0.2, size=mol.coords.shape)
+    ctx.set_coords(moved)
+    x = torch.tensor(pts[::5], device="cuda")
+    W = np.random.default_rng(2).normal(size=(4 * mol.nao, 16))
+    p64 = ctx.project_axes(x, ("ao", "dx", "dy", "dz"), W, "fp64").cpu().numpy()
+    pm = ctx.project_axes(x, ("ao", "dx", "dy", "dz"), W, "mixed").cpu().numpy()
+    scale = np.abs(p64).max()
+    assert np.abs(pm - p64).max() <= 1e-4 * scale
+    ctx.set_coords(mol.coords)
