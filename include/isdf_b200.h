@@ -167,6 +167,44 @@ int isdf_select_fit_host(isdf_ctx* ctx, const isdf_select_args* args, const doub
                          const double* w_host, int64_t ng, int64_t* pivots_host, int64_t capacity,
                          int64_t* npivots, isdf_select_info* select_info, int32_t want_error,
                          double* theta_host, isdf_fit_info* fit_info);
+/* ---- grid-sharded rand_sketch (one rank per GPU) ---------------------------------
+ * The distributed form of AnchorSelection::select + the fit for
+ * RandomizedQuadratureKhatriRao (cpp/src/anchor_select_randomized_id.cpp:92-374;
+ * the reference's DistributedAnchorSelection is a stub that throws,
+ * cpp/src/anchor_select.cpp:175-181, cpp/src/anchor_select_pybind.cpp:224-240).  Every rank holds a contiguous
+ * shard of the grid, in grid order; the caller supplies the collectives:
+ *  1. isdf_sketch_shard_project: compaction and projection of this shard;
+ *     returns its per-component sums of squares (sum them over ranks);
+ *  2. isdf_sketch_shard_combine: this shard's sketch columns yt[ell][n_kept]
+ *     with the global axis scales, their error bounds (mixed form), kept grid
+ *     indices, coordinates and weights (gather all of them over ranks);
+ *  3. isdf_sketch_select_gathered (every rank, same gathered inputs):
+ *     pivoted QR of the gathered sketch + rank logic; pivots are positions in
+ *     the gathered kept-point order;
+ *  4. isdf_fit_at on each shard with the anchors' coordinates and weights;
+ *     sums_host = {err2, exact2} of the shard (sum over ranks).
+ * The result equals the single-GPU selection on the concatenated grid. */
+typedef struct isdf_sketch_shard isdf_sketch_shard;
+int isdf_sketch_shard_project(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz_dev,
+                              const double* w_dev, int64_t ng, int64_t ng_total, isdf_sketch_shard** out,
+                              int64_t* n_kept, int64_t* ell, double* sumsq_host, void* stream);
+/* yt_dev: ell x n_kept (leading dimension n_kept); delta_dev: n_kept (mixed
+ * form; zeros in the FP64 form; may be null there); kept_dev: n_kept grid
+ * indices within the shard; kept_xyz_dev/kept_w_dev: n_kept x 3 / n_kept;
+ * scales_host: one per axis entry.  The shard's grid must still be valid. */
+int isdf_sketch_shard_combine(isdf_sketch_shard* shard, const double* sumsq_global_host, double* yt_dev,
+                              double* delta_dev, int64_t* kept_dev, double* kept_xyz_dev,
+                              double* kept_w_dev, double* scales_host, void* stream);
+void isdf_sketch_shard_free(isdf_sketch_shard* shard);
+int isdf_sketch_select_gathered(isdf_ctx* ctx, const isdf_select_args* args, double* yt_dev, int64_t n,
+                                const double* kept_xyz_dev, const double* kept_w_dev, double* delta_dev,
+                                const double* scales_host, int64_t* pivots_host, int64_t capacity,
+                                int64_t* npivots, isdf_select_info* info, void* stream);
+/* isdf_fit with anchors given by host coordinates (k x 3) and weights. */
+int isdf_fit_at(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t ng,
+                const double* anchor_xyz_host, const double* anchor_w_host, int64_t k, int32_t precision,
+                int32_t want_error, double* theta_dev, isdf_fit_info* info, double* sums_host, void* stream);
+
 /* Pair-space error of a given Theta (k x n_kept, leading dimension n_kept),
  * recomputed with FP64 AO values. */
 int isdf_pair_error(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t ng,

@@ -28,6 +28,8 @@ SYMBOLS = [
     "isdf_profile_enable", "isdf_profile_read", "isdf_project_axes",
     "isdf_energy_gradient", "isdf_ctx_set_coords", "isdf_pair_error_terms_noalloc",
     "isdf_select_fit", "isdf_select_fit_host",
+    "isdf_sketch_shard_project", "isdf_sketch_shard_combine", "isdf_sketch_shard_free",
+    "isdf_sketch_select_gathered", "isdf_fit_at",
 ]
 
 ALGORITHMS = {"qrcp_dense": 0, "qrcp_online": 1, "rand_sketch": 2}
@@ -91,6 +93,15 @@ def lib():
         L.isdf_select_fit_host.argtypes = [P, ctypes.POINTER(SelectArgs), P, P, I64, P, I64,
                                            ctypes.POINTER(I64), ctypes.POINTER(SelectInfo), I32, P,
                                            ctypes.POINTER(FitInfo)]
+        L.isdf_sketch_shard_project.argtypes = [P, ctypes.POINTER(SelectArgs), P, P, I64, I64,
+                                                ctypes.POINTER(P), ctypes.POINTER(I64),
+                                                ctypes.POINTER(I64), P, P]
+        L.isdf_sketch_shard_combine.argtypes = [P, P, P, P, P, P, P, P, P]
+        L.isdf_sketch_shard_free.argtypes = [P]
+        L.isdf_sketch_shard_free.restype = None
+        L.isdf_sketch_select_gathered.argtypes = [P, ctypes.POINTER(SelectArgs), P, I64, P, P, P, P, P,
+                                                  I64, ctypes.POINTER(I64), ctypes.POINTER(SelectInfo), P]
+        L.isdf_fit_at.argtypes = [P, P, P, I64, P, P, I64, I32, I32, P, ctypes.POINTER(FitInfo), P, P]
         L.isdf_pair_error.argtypes = [P, P, P, I64, P, I64, P, ctypes.POINTER(F64),
                                       ctypes.POINTER(F64), P]
         L.isdf_pair_error_terms.argtypes = [I64, I64, P, P, P, P, P, P, P]
@@ -203,6 +214,62 @@ class Context:
         del keep
         return piv[:n.value].copy(), sinfo, finfo
 
+    # ---- grid-sharded selection phases (see mp_isdf_b200.sharded) ----------------
+    def sketch_shard_project(self, xyz, w, ng_total, **kw):
+        """Project this rank's grid shard (device tensors).  Returns (shard
+        handle, kept points, sketch rows, per-component sums of squares [4])."""
+        args, keep = make_select_args(**kw)
+        h, n, ell = P(), I64(), I64()
+        sumsq = np.zeros(4)
+        check(lib().isdf_sketch_shard_project(self.h, ctypes.byref(args), _ptr(xyz), _ptr(w), xyz.shape[0],
+                                              int(ng_total), ctypes.byref(h), ctypes.byref(n),
+                                              ctypes.byref(ell), _ptr(sumsq), _stream(xyz)))
+        del keep
+        return SketchShard(h.value, xyz), n.value, ell.value, sumsq
+
+    def sketch_shard_combine(self, shard, sumsq_global, ell, n_kept, naxes):
+        """The shard's sketch columns with the global scales: (yt [ell, n_kept],
+        delta [n_kept], kept grid indices, kept xyz [n_kept, 3], kept w, scales)."""
+        import torch
+        dev = shard.xyz.device
+        yt = torch.empty(ell, max(n_kept, 1), dtype=torch.float64, device=dev)
+        delta = torch.zeros(max(n_kept, 1), dtype=torch.float64, device=dev)
+        kept = torch.empty(max(n_kept, 1), dtype=torch.int64, device=dev)
+        kxyz = torch.empty(max(n_kept, 1), 3, dtype=torch.float64, device=dev)
+        kw_ = torch.empty(max(n_kept, 1), dtype=torch.float64, device=dev)
+        scales = np.ones(naxes)
+        sg = _np(sumsq_global, np.float64)
+        check(lib().isdf_sketch_shard_combine(shard.h, _ptr(sg), _ptr(yt), _ptr(delta), _ptr(kept), _ptr(kxyz),
+                                              _ptr(kw_), _ptr(scales), _stream(shard.xyz)))
+        return (yt[:, :n_kept], delta[:n_kept], kept[:n_kept], kxyz[:n_kept], kw_[:n_kept], scales)
+
+    def sketch_select_gathered(self, yt, kept_xyz, kept_w, delta, scales, **kw):
+        """Pivoted QR of a gathered sketch (device tensors; yt contiguous
+        [ell, n]); returns (positions in the gathered order, SelectInfo)."""
+        args, keep = make_select_args(**kw)
+        n = yt.shape[1]
+        piv = np.empty(max(n, 1), dtype=np.int64)
+        npiv = I64()
+        info = SelectInfo()
+        sc = _np(scales, np.float64)
+        check(lib().isdf_sketch_select_gathered(self.h, ctypes.byref(args), _ptr(yt), n, _ptr(kept_xyz),
+                                                _ptr(kept_w), _ptr(delta), _ptr(sc), _ptr(piv), len(piv),
+                                                ctypes.byref(npiv), ctypes.byref(info), _stream(yt)))
+        del keep
+        return piv[:npiv.value].copy(), info
+
+    def fit_at(self, xyz, w, anchor_xyz, anchor_w, theta, precision="fp64", want_error=True):
+        """Fit on device points with anchors given by coordinates; returns
+        (FitInfo, [err2, exact2] of these points)."""
+        axyz = _np(anchor_xyz, np.float64).reshape(-1, 3)
+        aw = _np(anchor_w, np.float64)
+        info = FitInfo()
+        sums = np.zeros(2)
+        check(lib().isdf_fit_at(self.h, _ptr(xyz), _ptr(w), xyz.shape[0], _ptr(axyz), _ptr(aw), len(aw),
+                                1 if precision == "mixed" else 0, int(want_error), _ptr(theta),
+                                ctypes.byref(info), _ptr(sums), _stream(xyz)))
+        return info, sums
+
     def pair_error(self, xyz, w, anchors, theta):
         a = _np(anchors, np.int64)
         l2, rel = F64(), F64()
@@ -299,6 +366,25 @@ class Context:
                                   1 if precision == "mixed" else 0, int(want_error), _ptr(theta),
                                   ctypes.byref(info)))
         return theta[:len(a) * info.n_kept].reshape(len(a), info.n_kept), info
+
+
+class SketchShard:
+    """Owns a projected grid shard (isdf_sketch_shard) until it is freed."""
+
+    def __init__(self, h, xyz):
+        self.h = h
+        self.xyz = xyz     # keeps the shard's grid alive for the combine step
+
+    def free(self):
+        if self.h:
+            lib().isdf_sketch_shard_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 def make_select_args(algorithm="rand_sketch", axes=("ao",), axis_weights=None, tolerance=1e-10,

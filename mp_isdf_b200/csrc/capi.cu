@@ -328,10 +328,17 @@ int isdf_select_host(isdf_ctx* ctx, const isdf_select_args* args, const double* 
 
 namespace {
 
+// Anchors given by host coordinates and weights instead of grid indices.
+struct AnchorCoords {
+    const double* xyz = nullptr;   // k x 3
+    const double* w = nullptr;     // k
+};
+
 void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, const int64_t* anchors,
               int64_t k, int32_t precision, const double* theta_in, double* theta_out,
               isdf_fit_info* info, double* l2, double* rel, cudaStream_t s, bool want_error = true,
-              const isdf::RetainedAo* ra = nullptr) {
+              const isdf::RetainedAo* ra = nullptr, const AnchorCoords* ac = nullptr,
+              double* sums = nullptr) {
     auto& c = ctx_of(ctx);
     DeviceGuard dg(c.device);
     if (ng < 0 || k < 0) isdf::fail(isdf::kInvalid, "sizes must be nonnegative");
@@ -346,11 +353,21 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
         kp_own = isdf::compact_points(xyz, w, ng, s);
     }
     const isdf::KeptPoints& kp = reuse ? ra->kp : kp_own;
-    isdf::DeviceBuffer<int64_t> didx;
-    upload(didx, anchors, static_cast<size_t>(k), s);
     isdf::DeviceBuffer<double> apts(static_cast<size_t>(3 * std::max<int64_t>(k, 1)), s),
         aw(std::max<int64_t>(k, 1), s);
-    isdf::gather_points(xyz, w, didx.get(), k, ng, apts.get(), aw.get(), s);
+    if (ac) {
+        if (k && (!ac->xyz || !ac->w)) isdf::fail(isdf::kInvalid, "anchor coordinates and weights are required");
+        for (int64_t i = 0; i < 3 * k; ++i)
+            if (!std::isfinite(ac->xyz[i])) isdf::fail(isdf::kInvalid, "anchor coordinates must be finite");
+        if (k) {
+            ISDF_CUDA(cudaMemcpyAsync(apts.get(), ac->xyz, 3 * k * sizeof(double), cudaMemcpyHostToDevice, s));
+            ISDF_CUDA(cudaMemcpyAsync(aw.get(), ac->w, k * sizeof(double), cudaMemcpyHostToDevice, s));
+        }
+    } else {
+        isdf::DeviceBuffer<int64_t> didx;
+        upload(didx, anchors, static_cast<size_t>(k), s);
+        isdf::gather_points(xyz, w, didx.get(), k, ng, apts.get(), aw.get(), s);
+    }
     isdf::AnchorFactor f;
     {
         ISDF_PROFILE("phase:factor_anchors", s);
@@ -395,6 +412,10 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
     }
     if (l2) *l2 = el2;
     if (rel) *rel = erel;
+    if (sums) {
+        sums[0] = o.err2;
+        sums[1] = o.exact2;
+    }
 }
 
 }  // namespace
@@ -579,6 +600,92 @@ int isdf_pair_error_terms(int64_t n, int64_t k, const double* q, const double* H
         const double a = std::sqrt(std::max(acc[0], 0.0));
         out[0] = a;
         out[1] = acc[1] ? a / std::sqrt(acc[1]) : (a == 0 ? 0.0 : INFINITY);
+    });
+}
+
+// ---- grid-sharded selection phases -----------------------------------------------
+struct isdf_sketch_shard {
+    isdf_ctx* ctx = nullptr;
+    isdf::SketchShard st;
+};
+
+int isdf_sketch_shard_project(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz,
+                              const double* w, int64_t ng, int64_t ng_total, isdf_sketch_shard** out,
+                              int64_t* n_kept, int64_t* ell, double* sumsq_host, void* stream) {
+    return guarded([&] {
+        if (!out) isdf::fail(isdf::kInvalid, "null shard handle");
+        *out = nullptr;
+        if (!args) isdf::fail(isdf::kInvalid, "selection arguments are required");
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        isdf::SelectOptions o = options_of(args);
+        if (o.algorithm != ISDF_RAND_SKETCH_QUADRATURE)
+            isdf::fail(isdf::kInvalid, "grid-sharded selection supports rand_sketch (quadrature)");
+        if (ng < 0 || ng_total < ng) isdf::fail(isdf::kInvalid, "invalid shard or total grid size");
+        isdf::validate_axis_weights(o.axis_weights.empty() ? nullptr : o.axis_weights.data(),
+                                    static_cast<int>(o.axes.size()));
+        auto h = std::make_unique<isdf_sketch_shard>();
+        h->ctx = ctx;
+        isdf::sketch_shard_project(c, xyz, w, ng, o, ng_total, h->st, as_stream(stream));
+        if (n_kept) *n_kept = h->st.kp.n;
+        if (ell) *ell = h->st.su.ell;
+        if (sumsq_host) std::memcpy(sumsq_host, h->st.sumsq, 4 * sizeof(double));
+        *out = h.release();
+    });
+}
+
+int isdf_sketch_shard_combine(isdf_sketch_shard* h, const double* sumsq_global, double* yt, double* delta,
+                              int64_t* kept, double* kept_xyz, double* kept_w, double* scales_host,
+                              void* stream) {
+    return guarded([&] {
+        if (!h || !sumsq_global || (!yt && h->st.kp.n)) isdf::fail(isdf::kInvalid, "invalid shard combine arguments");
+        auto& c = ctx_of(h->ctx);
+        DeviceGuard dg(c.device);
+        std::vector<double> scales;
+        isdf::sketch_shard_combine(c, h->st, sumsq_global, yt, delta, kept, kept_xyz, kept_w, scales,
+                                   as_stream(stream));
+        if (scales_host) std::memcpy(scales_host, scales.data(), scales.size() * sizeof(double));
+    });
+}
+
+void isdf_sketch_shard_free(isdf_sketch_shard* h) { delete h; }
+
+int isdf_sketch_select_gathered(isdf_ctx* ctx, const isdf_select_args* args, double* yt, int64_t n,
+                                const double* kept_xyz, const double* kept_w, double* delta,
+                                const double* scales_host, int64_t* pivots, int64_t capacity,
+                                int64_t* npivots, isdf_select_info* info, void* stream) {
+    return guarded([&] {
+        if (npivots) *npivots = 0;
+        if (!args || !scales_host || n < 0) isdf::fail(isdf::kInvalid, "invalid gathered selection arguments");
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        isdf::SelectOptions o = options_of(args);
+        if (o.algorithm != ISDF_RAND_SKETCH_QUADRATURE)
+            isdf::fail(isdf::kInvalid, "grid-sharded selection supports rand_sketch (quadrature)");
+        if (info) std::memset(info, 0, sizeof(*info));
+        const std::vector<double> scales(scales_host, scales_host + o.axes.size());
+        isdf::SketchDiagnostics d;
+        std::vector<int64_t> out =
+            isdf::select_sketch_gathered(c, o, yt, n, kept_xyz, kept_w, delta, scales, &d, as_stream(stream));
+        if (info) {
+            info->sketch_rows = d.ell;
+            info->numerical_rank = d.numerical_rank;
+            info->relative_residual = d.relative_tail;
+            info->verifications = d.reverified;
+        }
+        if (static_cast<int64_t>(out.size()) > capacity) isdf::fail(isdf::kInvalid, "pivot buffer is too small");
+        if (!out.empty()) std::memcpy(pivots, out.data(), out.size() * sizeof(int64_t));
+        if (npivots) *npivots = static_cast<int64_t>(out.size());
+    });
+}
+
+int isdf_fit_at(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, const double* anchor_xyz,
+                const double* anchor_w, int64_t k, int32_t precision, int32_t want_error, double* theta,
+                isdf_fit_info* info, double* sums_host, void* stream) {
+    return guarded([&] {
+        const AnchorCoords ac{anchor_xyz, anchor_w};
+        fit_impl(ctx, xyz, w, ng, nullptr, k, precision, nullptr, theta, info, nullptr, nullptr,
+                 as_stream(stream), want_error != 0, nullptr, &ac, sums_host);
     });
 }
 

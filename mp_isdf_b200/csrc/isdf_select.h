@@ -111,6 +111,52 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
                                         int64_t ng, const SelectOptions& o, cudaStream_t s,
                                         SketchDiagnostics* diag = nullptr, RetainedAo* keep = nullptr);
 
+// Validated sketch parameters for n kept points (cpp/src/anchor_select_randomized_id.cpp:116-191).
+struct SketchSetup {
+    AxisSpec ax{};
+    int64_t d = 0, ell = 0, physical_rank = 0;
+    bool mixed = false;              // mixed-precision form applies
+};
+SketchSetup sketch_setup(const Context& c, const SelectOptions& o, int64_t n);
+
+// Tails, numerical rank, cap and the selected rank of a sketch QR
+// (cpp/src/anchor_select_randomized_id.cpp:320-374).
+struct SketchRank {
+    int64_t rank = 0, numerical_rank = 0, cap = 0;
+    double relative_tail = 0;
+    std::vector<double> tails;
+};
+SketchRank sketch_rank(const SketchQR& qr, int64_t ell, int64_t n, const SelectOptions& o,
+                       int64_t physical_rank);
+
+// Grid-sharded rand_sketch.  Each rank projects its shard (sketch_shard_project,
+// returning per-component sums of squares), the ranks sum those, each rank
+// forms its shard's sketch columns with the global axis scales
+// (sketch_shard_combine), and every rank runs the pivoted QR of the gathered
+// sketch (select_sketch_gathered), which returns positions in the gathered
+// kept-point order.
+struct SketchShard {
+    SelectOptions o;
+    SketchSetup su;
+    KeptPoints kp;
+    std::vector<double> u, v;
+    DeviceBuffer<float> Pf, psq;     // mixed: projections, per-point sums of squares
+    DeviceBuffer<double> Pd;         // FP64: projections
+    double sumsq[4] = {0, 0, 0, 0};
+    const double* pts = nullptr;     // the shard's grid (caller's device arrays)
+    const double* w = nullptr;
+    int64_t ng = 0;
+};
+void sketch_shard_project(const Context& c, const double* pts, const double* w, int64_t ng,
+                          const SelectOptions& o, int64_t n_total, SketchShard& st, cudaStream_t s);
+void sketch_shard_combine(const Context& c, SketchShard& st, const double* sumsq_global, double* Yt,
+                          double* delta, int64_t* kept_out, double* kept_xyz, double* kept_w,
+                          std::vector<double>& scales, cudaStream_t s);
+std::vector<int64_t> select_sketch_gathered(const Context& c, const SelectOptions& o, double* Yt, int64_t n,
+                                            const double* kept_xyz, const double* kept_w, double* delta,
+                                            const std::vector<double>& scales, SketchDiagnostics* diag,
+                                            cudaStream_t s);
+
 // qrcp_dense / qrcp_online: greedy max-residual pivoting of the weighted
 // pair columns sqrt|w_g| f_g (x) f_g, computed without materialising them.
 std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const double* w,

@@ -11,6 +11,7 @@
 //   Y[s,g] = sqrt|w_g|/sqrt(ell) (f_g.u_s)(f_g.v_s)   :297-309
 //   dgeqp3 of Y, row energies -> tails, numerical rank, exact-rank / tolerance
 //   rank selection                          cpp/src/anchor_select_randomized_id.cpp:320-374
+#include "isdf_fit.h"
 #include "isdf_project.h"
 #include "isdf_select.h"
 #include "isdf_reduce.cuh"
@@ -388,17 +389,86 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
 // ------------------------------------------------------------------------------
 // rand_sketch (quadrature) driver
 // ------------------------------------------------------------------------------
-std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, const double* w,
-                                        int64_t ng, const SelectOptions& o, cudaStream_t s,
-                                        SketchDiagnostics* diag_out, RetainedAo* keep) {
+SketchSetup sketch_setup(const Context& c, const SelectOptions& o, int64_t n) {
     if (!std::isfinite(o.tolerance) || o.tolerance < 0 || o.batch_size <= 0 ||
         o.oversampling <= 0 || (!o.max_rank && o.sketch_size <= o.oversampling))
         fail(kInvalid, "invalid randomized ID grid, tolerance, batch, sketch or rank/oversampling");
-    AxisSpec ax = make_axis_spec(c, o.axes.data(), static_cast<int>(o.axes.size()));
-    const int64_t d = static_cast<int64_t>(ax.naxes) * c.nao;
+    SketchSetup su;
+    su.ax = make_axis_spec(c, o.axes.data(), static_cast<int>(o.axes.size()));
+    su.d = static_cast<int64_t>(su.ax.naxes) * c.nao;
     if (o.max_rank > std::numeric_limits<int64_t>::max() - o.oversampling)
         fail(kOverflow, "randomized ID rank + oversampling overflows size_t");
     const int64_t requested = o.max_rank ? o.max_rank + o.oversampling : o.sketch_size;
+    su.physical_rank = su.d * (su.d + 1) / 2;
+    if (n == 0) return su;
+    const int64_t physical_limit = su.physical_rank + o.oversampling;
+    const int64_t backend_limit = std::numeric_limits<int64_t>::max() / n;
+    su.ell = requested <= backend_limit ? requested : std::min({requested, physical_limit, backend_limit});
+    if (su.ell <= o.oversampling ||
+        (o.max_rank && std::min(o.max_rank, su.physical_rank) > su.ell - o.oversampling))
+        fail(kInvalid, "randomized ID sketch/rank exceeds the ILP64 QRCP backend limit for this "
+                       "grid; reduce the sketch/rank or use a tiled QRCP backend");
+    if (o.max_rank > std::min(n, su.physical_rank))
+        fail(kInvalid, "requested anchor_rank exceeds eligible candidates or physical pair rank");
+    // the mixed form needs the tensor-core shape and room for one point's AO
+    // components in shared memory for the FP64 re-verification of candidates
+    su.mixed = o.precision == 1 && project_tc_supported(su.ax.naxes, static_cast<int>(2 * su.ell)) &&
+               su.ell <= 64 && c.nao <= kMaxVerifiedNao;
+    return su;
+}
+
+SketchRank sketch_rank(const SketchQR& qr, int64_t ell, int64_t n, const SelectOptions& o,
+                       int64_t physical_rank) {
+    SketchRank r;
+    const int64_t steps = std::min(ell, n);
+    r.tails.assign(steps + 1, 0.0);
+    double diag_max = 0;
+    for (int64_t i = steps; i-- > 0;) {
+        r.tails[i] = std::hypot(r.tails[i + 1], std::sqrt(qr.energy[i]));
+        diag_max = std::max(diag_max, qr.diag[i]);
+    }
+    if (!std::isfinite(r.tails[0]) || !std::isfinite(diag_max))
+        fail(kOverflow, "non-finite randomized ID QR residual");
+    const double norm = r.tails[0];
+    const double floor = std::numeric_limits<double>::epsilon() *
+                         static_cast<double>(std::max(ell, n)) * diag_max;
+    r.numerical_rank = steps;
+    for (int64_t i = 0; i < steps; ++i)
+        if (qr.diag[i] <= floor) { r.numerical_rank = i; break; }
+    r.cap = std::min({o.max_rank ? o.max_rank : ell - o.oversampling, ell - o.oversampling, steps,
+                      physical_rank, r.numerical_rank});
+    if (o.max_rank && r.numerical_rank < o.max_rank)
+        fail(kInvalid, "requested anchor_rank exceeds the numerical rank of the randomized sketch");
+    r.rank = o.max_rank ? o.max_rank : r.cap;
+    if (!o.max_rank)
+        for (int64_t i = 0; i <= r.cap; ++i)
+            if (r.tails[i] <= o.tolerance * norm) { r.rank = i; break; }
+    r.relative_tail = norm ? r.tails[r.rank] / norm : 0.0;
+    for (int64_t i = 0; i < r.rank; ++i)
+        if (qr.jpvt[i] < 0 || qr.jpvt[i] >= n) fail(kRuntime, "randomized ID QRCP returned invalid pivot");
+    return r;
+}
+
+namespace {
+
+void fill_diag(SketchDiagnostics* d, int64_t ell, const SketchRank& r, const SketchQR& qr) {
+    if (!d) return;
+    d->ell = ell;
+    d->numerical_rank = r.numerical_rank;
+    d->cap = r.cap;
+    d->rank = r.rank;
+    d->relative_tail = r.relative_tail;
+    d->diag = qr.diag;
+    d->reverified = qr.reverified;
+    d->tails = r.tails;
+}
+
+}  // namespace
+
+std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, const double* w,
+                                        int64_t ng, const SelectOptions& o, cudaStream_t s,
+                                        SketchDiagnostics* diag_out, RetainedAo* keep) {
+    sketch_setup(c, o, 0);   // option checks before any device work
     ISDF_PROFILE("phase:select", s);
     KeptPoints kp;
     {
@@ -407,83 +477,186 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
     }
     const int64_t n = kp.n;
     if (n == 0) return {};
-    const int64_t physical_rank = d * (d + 1) / 2;
-    const int64_t physical_limit = physical_rank + o.oversampling;
-    const int64_t backend_limit = std::numeric_limits<int64_t>::max() / n;
-    const int64_t ell = requested <= backend_limit
-                            ? requested
-                            : std::min({requested, physical_limit, backend_limit});
-    if (ell <= o.oversampling ||
-        (o.max_rank && std::min(o.max_rank, physical_rank) > ell - o.oversampling))
-        fail(kInvalid, "randomized ID sketch/rank exceeds the ILP64 QRCP backend limit for this "
-                       "grid; reduce the sketch/rank or use a tiled QRCP backend");
-    if (o.max_rank > std::min(n, physical_rank))
-        fail(kInvalid, "requested anchor_rank exceeds eligible candidates or physical pair rank");
+    const SketchSetup su = sketch_setup(c, o, n);
+    const AxisSpec& ax = su.ax;
+    const int64_t ell = su.ell;
     std::vector<double> u, v;
     {
         ISDF_PROFILE("phase:sketch_factors", s);
-        sketch_factors(d, ell, o.seed, u, v);
+        sketch_factors(su.d, ell, o.seed, u, v);
     }
     const int64_t ldy = n;
     DeviceBuffer<double> Yt(static_cast<size_t>(ell * n), s);
     const double* aw = o.axis_weights.empty() ? nullptr : o.axis_weights.data();
     SketchQR qr;
-    // the mixed form needs the tensor-core shape and room for one point's AO
-    // components in shared memory for the FP64 re-verification of candidates
-    if (o.precision == 1 && project_tc_supported(ax.naxes, static_cast<int>(2 * ell)) && ell <= 64 &&
-        c.nao <= kMaxVerifiedNao) {
+    if (su.mixed) {
         MixedSketch ms = sketch_mixed(c, pts, kp, w, ax, aw, ell, u, v, Yt.get(), ldy, s, keep);
         ISDF_PROFILE("phase:qrcp", s);
         qr = qrcp_sketch(Yt.get(), ldy, ell, n, s, &ms.source);
     } else {
-        const int64_t chunk = std::max<int64_t>(1024, std::min<int64_t>(n, (int64_t(1) << 28) / d));
+        const int64_t chunk = std::max<int64_t>(1024, std::min<int64_t>(n, (int64_t(1) << 28) / su.d));
         sketch_fp64(c, pts, kp, w, ax, aw, ell, u, v, Yt.get(), ldy, chunk, s);
         qr = qrcp_sketch(Yt.get(), ldy, ell, n, s);
     }
-    const int64_t steps = std::min(ell, n);
-    std::vector<double> tails(steps + 1, 0.0);
-    double diag_max = 0;
-    for (int64_t i = steps; i-- > 0;) {
-        tails[i] = std::hypot(tails[i + 1], std::sqrt(qr.energy[i]));
-        diag_max = std::max(diag_max, qr.diag[i]);
-    }
-    if (!std::isfinite(tails[0]) || !std::isfinite(diag_max))
-        fail(kOverflow, "non-finite randomized ID QR residual");
-    const double norm = tails[0];
-    const double floor = std::numeric_limits<double>::epsilon() *
-                         static_cast<double>(std::max(ell, n)) * diag_max;
-    int64_t numerical_rank = steps;
-    for (int64_t i = 0; i < steps; ++i)
-        if (qr.diag[i] <= floor) { numerical_rank = i; break; }
-    const int64_t cap = std::min({o.max_rank ? o.max_rank : ell - o.oversampling,
-                                  ell - o.oversampling, steps, physical_rank, numerical_rank});
-    if (o.max_rank && numerical_rank < o.max_rank)
-        fail(kInvalid, "requested anchor_rank exceeds the numerical rank of the randomized sketch");
-    int64_t rank = o.max_rank ? o.max_rank : cap;
-    if (!o.max_rank)
-        for (int64_t i = 0; i <= cap; ++i)
-            if (tails[i] <= o.tolerance * norm) { rank = i; break; }
+    const SketchRank r = sketch_rank(qr, ell, n, o, su.physical_rank);
     // original grid ids of the pivots (a gather of `rank` entries of the kept index)
-    std::vector<int64_t> selected(rank);
-    for (int64_t i = 0; i < rank; ++i) {
-        const int64_t pv = qr.jpvt[i];
-        if (pv < 0 || pv >= n) fail(kRuntime, "randomized ID QRCP returned invalid pivot");
-        ISDF_CUDA(cudaMemcpyAsync(&selected[i], kp.index.get() + pv, sizeof(int64_t),
+    std::vector<int64_t> selected(r.rank);
+    for (int64_t i = 0; i < r.rank; ++i)
+        ISDF_CUDA(cudaMemcpyAsync(&selected[i], kp.index.get() + qr.jpvt[i], sizeof(int64_t),
                                   cudaMemcpyDeviceToHost, s));
-    }
     ISDF_CUDA(cudaStreamSynchronize(s));
-    if (diag_out) {
-        diag_out->ell = ell;
-        diag_out->numerical_rank = numerical_rank;
-        diag_out->cap = cap;
-        diag_out->rank = rank;
-        diag_out->relative_tail = norm ? tails[rank] / norm : 0.0;
-        diag_out->diag = qr.diag;
-        diag_out->reverified = qr.reverified;
-        diag_out->tails = tails;
-    }
+    fill_diag(diag_out, ell, r, qr);
     if (keep && keep->valid) keep->kp = std::move(kp);
     return selected;
+}
+
+// ------------------------------------------------------------------------------
+// grid-sharded rand_sketch: per-shard projection, global scales, per-shard
+// sketch columns, then the pivoted QR of the gathered sketch on every rank
+// ------------------------------------------------------------------------------
+void sketch_shard_project(const Context& c, const double* pts, const double* w, int64_t ng,
+                          const SelectOptions& o, int64_t n_total, SketchShard& st, cudaStream_t s) {
+    st.o = o;
+    st.pts = pts;
+    st.w = w;
+    st.ng = ng;
+    st.kp = compact_points(pts, w, ng, s);
+    st.su = sketch_setup(c, o, std::max<int64_t>(n_total, 1));
+    const int64_t n = st.kp.n, ell = st.su.ell, d = st.su.d;
+    const int naxes = st.su.ax.naxes, nout = static_cast<int>(2 * ell);
+    sketch_factors(d, ell, o.seed, st.u, st.v);
+    for (double& x : st.sumsq) x = 0.0;
+    if (n == 0) return;
+    DeviceBuffer<double> sumsq(4, s);
+    sumsq.zero(s);
+    if (st.su.mixed) {
+        std::vector<int> comps(st.su.ax.comp, st.su.ax.comp + naxes);
+        DeviceBuffer<double> du(st.u.size(), s), dv(st.v.size(), s);
+        ISDF_CUDA(cudaMemcpyAsync(du.get(), st.u.data(), st.u.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        ISDF_CUDA(cudaMemcpyAsync(dv.get(), st.v.data(), st.v.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        const WSource srcs[2] = {{du.get(), static_cast<int64_t>(c.nao) * ell, ell, 1, static_cast<int>(ell), 0},
+                                 {dv.get(), static_cast<int64_t>(c.nao) * ell, ell, 1, static_cast<int>(ell),
+                                  static_cast<int>(ell)}};
+        ProjectPlan plan = make_project_plan(c, comps, nout, srcs, 2, s);
+        st.Pf.reset(static_cast<size_t>(n) * naxes * nout, s);
+        st.psq.reset(static_cast<size_t>(n) * 4, s);
+        st.psq.zero(s);
+        DeviceBuffer<int> err(1, s);
+        err.zero(s);
+        project_tc(c, plan, pts, st.kp.index.get(), n, w, st.Pf.get(), 1, n, sumsq.get(), st.psq.get(),
+                   err.get(), s);
+        int herr = 0;
+        ISDF_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        if (herr) fail(kRuntime, "tensor-core sketch pipeline timed out (error flags " + std::to_string(herr) + ")");
+    } else {
+        std::vector<double> hw(static_cast<size_t>(d * nout));
+        for (int64_t j = 0; j < d; ++j)
+            for (int64_t t = 0; t < ell; ++t) {
+                hw[j * nout + t] = st.u[j * ell + t];
+                hw[j * nout + ell + t] = st.v[j * ell + t];
+            }
+        DeviceBuffer<double> W(hw.size(), s);
+        ISDF_CUDA(cudaMemcpyAsync(W.get(), hw.data(), hw.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        st.Pd.reset(static_cast<size_t>(n) * naxes * nout, s);
+        const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(n, std::max<int64_t>(1024, (int64_t(1) << 28) / d)));
+        DeviceBuffer<double> F(static_cast<size_t>(chunk * d), s);
+        for (int64_t g0 = 0; g0 < n; g0 += chunk) {
+            const int64_t b = std::min(chunk, n - g0);
+            eval_axis_features<double>(c, pts, st.kp.index.get() + g0, b, st.su.ax, F.get(), d, sumsq.get(),
+                                       nullptr, s);
+            gemm_f64(b, nout, c.nao, F.get(), d, c.nao, W.get(), nout, static_cast<int64_t>(c.nao) * nout,
+                     st.Pd.get() + g0 * naxes * nout, naxes * nout, nout, naxes, false, s);
+        }
+        ISDF_CUDA(cudaStreamSynchronize(s));   // host weight image goes out of scope
+    }
+    ISDF_CUDA(cudaMemcpyAsync(st.sumsq, sumsq.get(), sizeof(st.sumsq), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+}
+
+void sketch_shard_combine(const Context& c, SketchShard& st, const double* sumsq_global, double* Yt,
+                          double* delta, int64_t* kept_out, double* kept_xyz, double* kept_w,
+                          std::vector<double>& scales, cudaStream_t s) {
+    const int64_t n = st.kp.n, ell = st.su.ell;
+    const int naxes = st.su.ax.naxes;
+    const double* aw = st.o.axis_weights.empty() ? nullptr : st.o.axis_weights.data();
+    scales.assign(naxes, 1.0);
+    // every shard derives the same scales from the same global sums
+    if (naxes > 1) scales = axis_scales_from_sumsq(st.su.ax, sumsq_global, aw, true);
+    if (n == 0) return;
+    DeviceBuffer<double> dsc(naxes, s);
+    ISDF_CUDA(cudaMemcpyAsync(dsc.get(), scales.data(), naxes * sizeof(double), cudaMemcpyHostToDevice, s));
+    DeviceBuffer<int> bad(1, s);
+    bad.zero(s);
+    if (st.su.mixed) {
+        require(delta != nullptr, "the mixed sketch needs its per-column error bounds");
+        DeviceBuffer<int> dcomp(naxes, s);
+        ISDF_CUDA(cudaMemcpyAsync(dcomp.get(), st.su.ax.comp, naxes * sizeof(int), cudaMemcpyHostToDevice, s));
+        ISDF_PROFILE("sketch_combine", s);
+        combine_mixed_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(
+            st.Pf.get(), st.psq.get(), naxes, dcomp.get(), ell, naxes > 1 ? dsc.get() : nullptr, st.w,
+            st.kp.index.get(), n, Yt, n, delta, bad.get());
+        ISDF_LAUNCH_CHECK();
+        ISDF_CUDA(cudaStreamSynchronize(s));
+    } else {
+        ISDF_PROFILE("sketch_combine", s);
+        combine_sketch_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(
+            st.Pd.get(), naxes, ell, naxes > 1 ? dsc.get() : nullptr, st.w, st.kp.index.get(), n, Yt, n,
+            bad.get());
+        ISDF_LAUNCH_CHECK();
+        if (delta) ISDF_CUDA(cudaMemsetAsync(delta, 0, n * sizeof(double), s));
+    }
+    if (kept_out)
+        ISDF_CUDA(cudaMemcpyAsync(kept_out, st.kp.index.get(), n * sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
+    if (kept_xyz && kept_w) gather_points(st.pts, st.w, st.kp.index.get(), n, st.ng, kept_xyz, kept_w, s);
+    int hbad = 0;
+    ISDF_CUDA(cudaMemcpyAsync(&hbad, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    if (hbad) fail(kOverflow, "non-finite randomized ID sketch");
+}
+
+std::vector<int64_t> select_sketch_gathered(const Context& c, const SelectOptions& o, double* Yt, int64_t n,
+                                            const double* kept_xyz, const double* kept_w, double* delta,
+                                            const std::vector<double>& scales, SketchDiagnostics* diag_out,
+                                            cudaStream_t s) {
+    if (n == 0) return {};
+    const SketchSetup su = sketch_setup(c, o, n);
+    require(static_cast<int>(scales.size()) == su.ax.naxes, "one scale per axis entry is required");
+    SketchQR qr;
+    if (delta && su.mixed) {
+        // FP64 re-verification source over the gathered kept points
+        std::vector<double> u, v;
+        sketch_factors(su.d, su.ell, o.seed, u, v);
+        const int64_t d = su.d, nout = 2 * su.ell;
+        std::vector<double> hwt(static_cast<size_t>(d * nout));
+        for (int64_t j = 0; j < d; ++j)
+            for (int64_t t = 0; t < su.ell; ++t) {
+                hwt[t * d + j] = u[j * su.ell + t];
+                hwt[(su.ell + t) * d + j] = v[j * su.ell + t];
+            }
+        DeviceBuffer<double> WT(hwt.size(), s), dsc(scales.size(), s);
+        DeviceBuffer<int64_t> idx(n, s);
+        ISDF_CUDA(cudaMemcpyAsync(WT.get(), hwt.data(), hwt.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        ISDF_CUDA(cudaMemcpyAsync(dsc.get(), scales.data(), scales.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        iota_i64(idx.get(), n, s);
+        ExactSketchSource src;
+        src.ctx = &c;
+        src.naxes = su.ax.naxes;
+        for (int a = 0; a < su.ax.naxes; ++a) src.comp[a] = su.ax.comp[a];
+        src.scales = dsc.get();
+        src.WT = WT.get();
+        src.pts = kept_xyz;
+        src.index = idx.get();
+        src.w = kept_w;
+        src.ell = su.ell;
+        src.delta = delta;
+        qr = qrcp_sketch(Yt, n, su.ell, n, s, &src);
+    } else {
+        qr = qrcp_sketch(Yt, n, su.ell, n, s);
+    }
+    const SketchRank r = sketch_rank(qr, su.ell, n, o, su.physical_rank);
+    fill_diag(diag_out, su.ell, r, qr);
+    return std::vector<int64_t>(qr.jpvt.begin(), qr.jpvt.begin() + r.rank);
 }
 
 }  // namespace isdf

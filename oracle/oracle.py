@@ -286,25 +286,12 @@ def select_qrcp_dense(ctx, pts, w, axes, tolerance=1e-10, max_rank=0, scales=Non
     return out
 
 
-def select_rand_sketch(ctx, pts, w, axes, tolerance=1e-10, max_rank=0, sketch_size=128,
-                       oversampling=16, seed=7, scales=None, return_details=False):
-    """Quadrature Khatri-Rao sketch + dgeqp3 (``anchor_select_randomized_id.cpp``)."""
+def sketch_qr_rank(y, ell, oversampling, tolerance, max_rank, physical_rank):
+    """dgeqp3 of the sketch Y (y: [n, ell]) and the rank rule of
+    ``anchor_select_randomized_id.cpp:320-374``: (positions 0..n-1, details)."""
     from scipy.linalg.lapack import dgeqp3
-    if oversampling == 0 or (not max_rank and sketch_size <= oversampling):
-        raise ValueError("invalid randomized ID grid, tolerance, batch, sketch or rank/oversampling")
-    w = np.asarray(w, float)
-    keep = np.flatnonzero(w != 0)
-    d = len(axes) * ctx.nao
-    ell = max_rank + oversampling if max_rank else sketch_size
-    n = len(keep)
-    if n == 0:
-        return ([], {}) if return_details else []
-    physical_rank = d * (d + 1) // 2
-    if max_rank > min(n, physical_rank):
-        raise ValueError("requested anchor_rank exceeds eligible candidates or physical pair rank")
-    u, v = sketch_factors(d, ell, seed)
-    y = ctx.sketch(pts[keep], w[keep], axes, scales, u, v, ell)   # [n, ell]
-    ymat = np.asfortranarray(y.T)                                  # ell x n column-major
+    n = len(y)
+    ymat = np.asfortranarray(np.asarray(y, float).T)              # ell x n column-major
     qr_, jpvt, tau, work, info = dgeqp3(ymat)
     if info != 0:
         raise RuntimeError("dgeqp3 failed")
@@ -332,6 +319,30 @@ def select_rand_sketch(ctx, pts, w, axes, tolerance=1e-10, max_rank=0, sketch_si
             if tails[i] <= tolerance * norm:
                 rank = i
                 break
+    pos = [int(jpvt[i] - 1) for i in range(rank)]
+    return pos, dict(jpvt=jpvt - 1, diag=diag, tails=tails, numerical_rank=numerical_rank)
+
+
+def select_rand_sketch(ctx, pts, w, axes, tolerance=1e-10, max_rank=0, sketch_size=128,
+                       oversampling=16, seed=7, scales=None, return_details=False):
+    """Quadrature Khatri-Rao sketch + dgeqp3 (``anchor_select_randomized_id.cpp``)."""
+    if oversampling == 0 or (not max_rank and sketch_size <= oversampling):
+        raise ValueError("invalid randomized ID grid, tolerance, batch, sketch or rank/oversampling")
+    w = np.asarray(w, float)
+    keep = np.flatnonzero(w != 0)
+    d = len(axes) * ctx.nao
+    ell = max_rank + oversampling if max_rank else sketch_size
+    n = len(keep)
+    if n == 0:
+        return ([], {}) if return_details else []
+    physical_rank = d * (d + 1) // 2
+    if max_rank > min(n, physical_rank):
+        raise ValueError("requested anchor_rank exceeds eligible candidates or physical pair rank")
+    u, v = sketch_factors(d, ell, seed)
+    y = ctx.sketch(pts[keep], w[keep], axes, scales, u, v, ell)   # [n, ell]
+    pos, det = sketch_qr_rank(y, ell, oversampling, tolerance, max_rank, physical_rank)
+    jpvt, diag, tails, numerical_rank = det["jpvt"] + 1, det["diag"], det["tails"], det["numerical_rank"]
+    rank = len(pos)
     piv = [int(keep[jpvt[i] - 1]) for i in range(rank)]
     if return_details:
         return piv, dict(y=y, diag=diag, tails=tails, numerical_rank=numerical_rank,
@@ -400,7 +411,8 @@ def gram_fit(ctx, coords, weights, anchor_coords, anchor_weights):
                            _p(np.ascontiguousarray(anchor_weights, float)), _p(theta),
                            _p(err2), _p(ex2))
     err2 = max(err2[0], 0.0)
-    return theta, {"l2": np.sqrt(err2), "relative": np.sqrt(err2 / ex2[0]) if ex2[0] else 0.0}
+    return theta, {"l2": np.sqrt(err2), "relative": np.sqrt(err2 / ex2[0]) if ex2[0] else 0.0,
+                   "err2": err2, "exact2": float(ex2[0])}
 
 
 # ---------------------------------------------------------------------------

@@ -1,0 +1,149 @@
+"""Grid-sharded selection + fit (mp_isdf_b200.sharded).
+
+CPU: two gloo ranks run the protocol with the oracle backend and must give
+the single-process oracle's anchors, Theta columns and pair error.  GPU: the
+library's sharded phases with two shards in one process (threads standing in
+for ranks, no collectives between kernels) against isdf_select_fit on the
+whole grid.
+"""
+import json
+import os
+import socket
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+KW = dict(axes=("ao", "dx", "dy", "dz"), axis_weights=[1.0, 0.5, 0.5, 0.5], max_rank=6, oversampling=8,
+          seed=4)
+
+
+def _system():
+    from mp_isdf_b200 import inputs
+    symbols, xyz = inputs.water_cluster((2, 1, 1), seed=11)
+    mol = inputs.build_tables(symbols, xyz)
+    pts, w = inputs.becke_grid(symbols, xyz, level=0)
+    return mol, pts, w
+
+
+def _split(ng, size):
+    edges = np.linspace(0, ng, size + 1).astype(int)
+    return [(edges[r], edges[r + 1]) for r in range(size)]
+
+
+def _gloo_rank(rank, size, port, out_dir):
+    import torch
+    import torch.distributed as dist
+    from mp_isdf_b200.sharded import TorchComm, select_fit_sharded
+    from sharded_helpers import OracleBackend
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=size)
+    try:
+        mol, pts, w = _system()
+        lo, hi = _split(len(pts), size)[rank]
+        res = select_fit_sharded(OracleBackend(mol), TorchComm(), torch.as_tensor(pts[lo:hi]),
+                                 torch.as_tensor(w[lo:hi]), lo, len(pts), **KW)
+        np.save(os.path.join(out_dir, f"theta{rank}.npy"), res.theta.numpy())
+        with open(os.path.join(out_dir, f"res{rank}.json"), "w") as f:
+            json.dump({"anchors": res.anchors.tolist(), "pair_relative": res.pair_relative,
+                       "kept_offset": res.kept_offset, "counts": res.counts}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_gloo_two_ranks_match_single_process():
+    import torch.multiprocessing as mp
+    from oracle import oracle as O
+    mol, pts, w = _system()
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_gloo_rank, args=(2, _free_port(), d), nprocs=2, join=True, start_method="spawn")
+        res = [json.load(open(os.path.join(d, f"res{r}.json"))) for r in range(2)]
+        thetas = [np.load(os.path.join(d, f"theta{r}.npy")) for r in range(2)]
+    assert res[0]["anchors"] == res[1]["anchors"]
+    assert res[0]["counts"][0] > 0 and res[0]["counts"][1] > 0
+    oc = O.OracleContext(mol.atm, mol.bas, mol.env)
+    codes = [O.AXIS_CODES[a] for a in KW["axes"]]
+    scales = O.axis_scales(oc, pts, w, codes, KW["axis_weights"])
+    ref = O.select_rand_sketch(oc, pts, w, codes, max_rank=KW["max_rank"], oversampling=KW["oversampling"],
+                               seed=KW["seed"], scales=scales)
+    assert res[0]["anchors"] == ref
+    keep = w != 0
+    theta_ref, err = O.gram_fit(oc, pts[keep], w[keep], pts[ref], w[ref])
+    theta = np.concatenate(thetas, axis=1)
+    np.testing.assert_allclose(theta, theta_ref, rtol=1e-9, atol=1e-9 * np.abs(theta_ref).max())
+    np.testing.assert_allclose(res[0]["pair_relative"], err["relative"], rtol=1e-10)
+    np.testing.assert_allclose(res[1]["pair_relative"], err["relative"], rtol=1e-10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_cuda_phases_two_shards_match_select_fit(precision):
+    import threading
+    import torch
+    from mp_isdf_b200 import capi
+    from mp_isdf_b200.sharded import CudaBackend, select_fit_sharded
+    from sharded_helpers import ThreadComm
+    mol, pts, w = _system()
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    x = torch.tensor(pts, device="cuda")
+    wt = torch.tensor(w, device="cuda")
+    theta = torch.zeros(KW["max_rank"] * len(pts), dtype=torch.float64, device="cuda")
+    piv, _, finfo = ctx.select_fit(x, wt, theta, want_error=True, precision=precision, **KW)
+    torch.cuda.synchronize()
+    size = 2
+    shared = ThreadComm.Shared(size)
+    results, errors = [None] * size, []
+
+    def run(rank):
+        try:
+            torch.cuda.set_device(0)
+            c = capi.Context(mol.atm, mol.bas, mol.env)
+            lo, hi = _split(len(pts), size)[rank]
+            results[rank] = select_fit_sharded(CudaBackend(c), ThreadComm(rank, size, shared),
+                                               x[lo:hi].contiguous(), wt[lo:hi].contiguous(), lo, len(pts),
+                                               precision=precision, **KW)
+            torch.cuda.synchronize()
+        except Exception as e:  # surfaced below
+            errors.append(e)
+            shared.barrier.abort()
+
+    threads = [threading.Thread(target=run, args=(r,)) for r in range(size)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    np.testing.assert_array_equal(results[0].anchors, piv)
+    np.testing.assert_array_equal(results[1].anchors, piv)
+    th_sharded = torch.cat([r.theta for r in results], dim=1).cpu().numpy()
+    k, n = len(piv), finfo.n_kept
+    th_ref = theta[:k * n].view(k, n).cpu().numpy()
+    scale = max(1.0, finfo.condition) ** 2
+    rel = np.abs(th_sharded - th_ref).max() / np.abs(th_ref).max()
+    assert rel <= (1e-5 if precision == "mixed" else 1e-12) * scale, rel
+    assert abs(results[0].pair_relative - finfo.pair_relative) <= 1e-8 * finfo.pair_relative
+
+
+@pytest.mark.gpu
+def test_cuda_single_rank_local_comm():
+    import torch
+    from mp_isdf_b200 import capi
+    from mp_isdf_b200.sharded import CudaBackend, LocalComm, select_fit_sharded
+    mol, pts, w = _system()
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    x = torch.tensor(pts, device="cuda")
+    wt = torch.tensor(w, device="cuda")
+    res = select_fit_sharded(CudaBackend(ctx), LocalComm(), x, wt, 0, len(pts), precision="mixed", **KW)
+    piv, _ = ctx.select(x, wt, precision="mixed", **KW)
+    np.testing.assert_array_equal(res.anchors, piv)
