@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--mode", choices=("auto", "sharded", "replicas"), default="auto",
+                    help="N > 1: shard one cluster's grid over the ranks (auto, for rand_sketch "
+                         "configs) or run one cluster per rank")
     ap.add_argument("--max-points", type=int, default=0,
                     help="keep every k-th grid point so that at most this many remain "
                          "(small cases for profiling; 0 = full grid)")
@@ -333,9 +336,25 @@ def run_ours(args, rank, world, local_rank):
     def sel_kw(precision):
         return selection_kwargs(cfg, names, factors, precision)
 
-    def step(precision):
-        # selection + fit in one library call (isdf_select_fit)
-        return ctx.select_fit(x, wt, theta, want_error=False, **sel_kw(precision))
+    sharded = cfg["algorithm"] == "rand_sketch" and (
+        args.mode == "sharded" or (args.mode == "auto" and world > 1))
+    if sharded:
+        # one cluster per step, its grid split into contiguous per-rank shards
+        from mp_isdf_b200.sharded import CudaBackend, LocalComm, TorchComm, select_fit_sharded
+        edges = np.linspace(0, n, world + 1).astype(np.int64)
+        lo, hi = int(edges[rank]), int(edges[rank + 1])
+        xs, ws = x[lo:hi].contiguous(), wt[lo:hi].contiguous()
+        comm = TorchComm() if world > 1 else LocalComm()
+        backend = CudaBackend(ctx)
+
+        def step(precision, want_error=False):
+            r = select_fit_sharded(backend, comm, xs, ws, lo, n, want_error=want_error, **sel_kw(precision))
+            return r.anchors, r.select_info, r.fit_info, r
+    else:
+        def step(precision, want_error=False):
+            # selection + fit in one library call (isdf_select_fit)
+            piv, sinfo, finfo = ctx.select_fit(x, wt, theta, want_error=want_error, **sel_kw(precision))
+            return piv, sinfo, finfo, None
 
     results = {}
     for precision in forms:
@@ -356,7 +375,7 @@ def run_ours(args, rank, world, local_rank):
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record()
-            piv, sinfo, finfo = step(precision)
+            piv, sinfo, finfo, _ = step(precision)
             b.record()
             torch.cuda.synchronize()
             times.append(a.elapsed_time(b) / 1e3)
@@ -380,7 +399,11 @@ def run_ours(args, rank, world, local_rank):
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             total = float(t.item())
         # pair-space error of this form's Theta, evaluated with FP64 AO values (untimed)
-        pl2, prel = ctx.pair_error(x, wt, piv, theta)
+        if sharded:
+            _, _, finfo, r = step(precision, want_error=True)
+            pl2, prel = r.pair_l2, r.pair_relative
+        else:
+            pl2, prel = ctx.pair_error(x, wt, piv, theta)
         einfo = {"pair_l2": pl2, "pair_relative": prel, "fit_path": finfo.fit_path,
                  "mixed_bound": finfo.mixed_bound}
         torch.cuda.synchronize()
@@ -390,12 +413,37 @@ def run_ours(args, rank, world, local_rank):
 
     head = forms[0]
     res = results[head]
-    per_cluster = res["total"] / args.steps / world
+    # replicas: each rank times its own cluster; sharded: all ranks one cluster
+    per_cluster = res["total"] / args.steps / (1 if sharded else world)
     launches = sum(c for _, c in res["prof"].values()) // max(args.steps, 1)
 
     # e2e through the host-buffer C-ABI (headline form)
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and sharded:
+        # each rank uploads its shard from pinned memory and downloads its Theta columns
+        pts_h = torch.from_numpy(np.ascontiguousarray(pts[lo:hi])).pin_memory()
+        w_h = torch.from_numpy(np.ascontiguousarray(w[lo:hi])).pin_memory()
+        e2e_times = []
+        for i in range(max(1, min(3, args.steps)) + 1):
+            torch.cuda.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
+            t0 = time.perf_counter()
+            xd = pts_h.to(dev, non_blocking=True)
+            wd = w_h.to(dev, non_blocking=True)
+            r = select_fit_sharded(backend, comm, xd, wd, lo, n, want_error=False, **sel_kw(head))
+            th = r.theta.cpu()
+            dt = time.perf_counter() - t0
+            if i:
+                e2e_times.append(dt)
+        t = torch.tensor([statistics.mean(e2e_times)], device=dev, dtype=torch.float64)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e = {"value": float(t.item()), "unit": "s",
+               "h2d_bytes_per_step": int(pts_h.numel() * 8 + w_h.numel() * 8),
+               "d2h_bytes_per_step": int(th.numel() * 8 + 8 * len(r.anchors)),
+               "path": "grid-sharded select+fit (shard from pinned memory, Theta columns back; max over ranks)"}
+    elif not args.no_e2e:
         # pinned host buffers: inputs copied in by each call, Theta copied out
         pts_h = torch.from_numpy(np.ascontiguousarray(pts)).pin_memory().numpy()
         w_h = torch.from_numpy(np.ascontiguousarray(w)).pin_memory().numpy()
@@ -408,14 +456,14 @@ def run_ours(args, rank, world, local_rank):
             dt = time.perf_counter() - t0
             if i:
                 e2e_times.append(dt)
-        h2d = 2 * (pts_h.nbytes + w_h.nbytes)
+        h2d = pts_h.nbytes + w_h.nbytes
         d2h = th.nbytes + 8 * len(piv_h)
         e2e = {"value": statistics.mean(e2e_times) / world, "unit": "s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "path": "isdf_select_fit_host (pinned host buffers, wall clock)"}
 
     adjoint = None
-    if cfg.get("electrons") and not args.no_adjoint:
+    if cfg.get("electrons") and not args.no_adjoint and world == 1:
         adjoint = time_adjoint(ctx, mol, x, wt, results[head]["piv"], cfg)
 
     if rank != 0:
@@ -492,10 +540,10 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": per_cluster, "unit": "s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["total"] / args.steps * 1e3,
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": False, "scaling": "strong" if sharded else "weak", "vs_baseline": None,
         "dtype": "f64" if head == "fp64" else "bf16x3+f32+f64", "data": "synthetic",
         "config": workload_desc(args.config, cfg, mol, pts, w, names, head)
-        | {"parallelism": f"replicas x{world}"},
+        | {"parallelism": (f"grid shards x{world} (one cluster)" if sharded else f"replicas x{world}")},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": res["clocks"], "kernels": kernels, "forms": forms_out, **extra,
         "adjoint": adjoint,
