@@ -220,12 +220,32 @@ AnchorFactor factor_anchors(const Context& c, const double* anchor_pts, const do
     hadamard_square_kernel<<<blocks_for(k * k), 256, 0, s>>>(S.get(), k * k, f.M.get());
     ISDF_LAUNCH_CHECK();
 
-    // R factor of C^T (nao^2 x k) by CGS2, or the Gram matrix M when C^T is too large.
+    // Singular values of C^T and T = pinv(C C^T) on the retained ones.  First
+    // from the eigen-decomposition of M = C C^T (the route of the FP64 oracle);
+    // when an eigenvalue of M falls below 1e-10 of the largest, a singular
+    // value of C is within ~1e-5 of the cutoff's scale and M's roundoff could
+    // decide it, so the R factor of an explicit CGS2 QR of C^T (nao^2 x k) is
+    // used instead.
     const int64_t m = nao * nao;
-    std::vector<double> R(static_cast<size_t>(k * k), 0.0);   // column-major
-    double power = 2.0;
-    DeviceBuffer<double> A(static_cast<size_t>(k * k), s), V(static_cast<size_t>(k * k), s);
-    if (m * k <= (int64_t(1) << 30)) {
+    double power = 1.0;                 // singular values of M are s^2
+    DeviceBuffer<double> A(static_cast<size_t>(k * k), s), V(static_cast<size_t>(k * k), s), sv(k, s);
+    DeviceBuffer<int> sweeps(1, s);
+    std::vector<double> hs(k);
+    auto svd = [&]() {
+        jacobi_svd_kernel<<<1, 1024, 0, s>>>(A.get(), V.get(), static_cast<int>(k), 60, sweeps.get());
+        ISDF_LAUNCH_CHECK();
+        column_norms_kernel<<<static_cast<unsigned>(k), 32, 0, s>>>(A.get(), static_cast<int>(k), sv.get());
+        ISDF_LAUNCH_CHECK();
+        ISDF_CUDA(cudaMemcpyAsync(hs.data(), sv.get(), k * sizeof(double), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+    };
+    ISDF_CUDA(cudaMemcpyAsync(A.get(), f.M.get(), k * k * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    svd();
+    const double lam_max = *std::max_element(hs.begin(), hs.end());
+    const double lam_min = *std::min_element(hs.begin(), hs.end());
+    f.gram_fallback = true;
+    if (!(lam_min >= 1e-10 * lam_max) && m * k <= (int64_t(1) << 30)) {
+        std::vector<double> R(static_cast<size_t>(k * k), 0.0);   // column-major
         DeviceBuffer<double> Q(static_cast<size_t>(m * k), s), a(m, s), r(m, s), t(k, s), nrm(1, s);
         std::vector<double> ht(k);
         for (int64_t j = 0; j < k; ++j) {
@@ -251,21 +271,10 @@ AnchorFactor factor_anchors(const Context& c, const double* anchor_pts, const do
             scale_copy(r.get(), rjj > 0 ? 1.0 / rjj : 0.0, m, Q.get() + j * m, s);
         }
         ISDF_CUDA(cudaMemcpyAsync(A.get(), R.data(), R.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        svd();
         power = 2.0;   // T = V S^-2 V^T from the SVD of R
-    } else {
-        ISDF_CUDA(cudaMemcpyAsync(A.get(), f.M.get(), k * k * sizeof(double), cudaMemcpyDeviceToDevice, s));
-        power = 1.0;   // singular values of M are s^2
-        f.gram_fallback = true;
+        f.gram_fallback = false;
     }
-    DeviceBuffer<int> sweeps(1, s);
-    jacobi_svd_kernel<<<1, 1024, 0, s>>>(A.get(), V.get(), static_cast<int>(k), 60, sweeps.get());
-    ISDF_LAUNCH_CHECK();
-    DeviceBuffer<double> sv(k, s);
-    column_norms_kernel<<<static_cast<unsigned>(k), 32, 0, s>>>(A.get(), static_cast<int>(k), sv.get());
-    ISDF_LAUNCH_CHECK();
-    std::vector<double> hs(k);
-    ISDF_CUDA(cudaMemcpyAsync(hs.data(), sv.get(), k * sizeof(double), cudaMemcpyDeviceToHost, s));
-    ISDF_CUDA(cudaStreamSynchronize(s));
     if (f.gram_fallback)
         for (auto& x : hs) x = std::sqrt(std::max(x, 0.0));
     f.sv = hs;

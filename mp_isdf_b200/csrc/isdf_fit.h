@@ -15,7 +15,7 @@ struct AnchorFactor {
     std::vector<double> sv;               // singular values of C^T, descending
     int retained = 0;
     double condition = 0;
-    bool gram_fallback = false;           // SVD taken of M instead of R (very large C^T)
+    bool gram_fallback = false;           // singular values from M (well-separated from the cutoff, or C^T too large)
 };
 
 struct FitOutput {
