@@ -170,11 +170,11 @@ __global__ void __launch_bounds__(kPtsPerBlock * kShellLanes)
 ao_raw_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restrict__ exps,
               const T* __restrict__ coefs, const double* __restrict__ pts,
               int64_t n, T* val, T* grad, int64_t ld, bool want_val) {
-    const int64_t p = static_cast<int64_t>(blockIdx.x) * kPtsPerBlock + threadIdx.x;
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const double px = pts[3 * p], py = pts[3 * p + 1], pz = pts[3 * p + 2];
     RawSink<T> sink{val, grad, p, n, ld, want_val};
-    for (int sh = threadIdx.y; sh < nshell; sh += kShellLanes) {
+    for (int sh = threadIdx.y; sh < nshell; sh += blockDim.y) {
         const ShellDesc b = shells[sh];
         eval_shell_any<T, GRAD>(b, px - b.x, py - b.y, pz - b.z, exps, coefs, sink);
     }
@@ -229,8 +229,11 @@ void eval_ao(const Context& c, const double* pts, int64_t n, T* out_val, T* out_
              int64_t ld, cudaStream_t s) {
     if (n == 0 || c.nao == 0) return;
     ISDF_PROFILE(sizeof(T) == 8 ? "ao_eval_f64" : "ao_eval_f32", s);
-    dim3 block(kPtsPerBlock, kShellLanes);
-    const int64_t nb = (n + kPtsPerBlock - 1) / kPtsPerBlock;
+    // few points (anchors, candidate columns): one point per block, its shells
+    // spread over the block; otherwise 32 points x 4 shell lanes
+    const bool few = n <= 2048;
+    const dim3 block = few ? dim3(1, kPtsPerBlock * kShellLanes) : dim3(kPtsPerBlock, kShellLanes);
+    const int64_t nb = (n + block.x - 1) / block.x;
     require(nb < (1ll << 31), "too many grid points for one launch");
     if (out_grad)
         ao_raw_kernel<T, true><<<static_cast<unsigned>(nb), block, 0, s>>>(

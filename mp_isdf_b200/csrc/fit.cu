@@ -105,6 +105,15 @@ jacobi_svd_kernel(double* A, double* V, int k, int max_sweeps, int* sweeps_out) 
 }
 
 // s[j] = |A[:, j]|
+// S[a][b] = phi_a . phi_b for rows a, b of A (k x n), one warp per entry.
+__global__ void gram_rows_kernel(const double* __restrict__ A, int k, int n, double* __restrict__ S) {
+    const int a = blockIdx.x / k, b = blockIdx.x % k;
+    double acc = 0;
+    for (int i = threadIdx.x; i < n; i += 32) acc += A[static_cast<int64_t>(a) * n + i] * A[static_cast<int64_t>(b) * n + i];
+    acc = warp_allsum(acc);
+    if (threadIdx.x == 0) S[blockIdx.x] = acc;
+}
+
 __global__ void column_norms_kernel(const double* __restrict__ A, int k, double* __restrict__ s) {
     const int j = blockIdx.x;
     double acc = 0;
@@ -216,7 +225,14 @@ AnchorFactor factor_anchors(const Context& c, const double* anchor_pts, const do
     transpose_kernel<<<blocks_for(k * nao), 256, 0, s>>>(f.phi_a.get(), k, nao, f.phi_aT.get());
     ISDF_LAUNCH_CHECK();
     DeviceBuffer<double> S(static_cast<size_t>(k * k), s);
-    gemm_f64(k, k, nao, f.phi_a.get(), nao, 0, f.phi_aT.get(), k, 0, S.get(), k, 0, 1, false, s);
+    if (k <= 64) {
+        // a few anchors: one warp per entry of the symmetric k x k Gram
+        gram_rows_kernel<<<static_cast<unsigned>(k * k), 32, 0, s>>>(f.phi_a.get(), static_cast<int>(k),
+                                                                     static_cast<int>(nao), S.get());
+        ISDF_LAUNCH_CHECK();
+    } else {
+        gemm_f64(k, k, nao, f.phi_a.get(), nao, 0, f.phi_aT.get(), k, 0, S.get(), k, 0, 1, false, s);
+    }
     hadamard_square_kernel<<<blocks_for(k * k), 256, 0, s>>>(S.get(), k * k, f.M.get());
     ISDF_LAUNCH_CHECK();
 
