@@ -374,6 +374,8 @@ namespace {
 // |dG_ga| <= kFitGramBound |phi_g| |phi_a|  (dh = 2 G dG + dG^2).
 constexpr double kFitGramBound = 2e-5;
 
+// KMAX >= k: the per-point vectors stay in registers (loops unrolled to KMAX).
+template <int KMAX>
 __global__ void __launch_bounds__(256)
 fit_mixed_kernel(const float* __restrict__ G, const float* __restrict__ psq, int64_t n, int k,
                  const double* __restrict__ T, const double* __restrict__ M,
@@ -391,40 +393,59 @@ fit_mixed_kernel(const float* __restrict__ G, const float* __restrict__ psq, int
     __syncthreads();
     const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     double mx = 0, dh2 = 0, e2 = 0, q2 = 0;
+    double h[KMAX], x[KMAX], twl[KMAX];
+#pragma unroll
+    for (int a = 0; a < KMAX; ++a) { h[a] = 0.0; x[a] = 0.0; twl[a] = 0.0; }
     if (g < n) {
-        double h[64], x[64];
         const double qg = static_cast<double>(psq[g * 4]);   // |phi_g|^2
         const double fn = sqrt(qg);
-        const double aw = fabs(w[index[g]]);
-        for (int a = 0; a < k; ++a) {
-            const double gv = static_cast<double>(G[g * k + a]);
-            h[a] = gv * gv;
-            const double dG = kFitGramBound * fn * anorm[a];
-            const double dh = 2.0 * fabs(gv) * dG + dG * dG;
-            dh2 += dh * dh;
-        }
-        const double wg = w[index[g]];
+        const int64_t gi = index[g];
+        const double wg = w[gi], aw = fabs(wg);
+#pragma unroll
+        for (int a = 0; a < KMAX; ++a)
+            if (a < k) {
+                const double gv = static_cast<double>(G[g * k + a]);
+                h[a] = gv * gv;
+                const double dG = kFitGramBound * fn * anorm[a];
+                const double dh = 2.0 * fabs(gv) * dG + dG * dG;
+                dh2 += dh * dh;
+            }
         double xh = 0;
-        for (int a = 0; a < k; ++a) {
-            double xa = 0;
-            for (int b = 0; b < k; ++b) xa += Ts[a * k + b] * h[b];
-            x[a] = xa;
-            xh += xa * h[a];
-            mx = fmax(mx, fabs(xa));
-            const double th = xa / wa[a];
-            theta[a * ldt + g] = th;
-            atomicAdd(&tws[a], th * wg);
-        }
+#pragma unroll
+        for (int a = 0; a < KMAX; ++a)
+            if (a < k) {
+                double xa = 0;
+#pragma unroll
+                for (int b = 0; b < KMAX; ++b)
+                    if (b < k) xa += Ts[a * k + b] * h[b];
+                x[a] = xa;
+                xh += xa * h[a];
+                mx = fmax(mx, fabs(xa));
+                const double th = xa / wa[a];
+                theta[a * ldt + g] = th;
+                twl[a] = th * wg;
+            }
         double xmx = 0;
-        for (int a = 0; a < k; ++a) {
-            double t = 0;
-            for (int b = 0; b < k; ++b) t += Ms[a * k + b] * x[b];
-            xmx += x[a] * t;
-        }
+#pragma unroll
+        for (int a = 0; a < KMAX; ++a)
+            if (a < k) {
+                double t = 0;
+#pragma unroll
+                for (int b = 0; b < KMAX; ++b)
+                    if (b < k) t += Ms[a * k + b] * x[b];
+                xmx += x[a] * t;
+            }
         dh2 *= aw;
         e2 = aw * (qg * qg - 2.0 * xh + xmx);
         q2 = aw * qg * qg;
     }
+    // Theta.w partial sums: warp reduction, one shared-memory add per warp
+#pragma unroll
+    for (int a = 0; a < KMAX; ++a)
+        if (a < k) {
+            const double v = warp_sum(twl[a]);
+            if (threadIdx.x % 32 == 0) atomicAdd(&tws[a], v);
+        }
     dh2 = block_sum<256>(dh2, red);
     e2 = block_sum<256>(e2, red);
     q2 = block_sum<256>(q2, red);
@@ -490,7 +511,8 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
     {
         ISDF_PROFILE("fit_mixed", s);
         const size_t smem = static_cast<size_t>(2 * k * k + k) * sizeof(double);
-        fit_mixed_kernel<<<blocks_for(n), 256, smem, s>>>(G.get(), point_sq, n, static_cast<int>(k),
+        auto kern = k <= 16 ? fit_mixed_kernel<16> : k <= 32 ? fit_mixed_kernel<32> : fit_mixed_kernel<64>;
+        kern<<<blocks_for(n), 256, smem, s>>>(G.get(), point_sq, n, static_cast<int>(k),
                                                           f.T.get(), f.M.get(), anorm.get(), f.wa.get(),
                                                           w, kp.index.get(), theta, ldt, tw.get(),
                                                           acc.get());
