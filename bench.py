@@ -369,6 +369,7 @@ def run_ours(args, rank, world, local_rank):
         sampler.start()
         times = []
         prof_all, step_phases = {}, []
+        launches0 = capi.launch_count()
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -386,6 +387,7 @@ def run_ours(args, rank, world, local_rank):
                 acc = prof_all.setdefault(name, [0.0, 0])
                 acc[0] += ms
                 acc[1] += cnt
+        launched = capi.launch_count() - launches0
         clocks = sampler.stop()
         capi.profile_enable(False)
         prof_all = {k: tuple(v) for k, v in prof_all.items()}
@@ -408,6 +410,7 @@ def run_ours(args, rank, world, local_rank):
                  "mixed_bound": finfo.mixed_bound}
         torch.cuda.synchronize()
         results[precision] = dict(total=total, times=times, prof=prof, phases=phases, step_phases=step_phases,
+                                  launches=launched / max(args.steps, 1),
                                   clocks=clocks,
                                   piv=[int(p) for p in piv], sinfo=sinfo, einfo=einfo)
 
@@ -415,7 +418,7 @@ def run_ours(args, rank, world, local_rank):
     res = results[head]
     # replicas: each rank times its own cluster; sharded: all ranks one cluster
     per_cluster = res["total"] / args.steps / (1 if sharded else world)
-    launches = sum(c for _, c in res["prof"].values()) // max(args.steps, 1)
+    launches = int(round(res["launches"]))   # this library's kernel launches per timed step
 
     # e2e through the host-buffer C-ABI (headline form)
     e2e = None

@@ -263,6 +263,9 @@ int isdf_project_axes(isdf_ctx* ctx, const double* xyz_dev, int64_t ng, const in
  * default.  isdf_profile_read synchronises the recorded events, returns up to
  * `max` families sorted by total time (names: 48 bytes each) and clears the
  * record. */
+/* Number of kernels this library has launched in the process so far (all
+ * devices); differences around a call count its launches. */
+int64_t isdf_launch_count(void);
 int isdf_profile_enable(int32_t on);
 int isdf_profile_read(int32_t max, char* names, double* total_ms, int64_t* launches, int32_t* count);
 

@@ -27,7 +27,7 @@ SYMBOLS = [
     "isdf_fit", "isdf_fit_host", "isdf_pair_error", "isdf_pair_error_terms",
     "isdf_profile_enable", "isdf_profile_read", "isdf_project_axes",
     "isdf_energy_gradient", "isdf_ctx_set_coords", "isdf_pair_error_terms_noalloc",
-    "isdf_select_fit", "isdf_select_fit_host",
+    "isdf_select_fit", "isdf_select_fit_host", "isdf_launch_count",
     "isdf_sketch_shard_project", "isdf_sketch_shard_combine", "isdf_sketch_shard_free",
     "isdf_sketch_select_gathered", "isdf_fit_at",
 ]
@@ -110,6 +110,8 @@ def lib():
         L.isdf_energy_gradient.argtypes = [P, P, P, I64, P, I64, P, ctypes.POINTER(F64), P, P]
         L.isdf_ctx_set_coords.argtypes = [P, P]
         L.isdf_profile_enable.argtypes = [I32]
+        L.isdf_launch_count.argtypes = []
+        L.isdf_launch_count.restype = I64
         L.isdf_profile_read.argtypes = [I32, P, P, P, ctypes.POINTER(I32)]
         _lib = L
     return _lib
@@ -407,6 +409,11 @@ def make_select_args(algorithm="rand_sketch", axes=("ao",), axis_weights=None, t
     args.precision = 1 if precision == "mixed" else 0
     args.debug = int(debug)
     return args, (ax, aw)
+
+
+def launch_count():
+    """Kernels launched by the library so far in this process."""
+    return int(lib().isdf_launch_count())
 
 
 def profile_enable(on=True):

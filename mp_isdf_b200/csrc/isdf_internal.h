@@ -40,7 +40,13 @@ inline void require(bool ok, const std::string& msg) { if (!ok) fail(kInvalid, m
         if (err__ != cudaSuccess)                                                        \
             ::isdf::fail(::isdf::kCuda, std::string(#expr) + ": " + cudaGetErrorString(err__)); \
     } while (0)
-#define ISDF_LAUNCH_CHECK() ISDF_CUDA(cudaGetLastError())
+// Counts this library's kernel launches (isdf_launch_count) and checks them.
+void count_launches(int64_t k);
+#define ISDF_LAUNCH_CHECK()                  \
+    do {                                     \
+        ISDF_CUDA(cudaGetLastError());       \
+        ::isdf::count_launches(1);           \
+    } while (0)
 
 // ---- profiling -----------------------------------------------------------------
 // Scoped CUDA-event pair around the launches of one kernel family (no-op

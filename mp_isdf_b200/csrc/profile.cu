@@ -38,6 +38,12 @@ cudaEvent_t take_event() {
 
 bool profiling_enabled() { return g_enabled.load(std::memory_order_relaxed); }
 
+namespace {
+std::atomic<int64_t> g_launches{0};
+}  // namespace
+
+void count_launches(int64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
 ProfileScope::ProfileScope(const char* name, cudaStream_t s) : name_(name), s_(s) {
     if (!profiling_enabled()) return;
     std::lock_guard<std::mutex> lk(g_mu);
@@ -56,6 +62,8 @@ ProfileScope::~ProfileScope() {
 }  // namespace isdf
 
 extern "C" {
+
+int64_t isdf_launch_count(void) { return isdf::g_launches.load(std::memory_order_relaxed); }
 
 int isdf_profile_enable(int32_t on) {
     isdf::g_enabled.store(on != 0);

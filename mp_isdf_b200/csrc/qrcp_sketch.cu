@@ -352,6 +352,7 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
         if (exact) {
             ISDF_PROFILE("qrcp_sketch_verify", s);
             lb_reduce_kernel<<<1, 1024, 0, s>>>(lbp.get(), nblocks, lb.get());
+            ISDF_LAUNCH_CHECK();
             count.zero(s);
             candidates_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(st, lb.get(), cand.get(),
                                                                                       count.get());

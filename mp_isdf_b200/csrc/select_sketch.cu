@@ -64,6 +64,7 @@ KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStr
     DeviceBuffer<char> tmp(tmp_bytes, s);
     ISDF_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tmp_bytes, it, keep.get(), kp.index.get(),
                                          count.get(), n, s));
+    count_launches(2);   // the selection's initialisation and sweep kernels
     int hbad = 0;
     int64_t hcount = 0;
     ISDF_CUDA(cudaMemcpyAsync(&hbad, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
