@@ -257,6 +257,13 @@ int isdf_project_axes(isdf_ctx* ctx, const double* xyz_dev, int64_t ng, const in
                       int32_t naxes, const double* W_host, int32_t nout, int32_t precision,
                       double* out_dev, void* stream);
 
+/* Gaussian sketch factors of rand_sketch: U, V (d x ell, row-major u[a*ell+s])
+ * from std::mt19937_64(seed) and std::mt19937_64(seed ^ 0x9e3779b97f4a7c15)
+ * through std::normal_distribution<double>
+ * (cpp/src/anchor_select_randomized_id.cpp:269-279).  Host only, no device
+ * work; u_host and v_host hold d*ell doubles each. */
+int isdf_sketch_factors(int64_t d, int64_t ell, uint64_t seed, double* u_host, double* v_host);
+
 /* ---- profiling ---------------------------------------------------------------
  * No counterpart in the reference beyond its per-stage wall times
  * (python/isdf.py:384-396): CUDA-event timing per kernel family, off by

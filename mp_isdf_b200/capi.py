@@ -27,7 +27,7 @@ SYMBOLS = [
     "isdf_fit", "isdf_fit_host", "isdf_pair_error", "isdf_pair_error_terms",
     "isdf_profile_enable", "isdf_profile_read", "isdf_project_axes",
     "isdf_energy_gradient", "isdf_ctx_set_coords", "isdf_pair_error_terms_noalloc",
-    "isdf_select_fit", "isdf_select_fit_host", "isdf_launch_count",
+    "isdf_select_fit", "isdf_select_fit_host", "isdf_launch_count", "isdf_sketch_factors",
     "isdf_sketch_shard_project", "isdf_sketch_shard_combine", "isdf_sketch_shard_free",
     "isdf_sketch_select_gathered", "isdf_fit_at",
 ]
@@ -112,6 +112,7 @@ def lib():
         L.isdf_profile_enable.argtypes = [I32]
         L.isdf_launch_count.argtypes = []
         L.isdf_launch_count.restype = I64
+        L.isdf_sketch_factors.argtypes = [I64, I64, ctypes.c_uint64, P, P]
         L.isdf_profile_read.argtypes = [I32, P, P, P, ctypes.POINTER(I32)]
         _lib = L
     return _lib
@@ -409,6 +410,14 @@ def make_select_args(algorithm="rand_sketch", axes=("ao",), axis_weights=None, t
     args.precision = 1 if precision == "mixed" else 0
     args.debug = int(debug)
     return args, (ax, aw)
+
+
+def sketch_factors(d, ell, seed):
+    """The rand_sketch Gaussian factors U, V (d x ell each), computed on the host."""
+    u = np.empty((d, ell), dtype=np.float64)
+    v = np.empty((d, ell), dtype=np.float64)
+    check(lib().isdf_sketch_factors(d, ell, seed, u.ctypes.data, v.ctypes.data))
+    return u, v
 
 
 def launch_count():

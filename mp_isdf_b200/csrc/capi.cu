@@ -3,6 +3,7 @@
 #include "isdf_adjoint.h"
 #include "isdf_fit.h"
 #include "isdf_project.h"
+#include "isdf_select.h"
 
 #include <cstdio>
 #include <cstring>
@@ -544,6 +545,14 @@ int isdf_ctx_set_coords(isdf_ctx* ctx, const double* coords) {
         if (!coords) isdf::fail(isdf::kInvalid, "null coordinates");
         ISDF_CUDA(cudaDeviceSynchronize());
         isdf::set_atom_coords(c, coords);
+    });
+}
+
+int isdf_sketch_factors(int64_t d, int64_t ell, uint64_t seed, double* u_host, double* v_host) {
+    return guarded([&] {
+        isdf::require(d >= 0 && ell >= 0, "sketch factor sizes must be non-negative");
+        isdf::require(d * ell == 0 || (u_host && v_host), "null output buffer");
+        isdf::sketch_factors(d, ell, seed, u_host, v_host);
     });
 }
 

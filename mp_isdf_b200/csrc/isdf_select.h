@@ -68,6 +68,9 @@ AxisSpec make_axis_spec(const Context& c, const int32_t* axes, int naxes);
 void validate_axis_weights(const double* axis_weights, int naxes);
 std::vector<double> axis_scales_from_sumsq(const AxisSpec& ax, const double* sumsq4,
                                            const double* axis_weights, bool any_eligible);
+// Gaussian sketch factors U, V (d x ell, u[a*ell+s]): std::normal_distribution
+// over std::mt19937_64(seed) and std::mt19937_64(seed ^ 0x9e3779b97f4a7c15).
+void sketch_factors(int64_t d, int64_t ell, uint64_t seed, double* u, double* v);
 void sketch_factors(int64_t d, int64_t ell, uint64_t seed, std::vector<double>& u,
                     std::vector<double>& v);
 

@@ -27,6 +27,9 @@ namespace {
 
 constexpr int kQrThreads = 256;
 constexpr int kExactBlocks = 148;   // fixed grid of the candidate re-verification
+constexpr int kRegRows = 32;        // trailing rows the update stages in shared memory
+constexpr int kSplitCands = 16;     // up to this many candidates are split over blocks
+constexpr int kMaxSketchRows = 128;
 
 struct QrState {
     double* Yt; int64_t ldy; int64_t m; int64_t n;
@@ -38,108 +41,171 @@ struct QrState {
     double* diag;        // |R_jj| per step
     double* energy;      // row energies of R per step
     int64_t* jpvt;       // pivot columns per step
-    ArgKey* partial;     // per block
-    double* est;         // verified mode: squared trailing norms
-    double* delta;       // verified mode: error bounds (0 = exact)
-    double* lb_partial;  // verified mode: per-block best lower bound
+    ArgKey* partial;     // per block of the column sweep
+    // verified mode
+    double* est;                  // squared trailing norms
+    double* delta;                // error bounds (0 = exact)
+    unsigned long long* lb_bits;  // best lower bound max(sqrt(est) - delta, 0), as its bits
+    int64_t* count;               // candidates of this step
+    ArgKey* xpartial;             // per re-verification block
 };
 
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
 // Apply reflector j-1 (if j > 0) to every unselected column, accumulate the
-// final row-(j-1) energy and produce per-block argmax keys of the rows j..m-1
-// norms (and, in verified mode, the squared norms and best lower bound).
+// final row-(j-1) energy and form the squared norms of rows j..m-1: as
+// per-block argmax keys, or in verified mode as est[] plus the best lower
+// bound, kept by an atomic max on its bits (non-negative doubles order like
+// their bit patterns).  Row j-1 of an unselected column is final there
+// (R[j-1][g]) and nothing reads it again, so only rows j..m-1 are stored.
+// STAGED: the touched rows (at most kRegRows) are copied once into shared
+// memory (xs[row][thread], cp.async: no registers held while they are in
+// flight) and read from there by the dot product and the update.
+template <bool STAGED>
 __global__ void __launch_bounds__(kQrThreads) qr_update_kernel(QrState st, int64_t j) {
     __shared__ ArgKey ksh[kQrThreads / 32];
     __shared__ double esh[kQrThreads / 32];
     __shared__ double lsh[kQrThreads / 32];
-    const int64_t g = static_cast<int64_t>(blockIdx.x) * kQrThreads + threadIdx.x;
-    ArgKey key = key_none();
-    double e = 0.0, lb = -1.0;
-    if (g < st.n && !st.selected[g]) {
-        double* col = st.Yt + g;
-        const int64_t ld = st.ldy;
-        if (j > 0) {
-            const double t = st.tau[j - 1];
-            const double* v = st.vhist + (j - 1) * st.m;
-            if (t != 0.0) {
-                double dot = 0;
-                for (int64_t i = j - 1; i < st.m; ++i) dot += v[i] * col[i * ld];
-                dot *= t;
-                for (int64_t i = j - 1; i < st.m; ++i) col[i * ld] -= v[i] * dot;
+    __shared__ double vsh[kRegRows];
+    extern __shared__ double xs[];   // STAGED: [kRegRows][kQrThreads]
+    const int tid = threadIdx.x;
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * kQrThreads + tid;
+    const bool verified = st.est != nullptr;
+    const int64_t m = st.m, ld = st.ldy;
+    const int64_t r0 = j > 0 ? j - 1 : 0;   // first row touched
+    const bool active = g < st.n && !st.selected[g];
+    double* col = st.Yt + g;
+    if constexpr (STAGED) {
+        const int cnt = static_cast<int>(m - r0);
+        if (active) {
+            const double* src = col + r0 * ld;
+            for (int i = 0; i < cnt; ++i, src += ld) {
+                const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(&xs[i * kQrThreads + tid]));
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
             }
-            const double r = col[(j - 1) * ld];
-            e = r * r;
         }
-        if (j < st.m) {
-            double nrm = 0;
-            for (int64_t i = j; i < st.m; ++i) { const double x = col[i * ld]; nrm += x * x; }
-            key = ArgKey{nrm, st.pos[g], g};
-            if (st.est) {
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        // the reflector's touched entries, read by every thread
+        if (j > 0 && tid < cnt) vsh[tid] = st.vhist[(j - 1) * m + r0 + tid];
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();
+    }
+    ArgKey key = key_none();
+    double e = 0.0, lb = 0.0;
+    if (active) {
+        const double t = j > 0 ? st.tau[j - 1] : 0.0;
+        double nrm = 0;
+        if constexpr (STAGED) {
+            const int cnt = static_cast<int>(m - r0);
+            const double* x = xs + tid;
+            double dot = 0;
+            if (t != 0.0) {
+                for (int i = 0; i < cnt; ++i) dot += vsh[i] * x[i * kQrThreads];
+                dot *= t;
+            }
+            if (j > 0) {
+                const double x0 = x[0] - vsh[0] * dot;
+                e = x0 * x0;
+            }
+            double* dst = col + j * ld;
+            for (int i = j > 0 ? 1 : 0; i < cnt; ++i, dst += ld) {
+                double xi = x[i * kQrThreads];
+                if (t != 0.0) {
+                    xi -= vsh[i] * dot;
+                    *dst = xi;
+                }
+                nrm += xi * xi;
+            }
+        } else {
+            const double* v = st.vhist + (j > 0 ? (j - 1) * m : 0);
+            double dot = 0;
+            if (t != 0.0) {
+                for (int64_t i = r0; i < m; ++i) dot += v[i] * col[i * ld];
+                dot *= t;
+            }
+            if (j > 0) {
+                const double x0 = col[r0 * ld] - v[r0] * dot;
+                e = x0 * x0;
+            }
+            for (int64_t i = j; i < m; ++i) {
+                double x = col[i * ld];
+                if (t != 0.0) {
+                    x -= v[i] * dot;
+                    col[i * ld] = x;
+                }
+                nrm += x * x;
+            }
+        }
+        if (j < m) {
+            if (verified) {
                 st.est[g] = nrm;
-                lb = sqrt(nrm) - st.delta[g];
+                lb = fmax(sqrt(nrm) - st.delta[g], 0.0);
+            } else {
+                key = ArgKey{nrm, st.pos[g], g};
             }
         }
     }
     e = warp_sum(e);
-    double lw = lb;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) lw = fmax(lw, __shfl_down_sync(0xffffffffu, lw, o));
-    if (threadIdx.x % 32 == 0) { esh[threadIdx.x / 32] = e; lsh[threadIdx.x / 32] = lw; }
-    ArgKey best = block_best<kQrThreads>(key, ksh);
-    if (threadIdx.x == 0) {
-        double et = 0, lt = -1.0;
+    lb = warp_max(lb);
+    if (tid % 32 == 0) { esh[tid / 32] = e; lsh[tid / 32] = lb; }
+    ArgKey best = key_none();
+    if (!verified) best = block_best<kQrThreads>(key, ksh);
+    else __syncthreads();
+    if (tid == 0) {
+        double et = 0, lt = 0.0;
         for (int i = 0; i < kQrThreads / 32; ++i) { et += esh[i]; lt = fmax(lt, lsh[i]); }
         if (j > 0 && et != 0.0) atomicAdd(&st.energy[j - 1], et);
-        st.partial[blockIdx.x] = best;
-        if (st.lb_partial) st.lb_partial[blockIdx.x] = lt;
+        if (!verified) st.partial[blockIdx.x] = best;
+        else if (lt > 0.0) atomicMax(st.lb_bits, static_cast<unsigned long long>(__double_as_longlong(lt)));
     }
 }
 
-// Verified mode: argmax keys from the (partly re-verified) squared norms.
-__global__ void __launch_bounds__(kQrThreads) est_argmax_kernel(QrState st) {
+// Verified mode: every unselected column whose interval reaches the best
+// lower bound (and is not exact yet) is listed for recomputation; the others
+// enter the per-block argmax keys directly.
+__global__ void __launch_bounds__(kQrThreads) candidates_kernel(QrState st, int64_t* cand) {
     __shared__ ArgKey ksh[kQrThreads / 32];
     const int64_t g = static_cast<int64_t>(blockIdx.x) * kQrThreads + threadIdx.x;
+    const double lb = __longlong_as_double(static_cast<long long>(*st.lb_bits));
     ArgKey key = key_none();
-    if (g < st.n && !st.selected[g]) key = ArgKey{st.est[g], st.pos[g], g};
-    ArgKey best = block_best<kQrThreads>(key, ksh);
+    if (g < st.n && !st.selected[g]) {
+        const double d = st.delta[g], e = st.est[g];
+        if (d > 0.0 && sqrt(e) + d >= lb) {
+            const int64_t i = static_cast<int64_t>(
+                atomicAdd(reinterpret_cast<unsigned long long*>(st.count), 1ull));
+            cand[i] = g;
+        } else {
+            key = ArgKey{e, st.pos[g], g};
+        }
+    }
+    const ArgKey best = block_best<kQrThreads>(key, ksh);
     if (threadIdx.x == 0) st.partial[blockIdx.x] = best;
 }
 
-// Verified mode: best lower bound, then the list of columns to recompute.
-__global__ void __launch_bounds__(1024) lb_reduce_kernel(const double* lb_partial, int nblocks,
-                                                         double* lb_out) {
-    __shared__ double sh[32];
-    double v = -1.0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v = fmax(v, lb_partial[b]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    if (threadIdx.x % 32 == 0) sh[threadIdx.x / 32] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < 32; ++i) v = fmax(v, sh[i]);
-        lb_out[0] = v;
-    }
-}
-
-__global__ void candidates_kernel(QrState st, const double* lb, int64_t* cand, int64_t* count) {
-    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (g >= st.n || st.selected[g]) return;
-    const double d = st.delta[g];
-    if (d > 0.0 && sqrt(st.est[g]) + d >= lb[0]) {
-        const int64_t i = static_cast<int64_t>(atomicAdd(reinterpret_cast<unsigned long long*>(count), 1ull));
-        cand[i] = g;
-    }
-}
-
-// Reduce the block keys, record the pivot, swap positions, build reflector j.
-__global__ void __launch_bounds__(1024) qr_pivot_kernel(QrState st, int64_t j, int nblocks) {
+// Reduce the block keys (and, verified, the re-verification blocks' keys),
+// record the pivot, swap positions, build reflector j; then clear the
+// verified-mode step state for step j+1.
+__global__ void __launch_bounds__(1024) qr_pivot_kernel(QrState st, int64_t j, int nblocks, int nxblocks) {
     __shared__ ArgKey ksh[32];
     ArgKey k = key_none();
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
         if (key_better(st.partial[b], k)) k = st.partial[b];
+    for (int b = threadIdx.x; b < nxblocks; b += blockDim.x)
+        if (key_better(st.xpartial[b], k)) k = st.xpartial[b];
     k = block_best<1024>(k, ksh);
     __shared__ int64_t piv;
     __shared__ double sh_scale;
-    if (threadIdx.x == 0) piv = k.col;
+    if (threadIdx.x == 0) {
+        piv = k.col;
+        if (st.count) {
+            *st.count = 0;
+            *st.lb_bits = 0ull;
+        }
+    }
     __syncthreads();
     if (piv < 0) return;   // every column already pivoted (cannot happen for j < min(m, n))
     if (threadIdx.x == 0) {
@@ -198,84 +264,142 @@ struct ExactArgs {
     int64_t ell;
 };
 
-// FP64 recomputation of sketch column g (block-wide; feat holds kNComp*nao
-// AO values, 2*ell projections and m sketch rows).
+// FP64 AO values (and gradients) of grid point gi, component-major in feat.
 template <bool GRAD, int LMAX>
-__device__ void exact_column(const ExactArgs& ea, const QrState& st, int64_t g, int64_t j, double* feat) {
-    constexpr int kNComp = GRAD ? 4 : 1;
-    const int64_t gi = ea.index[g];
-    const int nao = ea.nao;
-    const int64_t d = static_cast<int64_t>(ea.naxes) * nao;
-    double* lr = feat + kNComp * nao;
+__device__ void exact_features(const ExactArgs& ea, int64_t gi, double* feat) {
     const double px = ea.pts[3 * gi], py = ea.pts[3 * gi + 1], pz = ea.pts[3 * gi + 2];
-    CompSink sink{feat, nao};
+    CompSink sink{feat, ea.nao};
     for (int sh = threadIdx.x; sh < ea.nshell; sh += blockDim.x) {
         const ShellDesc b = ea.shells[sh];
         eval_shell_any<double, GRAD, LMAX>(b, px - b.x, py - b.y, pz - b.z, ea.exps, ea.coefs, sink);
     }
     __syncthreads();
-    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
-    // projections lr[s2] = sum_a scale_a comp_a(g) . WT[s2][a]
-    for (int64_t s2 = warp; s2 < 2 * ea.ell; s2 += blockDim.x / 32) {
-        const double* wt = ea.WT + s2 * d;
+}
+
+// Projections lr[s2] = sum_a scale_a comp_a(g) . WT[s2][a] for s2 in
+// [s2a, s2b): one warp per s2 when the range is wide, otherwise the warps
+// split each s2's AO range and add their partial sums (part: >= 256 doubles).
+template <bool GRAD>
+__device__ void exact_projections(const ExactArgs& ea, const double* feat, double* lr, int s2a, int s2b,
+                                  double* part) {
+    const int nao = ea.nao;
+    const int64_t d = static_cast<int64_t>(ea.naxes) * nao;
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nw = blockDim.x / 32;
+    const int cnt = s2b - s2a;
+    const int nseg = max(1, nw / cnt);
+    for (int item = warp; item < cnt * nseg; item += nw) {
+        const int si = item / nseg, seg = item % nseg;
+        const double* wt = ea.WT + (s2a + si) * d;
         double acc = 0;
         for (int a = 0; a < ea.naxes; ++a) {
             const double* f = feat + (GRAD ? ea.comp[a] : 0) * nao;
             const double* wa = wt + static_cast<int64_t>(a) * nao;
             double pa = 0;
-            for (int i = lane; i < nao; i += 32) pa += f[i] * wa[i];
+            for (int i = seg * 32 + lane; i < nao; i += 32 * nseg) pa += f[i] * wa[i];
             acc += ea.scales[a] * pa;
         }
         acc = warp_sum(acc);
-        if (lane == 0) lr[s2] = acc;
+        if (lane == 0) part[item] = acc;
     }
     __syncthreads();
-    // apply the j previous reflectors to the sketch column (warp 0, lanes over rows)
-    if (warp == 0) {
-        const int64_t m = st.m;
-        double* y = lr + 2 * ea.ell;
-        const double sw = sqrt(fabs(ea.w[gi])) / sqrt(static_cast<double>(ea.ell));
-        for (int64_t s = lane; s < m; s += 32) y[s] = sw * lr[s] * lr[ea.ell + s];
-        __syncwarp();
-        for (int64_t i = 0; i < j; ++i) {
-            const double t = st.tau[i];
-            if (t == 0.0) continue;
-            const double* v = st.vhist + i * m;
-            double dot = 0;
-            for (int64_t r = i + lane; r < m; r += 32) dot += v[r] * y[r];
-            dot = warp_allsum(dot) * t;
-            for (int64_t r = i + lane; r < m; r += 32) y[r] -= v[r] * dot;
-            __syncwarp();
-        }
-        double nrm = 0;
-        for (int64_t s = lane; s < m; s += 32) {
-            st.Yt[s * st.ldy + g] = y[s];
-            if (s >= j) nrm += y[s] * y[s];
-        }
-        nrm = warp_sum(nrm);
-        if (lane == 0) {
-            st.est[g] = nrm;
-            st.delta[g] = 0.0;
-        }
+    for (int si = threadIdx.x; si < cnt; si += blockDim.x) {
+        double sum = 0;
+        for (int seg = 0; seg < nseg; ++seg) sum += part[si * nseg + seg];
+        lr[s2a + si] = sum;
     }
+    __syncthreads();
 }
 
-// Re-verifies the candidates cand[0 .. *count) chosen on the device this step;
-// the grid is fixed, so the host needs no count before the launch.
+// Sketch column g from its projections (warp 0): y_s = sw lr[s] lr[ell+s],
+// the j previous reflectors, rows stored, squared trailing norm into est[g]
+// with a zero bound.  Returns the column's argmax key (lane 0).
+__device__ ArgKey exact_finish(const ExactArgs& ea, const QrState& st, int64_t g, int64_t j, const double* lr,
+                               double* y) {
+    const int lane = threadIdx.x % 32;
+    const int64_t m = st.m;
+    const int64_t gi = ea.index[g];
+    const double sw = sqrt(fabs(ea.w[gi])) / sqrt(static_cast<double>(ea.ell));
+    for (int64_t s = lane; s < m; s += 32) y[s] = sw * lr[s] * lr[ea.ell + s];
+    __syncwarp();
+    for (int64_t i = 0; i < j; ++i) {
+        const double t = st.tau[i];
+        if (t == 0.0) continue;
+        const double* v = st.vhist + i * m;
+        double dot = 0;
+        for (int64_t r = i + lane; r < m; r += 32) dot += v[r] * y[r];
+        dot = warp_allsum(dot) * t;
+        for (int64_t r = i + lane; r < m; r += 32) y[r] -= v[r] * dot;
+        __syncwarp();
+    }
+    double nrm = 0;
+    for (int64_t s = lane; s < m; s += 32) {
+        st.Yt[s * st.ldy + g] = y[s];
+        if (s >= j) nrm += y[s] * y[s];
+    }
+    nrm = warp_sum(nrm);
+    ArgKey k = key_none();
+    if (lane == 0) {
+        st.est[g] = nrm;
+        st.delta[g] = 0.0;
+        k = ArgKey{nrm, st.pos[g], g};
+    }
+    return k;
+}
+
+// Re-verifies the candidates cand[0 .. *count) listed on the device this step
+// (fixed grid, so the host needs no count before the launch) and leaves one
+// argmax key per block.  Few candidates: each column's projections are split
+// over several blocks (each evaluates the point's AOs itself); the block that
+// completes a column last, seen by an atomic counter, finishes it.  Many:
+// one block per column.
 template <bool GRAD, int LMAX, int NTHR>
 __global__ void __launch_bounds__(NTHR)
-exact_columns_kernel(ExactArgs ea, QrState st, const int64_t* cand, const int64_t* count, int64_t j,
-                     unsigned long long* total) {
+exact_columns_kernel(ExactArgs ea, QrState st, const int64_t* cand, int64_t j, unsigned long long* total,
+                     double* lr_split, unsigned* done) {
+    constexpr int kNComp = GRAD ? 4 : 1;
     extern __shared__ double feat[];
-    const int64_t nc = *count;
+    __shared__ double part[256];
+    __shared__ int last_sh;
+    double* lr = feat + kNComp * ea.nao;
+    double* y = lr + 2 * ea.ell;
+    const int64_t nc = *st.count;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(total, static_cast<unsigned long long>(nc));
-    for (int64_t ci = blockIdx.x; ci < nc; ci += gridDim.x) {
-        exact_column<GRAD, LMAX>(ea, st, cand[ci], j, feat);
-        __syncthreads();   // feat is reused by the next candidate
+    const int ell2 = static_cast<int>(2 * ea.ell);
+    int nsl = 1;
+    if (nc > 0 && nc <= kSplitCands) nsl = max(1, min(ell2, static_cast<int>(gridDim.x / nc)));
+    const int per = (ell2 + nsl - 1) / nsl;
+    nsl = (ell2 + per - 1) / per;
+    ArgKey best = key_none();
+    for (int64_t it = blockIdx.x; it < nc * nsl; it += gridDim.x) {
+        const int64_t ci = it / nsl;
+        const int sl = static_cast<int>(it % nsl);
+        const int64_t g = cand[ci];
+        const int s2a = sl * per, s2b = min(ell2, s2a + per);
+        exact_features<GRAD, LMAX>(ea, ea.index[g], feat);
+        exact_projections<GRAD>(ea, feat, lr, s2a, s2b, part);
+        if (nsl > 1) {
+            for (int s2 = s2a + threadIdx.x; s2 < s2b; s2 += blockDim.x) lr_split[ci * ell2 + s2] = lr[s2];
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) last_sh = atomicAdd(&done[ci], 1u) == static_cast<unsigned>(nsl - 1);
+            __syncthreads();
+            if (!last_sh) continue;
+            __threadfence();
+            for (int s2 = threadIdx.x; s2 < ell2; s2 += blockDim.x) lr[s2] = __ldcg(&lr_split[ci * ell2 + s2]);
+            if (threadIdx.x == 0) done[ci] = 0u;   // ready for the next step
+            __syncthreads();
+        }
+        if (threadIdx.x < 32) {
+            const ArgKey k = exact_finish(ea, st, g, j, lr, y);
+            if (threadIdx.x == 0 && key_better(k, best)) best = k;
+        }
+        __syncthreads();   // feat is reused by the next item
     }
+    if (threadIdx.x == 0) st.xpartial[blockIdx.x] = best;
 }
 
-using ExactKernelFn = void (*)(ExactArgs, QrState, const int64_t*, const int64_t*, int64_t, unsigned long long*);
+using ExactKernelFn = void (*)(ExactArgs, QrState, const int64_t*, int64_t, unsigned long long*, double*,
+                               unsigned*);
 struct ExactKernel {
     ExactKernelFn fn = nullptr;
     int threads = 0;
@@ -302,33 +426,43 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
     SketchQR out;
     const int64_t steps = std::min(m, n);
     if (steps == 0) return out;
-    if (exact) require(m <= 128, "verified sketch QR supports at most 128 sketch rows");
+    if (exact) require(m <= kMaxSketchRows, "verified sketch QR supports at most 128 sketch rows");
     const int nblocks = static_cast<int>((n + kQrThreads - 1) / kQrThreads);
     DeviceBuffer<int64_t> pos(n, s), col_at(n, s), jpvt(steps, s);
     DeviceBuffer<char> selected(n, s);
     DeviceBuffer<double> vhist(static_cast<size_t>(m * steps), s), tau(steps, s), diag(steps, s),
         energy(steps, s);
-    DeviceBuffer<ArgKey> partial(nblocks, s);
-    DeviceBuffer<double> est, lbp, lb;
+    DeviceBuffer<ArgKey> partial(nblocks, s), xpartial;
+    DeviceBuffer<double> est, lr_split;
+    DeviceBuffer<unsigned long long> lb_bits;
+    DeviceBuffer<unsigned> done;
     DeviceBuffer<int64_t> cand, count;
     selected.zero(s);
     energy.zero(s);
     iota_i64(pos.get(), n, s);
     iota_i64(col_at.get(), n, s);
     QrState st{Yt, ldy, m, n, pos.get(), col_at.get(), selected.get(), vhist.get(), tau.get(),
-               diag.get(), energy.get(), jpvt.get(), partial.get(), nullptr, nullptr, nullptr};
+               diag.get(), energy.get(), jpvt.get(), partial.get(), nullptr, nullptr, nullptr, nullptr,
+               nullptr};
     ExactArgs ea{};
     size_t exact_smem = 0;
     ExactKernel exact_kernel;
     if (exact) {
         est.reset(n, s);
-        lbp.reset(nblocks, s);
-        lb.reset(1, s);
+        lb_bits.reset(1, s);
         cand.reset(n, s);
         count.reset(1, s);
+        xpartial.reset(kExactBlocks, s);
+        lr_split.reset(static_cast<size_t>(kSplitCands) * 2 * exact->ell, s);
+        done.reset(kSplitCands, s);
+        lb_bits.zero(s);
+        count.zero(s);
+        done.zero(s);
         st.est = est.get();
         st.delta = exact->delta;
-        st.lb_partial = lbp.get();
+        st.lb_bits = lb_bits.get();
+        st.count = count.get();
+        st.xpartial = xpartial.get();
         const Context& c = *exact->ctx;
         ea.shells = c.d_shells; ea.nshell = c.nshell; ea.exps = c.d_exp; ea.coefs = c.d_coef;
         ea.nao = c.nao; ea.naxes = exact->naxes; ea.grad = 0;
@@ -342,30 +476,31 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
     }
     DeviceBuffer<unsigned long long> reverified_d(1, s);
     reverified_d.zero(s);
+    constexpr size_t kStagedBytes = static_cast<size_t>(kRegRows) * kQrThreads * sizeof(double);
+    ISDF_CUDA(cudaFuncSetAttribute(qr_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kStagedBytes)));
     for (int64_t j = 0; j <= steps; ++j) {
         {
             ISDF_PROFILE("qrcp_sketch_update", s);
-            qr_update_kernel<<<nblocks, kQrThreads, 0, s>>>(st, j);
+            const int64_t touched = m - (j > 0 ? j - 1 : 0);
+            if (touched <= kRegRows)
+                qr_update_kernel<true><<<nblocks, kQrThreads, kStagedBytes, s>>>(st, j);
+            else
+                qr_update_kernel<false><<<nblocks, kQrThreads, 0, s>>>(st, j);
             ISDF_LAUNCH_CHECK();
         }
         if (j == steps) break;
         if (exact) {
             ISDF_PROFILE("qrcp_sketch_verify", s);
-            lb_reduce_kernel<<<1, 1024, 0, s>>>(lbp.get(), nblocks, lb.get());
+            candidates_kernel<<<nblocks, kQrThreads, 0, s>>>(st, cand.get());
             ISDF_LAUNCH_CHECK();
-            count.zero(s);
-            candidates_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(st, lb.get(), cand.get(),
-                                                                                      count.get());
-            ISDF_LAUNCH_CHECK();
-            exact_kernel.fn<<<kExactBlocks, exact_kernel.threads, exact_smem, s>>>(ea, st, cand.get(), count.get(), j,
-                                                                reverified_d.get());
-            ISDF_LAUNCH_CHECK();
-            est_argmax_kernel<<<nblocks, kQrThreads, 0, s>>>(st);
+            exact_kernel.fn<<<kExactBlocks, exact_kernel.threads, exact_smem, s>>>(
+                ea, st, cand.get(), j, reverified_d.get(), lr_split.get(), done.get());
             ISDF_LAUNCH_CHECK();
         }
         {
             ISDF_PROFILE("qrcp_sketch_pivot", s);
-            qr_pivot_kernel<<<1, 1024, 0, s>>>(st, j, nblocks);
+            qr_pivot_kernel<<<1, 1024, 0, s>>>(st, j, nblocks, exact ? kExactBlocks : 0);
             ISDF_LAUNCH_CHECK();
         }
     }

@@ -122,20 +122,126 @@ void validate_axis_weights(const double* axis_weights, int naxes) {
 // ------------------------------------------------------------------------------
 // sketch
 // ------------------------------------------------------------------------------
+namespace {
+
+// std::normal_distribution<double>(0, 1) over std::mt19937_64, drawn as
+// libstdc++ does it (Marsaglia's polar method): an attempt takes two engine
+// outputs, each made a uniform in [0, 1) by generate_canonical<double, 53>
+// (one 64-bit output rounded once to double and scaled by 2^-64; 1.0 becomes
+// the largest double below 1), x = 2u - 1, y = 2u' - 1, and is rejected
+// unless 0 < x^2 + y^2 <= 1; an accepted attempt yields y f, then x f, with
+// f = sqrt(-2 ln(r2) / r2).  Only the engine is sequential: one thread per
+// stream draws the outputs and counts the accepted attempts per block of
+// attempts, then worker threads transform the blocks into their known places.
+inline double canonical53(uint64_t r) {
+    // the exact value hi 2^32 + lo rounded once: the correctly rounded conversion
+    const double x = (static_cast<double>(static_cast<uint32_t>(r >> 32)) * 0x1p32 +
+                      static_cast<double>(static_cast<uint32_t>(r))) * 0x1p-64;
+    return x >= 1.0 ? std::nextafter(1.0, 0.0) : x;
+}
+
+constexpr double kStdDev = 1.0, kMean = 0.0;
+constexpr int64_t kPolarBlock = 4096;   // attempts per block of the transform
+
+struct PolarDraws {
+    std::vector<uint64_t> raw;        // two engine outputs per attempt
+    std::vector<int64_t> block_out;   // deviates produced before each block (+ the total)
+    int64_t attempts = 0;
+};
+
+// The sequential part: engine outputs until `pairs` attempts are accepted.
+void polar_draw(uint64_t seed, int64_t pairs, PolarDraws& pd) {
+    std::mt19937_64 gen(seed);
+    pd.block_out.clear();
+    int64_t acc = 0, a = 0;
+    while (acc < pairs) {
+        if (a % kPolarBlock == 0) {
+            pd.block_out.push_back(2 * acc);
+            if (static_cast<int64_t>(pd.raw.size()) < 2 * (a + kPolarBlock))
+                pd.raw.resize(static_cast<size_t>(2 * (a + kPolarBlock)));
+        }
+        const uint64_t r0 = gen(), r1 = gen();
+        pd.raw[2 * a] = r0;
+        pd.raw[2 * a + 1] = r1;
+        const double x = 2.0 * canonical53(r0) - 1.0;
+        const double y = 2.0 * canonical53(r1) - 1.0;
+        const double r2 = x * x + y * y;
+        acc += (r2 <= 1.0 && r2 != 0.0) ? 1 : 0;
+        ++a;
+    }
+    pd.attempts = a;
+    pd.block_out.push_back(2 * acc);
+}
+
+// Deviates of block b, written at their place in out[0, count).
+void polar_block(const PolarDraws& pd, int64_t b, double* out, int64_t count) {
+    int64_t o = pd.block_out[b];
+    const int64_t a1 = std::min(pd.attempts, (b + 1) * kPolarBlock);
+    for (int64_t a = b * kPolarBlock; a < a1 && o < count; ++a) {
+        const double x = 2.0 * canonical53(pd.raw[2 * a]) - 1.0;
+        const double y = 2.0 * canonical53(pd.raw[2 * a + 1]) - 1.0;
+        const double r2 = x * x + y * y;
+        if (r2 > 1.0 || r2 == 0.0) continue;
+        const double f = std::sqrt(-2 * std::log(r2) / r2);
+        out[o++] = y * f * kStdDev + kMean;
+        if (o < count) out[o++] = x * f * kStdDev + kMean;
+    }
+}
+
+}  // namespace
+
+void sketch_factors(int64_t d, int64_t ell, uint64_t seed, double* u, double* v) {
+    // Two independent streams; fill order i = a*ell + s.
+    const int64_t count = d * ell;
+    if (count <= 0) return;
+    const uint64_t seeds[2] = {seed, seed ^ 0x9e3779b97f4a7c15ULL};
+    double* outs[2] = {u, v};
+    // this calling thread's draws, kept so later calls touch no fresh pages
+    // (the helper threads reach them through the pointer)
+    thread_local PolarDraws kept[2];
+    PolarDraws* pds = kept;
+    {
+        std::thread tv([pds, &seeds, count] { polar_draw(seeds[1], (count + 1) / 2, pds[1]); });
+        polar_draw(seeds[0], (count + 1) / 2, pds[0]);
+        tv.join();
+    }
+    const int64_t nb[2] = {static_cast<int64_t>(pds[0].block_out.size()) - 1,
+                           static_cast<int64_t>(pds[1].block_out.size()) - 1};
+    const int nw = static_cast<int>(std::clamp<int64_t>(std::thread::hardware_concurrency(), 1,
+                                                        std::min<int64_t>(16, nb[0] + nb[1])));
+    auto work = [&, pds](int w) {
+        for (int k = 0; k < 2; ++k)
+            for (int64_t b = w; b < nb[k]; b += nw) polar_block(pds[k], b, outs[k], count);
+    };
+    std::vector<std::thread> workers;
+    for (int w = 1; w < nw; ++w) workers.emplace_back(work, w);
+    work(0);
+    for (auto& t : workers) t.join();
+    // the first deviates must be the standard library's own (another library
+    // may draw differently): otherwise draw everything through it
+    bool same = true;
+    for (int k = 0; k < 2 && same; ++k) {
+        std::mt19937_64 gen(seeds[k]);
+        std::normal_distribution<double> normal(kMean, kStdDev);
+        for (int64_t i = 0; i < std::min<int64_t>(count, 64) && same; ++i) same = normal(gen) == outs[k][i];
+    }
+    if (!same) {
+        auto fill = [count](uint64_t sd, double* o) {
+            std::mt19937_64 gen(sd);
+            std::normal_distribution<double> normal(kMean, kStdDev);
+            for (int64_t i = 0; i < count; ++i) o[i] = normal(gen);
+        };
+        std::thread tv(fill, seeds[1], v);
+        fill(seeds[0], u);
+        tv.join();
+    }
+}
+
 void sketch_factors(int64_t d, int64_t ell, uint64_t seed, std::vector<double>& u,
                     std::vector<double>& v) {
-    // Two independent streams; fill order i = a*ell + s.
-    // The streams are independent, so each fills its matrix on its own thread.
     u.resize(static_cast<size_t>(d * ell));
     v.resize(static_cast<size_t>(d * ell));
-    auto fill = [d, ell](uint64_t sd, std::vector<double>& out) {
-        std::mt19937_64 gen(sd);
-        std::normal_distribution<double> normal(0, 1);
-        for (int64_t i = 0; i < d * ell; ++i) out[i] = normal(gen);
-    };
-    std::thread tv(fill, seed ^ 0x9e3779b97f4a7c15ULL, std::ref(v));
-    fill(seed, u);
-    tv.join();
+    sketch_factors(d, ell, seed, u.data(), v.data());
 }
 
 namespace {

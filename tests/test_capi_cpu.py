@@ -89,3 +89,15 @@ def test_inputs_generator_shapes():
     assert len(sym) == 192
     tables = inputs.build_tables(sym, xyz)
     assert tables.nao == 1536
+
+
+@pytest.mark.parametrize("d,ell,seed", [(1, 1, 0), (7, 3, 11), (96, 12, 2), (6144, 26, 7)])
+def test_sketch_factors_match_standard_library_streams(d, ell, seed):
+    """U/V of rand_sketch (threaded polar-method draws) equal the oracle's
+    std::normal_distribution streams bit for bit, odd counts included."""
+    from mp_isdf_b200 import capi
+    from oracle import oracle as O
+    u, v = capi.sketch_factors(d, ell, seed)
+    ou, ov = O.sketch_factors(d, ell, seed)
+    assert np.array_equal(u, ou)
+    assert np.array_equal(v, ov)
