@@ -70,50 +70,63 @@ struct SphPoly {
     }
 };
 
+// Contractions [g0, g0 + ng) of shell b (ng <= NG): radial sums over the
+// primitives, then every component of every spherical function.
+template <class T, int L, bool GRAD, int NG, class Sink>
+__device__ __forceinline__ void eval_shell_group(const ShellDesc& b, const SphPoly<T, L, GRAD>& poly, T x, T y,
+                                                 T z, T r2, const T* __restrict__ exps,
+                                                 const T* __restrict__ coefs, Sink& sink, int g0, int ng) {
+    constexpr int NS = 2 * L + 1;
+    T R[NG], Rp[NG];
+#pragma unroll
+    for (int j = 0; j < NG; ++j) { R[j] = T(0); Rp[j] = T(0); }
+    for (int p = 0; p < b.nprim; ++p) {
+        const T a = exps[b.prim_off + p];
+        const T arg = a * r2;
+        if (arg > T(kExpCut)) continue;
+        const T e = ao_exp(-arg);
+#pragma unroll
+        for (int j = 0; j < NG; ++j)
+            if (NG == 1 || j < ng) {
+                const T cc = coefs[b.coef_off + (g0 + j) * b.nprim + p] * e;
+                R[j] += cc;
+                if constexpr (GRAD) Rp[j] -= a * cc;
+            }
+    }
+#pragma unroll
+    for (int j = 0; j < NG; ++j)
+        if (NG == 1 || j < ng) {
+            const int ao0 = b.ao_off + (g0 + j) * NS;
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                sink.template put<0>(ao0 + s, R[j] * poly.v[s]);
+                if constexpr (GRAD) {
+                    const T two_rp = T(2) * Rp[j] * poly.v[s];
+                    sink.template put<1>(ao0 + s, R[j] * poly.vx[s] + x * two_rp);
+                    sink.template put<2>(ao0 + s, R[j] * poly.vy[s] + y * two_rp);
+                    sink.template put<3>(ao0 + s, R[j] * poly.vz[s] + z * two_rp);
+                }
+            }
+        }
+}
+
 // `sink.put<C>(ao, v)` receives component C (0 value, 1..3 d/dx, d/dy, d/dz)
 // of AO index `ao` for the contractions [ctr0, ctr1) of shell b, given the
-// offset (x, y, z) from the shell centre and r2 = |offset|^2.
+// offset (x, y, z) from the shell centre and r2 = |offset|^2.  A single
+// contraction (the common case) takes a path without a group's unused lanes.
 template <class T, int L, bool GRAD, class Sink>
 __device__ __forceinline__ void eval_shell_core(const ShellDesc& b, T x, T y, T z, T r2,
                                                 const T* __restrict__ exps, const T* __restrict__ coefs,
                                                 Sink& sink, int ctr0, int ctr1) {
-    constexpr int NS = 2 * L + 1;
     const SphPoly<T, L, GRAD> poly(x, y, z);
     const int cend = min(b.nctr, ctr1);
-    for (int g0 = ctr0; g0 < cend; g0 += kMaxCtrGroup) {
-        const int ng = min(kMaxCtrGroup, cend - g0);
-        T R[kMaxCtrGroup], Rp[kMaxCtrGroup];
-#pragma unroll
-        for (int j = 0; j < kMaxCtrGroup; ++j) { R[j] = T(0); Rp[j] = T(0); }
-        for (int p = 0; p < b.nprim; ++p) {
-            const T a = exps[b.prim_off + p];
-            const T arg = a * r2;
-            if (arg > T(kExpCut)) continue;
-            const T e = ao_exp(-arg);
-#pragma unroll
-            for (int j = 0; j < kMaxCtrGroup; ++j)
-                if (j < ng) {
-                    const T cc = coefs[b.coef_off + (g0 + j) * b.nprim + p] * e;
-                    R[j] += cc;
-                    if constexpr (GRAD) Rp[j] -= a * cc;
-                }
-        }
-#pragma unroll
-        for (int j = 0; j < kMaxCtrGroup; ++j)
-            if (j < ng) {
-                const int ao0 = b.ao_off + (g0 + j) * NS;
-#pragma unroll
-                for (int s = 0; s < NS; ++s) {
-                    sink.template put<0>(ao0 + s, R[j] * poly.v[s]);
-                    if constexpr (GRAD) {
-                        const T two_rp = T(2) * Rp[j] * poly.v[s];
-                        sink.template put<1>(ao0 + s, R[j] * poly.vx[s] + x * two_rp);
-                        sink.template put<2>(ao0 + s, R[j] * poly.vy[s] + y * two_rp);
-                        sink.template put<3>(ao0 + s, R[j] * poly.vz[s] + z * two_rp);
-                    }
-                }
-            }
+    if (cend - ctr0 == 1) {
+        eval_shell_group<T, L, GRAD, 1>(b, poly, x, y, z, r2, exps, coefs, sink, ctr0, 1);
+        return;
     }
+    for (int g0 = ctr0; g0 < cend; g0 += kMaxCtrGroup)
+        eval_shell_group<T, L, GRAD, kMaxCtrGroup>(b, poly, x, y, z, r2, exps, coefs, sink, g0,
+                                                   min(kMaxCtrGroup, cend - g0));
 }
 
 // Runtime dispatch on l up to LMAX (at least the context's largest angular

@@ -210,8 +210,11 @@ project_tc_kernel(ProjectArgs args) {
                         const float dy = (pyh - ch.y) + (pyl - cl.y);
                         const float dz = (pzh - ch.z) + (pzl - cl.z);
                         const float r2 = dx * dx + dy * dy + dz * dz;
-                        // the same r2 decides the screening and every primitive's cutoff
-                        if (ch.w * r2 > static_cast<float>(kExpCut)) {
+                        // the same r2 decides the screening and every primitive's cutoff:
+                        // a point beyond the cutoff of the shell's smallest exponent gets
+                        // exact zeros from the evaluation too, so the zero fill is taken
+                        // only when it holds for the whole warp (no divergent paths)
+                        if (__all_sync(__activemask(), ch.w * r2 > static_cast<float>(kExpCut))) {
                             // every primitive is cut off: the piece is exactly zero here
                             for (int k = pc.w; k < pc.w + pc.z * ns; ++k)
 #pragma unroll

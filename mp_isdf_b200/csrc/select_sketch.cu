@@ -20,6 +20,7 @@
 #include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <limits>
 #include <random>
@@ -132,7 +133,8 @@ namespace {
 // unless 0 < x^2 + y^2 <= 1; an accepted attempt yields y f, then x f, with
 // f = sqrt(-2 ln(r2) / r2).  Only the engine is sequential: one thread per
 // stream draws the outputs and counts the accepted attempts per block of
-// attempts, then worker threads transform the blocks into their known places.
+// attempts, and worker threads transform each block into its known place as
+// soon as it is published.
 inline double canonical53(uint64_t r) {
     // the exact value hi 2^32 + lo rounded once: the correctly rounded conversion
     const double x = (static_cast<double>(static_cast<uint32_t>(r >> 32)) * 0x1p32 +
@@ -141,50 +143,55 @@ inline double canonical53(uint64_t r) {
 }
 
 constexpr double kStdDev = 1.0, kMean = 0.0;
-constexpr int64_t kPolarBlock = 4096;   // attempts per block of the transform
+constexpr int64_t kPolarBlock = 2048;   // attempts per block of the transform
 
 struct PolarDraws {
     std::vector<uint64_t> raw;        // two engine outputs per attempt
-    std::vector<int64_t> block_out;   // deviates produced before each block (+ the total)
-    int64_t attempts = 0;
+    std::vector<int64_t> block_out;   // deviates produced before each block
+    int64_t nblocks = 0;              // blocks drawn (read after the join)
+    std::atomic<int64_t> published{0};
+    std::atomic<bool> done{false};
 };
 
-// The sequential part: engine outputs until `pairs` attempts are accepted.
-void polar_draw(uint64_t seed, int64_t pairs, PolarDraws& pd) {
+// The sequential part: engine outputs until `pairs` attempts are accepted,
+// published block by block with the deviates produced so far (at most
+// max_blocks; the caller finishes a stream that needs more).  Returns the
+// engine for that tail.
+std::mt19937_64 polar_draw(uint64_t seed, int64_t pairs, int64_t max_blocks, PolarDraws& pd) {
     std::mt19937_64 gen(seed);
-    pd.block_out.clear();
-    int64_t acc = 0, a = 0;
-    while (acc < pairs) {
-        if (a % kPolarBlock == 0) {
-            pd.block_out.push_back(2 * acc);
-            if (static_cast<int64_t>(pd.raw.size()) < 2 * (a + kPolarBlock))
-                pd.raw.resize(static_cast<size_t>(2 * (a + kPolarBlock)));
+    int64_t acc = 0, a = 0, b = 0;
+    pd.block_out[0] = 0;
+    while (acc < pairs && b < max_blocks) {
+        const int64_t a1 = a + kPolarBlock;
+        for (; a < a1 && acc < pairs; ++a) {
+            const uint64_t r0 = gen(), r1 = gen();
+            pd.raw[2 * a] = r0;
+            pd.raw[2 * a + 1] = r1;
+            const double x = 2.0 * canonical53(r0) - 1.0;
+            const double y = 2.0 * canonical53(r1) - 1.0;
+            const double r2 = x * x + y * y;
+            acc += (r2 <= 1.0 && r2 != 0.0) ? 1 : 0;
         }
-        const uint64_t r0 = gen(), r1 = gen();
-        pd.raw[2 * a] = r0;
-        pd.raw[2 * a + 1] = r1;
-        const double x = 2.0 * canonical53(r0) - 1.0;
-        const double y = 2.0 * canonical53(r1) - 1.0;
-        const double r2 = x * x + y * y;
-        acc += (r2 <= 1.0 && r2 != 0.0) ? 1 : 0;
-        ++a;
+        pd.block_out[b + 1] = 2 * acc;
+        pd.published.store(++b, std::memory_order_release);
     }
-    pd.attempts = a;
-    pd.block_out.push_back(2 * acc);
+    pd.nblocks = b;
+    pd.done.store(true, std::memory_order_release);
+    return gen;
 }
 
-// Deviates of block b, written at their place in out[0, count).
+// Deviates of a published block b, written at their place in out[0, count).
 void polar_block(const PolarDraws& pd, int64_t b, double* out, int64_t count) {
     int64_t o = pd.block_out[b];
-    const int64_t a1 = std::min(pd.attempts, (b + 1) * kPolarBlock);
-    for (int64_t a = b * kPolarBlock; a < a1 && o < count; ++a) {
+    const int64_t o1 = std::min(count, pd.block_out[b + 1]);
+    for (int64_t a = b * kPolarBlock; o < o1; ++a) {
         const double x = 2.0 * canonical53(pd.raw[2 * a]) - 1.0;
         const double y = 2.0 * canonical53(pd.raw[2 * a + 1]) - 1.0;
         const double r2 = x * x + y * y;
         if (r2 > 1.0 || r2 == 0.0) continue;
         const double f = std::sqrt(-2 * std::log(r2) / r2);
         out[o++] = y * f * kStdDev + kMean;
-        if (o < count) out[o++] = x * f * kStdDev + kMean;
+        if (o < o1) out[o++] = x * f * kStdDev + kMean;
     }
 }
 
@@ -196,27 +203,57 @@ void sketch_factors(int64_t d, int64_t ell, uint64_t seed, double* u, double* v)
     if (count <= 0) return;
     const uint64_t seeds[2] = {seed, seed ^ 0x9e3779b97f4a7c15ULL};
     double* outs[2] = {u, v};
-    // this calling thread's draws, kept so later calls touch no fresh pages
-    // (the helper threads reach them through the pointer)
-    thread_local PolarDraws kept[2];
-    PolarDraws* pds = kept;
-    {
-        std::thread tv([pds, &seeds, count] { polar_draw(seeds[1], (count + 1) / 2, pds[1]); });
-        polar_draw(seeds[0], (count + 1) / 2, pds[0]);
-        tv.join();
+    const int64_t pairs = (count + 1) / 2;
+    // attempts are accepted with probability pi/4: far more blocks than any
+    // stream needs in practice; a stream that needs more is finished below
+    const int64_t max_blocks = (pairs * 3 / 2) / kPolarBlock + 4;
+    // the calling thread's buffers, kept so later calls touch no fresh pages
+    thread_local std::vector<uint64_t> raw_keep[2];
+    thread_local std::vector<int64_t> out_keep[2];
+    PolarDraws pd[2];
+    for (int k = 0; k < 2; ++k) {
+        raw_keep[k].resize(static_cast<size_t>(2 * max_blocks * kPolarBlock));
+        out_keep[k].resize(static_cast<size_t>(max_blocks + 1));
+        pd[k].raw.swap(raw_keep[k]);
+        pd[k].block_out.swap(out_keep[k]);
     }
-    const int64_t nb[2] = {static_cast<int64_t>(pds[0].block_out.size()) - 1,
-                           static_cast<int64_t>(pds[1].block_out.size()) - 1};
-    const int nw = static_cast<int>(std::clamp<int64_t>(std::thread::hardware_concurrency(), 1,
-                                                        std::min<int64_t>(16, nb[0] + nb[1])));
-    auto work = [&, pds](int w) {
+    // two threads draw (one per stream) while the others transform each
+    // published block; a worker takes every nw-th block of each stream
+    const int nw = static_cast<int>(std::clamp(std::thread::hardware_concurrency(), 3u, 12u)) - 2;
+    std::mt19937_64 tail_gen[2];
+    auto work = [&pd, &outs, count, nw](int w) {
         for (int k = 0; k < 2; ++k)
-            for (int64_t b = w; b < nb[k]; b += nw) polar_block(pds[k], b, outs[k], count);
+            for (int64_t b = w;; b += nw) {
+                // wait until block b is drawn or the stream ended before it
+                while (pd[k].published.load(std::memory_order_acquire) <= b &&
+                       !pd[k].done.load(std::memory_order_acquire))
+                    std::this_thread::yield();
+                if (b >= pd[k].published.load(std::memory_order_acquire)) break;
+                polar_block(pd[k], b, outs[k], count);
+            }
     };
-    std::vector<std::thread> workers;
-    for (int w = 1; w < nw; ++w) workers.emplace_back(work, w);
-    work(0);
-    for (auto& t : workers) t.join();
+    {
+        std::vector<std::thread> threads;
+        threads.emplace_back([&] { tail_gen[1] = polar_draw(seeds[1], pairs, max_blocks, pd[1]); });
+        for (int w = 0; w < nw; ++w) threads.emplace_back(work, w);
+        tail_gen[0] = polar_draw(seeds[0], pairs, max_blocks, pd[0]);
+        for (auto& t : threads) t.join();
+    }
+    for (int k = 0; k < 2; ++k) {
+        // practically never: continue the engine where the blocks end
+        int64_t o = pd[k].block_out[pd[k].nblocks];
+        while (o < count) {
+            const double x = 2.0 * canonical53(tail_gen[k]()) - 1.0;
+            const double y = 2.0 * canonical53(tail_gen[k]()) - 1.0;
+            const double r2 = x * x + y * y;
+            if (r2 > 1.0 || r2 == 0.0) continue;
+            const double f = std::sqrt(-2 * std::log(r2) / r2);
+            outs[k][o++] = y * f * kStdDev + kMean;
+            if (o < count) outs[k][o++] = x * f * kStdDev + kMean;
+        }
+        pd[k].raw.swap(raw_keep[k]);
+        pd[k].block_out.swap(out_keep[k]);
+    }
     // the first deviates must be the standard library's own (another library
     // may draw differently): otherwise draw everything through it
     bool same = true;
