@@ -43,8 +43,8 @@ enum isdf_algorithm {
     ISDF_QRCP_ONLINE = 1,            /* OnlineQRColumnPivoting */
     ISDF_RAND_SKETCH_QUADRATURE = 2, /* RandomizedQuadratureKhatriRao */
     ISDF_CVT = 3,                    /* CentroidalVoronoi (not on this path) */
-    ISDF_RAND_SKETCH_DENSITY = 4,    /* RandomizedAODensityKhatriRao (not on this path) */
-    ISDF_RAND_SKETCH_DENSITY_NORM = 5
+    ISDF_RAND_SKETCH_DENSITY = 4,    /* RandomizedAODensityKhatriRao (FP64 form) */
+    ISDF_RAND_SKETCH_DENSITY_NORM = 5 /* RandomizedAODensityNormalizedKhatriRao (FP64 form) */
 };
 
 enum isdf_precision { ISDF_FP64 = 0, ISDF_MIXED = 1 };
@@ -107,6 +107,13 @@ typedef struct isdf_select_args {
     uint64_t seed;               /* default 7 */
     int32_t precision;           /* enum isdf_precision (rand_sketch only) */
     int32_t debug;               /* print a summary line on stderr */
+    /* density sketches (ISDF_RAND_SKETCH_DENSITY[_NORM], FP64 form, axes = {AO}):
+     * ngrid finite nonnegative importances m_g (device memory for isdf_select /
+     * isdf_select_fit, host memory for the _host variants); points with m_g = 0
+     * or squared AO norm <= ao_screening_threshold are not candidates
+     * (cpp/src/anchor_select_randomized_id.cpp:104-115, 231-260). */
+    const double* point_importance;
+    double ao_screening_threshold;   /* default 1e-24 */
 } isdf_select_args;
 
 typedef struct isdf_select_info {

@@ -32,7 +32,8 @@ SYMBOLS = [
     "isdf_sketch_select_gathered", "isdf_fit_at",
 ]
 
-ALGORITHMS = {"qrcp_dense": 0, "qrcp_online": 1, "rand_sketch": 2}
+ALGORITHMS = {"qrcp_dense": 0, "qrcp_online": 1, "rand_sketch": 2, "rand_sketch_density": 4,
+              "rand_sketch_density_col_norm": 5}
 AXES = {"ao": 0, "dx": 1, "dy": 2, "dz": 3, "occ": 4}
 
 
@@ -40,7 +41,8 @@ class SelectArgs(ctypes.Structure):
     _fields_ = [("algorithm", I32), ("naxes", I32), ("axes", P), ("axis_weights", P),
                 ("tolerance", F64), ("max_rank", I64), ("batch_size", I64),
                 ("sketch_size", I64), ("oversampling", I64), ("seed", ctypes.c_uint64),
-                ("precision", I32), ("debug", I32)]
+                ("precision", I32), ("debug", I32), ("point_importance", P),
+                ("ao_screening_threshold", F64)]
 
 
 class SelectInfo(ctypes.Structure):
@@ -179,10 +181,11 @@ class Context:
 
     def select(self, xyz, w, algorithm="rand_sketch", axes=("ao",), axis_weights=None,
                tolerance=1e-10, max_rank=0, batch_size=128, sketch_size=128, oversampling=16,
-               seed=7, precision="fp64", debug=False):
+               seed=7, precision="fp64", debug=False, point_importance=None, ao_screening_threshold=1e-24):
         """Anchor selection on device-resident points/weights; returns (pivots, info)."""
         args, keep = make_select_args(algorithm, axes, axis_weights, tolerance, max_rank,
-                                      batch_size, sketch_size, oversampling, seed, precision, debug)
+                                      batch_size, sketch_size, oversampling, seed, precision, debug,
+                                      point_importance, ao_screening_threshold)
         ng = xyz.shape[0]
         piv = np.empty(max(ng, 1), dtype=np.int64)
         n = I64()
@@ -392,7 +395,10 @@ class SketchShard:
 
 def make_select_args(algorithm="rand_sketch", axes=("ao",), axis_weights=None, tolerance=1e-10,
                      max_rank=0, batch_size=128, sketch_size=128, oversampling=16, seed=7,
-                     precision="fp64", debug=False):
+                     precision="fp64", debug=False, point_importance=None, ao_screening_threshold=1e-24):
+    """isdf_select_args (and the arrays it points at, to keep alive).  For the
+    density sketches `point_importance` is a float64 vector over the grid: a
+    CUDA tensor for the device entry points, host memory for the _host ones."""
     args = SelectArgs()
     lib().isdf_select_args_default(ctypes.byref(args))
     ax = np.array([AXES[a] if isinstance(a, str) else int(a) for a in axes], dtype=np.int32)
@@ -409,7 +415,12 @@ def make_select_args(algorithm="rand_sketch", axes=("ao",), axis_weights=None, t
     args.seed = seed
     args.precision = 1 if precision == "mixed" else 0
     args.debug = int(debug)
-    return args, (ax, aw)
+    imp = None
+    if point_importance is not None:
+        imp = point_importance if hasattr(point_importance, "data_ptr") else _np(point_importance, np.float64)
+        args.point_importance = _ptr(imp)
+    args.ao_screening_threshold = ao_screening_threshold
+    return args, (ax, aw, imp)
 
 
 def sketch_factors(d, ell, seed):

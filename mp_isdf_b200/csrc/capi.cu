@@ -76,9 +76,24 @@ isdf::SelectOptions options_of(const isdf_select_args* a) {
     o.seed = a->seed;
     o.precision = a->precision;
     o.debug = a->debug != 0;
+    o.importance = a->point_importance;
+    o.ao_threshold = a->ao_screening_threshold;
     if (o.max_rank < 0 || o.batch_size < 0 || o.sketch_size < 0 || o.oversampling < 0)
         isdf::fail(isdf::kInvalid, "sizes must be nonnegative");
     return o;
+}
+
+// The host-buffer entry points take the importance vector in host memory: a
+// copy of the arguments pointing at a device copy of it.
+isdf_select_args device_importance(const isdf_select_args* a, isdf::DeviceBuffer<double>& dm, int64_t ng,
+                                   cudaStream_t s) {
+    if (!a) isdf::fail(isdf::kInvalid, "null selection arguments");
+    isdf_select_args out = *a;
+    if (a->point_importance && ng > 0) {
+        upload(dm, a->point_importance, static_cast<size_t>(ng), s);
+        out.point_importance = dm.get();
+    }
+    return out;
 }
 
 }  // namespace
@@ -226,6 +241,8 @@ void isdf_select_args_default(isdf_select_args* a) {
     a->oversampling = 16;
     a->seed = 7;
     a->precision = ISDF_FP64;
+    a->point_importance = nullptr;
+    a->ao_screening_threshold = 1e-24;
 }
 
 namespace {
@@ -265,7 +282,9 @@ std::vector<int64_t> select_impl(isdf_ctx* ctx, const isdf_select_args* args, co
                          static_cast<long long>(d.reselections), static_cast<long long>(d.exact_scans));
         break;
     }
-    case ISDF_RAND_SKETCH_QUADRATURE: {
+    case ISDF_RAND_SKETCH_QUADRATURE:
+    case ISDF_RAND_SKETCH_DENSITY:
+    case ISDF_RAND_SKETCH_DENSITY_NORM: {
         isdf::SketchDiagnostics d;
         out = isdf::select_rand_sketch(c, xyz, w, ng, o, s, &d, keep);
         if (info) {
@@ -276,9 +295,12 @@ std::vector<int64_t> select_impl(isdf_ctx* ctx, const isdf_select_args* args, co
         }
         if (o.debug)
             std::fprintf(stderr,
-                         "[rand_sketch:quadrature] rank=%lld sketch_size=%lld oversampling=%lld "
+                         "[rand_sketch:%s] rank=%lld sketch_size=%lld oversampling=%lld "
                          "sketch_relative_frobenius=%.6e numerical_rank=%lld rank_cap=%lld "
                          "seed=%llu precision=%s space=device\n",
+                         o.algorithm == ISDF_RAND_SKETCH_DENSITY_NORM ? "density_col_norm"
+                         : o.algorithm == ISDF_RAND_SKETCH_DENSITY   ? "density"
+                                                                     : "quadrature",
                          static_cast<long long>(d.rank), static_cast<long long>(d.ell),
                          static_cast<long long>(o.oversampling), d.relative_tail,
                          static_cast<long long>(d.numerical_rank), static_cast<long long>(d.cap),
@@ -286,8 +308,6 @@ std::vector<int64_t> select_impl(isdf_ctx* ctx, const isdf_select_args* args, co
         break;
     }
     case ISDF_CVT:
-    case ISDF_RAND_SKETCH_DENSITY:
-    case ISDF_RAND_SKETCH_DENSITY_NORM:
         isdf::fail(isdf::kNotImplemented,
                    "this anchor selection algorithm is outside the B200 hot path (NYI)");
     default:
@@ -318,10 +338,11 @@ int isdf_select_host(isdf_ctx* ctx, const isdf_select_args* args, const double* 
         auto& c = ctx_of(ctx);
         DeviceGuard dg(c.device);
         cudaStream_t s = ctx->stream;
-        isdf::DeviceBuffer<double> dx, dw;
+        isdf::DeviceBuffer<double> dx, dw, dm;
         upload(dx, xyz, static_cast<size_t>(3 * std::max<int64_t>(ng, 0)), s);
         upload(dw, w, static_cast<size_t>(std::max<int64_t>(ng, 0)), s);
-        const int r = isdf_select(ctx, args, dx.get(), dw.get(), ng, pivots, capacity, npivots, info, s);
+        isdf_select_args a = device_importance(args, dm, ng, s);
+        const int r = isdf_select(ctx, &a, dx.get(), dw.get(), ng, pivots, capacity, npivots, info, s);
         if (r != ISDF_OK) throw isdf::Error(r, g_last_error);
     });
     return rc;
@@ -481,12 +502,13 @@ int isdf_select_fit_host(isdf_ctx* ctx, const isdf_select_args* args, const doub
         cudaStream_t s = ctx->stream;
         if (npivots) *npivots = 0;
         if (!args) isdf::fail(isdf::kInvalid, "selection arguments are required");
-        isdf::DeviceBuffer<double> dx, dw;
+        isdf::DeviceBuffer<double> dx, dw, dm;
         upload(dx, xyz, static_cast<size_t>(3 * std::max<int64_t>(ng, 0)), s);
         upload(dw, w, static_cast<size_t>(std::max<int64_t>(ng, 0)), s);
+        isdf_select_args a = device_importance(args, dm, ng, s);
         std::lock_guard<std::mutex> lock(c.ws_mu);   // workspace held to the end of the fit
         isdf::RetainedAo keep;
-        std::vector<int64_t> out = select_impl(ctx, args, dx.get(), dw.get(), ng, select_info, s, &keep);
+        std::vector<int64_t> out = select_impl(ctx, &a, dx.get(), dw.get(), ng, select_info, s, &keep);
         if (static_cast<int64_t>(out.size()) > capacity)
             isdf::fail(isdf::kInvalid, "pivot buffer is too small");
         if (!out.empty()) std::memcpy(pivots, out.data(), out.size() * sizeof(int64_t));

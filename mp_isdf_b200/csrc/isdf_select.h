@@ -11,8 +11,11 @@ struct KeptPoints {
 };
 
 // Flags non-finite weights (always) and non-finite coordinates of kept points,
-// and compacts the nonzero-weight points in their original order.
-KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStream_t s);
+// and compacts the nonzero-weight points in their original order.  With an
+// importance vector (density sketches) every entry must be finite and
+// nonnegative, and points of zero importance are dropped too.
+KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStream_t s,
+                          const double* importance = nullptr);
 
 struct SelectOptions {
     int algorithm = 0;               // LocalAnchorSelectionAlgorithm code
@@ -26,6 +29,8 @@ struct SelectOptions {
     uint64_t seed = 7;
     int precision = 0;               // 0 FP64, 1 mixed
     bool debug = false;
+    const double* importance = nullptr;  // density sketches: per grid point (device)
+    double ao_threshold = 1e-24;         // density sketches: squared AO norm screen
 };
 
 struct SketchDiagnostics {

@@ -11,6 +11,7 @@
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -130,20 +131,32 @@ struct Selector {
                                 py::object cvt_weights, std::size_t cvt_max_iter, double cvt_tol,
                                 const std::vector<double>& axis_weights, py::object point_importance,
                                 double ao_screening_threshold, const std::string& precision) {
-        (void)audit; (void)cvt_max_iter; (void)cvt_tol; (void)ao_screening_threshold;
+        (void)audit; (void)cvt_max_iter; (void)cvt_tol;
         auto pts = points_of(points, "expected points[ngrid,3]");
         if (weights.ndim() != 1 || weights.shape(0) != pts.shape(0))
             throw std::invalid_argument("expected weights[ngrid]");
         auto ax = read_axes(axes);
-        if (!cvt_weights.is_none() || !point_importance.is_none() ||
-            algorithm == LocalAlgo::CentroidalVoronoi ||
-            algorithm == LocalAlgo::RandomizedAODensityKhatriRao ||
-            algorithm == LocalAlgo::RandomizedAODensityNormalizedKhatriRao) {
-            if ((algorithm == LocalAlgo::RandomizedAODensityKhatriRao ||
-                 algorithm == LocalAlgo::RandomizedAODensityNormalizedKhatriRao) &&
-                (ax.size() != 1 || ax[0] != ISDF_AXIS_AO))
+        const bool density = algorithm == LocalAlgo::RandomizedAODensityKhatriRao ||
+                             algorithm == LocalAlgo::RandomizedAODensityNormalizedKhatriRao;
+        if (!cvt_weights.is_none() || algorithm == LocalAlgo::CentroidalVoronoi)
+            throw NotImplemented("CVT is outside the B200 hot path (NYI)");
+        // density sketches (cpp/src/anchor_select_randomized_id.cpp:104-118)
+        FloatArray importance;
+        if (density) {
+            if (point_importance.is_none())
+                throw std::invalid_argument("point_importance must have shape (ngrid,)");
+            importance = FloatArray::ensure(point_importance);
+            if (!importance || importance.ndim() != 1 || importance.shape(0) != pts.shape(0))
+                throw std::invalid_argument("point_importance must have shape (ngrid,)");
+            for (py::ssize_t i = 0; i < importance.shape(0); ++i) {
+                const double m = importance.data()[i];
+                if (!std::isfinite(m) || m < 0)
+                    throw std::invalid_argument("point_importance must be finite and nonnegative");
+            }
+            if (!std::isfinite(ao_screening_threshold) || ao_screening_threshold < 0)
+                throw std::invalid_argument("AO screening threshold must be finite and nonnegative");
+            if (ax.size() != 1 || ax[0] != ISDF_AXIS_AO)
                 throw std::invalid_argument("density Khatri-Rao sketches with non-AO axis features are NYI");
-            throw NotImplemented("CVT and density sketches are outside the B200 hot path (NYI)");
         }
         check_occupied(ax, mo_coeff, nocc, ctx->nao);
         parse_space(space);
@@ -165,6 +178,10 @@ struct Selector {
         a.seed = seed;
         a.precision = precision == "mixed" ? ISDF_MIXED : ISDF_FP64;
         a.debug = debug;
+        if (density) {
+            a.point_importance = importance.data();
+            a.ao_screening_threshold = ao_screening_threshold;
+        }
         const int64_t ng = pts.shape(0);
         std::vector<int64_t> piv(static_cast<size_t>(std::max<int64_t>(ng, 1)));
         int64_t np = 0;

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdio>
 #include <limits>
 #include <random>
 #include <thread>
@@ -34,12 +35,19 @@ namespace isdf {
 namespace {
 
 __global__ void flag_points_kernel(const double* __restrict__ pts, const double* __restrict__ w,
-                                   int64_t n, char* __restrict__ keep, int* __restrict__ bad) {
+                                   const double* __restrict__ importance, int64_t n,
+                                   char* __restrict__ keep, int* __restrict__ bad) {
     const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (g >= n) return;
+    bool important = true;
+    if (importance) {
+        const double m = importance[g];
+        if (!isfinite(m) || m < 0.0) atomicOr(bad, 4);
+        important = m != 0.0;
+    }
     const double wg = w[g];
     if (!isfinite(wg)) { atomicOr(bad, 1); keep[g] = 0; return; }
-    const bool k = wg != 0.0;
+    const bool k = wg != 0.0 && important;
     keep[g] = k;
     if (k && !(isfinite(pts[3 * g]) && isfinite(pts[3 * g + 1]) && isfinite(pts[3 * g + 2])))
         atomicOr(bad, 2);
@@ -47,7 +55,8 @@ __global__ void flag_points_kernel(const double* __restrict__ pts, const double*
 
 }  // namespace
 
-KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStream_t s) {
+KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStream_t s,
+                          const double* importance) {
     KeptPoints kp;
     kp.index.reset(std::max<int64_t>(n, 1), s);
     if (n == 0) return kp;
@@ -55,8 +64,8 @@ KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStr
     DeviceBuffer<int> bad(1, s);
     DeviceBuffer<int64_t> count(1, s);
     bad.zero(s);
-    flag_points_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(pts, w, n, keep.get(),
-                                                                              bad.get());
+    flag_points_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(pts, w, importance, n,
+                                                                              keep.get(), bad.get());
     ISDF_LAUNCH_CHECK();
     size_t tmp_bytes = 0;
     thrust::counting_iterator<int64_t> it(0);
@@ -71,6 +80,7 @@ KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStr
     ISDF_CUDA(cudaMemcpyAsync(&hbad, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaMemcpyAsync(&hcount, count.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaStreamSynchronize(s));
+    if (hbad & 4) fail(kInvalid, "point_importance must be finite and nonnegative");
     if (hbad & 1) fail(kInvalid, "grid weights must be finite");
     if (hbad & 2) fail(kInvalid, "grid coordinates must be finite");
     kp.n = hcount;
@@ -364,6 +374,136 @@ void sketch_fp64(const Context& c, const double* pts, const KeptPoints& kp, cons
     if (hbad) fail(kOverflow, "non-finite randomized ID sketch");
 }
 
+namespace {
+
+// Squared norm of each feature row (one warp per row).
+__global__ void row_sumsq_kernel(const double* __restrict__ F, int64_t rows, int64_t d,
+                                 double* __restrict__ out) {
+    const int64_t r = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (r >= rows) return;
+    double acc = 0;
+    for (int64_t a = lane; a < d; a += 32) {
+        const double x = F[r * d + a];
+        acc += x * x;
+    }
+    acc = warp_allsum(acc);
+    if (lane == 0) out[r] = acc;
+}
+
+__global__ void flag_screen_kernel(const double* __restrict__ q, int64_t n, double threshold,
+                                   char* __restrict__ keep, int* __restrict__ bad) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const double v = q[g];
+    if (!isfinite(v)) atomicOr(bad, 1);
+    keep[g] = v > threshold;
+}
+
+// Y[s][i] = sqrt(m_g)/sqrt(ell) (f.u_s)(f.v_s) for the screened points g =
+// pos[i] (f = phi_g, or phi_g / |phi_g| in the normalized form); also the
+// surviving grid indices.
+__global__ void combine_density_kernel(const double* __restrict__ P, const double* __restrict__ q,
+                                       const int64_t* __restrict__ pos, int64_t n2, int64_t ell,
+                                       const double* __restrict__ importance,
+                                       const int64_t* __restrict__ index, bool normalized,
+                                       double* __restrict__ Yt, int64_t* __restrict__ index2,
+                                       int* __restrict__ bad) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n2) return;
+    const int64_t g = pos[i];
+    const int64_t gi = index[g];
+    index2[i] = gi;
+    const double sw = sqrt(importance[gi]);
+    const double inv = normalized ? 1.0 / sqrt(q[g]) : 1.0;
+    const double scaling = 1.0 / sqrt(static_cast<double>(ell));
+    const double* pg = P + g * 2 * ell;
+    bool ok = true;
+    for (int64_t s = 0; s < ell; ++s) {
+        const double y = scaling * sw * (inv * pg[s]) * (inv * pg[ell + s]);
+        ok = ok && isfinite(y);
+        Yt[s * n2 + i] = y;
+    }
+    if (!ok) atomicOr(bad, 1);
+}
+
+}  // namespace
+
+// AO-density Khatri-Rao sketch in FP64 (anchor_select_randomized_id.cpp:231-309):
+// features are the AO values of the kept points; points whose squared AO norm
+// is <= threshold leave the candidate set (kp is compacted to the survivors,
+// in order), and column g of the sketch is sqrt(m_g)/sqrt(ell) (f.u_s)(f.v_s)
+// with f = phi_g, or phi_g/|phi_g| in the normalized form.  Returns Yt
+// (ell x kp.n, leading dimension kp.n).
+DeviceBuffer<double> sketch_density_fp64(const Context& c, const double* pts, KeptPoints& kp,
+                                         const double* importance, int64_t ell,
+                                         const std::vector<double>& u, const std::vector<double>& v,
+                                         bool normalized, double threshold, int64_t chunk,
+                                         cudaStream_t s) {
+    const int nao = c.nao;
+    const int64_t d = nao;
+    const int64_t n = kp.n;
+    const int32_t ao_axis = 0;
+    const AxisSpec ax = make_axis_spec(c, &ao_axis, 1);
+    std::vector<double> hw(static_cast<size_t>(d * 2 * ell));
+    for (int64_t j = 0; j < d; ++j)
+        for (int64_t t = 0; t < ell; ++t) {
+            hw[j * 2 * ell + t] = u[j * ell + t];
+            hw[j * 2 * ell + ell + t] = v[j * ell + t];
+        }
+    DeviceBuffer<double> W(hw.size(), s);
+    ISDF_CUDA(cudaMemcpyAsync(W.get(), hw.data(), hw.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    DeviceBuffer<double> P(static_cast<size_t>(std::max<int64_t>(n, 1) * 2 * ell), s), q(std::max<int64_t>(n, 1), s);
+    chunk = std::max<int64_t>(1, std::min(chunk, n));
+    DeviceBuffer<double> F(static_cast<size_t>(chunk * d), s);
+    for (int64_t g0 = 0; g0 < n; g0 += chunk) {
+        const int64_t b = std::min(chunk, n - g0);
+        eval_axis_features<double>(c, pts, kp.index.get() + g0, b, ax, F.get(), d, nullptr, nullptr, s);
+        gemm_f64(b, 2 * ell, nao, F.get(), d, 0, W.get(), 2 * ell, 0, P.get() + g0 * 2 * ell, 2 * ell, 0, 1,
+                 false, s);
+        row_sumsq_kernel<<<static_cast<unsigned>((b * 32 + 255) / 256), 256, 0, s>>>(F.get(), b, d,
+                                                                                     q.get() + g0);
+        ISDF_LAUNCH_CHECK();
+    }
+    // screening: the surviving positions, in order
+    DeviceBuffer<char> keep(std::max<int64_t>(n, 1), s);
+    DeviceBuffer<int> bad(1, s);
+    DeviceBuffer<int64_t> pos(std::max<int64_t>(n, 1), s), count(1, s);
+    bad.zero(s);
+    flag_screen_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(q.get(), n, threshold, keep.get(),
+                                                                            bad.get());
+    ISDF_LAUNCH_CHECK();
+    size_t tmp_bytes = 0;
+    thrust::counting_iterator<int64_t> it(0);
+    ISDF_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp_bytes, it, keep.get(), pos.get(), count.get(), n, s));
+    DeviceBuffer<char> tmp(tmp_bytes, s);
+    ISDF_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tmp_bytes, it, keep.get(), pos.get(), count.get(), n, s));
+    count_launches(2);
+    int hbad = 0;
+    int64_t n2 = 0;
+    ISDF_CUDA(cudaMemcpyAsync(&hbad, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(&n2, count.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    if (hbad) fail(kOverflow, "non-finite AO squared norm");
+    DeviceBuffer<double> Yt(static_cast<size_t>(std::max<int64_t>(n2, 1) * ell), s);
+    KeptPoints kp2;
+    kp2.index.reset(std::max<int64_t>(n2, 1), s);
+    kp2.n = n2;
+    if (n2 > 0) {
+        bad.zero(s);
+        ISDF_PROFILE("sketch_combine", s);
+        combine_density_kernel<<<static_cast<unsigned>((n2 + 255) / 256), 256, 0, s>>>(
+            P.get(), q.get(), pos.get(), n2, ell, importance, kp.index.get(), normalized, Yt.get(),
+            kp2.index.get(), bad.get());
+        ISDF_LAUNCH_CHECK();
+        ISDF_CUDA(cudaMemcpyAsync(&hbad, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        if (hbad) fail(kOverflow, "non-finite randomized ID sketch");
+    }
+    kp = std::move(kp2);
+    return Yt;
+}
+
 // ------------------------------------------------------------------------------
 // mixed-precision sketch: fused FP32 AO evaluation + split-BF16 tensor-core
 // projection, FP64 combination with per-column error bounds
@@ -613,14 +753,27 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
                                         int64_t ng, const SelectOptions& o, cudaStream_t s,
                                         SketchDiagnostics* diag_out, RetainedAo* keep) {
     sketch_setup(c, o, 0);   // option checks before any device work
+    const bool density = o.algorithm == 4 || o.algorithm == 5;
+    if (density) {
+        if (!o.importance) fail(kInvalid, "point_importance must have shape (ngrid,)");
+        if (!std::isfinite(o.ao_threshold) || o.ao_threshold < 0)
+            fail(kInvalid, "AO screening threshold must be finite and nonnegative");
+        if (o.axes.size() != 1 || o.axes[0] != 0)
+            fail(kInvalid, "density Khatri-Rao sketches with non-AO axis features are NYI");
+        if (o.precision != 0)
+            fail(kNotImplemented, "density Khatri-Rao sketches are implemented in the FP64 form only");
+    }
     ISDF_PROFILE("phase:select", s);
     KeptPoints kp;
     {
         ISDF_PROFILE("phase:compact", s);
-        kp = compact_points(pts, w, ng, s);
+        kp = compact_points(pts, w, ng, s, density ? o.importance : nullptr);
     }
-    const int64_t n = kp.n;
-    if (n == 0) return {};
+    int64_t n = kp.n;
+    if (n == 0) {
+        if (density && o.max_rank) fail(kInvalid, "requested anchor_rank exceeds eligible candidates");
+        return {};
+    }
     const SketchSetup su = sketch_setup(c, o, n);
     const AxisSpec& ax = su.ax;
     const int64_t ell = su.ell;
@@ -629,10 +782,36 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
         ISDF_PROFILE("phase:sketch_factors", s);
         sketch_factors(su.d, ell, o.seed, u, v);
     }
-    const int64_t ldy = n;
-    DeviceBuffer<double> Yt(static_cast<size_t>(ell * n), s);
     const double* aw = o.axis_weights.empty() ? nullptr : o.axis_weights.data();
     SketchQR qr;
+    if (density) {
+        const int64_t candidates = n;
+        const int64_t chunk = std::max<int64_t>(1024, std::min<int64_t>(n, (int64_t(1) << 28) / su.d));
+        DeviceBuffer<double> Yd = sketch_density_fp64(c, pts, kp, o.importance, ell, u, v, o.algorithm == 5,
+                                                      o.ao_threshold, chunk, s);
+        n = kp.n;
+        if (o.max_rank > std::min(n, su.physical_rank))
+            fail(kInvalid, "requested anchor_rank exceeds eligible candidates or physical pair rank");
+        if (o.debug)
+            std::fprintf(stderr,
+                         "[density sketch screening] candidates=%lld eligible=%lld screened_ao=%lld "
+                         "ao_norm2_threshold=%g\n",
+                         static_cast<long long>(candidates), static_cast<long long>(n),
+                         static_cast<long long>(candidates - n), o.ao_threshold);
+        if (n == 0) return {};
+        ISDF_PROFILE("phase:qrcp", s);
+        qr = qrcp_sketch(Yd.get(), n, ell, n, s);
+        const SketchRank r = sketch_rank(qr, ell, n, o, su.physical_rank);
+        std::vector<int64_t> selected(r.rank);
+        for (int64_t i = 0; i < r.rank; ++i)
+            ISDF_CUDA(cudaMemcpyAsync(&selected[i], kp.index.get() + qr.jpvt[i], sizeof(int64_t),
+                                      cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        fill_diag(diag_out, ell, r, qr);
+        return selected;
+    }
+    const int64_t ldy = n;
+    DeviceBuffer<double> Yt(static_cast<size_t>(ell * n), s);
     if (su.mixed) {
         MixedSketch ms = sketch_mixed(c, pts, kp, w, ax, aw, ell, u, v, Yt.get(), ldy, s, keep);
         ISDF_PROFILE("phase:qrcp", s);

@@ -350,6 +350,53 @@ def select_rand_sketch(ctx, pts, w, axes, tolerance=1e-10, max_rank=0, sketch_si
     return piv
 
 
+def select_density_sketch(ctx, pts, w, importance, normalized=False, tolerance=1e-10, max_rank=0,
+                          sketch_size=128, oversampling=16, seed=7, ao_screening_threshold=1e-24,
+                          return_details=False):
+    """AO-density Khatri-Rao sketch + dgeqp3 (``anchor_select_randomized_id.cpp:104-118,
+    131-146, 231-309``): candidates are the points with w != 0 and importance m != 0
+    whose squared AO norm q exceeds the screening threshold; column g of the
+    sketch is sqrt(m_g)/sqrt(ell) (f.u_s)(f.v_s) with f = phi_g, or phi_g/sqrt(q_g)
+    in the normalized (``density_col_norm``) form.  Only the AO axis."""
+    w = np.asarray(w, float)
+    importance = np.asarray(importance, float)
+    if importance.shape != (len(pts),):
+        raise ValueError("point_importance must have shape (ngrid,)")
+    if not np.isfinite(importance).all() or np.any(importance < 0):
+        raise ValueError("point_importance must be finite and nonnegative")
+    if not np.isfinite(ao_screening_threshold) or ao_screening_threshold < 0:
+        raise ValueError("AO screening threshold must be finite and nonnegative")
+    if oversampling == 0 or (not max_rank and sketch_size <= oversampling):
+        raise ValueError("invalid randomized ID grid, tolerance, batch, sketch or rank/oversampling")
+    keep = np.flatnonzero((w != 0) & (importance != 0))
+    if len(keep) == 0:
+        if max_rank:
+            raise ValueError("requested anchor_rank exceeds eligible candidates")
+        return ([], {}) if return_details else []
+    d = ctx.nao
+    ell = max_rank + oversampling if max_rank else sketch_size
+    ao = ctx.eval_ao(pts[keep])
+    q = np.einsum("ga,ga->g", ao, ao)
+    if not np.isfinite(q).all():
+        raise OverflowError("non-finite AO squared norm")
+    elig = q > ao_screening_threshold
+    keep, ao, q = keep[elig], ao[elig], q[elig]
+    n = len(keep)
+    physical_rank = d * (d + 1) // 2
+    if max_rank > min(n, physical_rank):
+        raise ValueError("requested anchor_rank exceeds eligible candidates or physical pair rank")
+    if n == 0:
+        return ([], {}) if return_details else []
+    u, v = sketch_factors(d, ell, seed)
+    f = ao / np.sqrt(q)[:, None] if normalized else ao
+    y = (np.sqrt(importance[keep]) / np.sqrt(ell))[:, None] * (f @ u) * (f @ v)
+    pos, det = sketch_qr_rank(y, ell, oversampling, tolerance, max_rank, physical_rank)
+    piv = [int(keep[p]) for p in pos]
+    if return_details:
+        return piv, dict(y=y, keep=keep, q=q, **det)
+    return piv
+
+
 # ---------------------------------------------------------------------------
 # fit and pair error (python/isdf.py)
 # ---------------------------------------------------------------------------

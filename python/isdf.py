@@ -34,6 +34,8 @@ from mp_isdf_b200 import inputs  # noqa: E402
 
 KHATRIRAO_SKETCH_TECHNIQUES = ("quadrature", "density", "density_col_norm")
 DENSITY_SKETCHES = ("density", "density_col_norm")
+SKETCH_ENUM = {"quadrature": "RandomizedQuadratureKhatriRao", "density": "RandomizedAODensityKhatriRao",
+               "density_col_norm": "RandomizedAODensityNormalizedKhatriRao"}
 SKETCH_ALGORITHMS = ("rand_sketch",)
 AXES = {
     "ao": mp_isdf.AxisType.AtomicOrbital,
@@ -83,18 +85,59 @@ class Molecule:
         return cls(d["atm"], d["bas"], d["env"])
 
 
+def _validate_point_importance(importance, ngrid):
+    """``python/isdf.py:231-235``."""
+    importance = np.asarray(importance, dtype=np.float64)
+    if importance.shape != (ngrid,) or not np.isfinite(importance).all() or np.any(importance < 0):
+        raise ValueError("point_importance must be a finite nonnegative array of shape (ngrid,)")
+    return np.ascontiguousarray(importance)
+
+
+def _normalized_pair_error(context, coords, anchor_ao, anchor_weights, theta, importance, threshold,
+                           space, batch=65536):
+    """Density-weighted relative-column error (``python/isdf.py:266-287``):
+    sum_g m_g |p_g - sum_k c_k p_k|^2 / q_g^2 over points with q_g = |phi_g|^2 >
+    threshold, relative to sum_g m_g; by the Gram expansion |p_g - C^T c|^2 =
+    q^2 - 2 c.h + c^T M c (h = (Phi_a phi_g)^2, M = (Phi_a Phi_a^T)^2), so no pair
+    vector is formed."""
+    M = (anchor_ao @ anchor_ao.T) ** 2
+    residual_sq = total = screened = 0.0
+    for g0 in range(0, len(coords), batch):
+        ao = context.eval_ao(coords[g0:g0 + batch], space=space)
+        m = importance[g0:g0 + batch]
+        q = np.einsum("ga,ga->g", ao, ao)
+        c = (np.asarray(theta)[:, g0:g0 + batch] * anchor_weights[:, None]).T
+        h = (ao @ anchor_ao.T) ** 2
+        r2 = q * q - 2 * np.einsum("gk,gk->g", c, h) + np.einsum("gk,kl,gl->g", c, M, c)
+        inc = (q > threshold) & (m != 0)
+        screened += float(m[q <= threshold].sum())
+        residual_sq += float(np.sum(m[inc] * np.maximum(r2[inc], 0.0) / q[inc] ** 2))
+        total += float(m[inc].sum())
+    return {"l2": float(np.sqrt(residual_sq)),
+            "relative": float(np.sqrt(residual_sq / total)) if total else 0.0,
+            "included_mass": float(total), "screened_mass": float(screened)}
+
+
 def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), axis_weights=None,
                space="auto", anchor_algorithm="qrcp_dense", sketch="quadrature",
                anchor_batch_size=128, fit_batch_size=2048, anchor_sketch_size=128,
                anchor_oversampling=16, anchor_seed=7, selection_only=False, debug=False,
                pair_space_error=False, report_timings=False, report_dimensions=False, grid=None,
-               precision="fp64"):
+               precision="fp64", point_importance=None, density_weight="electron_density",
+               ao_screening_threshold=1e-24):
     """Selection-to-fit slice of ``build_isdf`` (``python/isdf.py:287-672``).
 
     `grid` is an optional (coords, weights) pair; otherwise a Becke-partitioned
     atom-centred grid of the requested level is generated for the synthetic
     waters.  `precision` selects the FP64 or mixed (FP32 AO / split-BF16
     tensor-core / FP64 QR and solve) form on the B200.
+
+    Density sketches (`sketch="density"` / `"density_col_norm"`, rand_sketch,
+    AO axis only, FP64 form) weight pair columns by sqrt(point_importance) and
+    screen points whose squared AO norm is <= `ao_screening_threshold`
+    (``python/isdf.py:322-340``).  `point_importance` is the complete m on the
+    grid; generating it needs an RKS B3LYP density (PySCF), which this build
+    does not have, so it must be given.
     """
     started = time.perf_counter()
     last = started
@@ -122,10 +165,17 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
     if sketch_algorithm:
         if sketch not in KHATRIRAO_SKETCH_TECHNIQUES:
             raise ValueError(f"sketch must be one of {KHATRIRAO_SKETCH_TECHNIQUES} for rand_sketch")
-        if sketch in DENSITY_SKETCHES:
-            raise NotImplementedError("density Khatri--Rao sketches are outside the B200 hot path (NYI)")
     elif sketch != "quadrature":
         raise ValueError("non-default sketch requires anchor_algorithm='rand_sketch'")
+    density_sketch = sketch_algorithm and sketch in DENSITY_SKETCHES
+    if density_sketch and axis_types != [mp_isdf.AxisType.AtomicOrbital]:
+        raise NotImplementedError("density Khatri--Rao sketches with non-AO axis features are NYI")
+    if density_weight not in ("electron_density", "quadrature_density"):
+        raise ValueError("density_weight must be electron_density or quadrature_density")
+    if not np.isfinite(ao_screening_threshold) or ao_screening_threshold < 0:
+        raise ValueError("ao_screening_threshold must be finite and nonnegative")
+    if point_importance is not None and not density_sketch:
+        raise ValueError("point_importance requires CVT or a density sketch")
     if anchor_algorithm not in ("qrcp_dense", "qrcp_online", *SKETCH_ALGORITHMS):
         if anchor_algorithm in ("cvt", "rbrp", "rbrp_id"):
             raise NotImplementedError(f"{anchor_algorithm} is outside the B200 hot path (NYI)")
@@ -184,14 +234,24 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
             if anchor_rank > 0:
                 dims += f" requested_rank={anchor_rank} (anchor_sketch_size ignored)"
         print(dims, flush=True)
+    importance = None
+    if density_sketch:
+        if point_importance is None:
+            raise NotImplementedError("the selection density needs an RKS B3LYP calculation (PySCF), "
+                                      "which is not available here; pass point_importance")
+        importance = _validate_point_importance(point_importance, len(all_coords))
+        record("point_importance")
     algo = {"qrcp_dense": mp_isdf.LocalAnchorSelectionAlgorithm.QRColumnPivoting,
             "qrcp_online": mp_isdf.LocalAnchorSelectionAlgorithm.OnlineQRColumnPivoting,
             "rand_sketch": mp_isdf.LocalAnchorSelectionAlgorithm.RandomizedQuadratureKhatriRao}[anchor_algorithm]
+    if density_sketch:
+        algo = getattr(mp_isdf.LocalAnchorSelectionAlgorithm, SKETCH_ENUM[sketch])
     anchor_indices = np.asarray(selector.select(
         all_coords, all_weights, axis_types, tolerance=anchor_tol, max_rank=anchor_rank,
         algorithm=algo, space=space, batch_size=anchor_batch_size, debug=debug,
         sketch_size=anchor_sketch_size, oversampling=anchor_oversampling, seed=anchor_seed,
         axis_weights=list(axis_weights) if axis_weights is not None else [],
+        point_importance=importance, ao_screening_threshold=ao_screening_threshold,
         precision=precision), dtype=np.intp)
     if len(anchor_indices) == 0:
         raise ValueError("anchor selection found no anchors; adjust settings or grid")
@@ -217,6 +277,10 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
     pair_space_errors = None
     if pair_space_error:
         pair_space_errors = {"scalar": {"l2": fit["pair_l2"], "relative": fit["pair_relative"]}}
+        if importance is not None:
+            pair_space_errors["density_normalized"] = _normalized_pair_error(
+                context, coords, anchor_ao, anchor_weights, interp_vecs, importance[keep],
+                ao_screening_threshold, space)
         record("pair_space_check")
     # Overlap reconstruction (python/isdf.py:665-671); without int1e_ovlp the
     # reference overlap is the grid quadrature Phi^T diag(w) Phi (small systems).
@@ -256,6 +320,12 @@ def main(argv=None):
     parser.add_argument("--anchor-sketch-size", type=int, default=128)
     parser.add_argument("--anchor-oversampling", type=int, default=16)
     parser.add_argument("--anchor-seed", type=int, default=7)
+    parser.add_argument("--density-weight", choices=("electron_density", "quadrature_density"),
+                        default="electron_density", help="density sketch importance: rho or abs(w)*rho")
+    parser.add_argument("--ao-screening-threshold", type=float, default=1e-24,
+                        help="density sketch squared AO norm cutoff (selection only)")
+    parser.add_argument("--importance-file", default=None,
+                        help=".npy with the density sketch importance m over the grid (no RKS here)")
     parser.add_argument("--axes", default="ao")
     parser.add_argument("--space", choices=("auto", "host", "device"), default="auto")
     parser.add_argument("--pair-space-error", action="store_true")
@@ -270,6 +340,8 @@ def main(argv=None):
         parser.error("--anchor-rank must be nonnegative")
     if args.anchor_algorithm not in SKETCH_ALGORITHMS and args.sketch is not None:
         parser.error("--sketch requires --anchor-algorithm rand_sketch")
+    if not np.isfinite(args.ao_screening_threshold) or args.ao_screening_threshold < 0:
+        parser.error("--ao-screening-threshold must be finite and nonnegative")
     if args.anchor_batch_size <= 0:
         parser.error("--anchor-batch-size must be positive")
     if args.fit_batch_size <= 0:
@@ -314,7 +386,10 @@ def main(argv=None):
                         anchor_oversampling=args.anchor_oversampling, anchor_seed=args.anchor_seed,
                         pair_space_error=args.pair_space_error, report_timings=not args.debug,
                         debug=args.debug, report_dimensions=True, grid=grid,
-                        precision=args.precision)
+                        precision=args.precision,
+                        point_importance=np.load(args.importance_file) if args.importance_file else None,
+                        density_weight=args.density_weight,
+                        ao_screening_threshold=args.ao_screening_threshold)
     print(f"Grid points: {len(result['coordinates'])}; AOs: {result['X1'].shape[1]}; "
           f"anchors: {len(result['anchor_indices'])}")
     if args.anchor_rank and len(result["anchor_indices"]) == args.anchor_rank:
