@@ -264,6 +264,24 @@ int isdf_project_axes(isdf_ctx* ctx, const double* xyz_dev, int64_t ng, const in
                       int32_t naxes, const double* W_host, int32_t nout, int32_t precision,
                       double* out_dev, void* stream);
 
+/* Spherical-cell grid Coulomb metric between two sets of interpolation
+ * vectors (grid_cross_metric, python/isdf.py:80-97; with left = right and
+ * symmetrize = 1 it is grid_coulomb_metric, :48-68):
+ *   V[a][b] = sum_{g,h} left[a][g] w_g K_gh w_h right[b][h],
+ *   K_gh = 1/|r_g - r_h| (g != h; 0 for coincident points),
+ *   K_gg = (32/15) pi^2 (3/(4 pi))^(5/3) |w_g|^(-1/3).
+ * left: kl x n, right: kr x n (row-major, leading dimensions ldl, ldr >= n,
+ * not weight-scaled), xyz: n x 3, w: n; kr <= 64.  metric_host: kl x kr,
+ * (V + V^T)/2 when symmetrize (requires kl = kr).  FP64 throughout.  The
+ * device variant takes device pointers and a stream; the _host variant host
+ * buffers (ctx may be NULL there: the current device). */
+int isdf_grid_metric(isdf_ctx* ctx, const double* left_dev, int64_t ldl, int64_t kl, const double* right_dev,
+                     int64_t ldr, int64_t kr, const double* xyz_dev, const double* w_dev, int64_t n,
+                     int32_t symmetrize, double* metric_host, void* stream);
+int isdf_grid_metric_host(isdf_ctx* ctx, const double* left_host, int64_t kl, const double* right_host,
+                          int64_t kr, const double* xyz_host, const double* w_host, int64_t n,
+                          int32_t symmetrize, double* metric_host);
+
 /* Gaussian sketch factors of rand_sketch: U, V (d x ell, row-major u[a*ell+s])
  * from std::mt19937_64(seed) and std::mt19937_64(seed ^ 0x9e3779b97f4a7c15)
  * through std::normal_distribution<double>

@@ -28,6 +28,7 @@ SYMBOLS = [
     "isdf_profile_enable", "isdf_profile_read", "isdf_project_axes",
     "isdf_energy_gradient", "isdf_ctx_set_coords", "isdf_pair_error_terms_noalloc",
     "isdf_select_fit", "isdf_select_fit_host", "isdf_launch_count", "isdf_sketch_factors",
+    "isdf_grid_metric", "isdf_grid_metric_host",
     "isdf_sketch_shard_project", "isdf_sketch_shard_combine", "isdf_sketch_shard_free",
     "isdf_sketch_select_gathered", "isdf_fit_at",
 ]
@@ -115,6 +116,8 @@ def lib():
         L.isdf_launch_count.argtypes = []
         L.isdf_launch_count.restype = I64
         L.isdf_sketch_factors.argtypes = [I64, I64, ctypes.c_uint64, P, P]
+        L.isdf_grid_metric.argtypes = [P, P, I64, I64, P, I64, I64, P, P, I64, I32, P, P]
+        L.isdf_grid_metric_host.argtypes = [P, P, I64, P, I64, P, P, I64, I32, P]
         L.isdf_profile_read.argtypes = [I32, P, P, P, ctypes.POINTER(I32)]
         _lib = L
     return _lib
@@ -166,7 +169,13 @@ class Context:
             lib().isdf_ctx_destroy(self.h)
             self.h = None
 
-    __del__ = close
+    def __del__(self):
+        # at interpreter exit the module's globals may already be gone; the
+        # process teardown releases the device context then
+        try:
+            self.close()
+        except Exception:
+            pass
 
     # ---- device tensors ------------------------------------------------------
     def eval_ao(self, xyz, values=None, grad=None, dtype=None):
@@ -296,6 +305,17 @@ class Context:
                                       _stream(xyz)))
         return out
 
+    def grid_metric(self, xyz, w, left, right=None):
+        """Grid Coulomb metric of device tensors (left/right: k x n float64,
+        not weight-scaled); right=None gives the symmetrised metric of `left`."""
+        sym = right is None
+        right = left if sym else right
+        out = np.empty((left.shape[0], right.shape[0]), dtype=np.float64)
+        check(lib().isdf_grid_metric(self.h, _ptr(left), left.stride(0), left.shape[0], _ptr(right),
+                                     right.stride(0), right.shape[0], _ptr(xyz), _ptr(w), xyz.shape[0],
+                                     int(sym), _ptr(out), _stream(xyz)))
+        return out
+
     def set_coords(self, coords):
         """Move the atoms (natm x 3, bohr)."""
         c = _np(coords, np.float64).reshape(self.natm, 3)
@@ -421,6 +441,22 @@ def make_select_args(algorithm="rand_sketch", axes=("ao",), axis_weights=None, t
         args.point_importance = _ptr(imp)
     args.ao_screening_threshold = ao_screening_threshold
     return args, (ax, aw, imp)
+
+
+def grid_metric_host(left, xyz, w, right=None, ctx=None):
+    """Grid Coulomb metric between interpolation-vector sets (host arrays;
+    left/right: k x n, not weight-scaled).  right=None: the symmetrised metric
+    of `left` with itself."""
+    left = _np(left, np.float64)
+    sym = right is None
+    right = left if sym else _np(right, np.float64)
+    xyz = _np(xyz, np.float64).reshape(-1, 3)
+    w = _np(w, np.float64)
+    out = np.empty((left.shape[0], right.shape[0]), dtype=np.float64)
+    check(lib().isdf_grid_metric_host(ctx.h if ctx is not None else None, _ptr(left), left.shape[0],
+                                      _ptr(right), right.shape[0], _ptr(xyz), _ptr(w), len(w), int(sym),
+                                      _ptr(out)))
+    return out
 
 
 def sketch_factors(d, ell, seed):

@@ -2,6 +2,7 @@
 #include "../../include/isdf_b200.h"
 #include "isdf_adjoint.h"
 #include "isdf_fit.h"
+#include "isdf_metric.h"
 #include "isdf_project.h"
 #include "isdf_select.h"
 
@@ -567,6 +568,44 @@ int isdf_ctx_set_coords(isdf_ctx* ctx, const double* coords) {
         if (!coords) isdf::fail(isdf::kInvalid, "null coordinates");
         ISDF_CUDA(cudaDeviceSynchronize());
         isdf::set_atom_coords(c, coords);
+    });
+}
+
+int isdf_grid_metric(isdf_ctx* ctx, const double* left, int64_t ldl, int64_t kl, const double* right,
+                     int64_t ldr, int64_t kr, const double* xyz, const double* w, int64_t n,
+                     int32_t symmetrize, double* metric_host, void* stream) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        if (kl < 0 || kr < 0 || n < 0 || kl > INT32_MAX || kr > INT32_MAX)
+            isdf::fail(isdf::kInvalid, "invalid grid metric sizes");
+        if (!metric_host || (n > 0 && (!xyz || !w)) || (n > 0 && kl > 0 && !left) || (n > 0 && kr > 0 && !right))
+            isdf::fail(isdf::kInvalid, "null grid metric buffer");
+        isdf::grid_metric(left, ldl, static_cast<int>(kl), right, ldr, static_cast<int>(kr), xyz, w, n,
+                          symmetrize != 0, metric_host, as_stream(stream));
+    });
+}
+
+int isdf_grid_metric_host(isdf_ctx* ctx, const double* left, int64_t kl, const double* right, int64_t kr,
+                          const double* xyz, const double* w, int64_t n, int32_t symmetrize,
+                          double* metric_host) {
+    return guarded([&] {
+        int dev = 0;
+        if (ctx) dev = ctx_of(ctx).device;
+        else ISDF_CUDA(cudaGetDevice(&dev));
+        DeviceGuard dg(dev);
+        if (kl < 0 || kr < 0 || n < 0 || kl > INT32_MAX || kr > INT32_MAX)
+            isdf::fail(isdf::kInvalid, "invalid grid metric sizes");
+        if (!metric_host || (n > 0 && (!xyz || !w)) || (n > 0 && kl > 0 && !left) || (n > 0 && kr > 0 && !right))
+            isdf::fail(isdf::kInvalid, "null grid metric buffer");
+        cudaStream_t s = ctx ? ctx->stream : nullptr;
+        isdf::DeviceBuffer<double> dl, dr, dx, dw;
+        upload(dl, left, static_cast<size_t>(kl * n), s);
+        upload(dr, right, static_cast<size_t>(kr * n), s);
+        upload(dx, xyz, static_cast<size_t>(3 * n), s);
+        upload(dw, w, static_cast<size_t>(n), s);
+        isdf::grid_metric(dl.get(), n, static_cast<int>(kl), dr.get(), n, static_cast<int>(kr), dx.get(),
+                          dw.get(), n, symmetrize != 0, metric_host, s);
     });
 }
 

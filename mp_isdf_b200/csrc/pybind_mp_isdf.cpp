@@ -272,6 +272,35 @@ PYBIND11_MODULE(mp_isdf, m) {
             return c.evaluate(coords, true, space);
         }, py::arg("coords"), py::arg("space") = "auto", "Return x,y,z AO gradients with shape (3, ngrid, nao).");
 
+    // grid Coulomb metric (python/isdf.py:48-97): interpolation vectors k x n
+    auto metric = [](const FloatArray& left, py::object right, const FloatArray& coords, const FloatArray& weights) {
+        if (left.ndim() != 2) throw std::invalid_argument("interpolation vectors must have shape (k, ngrid)");
+        auto pts = points_of(coords, "expected coords[ngrid,3]");
+        const int64_t n = pts.shape(0);
+        if (weights.ndim() != 1 || weights.shape(0) != n || left.shape(1) != n)
+            throw std::invalid_argument("interpolation vectors, coords and weights disagree on ngrid");
+        const bool sym = right.is_none();
+        FloatArray r = sym ? left : right.cast<FloatArray>();
+        if (r.ndim() != 2 || r.shape(1) != n)
+            throw std::invalid_argument("interpolation vectors, coords and weights disagree on ngrid");
+        py::array_t<double> out({left.shape(0), r.shape(0)});
+        int rc;
+        {
+            py::gil_scoped_release release;
+            rc = isdf_grid_metric_host(nullptr, left.data(), left.shape(0), r.data(), r.shape(0), pts.data(),
+                                       weights.data(), n, sym ? 1 : 0, out.mutable_data());
+        }
+        check(rc);
+        return out;
+    };
+    m.def("grid_coulomb_metric", [metric](const FloatArray& interp_vecs, const FloatArray& coords,
+                                          const FloatArray& weights) {
+        return metric(interp_vecs, py::none(), coords, weights);
+    }, py::arg("interp_vecs"), py::arg("coords"), py::arg("weights"));
+    m.def("grid_cross_metric", [metric](const FloatArray& left, const FloatArray& right, const FloatArray& coords,
+                                        const FloatArray& weights) {
+        return metric(left, right, coords, weights);
+    }, py::arg("left"), py::arg("right"), py::arg("coords"), py::arg("weights"));
     m.def("eval_ao", [](const IntArray& atm, const IntArray& bas, const FloatArray& env,
                         const FloatArray& coords, const std::string& space) {
         Context c(atm, bas, env);

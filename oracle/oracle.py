@@ -398,6 +398,47 @@ def select_density_sketch(ctx, pts, w, importance, normalized=False, tolerance=1
 
 
 # ---------------------------------------------------------------------------
+# grid Coulomb metric (python/isdf.py:48-97)
+# ---------------------------------------------------------------------------
+C_SPHERE = (32.0 / 15.0) * np.pi ** 2 * (3.0 / (4.0 * np.pi)) ** (5.0 / 3.0)
+
+
+def grid_cross_metric(left, right, coords, weights, block=256):
+    """sum_{g,h} left[a,g] w_g K_gh w_h right[b,h] with K_gh = 1/|r_g - r_h|
+    off the diagonal (0 for coincident points) and K_gg = c |w_g|^(-1/3)
+    (``python/isdf.py:80-97``), accumulated over row blocks of K."""
+    coords = np.asarray(coords, float)
+    weights = np.asarray(weights, float)
+    lw = np.asarray(left, float).T * weights[:, None]
+    rw = np.asarray(right, float).T * weights[:, None]
+    out = np.zeros((lw.shape[1], rw.shape[1]))
+    for g0 in range(0, len(weights), block):
+        g1 = min(g0 + block, len(weights))
+        r = np.linalg.norm(coords[g0:g1, None, :] - coords[None, :, :], axis=-1)
+        kern = np.divide(1.0, r, out=np.zeros_like(r), where=r > 0)
+        rows = np.arange(g0, g1)
+        kern[rows - g0, rows] = C_SPHERE * np.abs(weights[rows]) ** (-1.0 / 3.0)
+        out += lw[g0:g1].T @ (kern @ rw)
+    return out
+
+
+def grid_coulomb_metric(interp_vecs, coords, weights):
+    """Symmetrised metric of one set (``python/isdf.py:48-68``)."""
+    v = grid_cross_metric(interp_vecs, interp_vecs, coords, weights)
+    return 0.5 * (v + v.T)
+
+
+def isdf_jk(x, z, dm):
+    """ISDF J and K of a symmetric density matrix (``python/isdf.py:130-151``):
+    (mu nu|lam sig) ~ sum_pq X[p,mu] X[p,nu] Z[p,q] X[q,lam] X[q,sig]."""
+    x = np.asarray(x, float)
+    d = x @ dm @ x.T
+    j = x.T @ ((z @ np.diag(d))[:, None] * x)
+    k = x.T @ (z * d) @ x
+    return 0.5 * (j + j.T), 0.5 * (k + k.T)
+
+
+# ---------------------------------------------------------------------------
 # fit and pair error (python/isdf.py)
 # ---------------------------------------------------------------------------
 def physical_pair_refit(anchor_pairs, anchor_weights, ao, batch_size=2048):

@@ -7,8 +7,9 @@ module of this repository.  PySCF is not required: molecules are either
 synthetic water clusters (``--molecule water:4x4x4[:seed]``, the seeded
 cc-pVDZ-shaped basis of ``mp_isdf_b200.inputs``) or libcint tables loaded from
 an ``.npz`` file with arrays atm, bas, env (and optionally coords, weights).
-The Coulomb metric, J/K and derivative targets are outside this path
-(``--no-metric`` is implied).
+The Coulomb metric is available in its grid form (``--metric-algorithm grid``,
+computed on the GPU; without ``--no-metric``); the integral-direct Cholesky
+metrics and derivative targets are outside this path.
 
 Example:
   python python/isdf.py --molecule water:2x2x1 --level 2 --axes ao \
@@ -85,6 +86,46 @@ class Molecule:
         return cls(d["atm"], d["bas"], d["env"])
 
 
+def grid_coulomb_metric(interp_vecs, coords, weights):
+    """Spherical-cell grid Coulomb metric (``python/isdf.py:48-68``), computed
+    on the GPU by the library's FP64 all-pairs kernel.  interp_vecs has shape
+    (Nanchor, Ngrid) and is NOT weight-scaled."""
+    return mp_isdf.grid_coulomb_metric(np.ascontiguousarray(interp_vecs, dtype=np.float64),
+                                       np.ascontiguousarray(coords, dtype=np.float64),
+                                       np.ascontiguousarray(weights, dtype=np.float64))
+
+
+def grid_cross_metric(left, right, coords, weights):
+    """Grid Coulomb metric between two independently fitted channel sets
+    (``python/isdf.py:80-97``), on the GPU."""
+    return mp_isdf.grid_cross_metric(np.ascontiguousarray(left, dtype=np.float64),
+                                     np.ascontiguousarray(right, dtype=np.float64),
+                                     np.ascontiguousarray(coords, dtype=np.float64),
+                                     np.ascontiguousarray(weights, dtype=np.float64))
+
+
+def evaluate_isdf_jk(result, dm):
+    """Return (J, K) for a real symmetric AO density matrix
+    (``python/isdf.py:130-151``).  The metric in `result` already includes both
+    anchor quadrature weights; (mu nu|lam sig) is approximated by
+    sum_pq X[p,mu] X[p,nu] Z[p,q] X[q,lam] X[q,sig] with X[p,mu] = AO_mu(anchor_p)."""
+    x = np.asarray(result["X1"])
+    z = result["coulomb_metric"]
+    if z is None:
+        raise ValueError("a Coulomb metric is required to evaluate J and K")
+    density = np.asarray(dm, dtype=np.float64)
+    if density.shape != (x.shape[1], x.shape[1]) or not np.isfinite(density).all():
+        raise ValueError("dm must be a finite AO density matrix of shape (nao,nao)")
+    if not np.allclose(density, density.T, rtol=1e-12, atol=1e-12):
+        raise ValueError("dm must be symmetric")
+    if np.shape(z) != (len(x), len(x)):
+        raise ValueError("Coulomb metric has the wrong anchor dimensions")
+    anchor_density = x @ density @ x.T
+    coulomb = x.T @ ((z @ np.diag(anchor_density))[:, None] * x)
+    exchange = x.T @ (z * anchor_density) @ x
+    return 0.5 * (coulomb + coulomb.T), 0.5 * (exchange + exchange.T)
+
+
 def _validate_point_importance(importance, ngrid):
     """``python/isdf.py:231-235``."""
     importance = np.asarray(importance, dtype=np.float64)
@@ -124,7 +165,7 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
                anchor_oversampling=16, anchor_seed=7, selection_only=False, debug=False,
                pair_space_error=False, report_timings=False, report_dimensions=False, grid=None,
                precision="fp64", point_importance=None, density_weight="electron_density",
-               ao_screening_threshold=1e-24):
+               ao_screening_threshold=1e-24, compute_metric=False, metric_algorithm="grid"):
     """Selection-to-fit slice of ``build_isdf`` (``python/isdf.py:287-672``).
 
     `grid` is an optional (coords, weights) pair; otherwise a Becke-partitioned
@@ -138,6 +179,11 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
     (``python/isdf.py:322-340``).  `point_importance` is the complete m on the
     grid; generating it needs an RKS B3LYP density (PySCF), which this build
     does not have, so it must be given.
+
+    `compute_metric=True` with `metric_algorithm="grid"` adds the anchor-
+    weighted grid Coulomb metric (``python/isdf.py:674-683``) as
+    `coulomb_metric`; the integral-direct Cholesky metrics need ERIs that are
+    outside this path.
     """
     started = time.perf_counter()
     last = started
@@ -176,6 +222,12 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
         raise ValueError("ao_screening_threshold must be finite and nonnegative")
     if point_importance is not None and not density_sketch:
         raise ValueError("point_importance requires CVT or a density sketch")
+    if metric_algorithm not in ("grid", "unblocked_greedy", "unblocked_uniform"):
+        raise ValueError(f"unknown metric algorithm: {metric_algorithm!r}")
+    if selection_only and compute_metric:
+        raise ValueError("selection_only requires compute_metric=False")
+    if compute_metric and metric_algorithm != "grid":
+        raise NotImplementedError("the integral-direct Cholesky metrics are outside the B200 hot path (NYI)")
     if anchor_algorithm not in ("qrcp_dense", "qrcp_online", *SKETCH_ALGORITHMS):
         if anchor_algorithm in ("cvt", "rbrp", "rbrp_id"):
             raise NotImplementedError(f"{anchor_algorithm} is outside the B200 hot path (NYI)")
@@ -260,6 +312,7 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
         return {"anchor_indices": anchor_indices, "anchor_coords": all_coords[anchor_indices],
                 "anchor_weights": all_weights[anchor_indices], "coordinates": all_coords[keep],
                 "weights": all_weights[keep], "interp_vecs": None, "pair_space_errors": None,
+                "coulomb_metric": None,
                 "fit_diagnostics": None, "elapsed": last - started, "timings": timings}
 
     coords = all_coords[keep]
@@ -294,7 +347,12 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
         overlap_relative_error = (np.linalg.norm(overlap_approx - overlap) /
                                   max(np.linalg.norm(overlap), 1e-30))
     record("overlap_check")
-    return {"anchor_indices": anchor_indices, "fit_diagnostics": fit_diagnostics,
+    metric = None
+    if compute_metric:
+        raw = grid_coulomb_metric(interp_vecs, coords, weights)
+        metric = anchor_weights[:, None] * raw * anchor_weights[None, :]
+        record("coulomb_metric")
+    return {"anchor_indices": anchor_indices, "fit_diagnostics": fit_diagnostics, "coulomb_metric": metric,
             "anchor_coords": anchor_coords, "anchor_weights": anchor_weights,
             "coordinates": coords, "weights": weights, "interp_vecs": interp_vecs,
             "overlap_reconstruction": overlap_approx,
@@ -329,8 +387,10 @@ def main(argv=None):
     parser.add_argument("--axes", default="ao")
     parser.add_argument("--space", choices=("auto", "host", "device"), default="auto")
     parser.add_argument("--pair-space-error", action="store_true")
-    parser.add_argument("--no-metric", action="store_true",
-                        help="accepted for compatibility; the metric is outside this path")
+    parser.add_argument("--no-metric", action="store_true", help="skip the Coulomb metric")
+    parser.add_argument("--metric-algorithm", choices=("grid", "unblocked_greedy", "unblocked_uniform"),
+                        default=None, help="grid: spherical-cell grid metric on the GPU (the "
+                        "Cholesky metrics are outside this path); without it no metric is computed")
     parser.add_argument("--debug", action="store_true")
     parser.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
     parser.add_argument("--grid-file", default=None, help=".npz with coords and weights")
@@ -389,7 +449,9 @@ def main(argv=None):
                         precision=args.precision,
                         point_importance=np.load(args.importance_file) if args.importance_file else None,
                         density_weight=args.density_weight,
-                        ao_screening_threshold=args.ao_screening_threshold)
+                        ao_screening_threshold=args.ao_screening_threshold,
+                        compute_metric=bool(args.metric_algorithm) and not args.no_metric,
+                        metric_algorithm=args.metric_algorithm or "grid")
     print(f"Grid points: {len(result['coordinates'])}; AOs: {result['X1'].shape[1]}; "
           f"anchors: {len(result['anchor_indices'])}")
     if args.anchor_rank and len(result["anchor_indices"]) == args.anchor_rank:
@@ -401,6 +463,10 @@ def main(argv=None):
         for label, error in result["pair_space_errors"].items():
             print(f"Pair-space {label} grid L2 error: {error['l2']:.3e}; "
                   f"relative error: {error['relative']:.3e}")
+    if result["coulomb_metric"] is not None:
+        z = result["coulomb_metric"]
+        print(f"Coulomb metric (grid): {z.shape[0]}x{z.shape[1]}; "
+              f"diagonal range [{np.min(np.diag(z)):.6e}, {np.max(np.diag(z)):.6e}]")
     if not args.debug:
         print(f"ISDF build time: {result['elapsed']:.6f} s")
     else:
