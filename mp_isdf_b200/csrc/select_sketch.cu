@@ -23,6 +23,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <future>
 #include <limits>
 #include <random>
 #include <thread>
@@ -764,6 +765,22 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
             fail(kNotImplemented, "density Khatri-Rao sketches are implemented in the FP64 form only");
     }
     ISDF_PROFILE("phase:select", s);
+    // The Gaussian factors depend on (d, ell, seed) only, and ell on the kept
+    // count only through the ILP64 limit: when the requested ell is within the
+    // limit for the whole grid it is the final one, so the factors are drawn on
+    // a host thread while the device compacts the points.
+    std::vector<double> u, v;
+    const int64_t d_pre = static_cast<int64_t>(o.axes.size()) * c.nao;
+    const int64_t ell_req = o.max_rank ? o.max_rank + o.oversampling : o.sketch_size;
+    int64_t ell_pre = -1;
+    std::future<void> pre;
+    if (ng > 0 && ell_req > o.oversampling && ell_req <= std::numeric_limits<int64_t>::max() / ng &&
+        d_pre > 0 && d_pre <= (int64_t(1) << 40) / ell_req) {
+        ell_pre = ell_req;
+        pre = std::async(std::launch::async, [&u, &v, d_pre, ell_pre, &o] {
+            sketch_factors(d_pre, ell_pre, o.seed, u, v);
+        });
+    }
     KeptPoints kp;
     {
         ISDF_PROFILE("phase:compact", s);
@@ -777,10 +794,10 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
     const SketchSetup su = sketch_setup(c, o, n);
     const AxisSpec& ax = su.ax;
     const int64_t ell = su.ell;
-    std::vector<double> u, v;
     {
         ISDF_PROFILE("phase:sketch_factors", s);
-        sketch_factors(su.d, ell, o.seed, u, v);
+        if (pre.valid()) pre.get();
+        if (ell_pre != ell || d_pre != su.d) sketch_factors(su.d, ell, o.seed, u, v);
     }
     const double* aw = o.axis_weights.empty() ? nullptr : o.axis_weights.data();
     SketchQR qr;
