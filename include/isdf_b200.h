@@ -88,6 +88,16 @@ int isdf_evaluate_axis(isdf_ctx* ctx, const double* xyz_dev, int64_t ng, const i
                        int32_t naxes, double* out_dev, void* stream);
 int isdf_evaluate_axis_host(isdf_ctx* ctx, const double* xyz_host, int64_t ng,
                             const int32_t* axes_host, int32_t naxes, double* out_host);
+/* The same with OccupiedOrbital entries allowed (anchor_select.cpp:18-52,
+ * anchor_select_impl.hpp:69-72): their block is psi_j = sum_mu phi_mu C[mu][j],
+ * j < nocc, with mo_coeff_host row-major nao x nao and 1 <= nocc <= nao; the
+ * output has ng x (sum of the entries' widths) features (nao per AO/gradient
+ * entry, nocc per occupied entry).  out_dev / out_host as above. */
+int isdf_evaluate_axis_mo(isdf_ctx* ctx, const double* xyz_dev, int64_t ng, const int32_t* axes_host,
+                          int32_t naxes, const double* mo_coeff_host, int64_t nocc, double* out_dev,
+                          void* stream);
+int isdf_evaluate_axis_mo_host(isdf_ctx* ctx, const double* xyz_host, int64_t ng, const int32_t* axes_host,
+                               int32_t naxes, const double* mo_coeff_host, int64_t nocc, double* out_host);
 
 /* ---- anchor selection ------------------------------------------------------
  * Replaces AnchorSelection::select (cpp/src/anchor_select.cpp:79-173,
@@ -114,6 +124,11 @@ typedef struct isdf_select_args {
      * (cpp/src/anchor_select_randomized_id.cpp:104-115, 231-260). */
     const double* point_importance;
     double ao_screening_threshold;   /* default 1e-24 */
+    /* OccupiedOrbital axis: row-major nao x nao MO coefficients in host memory
+     * and the occupied count (cpp/src/anchor_select.cpp:43-49).  The FP64 forms
+     * evaluate it; a mixed rand_sketch with an occupied entry runs in FP64. */
+    const double* mo_coeff;
+    int64_t nocc;
 } isdf_select_args;
 
 typedef struct isdf_select_info {

@@ -28,7 +28,7 @@ SYMBOLS = [
     "isdf_profile_enable", "isdf_profile_read", "isdf_project_axes",
     "isdf_energy_gradient", "isdf_ctx_set_coords", "isdf_pair_error_terms_noalloc",
     "isdf_select_fit", "isdf_select_fit_host", "isdf_launch_count", "isdf_sketch_factors",
-    "isdf_grid_metric", "isdf_grid_metric_host",
+    "isdf_grid_metric", "isdf_grid_metric_host", "isdf_evaluate_axis_mo", "isdf_evaluate_axis_mo_host",
     "isdf_sketch_shard_project", "isdf_sketch_shard_combine", "isdf_sketch_shard_free",
     "isdf_sketch_select_gathered", "isdf_fit_at",
 ]
@@ -43,7 +43,7 @@ class SelectArgs(ctypes.Structure):
                 ("tolerance", F64), ("max_rank", I64), ("batch_size", I64),
                 ("sketch_size", I64), ("oversampling", I64), ("seed", ctypes.c_uint64),
                 ("precision", I32), ("debug", I32), ("point_importance", P),
-                ("ao_screening_threshold", F64)]
+                ("ao_screening_threshold", F64), ("mo_coeff", P), ("nocc", I64)]
 
 
 class SelectInfo(ctypes.Structure):
@@ -83,6 +83,8 @@ def lib():
         L.isdf_eval_ao_host.argtypes = [P, P, I64, P, P]
         L.isdf_evaluate_axis.argtypes = [P, P, I64, P, I32, P, P]
         L.isdf_evaluate_axis_host.argtypes = [P, P, I64, P, I32, P]
+        L.isdf_evaluate_axis_mo.argtypes = [P, P, I64, P, I32, P, I64, P, P]
+        L.isdf_evaluate_axis_mo_host.argtypes = [P, P, I64, P, I32, P, I64, P]
         L.isdf_select_args_default.argtypes = [ctypes.POINTER(SelectArgs)]
         L.isdf_select.argtypes = [P, ctypes.POINTER(SelectArgs), P, P, I64, P, I64,
                                   ctypes.POINTER(I64), ctypes.POINTER(SelectInfo), P]
@@ -190,11 +192,12 @@ class Context:
 
     def select(self, xyz, w, algorithm="rand_sketch", axes=("ao",), axis_weights=None,
                tolerance=1e-10, max_rank=0, batch_size=128, sketch_size=128, oversampling=16,
-               seed=7, precision="fp64", debug=False, point_importance=None, ao_screening_threshold=1e-24):
+               seed=7, precision="fp64", debug=False, point_importance=None, ao_screening_threshold=1e-24,
+               mo_coeff=None, nocc=0):
         """Anchor selection on device-resident points/weights; returns (pivots, info)."""
         args, keep = make_select_args(algorithm, axes, axis_weights, tolerance, max_rank,
                                       batch_size, sketch_size, oversampling, seed, precision, debug,
-                                      point_importance, ao_screening_threshold)
+                                      point_importance, ao_screening_threshold, mo_coeff, nocc)
         ng = xyz.shape[0]
         piv = np.empty(max(ng, 1), dtype=np.int64)
         n = I64()
@@ -316,6 +319,18 @@ class Context:
                                      int(sym), _ptr(out), _stream(xyz)))
         return out
 
+    def evaluate_axis_host(self, xyz, axes, mo_coeff=None, nocc=0):
+        """Concatenated axis features (host arrays; occupied-orbital entries
+        nocc wide from the row-major nao x nao `mo_coeff`)."""
+        ax = np.array([AXES[a] if isinstance(a, str) else int(a) for a in axes], dtype=np.int32)
+        xyz = _np(xyz, np.float64).reshape(-1, 3)
+        mo = None if mo_coeff is None else _np(mo_coeff, np.float64)
+        d = sum(nocc if a == 4 else self.nao for a in ax)
+        out = np.empty((len(xyz), d), dtype=np.float64)
+        check(lib().isdf_evaluate_axis_mo_host(self.h, _ptr(xyz), len(xyz), _ptr(ax), len(ax), _ptr(mo),
+                                               int(nocc), _ptr(out)))
+        return out
+
     def set_coords(self, coords):
         """Move the atoms (natm x 3, bohr)."""
         c = _np(coords, np.float64).reshape(self.natm, 3)
@@ -415,7 +430,8 @@ class SketchShard:
 
 def make_select_args(algorithm="rand_sketch", axes=("ao",), axis_weights=None, tolerance=1e-10,
                      max_rank=0, batch_size=128, sketch_size=128, oversampling=16, seed=7,
-                     precision="fp64", debug=False, point_importance=None, ao_screening_threshold=1e-24):
+                     precision="fp64", debug=False, point_importance=None, ao_screening_threshold=1e-24,
+                     mo_coeff=None, nocc=0):
     """isdf_select_args (and the arrays it points at, to keep alive).  For the
     density sketches `point_importance` is a float64 vector over the grid: a
     CUDA tensor for the device entry points, host memory for the _host ones."""
@@ -440,7 +456,12 @@ def make_select_args(algorithm="rand_sketch", axes=("ao",), axis_weights=None, t
         imp = point_importance if hasattr(point_importance, "data_ptr") else _np(point_importance, np.float64)
         args.point_importance = _ptr(imp)
     args.ao_screening_threshold = ao_screening_threshold
-    return args, (ax, aw, imp)
+    mo = None
+    if mo_coeff is not None:
+        mo = _np(mo_coeff, np.float64)
+        args.mo_coeff = _ptr(mo)
+        args.nocc = int(nocc)
+    return args, (ax, aw, imp, mo)
 
 
 def grid_metric_host(left, xyz, w, right=None, ctx=None):

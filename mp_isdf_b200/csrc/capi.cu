@@ -79,6 +79,8 @@ isdf::SelectOptions options_of(const isdf_select_args* a) {
     o.debug = a->debug != 0;
     o.importance = a->point_importance;
     o.ao_threshold = a->ao_screening_threshold;
+    o.mo_host = a->mo_coeff;
+    o.nocc = a->nocc;
     if (o.max_rank < 0 || o.batch_size < 0 || o.sketch_size < 0 || o.oversampling < 0)
         isdf::fail(isdf::kInvalid, "sizes must be nonnegative");
     return o;
@@ -200,35 +202,49 @@ int isdf_eval_ao_host(isdf_ctx* ctx, const double* xyz, int64_t ng, double* valu
     });
 }
 
-int isdf_evaluate_axis(isdf_ctx* ctx, const double* xyz, int64_t ng, const int32_t* axes,
-                       int32_t naxes, double* out, void* stream) {
+int isdf_evaluate_axis_mo(isdf_ctx* ctx, const double* xyz, int64_t ng, const int32_t* axes, int32_t naxes,
+                          const double* mo_host, int64_t nocc, double* out, void* stream) {
     return guarded([&] {
         auto& c = ctx_of(ctx);
         DeviceGuard dg(c.device);
+        cudaStream_t s = as_stream(stream);
         if (!axes) isdf::fail(isdf::kInvalid, "axis list must not be empty");
-        isdf::AxisSpec ax = isdf::make_axis_spec(c, axes, naxes);
-        isdf::eval_axis_features<double>(c, xyz, nullptr, ng, ax, out,
-                                         static_cast<int64_t>(naxes) * c.nao, nullptr, nullptr,
-                                         as_stream(stream));
+        isdf::DeviceBuffer<double> dmo;
+        if (mo_host) upload(dmo, mo_host, static_cast<size_t>(c.nao) * c.nao, s);
+        isdf::AxisSpec ax = isdf::make_axis_spec(c, axes, naxes, dmo.get(), nocc);
+        isdf::eval_axis_features<double>(c, xyz, nullptr, ng, ax, out, ax.d, nullptr, nullptr, s);
+        ISDF_CUDA(cudaStreamSynchronize(s));   // the MO copy outlives its use
     });
 }
 
-int isdf_evaluate_axis_host(isdf_ctx* ctx, const double* xyz, int64_t ng, const int32_t* axes,
-                            int32_t naxes, double* out) {
+int isdf_evaluate_axis_mo_host(isdf_ctx* ctx, const double* xyz, int64_t ng, const int32_t* axes,
+                               int32_t naxes, const double* mo_host, int64_t nocc, double* out) {
     return guarded([&] {
         auto& c = ctx_of(ctx);
         DeviceGuard dg(c.device);
         cudaStream_t s = ctx->stream;
         if (!axes) isdf::fail(isdf::kInvalid, "axis list must not be empty");
-        isdf::AxisSpec ax = isdf::make_axis_spec(c, axes, naxes);
+        isdf::DeviceBuffer<double> dmo;
+        if (mo_host) upload(dmo, mo_host, static_cast<size_t>(c.nao) * c.nao, s);
+        isdf::AxisSpec ax = isdf::make_axis_spec(c, axes, naxes, dmo.get(), nocc);
         if (ng <= 0) return;
-        const int64_t d = static_cast<int64_t>(naxes) * c.nao;
+        const int64_t d = ax.d;
         isdf::DeviceBuffer<double> dx, dout(static_cast<size_t>(ng * d), s);
         upload(dx, xyz, static_cast<size_t>(3 * ng), s);
         isdf::eval_axis_features<double>(c, dx.get(), nullptr, ng, ax, dout.get(), d, nullptr, nullptr, s);
         ISDF_CUDA(cudaMemcpyAsync(out, dout.get(), ng * d * sizeof(double), cudaMemcpyDeviceToHost, s));
         ISDF_CUDA(cudaStreamSynchronize(s));
     });
+}
+
+int isdf_evaluate_axis(isdf_ctx* ctx, const double* xyz, int64_t ng, const int32_t* axes,
+                       int32_t naxes, double* out, void* stream) {
+    return isdf_evaluate_axis_mo(ctx, xyz, ng, axes, naxes, nullptr, 0, out, stream);
+}
+
+int isdf_evaluate_axis_host(isdf_ctx* ctx, const double* xyz, int64_t ng, const int32_t* axes,
+                            int32_t naxes, double* out) {
+    return isdf_evaluate_axis_mo_host(ctx, xyz, ng, axes, naxes, nullptr, 0, out);
 }
 
 void isdf_select_args_default(isdf_select_args* a) {

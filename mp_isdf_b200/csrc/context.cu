@@ -158,7 +158,8 @@ struct AxisSink {
         if (!((ax->need_mask >> C) & 1)) return;
         if (count) sq[C] += static_cast<double>(v) * static_cast<double>(v);
         for (int a = 0; a < ax->naxes; ++a)
-            if (ax->comp[a] == C) out[p * ld + off[a] + ao] = static_cast<T>(ax->scale[a] * static_cast<double>(v));
+            if (ax->comp[a] == C && !ax->occ[a])
+                out[p * ld + off[a] + ao] = static_cast<T>(ax->scale[a] * static_cast<double>(v));
     }
 };
 
@@ -189,7 +190,7 @@ ao_axis_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __rest
     __shared__ double red[kPtsPerBlock * kShellLanes][4];
     __shared__ int off[16];
     const int tid = threadIdx.y * kPtsPerBlock + threadIdx.x;
-    if (tid < ax.naxes) off[tid] = tid * nao;
+    if (tid < ax.naxes) off[tid] = ax.offset[tid];
     __syncthreads();
     const int64_t p = static_cast<int64_t>(blockIdx.x) * kPtsPerBlock + threadIdx.x;
     AxisSink<T> sink{out, p, ld, &ax, off, {0, 0, 0, 0}, false};
@@ -213,6 +214,31 @@ ao_axis_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __rest
         }
         if (tid < 4 && ((ax.need_mask >> tid) & 1)) atomicAdd(&sumsq[tid], red[0][tid]);
     }
+}
+
+// Occupied-orbital block: out[p][j] *= scale, and the squared unscaled values
+// of the counted points added into sumsq[4].
+__global__ void occ_block_kernel(double* out, int64_t ld, int64_t n, int nocc, double scale,
+                                 const int64_t* __restrict__ index, const double* __restrict__ weights,
+                                 double* sumsq) {
+    __shared__ double red[256];
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    double sq = 0;
+    if (i < n * nocc) {
+        const int64_t p = i / nocc, j = i % nocc;
+        const double v = out[p * ld + j];
+        const int64_t gi = index ? index[p] : p;
+        if (sumsq && (weights == nullptr || weights[gi] != 0.0)) sq = v * v;
+        out[p * ld + j] = scale * v;
+    }
+    if (!sumsq) return;
+    red[threadIdx.x] = sq;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && red[0] != 0.0) atomicAdd(&sumsq[4], red[0]);
 }
 
 template <class T> const T* exps_of(const Context& c);
@@ -266,6 +292,37 @@ void eval_axis_features(const Context& c, const double* pts, const int64_t* inde
             c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, index, n, ax,
             out, ld, sumsq, weights, c.nao);
     ISDF_LAUNCH_CHECK();
+    if (!ax.has_occ) return;
+    // occupied-orbital entries: psi = Phi C_occ (anchor_select_impl.hpp:69-72),
+    // from the AO values of the same points, then scaled (sumsq slot 4)
+    if constexpr (sizeof(T) != 8) {
+        fail(kNotImplemented, "the OccupiedOrbital axis is evaluated in FP64 only");
+    } else {
+        AxisSpec vs{};
+        vs.naxes = 1;
+        vs.comp[0] = 0;
+        vs.scale[0] = 1.0;
+        vs.need_mask = 1;
+        vs.offset[0] = 0;
+        vs.width[0] = c.nao;
+        vs.occ[0] = false;
+        vs.d = c.nao;
+        DeviceBuffer<double> phi(static_cast<size_t>(n) * c.nao, s);
+        ao_axis_kernel<double, false><<<static_cast<unsigned>(nb), block, 0, s>>>(
+            c.d_shells, c.nshell, c.d_exp, c.d_coef, pts, index, n, vs, phi.get(), c.nao, nullptr, nullptr,
+            c.nao);
+        ISDF_LAUNCH_CHECK();
+        bool counted = false;   // repeated occupied entries add their sum of squares once
+        for (int a = 0; a < ax.naxes; ++a) {
+            if (!ax.occ[a]) continue;
+            gemm_f64(n, ax.nocc, c.nao, phi.get(), c.nao, 0, ax.mo, c.nao, 0, out + ax.offset[a], ld, 0, 1,
+                     false, s);
+            occ_block_kernel<<<static_cast<unsigned>((n * ax.nocc + 255) / 256), 256, 0, s>>>(
+                out + ax.offset[a], ld, n, ax.nocc, ax.scale[a], index, weights, counted ? nullptr : sumsq);
+            ISDF_LAUNCH_CHECK();
+            counted = true;
+        }
+    }
 }
 
 template void eval_ao<double>(const Context&, const double*, int64_t, double*, double*, int64_t, cudaStream_t);

@@ -187,6 +187,16 @@ struct AxisSpec {
     int comp[16];      // component of each axis entry (0..3)
     double scale[16];  // scale of each axis entry
     int need_mask = 0; // bit c set if component c is needed
+    // feature layout: entry a occupies features [offset[a], offset[a] + width[a])
+    int offset[16];
+    int width[16];
+    int64_t d = 0;               // total features
+    // occupied-orbital entries: psi_j = sum_mu phi_mu C[mu][j], j < nocc, with
+    // C row-major nao x nao in device memory (mo)
+    bool occ[16];
+    int nocc = 0;
+    const double* mo = nullptr;
+    bool has_occ = false;
 };
 template <class T>
 void eval_axis_features(const Context& c, const double* pts, const int64_t* index, int64_t n,

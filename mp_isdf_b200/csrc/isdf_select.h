@@ -31,7 +31,17 @@ struct SelectOptions {
     bool debug = false;
     const double* importance = nullptr;  // density sketches: per grid point (device)
     double ao_threshold = 1e-24;         // density sketches: squared AO norm screen
+    const double* mo_host = nullptr;     // OccupiedOrbital: row-major nao x nao (host)
+    int64_t nocc = 0;
 };
+
+// Device copy of the MO coefficients of the options (empty without them) and
+// the axis spec built with it.
+struct AxisSetup {
+    DeviceBuffer<double> mo;
+    AxisSpec ax;
+};
+AxisSetup make_axis_setup(const Context& c, const SelectOptions& o, cudaStream_t s);
 
 struct SketchDiagnostics {
     int64_t ell = 0, numerical_rank = 0, cap = 0, rank = 0;
@@ -69,7 +79,9 @@ struct ExactSketchSource {
     double* delta = nullptr;         // per-column absolute error bounds (0 = exact)
 };
 
-AxisSpec make_axis_spec(const Context& c, const int32_t* axes, int naxes);
+// mo (device, row-major nao x nao) and nocc are needed for the OccupiedOrbital axis.
+AxisSpec make_axis_spec(const Context& c, const int32_t* axes, int naxes, const double* mo = nullptr,
+                        int64_t nocc = 0);
 void validate_axis_weights(const double* axis_weights, int naxes);
 std::vector<double> axis_scales_from_sumsq(const AxisSpec& ax, const double* sumsq4,
                                            const double* axis_weights, bool any_eligible);
@@ -124,8 +136,10 @@ struct SketchSetup {
     AxisSpec ax{};
     int64_t d = 0, ell = 0, physical_rank = 0;
     bool mixed = false;              // mixed-precision form applies
+    DeviceBuffer<double> mo;         // device MO coefficients (occupied-orbital axis)
 };
-SketchSetup sketch_setup(const Context& c, const SelectOptions& o, int64_t n);
+// n = 0: option checks only; n > 0 also copies the MO coefficients to the device (on s).
+SketchSetup sketch_setup(const Context& c, const SelectOptions& o, int64_t n, cudaStream_t s = nullptr);
 
 // Tails, numerical rank, cap and the selected rank of a sketch QR
 // (cpp/src/anchor_select_randomized_id.cpp:320-374).

@@ -106,17 +106,25 @@ std::vector<int32_t> read_axes(py::object axes) {
     return out;
 }
 
-void check_occupied(const std::vector<int32_t>& axes, py::object mo_coeff, std::size_t nocc, int64_t nao) {
+// The MO coefficients of an OccupiedOrbital axis (cpp/src/anchor_select_pybind.cpp:43-53,
+// cpp/src/anchor_select.cpp:43-49); an empty array when no entry needs them.
+FloatArray check_occupied(const std::vector<int32_t>& axes, py::object mo_coeff, std::size_t nocc, int64_t nao) {
     bool occ = false;
     for (auto a : axes) occ |= a == ISDF_AXIS_OCC;
-    if (!occ) return;
+    if (!occ) return FloatArray();
     if (mo_coeff.is_none() || nocc == 0 || static_cast<int64_t>(nocc) > nao)
         throw std::invalid_argument(
             "OccupiedOrbital requires row-major (nao,nao) RHF mo_coeff and 1 <= nocc <= nao");
     auto c = mo_coeff.cast<FloatArray>();
     if (c.ndim() != 2 || c.shape(0) != nao || c.shape(1) != nao)
         throw std::invalid_argument("mo_coeff must have shape (nao,nao)");
-    throw NotImplemented("the OccupiedOrbital axis is outside the B200 hot path (NYI)");
+    return c;
+}
+
+int64_t feature_width(const std::vector<int32_t>& axes, std::size_t nocc, int64_t nao) {
+    int64_t d = 0;
+    for (auto a : axes) d += a == ISDF_AXIS_OCC ? static_cast<int64_t>(nocc) : nao;
+    return d;
 }
 
 struct Selector {
@@ -158,7 +166,7 @@ struct Selector {
             if (ax.size() != 1 || ax[0] != ISDF_AXIS_AO)
                 throw std::invalid_argument("density Khatri-Rao sketches with non-AO axis features are NYI");
         }
-        check_occupied(ax, mo_coeff, nocc, ctx->nao);
+        FloatArray mo = check_occupied(ax, mo_coeff, nocc, ctx->nao);
         parse_space(space);
         if (!axis_weights.empty() && axis_weights.size() != ax.size())
             throw std::invalid_argument("axis weights must match axes");
@@ -182,6 +190,10 @@ struct Selector {
             a.point_importance = importance.data();
             a.ao_screening_threshold = ao_screening_threshold;
         }
+        if (mo) {
+            a.mo_coeff = mo.data();
+            a.nocc = static_cast<int64_t>(nocc);
+        }
         const int64_t ng = pts.shape(0);
         std::vector<int64_t> piv(static_cast<size_t>(std::max<int64_t>(ng, 1)));
         int64_t np = 0;
@@ -200,16 +212,17 @@ struct Selector {
     py::array_t<double> evaluate_axis(const FloatArray& points, py::object axes, py::object mo_coeff,
                                       std::size_t nocc, const std::string& space) {
         auto ax = read_axes(axes);
-        check_occupied(ax, mo_coeff, nocc, ctx->nao);
+        FloatArray mo = check_occupied(ax, mo_coeff, nocc, ctx->nao);
         parse_space(space);
         auto pts = points_of(points, "expected points[ngrid,3]");
         const py::ssize_t ng = pts.shape(0);
-        py::array_t<double> out({ng, static_cast<py::ssize_t>(ax.size() * ctx->nao)});
+        py::array_t<double> out({ng, static_cast<py::ssize_t>(feature_width(ax, nocc, ctx->nao))});
         int rc;
         {
             py::gil_scoped_release release;
-            rc = isdf_evaluate_axis_host(ctx->h, pts.data(), ng, ax.data(), static_cast<int32_t>(ax.size()),
-                                         out.mutable_data());
+            rc = isdf_evaluate_axis_mo_host(ctx->h, pts.data(), ng, ax.data(), static_cast<int32_t>(ax.size()),
+                                            mo ? mo.data() : nullptr, static_cast<int64_t>(nocc),
+                                            out.mutable_data());
         }
         check(rc);
         return out;

@@ -38,11 +38,16 @@ __global__ void gather_weights_kernel(const double* __restrict__ w, const int64_
 }
 
 // F[:, a-block] *= scale[a]
-__global__ void scale_columns_kernel(double* F, int64_t n, int64_t d, int nao,
+// Column j of F (the features of axis entry a, offset[a] <= j < offset[a] +
+// width[a]) times scales[a].
+__global__ void scale_columns_kernel(double* F, int64_t n, int64_t d, AxisSpec ax,
                                      const double* __restrict__ scales) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n * d) return;
-    F[i] *= scales[(i % d) / nao];
+    const int j = static_cast<int>(i % d);
+    int a = 0;
+    while (a + 1 < ax.naxes && j >= ax.offset[a + 1]) ++a;
+    F[i] *= scales[a];
 }
 
 __global__ void init_est_kernel(const double* __restrict__ sw, const double* __restrict__ nf,
@@ -215,8 +220,9 @@ std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const d
                               : "invalid weights, axis list, or tolerance");
     validate_axis_weights(o.axis_weights.empty() ? nullptr : o.axis_weights.data(),
                           static_cast<int>(o.axes.size()));
-    AxisSpec ax = make_axis_spec(c, o.axes.data(), static_cast<int>(o.axes.size()));
-    const int64_t d = static_cast<int64_t>(ax.naxes) * c.nao;
+    AxisSetup axs = make_axis_setup(c, o, s);
+    const AxisSpec& ax = axs.ax;
+    const int64_t d = ax.d;
     if (d > 46340)
         fail(kOverflow, online ? "AO pair dimension is too large" : "pair-product matrix is too large");
     KeptPoints kp = compact_points(pts, w, ng, s);
@@ -228,19 +234,19 @@ std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const d
     const int64_t m = q.m;
     q.nblocks = static_cast<int>((n + kNT - 1) / kNT);
     q.F.reset(static_cast<size_t>(n * d), s);
-    DeviceBuffer<double> sumsq(4, s);
+    DeviceBuffer<double> sumsq(5, s);
     sumsq.zero(s);
     eval_axis_features<double>(c, pts, kp.index.get(), n, ax, q.F.get(), d,
                                ax.naxes > 1 ? sumsq.get() : nullptr, nullptr, s);
     if (ax.naxes > 1) {
-        double h[4];
+        double h[5];
         ISDF_CUDA(cudaMemcpyAsync(h, sumsq.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
         ISDF_CUDA(cudaStreamSynchronize(s));
         auto sc = axis_scales_from_sumsq(ax, h, o.axis_weights.empty() ? nullptr : o.axis_weights.data(), true);
         DeviceBuffer<double> dsc(sc.size(), s);
         ISDF_CUDA(cudaMemcpyAsync(dsc.get(), sc.data(), sc.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         scale_columns_kernel<<<static_cast<unsigned>((n * d + 255) / 256), 256, 0, s>>>(
-            q.F.get(), n, d, c.nao, dsc.get());
+            q.F.get(), n, d, ax, dsc.get());
         ISDF_LAUNCH_CHECK();
         ISDF_CUDA(cudaStreamSynchronize(s));
     }

@@ -91,21 +91,46 @@ KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStr
 // ------------------------------------------------------------------------------
 // axis bookkeeping
 // ------------------------------------------------------------------------------
-AxisSpec make_axis_spec(const Context& c, const int32_t* axes, int naxes) {
+AxisSpec make_axis_spec(const Context& c, const int32_t* axes, int naxes, const double* mo, int64_t nocc) {
     require(naxes > 0, "axis list must not be empty");
     if (naxes > 16) fail(kNotImplemented, "more than 16 axis entries are not supported");
     AxisSpec ax{};
     ax.naxes = naxes;
+    int64_t d = 0;
     for (int a = 0; a < naxes; ++a) {
         const int t = axes[a];
-        if (t == 4) fail(kNotImplemented, "the OccupiedOrbital axis is not implemented on the B200 path");
-        require(t >= 0 && t <= 3, "unknown AxisType");
-        ax.comp[a] = t;
+        require(t >= 0 && t <= 4, "unknown AxisType");
+        ax.occ[a] = t == 4;
+        if (t == 4) {
+            // cpp/src/anchor_select.cpp:43-49
+            if (!mo || nocc < 1 || nocc > c.nao)
+                fail(kInvalid, "OccupiedOrbital requires row-major (nao,nao) RHF mo_coeff and 1 <= nocc <= nao");
+            ax.has_occ = true;
+            ax.nocc = static_cast<int>(nocc);
+            ax.mo = mo;
+        }
+        ax.comp[a] = t == 4 ? 0 : t;
         ax.scale[a] = 1.0;
-        ax.need_mask |= 1 << t;
+        ax.need_mask |= 1 << ax.comp[a];
+        ax.width[a] = t == 4 ? static_cast<int>(nocc) : c.nao;
+        ax.offset[a] = static_cast<int>(d);
+        d += ax.width[a];
     }
-    require(c.nao > 0, "no orbital features available");
+    require(c.nao > 0 && d > 0, "no orbital features available");
+    require(d < (int64_t(1) << 30), "axis feature count is too large");
+    ax.d = d;
     return ax;
+}
+
+AxisSetup make_axis_setup(const Context& c, const SelectOptions& o, cudaStream_t s) {
+    AxisSetup st;
+    if (o.mo_host && c.nao > 0) {
+        st.mo.reset(static_cast<size_t>(c.nao) * c.nao, s);
+        ISDF_CUDA(cudaMemcpyAsync(st.mo.get(), o.mo_host, static_cast<size_t>(c.nao) * c.nao * sizeof(double),
+                                  cudaMemcpyHostToDevice, s));
+    }
+    st.ax = make_axis_spec(c, o.axes.data(), static_cast<int>(o.axes.size()), st.mo.get(), o.nocc);
+    return st;
 }
 
 std::vector<double> axis_scales_from_sumsq(const AxisSpec& ax, const double* sumsq4,
@@ -113,7 +138,8 @@ std::vector<double> axis_scales_from_sumsq(const AxisSpec& ax, const double* sum
     std::vector<double> scales;
     if (!any_eligible) return scales;
     for (int a = 0; a < ax.naxes; ++a) {
-        const double norm = std::sqrt(sumsq4[ax.comp[a]]);
+        // slot 4 holds the occupied-orbital features' sum of squares
+        const double norm = std::sqrt(sumsq4[ax.occ[a] ? 4 : ax.comp[a]]);
         if (!(norm > 0) || !std::isfinite(norm))
             fail(kInvalid, "axis Frobenius norm must be finite and positive");
         const double scale = (axis_weights ? axis_weights[a] : 1.0) / norm;
@@ -325,9 +351,8 @@ void sketch_fp64(const Context& c, const double* pts, const KeptPoints& kp, cons
                  const AxisSpec& ax, const double* axis_weights, int64_t ell,
                  const std::vector<double>& u, const std::vector<double>& v, double* Yt,
                  int64_t ldy, int64_t chunk, cudaStream_t s) {
-    const int nao = c.nao;
     const int naxes = ax.naxes;
-    const int64_t d = static_cast<int64_t>(naxes) * nao;
+    const int64_t d = ax.d;
     const int64_t n = kp.n;
     // W[j][0..ell) = U row j, W[j][ell..2ell) = V row j
     std::vector<double> hw(static_cast<size_t>(d * 2 * ell));
@@ -340,21 +365,30 @@ void sketch_fp64(const Context& c, const double* pts, const KeptPoints& kp, cons
     ISDF_CUDA(cudaMemcpyAsync(W.get(), hw.data(), hw.size() * sizeof(double),
                               cudaMemcpyHostToDevice, s));
     DeviceBuffer<double> P(static_cast<size_t>(n * naxes * 2 * ell), s);
-    DeviceBuffer<double> sumsq(4, s);
+    DeviceBuffer<double> sumsq(5, s);
     sumsq.zero(s);
     chunk = std::max<int64_t>(1, std::min(chunk, n));
     DeviceBuffer<double> F(static_cast<size_t>(chunk * d), s);
+    bool uniform = true;   // every entry nao wide: one batched GEMM
+    for (int a = 0; a < naxes; ++a) uniform = uniform && ax.width[a] == c.nao && ax.offset[a] == a * c.nao;
     for (int64_t g0 = 0; g0 < n; g0 += chunk) {
         const int64_t b = std::min(chunk, n - g0);
         eval_axis_features<double>(c, pts, kp.index.get() + g0, b, ax, F.get(), d,
                                    naxes > 1 ? sumsq.get() : nullptr, nullptr, s);
         // per-axis partial projections P[g][a][0..2ell)
-        gemm_f64(b, 2 * ell, nao, F.get(), d, nao, W.get(), 2 * ell, nao * 2 * ell,
-                 P.get() + g0 * naxes * 2 * ell, naxes * 2 * ell, 2 * ell, naxes, false, s);
+        if (uniform) {
+            gemm_f64(b, 2 * ell, c.nao, F.get(), d, c.nao, W.get(), 2 * ell, c.nao * 2 * ell,
+                     P.get() + g0 * naxes * 2 * ell, naxes * 2 * ell, 2 * ell, naxes, false, s);
+        } else {
+            for (int a = 0; a < naxes; ++a)
+                gemm_f64(b, 2 * ell, ax.width[a], F.get() + ax.offset[a], d, 0,
+                         W.get() + static_cast<int64_t>(ax.offset[a]) * 2 * ell, 2 * ell, 0,
+                         P.get() + g0 * naxes * 2 * ell + a * 2 * ell, naxes * 2 * ell, 0, 1, false, s);
+        }
     }
     DeviceBuffer<double> dscales;
     if (naxes > 1) {
-        double h[4];
+        double h[5];
         ISDF_CUDA(cudaMemcpyAsync(h, sumsq.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
         ISDF_CUDA(cudaStreamSynchronize(s));
         auto sc = axis_scales_from_sumsq(ax, h, axis_weights, n > 0);
@@ -674,13 +708,15 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
 // ------------------------------------------------------------------------------
 // rand_sketch (quadrature) driver
 // ------------------------------------------------------------------------------
-SketchSetup sketch_setup(const Context& c, const SelectOptions& o, int64_t n) {
+SketchSetup sketch_setup(const Context& c, const SelectOptions& o, int64_t n, cudaStream_t s) {
     if (!std::isfinite(o.tolerance) || o.tolerance < 0 || o.batch_size <= 0 ||
         o.oversampling <= 0 || (!o.max_rank && o.sketch_size <= o.oversampling))
         fail(kInvalid, "invalid randomized ID grid, tolerance, batch, sketch or rank/oversampling");
     SketchSetup su;
-    su.ax = make_axis_spec(c, o.axes.data(), static_cast<int>(o.axes.size()));
-    su.d = static_cast<int64_t>(su.ax.naxes) * c.nao;
+    // the host MO pointer only validates here; the device copy is made below
+    su.ax = make_axis_spec(c, o.axes.data(), static_cast<int>(o.axes.size()), o.mo_host, o.nocc);
+    su.ax.mo = nullptr;
+    su.d = su.ax.d;
     if (o.max_rank > std::numeric_limits<int64_t>::max() - o.oversampling)
         fail(kOverflow, "randomized ID rank + oversampling overflows size_t");
     const int64_t requested = o.max_rank ? o.max_rank + o.oversampling : o.sketch_size;
@@ -698,7 +734,14 @@ SketchSetup sketch_setup(const Context& c, const SelectOptions& o, int64_t n) {
     // the mixed form needs the tensor-core shape and room for one point's AO
     // components in shared memory for the FP64 re-verification of candidates
     su.mixed = o.precision == 1 && project_tc_supported(su.ax.naxes, static_cast<int>(2 * su.ell)) &&
-               su.ell <= 64 && c.nao <= kMaxVerifiedNao;
+               su.ell <= 64 && c.nao <= kMaxVerifiedNao && !su.ax.has_occ;
+    if (su.ax.has_occ) {
+        // occupied-orbital features are FP64 only: the FP64 form runs
+        su.mo.reset(static_cast<size_t>(c.nao) * c.nao, s);
+        ISDF_CUDA(cudaMemcpyAsync(su.mo.get(), o.mo_host, static_cast<size_t>(c.nao) * c.nao * sizeof(double),
+                                  cudaMemcpyHostToDevice, s));
+        su.ax.mo = su.mo.get();
+    }
     return su;
 }
 
@@ -791,7 +834,7 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
         if (density && o.max_rank) fail(kInvalid, "requested anchor_rank exceeds eligible candidates");
         return {};
     }
-    const SketchSetup su = sketch_setup(c, o, n);
+    const SketchSetup su = sketch_setup(c, o, n, s);
     const AxisSpec& ax = su.ax;
     const int64_t ell = su.ell;
     {
@@ -861,7 +904,8 @@ void sketch_shard_project(const Context& c, const double* pts, const double* w, 
     st.w = w;
     st.ng = ng;
     st.kp = compact_points(pts, w, ng, s);
-    st.su = sketch_setup(c, o, std::max<int64_t>(n_total, 1));
+    st.su = sketch_setup(c, o, std::max<int64_t>(n_total, 1), s);
+    if (st.su.ax.has_occ) fail(kInvalid, "grid-sharded selection supports the ao, dx, dy, dz axes");
     const int64_t n = st.kp.n, ell = st.su.ell, d = st.su.d;
     const int naxes = st.su.ax.naxes, nout = static_cast<int>(2 * ell);
     sketch_factors(d, ell, o.seed, st.u, st.v);
@@ -960,7 +1004,8 @@ std::vector<int64_t> select_sketch_gathered(const Context& c, const SelectOption
                                             const std::vector<double>& scales, SketchDiagnostics* diag_out,
                                             cudaStream_t s) {
     if (n == 0) return {};
-    const SketchSetup su = sketch_setup(c, o, n);
+    const SketchSetup su = sketch_setup(c, o, n, s);
+    if (su.ax.has_occ) fail(kInvalid, "grid-sharded selection supports the ao, dx, dy, dz axes");
     require(static_cast<int>(scales.size()) == su.ax.naxes, "one scale per axis entry is required");
     SketchQR qr;
     if (delta && su.mixed) {

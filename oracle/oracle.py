@@ -258,6 +258,68 @@ def axis_scales(ctx, pts, w, axes, axis_weights=None, exact_order=True):
     return factors / norms
 
 
+def occ_features(ctx, pts, axes, mo_coeff=None, nocc=0, scales=None):
+    """Concatenated axis features with OccupiedOrbital entries (code 4)
+    (``cpp/src/anchor_select.cpp:18-52``, ``anchor_select_impl.hpp:55-77``):
+    AO values (0), gradients (1..3), and psi_j = sum_mu phi_mu C[mu][j],
+    j < nocc (4), each block times its scale."""
+    if 4 in list(axes) and (mo_coeff is None or not 1 <= nocc <= ctx.nao):
+        raise ValueError("OccupiedOrbital requires row-major (nao,nao) RHF mo_coeff and 1 <= nocc <= nao")
+    ao = ctx.eval_ao(pts)
+    grad = ctx.eval_ao_gradient(pts) if any(a in (1, 2, 3) for a in axes) else None
+    blocks = []
+    for i, a in enumerate(axes):
+        if a == 0:
+            b = ao
+        elif a == 4:
+            b = ao @ np.asarray(mo_coeff, float)[:, :nocc]
+        else:
+            b = grad[a - 1]
+        blocks.append(b * (1.0 if scales is None else scales[i]))
+    return np.hstack(blocks)
+
+
+def occ_axis_scales(ctx, pts, w, axes, mo_coeff, nocc, axis_weights=None):
+    """Global Frobenius scales (``cpp/src/anchor_select.cpp:437-480``) over the
+    nonzero-weight points, with occupied-orbital entries."""
+    if len(axes) <= 1:
+        return None
+    keep = np.asarray(w, float) != 0
+    f = occ_features(ctx, pts[keep], axes, mo_coeff, nocc)
+    widths = [nocc if a == 4 else ctx.nao for a in axes]
+    edges = np.cumsum([0] + widths)
+    norms = np.array([np.linalg.norm(f[:, edges[i]:edges[i + 1]]) for i in range(len(axes))])
+    factors = np.ones(len(axes)) if not axis_weights else np.asarray(axis_weights, float)
+    return factors / norms
+
+
+def select_qrcp_dense_features(f, keep, tolerance=1e-10, max_rank=0, w=None):
+    """qrcp_dense (dgeqp3 of the explicit pair matrix) over given features of the
+    kept points; returns original indices."""
+    from scipy.linalg import qr
+    A = pair_matrix(f, w)
+    m, n = A.shape
+    _, r, piv = qr(A, pivoting=True, mode="economic")
+    cap = min(m, n, max_rank if max_rank else min(m, n))
+    diag = np.abs(np.diag(r))
+    first = diag[0] if cap else 0.0
+    out = []
+    for i in range(cap):
+        if first == 0 or diag[i] <= tolerance * first:
+            break
+        out.append(int(keep[piv[i]]))
+    return out
+
+
+def select_rand_sketch_features(f, keep, w, ell, oversampling, seed, tolerance=1e-10, max_rank=0):
+    """Quadrature sketch + dgeqp3 + rank rule over given (scaled) features."""
+    d = f.shape[1]
+    u, v = sketch_factors(d, ell, seed)
+    y = (np.sqrt(np.abs(w)) / np.sqrt(ell))[:, None] * (f @ u) * (f @ v)
+    pos, _ = sketch_qr_rank(y, ell, oversampling, tolerance, max_rank, d * (d + 1) // 2)
+    return [int(keep[p]) for p in pos]
+
+
 def pair_matrix(features, w):
     """A[:, g] = sqrt|w_g| f_g (x) f_g (``cpp/src/anchor_select_qrcp.cpp:253-267``)."""
     outer = np.einsum("gi,gj->gij", features, features).reshape(len(features), -1)

@@ -165,7 +165,8 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
                anchor_oversampling=16, anchor_seed=7, selection_only=False, debug=False,
                pair_space_error=False, report_timings=False, report_dimensions=False, grid=None,
                precision="fp64", point_importance=None, density_weight="electron_density",
-               ao_screening_threshold=1e-24, compute_metric=False, metric_algorithm="grid"):
+               ao_screening_threshold=1e-24, compute_metric=False, metric_algorithm="grid",
+               mo_coeff=None, nocc=0):
     """Selection-to-fit slice of ``build_isdf`` (``python/isdf.py:287-672``).
 
     `grid` is an optional (coords, weights) pair; otherwise a Becke-partitioned
@@ -179,6 +180,10 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
     (``python/isdf.py:322-340``).  `point_importance` is the complete m on the
     grid; generating it needs an RKS B3LYP density (PySCF), which this build
     does not have, so it must be given.
+
+    The occupied-orbital axis (`"occ"`) takes the row-major (nao, nao) RHF
+    `mo_coeff` and `nocc` (the reference takes them from a PySCF RHF,
+    ``python/isdf.py:505-511``).
 
     `compute_metric=True` with `metric_algorithm="grid"` adds the anchor-
     weighted grid Coulomb metric (``python/isdf.py:674-683``) as
@@ -251,8 +256,10 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
         raise ValueError("anchor_seed must be an unsigned 64-bit integer")
     if selection_only and pair_space_error:
         raise ValueError("pair_space_error requires fitting; disable selection_only")
-    if mp_isdf.AxisType.OccupiedOrbital in axis_types:
-        raise NotImplementedError("the occupied-orbital axis needs an RHF and is outside this path")
+    needs_occ = mp_isdf.AxisType.OccupiedOrbital in axis_types
+    if needs_occ and mo_coeff is None:
+        raise NotImplementedError("the occupied-orbital axis needs RHF MO coefficients (PySCF is not "
+                                  "available here); pass mo_coeff and nocc")
 
     if grid is None:
         if mol.symbols is None:
@@ -271,7 +278,7 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
     selector = mp_isdf.AnchorSelection(context)
     record("context")
     nao = context.nao
-    axis_width = nao * len(axis_types)
+    axis_width = sum(nocc if a == mp_isdf.AxisType.OccupiedOrbital else nao for a in axis_types)
     pair_rank_ceiling = axis_width * (axis_width + 1) // 2
     if report_dimensions:
         dims = (f"[ISDF dimensions] AOs={nao} axis_features={axis_width} "
@@ -304,6 +311,7 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
         sketch_size=anchor_sketch_size, oversampling=anchor_oversampling, seed=anchor_seed,
         axis_weights=list(axis_weights) if axis_weights is not None else [],
         point_importance=importance, ao_screening_threshold=ao_screening_threshold,
+        mo_coeff=np.ascontiguousarray(mo_coeff) if needs_occ else None, nocc=nocc if needs_occ else 0,
         precision=precision), dtype=np.intp)
     if len(anchor_indices) == 0:
         raise ValueError("anchor selection found no anchors; adjust settings or grid")
