@@ -43,6 +43,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--widened", action="store_true",
+                    help="also time the widened rows on this workload: the grid Coulomb metric of the "
+                         "fitted Theta, the FP64 density (column-normalized) sketch and the FP64 "
+                         "quadrature sketch with an occupied-orbital axis")
     ap.add_argument("--mode", choices=("auto", "sharded", "replicas"), default="auto",
                     help="N > 1: shard one cluster's grid over the ranks (auto, for rand_sketch "
                          "configs) or run one cluster per rank")
@@ -231,6 +235,94 @@ def time_adjoint(ctx, mol, x, wt, anchors, cfg, steps=3):
     return {"s": statistics.mean(times), "step_times_s": times, "energy": e,
             "grad_norm": float(np.linalg.norm(g)), "form": "FP64, fused grid pass: AO values and gradients recomputed per 128-point tile, never stored",
             "electrons": cfg["electrons"]}
+
+
+def _event_time(fn, reps=2):
+    """Seconds of the last of `reps` calls, CUDA events around each."""
+    import torch
+    out, t = None, 0.0
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        out = fn()
+        b.record()
+        torch.cuda.synchronize()
+        t = a.elapsed_time(b) / 1e3
+    return out, t
+
+
+def time_widened(ctx, mol, x, wt, w, theta, k, n_kept, cfg):
+    """The rows widened beyond the selection + fit path, on the bench workload:
+    the grid Coulomb metric of the fitted Theta (python/isdf.py:48-68), the FP64
+    density_col_norm sketch (importance = |w| times a seeded factor in
+    [0.5, 1.5]) and the FP64 quadrature sketch over the ao + occ axes (a seeded
+    orthogonal nao x nao MO matrix, nocc = electrons / 2)."""
+    import torch
+    keep = torch.as_tensor(w != 0, device=x.device)
+    xk, wk = x[keep].contiguous(), wt[keep].contiguous()
+    th = theta[:k * n_kept].view(k, n_kept)
+    _, t_metric = _event_time(lambda: ctx.grid_metric(xk, wk, th), reps=1)
+    rng = np.random.default_rng(cfg["seed"])
+    imp = torch.as_tensor(np.abs(w) * rng.uniform(0.5, 1.5, len(w)), device=x.device)
+    ov = cfg.get("oversampling", 16)
+    (piv_d, _), t_dens = _event_time(lambda: ctx.select(
+        x, wt, algorithm="rand_sketch_density_col_norm", axes=("ao",), max_rank=k, oversampling=ov,
+        seed=cfg.get("sketch_seed", 7), point_importance=imp))
+    nocc = max(1, int(cfg.get("electrons", 2 * k)) // 2)
+    mo, _ = np.linalg.qr(rng.normal(size=(mol.nao, mol.nao)))
+    (piv_o, _), t_occ = _event_time(lambda: ctx.select(
+        x, wt, algorithm="rand_sketch", axes=("ao", "occ"), max_rank=k, oversampling=ov,
+        seed=cfg.get("sketch_seed", 7), mo_coeff=np.ascontiguousarray(mo), nocc=nocc))
+    # FP64 roofline denominator: a cuBLAS DGEMM burst on this GPU (the measured
+    # peaks file holds HBM and BF16 only)
+    A = torch.randn(8192, 8192, dtype=torch.float64, device=x.device)
+    _, t_gemm = _event_time(lambda: A @ A, reps=3)
+    fp64_peak = 2.0 * 8192 ** 3 / t_gemm / 1e12
+    pairs = float(n_kept) * n_kept
+    flops_pair = 8 + 2 * k      # 3 differences, r^2 (1 mul + 2 FMA), k FMAs; rsqrt counted once
+    achieved = pairs * flops_pair / t_metric / 1e12
+    # CPU beside it: the oracle's restatements on bounded samples, scaled
+    from oracle import oracle as O
+    keep_idx = np.flatnonzero(w != 0)
+    rs = np.random.default_rng(1)
+    sub = np.sort(rs.choice(keep_idx, size=min(12000, len(keep_idx)), replace=False))
+    th_h = th.cpu().numpy()
+    pos = np.searchsorted(keep_idx, sub)
+    t0 = time.perf_counter()
+    O.grid_coulomb_metric(th_h[:, pos], np.asarray(x[keep].cpu())[pos], w[sub])
+    cpu_metric = (time.perf_counter() - t0) * (len(keep_idx) / len(sub)) ** 2
+    oc = O.OracleContext(mol.atm, mol.bas, mol.env)
+    sub2 = np.sort(rs.choice(keep_idx, size=min(3000, len(keep_idx)), replace=False))
+    pts_h = np.asarray(x.cpu())
+    t0 = time.perf_counter()
+    O.select_density_sketch(oc, pts_h[sub2], w[sub2], imp.cpu().numpy()[sub2], normalized=True, max_rank=k,
+                            oversampling=ov, seed=cfg.get("sketch_seed", 7))
+    cpu_dens = (time.perf_counter() - t0) * len(keep_idx) / len(sub2)
+    t0 = time.perf_counter()
+    sc = O.occ_axis_scales(oc, pts_h[sub2], w[sub2], [0, 4], mo, nocc)
+    f = O.occ_features(oc, pts_h[sub2], [0, 4], mo, nocc, sc)
+    O.select_rand_sketch_features(f, sub2, w[sub2], k + ov, ov, cfg.get("sketch_seed", 7), max_rank=k)
+    cpu_occ = (time.perf_counter() - t0) * len(keep_idx) / len(sub2)
+    cores = O.lib().oracle_num_threads()
+    return {
+        "grid_metric": {"s": t_metric, "points": n_kept, "anchors": k, "pairs_per_s": pairs / t_metric,
+                        "form": "FP64 all-pairs potential + FP64 GEMM",
+                        "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                                     "frac": achieved / fp64_peak, "flops_per_pair": flops_pair,
+                                     "peak_source": "cuBLAS DGEMM 8192^3 burst, measured here"},
+                        "cpu_baseline": {"value": cpu_metric, "unit": "s", "cores": 1, "kind": "port",
+                                         "sample": f"oracle NumPy restatement on {len(sub)} points, time x "
+                                                   f"(n/{len(sub)})^2"}},
+        "density_col_norm_sketch_fp64": {"s": t_dens, "anchors": [int(a) for a in piv_d],
+                                         "cpu_baseline": {"value": cpu_dens, "unit": "s", "cores": cores,
+                                                          "kind": "port", "sample": f"oracle on {len(sub2)} "
+                                                          "points, linear in points"}},
+        "occ_axis_sketch_fp64": {"s": t_occ, "axes": "ao,occ", "nocc": nocc, "anchors": [int(a) for a in piv_o],
+                                 "cpu_baseline": {"value": cpu_occ, "unit": "s", "cores": cores, "kind": "port",
+                                                  "sample": f"oracle on {len(sub2)} points, linear in points"}},
+    }
 
 
 def selection_kwargs(cfg, names, factors, precision):
@@ -469,6 +561,10 @@ def run_ours(args, rank, world, local_rank):
     if cfg.get("electrons") and not args.no_adjoint and world == 1:
         adjoint = time_adjoint(ctx, mol, x, wt, results[head]["piv"], cfg)
 
+    widened = None
+    if args.widened and world == 1:
+        widened = time_widened(ctx, mol, x, wt, w, theta, k, n_kept, cfg)
+
     if rank != 0:
         return
     hbm, bf16, peak_kind = peaks()
@@ -551,6 +647,8 @@ def run_ours(args, rank, world, local_rank):
         "clocks": res["clocks"], "kernels": kernels, "forms": forms_out, **extra,
         "adjoint": adjoint,
     }
+    if widened is not None:
+        line["widened"] = widened
     print(json.dumps(line), flush=True)
 
 
