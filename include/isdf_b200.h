@@ -297,6 +297,43 @@ int isdf_grid_metric_host(isdf_ctx* ctx, const double* left_host, int64_t kl, co
                           int64_t kr, const double* xyz_host, const double* w_host, int64_t n,
                           int32_t symmetrize, double* metric_host);
 
+/* ---- RBRP (robust blockwise random pivoting) ---------------------------------
+ * Replaces rbrp_ao_cpu / rbrp_ao_device (cpp/src/anchor_select_rbrp.cpp:195-320,
+ * cpp/src/anchor_select_rbrp_device.cpp, cpp/src/anchor_select_pybind.cpp:68-140):
+ * AO-only pivoting over the weighted AO pair rows of the grid points, with the
+ * optional interpolative decomposition (interp_vecs rank x n, transform
+ * rank x nao*nao).  The AO rows live on the GPU; sampling uses the reference's
+ * std::discrete_distribution over std::mt19937_64(seed). */
+typedef struct isdf_rbrp_args {
+    int64_t batch_size;      /* default 128 (validated; results do not depend on it) */
+    int64_t block_size;      /* default 16 */
+    double tolerance;        /* default 1e-10 */
+    int64_t max_rank;        /* 0 = min(n, pairs) */
+    uint64_t seed;           /* default 7 */
+    double tau_block;        /* NaN (default) = 1 / block_size */
+    double rank_rtol;        /* default 1e-12 */
+    int64_t refresh_every;   /* default 8 */
+    double svd_rtol;         /* default 1e-12 */
+    int32_t compute_id;      /* default 0 */
+} isdf_rbrp_args;
+void isdf_rbrp_args_default(isdf_rbrp_args* args);
+typedef struct isdf_rbrp_result isdf_rbrp_result;
+/* ao_host: n x nao row-major AO values, w_host: n nonzero weights (ctx may be NULL). */
+int isdf_rbrp_ao(isdf_ctx* ctx, const double* ao_host, const double* w_host, int64_t n, int64_t nao,
+                 const isdf_rbrp_args* args, isdf_rbrp_result** out);
+/* xyz_host: n x 3 points (AOs evaluated on the device), w_host: n nonzero weights. */
+int isdf_rbrp_points(isdf_ctx* ctx, const double* xyz_host, const double* w_host, int64_t n,
+                     const isdf_rbrp_args* args, isdf_rbrp_result** out);
+/* status: NUL-terminated, at most status_capacity bytes. */
+int isdf_rbrp_result_info(const isdf_rbrp_result* r, int64_t* rank, int64_t* nblocks, int64_t* n, int64_t* nao,
+                          double* relative_residual, double* condition, int64_t* retained_rank, char* status,
+                          int64_t status_capacity);
+/* indices: rank; history: nblocks x 4; interp_vecs: rank x n; transform: rank x nao*nao
+ * (the last two only with compute_id; any pointer may be NULL). */
+int isdf_rbrp_result_copy(const isdf_rbrp_result* r, int64_t* indices, double* history, double* interp_vecs,
+                          double* transform);
+void isdf_rbrp_result_free(isdf_rbrp_result* r);
+
 /* Gaussian sketch factors of rand_sketch: U, V (d x ell, row-major u[a*ell+s])
  * from std::mt19937_64(seed) and std::mt19937_64(seed ^ 0x9e3779b97f4a7c15)
  * through std::normal_distribution<double>

@@ -29,6 +29,8 @@ SYMBOLS = [
     "isdf_energy_gradient", "isdf_ctx_set_coords", "isdf_pair_error_terms_noalloc",
     "isdf_select_fit", "isdf_select_fit_host", "isdf_launch_count", "isdf_sketch_factors",
     "isdf_grid_metric", "isdf_grid_metric_host", "isdf_evaluate_axis_mo", "isdf_evaluate_axis_mo_host",
+    "isdf_rbrp_args_default", "isdf_rbrp_ao", "isdf_rbrp_points", "isdf_rbrp_result_info",
+    "isdf_rbrp_result_copy", "isdf_rbrp_result_free",
     "isdf_sketch_shard_project", "isdf_sketch_shard_combine", "isdf_sketch_shard_free",
     "isdf_sketch_select_gathered", "isdf_fit_at",
 ]
@@ -44,6 +46,12 @@ class SelectArgs(ctypes.Structure):
                 ("sketch_size", I64), ("oversampling", I64), ("seed", ctypes.c_uint64),
                 ("precision", I32), ("debug", I32), ("point_importance", P),
                 ("ao_screening_threshold", F64), ("mo_coeff", P), ("nocc", I64)]
+
+
+class RbrpArgs(ctypes.Structure):
+    _fields_ = [("batch_size", I64), ("block_size", I64), ("tolerance", F64), ("max_rank", I64),
+                ("seed", ctypes.c_uint64), ("tau_block", F64), ("rank_rtol", F64),
+                ("refresh_every", I64), ("svd_rtol", F64), ("compute_id", I32)]
 
 
 class SelectInfo(ctypes.Structure):
@@ -84,6 +92,14 @@ def lib():
         L.isdf_evaluate_axis.argtypes = [P, P, I64, P, I32, P, P]
         L.isdf_evaluate_axis_host.argtypes = [P, P, I64, P, I32, P]
         L.isdf_evaluate_axis_mo.argtypes = [P, P, I64, P, I32, P, I64, P, P]
+        L.isdf_rbrp_args_default.argtypes = [ctypes.POINTER(RbrpArgs)]
+        L.isdf_rbrp_args_default.restype = None
+        L.isdf_rbrp_ao.argtypes = [P, P, P, I64, I64, ctypes.POINTER(RbrpArgs), ctypes.POINTER(P)]
+        L.isdf_rbrp_points.argtypes = [P, P, P, I64, ctypes.POINTER(RbrpArgs), ctypes.POINTER(P)]
+        L.isdf_rbrp_result_info.argtypes = [P, P, P, P, P, P, P, P, ctypes.c_char_p, I64]
+        L.isdf_rbrp_result_copy.argtypes = [P, P, P, P, P]
+        L.isdf_rbrp_result_free.argtypes = [P]
+        L.isdf_rbrp_result_free.restype = None
         L.isdf_evaluate_axis_mo_host.argtypes = [P, P, I64, P, I32, P, I64, P]
         L.isdf_select_args_default.argtypes = [ctypes.POINTER(SelectArgs)]
         L.isdf_select.argtypes = [P, ctypes.POINTER(SelectArgs), P, P, I64, P, I64,
@@ -462,6 +478,50 @@ def make_select_args(algorithm="rand_sketch", axes=("ao",), axis_weights=None, t
         args.mo_coeff = _ptr(mo)
         args.nocc = int(nocc)
     return args, (ax, aw, imp, mo)
+
+
+def _rbrp_collect(h):
+    """Result dict of an isdf_rbrp_result handle (freed here), in the
+    reference's layout (cpp/src/anchor_select_pybind.cpp:68-91)."""
+    try:
+        rank, nb, n, nao, ret = I64(), I64(), I64(), I64(), I64()
+        rel, cond = F64(), F64()
+        status = ctypes.create_string_buffer(64)
+        check(lib().isdf_rbrp_result_info(h, ctypes.byref(rank), ctypes.byref(nb), ctypes.byref(n),
+                                          ctypes.byref(nao), ctypes.byref(rel), ctypes.byref(cond),
+                                          ctypes.byref(ret), status, 64))
+        idx = np.empty(rank.value, dtype=np.int64)
+        hist = np.empty((nb.value, 4))
+        interp = np.empty((rank.value, n.value))
+        transform = np.empty((rank.value, nao.value * nao.value))
+        check(lib().isdf_rbrp_result_copy(h, _ptr(idx), _ptr(hist), _ptr(interp), _ptr(transform)))
+        return {"indices": idx, "relative_residual": rel.value, "status": status.value.decode(),
+                "condition": cond.value, "retained_rank": ret.value, "history": hist,
+                "interp_vecs": interp, "transform": transform}
+    finally:
+        lib().isdf_rbrp_result_free(h)
+
+
+def rbrp_args(batch_size=128, block_size=16, tolerance=1e-10, max_rank=0, seed=7, tau_block=None,
+              rank_rtol=1e-12, refresh_every=8, svd_rtol=1e-12, compute_id=False):
+    a = RbrpArgs()
+    lib().isdf_rbrp_args_default(ctypes.byref(a))
+    a.batch_size, a.block_size, a.tolerance, a.max_rank, a.seed = batch_size, block_size, tolerance, max_rank, seed
+    a.tau_block = float("nan") if tau_block is None else tau_block
+    a.rank_rtol, a.refresh_every, a.svd_rtol, a.compute_id = rank_rtol, refresh_every, svd_rtol, int(compute_id)
+    return a
+
+
+def rbrp_ao(ao, weights, ctx=None, **kw):
+    """RBRP over host AO rows (n x nao) and weights; returns the result dict
+    (interp_vecs / transform are meaningful with compute_id=True)."""
+    ao = _np(ao, np.float64)
+    w = _np(weights, np.float64)
+    a = rbrp_args(**kw)
+    h = P()
+    check(lib().isdf_rbrp_ao(ctx.h if ctx is not None else None, _ptr(ao), _ptr(w), ao.shape[0], ao.shape[1],
+                             ctypes.byref(a), ctypes.byref(h)))
+    return _rbrp_collect(h)
 
 
 def grid_metric_host(left, xyz, w, right=None, ctx=None):

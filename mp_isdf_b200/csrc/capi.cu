@@ -4,8 +4,10 @@
 #include "isdf_fit.h"
 #include "isdf_metric.h"
 #include "isdf_project.h"
+#include "isdf_rbrp.h"
 #include "isdf_select.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -624,6 +626,126 @@ int isdf_grid_metric_host(isdf_ctx* ctx, const double* left, int64_t kl, const d
                           dw.get(), n, symmetrize != 0, metric_host, s);
     });
 }
+
+struct isdf_rbrp_result {
+    isdf::RbrpResult r;
+    int64_t n = 0, nao = 0;
+};
+
+void isdf_rbrp_args_default(isdf_rbrp_args* a) {
+    if (!a) return;
+    isdf::RbrpParams d;
+    a->batch_size = d.batch_size;
+    a->block_size = d.block_size;
+    a->tolerance = d.tolerance;
+    a->max_rank = d.max_rank;
+    a->seed = d.seed;
+    a->tau_block = d.tau_block;
+    a->rank_rtol = d.rank_rtol;
+    a->refresh_every = d.refresh_every;
+    a->svd_rtol = d.svd_rtol;
+    a->compute_id = 0;
+}
+
+namespace {
+
+isdf::RbrpParams rbrp_params(const isdf_rbrp_args* a) {
+    if (!a) isdf::fail(isdf::kInvalid, "RBRP arguments are required");
+    if (a->batch_size < 0 || a->block_size < 0 || a->max_rank < 0 || a->refresh_every < 0)
+        isdf::fail(isdf::kInvalid, "invalid RBRP dimensions, batch size or tolerances");
+    isdf::RbrpParams p;
+    p.batch_size = a->batch_size;
+    p.block_size = a->block_size;
+    p.tolerance = a->tolerance;
+    p.max_rank = a->max_rank;
+    p.seed = a->seed;
+    p.tau_block = a->tau_block;
+    p.rank_rtol = a->rank_rtol;
+    p.refresh_every = a->refresh_every;
+    p.svd_rtol = a->svd_rtol;
+    p.compute_id = a->compute_id != 0;
+    return p;
+}
+
+}  // namespace
+
+int isdf_rbrp_ao(isdf_ctx* ctx, const double* ao, const double* w, int64_t n, int64_t nao,
+                 const isdf_rbrp_args* args, isdf_rbrp_result** out) {
+    return guarded([&] {
+        if (!out) isdf::fail(isdf::kInvalid, "null result handle");
+        *out = nullptr;
+        int dev = 0;
+        if (ctx) dev = ctx_of(ctx).device;
+        else ISDF_CUDA(cudaGetDevice(&dev));
+        DeviceGuard dg(dev);
+        const isdf::RbrpParams p = rbrp_params(args);
+        if (n < 0 || nao < 0 || nao > INT32_MAX || (n > 0 && nao > 0 && (!ao || !w)))
+            isdf::fail(isdf::kInvalid, "expected ao[grid,nao] and weights[grid]");
+        cudaStream_t s = ctx ? ctx->stream : nullptr;
+        isdf::DeviceBuffer<double> dao, dw;
+        upload(dao, ao, static_cast<size_t>(n * nao), s);
+        upload(dw, w, static_cast<size_t>(n), s);
+        auto h = std::make_unique<isdf_rbrp_result>();
+        h->r = isdf::rbrp_ao(dao.get(), dw.get(), n, static_cast<int>(nao), p, s);
+        h->n = n;
+        h->nao = nao;
+        *out = h.release();
+    });
+}
+
+int isdf_rbrp_points(isdf_ctx* ctx, const double* xyz, const double* w, int64_t n, const isdf_rbrp_args* args,
+                     isdf_rbrp_result** out) {
+    return guarded([&] {
+        if (!out) isdf::fail(isdf::kInvalid, "null result handle");
+        *out = nullptr;
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        const isdf::RbrpParams p = rbrp_params(args);
+        if (n < 0 || (n > 0 && (!xyz || !w))) isdf::fail(isdf::kInvalid, "expected weights[ngrid]");
+        cudaStream_t s = ctx->stream;
+        isdf::DeviceBuffer<double> dx, dw, dao(static_cast<size_t>(std::max<int64_t>(n, 1)) * c.nao, s);
+        upload(dx, xyz, static_cast<size_t>(3 * n), s);
+        upload(dw, w, static_cast<size_t>(n), s);
+        isdf::eval_ao<double>(c, dx.get(), n, dao.get(), nullptr, c.nao, s);
+        auto h = std::make_unique<isdf_rbrp_result>();
+        h->r = isdf::rbrp_ao(dao.get(), dw.get(), n, c.nao, p, s);
+        h->n = n;
+        h->nao = c.nao;
+        *out = h.release();
+    });
+}
+
+int isdf_rbrp_result_info(const isdf_rbrp_result* r, int64_t* rank, int64_t* nblocks, int64_t* n, int64_t* nao,
+                          double* relres, double* condition, int64_t* retained, char* status, int64_t cap) {
+    return guarded([&] {
+        if (!r) isdf::fail(isdf::kInvalid, "null result handle");
+        if (rank) *rank = static_cast<int64_t>(r->r.indices.size());
+        if (nblocks) *nblocks = static_cast<int64_t>(r->r.history.size() / 4);
+        if (n) *n = r->n;
+        if (nao) *nao = r->nao;
+        if (relres) *relres = r->r.relative_residual;
+        if (condition) *condition = r->r.condition;
+        if (retained) *retained = r->r.retained_rank;
+        if (status && cap > 0) {
+            const size_t m = std::min<size_t>(r->r.status.size(), static_cast<size_t>(cap - 1));
+            std::memcpy(status, r->r.status.data(), m);
+            status[m] = '\0';
+        }
+    });
+}
+
+int isdf_rbrp_result_copy(const isdf_rbrp_result* r, int64_t* indices, double* history, double* interp,
+                          double* transform) {
+    return guarded([&] {
+        if (!r) isdf::fail(isdf::kInvalid, "null result handle");
+        if (indices) std::copy(r->r.indices.begin(), r->r.indices.end(), indices);
+        if (history) std::copy(r->r.history.begin(), r->r.history.end(), history);
+        if (interp) std::copy(r->r.interp_vecs.begin(), r->r.interp_vecs.end(), interp);
+        if (transform) std::copy(r->r.transform.begin(), r->r.transform.end(), transform);
+    });
+}
+
+void isdf_rbrp_result_free(isdf_rbrp_result* r) { delete r; }
 
 int isdf_sketch_factors(int64_t d, int64_t ell, uint64_t seed, double* u_host, double* v_host) {
     return guarded([&] {

@@ -13,6 +13,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -314,6 +315,96 @@ PYBIND11_MODULE(mp_isdf, m) {
                                         const FloatArray& weights) {
         return metric(left, right, coords, weights);
     }, py::arg("left"), py::arg("right"), py::arg("coords"), py::arg("weights"));
+    // RBRP (cpp/src/anchor_select_pybind.cpp:68-140): result dict in the reference's layout
+    auto rbrp_dict = [](isdf_rbrp_result* h, bool compute_id) {
+        struct Free { isdf_rbrp_result* h; ~Free() { isdf_rbrp_result_free(h); } } guard{h};
+        int64_t rank = 0, nb = 0, n = 0, nao = 0, ret = 0;
+        double rel = 0, cond = 0;
+        char status[64];
+        check(isdf_rbrp_result_info(h, &rank, &nb, &n, &nao, &rel, &cond, &ret, status, sizeof(status)));
+        py::array_t<int64_t> idx(rank);
+        py::array_t<double> hist({static_cast<py::ssize_t>(nb), py::ssize_t(4)});
+        py::array_t<double> theta({static_cast<py::ssize_t>(rank), static_cast<py::ssize_t>(compute_id ? n : 0)});
+        py::array_t<double> transform({static_cast<py::ssize_t>(rank), static_cast<py::ssize_t>(compute_id ? nao * nao : 0)});
+        check(isdf_rbrp_result_copy(h, idx.mutable_data(), hist.mutable_data(),
+                                    compute_id ? theta.mutable_data() : nullptr,
+                                    compute_id ? transform.mutable_data() : nullptr));
+        py::dict out;
+        py::list indices;
+        for (int64_t i = 0; i < rank; ++i) indices.append(idx.data()[i]);
+        out["indices"] = indices;
+        out["relative_residual"] = rel;
+        out["status"] = std::string(status);
+        out["condition"] = cond;
+        out["retained_rank"] = ret;
+        out["history"] = hist;
+        if (compute_id) {
+            out["interp_vecs"] = theta;
+            out["transform"] = transform;
+        }
+        return out;
+    };
+    auto rbrp_args_of = [](std::size_t batch_size, std::size_t block_size, double tolerance, std::size_t max_rank,
+                           std::uint64_t seed, py::object tau_block, double rank_rtol, std::size_t refresh_every,
+                           double svd_rtol, bool compute_id) {
+        isdf_rbrp_args a;
+        isdf_rbrp_args_default(&a);
+        a.batch_size = static_cast<int64_t>(batch_size);
+        a.block_size = static_cast<int64_t>(block_size);
+        a.tolerance = tolerance;
+        a.max_rank = static_cast<int64_t>(max_rank);
+        a.seed = seed;
+        a.tau_block = tau_block.is_none() ? std::numeric_limits<double>::quiet_NaN() : tau_block.cast<double>();
+        a.rank_rtol = rank_rtol;
+        a.refresh_every = static_cast<int64_t>(refresh_every);
+        a.svd_rtol = svd_rtol;
+        a.compute_id = compute_id ? 1 : 0;
+        return a;
+    };
+    m.def("rbrp_ao_cpu", [rbrp_dict, rbrp_args_of](const FloatArray& ao, const FloatArray& weights, std::size_t batch_size,
+                                                  std::size_t block_size, double tolerance, std::size_t max_rank,
+                                                  std::uint64_t seed, py::object tau_block, double rank_rtol,
+                                                  std::size_t refresh_every, double svd_rtol, bool compute_id) {
+        if (ao.ndim() != 2 || weights.ndim() != 1 || weights.shape(0) != ao.shape(0))
+            throw std::invalid_argument("expected ao[grid,nao] and weights[grid]");
+        isdf_rbrp_args a = rbrp_args_of(batch_size, block_size, tolerance, max_rank, seed, tau_block, rank_rtol,
+                                        refresh_every, svd_rtol, compute_id);
+        isdf_rbrp_result* h = nullptr;
+        int rc;
+        {
+            py::gil_scoped_release release;
+            rc = isdf_rbrp_ao(nullptr, ao.data(), weights.data(), ao.shape(0), ao.shape(1), &a, &h);
+        }
+        check(rc);
+        return rbrp_dict(h, compute_id);
+    }, py::arg("ao"), py::arg("weights"), py::arg("batch_size") = 128, py::arg("block_size") = 16,
+       py::arg("tolerance") = 1e-10, py::arg("max_rank") = 0, py::arg("seed") = 7, py::arg("tau_block") = py::none(),
+       py::arg("rank_rtol") = 1e-12, py::arg("refresh_every") = 8, py::arg("svd_rtol") = 1e-12,
+       py::arg("compute_id") = false,
+       "AO-only RBRP on nonzero grid rows (computed on the GPU); optional ID.");
+    m.def("rbrp_ao_device", [rbrp_dict, rbrp_args_of](const Selector& selector, const FloatArray& points,
+                                                     const FloatArray& weights, std::size_t batch_size,
+                                                     std::size_t block_size, double tolerance, std::size_t max_rank,
+                                                     std::uint64_t seed, py::object tau_block, double rank_rtol,
+                                                     std::size_t refresh_every, double svd_rtol, bool compute_id) {
+        auto pts = points_of(points, "expected points[ngrid,3]");
+        if (weights.ndim() != 1 || weights.shape(0) != pts.shape(0))
+            throw std::invalid_argument("expected weights[ngrid]");
+        isdf_rbrp_args a = rbrp_args_of(batch_size, block_size, tolerance, max_rank, seed, tau_block, rank_rtol,
+                                        refresh_every, svd_rtol, compute_id);
+        isdf_rbrp_result* h = nullptr;
+        int rc;
+        {
+            py::gil_scoped_release release;
+            rc = isdf_rbrp_points(selector.ctx->h, pts.data(), weights.data(), pts.shape(0), &a, &h);
+        }
+        check(rc);
+        return rbrp_dict(h, compute_id);
+    }, py::arg("selector"), py::arg("points"), py::arg("weights"), py::arg("batch_size") = 128,
+       py::arg("block_size") = 16, py::arg("tolerance") = 1e-10, py::arg("max_rank") = 0, py::arg("seed") = 7,
+       py::arg("tau_block") = py::none(), py::arg("rank_rtol") = 1e-12, py::arg("refresh_every") = 8,
+       py::arg("svd_rtol") = 1e-12, py::arg("compute_id") = false,
+       "AO-only RBRP with the AOs evaluated on the device; optional ID.");
     m.def("eval_ao", [](const IntArray& atm, const IntArray& bas, const FloatArray& env,
                         const FloatArray& coords, const std::string& space) {
         Context c(atm, bas, env);

@@ -374,4 +374,15 @@ void oracle_fit_apply(long long n, long long k, const double* G, const double* q
     *exact2 = x_acc;
 }
 
+// Weighted draws of RBRP (cpp/src/anchor_select_rbrp.cpp:249-258): one
+// std::mt19937_64(seed) for the whole run and a fresh
+// std::discrete_distribution over the remaining candidates' weights per draw.
+void* oracle_rng_new(uint64_t seed) { return new std::mt19937_64(seed); }
+void oracle_rng_free(void* rng) { delete static_cast<std::mt19937_64*>(rng); }
+long long oracle_rng_discrete(void* rng, const double* w, long long n)
+{
+    std::discrete_distribution<std::size_t> dist(w, w + n);
+    return static_cast<long long>(dist(*static_cast<std::mt19937_64*>(rng)));
+}
+
 } // extern "C"

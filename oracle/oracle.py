@@ -85,6 +85,11 @@ def lib():
                                     ctypes.c_longlong, P]
         L.oracle_grid_gram.argtypes = [P, P, ctypes.c_longlong, P, ctypes.c_longlong, P, P]
         L.oracle_fit_apply.argtypes = [ctypes.c_longlong, ctypes.c_longlong] + [P] * 9
+        L.oracle_rng_new.restype = P
+        L.oracle_rng_new.argtypes = [ctypes.c_uint64]
+        L.oracle_rng_free.argtypes = [P]
+        L.oracle_rng_discrete.restype = ctypes.c_longlong
+        L.oracle_rng_discrete.argtypes = [P, P, ctypes.c_longlong]
         L.oracle_last_error.restype = ctypes.c_char_p
         L.oracle_num_threads.restype = ctypes.c_int
         _lib = L
@@ -457,6 +462,165 @@ def select_density_sketch(ctx, pts, w, importance, normalized=False, tolerance=1
     if return_details:
         return piv, dict(y=y, keep=keep, q=q, **det)
     return piv
+
+
+# ---------------------------------------------------------------------------
+# RBRP (cpp/src/anchor_select_rbrp.cpp:195-320), explicit pair rows
+# ---------------------------------------------------------------------------
+def rbrp_pair_rows(ao, w):
+    """row_g[(mu, nu)] = sqrt|w_g| phi_mu phi_nu (x sqrt 2 off the diagonal), mu <= nu."""
+    n, nao = ao.shape
+    iu, ju = np.triu_indices(nao)
+    c = np.where(iu == ju, 1.0, np.sqrt(2.0))
+    return np.sqrt(np.abs(w))[:, None] * ao[:, iu] * ao[:, ju] * c[None, :]
+
+
+def rbrp_ao(ao, w, batch_size=128, block_size=16, tolerance=1e-10, max_rank=0, seed=7, tau_block=None,
+            rank_rtol=1e-12, refresh_every=8, svd_rtol=1e-12, compute_id=False):
+    """Robust blockwise random pivoting over the AO pair rows and its ID
+    (``cpp/src/anchor_select_rbrp.cpp:136-320``), with LAPACK dgeqp3 / dorgqr
+    (scipy) for the block QR and gesdd (numpy) for the small SVD."""
+    from scipy.linalg.lapack import dgeqp3, dorgqr
+    ao = np.asarray(ao, float)
+    w = np.asarray(w, float)
+    n, nao = ao.shape
+    if (not n or not nao or batch_size <= 0 or block_size <= 0 or not np.isfinite(tolerance) or tolerance < 0
+            or not np.isfinite(rank_rtol) or rank_rtol <= 0 or not np.isfinite(svd_rtol) or svd_rtol < 0
+            or (tau_block is not None and (not np.isfinite(tau_block) or not 0 <= tau_block < 1))):
+        raise ValueError("invalid RBRP dimensions, batch size or tolerances")
+    p = nao * (nao + 1) // 2
+    cap = min(p, n, max_rank if max_rank else min(n, p))
+    tau_block = (1.0 / block_size if block_size > 1 else 0.0) if tau_block is None else tau_block
+    if not np.all(np.isfinite(w)) or np.any(w == 0):
+        raise ValueError("RBRP requires finite nonzero weights")
+    if not np.all(np.isfinite(ao)):
+        raise ValueError("RBRP requires finite real AOs")
+    rows = rbrp_pair_rows(ao, w)
+    d = np.abs(w) * np.einsum("gi,gi->g", ao, ao) ** 2
+    total = float(np.sum(d))
+    target = tolerance * tolerance * total
+    q = np.zeros((0, p))
+    L = np.zeros((n, 0))
+    chosen = np.zeros(n, bool)
+    rng = lib().oracle_rng_new(np.uint64(seed))
+    indices, history, status, it = [], [], "rank_cap", 0
+
+    def residual():
+        e = rows - L @ q
+        r = np.einsum("gi,gi->g", e, e)
+        r[chosen] = 0.0
+        return r
+
+    try:
+        while True:
+            old = len(indices)
+            if old and (sum(d) <= target or (refresh_every and it % refresh_every == 0)):
+                d = residual()
+            if sum(d) <= target:
+                status = "tolerance"
+                break
+            if old >= cap:
+                break
+            active = [i for i in range(n) if d[i] > 0 and not chosen[i]]
+            if not active:
+                status = "no_candidates"
+                break
+            b = min(block_size, cap - old, len(active))
+            sample = []
+            for _ in range(b):
+                left = np.ascontiguousarray([d[i] for i in active])
+                pos = lib().oracle_rng_discrete(rng, _p(left), len(left))
+                sample.append(active.pop(pos))
+            v = rows[sample].T.copy()                          # p x b
+            original2 = float(np.sum(v * v))
+            for _ in range(2):
+                for j in range(b):
+                    for t in range(old):
+                        v[:, j] -= (v[:, j] @ q[t]) * q[t]
+            qr_, jpvt, tau_, _, info = dgeqp3(np.asfortranarray(v))
+            if info != 0:
+                raise RuntimeError("RBRP block geqp3 failed")
+            tails = np.zeros(b)
+            for row in range(b - 1, -1, -1):
+                tails[row] = (tails[row + 1] if row + 1 < b else 0.0) + np.sum(qr_[row, row:b] ** 2)
+            if not (tails[0] > 0) or not np.isfinite(tails[0]):
+                status = "numerical_rank"
+                break
+            keep = 0
+            for i in range(b):
+                if tails[i] >= tau_block * tails[0]:
+                    keep = i + 1
+            cutoff = rank_rtol * np.sqrt(original2)
+            for i in range(keep):
+                if abs(qr_[i, i]) <= cutoff:
+                    keep = i
+                    break
+            if not keep:
+                status = "numerical_rank"
+                break
+            qb, _, info = dorgqr(qr_[:, :keep], tau_[:keep])
+            if info != 0:
+                raise RuntimeError("RBRP block orgqr failed")
+            qb = np.array(qb)
+            for j in range(keep):
+                col = qb[:, j]
+                for _ in range(2):
+                    for t in range(old):
+                        col -= (q[t] @ col) * q[t]
+                    for t in range(j):
+                        col -= (qb[:, t] @ col) * qb[:, t]
+                nrm = np.linalg.norm(col)
+                if not (nrm > 0) or not np.isfinite(nrm):
+                    raise RuntimeError("RBRP block lost orthogonality")
+                qb[:, j] = col / nrm
+            prev = chosen.copy()
+            lnew = rows @ qb
+            lnew[prev] = 0.0
+            d = np.where(prev, 0.0, np.maximum(0.0, d - np.sum(lnew ** 2, axis=1)))
+            L = np.hstack([L, lnew])
+            q = np.vstack([q, qb.T])
+            for j in range(keep):
+                idx = sample[jpvt[j] - 1]
+                indices.append(idx)
+                chosen[idx] = True
+                d[idx] = 0.0
+            history.append([len(indices), b, keep, np.sqrt(sum(d) / total) if total else 0.0])
+            it += 1
+    finally:
+        lib().oracle_rng_free(rng)
+    d = residual()
+    rel = np.sqrt(sum(d) / total) if total else 0.0
+    if rel <= tolerance:
+        status = "tolerance"
+    elif status == "tolerance":
+        status = "roundoff_limited"
+    out = {"indices": indices, "relative_residual": rel, "status": status, "history": np.array(history),
+           "condition": 0.0, "retained_rank": 0}
+    if not compute_id or not indices:
+        return out
+    k = len(indices)
+    A = L[indices, :k]
+    u, s, vt = np.linalg.svd(A)
+    out["condition"] = s[0] / s[-1] if s[-1] else np.inf
+    retained = int(np.sum(s > svd_rtol * s[0]))
+    if not retained:
+        raise RuntimeError("RBRP anchor block has zero numerical rank")
+    out["retained_rank"] = retained
+    inv = vt[:retained].T @ np.diag(1.0 / s[:retained]) @ u[:, :retained].T
+    idx = np.array(indices)
+    sw = np.sqrt(np.abs(w))
+    fac = sw[idx] / w[idx]
+    theta = (L[:, :k] @ inv).T * fac[:, None] / sw[None, :]
+    theta[:, idx] = np.diag(1.0 / w[idx])
+    iu, ju = np.triu_indices(nao)
+    packed = (inv.T @ q[:k]) * fac[:, None]
+    packed = packed / np.where(iu == ju, 1.0, np.sqrt(2.0))[None, :]
+    transform = np.zeros((k, nao, nao))
+    transform[:, iu, ju] = packed
+    transform[:, ju, iu] = packed
+    out["interp_vecs"] = theta
+    out["transform"] = transform.reshape(k, nao * nao)
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -159,6 +159,26 @@ def _normalized_pair_error(context, coords, anchor_ao, anchor_weights, theta, im
             "included_mass": float(total), "screened_mass": float(screened)}
 
 
+def _pair_error(context, coords, weights, anchor_ao, anchor_weights, theta, space, batch=65536):
+    """Pair-space error of a given Theta (``python/isdf.py:154-191``):
+    sum_g |w_g| |p_g - sum_k Theta_kg w_k p_k|^2 in the Gram form
+    q^2 - 2 c.h + c^T M c (c = Theta_g w_a, h = (Phi_a phi_g)^2, M = (Phi_a Phi_a^T)^2),
+    relative to sum_g |w_g| q_g^2."""
+    M = (anchor_ao @ anchor_ao.T) ** 2
+    err2 = exact2 = 0.0
+    for g0 in range(0, len(coords), batch):
+        ao = context.eval_ao(coords[g0:g0 + batch], space=space)
+        aw = np.abs(weights[g0:g0 + batch])
+        q = np.einsum("ga,ga->g", ao, ao)
+        c = (np.asarray(theta)[:, g0:g0 + batch] * anchor_weights[:, None]).T
+        h = (ao @ anchor_ao.T) ** 2
+        r2 = q * q - 2 * np.einsum("gk,gk->g", c, h) + np.einsum("gk,kl,gl->g", c, M, c)
+        err2 += float(np.sum(aw * r2))
+        exact2 += float(np.sum(aw * q * q))
+    err2 = max(err2, 0.0)
+    return {"l2": float(np.sqrt(err2)), "relative": float(np.sqrt(err2 / exact2)) if exact2 else 0.0}
+
+
 def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), axis_weights=None,
                space="auto", anchor_algorithm="qrcp_dense", sketch="quadrature",
                anchor_batch_size=128, fit_batch_size=2048, anchor_sketch_size=128,
@@ -166,7 +186,8 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
                pair_space_error=False, report_timings=False, report_dimensions=False, grid=None,
                precision="fp64", point_importance=None, density_weight="electron_density",
                ao_screening_threshold=1e-24, compute_metric=False, metric_algorithm="grid",
-               mo_coeff=None, nocc=0):
+               mo_coeff=None, nocc=0, rbrp_block_size=16, rbrp_tau_block=None, rbrp_rank_rtol=1e-12,
+               rbrp_refresh_every=8, rbrp_svd_rtol=1e-12):
     """Selection-to-fit slice of ``build_isdf`` (``python/isdf.py:287-672``).
 
     `grid` is an optional (coords, weights) pair; otherwise a Becke-partitioned
@@ -233,10 +254,22 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
         raise ValueError("selection_only requires compute_metric=False")
     if compute_metric and metric_algorithm != "grid":
         raise NotImplementedError("the integral-direct Cholesky metrics are outside the B200 hot path (NYI)")
-    if anchor_algorithm not in ("qrcp_dense", "qrcp_online", *SKETCH_ALGORITHMS):
-        if anchor_algorithm in ("cvt", "rbrp", "rbrp_id"):
-            raise NotImplementedError(f"{anchor_algorithm} is outside the B200 hot path (NYI)")
+    rbrp_mode = anchor_algorithm in ("rbrp", "rbrp_id")
+    if anchor_algorithm not in ("qrcp_dense", "qrcp_online", "rbrp", "rbrp_id", *SKETCH_ALGORITHMS):
+        if anchor_algorithm == "cvt":
+            raise NotImplementedError("cvt is outside the B200 hot path (NYI)")
         raise ValueError(f"unknown anchor algorithm: {anchor_algorithm!r}")
+    if rbrp_mode:
+        # python/isdf.py:427-436
+        if axis_types != [mp_isdf.AxisType.AtomicOrbital]:
+            raise ValueError("RBRP currently requires axes=('ao',)")
+        if (not isinstance(rbrp_block_size, (int, np.integer)) or rbrp_block_size < 1 or
+                not isinstance(rbrp_refresh_every, (int, np.integer)) or rbrp_refresh_every < 0 or
+                not np.isfinite(rbrp_rank_rtol) or rbrp_rank_rtol <= 0 or
+                not np.isfinite(rbrp_svd_rtol) or rbrp_svd_rtol < 0 or
+                (rbrp_tau_block is not None and
+                 (not np.isfinite(rbrp_tau_block) or not 0 <= rbrp_tau_block < 1))):
+            raise ValueError("invalid RBRP block size, refresh interval or tolerances")
     if not isinstance(anchor_batch_size, (int, np.integer)) or anchor_batch_size <= 0:
         raise ValueError("anchor_batch_size must be a positive integer")
     if not isinstance(fit_batch_size, (int, np.integer)) or fit_batch_size <= 0:
@@ -300,19 +333,34 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
                                       "which is not available here; pass point_importance")
         importance = _validate_point_importance(point_importance, len(all_coords))
         record("point_importance")
+    rbrp_result = None
+    if rbrp_mode:
+        # python/isdf.py:564-589: RBRP on the nonzero-weight points, AOs on the device
+        settings = dict(batch_size=anchor_batch_size, block_size=rbrp_block_size,
+                        tolerance=anchor_tol, max_rank=anchor_rank, seed=anchor_seed,
+                        tau_block=rbrp_tau_block, rank_rtol=rbrp_rank_rtol,
+                        refresh_every=rbrp_refresh_every, svd_rtol=rbrp_svd_rtol,
+                        compute_id=(anchor_algorithm == "rbrp_id" and not selection_only))
+        rbrp_result = mp_isdf.rbrp_ao_device(selector, all_coords[keep], all_weights[keep], **settings)
+        anchor_indices = np.flatnonzero(keep)[np.asarray(rbrp_result["indices"], dtype=np.intp)]
+        if debug:
+            print(f"[rbrp] rank={len(anchor_indices)} residual={rbrp_result['relative_residual']:.6e} "
+                  f"status={rbrp_result['status']} blocks={len(rbrp_result['history'])}", flush=True)
     algo = {"qrcp_dense": mp_isdf.LocalAnchorSelectionAlgorithm.QRColumnPivoting,
             "qrcp_online": mp_isdf.LocalAnchorSelectionAlgorithm.OnlineQRColumnPivoting,
-            "rand_sketch": mp_isdf.LocalAnchorSelectionAlgorithm.RandomizedQuadratureKhatriRao}[anchor_algorithm]
+            "rand_sketch": mp_isdf.LocalAnchorSelectionAlgorithm.RandomizedQuadratureKhatriRao,
+            "rbrp": None, "rbrp_id": None}[anchor_algorithm]
     if density_sketch:
         algo = getattr(mp_isdf.LocalAnchorSelectionAlgorithm, SKETCH_ENUM[sketch])
-    anchor_indices = np.asarray(selector.select(
-        all_coords, all_weights, axis_types, tolerance=anchor_tol, max_rank=anchor_rank,
-        algorithm=algo, space=space, batch_size=anchor_batch_size, debug=debug,
-        sketch_size=anchor_sketch_size, oversampling=anchor_oversampling, seed=anchor_seed,
-        axis_weights=list(axis_weights) if axis_weights is not None else [],
-        point_importance=importance, ao_screening_threshold=ao_screening_threshold,
-        mo_coeff=np.ascontiguousarray(mo_coeff) if needs_occ else None, nocc=nocc if needs_occ else 0,
-        precision=precision), dtype=np.intp)
+    if not rbrp_mode:
+        anchor_indices = np.asarray(selector.select(
+            all_coords, all_weights, axis_types, tolerance=anchor_tol, max_rank=anchor_rank,
+            algorithm=algo, space=space, batch_size=anchor_batch_size, debug=debug,
+            sketch_size=anchor_sketch_size, oversampling=anchor_oversampling, seed=anchor_seed,
+            axis_weights=list(axis_weights) if axis_weights is not None else [],
+            point_importance=importance, ao_screening_threshold=ao_screening_threshold,
+            mo_coeff=np.ascontiguousarray(mo_coeff) if needs_occ else None, nocc=nocc if needs_occ else 0,
+            precision=precision), dtype=np.intp)
     if len(anchor_indices) == 0:
         raise ValueError("anchor selection found no anchors; adjust settings or grid")
     record("anchor_selection")
@@ -329,15 +377,28 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
     anchor_weights = all_weights[anchor_indices]
     anchor_ao = context.eval_ao(anchor_coords, space=space)
     record("ao_evaluation")
-    fit = mp_isdf.fit(context, all_coords, all_weights, anchor_indices, precision=precision,
-                      pair_space_error=pair_space_error)
-    interp_vecs = fit["interp_vecs"]
-    fit_diagnostics = {key: fit[key] for key in ("retained_rank", "condition",
-                                                 "max_abs_physical_coefficient")}
+    id_info = None
+    if anchor_algorithm == "rbrp_id":
+        # python/isdf.py:640-647: the RBRP interpolative decomposition is the fit
+        interp_vecs = np.asarray(rbrp_result["interp_vecs"])
+        id_info = {key: rbrp_result[key] for key in ("retained_rank", "condition", "relative_residual", "status")}
+        fit_diagnostics = None
+        theta_w = interp_vecs @ weights
+    else:
+        fit = mp_isdf.fit(context, all_coords, all_weights, anchor_indices, precision=precision,
+                          pair_space_error=pair_space_error)
+        interp_vecs = fit["interp_vecs"]
+        fit_diagnostics = {key: fit[key] for key in ("retained_rank", "condition",
+                                                     "max_abs_physical_coefficient")}
+        theta_w = np.asarray(fit["theta_w"][:len(anchor_weights)])
     record("isdf_fit")
     pair_space_errors = None
     if pair_space_error:
-        pair_space_errors = {"scalar": {"l2": fit["pair_l2"], "relative": fit["pair_relative"]}}
+        if anchor_algorithm == "rbrp_id":
+            pair_space_errors = {"scalar": _pair_error(context, coords, weights, anchor_ao, anchor_weights,
+                                                       interp_vecs, space)}
+        else:
+            pair_space_errors = {"scalar": {"l2": fit["pair_l2"], "relative": fit["pair_relative"]}}
         if importance is not None:
             pair_space_errors["density_normalized"] = _normalized_pair_error(
                 context, coords, anchor_ao, anchor_weights, interp_vecs, importance[keep],
@@ -346,7 +407,7 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
     # Overlap reconstruction (python/isdf.py:665-671); without int1e_ovlp the
     # reference overlap is the grid quadrature Phi^T diag(w) Phi (small systems).
     overlap_approx = np.einsum("ku,kv,k->uv", anchor_ao, anchor_ao,
-                               anchor_weights * np.asarray(fit["theta_w"][:len(anchor_weights)]),
+                               anchor_weights * theta_w,
                                optimize=True) if len(anchor_weights) <= 64 else None
     overlap_relative_error = None
     if overlap_approx is not None and nao <= 400 and len(coords) <= 400000:
@@ -361,6 +422,9 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
         metric = anchor_weights[:, None] * raw * anchor_weights[None, :]
         record("coulomb_metric")
     return {"anchor_indices": anchor_indices, "fit_diagnostics": fit_diagnostics, "coulomb_metric": metric,
+            "rbrp_diagnostics": ({key: rbrp_result[key] for key in ("relative_residual", "status", "history")}
+                                 if rbrp_result is not None else None),
+            "id_diagnostics": id_info,
             "anchor_coords": anchor_coords, "anchor_weights": anchor_weights,
             "coordinates": coords, "weights": weights, "interp_vecs": interp_vecs,
             "overlap_reconstruction": overlap_approx,
@@ -381,6 +445,12 @@ def main(argv=None):
     parser.add_argument("--anchor-algorithm", choices=("qrcp_dense", "qrcp_online", *SKETCH_ALGORITHMS,
                                                        "cvt", "rbrp", "rbrp_id"), default="qrcp_dense")
     parser.add_argument("--sketch", choices=KHATRIRAO_SKETCH_TECHNIQUES, default=None)
+    parser.add_argument("--rbrp-block-size", type=int, default=16)
+    parser.add_argument("--rbrp-tau-block", type=float, default=None,
+                        help="local QR trailing-energy threshold (default: 1/block_size)")
+    parser.add_argument("--rbrp-rank-rtol", type=float, default=1e-12)
+    parser.add_argument("--rbrp-refresh-every", type=int, default=8)
+    parser.add_argument("--rbrp-svd-rtol", type=float, default=1e-12)
     parser.add_argument("--anchor-batch-size", type=int, default=128)
     parser.add_argument("--fit-batch-size", type=int, default=2048)
     parser.add_argument("--anchor-sketch-size", type=int, default=128)
@@ -459,7 +529,10 @@ def main(argv=None):
                         density_weight=args.density_weight,
                         ao_screening_threshold=args.ao_screening_threshold,
                         compute_metric=bool(args.metric_algorithm) and not args.no_metric,
-                        metric_algorithm=args.metric_algorithm or "grid")
+                        metric_algorithm=args.metric_algorithm or "grid",
+                        rbrp_block_size=args.rbrp_block_size, rbrp_tau_block=args.rbrp_tau_block,
+                        rbrp_rank_rtol=args.rbrp_rank_rtol, rbrp_refresh_every=args.rbrp_refresh_every,
+                        rbrp_svd_rtol=args.rbrp_svd_rtol)
     print(f"Grid points: {len(result['coordinates'])}; AOs: {result['X1'].shape[1]}; "
           f"anchors: {len(result['anchor_indices'])}")
     if args.anchor_rank and len(result["anchor_indices"]) == args.anchor_rank:
