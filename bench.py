@@ -257,9 +257,11 @@ def time_widened(ctx, mol, x, wt, w, theta, k, n_kept, cfg):
     """The rows widened beyond the selection + fit path, on the bench workload:
     the grid Coulomb metric of the fitted Theta (python/isdf.py:48-68), the FP64
     density_col_norm sketch (importance = |w| times a seeded factor in
-    [0.5, 1.5]) and the FP64 quadrature sketch over the ao + occ axes (a seeded
-    orthogonal nao x nao MO matrix, nocc = electrons / 2)."""
+    [0.5, 1.5]), the FP64 quadrature sketch over the ao + occ axes (a seeded
+    orthogonal nao x nao MO matrix, nocc = electrons / 2) and, for bases of at
+    most 256 AOs, RBRP-ID over the kept points."""
     import torch
+    from mp_isdf_b200 import capi
     keep = torch.as_tensor(w != 0, device=x.device)
     xk, wk = x[keep].contiguous(), wt[keep].contiguous()
     th = theta[:k * n_kept].view(k, n_kept)
@@ -306,7 +308,22 @@ def time_widened(ctx, mol, x, wt, w, theta, k, n_kept, cfg):
     O.select_rand_sketch_features(f, sub2, w[sub2], k + ov, ov, cfg.get("sketch_seed", 7), max_rank=k)
     cpu_occ = (time.perf_counter() - t0) * len(keep_idx) / len(sub2)
     cores = O.lib().oracle_num_threads()
+    rbrp = None
+    if mol.nao <= 256:
+        # RBRP-ID over the kept points (AO pair rows nao (nao + 1) / 2 long)
+        pk, wk_h = pts_h[keep_idx], w[keep_idx]
+        r, t_rbrp = _event_time(lambda: capi.rbrp_points(ctx, pk, wk_h, max_rank=k, block_size=16,
+                                                         compute_id=True), reps=2)
+        aos = oc.eval_ao(pts_h[sub2])
+        t0 = time.perf_counter()
+        O.rbrp_ao(aos, w[sub2], max_rank=k, block_size=16, compute_id=True)
+        cpu_rbrp = (time.perf_counter() - t0) * len(keep_idx) / len(sub2)
+        rbrp = {"s": t_rbrp, "points": int(len(keep_idx)), "rank": len(r["indices"]), "status": r["status"],
+                "relative_residual": r["relative_residual"],
+                "cpu_baseline": {"value": cpu_rbrp, "unit": "s", "cores": cores, "kind": "port",
+                                 "sample": f"oracle (explicit pair rows) on {len(sub2)} points, linear in points"}}
     return {
+        "rbrp_id": rbrp,
         "grid_metric": {"s": t_metric, "points": n_kept, "anchors": k, "pairs_per_s": pairs / t_metric,
                         "form": "FP64 all-pairs potential + FP64 GEMM",
                         "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",

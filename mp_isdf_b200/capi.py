@@ -524,6 +524,16 @@ def rbrp_ao(ao, weights, ctx=None, **kw):
     return _rbrp_collect(h)
 
 
+def rbrp_points(ctx, xyz, weights, **kw):
+    """RBRP with the AOs of the host points evaluated on the device."""
+    xyz = _np(xyz, np.float64).reshape(-1, 3)
+    w = _np(weights, np.float64)
+    a = rbrp_args(**kw)
+    h = P()
+    check(lib().isdf_rbrp_points(ctx.h, _ptr(xyz), _ptr(w), len(w), ctypes.byref(a), ctypes.byref(h)))
+    return _rbrp_collect(h)
+
+
 def grid_metric_host(left, xyz, w, right=None, ctx=None):
     """Grid Coulomb metric between interpolation-vector sets (host arrays;
     left/right: k x n, not weight-scaled).  right=None: the symmetrised metric
