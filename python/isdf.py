@@ -560,7 +560,11 @@ def main(argv=None):
         rec = {"anchor_indices": [int(i) for i in result["anchor_indices"]],
                "timings": result["timings"], "elapsed": result["elapsed"],
                "pair_space_errors": result["pair_space_errors"],
-               "fit_diagnostics": {k: float(v) for k, v in result["fit_diagnostics"].items()},
+               "fit_diagnostics": ({k: float(v) for k, v in result["fit_diagnostics"].items()}
+                                   if result["fit_diagnostics"] is not None else None),
+               "id_diagnostics": ({k: (v if isinstance(v, str) else float(v))
+                                   for k, v in result["id_diagnostics"].items()}
+                                  if result.get("id_diagnostics") else None),
                "precision": args.precision, "axes": args.axes}
         Path(args.json).write_text(json.dumps(rec, indent=1))
     return result
