@@ -208,6 +208,15 @@ __global__ void __launch_bounds__(1024) qr_pivot_kernel(QrState st, int64_t j, i
     }
     __syncthreads();
     if (piv < 0) return;   // every column already pivoted (cannot happen for j < min(m, n))
+    // the pivot column's rows, loaded in parallel (strided by the leading
+    // dimension) when they fit; otherwise read in place
+    __shared__ double colsh[kMaxSketchRows];
+    const bool staged = st.m <= kMaxSketchRows;
+    const double* colg = st.Yt + piv;
+    auto row = [&](int64_t i) { return staged ? colsh[i] : colg[i * st.ldy]; };
+    if (staged)
+        for (int64_t i = threadIdx.x; i < st.m; i += blockDim.x) colsh[i] = colg[i * st.ldy];
+    __syncthreads();
     if (threadIdx.x == 0) {
         const int64_t p = piv;
         st.jpvt[j] = p;
@@ -219,10 +228,9 @@ __global__ void __launch_bounds__(1024) qr_pivot_kernel(QrState st, int64_t j, i
         st.pos[cj] = pp;
         st.col_at[j] = p;
         st.pos[p] = j;
-        const double* col = st.Yt + p;
-        const double alpha = col[j * st.ldy];
+        const double alpha = row(j);
         double xnorm = 0;
-        for (int64_t i = j + 1; i < st.m; ++i) xnorm = hypot(xnorm, col[i * st.ldy]);
+        for (int64_t i = j + 1; i < st.m; ++i) xnorm = hypot(xnorm, row(i));
         double beta, tau, scale;
         if (xnorm == 0.0) {
             beta = alpha; tau = 0.0; scale = 0.0;
@@ -237,13 +245,12 @@ __global__ void __launch_bounds__(1024) qr_pivot_kernel(QrState st, int64_t j, i
         sh_scale = scale;
     }
     __syncthreads();
-    const int64_t p = piv;
     double* v = st.vhist + j * st.m;
     for (int64_t i = threadIdx.x; i < st.m; i += blockDim.x) {
         double vi;
         if (i < j) vi = 0.0;
         else if (i == j) vi = 1.0;
-        else vi = st.Yt[i * st.ldy + p] * sh_scale;
+        else vi = row(i) * sh_scale;
         v[i] = vi;
     }
 }
