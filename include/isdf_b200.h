@@ -287,7 +287,9 @@ int isdf_project_axes(isdf_ctx* ctx, const double* xyz_dev, int64_t ng, const in
  *   K_gg = (32/15) pi^2 (3/(4 pi))^(5/3) |w_g|^(-1/3).
  * left: kl x n, right: kr x n (row-major, leading dimensions ldl, ldr >= n,
  * not weight-scaled), xyz: n x 3, w: n; kr <= 64.  metric_host: kl x kr,
- * (V + V^T)/2 when symmetrize (requires kl = kr).  FP64 throughout.  The
+ * (V + V^T)/2 when symmetrize (requires kl = kr).  FP64 throughout.  When
+ * symmetrize is set and left and right are the same pointer (and leading
+ * dimension), the symmetry of K is used: half the pairs are summed.  The
  * device variant takes device pointers and a stream; the _host variant host
  * buffers (ctx may be NULL there: the current device). */
 int isdf_grid_metric(isdf_ctx* ctx, const double* left_dev, int64_t ldl, int64_t kl, const double* right_dev,

@@ -617,13 +617,15 @@ int isdf_grid_metric_host(isdf_ctx* ctx, const double* left, int64_t kl, const d
         if (!metric_host || (n > 0 && (!xyz || !w)) || (n > 0 && kl > 0 && !left) || (n > 0 && kr > 0 && !right))
             isdf::fail(isdf::kInvalid, "null grid metric buffer");
         cudaStream_t s = ctx ? ctx->stream : nullptr;
+        // one set given on both sides: one upload, so the device sees one set
+        const bool same = left == right && kl == kr;
         isdf::DeviceBuffer<double> dl, dr, dx, dw;
         upload(dl, left, static_cast<size_t>(kl * n), s);
-        upload(dr, right, static_cast<size_t>(kr * n), s);
+        if (!same) upload(dr, right, static_cast<size_t>(kr * n), s);
         upload(dx, xyz, static_cast<size_t>(3 * n), s);
         upload(dw, w, static_cast<size_t>(n), s);
-        isdf::grid_metric(dl.get(), n, static_cast<int>(kl), dr.get(), n, static_cast<int>(kr), dx.get(),
-                          dw.get(), n, symmetrize != 0, metric_host, s);
+        isdf::grid_metric(dl.get(), n, static_cast<int>(kl), same ? dl.get() : dr.get(), n, static_cast<int>(kr),
+                          dx.get(), dw.get(), n, symmetrize != 0, metric_host, s);
     });
 }
 

@@ -83,6 +83,42 @@ def test_grid_metric_matches_oracle(grid, k):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [37, 129, 1000, 4097])
+@pytest.mark.parametrize("k", [5, 17, 40])
+def test_one_set_half_pairs_form(grid, n, k):
+    """One set on both sides sums half the pairs (tiles above the diagonal, the
+    diagonal tile at weight 1/2); the same values in two buffers take the full
+    sum and (V + V^T)/2.  Both equal the oracle: grids smaller than a row block,
+    ragged tile edges, k across the column-block widths."""
+    import torch
+    from mp_isdf_b200 import capi
+    from mp_isdf_b200 import inputs
+    pts, w = grid
+    rng = np.random.default_rng(n + k)
+    sel = np.sort(rng.choice(len(w), size=min(n, len(w)), replace=False))
+    sel[1] = sel[0]                     # a coincident pair
+    p, ww = pts[sel].copy(), w[sel].copy()
+    theta = rng.normal(size=(k, len(ww)))
+    ref = O.grid_coulomb_metric(theta, p, ww)
+    symbols, xyz = inputs.water_cluster((1, 1, 1), seed=0)
+    mol = inputs.build_tables(symbols, xyz)
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    x = torch.tensor(p, device="cuda")
+    wt = torch.tensor(ww, device="cuda")
+    lt = torch.tensor(theta, device="cuda")
+    half = ctx.grid_metric(x, wt, lt)
+    _close(half, ref)
+    assert np.array_equal(half, half.T)
+    copy = lt.clone()
+    full = np.empty((k, k))
+    capi.check(capi.lib().isdf_grid_metric(ctx.h, capi._ptr(lt), lt.stride(0), k, capi._ptr(copy), copy.stride(0),
+                                           k, capi._ptr(x), capi._ptr(wt), len(ww), 1, capi._ptr(full),
+                                           capi._stream(x)))
+    _close(full, ref)
+    np.testing.assert_allclose(half, full, rtol=1e-12, atol=1e-12 * np.abs(full).max())
+
+
+@pytest.mark.gpu
 def test_grid_cross_metric_device_and_module(grid):
     import torch
     import mp_isdf
