@@ -264,27 +264,31 @@ project_tc_kernel(ProjectArgs args) {
             if (args.point_sq && valid)
                 for (int cc = 0; cc < 4; ++cc)
                     if ((args.comp_mask >> cc) & 1) atomicAdd(&args.point_sq[g * 4 + cc], psq[cc]);
-            // 4. epilogue (warps 0-3: TMEM lane quarter = warp).  The next tile's
-            // first MMA waits for every producer's arrival, so it cannot
-            // overwrite the accumulators before they are read here.
-            if (warp < 4) {
+            // 4. epilogue over every producer warp: a warp reads TMEM lane quarter
+            // warp % 4 and takes every PPT-th group of 16 accumulator columns
+            // (groups past nout are never read).  The next tile's first MMA waits
+            // for every producer's arrival, so it cannot overwrite the
+            // accumulators before they are read here.
+            constexpr int kGroups = NT / 16;
+            if ((warp >> 2) < NAX * kGroups) {
                 if (!tc::mbar_wait(acc_full, t & 1)) fail_wait(1);
                 tc::tc_fence_after();
-                const int row = warp * 32 + lane;
+                const int quarter = warp & 3;
+                const int row = quarter * 32 + lane;
                 const int64_t gg = tile * kRows + row;
-                for (int a = 0; a < NAX; ++a) {
-                    for (int c0 = 0; c0 < NT; c0 += 16) {
-                        uint32_t r[16];
-                        tc::tmem_ld16(tmem_base + (static_cast<uint32_t>(warp * 32) << 16) +
-                                          static_cast<uint32_t>(a * NT + c0), r);
-                        tc::tmem_ld_wait();
-                        if (gg < n) {
-                            const int64_t cs = args.col_stride;
-                            float* out = args.out + gg * args.ld_out + (a * args.nout + c0) * cs;
+                for (int gi = warp >> 2; gi < NAX * kGroups; gi += PPT) {
+                    const int a = gi / kGroups, c0 = (gi % kGroups) * 16;
+                    if (c0 >= args.nout) continue;
+                    uint32_t r[16];
+                    tc::tmem_ld16(tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
+                                      static_cast<uint32_t>(a * NT + c0), r);
+                    tc::tmem_ld_wait();
+                    if (gg < n) {
+                        const int64_t cs = args.col_stride;
+                        float* out = args.out + gg * args.ld_out + (a * args.nout + c0) * cs;
 #pragma unroll
-                            for (int i = 0; i < 16; ++i)
-                                if (c0 + i < args.nout) out[i * cs] = __uint_as_float(r[i]);
-                        }
+                        for (int i = 0; i < 16; ++i)
+                            if (c0 + i < args.nout) out[i * cs] = __uint_as_float(r[i]);
                     }
                 }
                 tc::tc_fence_before();
