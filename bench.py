@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-ao-eval", action="store_true",
+                    help="skip the standalone eval_ao timing over the whole grid")
     ap.add_argument("--widened", action="store_true",
                     help="also time the widened rows on this workload: the grid Coulomb metric of the "
                          "fitted Theta, the FP64 density (column-normalized) sketch and the FP64 "
@@ -251,6 +253,28 @@ def _event_time(fn, reps=2):
         torch.cuda.synchronize()
         t = a.elapsed_time(b) / 1e3
     return out, t
+
+
+def time_ao_eval(ctx, mol, x, hbm):
+    """Standalone AO evaluation (the eval_ao / eval_ao_gradient boundary) over
+    every grid point of the workload: FP64 values (Ng, nao) and FP32 values
+    plus gradients (Ng, nao) + (3, Ng, nao), CUDA events around the last of
+    three calls.  Algorithmic bytes: the output written plus 24 B of
+    coordinates read per point; the roofline is HBM."""
+    import torch
+    n, nao = x.shape[0], mol.nao
+    out = {}
+    for name, dt, grad in (("fp64_values", torch.float64, False), ("fp32_values_gradients", torch.float32, True)):
+        es = 8 if dt == torch.float64 else 4
+        v = torch.empty(n, nao, dtype=dt, device=x.device)
+        g = torch.empty(3, n, nao, dtype=dt, device=x.device) if grad else None
+        _, t = _event_time(lambda: ctx.eval_ao(x, v, g), reps=3)
+        units = n * nao * es * (4 if grad else 1) + n * 24
+        out[name] = {"ms": t * 1e3, "points": int(n), "algorithmic_bytes": int(units),
+                     "achieved_gbs": units / t / 1e9, "peak_gbs": hbm, "frac": units / t / 1e9 / hbm}
+        del v, g
+        torch.cuda.empty_cache()
+    return out
 
 
 def time_widened(ctx, mol, x, wt, w, theta, k, n_kept, cfg):
@@ -585,6 +609,10 @@ def run_ours(args, rank, world, local_rank):
     if cfg.get("electrons") and not args.no_adjoint and world == 1:
         adjoint = time_adjoint(ctx, mol, x, wt, results[head]["piv"], cfg)
 
+    ao_eval = None
+    if world == 1 and not args.no_ao_eval:
+        ao_eval = time_ao_eval(ctx, mol, x, peaks()[0])
+
     widened = None
     if args.widened and world == 1:
         widened = time_widened(ctx, mol, x, wt, w, theta, k, n_kept, cfg)
@@ -669,7 +697,7 @@ def run_ours(args, rank, world, local_rank):
         | {"parallelism": (f"grid shards x{world} (one cluster)" if sharded else f"replicas x{world}")},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": res["clocks"], "kernels": kernels, "forms": forms_out, **extra,
-        "adjoint": adjoint,
+        "adjoint": adjoint, "ao_eval": ao_eval,
     }
     if widened is not None:
         line["widened"] = widened

@@ -31,6 +31,7 @@ Context::~Context() {
     cudaFree(d_shell_lo);
     cudaFree(d_piece_begin);
     cudaFree(d_fill);
+    cudaFree(d_chunk_ao0);
     cudaFree(d_ao_slot);
     cudaFree(ws);
 }
@@ -181,6 +182,100 @@ ao_raw_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restr
     }
 }
 
+// Tiled evaluation for the (Ng, nao) / (3, Ng, nao) layouts: a block takes 32
+// points (lane = point) and walks the K-chunks of the context's chunk layout
+// (contiguous AO ranges of at most 32 slots holding whole contraction groups),
+// warp w evaluating the pieces that the layout balanced onto lane w.  The
+// chunk's values go to a padded shared tile [comp][slot][point]; then every
+// (component, point) row of the chunk is written as one contiguous run of
+// `fill` values, so a warp store covers up to 256 bytes instead of 32
+// scattered words.  The values are those of ao_raw_kernel bit for bit (same
+// offsets, same per-contraction arithmetic), except that a piece whose every
+// primitive is beyond the cutoff at all 32 points is written as +0 without
+// evaluation (the evaluation gives zeros there as well, possibly signed).
+constexpr int kTilePts = 32;
+constexpr int kTileStride = kTilePts + 1;   // padded point stride: conflict-free row reads
+
+template <class T>
+struct TileSink {
+    T* st; int p, base;
+    template <int C> __device__ __forceinline__ void put(int ao, T v) {
+        st[(C * 32 + ao + base) * kTileStride + p] = v;
+    }
+};
+
+struct TileArgs {
+    const ShellDesc* shells; const void* exps; const void* coefs;
+    const int4* pieces; const int* lane_begin; const int* fill; const int* chunk_ao0; int nchunks;
+    const double* pts; int64_t n, ld; void* val; void* grad; bool want_val;
+};
+
+template <class T, bool GRAD, int LMAX, int PPT>
+__global__ void __launch_bounds__(kTilePts * PPT) ao_tile_kernel(TileArgs a) {
+    constexpr int kNComp = GRAD ? 4 : 1;
+    __shared__ T st[kNComp * 32 * kTileStride];
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * kTilePts + lane;
+    const bool valid = g < a.n;
+    const double px = valid ? a.pts[3 * g] : 0.0, py = valid ? a.pts[3 * g + 1] : 0.0,
+                 pz = valid ? a.pts[3 * g + 2] : 0.0;
+    const T* exps = static_cast<const T*>(a.exps);
+    const T* coefs = static_cast<const T*>(a.coefs);
+    T* val = static_cast<T*>(a.val);
+    T* grad = static_cast<T*>(a.grad);
+    // a piece is skipped where amin r^2 exceeds the cutoff with a margin that
+    // covers amin's rounding to FP32 and r^2's rounding to T, so that every
+    // primitive of the shell is also cut in the evaluation
+    const double cut = kExpCut * 1.0001;
+    for (int c = 0; c < a.nchunks; ++c) {
+        const int pb = a.lane_begin[c * PPT + warp], pe = a.lane_begin[c * PPT + warp + 1];
+        for (int pi = pb; pi < pe; ++pi) {
+            const int4 pc = a.pieces[pi];
+            const ShellDesc b = a.shells[pc.x];
+            const int ns = 2 * b.l + 1;
+            const double dx = px - b.x, dy = py - b.y, dz = pz - b.z;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (__all_sync(0xffffffffu, !valid || static_cast<double>(b.amin) * r2 > cut)) {
+                for (int k = pc.w; k < pc.w + pc.z * ns; ++k)
+#pragma unroll
+                    for (int cc = 0; cc < kNComp; ++cc) st[(cc * 32 + k) * kTileStride + lane] = T(0);
+                continue;
+            }
+            TileSink<T> sink{st, lane, pc.w - (b.ao_off + pc.y * ns)};
+            eval_shell_rel<T, GRAD, LMAX>(b, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
+                                          static_cast<T>(r2), exps, coefs, sink, pc.y, pc.y + pc.z);
+        }
+        __syncthreads();
+        const int fill = a.fill[c], ao0 = a.chunk_ao0[c];
+        for (int r = (GRAD && !a.want_val ? 32 : 0) + warp; r < kNComp * 32; r += PPT) {
+            const int cc = r / 32, pt = r % 32;
+            const int64_t gp = static_cast<int64_t>(blockIdx.x) * kTilePts + pt;
+            if (gp < a.n && lane < fill) {
+                const T v = st[(cc * 32 + lane) * kTileStride + pt];
+                if (cc == 0) val[gp * a.ld + ao0 + lane] = v;
+                else grad[((cc - 1) * a.n + gp) * a.ld + ao0 + lane] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <class T, bool GRAD, int LMAX, int PPT>
+void launch_tile(const TileArgs& a, cudaStream_t s) {
+    const int64_t nb = (a.n + kTilePts - 1) / kTilePts;
+    require(nb < (1ll << 31), "too many grid points for one launch");
+    ao_tile_kernel<T, GRAD, LMAX, PPT><<<static_cast<unsigned>(nb), kTilePts * PPT, 0, s>>>(a);
+    ISDF_LAUNCH_CHECK();
+}
+
+template <class T, bool GRAD>
+void launch_tile_l(const Context& c, const TileArgs& a, cudaStream_t s) {
+    // lane counts as in piece_lanes_for_lmax()
+    if (c.lmax <= 2) launch_tile<T, GRAD, 2, 6>(a, s);
+    else if (c.lmax <= 4) launch_tile<T, GRAD, 4, 2>(a, s);
+    else launch_tile<T, GRAD, kMaxL, 2>(a, s);
+}
+
 template <class T, bool GRAD>
 __global__ void __launch_bounds__(kPtsPerBlock * kShellLanes)
 ao_axis_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restrict__ exps,
@@ -253,11 +348,19 @@ template <> const float* coefs_of<float>(const Context& c) { return c.d_coeff; }
 template <class T>
 void eval_ao(const Context& c, const double* pts, int64_t n, T* out_val, T* out_grad,
              int64_t ld, cudaStream_t s) {
+    require(out_val != nullptr || out_grad != nullptr, "AO evaluation needs a values or a gradient output");
     if (n == 0 || c.nao == 0) return;
     ISDF_PROFILE(sizeof(T) == 8 ? "ao_eval_f64" : "ao_eval_f32", s);
     // few points (anchors, candidate columns): one point per block, its shells
     // spread over the block; otherwise 32 points x 4 shell lanes
     const bool few = n <= 2048;
+    if (!few) {
+        TileArgs a{c.d_shells, exps_of<T>(c), coefs_of<T>(c), c.d_pieces, c.d_piece_begin, c.d_fill,
+                   c.d_chunk_ao0, c.nchunks, pts, n, ld, out_val, out_grad, out_val != nullptr};
+        if (out_grad) launch_tile_l<T, true>(c, a, s);
+        else launch_tile_l<T, false>(c, a, s);
+        return;
+    }
     const dim3 block = few ? dim3(1, kPtsPerBlock * kShellLanes) : dim3(kPtsPerBlock, kShellLanes);
     const int64_t nb = (n + block.x - 1) / block.x;
     require(nb < (1ll << 31), "too many grid points for one launch");

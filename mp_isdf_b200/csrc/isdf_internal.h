@@ -143,6 +143,7 @@ struct Context {
     int piece_lanes = 0;                  // producer lanes per point the layout is balanced for
     int* d_piece_begin = nullptr;         // lane j of chunk c: [begin[c*lanes + j], begin[c*lanes + j + 1])
     int* d_fill = nullptr;                // used slots per chunk
+    int* d_chunk_ao0 = nullptr;           // first AO of each chunk (a chunk is a contiguous AO range)
     int2* d_ao_slot = nullptr;            // (chunk, slot) of each AO
     // Grow-only device workspace of the fused selection + fit (the stored AO
     // tiles and the sketch projections), kept across calls so that repeated

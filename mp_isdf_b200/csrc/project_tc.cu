@@ -470,6 +470,9 @@ void build_chunk_layout(Context& c) {
     up(c.d_pieces, pieces);
     up(c.d_piece_begin, lane_begin);
     up(c.d_fill, fill);
+    std::vector<int> ao0(fill.size(), 0);
+    for (size_t i = 1; i < fill.size(); ++i) ao0[i] = ao0[i - 1] + fill[i - 1];
+    up(c.d_chunk_ao0, ao0);
     up(c.d_ao_slot, ao_slot);
 }
 

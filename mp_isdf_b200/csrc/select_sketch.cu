@@ -23,6 +23,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <future>
 #include <limits>
 #include <random>
@@ -176,11 +177,76 @@ inline double canonical53(uint64_t r) {
     // the exact value hi 2^32 + lo rounded once: the correctly rounded conversion
     const double x = (static_cast<double>(static_cast<uint32_t>(r >> 32)) * 0x1p32 +
                       static_cast<double>(static_cast<uint32_t>(r))) * 0x1p-64;
-    return x >= 1.0 ? std::nextafter(1.0, 0.0) : x;
+    return x >= 1.0 ? 0x1.fffffffffffffp-1 : x;   // the largest double below 1
 }
 
 constexpr double kStdDev = 1.0, kMean = 0.0;
 constexpr int64_t kPolarBlock = 2048;   // attempts per block of the transform
+
+// std::mt19937_64 as the C++ standard defines it ([rand.eng.mers], [rand.predef]:
+// w 64, n 312, m 156, r 31, a 0xb5026f5aa96619e9, u 29 d 0x5555555555555555,
+// s 17 b 0x71d67fffeda60000, t 37 c 0xfff7eee000000000, l 43,
+// f 6364136223846793005), producing its outputs 312 at a time: the state
+// transition runs over the whole array in branch-free loops and the tempering
+// in a separate loop, both of which the compiler vectorises.  The output
+// sequence is the standard engine's for the same seed.
+class Mt64Blocks {
+public:
+    static constexpr int kN = 312, kM = 156;
+    explicit Mt64Blocks(uint64_t seed) {
+        x_[0] = seed;
+        for (int i = 1; i < kN; ++i) x_[i] = 6364136223846793005ULL * (x_[i - 1] ^ (x_[i - 1] >> 62)) + i;
+    }
+    uint64_t operator()() {
+        if (idx_ == kN) { transition(); temper(buf_); idx_ = 0; }
+        return buf_[idx_++];
+    }
+    // the next `count` outputs, in order
+    void fill(uint64_t* out, int64_t count) {
+        while (count > 0) {
+            if (idx_ == kN) {
+                transition();
+                if (count >= kN) {   // a whole block straight into the output
+                    temper(out);
+                    out += kN;
+                    count -= kN;
+                    continue;
+                }
+                temper(buf_);
+                idx_ = 0;
+            }
+            const int64_t take = std::min<int64_t>(count, kN - idx_);
+            std::memcpy(out, buf_ + idx_, static_cast<size_t>(take) * sizeof(uint64_t));
+            out += take;
+            count -= take;
+            idx_ += static_cast<int>(take);
+        }
+    }
+
+private:
+    static uint64_t twist(uint64_t cur, uint64_t next, uint64_t far) {
+        constexpr uint64_t kUpper = ~((uint64_t(1) << 31) - 1), kLower = (uint64_t(1) << 31) - 1;
+        const uint64_t y = (cur & kUpper) | (next & kLower);
+        return far ^ (y >> 1) ^ ((uint64_t(0) - (y & 1)) & 0xb5026f5aa96619e9ULL);
+    }
+    __attribute__((optimize("O3"))) void transition() {
+        for (int i = 0; i < kN - kM; ++i) x_[i] = twist(x_[i], x_[i + 1], x_[i + kM]);
+        for (int i = kN - kM; i < kN - 1; ++i) x_[i] = twist(x_[i], x_[i + 1], x_[i + kM - kN]);
+        x_[kN - 1] = twist(x_[kN - 1], x_[0], x_[kM - 1]);
+    }
+    __attribute__((optimize("O3"))) void temper(uint64_t* out) const {
+        for (int i = 0; i < kN; ++i) {
+            uint64_t z = x_[i];
+            z ^= (z >> 29) & 0x5555555555555555ULL;
+            z ^= (z << 17) & 0x71d67fffeda60000ULL;
+            z ^= (z << 37) & 0xfff7eee000000000ULL;
+            out[i] = z ^ (z >> 43);
+        }
+    }
+    uint64_t x_[kN];
+    uint64_t buf_[kN];
+    int idx_ = kN;
+};
 
 struct PolarDraws {
     std::vector<uint64_t> raw;        // two engine outputs per attempt
@@ -193,22 +259,23 @@ struct PolarDraws {
 // The sequential part: engine outputs until `pairs` attempts are accepted,
 // published block by block with the deviates produced so far (at most
 // max_blocks; the caller finishes a stream that needs more).  Returns the
-// engine for that tail.
-std::mt19937_64 polar_draw(uint64_t seed, int64_t pairs, int64_t max_blocks, PolarDraws& pd) {
-    std::mt19937_64 gen(seed);
-    int64_t acc = 0, a = 0, b = 0;
+// engine for that tail: it stands right after the last block's outputs,
+// which are then all consumed.
+Mt64Blocks polar_draw(uint64_t seed, int64_t pairs, int64_t max_blocks, PolarDraws& pd) {
+    Mt64Blocks gen(seed);
+    int64_t acc = 0, b = 0;
     pd.block_out[0] = 0;
     while (acc < pairs && b < max_blocks) {
-        const int64_t a1 = a + kPolarBlock;
-        for (; a < a1 && acc < pairs; ++a) {
-            const uint64_t r0 = gen(), r1 = gen();
-            pd.raw[2 * a] = r0;
-            pd.raw[2 * a + 1] = r1;
-            const double x = 2.0 * canonical53(r0) - 1.0;
-            const double y = 2.0 * canonical53(r1) - 1.0;
+        const uint64_t* raw = pd.raw.data() + 2 * b * kPolarBlock;
+        gen.fill(pd.raw.data() + 2 * b * kPolarBlock, 2 * kPolarBlock);
+        int64_t n_ok = 0;
+        for (int64_t a = 0; a < kPolarBlock; ++a) {
+            const double x = 2.0 * canonical53(raw[2 * a]) - 1.0;
+            const double y = 2.0 * canonical53(raw[2 * a + 1]) - 1.0;
             const double r2 = x * x + y * y;
-            acc += (r2 <= 1.0 && r2 != 0.0) ? 1 : 0;
+            n_ok += (r2 <= 1.0) & (r2 != 0.0);
         }
+        acc += n_ok;
         pd.block_out[b + 1] = 2 * acc;
         pd.published.store(++b, std::memory_order_release);
     }
@@ -257,7 +324,7 @@ void sketch_factors(int64_t d, int64_t ell, uint64_t seed, double* u, double* v)
     // two threads draw (one per stream) while the others transform each
     // published block; a worker takes every nw-th block of each stream
     const int nw = static_cast<int>(std::clamp(std::thread::hardware_concurrency(), 3u, 12u)) - 2;
-    std::mt19937_64 tail_gen[2];
+    Mt64Blocks tail_gen[2] = {Mt64Blocks(seeds[0]), Mt64Blocks(seeds[1])};
     auto work = [&pd, &outs, count, nw](int w) {
         for (int k = 0; k < 2; ++k)
             for (int64_t b = w;; b += nw) {

@@ -88,6 +88,66 @@ def test_ao_float32_and_device_tensor_path(small_water):
     assert np.max(np.abs(g32.cpu().numpy() - gref) / gscale) < 4e-6
 
 
+@pytest.mark.parametrize("extra_l", [None, 4, 6])
+def test_ao_tiled_path_matches_point_path_and_oracle(small_water, extra_l):
+    """Grids above 2048 points take the tiled evaluator (32 points per block,
+    chunk rows stored contiguously); fewer take one point per block.  Both
+    give the same values (up to the contraction of a product into an FMA,
+    which may differ between kernels), over a ragged point count,
+    a block of points far from every atom (whole pieces skipped by the
+    warp-wide cutoff test) and, with an added l = 4 or l = 6 shell, the
+    two-lane layouts; FP64 also against the oracle."""
+    import torch
+    from mp_isdf_b200 import capi, inputs
+    mol, pts, w = small_water
+    if extra_l is None:
+        tables = mol
+    else:
+        def shells_of(sym):
+            sh = inputs.element_shells(sym)
+            if sym == "O":
+                sh = sh + [inputs.Shell(extra_l, np.array([2.1, 0.6]), np.array([[0.7, 0.4], [0.0, 1.0]]))]
+            return sh
+        tables = inputs.build_tables(mol.symbols, mol.coords, shells_of)
+    ctx = capi.Context(tables.atm, tables.bas, tables.env)
+    oc = O.OracleContext(tables.atm, tables.bas, tables.env)
+    rng = np.random.default_rng(3)
+    far = mol.coords[0] + np.array([40.0, 0.0, 0.0]) + rng.normal(size=(64, 3))
+    p = np.vstack([pts[: 2000], far, mol.coords, rng.normal(size=(1000, 3)) * 3 + mol.coords[1]])
+    n, nao = len(p), tables.nao
+    assert n > 2048 and n % 32 != 0
+    xyz = torch.tensor(p, device="cuda")
+    sub = torch.arange(0, n, 3, device="cuda")   # 1023 points: the one-point-per-block path
+    with pytest.raises(capi.IsdfError, match="needs a values or a gradient output"):
+        ctx.eval_ao(xyz, None, None, dtype=torch.float64)   # nothing to write
+    for dt, tol in ((torch.float64, 1e-14), (torch.float32, 1e-6)):
+        v = torch.empty(n, nao, dtype=dt, device="cuda")
+        g = torch.empty(3, n, nao, dtype=dt, device="cuda")
+        ctx.eval_ao(xyz, v, g)
+        vo = torch.empty(n, nao, dtype=dt, device="cuda")
+        ctx.eval_ao(xyz, vo)
+        go = torch.empty(3, n, nao, dtype=dt, device="cuda")
+        ctx.eval_ao(xyz, None, go, dtype=dt)
+        vs = torch.empty(len(sub), nao, dtype=dt, device="cuda")
+        gs = torch.empty(3, len(sub), nao, dtype=dt, device="cuda")
+        ctx.eval_ao(xyz[sub].contiguous(), vs, gs)
+        torch.cuda.synchronize()
+        assert torch.equal(g, go)   # the same kernel with and without the values written
+        vt, gt = v[sub].double().cpu().numpy(), g[:, sub].double().cpu().numpy()
+        vp, gp = vs.double().cpu().numpy(), gs.double().cpu().numpy()
+        vscale = np.abs(vp).max(axis=1, keepdims=True) + 1e-300
+        gscale = np.abs(gp).max(axis=2, keepdims=True) + 1e-300
+        # values alone come from the kernel without gradients (its own FMA contraction)
+        vv = vo[sub].double().cpu().numpy()
+        assert np.max(np.abs(vv - vp) / vscale) <= tol
+        assert np.max(np.abs(vt - vp) / vscale) <= tol
+        assert np.max(np.abs(gt - gp) / gscale) <= tol
+        assert not v[2000:2064].any() and not g[:, 2000:2064].any()   # far block: exact zeros
+        if dt == torch.float64:
+            np.testing.assert_allclose(v.cpu().numpy(), oc.eval_ao(p), rtol=1e-11, atol=1e-12)
+            np.testing.assert_allclose(g.cpu().numpy(), oc.eval_ao_gradient(p), rtol=1e-11, atol=1e-12)
+
+
 def test_evaluate_axis_matches_oracle(water, mpi):
     mol, pts, w, c, sel, oc = water
     p = pts[::211]
