@@ -182,18 +182,21 @@ ao_raw_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restr
     }
 }
 
-// Tiled evaluation for the (Ng, nao) / (3, Ng, nao) layouts: a block takes 32
-// points (lane = point) and walks the K-chunks of the context's chunk layout
-// (contiguous AO ranges of at most 32 slots holding whole contraction groups),
-// warp w evaluating the pieces that the layout balanced onto lane w.  The
-// chunk's values go to a padded shared tile [comp][slot][point]; then every
-// (component, point) row of the chunk is written as one contiguous run of
-// `fill` values, so a warp store covers up to 256 bytes instead of 32
-// scattered words.  The values are those of ao_raw_kernel bit for bit (same
-// offsets, same per-contraction arithmetic), except that a piece whose every
-// primitive is beyond the cutoff at all 32 points is written as +0 without
-// evaluation (the evaluation gives zeros there as well, possibly signed).
-constexpr int kTilePts = 32;
+// Tiled evaluation for the (Ng, nao) / (3, Ng, nao) layouts: a block takes 64
+// points (two warps per piece lane, lane = point) and walks the K-chunks of
+// the context's chunk layout (contiguous AO ranges of at most 32 slots holding
+// whole contraction groups); the two warps of lane j evaluate the pieces that
+// the layout balanced onto lane j, for points 0-31 and 32-63, so each piece's
+// metadata is read twice close together.  The chunk's values go to a padded
+// shared tile [comp][slot][point]; then every (component, point) row of the
+// chunk is written as one contiguous run of `fill` values from a row pointer
+// formed once per block, so a warp store covers up to 256 bytes instead of 32
+// scattered words.  The values are those of ao_raw_kernel up to the
+// contraction of products into FMAs (same offsets, same per-contraction
+// arithmetic), except that a piece whose every primitive is beyond the cutoff
+// at all 32 points of a warp is written as +0 without evaluation (the
+// evaluation gives zeros there as well, possibly signed).
+constexpr int kTilePts = 64;
 constexpr int kTileStride = kTilePts + 1;   // padded point stride: conflict-free row reads
 
 template <class T>
@@ -210,25 +213,44 @@ struct TileArgs {
     const double* pts; int64_t n, ld; void* val; void* grad; bool want_val;
 };
 
+template <class T, bool GRAD>
+constexpr size_t tile_smem_bytes() {
+    return (GRAD ? 4 : 1) * 32 * kTileStride * sizeof(T) + (GRAD ? 4 : 1) * kTilePts * sizeof(T*);
+}
+
 template <class T, bool GRAD, int LMAX, int PPT>
-__global__ void __launch_bounds__(kTilePts * PPT) ao_tile_kernel(TileArgs a) {
+__global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) ao_tile_kernel(TileArgs a) {
     constexpr int kNComp = GRAD ? 4 : 1;
-    __shared__ T st[kNComp * 32 * kTileStride];
+    constexpr int kWarps = kTilePts / 32 * PPT;
+    extern __shared__ __align__(16) uint8_t tile_raw[];
+    T** rowp = reinterpret_cast<T**>(tile_raw);                       // [kNComp][kTilePts]
+    T* st = reinterpret_cast<T*>(tile_raw + kNComp * kTilePts * sizeof(T*));
     const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
-    const int64_t g = static_cast<int64_t>(blockIdx.x) * kTilePts + lane;
+    const int lanegrp = warp % PPT, p = (warp / PPT) * 32 + lane;
+    const int64_t b0 = static_cast<int64_t>(blockIdx.x) * kTilePts;
+    const int64_t g = b0 + p;
     const bool valid = g < a.n;
     const double px = valid ? a.pts[3 * g] : 0.0, py = valid ? a.pts[3 * g + 1] : 0.0,
                  pz = valid ? a.pts[3 * g + 2] : 0.0;
     const T* exps = static_cast<const T*>(a.exps);
     const T* coefs = static_cast<const T*>(a.coefs);
-    T* val = static_cast<T*>(a.val);
-    T* grad = static_cast<T*>(a.grad);
+    // output row of (component, point), or null where nothing is written
+    for (int i = threadIdx.x; i < kNComp * kTilePts; i += blockDim.x) {
+        const int cc = i / kTilePts;
+        const int64_t gp = b0 + i % kTilePts;
+        T* r = nullptr;
+        if (gp < a.n) {
+            if (cc == 0) r = a.want_val ? static_cast<T*>(a.val) + gp * a.ld : nullptr;
+            else r = static_cast<T*>(a.grad) + ((cc - 1) * a.n + gp) * a.ld;
+        }
+        rowp[i] = r;
+    }
     // a piece is skipped where amin r^2 exceeds the cutoff with a margin that
     // covers amin's rounding to FP32 and r^2's rounding to T, so that every
     // primitive of the shell is also cut in the evaluation
     const double cut = kExpCut * 1.0001;
     for (int c = 0; c < a.nchunks; ++c) {
-        const int pb = a.lane_begin[c * PPT + warp], pe = a.lane_begin[c * PPT + warp + 1];
+        const int pb = a.lane_begin[c * PPT + lanegrp], pe = a.lane_begin[c * PPT + lanegrp + 1];
         for (int pi = pb; pi < pe; ++pi) {
             const int4 pc = a.pieces[pi];
             const ShellDesc b = a.shells[pc.x];
@@ -238,23 +260,19 @@ __global__ void __launch_bounds__(kTilePts * PPT) ao_tile_kernel(TileArgs a) {
             if (__all_sync(0xffffffffu, !valid || static_cast<double>(b.amin) * r2 > cut)) {
                 for (int k = pc.w; k < pc.w + pc.z * ns; ++k)
 #pragma unroll
-                    for (int cc = 0; cc < kNComp; ++cc) st[(cc * 32 + k) * kTileStride + lane] = T(0);
+                    for (int cc = 0; cc < kNComp; ++cc) st[(cc * 32 + k) * kTileStride + p] = T(0);
                 continue;
             }
-            TileSink<T> sink{st, lane, pc.w - (b.ao_off + pc.y * ns)};
+            TileSink<T> sink{st, p, pc.w - (b.ao_off + pc.y * ns)};
             eval_shell_rel<T, GRAD, LMAX>(b, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
                                           static_cast<T>(r2), exps, coefs, sink, pc.y, pc.y + pc.z);
         }
         __syncthreads();
         const int fill = a.fill[c], ao0 = a.chunk_ao0[c];
-        for (int r = (GRAD && !a.want_val ? 32 : 0) + warp; r < kNComp * 32; r += PPT) {
-            const int cc = r / 32, pt = r % 32;
-            const int64_t gp = static_cast<int64_t>(blockIdx.x) * kTilePts + pt;
-            if (gp < a.n && lane < fill) {
-                const T v = st[(cc * 32 + lane) * kTileStride + pt];
-                if (cc == 0) val[gp * a.ld + ao0 + lane] = v;
-                else grad[((cc - 1) * a.n + gp) * a.ld + ao0 + lane] = v;
-            }
+        for (int r = warp; r < kNComp * kTilePts; r += kWarps) {
+            T* row = rowp[r];
+            if (row != nullptr && lane < fill)
+                row[ao0 + lane] = st[((r / kTilePts) * 32 + lane) * kTileStride + r % kTilePts];
         }
         __syncthreads();
     }
@@ -264,7 +282,11 @@ template <class T, bool GRAD, int LMAX, int PPT>
 void launch_tile(const TileArgs& a, cudaStream_t s) {
     const int64_t nb = (a.n + kTilePts - 1) / kTilePts;
     require(nb < (1ll << 31), "too many grid points for one launch");
-    ao_tile_kernel<T, GRAD, LMAX, PPT><<<static_cast<unsigned>(nb), kTilePts * PPT, 0, s>>>(a);
+    constexpr size_t smem = tile_smem_bytes<T, GRAD>();
+    auto kern = ao_tile_kernel<T, GRAD, LMAX, PPT>;
+    if constexpr (smem > 48 * 1024)
+        ISDF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    kern<<<static_cast<unsigned>(nb), kTilePts / 32 * PPT * 32, smem, s>>>(a);
     ISDF_LAUNCH_CHECK();
 }
 
