@@ -12,6 +12,7 @@
 #include <cstring>
 #include <memory>
 #include <new>
+#include <vector>
 
 struct isdf_ctx {
     std::unique_ptr<isdf::Context> c;
@@ -379,7 +380,7 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
               int64_t k, int32_t precision, const double* theta_in, double* theta_out,
               isdf_fit_info* info, double* l2, double* rel, cudaStream_t s, bool want_error = true,
               const isdf::RetainedAo* ra = nullptr, const AnchorCoords* ac = nullptr,
-              double* sums = nullptr) {
+              double* sums = nullptr, const isdf::FitChunkHook* on_chunk = nullptr) {
     auto& c = ctx_of(ctx);
     DeviceGuard dg(c.device);
     if (ng < 0 || k < 0) isdf::fail(isdf::kInvalid, "sizes must be nonnegative");
@@ -419,7 +420,7 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
     isdf::FitOutput o;
     if (!have && precision == ISDF_MIXED && isdf::fit_mixed_supported(k)) {
         o = isdf::fit_grid_mixed(c, xyz, w, kp, f, theta, kp.n, s, reuse ? ra->tiles : nullptr,
-                                 reuse ? ra->psq.get() : nullptr);
+                                 reuse ? ra->psq.get() : nullptr, on_chunk);
         o.path = 1;
         if (!(o.mixed_bound <= isdf::kMixedFitTolerance)) {
             // the anchors' conditioning can amplify the BF16x3 Gram error past
@@ -511,6 +512,45 @@ int isdf_select_fit(isdf_ctx* ctx, const isdf_select_args* args, const double* x
     });
 }
 
+namespace {
+
+// A copy stream and its events for streaming results out while the compute
+// stream runs; finish() (or the destructor, on an error path) waits for the
+// copies and releases them.
+struct ChunkCopies {
+    cudaStream_t stream = nullptr;
+    std::vector<cudaEvent_t> events;
+    void begin() {
+        if (!stream) ISDF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    }
+    cudaEvent_t event() {
+        cudaEvent_t e = nullptr;
+        ISDF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        events.push_back(e);
+        return e;
+    }
+    bool used() const { return stream != nullptr; }
+    void finish() {
+        if (stream) {
+            const cudaError_t r = cudaStreamSynchronize(stream);
+            release();
+            ISDF_CUDA(r);
+        }
+    }
+    void release() {
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+        events.clear();
+        if (stream) {
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
+        stream = nullptr;
+    }
+    ~ChunkCopies() { release(); }
+};
+
+}  // namespace
+
 int isdf_select_fit_host(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz,
                          const double* w, int64_t ng, int64_t* pivots, int64_t capacity,
                          int64_t* npivots, isdf_select_info* select_info, int32_t want_error,
@@ -534,9 +574,25 @@ int isdf_select_fit_host(isdf_ctx* ctx, const isdf_select_args* args, const doub
         const int64_t np = static_cast<int64_t>(out.size());
         isdf::DeviceBuffer<double> dt(static_cast<size_t>(std::max<int64_t>(1, np * ng)), s);
         isdf_fit_info local{};
+        // In the mixed fit over the stored AO tiles, each chunk's Theta columns
+        // are copied out on a second stream while the next chunk is fitted; if
+        // the mixed Theta is then rejected (FP64 recompute), it is copied again.
+        ChunkCopies cp;
+        isdf::FitChunkHook hook = [&](int64_t g0, int64_t m) {
+            const int64_t n = keep.kp.n;
+            cp.begin();
+            cudaEvent_t ev = cp.event();
+            ISDF_CUDA(cudaEventRecord(ev, s));
+            ISDF_CUDA(cudaStreamWaitEvent(cp.stream, ev, 0));
+            ISDF_CUDA(cudaMemcpy2DAsync(theta_host + g0, n * sizeof(double), dt.get() + g0, n * sizeof(double),
+                                        m * sizeof(double), np, cudaMemcpyDeviceToHost, cp.stream));
+        };
+        const bool stream_out = theta_host && np > 0 && keep.valid;
         fit_impl(ctx, dx.get(), dw.get(), ng, out.data(), np, args->precision, nullptr, dt.get(), &local,
-                 nullptr, nullptr, s, want_error != 0, &keep);
-        if (theta_host && np * local.n_kept)
+                 nullptr, nullptr, s, want_error != 0, &keep, nullptr, nullptr, stream_out ? &hook : nullptr);
+        const bool copied = cp.used() && local.fit_path == 1;
+        cp.finish();
+        if (theta_host && np * local.n_kept && !copied)
             ISDF_CUDA(cudaMemcpyAsync(theta_host, dt.get(), np * local.n_kept * sizeof(double),
                                       cudaMemcpyDeviceToHost, s));
         ISDF_CUDA(cudaStreamSynchronize(s));

@@ -477,7 +477,7 @@ bool fit_mixed_supported(int64_t k) { return k >= 1 && k <= 64 && project_tc_sup
 
 FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
                          const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s,
-                         const uint8_t* ao_tiles, const float* ao_psq) {
+                         const uint8_t* ao_tiles, const float* ao_psq, const FitChunkHook* on_chunk) {
     FitOutput out;
     const int64_t n = kp.n, k = f.k, nao = c.nao;
     out.theta_w.assign(k, 0.0);
@@ -499,24 +499,32 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
                                                             static_cast<int>(nao), anorm.get());
     ISDF_LAUNCH_CHECK();
     const float* point_sq = ao_psq;
-    if (ao_tiles) {
-        // AO values of these points already sit in HBM as split-BF16 tiles
-        gram_from_tiles(c, plan, ao_tiles, n, G.get(), k, err.get(), s);
-    } else {
+    if (!ao_tiles) {
         psq.reset(static_cast<size_t>(n * 4), s);
         psq.zero(s);
         project_tc(c, plan, pts, kp.index.get(), n, nullptr, G.get(), k, 1, nullptr, psq.get(), err.get(), s);
         point_sq = psq.get();
     }
-    {
-        ISDF_PROFILE("fit_mixed", s);
-        const size_t smem = static_cast<size_t>(2 * k * k + k) * sizeof(double);
-        auto kern = k <= 16 ? fit_mixed_kernel<16> : k <= 32 ? fit_mixed_kernel<32> : fit_mixed_kernel<64>;
-        kern<<<blocks_for(n), 256, smem, s>>>(G.get(), point_sq, n, static_cast<int>(k),
-                                                          f.T.get(), f.M.get(), anorm.get(), f.wa.get(),
-                                                          w, kp.index.get(), theta, ldt, tw.get(),
-                                                          acc.get());
-        ISDF_LAUNCH_CHECK();
+    // With stored tiles and a hook, the points go in a few chunks of whole
+    // 128-point tiles, each at least two waves of the stored-tile GEMM.
+    const int64_t tiles = (n + 127) / 128;
+    const int64_t nchunk = (ao_tiles && on_chunk) ? std::max<int64_t>(1, std::min<int64_t>(4, tiles / 296)) : 1;
+    const int64_t per = (tiles + nchunk - 1) / nchunk * 128;
+    const size_t smem = static_cast<size_t>(2 * k * k + k) * sizeof(double);
+    auto kern = k <= 16 ? fit_mixed_kernel<16> : k <= 32 ? fit_mixed_kernel<32> : fit_mixed_kernel<64>;
+    for (int64_t g0 = 0; g0 < n; g0 += per) {
+        const int64_t m = std::min(per, n - g0);
+        if (ao_tiles)
+            // AO values of these points already sit in HBM as split-BF16 tiles
+            gram_from_tiles(c, plan, ao_tiles + stored_tile_bytes(c, g0), m, G.get() + g0 * k, k, err.get(), s);
+        {
+            ISDF_PROFILE("fit_mixed", s);
+            kern<<<blocks_for(m), 256, smem, s>>>(G.get() + g0 * k, point_sq + g0 * 4, m, static_cast<int>(k),
+                                                  f.T.get(), f.M.get(), anorm.get(), f.wa.get(), w,
+                                                  kp.index.get() + g0, theta + g0, ldt, tw.get(), acc.get());
+            ISDF_LAUNCH_CHECK();
+        }
+        if (on_chunk && ao_tiles) (*on_chunk)(g0, m);
     }
     double h[6];
     int herr = 0;

@@ -3,6 +3,8 @@
 
 #include "isdf_select.h"
 
+#include <functional>
+
 namespace isdf {
 
 struct AnchorFactor {
@@ -43,11 +45,16 @@ FitOutput fit_grid(const Context& c, const double* pts, const double* w, const K
 // then h, X = T h and Theta in FP64.  The pair-space error is not evaluated
 // here (see fit_grid with have_theta).  With `ao_tiles` (the AO value tiles a
 // mixed sketch of the same kept points left in HBM) and their per-point sums
-// of squares `ao_psq`, G comes from a GEMM over the tiles instead.
+// of squares `ao_psq`, G comes from a GEMM over the tiles instead; then, with
+// `on_chunk`, the points are fitted in a few chunks and on_chunk(g0, m) is
+// called after the launches that write Theta's columns [g0, g0 + m) on s (a
+// caller can start copying those columns out while the next chunk runs).
 bool fit_mixed_supported(int64_t k);
+using FitChunkHook = std::function<void(int64_t g0, int64_t m)>;
 FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
                          const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s,
-                         const uint8_t* ao_tiles = nullptr, const float* ao_psq = nullptr);
+                         const uint8_t* ao_tiles = nullptr, const float* ao_psq = nullptr,
+                         const FitChunkHook* on_chunk = nullptr);
 
 void gather_points(const double* pts, const double* w, const int64_t* idx, int64_t n,
                    int64_t npts_total, double* out_pts, double* out_w, cudaStream_t s);

@@ -188,6 +188,33 @@ def test_select_fit_host_buffers(small_water):
     assert rel <= 1e-12 * max(1.0, fd.condition) ** 2, rel
 
 
+def test_select_fit_host_streams_theta_by_chunks():
+    """(H2O)32 at grid level 3: the mixed Theta is accepted (fit path 1), so the
+    host-buffer call fits the kept points in chunks and copies each chunk's
+    Theta columns out while the next is fitted.  Its Theta equals the device
+    call's bit for bit (per point the same tile GEMM and FP64 epilogue), into a
+    pinned and into a pageable host buffer."""
+    import torch
+    from mp_isdf_b200 import capi, inputs
+    mol, pts, w, cfg = inputs.make_config("c3")
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    kw = dict(algorithm="rand_sketch", axes=("ao",), max_rank=cfg["rank"], oversampling=cfg["oversampling"],
+              seed=cfg["sketch_seed"], precision="mixed")
+    x = torch.tensor(pts, device="cuda")
+    wt = torch.tensor(w, device="cuda")
+    theta = torch.zeros(cfg["rank"] * len(pts), dtype=torch.float64, device="cuda")
+    piv_d, _, fd = ctx.select_fit(x, wt, theta, want_error=False, **kw)
+    torch.cuda.synchronize()
+    assert fd.fit_path == 1 and fd.n_kept > 4 * 296 * 128
+    th_d = theta[:len(piv_d) * fd.n_kept].cpu().numpy().reshape(len(piv_d), fd.n_kept)
+    pinned = torch.empty(cfg["rank"] * len(pts), dtype=torch.float64).pin_memory().numpy()
+    for out in (pinned, None):
+        piv_h, th_h, si, fi = ctx.select_fit_host(pts, w, want_error=False, out=out, **kw)
+        np.testing.assert_array_equal(piv_h, piv_d)
+        assert fi.fit_path == 1 and fi.n_kept == fd.n_kept
+        np.testing.assert_array_equal(th_h, th_d)
+
+
 def test_mixed_projection_follows_moved_atoms(small_water):
     """After isdf_ctx_set_coords the tensor-core path evaluates AOs at the new
     centres: mixed and FP64 projections agree to the split-BF16 bound."""
