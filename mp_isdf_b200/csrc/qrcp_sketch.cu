@@ -490,8 +490,11 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
         {
             ISDF_PROFILE("qrcp_sketch_update", s);
             const int64_t touched = m - (j > 0 ? j - 1 : 0);
+            // shared memory for the rows this step stages only: later steps
+            // (fewer rows) keep more blocks, and more copies in flight, per SM
             if (touched <= kRegRows)
-                qr_update_kernel<true><<<nblocks, kQrThreads, kStagedBytes, s>>>(st, j);
+                qr_update_kernel<true><<<nblocks, kQrThreads,
+                                         static_cast<size_t>(touched) * kQrThreads * sizeof(double), s>>>(st, j);
             else
                 qr_update_kernel<false><<<nblocks, kQrThreads, 0, s>>>(st, j);
             ISDF_LAUNCH_CHECK();
