@@ -85,11 +85,29 @@ AxisSpec make_axis_spec(const Context& c, const int32_t* axes, int naxes, const 
 void validate_axis_weights(const double* axis_weights, int naxes);
 std::vector<double> axis_scales_from_sumsq(const AxisSpec& ax, const double* sumsq4,
                                            const double* axis_weights, bool any_eligible);
+// Page-locked host memory for vectors that are copied to the device, from a
+// process-wide cache of blocks (a block goes back to the cache when its vector
+// is freed, so repeated calls pin nothing new); pageable memory if pinning
+// fails.  Copies from it are true asynchronous DMA transfers.
+void* pinned_host_alloc(size_t bytes);
+void pinned_host_free(void* p, size_t bytes) noexcept;
+template <class T>
+struct PinnedAllocator {
+    using value_type = T;
+    PinnedAllocator() = default;
+    template <class U> PinnedAllocator(const PinnedAllocator<U>&) {}
+    T* allocate(size_t n) { return static_cast<T*>(pinned_host_alloc(n * sizeof(T))); }
+    void deallocate(T* p, size_t n) noexcept { pinned_host_free(p, n * sizeof(T)); }
+    template <class U> bool operator==(const PinnedAllocator<U>&) const { return true; }
+    template <class U> bool operator!=(const PinnedAllocator<U>&) const { return false; }
+};
+// Host copies of the sketch factors (uploaded once per selection).
+using HostFactors = std::vector<double, PinnedAllocator<double>>;
+
 // Gaussian sketch factors U, V (d x ell, u[a*ell+s]): std::normal_distribution
 // over std::mt19937_64(seed) and std::mt19937_64(seed ^ 0x9e3779b97f4a7c15).
 void sketch_factors(int64_t d, int64_t ell, uint64_t seed, double* u, double* v);
-void sketch_factors(int64_t d, int64_t ell, uint64_t seed, std::vector<double>& u,
-                    std::vector<double>& v);
+void sketch_factors(int64_t d, int64_t ell, uint64_t seed, HostFactors& u, HostFactors& v);
 
 // Full column-pivoted Householder QR of the ell x n sketch stored row-wise
 // (Yt[s*ldy + g]); modifies Yt.  With `exact`, columns whose error interval
@@ -124,7 +142,7 @@ struct RetainedAo {
 // axis entry is the plain AO value and the tiles fit in free device memory.
 MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& kp, const double* w,
                          const AxisSpec& ax, const double* axis_weights, int64_t ell,
-                         const std::vector<double>& u, const std::vector<double>& v, double* Yt,
+                         const HostFactors& u, const HostFactors& v, double* Yt,
                          int64_t ldy, cudaStream_t s, RetainedAo* keep = nullptr);
 
 std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, const double* w,
@@ -161,7 +179,7 @@ struct SketchShard {
     SelectOptions o;
     SketchSetup su;
     KeptPoints kp;
-    std::vector<double> u, v;
+    HostFactors u, v;
     DeviceBuffer<float> Pf, psq;     // mixed: projections, per-point sums of squares
     DeviceBuffer<double> Pd;         // FP64: projections
     double sumsq[4] = {0, 0, 0, 0};

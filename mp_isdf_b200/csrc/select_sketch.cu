@@ -23,9 +23,12 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <future>
 #include <limits>
+#include <mutex>
+#include <new>
 #include <random>
 #include <thread>
 
@@ -156,6 +159,63 @@ void validate_axis_weights(const double* axis_weights, int naxes) {
     for (int a = 0; a < naxes; ++a)
         if (!std::isfinite(axis_weights[a]) || axis_weights[a] <= 0)
             fail(kInvalid, "axis weights must be finite and positive");
+}
+
+// ------------------------------------------------------------------------------
+// pinned host blocks
+// ------------------------------------------------------------------------------
+namespace {
+struct PinnedBlock { void* p; size_t bytes; bool pinned; };
+std::mutex g_pinned_mu;
+std::vector<PinnedBlock> g_pinned_free;   // blocks returned by freed vectors
+std::vector<PinnedBlock> g_pinned_live;
+}  // namespace
+
+void* pinned_host_alloc(size_t bytes) {
+    if (bytes == 0) bytes = 1;
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mu);
+        // the smallest cached block that is large enough
+        size_t best = g_pinned_free.size();
+        for (size_t i = 0; i < g_pinned_free.size(); ++i)
+            if (g_pinned_free[i].bytes >= bytes &&
+                (best == g_pinned_free.size() || g_pinned_free[i].bytes < g_pinned_free[best].bytes))
+                best = i;
+        if (best < g_pinned_free.size()) {
+            const PinnedBlock b = g_pinned_free[best];
+            g_pinned_free.erase(g_pinned_free.begin() + static_cast<std::ptrdiff_t>(best));
+            g_pinned_live.push_back(b);
+            return b.p;
+        }
+    }
+    PinnedBlock b{nullptr, bytes, true};
+    if (cudaHostAlloc(&b.p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();   // not sticky: fall back to pageable memory
+        b.p = std::malloc(bytes);
+        b.pinned = false;
+        if (!b.p) throw std::bad_alloc();
+    }
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    g_pinned_live.push_back(b);
+    return b.p;
+}
+
+void pinned_host_free(void* p, size_t) noexcept {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    for (size_t i = 0; i < g_pinned_live.size(); ++i)
+        if (g_pinned_live[i].p == p) {
+            const PinnedBlock b = g_pinned_live[i];
+            g_pinned_live.erase(g_pinned_live.begin() + static_cast<std::ptrdiff_t>(i));
+            if (b.pinned && g_pinned_free.size() < 8) {
+                g_pinned_free.push_back(b);   // kept for the next selection
+            } else if (b.pinned) {
+                cudaFreeHost(b.p);
+            } else {
+                std::free(b.p);
+            }
+            return;
+        }
 }
 
 // ------------------------------------------------------------------------------
@@ -378,8 +438,7 @@ void sketch_factors(int64_t d, int64_t ell, uint64_t seed, double* u, double* v)
     }
 }
 
-void sketch_factors(int64_t d, int64_t ell, uint64_t seed, std::vector<double>& u,
-                    std::vector<double>& v) {
+void sketch_factors(int64_t d, int64_t ell, uint64_t seed, HostFactors& u, HostFactors& v) {
     u.resize(static_cast<size_t>(d * ell));
     v.resize(static_cast<size_t>(d * ell));
     sketch_factors(d, ell, seed, u.data(), v.data());
@@ -416,7 +475,7 @@ __global__ void combine_sketch_kernel(const double* __restrict__ P, int naxes, i
 
 void sketch_fp64(const Context& c, const double* pts, const KeptPoints& kp, const double* w,
                  const AxisSpec& ax, const double* axis_weights, int64_t ell,
-                 const std::vector<double>& u, const std::vector<double>& v, double* Yt,
+                 const HostFactors& u, const HostFactors& v, double* Yt,
                  int64_t ldy, int64_t chunk, cudaStream_t s) {
     const int naxes = ax.naxes;
     const int64_t d = ax.d;
@@ -539,7 +598,7 @@ __global__ void combine_density_kernel(const double* __restrict__ P, const doubl
 // (ell x kp.n, leading dimension kp.n).
 DeviceBuffer<double> sketch_density_fp64(const Context& c, const double* pts, KeptPoints& kp,
                                          const double* importance, int64_t ell,
-                                         const std::vector<double>& u, const std::vector<double>& v,
+                                         const HostFactors& u, const HostFactors& v,
                                          bool normalized, double threshold, int64_t chunk,
                                          cudaStream_t s) {
     const int nao = c.nao;
@@ -670,7 +729,7 @@ __global__ void factors_transpose_kernel(const double* __restrict__ u, const dou
 
 MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& kp, const double* w,
                          const AxisSpec& ax, const double* axis_weights, int64_t ell,
-                         const std::vector<double>& u, const std::vector<double>& v, double* Yt,
+                         const HostFactors& u, const HostFactors& v, double* Yt,
                          int64_t ldy, cudaStream_t s, RetainedAo* keep) {
     MixedSketch ms;
     const int nao = c.nao;
@@ -879,7 +938,7 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
     // count only through the ILP64 limit: when the requested ell is within the
     // limit for the whole grid it is the final one, so the factors are drawn on
     // a host thread while the device compacts the points.
-    std::vector<double> u, v;
+    HostFactors u, v;
     const int64_t d_pre = static_cast<int64_t>(o.axes.size()) * c.nao;
     const int64_t ell_req = o.max_rank ? o.max_rank + o.oversampling : o.sketch_size;
     int64_t ell_pre = -1;
@@ -1077,7 +1136,7 @@ std::vector<int64_t> select_sketch_gathered(const Context& c, const SelectOption
     SketchQR qr;
     if (delta && su.mixed) {
         // FP64 re-verification source over the gathered kept points
-        std::vector<double> u, v;
+        HostFactors u, v;
         sketch_factors(su.d, su.ell, o.seed, u, v);
         const int64_t d = su.d, nout = 2 * su.ell;
         std::vector<double> hwt(static_cast<size_t>(d * nout));
