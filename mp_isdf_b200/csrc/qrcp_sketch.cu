@@ -20,6 +20,7 @@
 #include "isdf_select.h"
 
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 
 namespace isdf {
@@ -158,6 +159,108 @@ __global__ void __launch_bounds__(kQrThreads) qr_update_kernel(QrState st, int64
     if (tid == 0) {
         double et = 0, lt = 0.0;
         for (int i = 0; i < kQrThreads / 32; ++i) { et += esh[i]; lt = fmax(lt, lsh[i]); }
+        if (j > 0 && et != 0.0) atomicAdd(&st.energy[j - 1], et);
+        if (!verified) st.partial[blockIdx.x] = best;
+        else if (lt > 0.0) atomicMax(st.lb_bits, static_cast<unsigned long long>(__double_as_longlong(lt)));
+    }
+}
+
+// Paired form of the staged update, for an even leading dimension and 16-byte
+// aligned rows: a thread takes two adjacent columns, copies each touched row
+// pair with one 16-byte cp.async and stores an updated pair with one 16-byte
+// store, halving the copy and store instructions; each column's arithmetic is
+// that of qr_update_kernel<true>, and a block still covers kQrThreads columns
+// (one argmax key per block, as the pivot kernel expects).
+constexpr int kPairThreads = kQrThreads / 2;
+__global__ void __launch_bounds__(kPairThreads) qr_update_pairs_kernel(QrState st, int64_t j) {
+    __shared__ ArgKey ksh[kPairThreads / 32];
+    __shared__ double esh[kPairThreads / 32];
+    __shared__ double lsh[kPairThreads / 32];
+    __shared__ double vsh[kRegRows];
+    extern __shared__ __align__(16) double xs[];   // [rows][kQrThreads], columns 2 tid and 2 tid + 1
+    const int tid = threadIdx.x;
+    const int64_t g0 = static_cast<int64_t>(blockIdx.x) * kQrThreads + 2 * tid;
+    const bool verified = st.est != nullptr;
+    const int64_t m = st.m, ld = st.ldy;
+    const int64_t r0 = j > 0 ? j - 1 : 0;   // first row touched
+    const int cnt = static_cast<int>(m - r0);
+    bool act[2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) act[c] = g0 + c < st.n && !st.selected[g0 + c];
+    if (act[0] || act[1]) {
+        const bool both = g0 + 1 < st.n;
+        const double* src = st.Yt + r0 * ld + g0;
+        for (int i = 0; i < cnt; ++i, src += ld) {
+            const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(&xs[i * kQrThreads + 2 * tid]));
+            if (both) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+            else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    if (j > 0 && tid < cnt) vsh[tid] = st.vhist[(j - 1) * m + r0 + tid];
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    ArgKey key = key_none();
+    double e = 0.0, lb = 0.0;
+    if (act[0] || act[1]) {
+        const double t = j > 0 ? st.tau[j - 1] : 0.0;
+        const double* x = xs + 2 * tid;
+        double dot[2] = {0.0, 0.0}, nrm[2] = {0.0, 0.0};
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+            if (act[c] && t != 0.0) {
+                double d = 0;
+                for (int i = 0; i < cnt; ++i) d += vsh[i] * x[i * kQrThreads + c];
+                dot[c] = d * t;
+            }
+        if (j > 0) {
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+                if (act[c]) {
+                    const double x0 = x[c] - vsh[0] * dot[c];
+                    e += x0 * x0;
+                }
+        }
+        double* dst = st.Yt + j * ld + g0;
+        for (int i = j > 0 ? 1 : 0; i < cnt; ++i, dst += ld) {
+            double x0 = x[i * kQrThreads], x1 = x[i * kQrThreads + 1];
+            if (t != 0.0) {
+                x0 -= vsh[i] * dot[0];
+                x1 -= vsh[i] * dot[1];
+                if (act[0] && act[1]) {
+                    *reinterpret_cast<double2*>(dst) = make_double2(x0, x1);
+                } else {
+                    if (act[0]) dst[0] = x0;
+                    if (act[1]) dst[1] = x1;
+                }
+            }
+            nrm[0] += x0 * x0;
+            nrm[1] += x1 * x1;
+        }
+        if (j < m) {
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                if (!act[c]) continue;
+                const int64_t g = g0 + c;
+                if (verified) {
+                    st.est[g] = nrm[c];
+                    lb = fmax(lb, fmax(sqrt(nrm[c]) - st.delta[g], 0.0));
+                } else {
+                    const ArgKey k{nrm[c], st.pos[g], g};
+                    if (key_better(k, key)) key = k;
+                }
+            }
+        }
+    }
+    e = warp_sum(e);
+    lb = warp_max(lb);
+    if (tid % 32 == 0) { esh[tid / 32] = e; lsh[tid / 32] = lb; }
+    ArgKey best = key_none();
+    if (!verified) best = block_best<kPairThreads>(key, ksh);
+    else __syncthreads();
+    if (tid == 0) {
+        double et = 0, lt = 0.0;
+        for (int i = 0; i < kPairThreads / 32; ++i) { et += esh[i]; lt = fmax(lt, lsh[i]); }
         if (j > 0 && et != 0.0) atomicAdd(&st.energy[j - 1], et);
         if (!verified) st.partial[blockIdx.x] = best;
         else if (lt > 0.0) atomicMax(st.lb_bits, static_cast<unsigned long long>(__double_as_longlong(lt)));
@@ -486,15 +589,21 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
     constexpr size_t kStagedBytes = static_cast<size_t>(kRegRows) * kQrThreads * sizeof(double);
     ISDF_CUDA(cudaFuncSetAttribute(qr_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kStagedBytes)));
+    ISDF_CUDA(cudaFuncSetAttribute(qr_update_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kStagedBytes)));
+    // two columns per thread where every row of the pairs is 16-byte aligned
+    const bool pairs = st.ldy % 2 == 0 && reinterpret_cast<uintptr_t>(st.Yt) % 16 == 0;
     for (int64_t j = 0; j <= steps; ++j) {
         {
             ISDF_PROFILE("qrcp_sketch_update", s);
             const int64_t touched = m - (j > 0 ? j - 1 : 0);
             // shared memory for the rows this step stages only: later steps
             // (fewer rows) keep more blocks, and more copies in flight, per SM
-            if (touched <= kRegRows)
-                qr_update_kernel<true><<<nblocks, kQrThreads,
-                                         static_cast<size_t>(touched) * kQrThreads * sizeof(double), s>>>(st, j);
+            const size_t staged = static_cast<size_t>(touched) * kQrThreads * sizeof(double);
+            if (touched <= kRegRows && pairs)
+                qr_update_pairs_kernel<<<nblocks, kPairThreads, staged, s>>>(st, j);
+            else if (touched <= kRegRows)
+                qr_update_kernel<true><<<nblocks, kQrThreads, staged, s>>>(st, j);
             else
                 qr_update_kernel<false><<<nblocks, kQrThreads, 0, s>>>(st, j);
             ISDF_LAUNCH_CHECK();

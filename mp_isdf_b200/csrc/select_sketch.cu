@@ -996,8 +996,10 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
         fill_diag(diag_out, ell, r, qr);
         return selected;
     }
-    const int64_t ldy = n;
-    DeviceBuffer<double> Yt(static_cast<size_t>(ell * n), s);
+    // an even row stride keeps every row 16-byte aligned for the QR update's
+    // paired copies (the padding column is never read)
+    const int64_t ldy = n + (n & 1);
+    DeviceBuffer<double> Yt(static_cast<size_t>(ell * ldy), s);
     if (su.mixed) {
         MixedSketch ms = sketch_mixed(c, pts, kp, w, ax, aw, ell, u, v, Yt.get(), ldy, s, keep);
         ISDF_PROFILE("phase:qrcp", s);
