@@ -179,7 +179,7 @@ def k_chunks(mol):
     return chunks + (1 if used or not chunks else 0)
 
 
-def algorithmic(family, cfg, mol, n_kept, naxes, ell, k):
+def algorithmic(family, cfg, mol, n_kept, naxes, ell, k, precision="fp64"):
     """(bound, units per kernel family over one step, unit).  Bytes are the
     minimal HBM traffic of the family's outputs/inputs; flops are 2*M*N*K."""
     nao = mol.nao
@@ -189,7 +189,11 @@ def algorithmic(family, cfg, mol, n_kept, naxes, ell, k):
         return "hbm", n_kept * d * s + n_kept * 24, "bytes"
     if family.startswith("ao_eval"):
         s = 8 if family.endswith("f64") else 4
-        return "hbm", (n_kept + k) * nao * s + n_kept * 24, "bytes"
+        if precision == "mixed":
+            # the mixed step evaluates FP64 AO values at the k anchors only
+            return "hbm", k * nao * s + k * 24, "bytes"
+        # FP64 step: the fit's AO values of every kept point and the anchors'
+        return "hbm", (n_kept + k) * nao * s + (n_kept + k) * 24, "bytes"
     if family == "gemm_f64":
         # sketch projection (reads F once) + fit Gram (reads Phi once)
         return "hbm", n_kept * d * 8 + n_kept * nao * 8, "bytes"
@@ -198,6 +202,10 @@ def algorithmic(family, cfg, mol, n_kept, naxes, ell, k):
     if family.startswith("qrcp_sketch_update"):
         return "hbm", sum(2 * (ell - j + 1) * n_kept * 8 for j in range(ell + 1)), "bytes"
     if family == "sketch_combine":
+        if precision == "mixed":
+            # FP32 projections + 4 FP32 squared norms in, FP64 sketch column
+            # and its error bound out
+            return "hbm", n_kept * (naxes * 2 * ell * 4 + 16 + ell * 8 + 8), "bytes"
         return "hbm", n_kept * (naxes * 2 * ell + ell) * 8, "bytes"
     if family == "gram_tiles":
         # stored split-BF16 AO tiles read once, G written once
@@ -373,6 +381,40 @@ def time_widened(ctx, mol, x, wt, w, theta, k, n_kept, cfg):
     }
 
 
+def golden_compare(cfg_key, piv, theta, n_kept, k, pair_rel):
+    """This form's anchors, Theta and pair error against the FP64 oracle's
+    golden fixture of the configuration (tests/golden/<key>.npz, written by
+    tests/golden/make_goldens.py): Theta at the fixture's sample of columns,
+    relative to its largest entry, and the pair error relative to the
+    oracle's.  None for reduced grids or configurations without a fixture."""
+    path = ROOT / "tests" / "golden" / f"{cfg_key}.npz"
+    if MAX_POINTS or not path.exists():
+        return None
+    g = np.load(path)
+    ref = [int(a) for a in g["anchors"]]
+    gold = float(g["pair_relative"])
+    out = {"fixture": f"tests/golden/{cfg_key}.npz", "oracle_pair_relative": gold,
+           "oracle_condition": float(g["condition"]), "oracle_min_step_gap": float(np.min(g["step_gap"]))}
+    div = next((j for j, (a, b) in enumerate(zip(piv, ref)) if a != b), None)
+    if div is None and len(piv) != len(ref):
+        div = min(len(piv), len(ref))
+    out["anchors_equal_oracle"] = div is None
+    if div is not None:
+        out["first_divergent_pivot"] = div
+        out["oracle_gap_at_divergence"] = float(g["step_gap"][div]) if div < len(g["step_gap"]) else None
+        out["theta_rel_err_vs_oracle"] = None
+        out["pair_rel_err_vs_oracle"] = None
+        return out
+    import torch
+    pos = torch.as_tensor(g["theta_pos"], device=theta.device)
+    th = theta[: k * n_kept].view(k, n_kept)[:, pos].cpu().numpy()
+    sample = g["theta_sample"]
+    out["theta_rel_err_vs_oracle"] = float(np.abs(th - sample).max() / np.abs(sample).max())
+    out["theta_columns_compared"] = int(sample.shape[1])
+    out["pair_rel_err_vs_oracle"] = abs(pair_rel - gold) / gold
+    return out
+
+
 def selection_kwargs(cfg, names, factors, precision):
     """isdf_select arguments of a config (algorithm, axes, rank, sketch)."""
     return dict(algorithm=cfg["algorithm"], axes=names, axis_weights=factors, max_rank=cfg["rank"],
@@ -384,7 +426,7 @@ def cpu_sample_size(cfg, mol, names):
     """Sample size of the CPU restatement run and whether it fits the host:
     dense pair QR materialises d^2 x n doubles as the reference does."""
     if cfg["algorithm"] == "rand_sketch":
-        return 3000, True
+        return 32768, True
     d2 = (len(names) * mol.nao) ** 2
     n = 1000
     return n, d2 * n * 8 <= 2e9
@@ -440,7 +482,7 @@ def run_reference(args, rank, world):
         v, cores, sample = cpu_sample(mol, pts, w, names, factors, cfg, n_sample=n_sample, seed=i)
         if i >= args.warmup:
             vals.append(v)
-    value = statistics.mean(vals)
+    value = statistics.median(vals)
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
@@ -448,7 +490,10 @@ def run_reference(args, rank, world):
         "impl": "reference",
         "config": workload_desc(args.config, cfg, mol, pts, w, names, precision),
         "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port",
-                         "sample": sample},
+                         "sample": sample + f"; median of {len(vals)} samples (seeds "
+                                            f"{args.warmup}..{args.warmup + len(vals) - 1})",
+                         "min": min(vals), "max": max(vals),
+                         "spread": (max(vals) - min(vals)) / value},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference CMake build needs network FetchContent (Kokkos, LAPACK++, SLATE, "
                 "libcint, MAGMA); timed is the C++/OpenMP restatement of its algorithm in oracle/",
@@ -547,7 +592,9 @@ def run_ours(args, rank, world, local_rank):
         else:
             pl2, prel = ctx.pair_error(x, wt, piv, theta)
         einfo = {"pair_l2": pl2, "pair_relative": prel, "fit_path": finfo.fit_path,
-                 "mixed_bound": finfo.mixed_bound}
+                 "mixed_bound": finfo.mixed_bound,
+                 "vs_oracle": golden_compare(args.config, [int(p) for p in piv], theta, n_kept, k, prel)
+                 if not sharded else None}
         torch.cuda.synchronize()
         results[precision] = dict(total=total, times=times, prof=prof, phases=phases, step_phases=step_phases,
                                   launches=launched / max(args.steps, 1),
@@ -638,7 +685,9 @@ def run_ours(args, rank, world, local_rank):
             useful = 2.0 * n_kept * len(names) * mol.nao * 2 * ell
             issued = 2.0 * n_kept * len(names) * nao_pad * nt * 3
             entry["roofline"] = {
-                "bound": "hbm", "achieved": units / t_launch / 1e9, "peak": hbm, "unit": "GB/s",
+                "bound": "hbm", "limiter": "instruction issue (ncu: ALU/FMA/LSU pipes, long-scoreboard and "
+                                          "barrier stalls), not DRAM or the tensor pipe",
+                "achieved": units / t_launch / 1e9, "peak": hbm, "unit": "GB/s",
                 "frac": units / t_launch / 1e9 / hbm, "algorithmic_bytes_per_launch": units,
                 "algorithmic_model": f"n_kept*nao*{ncomp} components*4 B (unfused AO output) + n_kept*24 B",
                 "traffic": MEASURED_TRAFFIC_PER_POINT[name] * n_kept,
@@ -648,7 +697,7 @@ def run_ours(args, rank, world, local_rank):
                            "issued_frac_of_bf16": issued / t_launch / 1e12 / bf16,
                            "issued_model": "3 split-BF16 products x 2*n*(naxes*K_slots)*N_tile"}}
         else:
-            bound, units, unit = algorithmic(name, cfg, mol, n_kept, len(names), ell, k)
+            bound, units, unit = algorithmic(name, cfg, mol, n_kept, len(names), ell, k, head)
             if units:
                 ach, pk, u = ((units / t_launch / 1e9, hbm, "GB/s") if bound == "hbm"
                               else (units / t_launch / 1e12, bf16, "TFLOP/s"))
@@ -666,8 +715,14 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_cpu and world == 1:
         n_sample, feasible = cpu_sample_size(cfg, mol, names)
         if feasible:
-            v, cores, sample = cpu_sample(mol, pts, w, names, factors, cfg, n_sample=n_sample)
-            cpu = {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": sample}
+            vals = []
+            for seed in range(3):
+                v, cores, sample = cpu_sample(mol, pts, w, names, factors, cfg, n_sample=n_sample, seed=seed)
+                vals.append(v)
+            med = statistics.median(vals)
+            cpu = {"value": med, "unit": "s", "cores": cores, "kind": "port",
+                   "sample": sample + "; median of 3 samples (seeds 0..2)",
+                   "min": min(vals), "max": max(vals), "spread": (max(vals) - min(vals)) / med}
         else:
             cpu = {"value": None, "unit": "s", "cores": None, "kind": "port",
                    "sample": "infeasible: the reference's explicit d^2 x n pair matrix does not fit host memory"}
@@ -677,7 +732,9 @@ def run_ours(args, rank, world, local_rank):
                         "step_times_s": r["times"], "anchors": r["piv"],
                         "pair_relative": r["einfo"]["pair_relative"], "pair_l2": r["einfo"]["pair_l2"],
                         "fit_path": r["einfo"]["fit_path"], "mixed_fit_bound": r["einfo"]["mixed_bound"],
+                        "vs_oracle": r["einfo"]["vs_oracle"],
                         "sketch_columns_reverified": r["sinfo"].verifications,
+                        "precision_used": "mixed" if r["sinfo"].precision_used else "fp64",
                         "phases_ms_per_step": {k: v[0] / args.steps for k, v in r["phases"].items()},
                         "phases_ms_each_step": r["step_phases"],
                         "clocks": r["clocks"]}
@@ -697,6 +754,8 @@ def run_ours(args, rank, world, local_rank):
         | {"parallelism": (f"grid shards x{world} (one cluster)" if sharded else f"replicas x{world}")},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": res["clocks"], "kernels": kernels, "forms": forms_out, **extra,
+        "theta_rel_err_vs_oracle": (res["einfo"]["vs_oracle"] or {}).get("theta_rel_err_vs_oracle"),
+        "pair_rel_err_vs_oracle": (res["einfo"]["vs_oracle"] or {}).get("pair_rel_err_vs_oracle"),
         "adjoint": adjoint, "ao_eval": ao_eval,
     }
     if widened is not None:

@@ -138,6 +138,11 @@ typedef struct isdf_select_info {
     int64_t verifications;       /* exact recomputations (pair QR: winners; mixed sketch: candidates) */
     int64_t reselections;
     double relative_residual;    /* sketch tail / pair-QR last |R_jj| / |R_00| */
+    int64_t precision_used;      /* form that ran: 0 FP64, 1 mixed.  A mixed request runs the
+                                  * FP64 form (and reports 0 here) for the pair-QR algorithms,
+                                  * the density sketches, an OccupiedOrbital axis, more AOs than
+                                  * the FP64 re-verification holds, or projections wider than
+                                  * the tensor-core kernel's accumulators */
 } isdf_select_info;
 
 void isdf_select_args_default(isdf_select_args* args);
@@ -248,7 +253,11 @@ int isdf_pair_error_terms(int64_t n, int64_t k, const double* q_dev, const doubl
  * Limits: k <= 64 anchors (larger k returns ISDF_ERR_INVALID); any n.  All
  * calls share that array, so calls whose GPU work overlaps race; serialise
  * them.  The first call on a device looks up the array's address once for
- * that device; make it before any stream capture. */
+ * that device; make it before any stream capture.  The address is kept until
+ * exit, so the entry point must not be used on a device after
+ * cudaDeviceReset.  Each call waits for its stream before returning (the two
+ * sums are copied to out_host).  Null q/w (n > 0) or H/X/M (n > 0, k > 0)
+ * return ISDF_ERR_INVALID before any launch. */
 int isdf_pair_error_terms_noalloc(int64_t n, int64_t k, const double* q_dev, const double* H_dev,
                                   const double* X_dev, const double* M_dev, const double* w_dev,
                                   double* out_host, void* stream);
@@ -259,7 +268,8 @@ int isdf_pair_error_terms_noalloc(int64_t n, int64_t k, const double* q_dev, con
  * rho_a(k) = phi(a_k)^T D phi(a_k), with grid, anchors (original grid
  * indices) and weights held fixed; grad_host receives dE/dR (natm x 3, bohr).
  * dm_host: AO density matrix (nao x nao, row-major).  AO values/gradients are
- * recomputed per grid chunk (FP64). */
+ * recomputed per grid chunk (FP64).  grad_host = NULL computes the energy
+ * alone (AO values only; no gradient sweep). */
 int isdf_energy_gradient(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t ng,
                          const int64_t* anchors_host, int64_t k, const double* dm_host,
                          double* energy, double* grad_host, void* stream);

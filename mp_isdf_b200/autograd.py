@@ -1,7 +1,9 @@
 """torch.autograd.Function for the nuclear gradient of the ISDF density
 functional E = sum_g w_g rho_ISDF(g)^2 (grid points, anchors and weights held
-fixed).  Forward and backward both run the B200 adjoint through the C-ABI
-(`isdf_energy_gradient`); there is no CPU path.
+fixed).  Forward runs the B200 adjoint through the C-ABI
+(`isdf_energy_gradient`); when the coordinates do not require a gradient it
+asks for the energy alone, which skips the gradient sweep.  There is no CPU
+path.
 """
 from __future__ import annotations
 
@@ -17,8 +19,11 @@ class IsdfEnergy(torch.autograd.Function):
     @staticmethod
     def forward(ctx_, coords, context, xyz, w, anchors, dm):
         context.set_coords(coords.detach().cpu().numpy())
-        e, g = context.energy_gradient(xyz, w, anchors, dm)
-        ctx_.save_for_backward(torch.as_tensor(g, dtype=coords.dtype, device=coords.device))
+        if ctx_.needs_input_grad[0]:
+            e, g = context.energy_gradient(xyz, w, anchors, dm)
+            ctx_.save_for_backward(torch.as_tensor(g, dtype=coords.dtype, device=coords.device))
+        else:
+            e = context.energy(xyz, w, anchors, dm)
         return torch.tensor(e, dtype=coords.dtype, device=coords.device)
 
     @staticmethod

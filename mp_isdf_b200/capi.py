@@ -56,7 +56,8 @@ class RbrpArgs(ctypes.Structure):
 
 class SelectInfo(ctypes.Structure):
     _fields_ = [("n_kept", I64), ("sketch_rows", I64), ("numerical_rank", I64),
-                ("verifications", I64), ("reselections", I64), ("relative_residual", F64)]
+                ("verifications", I64), ("reselections", I64), ("relative_residual", F64),
+                ("precision_used", I64)]
 
 
 class FitInfo(ctypes.Structure):
@@ -361,6 +362,15 @@ class Context:
         check(lib().isdf_energy_gradient(self.h, _ptr(xyz), _ptr(w), xyz.shape[0], _ptr(a), len(a),
                                          _ptr(d), ctypes.byref(e), _ptr(g), _stream(xyz)))
         return e.value, g
+
+    def energy(self, xyz, w, anchors, dm):
+        """E = sum_g w_g rho_ISDF(g)^2 alone (no gradient sweep), device tensors."""
+        a = _np(anchors, np.int64)
+        d = _np(dm, np.float64)
+        e = F64()
+        check(lib().isdf_energy_gradient(self.h, _ptr(xyz), _ptr(w), xyz.shape[0], _ptr(a), len(a),
+                                         _ptr(d), ctypes.byref(e), None, _stream(xyz)))
+        return e.value
 
     # ---- host arrays -----------------------------------------------------------
     def eval_ao_host(self, xyz, gradient=False):

@@ -212,7 +212,8 @@ struct GradSink {
     }
 };
 
-template <int LMAX, int KMAX>
+// GRAD = false: the energy alone (sweep 1 only).
+template <int LMAX, int KMAX, bool GRAD>
 __global__ void __launch_bounds__(kAdjPts * kAdjLanes, 1) adjoint_grid_kernel(AdjGridArgs args) {
     extern __shared__ double adj_smem[];
     double* Gs = adj_smem;                                   // [lanes][pts][KMAX]
@@ -266,6 +267,7 @@ __global__ void __launch_bounds__(kAdjPts * kAdjLanes, 1) adjoint_grid_kernel(Ad
             if (lane == 0) atomicAdd(e_s, e);
         }
         __syncthreads();
+        if constexpr (!GRAD) continue;
         // sweep 2: values and gradients; per shell, the warp's 32 points are
         // reduced before one shared-memory add per component
         GradSink<KMAX> gr{args.phia, args.dphia, args.nao, {}, 0.0, {0.0, 0.0, 0.0}};
@@ -290,9 +292,9 @@ __global__ void __launch_bounds__(kAdjPts * kAdjLanes, 1) adjoint_grid_kernel(Ad
 }
 
 template <int LMAX, int KMAX>
-void launch_adjoint_grid(const AdjGridArgs& a, cudaStream_t s) {
+void launch_adjoint_grid(const AdjGridArgs& a, bool grad, cudaStream_t s) {
     const size_t smem = (static_cast<size_t>(kAdjLanes + 1) * kAdjPts * KMAX + 3 * a.natm + KMAX + 1) * sizeof(double);
-    auto kern = adjoint_grid_kernel<LMAX, KMAX>;
+    auto kern = grad ? adjoint_grid_kernel<LMAX, KMAX, true> : adjoint_grid_kernel<LMAX, KMAX, false>;
     ISDF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     int dev = 0, nsm = 148;
     ISDF_CUDA(cudaGetDevice(&dev));
@@ -335,7 +337,7 @@ void set_atom_coords(Context& c, const double* coords) {
 
 AdjointResult energy_gradient(const Context& c, const double* pts, const double* w,
                               const KeptPoints& kp, const AnchorFactor& f, const double* dm,
-                              cudaStream_t s) {
+                              bool want_grad, cudaStream_t s) {
     AdjointResult r;
     const int64_t n = kp.n, k = f.k, nao = c.nao;
     r.grad.assign(static_cast<size_t>(c.natm) * 3, 0.0);
@@ -349,10 +351,8 @@ AdjointResult energy_gradient(const Context& c, const double* pts, const double*
         acc(static_cast<size_t>(3 * nao), s), energy(1, s);
     ISDF_CUDA(cudaMemcpyAsync(Dd.get(), dm, nao * nao * sizeof(double), cudaMemcpyHostToDevice, s));
     v.zero(s); B.zero(s); acc.zero(s); energy.zero(s);
-    {
-        // anchor AO gradients (anchor coordinates gathered by the caller into f)
+    if (want_grad)   // anchor AO gradients (anchor coordinates gathered by the caller into f)
         eval_ao<double>(c, f.anchor_pts.get(), k, nullptr, dphia.get(), nao, s);
-    }
     gemm_f64(k, nao, nao, f.phi_a.get(), nao, 0, Dd.get(), nao, 0, PhiD.get(), nao, 0, 1, false, s);
     rho_anchor_kernel<<<static_cast<unsigned>(k), 32, 0, s>>>(static_cast<int>(k), static_cast<int>(nao),
                                                                 PhiD.get(), f.phi_a.get(), rhoa.get());
@@ -383,13 +383,13 @@ AdjointResult energy_gradient(const Context& c, const double* pts, const double*
                       kp.index.get(), n, phia_pad.get(), dphia_pad.get(), z_pad.get(), gacc.get(), v.get(),
                       energy.get()};
         if (c.lmax <= 2) {
-            if (kmax == 8) launch_adjoint_grid<2, 8>(a, s);
-            else if (kmax == 16) launch_adjoint_grid<2, 16>(a, s);
-            else launch_adjoint_grid<2, 32>(a, s);
+            if (kmax == 8) launch_adjoint_grid<2, 8>(a, want_grad, s);
+            else if (kmax == 16) launch_adjoint_grid<2, 16>(a, want_grad, s);
+            else launch_adjoint_grid<2, 32>(a, want_grad, s);
         } else {
-            if (kmax == 8) launch_adjoint_grid<kMaxL, 8>(a, s);
-            else if (kmax == 16) launch_adjoint_grid<kMaxL, 16>(a, s);
-            else launch_adjoint_grid<kMaxL, 32>(a, s);
+            if (kmax == 8) launch_adjoint_grid<kMaxL, 8>(a, want_grad, s);
+            else if (kmax == 16) launch_adjoint_grid<kMaxL, 16>(a, want_grad, s);
+            else launch_adjoint_grid<kMaxL, 32>(a, want_grad, s);
         }
     }
     // otherwise the grid pass in chunks: AO values + gradients recomputed per chunk
@@ -403,17 +403,23 @@ AdjointResult energy_gradient(const Context& c, const double* pts, const double*
         ISDF_PROFILE("adjoint_grid", s);
         gather_kernel<<<nblk(b), 256, 0, s>>>(pts, w, kp.index.get() + g0, b, cp.get(), cw.get());
         ISDF_LAUNCH_CHECK();
-        eval_ao<double>(c, cp.get(), b, phi.get(), dphi.get(), nao, s);
+        eval_ao<double>(c, cp.get(), b, phi.get(), want_grad ? dphi.get() : nullptr, nao, s);
         gemm_f64(b, k, nao, phi.get(), nao, 0, f.phi_aT.get(), k, 0, G.get(), k, 0, 1, false, s);
         adjoint_point_kernel<<<nblk(b), 256, 0, s>>>(G.get(), cw.get(), b, static_cast<int>(k), z.get(),
                                                      alpha.get(), alphaT.get(), v.get(), energy.get());
         ISDF_LAUNCH_CHECK();
+        if (!want_grad) continue;
         // B += alpha^T Phi_chunk ; beta = alpha Phi_a
         gemm_f64(k, nao, b, alphaT.get(), b, 0, phi.get(), nao, 0, B.get(), nao, 0, 1, true, s);
         gemm_f64(b, nao, k, alpha.get(), k, 0, f.phi_a.get(), nao, 0, beta.get(), nao, 0, 1, false, s);
         dim3 cg(static_cast<unsigned>((nao + 255) / 256), 3);
         column_dot_kernel<<<cg, 256, 0, s>>>(beta.get(), dphi.get(), b, static_cast<int>(nao), acc.get());
         ISDF_LAUNCH_CHECK();
+    }
+    if (!want_grad) {
+        ISDF_CUDA(cudaMemcpyAsync(&r.energy, energy.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        return r;
     }
     // anchor terms
     anchor_terms_kernel<<<1, 256, 0, s>>>(static_cast<int>(k), static_cast<int>(nao), f.phi_a.get(), S.get(),

@@ -312,6 +312,7 @@ std::vector<int64_t> select_impl(isdf_ctx* ctx, const isdf_select_args* args, co
             info->numerical_rank = d.numerical_rank;
             info->relative_residual = d.relative_tail;
             info->verifications = d.reverified;
+            info->precision_used = d.precision_used;
         }
         if (o.debug)
             std::fprintf(stderr,
@@ -629,7 +630,7 @@ int isdf_energy_gradient(isdf_ctx* ctx, const double* xyz, const double* w, int6
         ISDF_PROFILE("phase:factor_anchors", s);
         f = isdf::factor_anchors(c, apts.get(), aw.get(), k, s);
     }
-        isdf::AdjointResult r = isdf::energy_gradient(c, xyz, w, kp, f, dm, s);
+        isdf::AdjointResult r = isdf::energy_gradient(c, xyz, w, kp, f, dm, grad != nullptr, s);
         if (energy) *energy = r.energy;
         if (grad) std::memcpy(grad, r.grad.data(), r.grad.size() * sizeof(double));
     });
@@ -861,6 +862,8 @@ int isdf_pair_error_terms(int64_t n, int64_t k, const double* q, const double* H
                           const double* M, const double* w, double* out, void* stream) {
     return guarded([&] {
         if (n < 0 || k < 0 || !out) isdf::fail(isdf::kInvalid, "invalid pair error terms");
+        if (n > 0 && (!q || !w || (k > 0 && (!H || !X || !M))))
+            isdf::fail(isdf::kInvalid, "null pair error term array");
         double acc[2] = {0, 0};
         if (n > 0) isdf::pair_error_terms(n, k, q, H, X, M, w, acc, as_stream(stream));
         const double a = std::sqrt(std::max(acc[0], 0.0));
@@ -938,6 +941,7 @@ int isdf_sketch_select_gathered(isdf_ctx* ctx, const isdf_select_args* args, dou
             info->numerical_rank = d.numerical_rank;
             info->relative_residual = d.relative_tail;
             info->verifications = d.reverified;
+            info->precision_used = d.precision_used;
         }
         if (static_cast<int64_t>(out.size()) > capacity) isdf::fail(isdf::kInvalid, "pivot buffer is too small");
         if (!out.empty()) std::memcpy(pivots, out.data(), out.size() * sizeof(int64_t));

@@ -12,9 +12,10 @@ struct AdjointResult {
 
 // E = sum_g w_g rho_ISDF(g)^2 and dE/dR over the kept points, for the anchors
 // factored in `f` and the AO density matrix `dm_host` (nao x nao, row-major).
+// want_grad = false computes E alone (AO values only, no gradient sweep).
 AdjointResult energy_gradient(const Context& c, const double* pts, const double* w,
                               const KeptPoints& kp, const AnchorFactor& f, const double* dm_host,
-                              cudaStream_t s);
+                              bool want_grad, cudaStream_t s);
 
 // Moves the atoms (and their shells) to new coordinates (natm x 3, bohr).
 void set_atom_coords(Context& c, const double* coords_host);

@@ -47,6 +47,7 @@ struct SketchDiagnostics {
     int64_t ell = 0, numerical_rank = 0, cap = 0, rank = 0;
     double relative_tail = 0;
     int64_t reverified = 0;          // mixed path: candidates recomputed in FP64
+    int64_t precision_used = 0;      // form that ran: 0 FP64, 1 mixed
     std::vector<double> diag, tails;
 };
 

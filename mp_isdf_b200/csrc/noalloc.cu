@@ -15,7 +15,12 @@
 //     streams, or two host threads) race on it; serialise them.
 //   * The first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current); make
-//     that first call before any stream capture.
+//     that first call before any stream capture.  The address is kept for the
+//     life of the process: after cudaDeviceReset on a device the library's
+//     module is loaded again and the kept address is stale, so do not call
+//     this entry point on a device after resetting it.
+//   * Each call copies the two sums to host memory and waits for its stream
+//     to finish before returning.
 #include "../../include/isdf_b200.h"
 #include "isdf_internal.h"
 #include "isdf_reduce.cuh"
@@ -112,6 +117,8 @@ extern "C" int isdf_pair_error_terms_noalloc(int64_t n, int64_t k, const double*
         if (n < 0 || k < 0 || !out) isdf::fail(isdf::kInvalid, "invalid pair error terms");
         if (k > isdf::kNoAllocMaxAnchors)
             isdf::fail(isdf::kInvalid, "isdf_pair_error_terms_noalloc supports at most 64 anchors");
+        if (n > 0 && (!q || !w || (k > 0 && (!H || !X || !M))))
+            isdf::fail(isdf::kInvalid, "null pair error term array");
         double acc[2] = {0, 0};
         if (n > 0) {
             cudaStream_t s = static_cast<cudaStream_t>(stream);

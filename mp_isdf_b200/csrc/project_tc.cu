@@ -510,7 +510,7 @@ ProjectPlan make_project_plan(const Context& c, const std::vector<int>& axis_com
     const int nax = static_cast<int>(axis_comp.size());
     pl.nax = nax;
     pl.nout = nout;
-    pl.nt = nout <= 16 ? 16 : nout <= 32 ? 32 : 64;
+    pl.nt = nout <= 16 ? 16 : nout <= 32 ? 32 : nout <= 64 ? 64 : 128;
     pl.grad = false;
     pl.comp_mask = 0;
     pl.lmax = c.lmax;
@@ -535,10 +535,12 @@ ProjectPlan make_project_plan(const Context& c, const std::vector<int>& axis_com
     return pl;
 }
 
+// Accumulator widths NT of 16, 32, 64 (up to 4 axis entries) or 128 (up to 3:
+// four 128-column accumulators with gradients exceed the shared-memory plan).
 bool project_tc_supported(int nax, int nout) {
-    if (nax < 1 || nax > 4 || nout < 1 || nout > 64) return false;
-    const int nt = nout <= 16 ? 16 : nout <= 32 ? 32 : 64;
-    return nax * nt <= 256;
+    if (nax < 1 || nax > 4 || nout < 1 || nout > 128) return false;
+    const int nt = nout <= 16 ? 16 : nout <= 32 ? 32 : nout <= 64 ? 64 : 128;
+    return nt < 128 ? nax * nt <= 256 : nax <= 3;
 }
 
 void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, const int64_t* index,
@@ -587,6 +589,8 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     ISDF_TC_CASE(2, 32, true) ISDF_TC_CASE(3, 32, true) ISDF_TC_CASE(4, 32, true)
     ISDF_TC_CASE(2, 16, true) ISDF_TC_CASE(3, 16, true) ISDF_TC_CASE(4, 16, true)
     ISDF_TC_CASE(2, 64, false) ISDF_TC_CASE(2, 32, false) ISDF_TC_CASE(2, 16, false)
+    ISDF_TC_CASE(1, 128, false) ISDF_TC_CASE(1, 128, true) ISDF_TC_CASE(2, 128, false)
+    ISDF_TC_CASE(2, 128, true) ISDF_TC_CASE(3, 128, true)
 #undef ISDF_TC_CASE
     fail(kNotImplemented, "tensor-core projection shape not instantiated");
 }

@@ -1017,6 +1017,7 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
                                   cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaStreamSynchronize(s));
     fill_diag(diag_out, ell, r, qr);
+    if (diag_out) diag_out->precision_used = su.mixed ? 1 : 0;
     if (keep && keep->valid) keep->kp = std::move(kp);
     return selected;
 }
@@ -1169,6 +1170,7 @@ std::vector<int64_t> select_sketch_gathered(const Context& c, const SelectOption
     }
     const SketchRank r = sketch_rank(qr, su.ell, n, o, su.physical_rank);
     fill_diag(diag_out, su.ell, r, qr);
+    if (diag_out) diag_out->precision_used = (delta && su.mixed) ? 1 : 0;
     return std::vector<int64_t>(qr.jpvt.begin(), qr.jpvt.begin() + r.rank);
 }
 

@@ -353,6 +353,139 @@ def select_qrcp_dense(ctx, pts, w, axes, tolerance=1e-10, max_rank=0, scales=Non
     return out
 
 
+def _top_two(res, chosen):
+    """First index of the largest residual norm among unchosen columns, its
+    norm, and the relative gap to the runner-up: (p, r_top, gap)."""
+    r = np.where(chosen, -np.inf, res)
+    p = int(np.argmax(r))                      # first maximum, as idamax
+    top = np.sqrt(max(r[p], 0.0))
+    r[p] = -np.inf
+    second = np.sqrt(max(np.max(r), 0.0)) if np.isfinite(np.max(r)) else 0.0
+    return p, top, ((top - second) / top) if top > 0 else 0.0
+
+
+def pair_qrcp_exact(features, w, steps, chunk=16384):
+    """Truncated column-pivoted QR of the weighted pair columns
+    a_g = sqrt|w_g| f_g (x) f_g with EXACT residual norms at every step.
+
+    This is the greedy rule of LAPACK ``dgeqp3`` that qrcp_dense applies to the
+    explicit d^2 x n pair matrix (``cpp/src/anchor_select_qrcp.cpp:172-223,
+    248-307``) and the max-norm rule of the online selector
+    (``cpp/src/anchor_select_online_qr.cpp:200-358``), for grids whose pair
+    matrix is too large to form.  The orthonormal pair basis is kept as
+    symmetric d x d matrices Q_j (Gram-Schmidt with one re-orthogonalisation),
+    so q_j . a_g = sqrt|w_g| f_g^T Q_j f_g and the squared residual of column g
+    after j steps is |a_g|^2 - sum_i (q_i . a_g)^2.
+
+    Returns (positions, |R_jj|, gaps): gaps[j] is the relative difference of
+    the two largest residual norms at step j -- the quantity that decides
+    whether an implementation's pivot at that step is forced (gap > 1e-10) or
+    a near tie.
+    """
+    F = np.ascontiguousarray(features, dtype=np.float64)
+    n, d = F.shape
+    sw = np.sqrt(np.abs(np.asarray(w, float)))
+    norm2 = (sw * np.einsum("gi,gi->g", F, F)) ** 2
+    coef = np.zeros((n, steps))
+    chosen = np.zeros(n, bool)
+    basis, pos, diag, gaps = [], [], [], []
+    for j in range(min(steps, n)):
+        res = norm2 - np.einsum("gj,gj->g", coef[:, :j], coef[:, :j])
+        p, top, gap = _top_two(res, chosen)
+        if top == 0:
+            break
+        pos.append(p)
+        diag.append(top)
+        gaps.append(gap)
+        v = sw[p] * np.outer(F[p], F[p])
+        for i, Q in enumerate(basis):
+            v -= coef[p, i] * Q
+        for Q in basis:                          # second Gram-Schmidt pass
+            v -= np.sum(Q * v) * Q
+        v /= np.linalg.norm(v)
+        v = 0.5 * (v + v.T)
+        basis.append(v)
+        for s0 in range(0, n, chunk):
+            Fc = F[s0:s0 + chunk]
+            coef[s0:s0 + chunk, j] = sw[s0:s0 + chunk] * np.einsum("gi,gi->g", Fc @ v, Fc)
+        chosen[p] = True
+    return pos, np.array(diag), np.array(gaps)
+
+
+def sketch_qrcp_exact(yt, steps):
+    """Column-pivoted Householder QR of the sketch Y (``yt``: ell x n) with
+    exact trailing column norms at every step: the pivot rule of ``dgeqp3``
+    in ``cpp/src/anchor_select_randomized_id.cpp:320-374`` without its norm
+    downdating.  Returns (positions, |R_jj|, gaps) as ``pair_qrcp_exact``."""
+    A = np.array(yt, dtype=np.float64, copy=True)
+    ell, n = A.shape
+    chosen = np.zeros(n, bool)
+    pos, diag, gaps = [], [], []
+    for j in range(min(steps, ell, n)):
+        sub = A[j:]
+        p, top, gap = _top_two(np.einsum("ij,ij->j", sub, sub), chosen)
+        if top == 0:
+            break
+        pos.append(p)
+        diag.append(top)
+        gaps.append(gap)
+        x = sub[:, p].copy()
+        alpha = -np.copysign(np.linalg.norm(x), x[0])
+        x[0] -= alpha
+        x /= np.linalg.norm(x)
+        sub -= 2.0 * np.outer(x, x @ sub)
+        chosen[p] = True
+    return pos, np.array(diag), np.array(gaps)
+
+
+def physical_fit_svd(phi_a):
+    """SVD of the transposed anchor pair matrix C^T (nao^2 x k),
+    C[k] = phi_a(k) (x) phi_a(k), with the cutoff s > 1e-12 s_0 of
+    ``_physical_pair_refit`` (``python/isdf.py:238-263``): (U, s, Vt) of the
+    retained singular triplets, and the condition number s_0 / s_last."""
+    k, nao = phi_a.shape
+    C = np.einsum("ki,kj->kij", phi_a, phi_a).reshape(k, nao * nao)
+    u, s, vt = np.linalg.svd(C.T, full_matrices=False)
+    keep = s > (1e-12 * s[0] if len(s) else 0)
+    cond = float(s[0] / s[-1]) if len(s) and s[-1] > 0 else float("inf")
+    return u[:, keep], s[keep], vt[keep], cond
+
+
+def physical_fit_columns(u, s, vt, anchor_weights, phi_cols, chunk=512):
+    """Theta columns of ``_physical_pair_refit`` (``python/isdf.py:238-263``),
+    Theta_g = (V S^-1 U^T p_g) / w_anchor with p_g = phi_g (x) phi_g, for the
+    given points' AO values; U^T p_g is formed as phi_g^T U_j phi_g per
+    retained singular vector so that no nao^2-long pair vector is stored."""
+    nao = phi_cols.shape[1]
+    r = u.shape[1]
+    ut_p = np.empty((r, len(phi_cols)))
+    for j in range(r):
+        Uj = u[:, j].reshape(nao, nao)
+        for s0 in range(0, len(phi_cols), chunk):
+            P = phi_cols[s0:s0 + chunk]
+            ut_p[j, s0:s0 + chunk] = np.einsum("gi,gi->g", P @ Uj, P)
+    return (vt.T @ (ut_p / s[:, None])) / np.asarray(anchor_weights, float)[:, None]
+
+
+def physical_pair_error(ctx, coords, weights, phi_a, s, vt):
+    """Pair-space error (``python/isdf.py:154-191``) of the SVD fit in Gram
+    form over all given points: err^2 = sum_g |w_g| (q_g^2 - 2 X_g.h_g +
+    X_g^T M X_g) with h_g = (Phi_a phi_g)^2, q_g = |phi_g|^2,
+    X_g = V S^-2 V^T h_g (= Theta_g * w_anchor), M = (Phi_a Phi_a^T)^2.
+    Returns {"l2", "relative", "err2", "exact2"}."""
+    G, q = ctx.grid_gram(coords, phi_a)
+    H = G * G
+    T = (vt.T / s ** 2) @ vt
+    M = (phi_a @ phi_a.T) ** 2
+    X = H @ T
+    aw = np.abs(np.asarray(weights, float))
+    per = q * q - 2.0 * np.einsum("gk,gk->g", X, H) + np.einsum("gk,gk->g", X @ M, X)
+    err2 = max(float(np.dot(aw, per)), 0.0)
+    exact2 = float(np.dot(aw, q * q))
+    return {"l2": np.sqrt(err2), "relative": np.sqrt(err2 / exact2) if exact2 else 0.0,
+            "err2": err2, "exact2": exact2}
+
+
 def sketch_qr_rank(y, ell, oversampling, tolerance, max_rank, physical_rank):
     """dgeqp3 of the sketch Y (y: [n, ell]) and the rank rule of
     ``anchor_select_randomized_id.cpp:320-374``: (positions 0..n-1, details)."""

@@ -101,3 +101,25 @@ def test_sketch_factors_match_standard_library_streams(d, ell, seed):
     ou, ov = O.sketch_factors(d, ell, seed)
     assert np.array_equal(u, ou)
     assert np.array_equal(v, ov)
+
+
+def test_pair_error_terms_reject_null_arrays_without_gpu():
+    """Both pair-error reductions reject null device arrays with
+    ISDF_ERR_INVALID before any CUDA call (so this runs without a GPU)."""
+    import ctypes
+    from mp_isdf_b200 import capi
+    L = capi.lib()
+    out = np.zeros(2)
+    P = ctypes.c_void_p
+    dummy = np.zeros(16)
+    d = P(dummy.ctypes.data)
+    for fn in (L.isdf_pair_error_terms, L.isdf_pair_error_terms_noalloc):
+        # null q / w with n > 0
+        assert fn(10, 2, None, d, d, d, d, out.ctypes.data_as(P), None) == 1
+        assert fn(10, 2, d, d, d, d, None, out.ctypes.data_as(P), None) == 1
+        # null H / X / M with n > 0 and k > 0
+        assert fn(10, 2, d, None, d, d, d, out.ctypes.data_as(P), None) == 1
+        assert fn(10, 2, d, d, None, d, d, out.ctypes.data_as(P), None) == 1
+        assert fn(10, 2, d, d, d, None, d, out.ctypes.data_as(P), None) == 1
+        # null output
+        assert fn(10, 2, d, d, d, d, d, None, None) == 1

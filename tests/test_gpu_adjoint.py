@@ -66,3 +66,55 @@ def test_autograd_function(system):
     g_ref = O.isdf_energy_gradient(oc, coords, weights, coords[piv], weights[piv], dm)
     np.testing.assert_allclose(R.grad.numpy(), 2.0 * g_ref, rtol=1e-8,
                                atol=1e-9 * np.abs(g_ref).max())
+
+
+# ---- benchmark configurations C4 ((H2O)8) and C5 ((H2O)64) ------------------
+GOLDEN = __import__("pathlib").Path(__file__).resolve().parent / "golden"
+
+
+def _golden_system(key):
+    import torch
+    from mp_isdf_b200 import capi, inputs
+    path = GOLDEN / f"{key}.npz"
+    if not path.exists():
+        pytest.fail(f"missing golden fixture {path.name}; run tests/golden/make_goldens.py {key}")
+    gold = dict(np.load(path))
+    mol, pts, w, cfg = inputs.make_config(key)
+    c = np.random.default_rng(int(gold["dm_seed"])).normal(size=(mol.nao, int(gold["dm_nocc"])))
+    dm = float(gold["dm_scale"]) * (c @ c.T)
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    x = torch.tensor(pts, device="cuda")
+    wt = torch.tensor(w, device="cuda")
+    return gold, mol, dm, ctx, x, wt
+
+
+@pytest.mark.parametrize("key", ["c4", "c5"])
+def test_gradient_at_config_matches_oracle_and_differences(key):
+    """dE/dR for every atom at the configuration's frozen FP64 anchors (the
+    oracle's qrcp_dense / rand_sketch anchors of the golden fixture) against
+    the oracle's FP64 gradient from AO dx/dy/dz values (1e-8 of max |g|) and
+    against central differences of the oracle energy at h = 1e-4 bohr (1e-6
+    of max |g|).  Where the plain h = 1e-4 difference carries an O(h^2)
+    truncation error above 1e-6 of max |g| -- estimated from the h/2
+    difference as 4/3 |fd_h - fd_h/2| -- the check uses the Richardson
+    extrapolation (4 fd_h/2 - fd_h)/3 and reports the coordinate."""
+    gold, mol, dm, ctx, x, wt = _golden_system(key)
+    anchors = gold["anchors"]
+    e, g = ctx.energy_gradient(x, wt, anchors, dm)
+    e_only = ctx.energy(x, wt, anchors, dm)
+    g_ref = gold["gradient"]
+    scale = np.abs(g_ref).max()
+    np.testing.assert_allclose(e, float(gold["energy"]), rtol=1e-10)
+    np.testing.assert_allclose(e_only, e, rtol=1e-12)
+    np.testing.assert_allclose(g, g_ref, rtol=0, atol=1e-8 * scale)
+    richardson = []
+    for (a, c), fh, fh2 in zip(gold["fd_coords"], gold["fd_h"], gold["fd_h2"]):
+        trunc = 4.0 / 3.0 * abs(fh - fh2)
+        if abs(g[a, c] - fh) <= 1e-6 * scale:
+            continue
+        assert trunc > 1e-6 * scale, (key, a, c, g[a, c], fh, trunc)
+        rich = (4.0 * fh2 - fh) / 3.0
+        assert abs(g[a, c] - rich) <= 1e-6 * scale, (key, a, c, g[a, c], rich)
+        richardson.append((int(a), int(c), float(abs(g[a, c] - fh) / scale)))
+    print(f"{key}: E {e:.12e}, max |g| {scale:.6e}, {len(gold['fd_coords'])} coordinates checked, "
+          f"h^2-limited (atom, axis, |g - fd_h| / max|g|): {richardson}")

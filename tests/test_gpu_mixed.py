@@ -231,3 +231,34 @@ def test_mixed_projection_follows_moved_atoms(small_water):
     scale = np.abs(p64).max()
     assert np.abs(pm - p64).max() <= 1e-4 * scale
     ctx.set_coords(mol.coords)
+
+
+@pytest.mark.parametrize("axes,expect_mixed", [
+    (("ao",), True),                    # 1 x 128-column accumulator
+    (("ao", "dz"), True),               # 2 x 128
+    (("ao", "dx", "dy"), True),         # 3 x 128
+    (("ao", "dx", "dy", "dz"), False),  # 4 x 128 columns exceed the shared-memory plan: FP64 form
+])
+def test_wide_sketch_reports_form_and_matches_fp64(small_water, axes, expect_mixed):
+    """rank 24 + oversampling 16 (ell = 40, 80 projection columns per axis):
+    the mixed form runs with 128-column accumulators for up to three axis
+    entries and reports the FP64 form otherwise; pivots equal the FP64 form's
+    and the oracle's either way."""
+    import torch
+    from mp_isdf_b200 import capi
+    mol, pts, w = small_water
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    x = torch.tensor(pts, device="cuda")
+    wt = torch.tensor(w, device="cuda")
+    kw = dict(axes=axes, max_rank=24, oversampling=16, seed=3)
+    p64, i64 = ctx.select(x, wt, precision="fp64", **kw)
+    pm, im = ctx.select(x, wt, precision="mixed", **kw)
+    assert i64.precision_used == 0
+    assert im.precision_used == (1 if expect_mixed else 0)
+    assert im.sketch_rows == 40
+    assert list(pm) == list(p64)
+    oc = O.OracleContext(mol.atm, mol.bas, mol.env)
+    codes = [O.AXIS_CODES[a] for a in axes]
+    scales = O.axis_scales(oc, pts, w, codes)
+    ref = O.select_rand_sketch(oc, pts, w, codes, max_rank=24, oversampling=16, seed=3, scales=scales)
+    assert list(pm) == ref

@@ -206,3 +206,45 @@ def test_adjoint_reference_matches_finite_differences(small_water):
         fd = (4 * fd2 - fd1) / 3
         np.testing.assert_allclose(grad[atom, c], fd, rtol=1e-6,
                                    atol=1e-6 * np.abs(grad).max())
+
+
+def test_exact_norm_qrcps_match_lapack_dgeqp3(small_water):
+    """The exact-norm truncated QRCPs that write the golden fixtures pick the
+    same pivots as LAPACK dgeqp3 (scipy) on the explicit pair matrix
+    (qrcp_dense, cpp/src/anchor_select_qrcp.cpp:248-307) and on the sketch
+    (cpp/src/anchor_select_randomized_id.cpp:320-374), with the same |R_jj|."""
+    mol, pts, w = small_water
+    oc = O.OracleContext(mol.atm, mol.bas, mol.env)
+    keep = np.flatnonzero(w != 0)
+    f = oc.axis_features(pts[keep], [0])
+    ref = O.select_qrcp_dense(oc, pts, w, [0], max_rank=12)
+    pos, diag, gaps = O.pair_qrcp_exact(f, w[keep], 12)
+    assert [int(keep[p]) for p in pos] == ref
+    assert np.all(gaps > 1e-10)
+    piv, det = O.select_rand_sketch(oc, pts, w, [0], max_rank=10, oversampling=16, seed=7,
+                                    return_details=True)
+    pos, diag, gaps = O.sketch_qrcp_exact(det["y"].T, 26)
+    assert pos == [int(j) for j in det["jpvt"][:26]]
+    np.testing.assert_allclose(diag, det["diag"][:26], rtol=1e-12)
+
+
+def test_golden_fixtures_are_consistent():
+    """Each committed golden fixture (tests/golden/*.npz) holds one anchor per
+    rank, positive step gaps, Theta on the sampled columns, and -- for the
+    randomized sketch -- anchors equal to LAPACK dgeqp3's pivots wherever the
+    exact-norm gap exceeds 1e-10."""
+    from pathlib import Path
+    files = sorted((Path(__file__).resolve().parent / "golden").glob("*.npz"))
+    assert {p.stem for p in files} >= {"c1", "c2", "c2o", "c3", "c4"}
+    for p in files:
+        g = np.load(p)
+        k = int(g["rank"])
+        assert len(g["anchors"]) == k and len(g["step_gap"]) == k
+        assert np.all(g["step_gap"] >= 0) and np.all(g["step_diag"] > 0)
+        assert g["theta_sample"].shape == (k, len(g["theta_pos"]))
+        assert 0 < float(g["pair_relative"]) < 1
+        if "dgeqp3_pivots" in g:
+            for j, (a, b) in enumerate(zip(g["anchors"], g["dgeqp3_pivots"])):
+                if a != b:
+                    assert g["step_gap"][j] <= 1e-10
+                    break
