@@ -168,8 +168,10 @@ typedef struct isdf_fit_info {
     double pair_l2;              /* sqrt(sum |w| |p - rec|^2) */
     double pair_relative;
     double theta_w[64];          /* sum_g Theta[a,g] w_g (first 64 anchors) */
-    int64_t fit_path;            /* 0 FP64; 1 mixed; 2 mixed requested, bound too loose -> FP64 */
-    double mixed_bound;          /* a-posteriori bound on the mixed fit's relative pair-error change */
+    int64_t fit_path;            /* 0 FP64; 1 mixed (tensor-core Gram + one FP64 refinement step);
+                                  * 2 mixed requested, bound above 1e-8 -> FP64 AO values */
+    double mixed_bound;          /* a-posteriori bound on the refined mixed fit's relative
+                                  * pair-error excess over the FP64 fit */
 } isdf_fit_info;
 
 int isdf_fit(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t ng,

@@ -424,8 +424,8 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
                                  reuse ? ra->psq.get() : nullptr, on_chunk);
         o.path = 1;
         if (!(o.mixed_bound <= isdf::kMixedFitTolerance)) {
-            // the anchors' conditioning can amplify the BF16x3 Gram error past
-            // the tolerance: recompute Theta with FP64 AO values
+            // a fit whose pair error is very small cannot absorb the stored
+            // tiles' representation error: recompute Theta with FP64 AO values
             const double bound = o.mixed_bound;
             o = isdf::fit_grid(c, xyz, w, kp, f, theta, kp.n, false, s);
             o.mixed_bound = bound;

@@ -24,13 +24,13 @@ struct FitOutput {
     int64_t n = 0;
     double err2 = 0, exact2 = 0, max_abs_coeff = 0;
     std::vector<double> theta_w;          // sum_g Theta[a, g] w_g
-    double mixed_bound = 0;               // bound on |rel. pair-error change| vs FP64 (mixed fit)
-    int path = 0;                         // 0 FP64, 1 mixed, 2 mixed bound too loose -> FP64
+    double mixed_bound = 0;               // bound on the refined mixed fit's relative pair-error excess over FP64
+    int path = 0;                         // 0 FP64, 1 mixed + FP64 refinement, 2 mixed bound too loose -> FP64
 };
 
-// Largest relative pair-error deviation from the FP64 fit that the mixed fit
-// accepts (10x below the 1e-8 target); beyond it the fit is redone in FP64.
-constexpr double kMixedFitTolerance = 1e-9;
+// Largest relative pair-error excess over the FP64 fit that the refined mixed
+// fit accepts (the 1e-8 target); beyond it the fit is redone with FP64 AO values.
+constexpr double kMixedFitTolerance = 1e-8;
 
 AnchorFactor factor_anchors(const Context& c, const double* anchor_pts, const double* anchor_w,
                             int64_t k, cudaStream_t s);
@@ -42,11 +42,15 @@ FitOutput fit_grid(const Context& c, const double* pts, const double* w, const K
                    cudaStream_t s);
 
 // Mixed precision: G from the fused FP32-AO / split-BF16 tensor-core projection,
-// then h, X = T h and Theta in FP64.  The pair-space error is not evaluated
-// here (see fit_grid with have_theta).  With `ao_tiles` (the AO value tiles a
-// mixed sketch of the same kept points left in HBM) and their per-point sums
-// of squares `ao_psq`, G comes from a GEMM over the tiles instead; then, with
-// `on_chunk`, the points are fitted in a few chunks and on_chunk(g0, m) is
+// then h, X0 = T h and Theta0 in FP64, followed by one FP64 iterative-refinement
+// step over the stored split-BF16 AO tiles (G in FP64 against FP64 anchor
+// values, X1 = X0 + T (h - M X0)); mixed_bound bounds the refined Theta's
+// relative pair-error excess over the FP64 fit.  The pair-space error is not
+// evaluated here (see fit_grid with have_theta).  With `ao_tiles` (the AO
+// value tiles a mixed sketch of the same kept points left in HBM) and their
+// per-point sums of squares `ao_psq`, G comes from a GEMM over the tiles
+// instead of a new projection (which otherwise stores the tiles itself); then,
+// with `on_chunk`, the points are fitted in a few chunks and on_chunk(g0, m) is
 // called after the launches that write Theta's columns [g0, g0 + m) on s (a
 // caller can start copying those columns out while the next chunk runs).
 bool fit_mixed_supported(int64_t k);

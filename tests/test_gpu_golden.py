@@ -10,10 +10,12 @@ Criteria, per configuration and form:
   <= 1e-10 relative, after which the two pivot sequences are not compared;
 * Theta (python/isdf.py:238-263) at the fixture's sample of columns: FP64
   within max(1e-10, 1e-14 cond(C)^2) of the largest entry, mixed within
-  1e-5 cond(C)^2 (the solve amplifies the ~1e-5 split-BF16 error of
-  Phi_g Phi_a^T by cond(M) = cond(C)^2);
+  1e-5 cond(C)^2 (the solve can amplify the stored tiles' ~5e-6 error of
+  Phi_g by cond(M) = cond(C)^2);
 * pair-space error (python/isdf.py:154-191): FP64 within 1e-9 relative of the
-  oracle's, mixed within 1e-8 relative.
+  oracle's, mixed within 1e-8 relative, reached by the tensor-core fit plus
+  its one FP64 refinement step (fit path 1, bound <= 1e-8) without an FP64
+  recomputation.
 """
 from pathlib import Path
 
@@ -91,6 +93,10 @@ def test_select_fit_matches_oracle(case, precision):
         assert theta_err <= max(1e-10, 1e-14 * cond ** 2), (theta_err, msg)
         assert pair_err <= 1e-9, (pair_err, msg)
     else:
+        # the tensor-core Gram plus one FP64 refinement step is accepted at
+        # every benchmark configuration: no FP64 recomputation of the fit
+        assert finfo.fit_path == 1, msg
+        assert finfo.mixed_bound <= 1e-8, (finfo.mixed_bound, msg)
         assert theta_err <= 1e-5 * max(1.0, cond) ** 2, (theta_err, msg)
         assert pair_err <= 1e-8, (pair_err, msg)
 
