@@ -168,9 +168,11 @@ typedef struct isdf_fit_info {
     double pair_l2;              /* sqrt(sum |w| |p - rec|^2) */
     double pair_relative;
     double theta_w[64];          /* sum_g Theta[a,g] w_g (first 64 anchors) */
-    int64_t fit_path;            /* 0 FP64; 1 mixed (tensor-core Gram + one FP64 refinement step);
-                                  * 2 mixed requested, bound above 1e-8 -> FP64 AO values */
-    double mixed_bound;          /* a-posteriori bound on the refined mixed fit's relative
+    int64_t fit_path;            /* 0 FP64; 1 mixed (tensor-core Gram); 3 mixed followed by one
+                                  * FP64 iterative-refinement step of Theta over the stored AO
+                                  * tiles (taken when the bound of path 1 exceeds 1e-8);
+                                  * 2 mixed requested, refined bound above 1e-8 -> FP64 AO values */
+    double mixed_bound;          /* a-posteriori bound on the accepted mixed Theta's relative
                                   * pair-error excess over the FP64 fit */
 } isdf_fit_info;
 

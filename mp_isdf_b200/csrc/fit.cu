@@ -367,36 +367,112 @@ FitOutput fit_grid(const Context& c, const double* pts, const double* w, const K
 
 namespace {
 
-// Mixed-precision fit epilogue: G (FP32, from the tensor-core projection) ->
-// h = G o G, X0 = T h, Theta0 = X0 / w_anchor in FP64 (the first iterate; the
-// FP64 refinement step below corrects it).
+// Mixed-precision fit epilogue, the first iterate: G (FP32, from the
+// tensor-core projection) -> h = G o G, X0 = T h, Theta0 = X0 / w_anchor in
+// FP64; also Theta.w, max |X|, and the terms of an a-posteriori bound on how far
+// the pair error of Theta0 can lie from the FP64 fit's:
+//   excess <= lambda_max(T) * sum_g |w_g| |dh_g|^2,
+//   |dG_ga| <= kFitGramBound |phi_g| |phi_a|  (dh = 2 G dG + dG^2).
+// When the bound exceeds the tolerance (ill-conditioned anchors amplify the
+// split-BF16 error of the anchors' side of G by cond(C)^2), the FP64
+// refinement step below follows.
+constexpr double kFitGramBound = 2e-5;
+
 // KMAX >= k: the per-point vectors stay in registers (loops unrolled to KMAX).
 template <int KMAX>
 __global__ void __launch_bounds__(256)
-fit_mixed_kernel(const float* __restrict__ G, int64_t n, int k, const double* __restrict__ T,
-                 const double* __restrict__ wa, double* __restrict__ theta, int64_t ldt) {
+fit_mixed_kernel(const float* __restrict__ G, const float* __restrict__ psq, int64_t n, int k,
+                 const double* __restrict__ T, const double* __restrict__ M,
+                 const double* __restrict__ anorm, const double* __restrict__ wa,
+                 const double* __restrict__ w, const int64_t* __restrict__ index,
+                 double* __restrict__ theta, int64_t ldt, double* __restrict__ tw,
+                 double* __restrict__ acc) {
     extern __shared__ double sm[];
     double* Ts = sm;                // k*k
-    for (int i = threadIdx.x; i < k * k; i += blockDim.x) Ts[i] = T[i];
+    double* Ms = sm + k * k;        // k*k
+    double* tws = sm + 2 * k * k;   // k partial sums
+    __shared__ double red[8];
+    for (int i = threadIdx.x; i < k * k; i += blockDim.x) { Ts[i] = T[i]; Ms[i] = M[i]; }
+    for (int i = threadIdx.x; i < k; i += blockDim.x) tws[i] = 0.0;
     __syncthreads();
     const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    double h[KMAX];
+    double mx = 0, dh2 = 0, e2 = 0, q2 = 0;
+    double h[KMAX], x[KMAX], twl[KMAX];
+#pragma unroll
+    for (int a = 0; a < KMAX; ++a) { h[a] = 0.0; x[a] = 0.0; twl[a] = 0.0; }
+    if (g < n) {
+        const double qg = static_cast<double>(psq[g * 4]);   // |phi_g|^2
+        const double fn = sqrt(qg);
+        const int64_t gi = index[g];
+        const double wg = w[gi], aw = fabs(wg);
+#pragma unroll
+        for (int a = 0; a < KMAX; ++a)
+            if (a < k) {
+                const double gv = static_cast<double>(G[g * k + a]);
+                h[a] = gv * gv;
+                const double dG = kFitGramBound * fn * anorm[a];
+                const double dh = 2.0 * fabs(gv) * dG + dG * dG;
+                dh2 += dh * dh;
+            }
+        double xh = 0;
+#pragma unroll
+        for (int a = 0; a < KMAX; ++a)
+            if (a < k) {
+                double xa = 0;
+#pragma unroll
+                for (int b = 0; b < KMAX; ++b)
+                    if (b < k) xa += Ts[a * k + b] * h[b];
+                x[a] = xa;
+                xh += xa * h[a];
+                mx = fmax(mx, fabs(xa));
+                const double th = xa / wa[a];
+                theta[a * ldt + g] = th;
+                twl[a] = th * wg;
+            }
+        double xmx = 0;
+#pragma unroll
+        for (int a = 0; a < KMAX; ++a)
+            if (a < k) {
+                double t = 0;
+#pragma unroll
+                for (int b = 0; b < KMAX; ++b)
+                    if (b < k) t += Ms[a * k + b] * x[b];
+                xmx += x[a] * t;
+            }
+        dh2 *= aw;
+        e2 = aw * (qg * qg - 2.0 * xh + xmx);
+        q2 = aw * qg * qg;
+    }
+    // Theta.w partial sums: warp reduction, one shared-memory add per warp
 #pragma unroll
     for (int a = 0; a < KMAX; ++a)
         if (a < k) {
-            const double gv = static_cast<double>(G[g * k + a]);
-            h[a] = gv * gv;
+            const double v = warp_sum(twl[a]);
+            if (threadIdx.x % 32 == 0) atomicAdd(&tws[a], v);
         }
+    dh2 = block_sum<256>(dh2, red);
+    e2 = block_sum<256>(e2, red);
+    q2 = block_sum<256>(q2, red);
+    if (threadIdx.x == 0) {
+        atomicAdd(&acc[3], dh2);
+        atomicAdd(&acc[4], e2);
+        atomicAdd(&acc[5], q2);
+    }
 #pragma unroll
-    for (int a = 0; a < KMAX; ++a)
-        if (a < k) {
-            double xa = 0;
-#pragma unroll
-            for (int b = 0; b < KMAX; ++b)
-                if (b < k) xa += Ts[a * k + b] * h[b];
-            theta[a * ldt + g] = xa / wa[a];
-        }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    if (threadIdx.x % 32 == 0)
+        atomicMax(reinterpret_cast<unsigned long long*>(&acc[2]),
+                  static_cast<unsigned long long>(__double_as_longlong(mx)));
+    __syncthreads();
+    for (int i = threadIdx.x; i < k; i += blockDim.x) atomicAdd(&tw[i], tws[i]);
+}
+
+__global__ void row_norms_kernel(const double* __restrict__ a, int rows, int cols, double* __restrict__ out) {
+    const int r = blockIdx.x;
+    double s = 0;
+    for (int c = threadIdx.x; c < cols; c += 32) s += a[static_cast<int64_t>(r) * cols + c] * a[static_cast<int64_t>(r) * cols + c];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) out[r] = sqrt(s);
 }
 
 }  // namespace
@@ -405,16 +481,19 @@ fit_mixed_kernel(const float* __restrict__ G, int64_t n, int k, const double* __
 // The tensor-core fit X0 = T h~ carries the split-BF16 error of BOTH operands
 // of G = Phi_g Phi_a^T; an error in the anchors' values perturbs C and is
 // amplified by cond(C)^2 in X.  The refinement recomputes
-//     G64[g][a] = sum_mu (hi + lo)[g][mu] phi_a(mu)     (FP64 FMAs, FP64 anchors)
-// from the same stored tiles (hi + lo is exact in FP64), h = G64 o G64, the
-// FP64 residual r = h - M X0 and X1 = X0 + T r, Theta = X1 / w_a.  Then only
-// the grid-side representation error dp_g = p~_g - p_g remains, and it is
-// projected, not amplified: the pair-error excess is
-//     sum_g |w_g| |P_C dp_g|^2 <= sum_g |w_g| |dp_g|^2 <= (2 eps + eps^2)^2 sum_g |w_g| q_g^2
-// with eps the relative 2-norm error of the stored AO values of a point.
+//     G64[g][a] = sum_mu x[g][mu] phi_a(mu)     (FP64 FMAs, FP64 anchors)
+// from the stored tiles, where x = hi + lo + r is the FP32 AO value exactly
+// (the fused kernel stores the BF16 remainder r next to the (hi, lo) tiles),
+// then h = G64 o G64, the FP64 residual r = h - M X0 and X1 = X0 + T r,
+// Theta = X1 / w_a.  Only the grid-side error dp_g = p~_g - p_g of the FP32
+// evaluation remains, and it is projected, not amplified: the pair-error
+// excess is
+//     sum_g |w_g| |P_C dp_g|^2 <= sum_g |w_g| |dp_g|^2,  |dp_g| <= 2 |x_g| d_g + d_g^2,
+// with d_g = 2^-19 |x_g| bounding |x_g - phi_g| (twice the largest 2-norm
+// error of the FP32 AO values measured against FP64 ones).
 namespace {
 
-constexpr double kTileValueEps = 4.8e-6;   // 2^-18 (hi + lo of FP32) + 2^-20 (FP32 evaluation)
+constexpr double kFp32EvalError = 1.0 / 524288.0;   // 2^-19
 
 // PhiS[c][j][a] = phi_a[a][ao0[c] + j] for the used slots j < fill[c], else 0
 // (row stride k).
@@ -435,63 +514,107 @@ __device__ __forceinline__ double bf16_bits_to_double(uint32_t bits16) {
     return static_cast<double>(__uint_as_float(bits16 << 16));
 }
 
-// H[g][a0 + a] = (sum_mu (hi + lo)[g][mu] phi_{a0+a}(mu))^2 for a < KMAX, a0 + a < k,
-// FP64 FMAs over the stored tiles; q[g] = sum_mu (hi + lo)^2 when a0 == 0.
-// One thread per point, one 128-point tile per block.
+// H[g][a0 + a] = (sum_mu x[g][mu] phi_{a0+a}(mu))^2 for a < KMAX, a0 + a < k, with
+// x = hi + lo + r from the stored tiles (FP64 FMAs); q[g] = sum_mu x^2 when a0 == 0.
+// One 128-point tile per block of 64 threads: thread t takes rows t and t + 64,
+// so every anchor value read from shared memory (two per 16-byte load) feeds
+// two FMAs.  hi + lo is exact in FP32 and so is (hi + lo) + r, whose exact
+// value is the FP32 AO value itself: one conversion to FP64 per entry.
+constexpr int kRefineThreads = 64;
+
 template <int KMAX>
-__global__ void __launch_bounds__(128)
-refine_gram_kernel(const uint8_t* __restrict__ tiles, int nchunks, int64_t n, int k, int a0,
-                   const double* __restrict__ img, double* __restrict__ H, double* __restrict__ q_out) {
-    __shared__ double S[32 * KMAX];
-    const int r = threadIdx.x;
+__global__ void __launch_bounds__(kRefineThreads)
+refine_gram_kernel(const uint8_t* __restrict__ tiles, const uint8_t* __restrict__ tiles_r, int nchunks,
+                   int64_t n, int k, int a0, const double* __restrict__ img, double* __restrict__ H,
+                   double* __restrict__ q_out) {
+    constexpr int KP = (KMAX + 1) & ~1;        // even row length: 16-byte loads of anchor pairs
+    __shared__ __align__(16) double S[32 * KP];
+    const int t = threadIdx.x;
     const int64_t tile = blockIdx.x;
-    const int64_t g = tile * 128 + r;
-    const bool valid = g < n;
-    // row r of a K-major interleaved 128 x 32 BF16 tile: core matrices of 8 rows
-    // x 8 K (16 B rows), K-adjacent ones 2048 B apart, M-adjacent ones 128 B apart
-    const uint32_t row_off = static_cast<uint32_t>(r >> 3) * 128u + static_cast<uint32_t>(r & 7) * 16u;
     const int na = min(KMAX, k - a0);
-    double G[KMAX];
+    // rows t and t + 64 of a K-major interleaved 128 x 32 BF16 tile: core
+    // matrices of 8 rows x 8 K (16 B rows), K-adjacent ones 2048 B apart,
+    // M-adjacent ones 128 B apart
+    uint32_t row_off[2];
+    bool valid[2];
 #pragma unroll
-    for (int a = 0; a < KMAX; ++a) G[a] = 0.0;
-    double q = 0.0;
+    for (int h = 0; h < 2; ++h) {
+        const int r = t + 64 * h;
+        row_off[h] = static_cast<uint32_t>(r >> 3) * 128u + static_cast<uint32_t>(r & 7) * 16u;
+        valid[h] = tile * 128 + r < n;
+    }
+    double G[2][KP];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int a = 0; a < KP; ++a) G[h][a] = 0.0;
+    double q[2] = {0.0, 0.0};
     for (int c = 0; c < nchunks; ++c) {
         __syncthreads();
-        for (int i = threadIdx.x; i < 32 * KMAX; i += blockDim.x) {
-            const int j = i / KMAX, a = i % KMAX;
+        for (int i = t; i < 32 * KP; i += kRefineThreads) {
+            const int j = i / KP, a = i % KP;
             S[i] = a < na ? img[(static_cast<int64_t>(c) * 32 + j) * k + a0 + a] : 0.0;
         }
         __syncthreads();
-        if (!valid) continue;
-        const uint8_t* hi = tiles + (static_cast<size_t>(tile) * nchunks + c) * 16384u;
+        const size_t blk = static_cast<size_t>(tile) * nchunks + c;
+        const uint8_t* hi = tiles + blk * 16384u;
         const uint8_t* lo = hi + 8192u;
+        const uint8_t* rm = tiles_r + blk * 8192u;
 #pragma unroll
         for (int kg = 0; kg < 4; ++kg) {
-            const uint4 vh = __ldcs(reinterpret_cast<const uint4*>(hi + kg * 2048u + row_off));
-            const uint4 vl = __ldcs(reinterpret_cast<const uint4*>(lo + kg * 2048u + row_off));
-            const uint32_t h4[4] = {vh.x, vh.y, vh.z, vh.w}, l4[4] = {vl.x, vl.y, vl.z, vl.w};
+            float x[2][8];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint4 vh = make_uint4(0, 0, 0, 0), vl = vh, vr = vh;
+                if (valid[h]) {
+                    vh = __ldcs(reinterpret_cast<const uint4*>(hi + kg * 2048u + row_off[h]));
+                    vl = __ldcs(reinterpret_cast<const uint4*>(lo + kg * 2048u + row_off[h]));
+                    vr = __ldcs(reinterpret_cast<const uint4*>(rm + kg * 2048u + row_off[h]));
+                }
+                const uint32_t h4[4] = {vh.x, vh.y, vh.z, vh.w}, l4[4] = {vl.x, vl.y, vl.z, vl.w},
+                               r4[4] = {vr.x, vr.y, vr.z, vr.w};
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const uint32_t sel = (e & 1) ? 0xffff0000u : 0x0000ffffu;
+                    const int shl = (e & 1) ? 0 : 16;
+                    const float fh = __uint_as_float((h4[e >> 1] & sel) << shl);
+                    const float fl = __uint_as_float((l4[e >> 1] & sel) << shl);
+                    const float fr = __uint_as_float((r4[e >> 1] & sel) << shl);
+                    x[h][e] = __fadd_rn(__fadd_rn(fh, fl), fr);   // the FP32 value, exactly
+                }
+            }
 #pragma unroll
             for (int e = 0; e < 8; ++e) {
-                const uint32_t hb = (e & 1) ? (h4[e >> 1] >> 16) : (h4[e >> 1] & 0xffffu);
-                const uint32_t lb = (e & 1) ? (l4[e >> 1] >> 16) : (l4[e >> 1] & 0xffffu);
-                const double x = bf16_bits_to_double(hb) + bf16_bits_to_double(lb);   // exact
-                q = fma(x, x, q);
-                const double* srow = S + (kg * 8 + e) * KMAX;
+                const double x0 = static_cast<double>(x[0][e]), x1 = static_cast<double>(x[1][e]);
+                q[0] = fma(x0, x0, q[0]);
+                q[1] = fma(x1, x1, q[1]);
+                const double2* srow = reinterpret_cast<const double2*>(S + (kg * 8 + e) * KP);
 #pragma unroll
-                for (int a = 0; a < KMAX; ++a) G[a] = fma(x, srow[a], G[a]);
+                for (int a = 0; a < KP / 2; ++a) {
+                    const double2 s2 = srow[a];
+                    G[0][2 * a] = fma(x0, s2.x, G[0][2 * a]);
+                    G[0][2 * a + 1] = fma(x0, s2.y, G[0][2 * a + 1]);
+                    G[1][2 * a] = fma(x1, s2.x, G[1][2 * a]);
+                    G[1][2 * a + 1] = fma(x1, s2.y, G[1][2 * a + 1]);
+                }
             }
         }
     }
-    if (!valid) return;
 #pragma unroll
-    for (int a = 0; a < KMAX; ++a)
-        if (a < na) H[g * k + a0 + a] = G[a] * G[a];
-    if (a0 == 0) q_out[g] = q;
+    for (int h = 0; h < 2; ++h) {
+        if (!valid[h]) continue;
+        const int64_t g = tile * 128 + t + 64 * h;
+#pragma unroll
+        for (int a = 0; a < KMAX; ++a)
+            if (a < na) H[g * k + a0 + a] = G[h][a] * G[h][a];
+        if (a0 == 0) q_out[g] = q[h];
+    }
 }
 
 // Per point: X0 = Theta0 w_a, r = H - M X0 (FP64 residual), X1 = X0 + T r,
-// Theta = X1 / w_a; with Theta.w per anchor, max |X1| and the pair-error sums
-// of the refined fit over the tile values, acc = {sum |w| e_g, sum |w| q_g^2, max}.
+// Theta = X1 / w_a; with Theta.w per anchor and acc = {sum |w| e_g (pair error
+// of the refined fit over the tile values), sum |w| q_g^2, max |X1|,
+// sum |w| (2 |x_g| d_g + d_g^2)^2 (the excess bound)}.
 __global__ void __launch_bounds__(256)
 refine_update_kernel(const double* __restrict__ H, const double* __restrict__ qv, int64_t n, int k,
                      const double* __restrict__ T, const double* __restrict__ M, const double* __restrict__ wa,
@@ -502,10 +625,10 @@ refine_update_kernel(const double* __restrict__ H, const double* __restrict__ qv
     for (int i = threadIdx.x; i < k; i += blockDim.x) tws[i] = 0.0;
     __syncthreads();
     const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    double e2 = 0.0, q2 = 0.0, mx = 0.0;
+    double e2 = 0.0, q2 = 0.0, mx = 0.0, b2 = 0.0;
     if (g < n) {
         const double* h = H + g * k;
-        double x0[64], r[64];
+        double x0[64], r[64], x1[64];
         for (int a = 0; a < k; ++a) x0[a] = theta[a * ldt + g] * wa[a];
         for (int a = 0; a < k; ++a) {
             double v = h[a];
@@ -516,9 +639,9 @@ refine_update_kernel(const double* __restrict__ H, const double* __restrict__ qv
         for (int a = 0; a < k; ++a) {
             double d = 0.0;
             for (int b = 0; b < k; ++b) d += __ldg(T + a * k + b) * r[b];
-            r[a] = x0[a] + d;                 // X1 (the residual is no longer needed)
+            x1[a] = x0[a] + d;
         }
-        for (int a = 0; a < k; ++a) x0[a] = r[a];
+        for (int a = 0; a < k; ++a) x0[a] = x1[a];
         double xmx = 0.0;
         const double wg = w[index[g]], aw = fabs(wg);
         for (int a = 0; a < k; ++a) {
@@ -534,12 +657,18 @@ refine_update_kernel(const double* __restrict__ H, const double* __restrict__ qv
         const double q = qv[g];
         e2 = aw * (q * q - 2.0 * xh + xmx);
         q2 = aw * q * q;
+        const double xn = sqrt(q);
+        const double d = kFp32EvalError * xn;
+        const double dp = 2.0 * xn * d + d * d;
+        b2 = aw * dp * dp;
     }
     e2 = block_sum<256>(e2, red);
     q2 = block_sum<256>(q2, red);
+    b2 = block_sum<256>(b2, red);
     if (threadIdx.x == 0) {
         atomicAdd(&acc[0], e2);
         atomicAdd(&acc[1], q2);
+        atomicAdd(&acc[3], b2);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
@@ -560,27 +689,28 @@ namespace {
 int refine_kmax(int64_t k) { return k <= 4 ? 4 : k <= 8 ? 8 : k <= 10 ? 10 : k <= 12 ? 12 : k <= 16 ? 16 : 32; }
 
 template <int K>
-void launch_refine_gram(const uint8_t* tiles, int nchunks, int64_t n, int k, const double* img, double* H,
-                        double* q, cudaStream_t s) {
+void launch_refine_gram(const uint8_t* tiles, const uint8_t* tiles_r, int nchunks, int64_t n, int k,
+                        const double* img, double* H, double* q, cudaStream_t s) {
     const unsigned grid = static_cast<unsigned>((n + 127) / 128);
     for (int a0 = 0; a0 < k; a0 += K) {
-        refine_gram_kernel<K><<<grid, 128, 0, s>>>(tiles, nchunks, n, k, a0, img, H, q);
+        refine_gram_kernel<K><<<grid, kRefineThreads, 0, s>>>(tiles, tiles_r, nchunks, n, k, a0, img, H, q);
         ISDF_LAUNCH_CHECK();
     }
 }
 
 // One FP64 refinement step of the Theta columns of n points whose AO tiles
 // start at `tiles`.
-void refine_theta(int kmax, const uint8_t* tiles, int nchunks, int64_t n, int k, const double* img,
+void refine_theta(int kmax, const uint8_t* tiles, const uint8_t* tiles_r, int nchunks, int64_t n, int k,
+                  const double* img,
                   const AnchorFactor& f, const double* w, const int64_t* index, double* theta, int64_t ldt,
                   double* H, double* q, double* tw, double* acc, cudaStream_t s) {
     switch (kmax) {
-    case 4: launch_refine_gram<4>(tiles, nchunks, n, k, img, H, q, s); break;
-    case 8: launch_refine_gram<8>(tiles, nchunks, n, k, img, H, q, s); break;
-    case 10: launch_refine_gram<10>(tiles, nchunks, n, k, img, H, q, s); break;
-    case 12: launch_refine_gram<12>(tiles, nchunks, n, k, img, H, q, s); break;
-    case 16: launch_refine_gram<16>(tiles, nchunks, n, k, img, H, q, s); break;
-    default: launch_refine_gram<32>(tiles, nchunks, n, k, img, H, q, s); break;
+    case 4: launch_refine_gram<4>(tiles, tiles_r, nchunks, n, k, img, H, q, s); break;
+    case 8: launch_refine_gram<8>(tiles, tiles_r, nchunks, n, k, img, H, q, s); break;
+    case 10: launch_refine_gram<10>(tiles, tiles_r, nchunks, n, k, img, H, q, s); break;
+    case 12: launch_refine_gram<12>(tiles, tiles_r, nchunks, n, k, img, H, q, s); break;
+    case 16: launch_refine_gram<16>(tiles, tiles_r, nchunks, n, k, img, H, q, s); break;
+    default: launch_refine_gram<32>(tiles, tiles_r, nchunks, n, k, img, H, q, s); break;
     }
     refine_update_kernel<<<blocks_for(n), 256, 0, s>>>(H, q, n, k, f.T.get(), f.M.get(), f.wa.get(), w, index,
                                                      theta, ldt, tw, acc);
@@ -591,10 +721,10 @@ void refine_theta(int kmax, const uint8_t* tiles, int nchunks, int64_t n, int k,
 
 FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
                          const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s,
-                         const uint8_t* ao_tiles, const float* ao_psq, const FitChunkHook* on_chunk) {
+                         const uint8_t* ao_tiles, const uint8_t* ao_tiles_r, const float* ao_psq,
+                         const FitChunkHook* on_chunk) {
     FitOutput out;
     const int64_t n = kp.n, k = f.k, nao = c.nao;
-    (void)ao_psq;   // the refinement forms |phi_g|^2 from the tiles themselves
     out.theta_w.assign(k, 0.0);
     if (n == 0 || k == 0) return out;
     ProjectPlan plan;
@@ -604,15 +734,79 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
         const WSource src{f.phi_a.get(), 0, 1, nao, static_cast<int>(k), 0};
         plan = make_project_plan(c, {0}, static_cast<int>(k), &src, 1, s);
     }
-    DeviceBuffer<float> G(static_cast<size_t>(n * k), s);
+    DeviceBuffer<float> G(static_cast<size_t>(n * k), s), psq;
     DeviceBuffer<int> err(1, s);
-    DeviceBuffer<double> racc(3, s), rtw(k, s);
+    DeviceBuffer<double> acc(6, s), tw(k, s), anorm(k, s);
     err.zero(s);
+    acc.zero(s);
+    tw.zero(s);
+    row_norms_kernel<<<static_cast<unsigned>(k), 32, 0, s>>>(f.phi_a.get(), static_cast<int>(k),
+                                                            static_cast<int>(nao), anorm.get());
+    ISDF_LAUNCH_CHECK();
+    const float* point_sq = ao_psq;
+    const uint8_t* tiles = ao_tiles;
+    const uint8_t* tiles_r = ao_tiles_r;
+    DeviceBuffer<uint8_t> own_tiles;
+    if (!ao_tiles || !ao_tiles_r || !ao_psq) {
+        // no tiles from a preceding sketch: the projection computes G and
+        // stores the tiles (hi, lo and remainder) for a refinement step
+        psq.reset(static_cast<size_t>(n * 4), s);
+        psq.zero(s);
+        own_tiles.reset(stored_tile_bytes(c, n) + stored_remainder_bytes(c, n), s);
+        project_tc(c, plan, pts, kp.index.get(), n, nullptr, G.get(), k, 1, nullptr, psq.get(), err.get(), s,
+                   own_tiles.get(), 0, own_tiles.get() + stored_tile_bytes(c, n));
+        point_sq = psq.get();
+        tiles = own_tiles.get();
+        tiles_r = own_tiles.get() + stored_tile_bytes(c, n);
+        ao_tiles = nullptr;
+    }
+    // With stored tiles and a hook, the points go in a few chunks of whole
+    // 128-point tiles, each at least two waves of the stored-tile GEMM.
+    const int64_t ntiles = (n + 127) / 128;
+    const int64_t nchunk = (ao_tiles && on_chunk) ? std::max<int64_t>(1, std::min<int64_t>(4, ntiles / 296)) : 1;
+    const int64_t per = (ntiles + nchunk - 1) / nchunk * 128;
+    const size_t smem = static_cast<size_t>(2 * k * k + k) * sizeof(double);
+    auto kern = k <= 16 ? fit_mixed_kernel<16> : k <= 32 ? fit_mixed_kernel<32> : fit_mixed_kernel<64>;
+    // 1. the tensor-core first iterate Theta0 and its a-posteriori bound
+    for (int64_t g0 = 0; g0 < n; g0 += per) {
+        const int64_t m = std::min(per, n - g0);
+        if (ao_tiles)
+            // AO values of these points already sit in HBM as split-BF16 tiles
+            gram_from_tiles(c, plan, ao_tiles + stored_tile_bytes(c, g0), m, G.get() + g0 * k, k, err.get(), s);
+        {
+            ISDF_PROFILE("fit_mixed", s);
+            kern<<<blocks_for(m), 256, smem, s>>>(G.get() + g0 * k, point_sq + g0 * 4, m, static_cast<int>(k),
+                                                  f.T.get(), f.M.get(), anorm.get(), f.wa.get(), w,
+                                                  kp.index.get() + g0, theta + g0, ldt, tw.get(), acc.get());
+            ISDF_LAUNCH_CHECK();
+        }
+        if (on_chunk && ao_tiles) (*on_chunk)(g0, m);
+    }
+    double h[6];
+    int herr = 0;
+    ISDF_CUDA(cudaMemcpyAsync(h, acc.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(out.theta_w.data(), tw.get(), k * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    if (herr) fail(kRuntime, "tensor-core fit pipeline timed out (error flags " + std::to_string(herr) + ")");
+    // lambda_max(T) = 1 / s_min^2 over the retained singular values of C^T
+    double smin = 0;
+    for (double x : f.sv)
+        if (x > 1e-12 * (f.sv.empty() ? 0.0 : f.sv.front())) smin = x;
+    const double lam = smin > 0 ? 1.0 / (smin * smin) : std::numeric_limits<double>::infinity();
+    out.mixed_bound = (h[4] > 0) ? lam * h[3] / (2.0 * h[4]) : std::numeric_limits<double>::infinity();
+    out.max_abs_coeff = h[2];
+    out.n = n;
+    out.err2 = std::numeric_limits<double>::quiet_NaN();
+    out.exact2 = std::numeric_limits<double>::quiet_NaN();
+    out.path = 1;
+    if (out.mixed_bound <= kMixedFitTolerance) return out;
+
+    // 2. one FP64 iterative-refinement step over the stored tiles
+    const int kmax = refine_kmax(k);
+    DeviceBuffer<double> img(static_cast<size_t>(c.nchunks) * 32 * k, s), racc(4, s), rtw(k, s);
     racc.zero(s);
     rtw.zero(s);
-    // anchor values at the K-chunk slots, for the FP64 refinement
-    const int kmax = refine_kmax(k);
-    DeviceBuffer<double> img(static_cast<size_t>(c.nchunks) * 32 * k, s);
     {
         const int64_t total = static_cast<int64_t>(c.nchunks) * 32 * k;
         anchor_slot_image_kernel<<<blocks_for(total), 256, 0, s>>>(f.phi_a.get(), static_cast<int>(k),
@@ -620,59 +814,23 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
                                                                    c.d_fill, img.get());
         ISDF_LAUNCH_CHECK();
     }
-    const uint8_t* tiles = ao_tiles;
-    DeviceBuffer<uint8_t> own_tiles;
-    if (!ao_tiles) {
-        // no tiles from a preceding sketch: the projection stores them for the refinement
-        own_tiles.reset(stored_tile_bytes(c, n), s);
-        project_tc(c, plan, pts, kp.index.get(), n, nullptr, G.get(), k, 1, nullptr, nullptr, err.get(), s,
-                   own_tiles.get(), 0);
-        tiles = own_tiles.get();
-    }
-    // With stored tiles and a hook, the points go in a few chunks of whole
-    // 128-point tiles, each at least two waves of the stored-tile GEMM.
-    const int64_t ntiles = (n + 127) / 128;
-    const int64_t nchunk = (ao_tiles && on_chunk) ? std::max<int64_t>(1, std::min<int64_t>(4, ntiles / 296)) : 1;
-    const int64_t per = (ntiles + nchunk - 1) / nchunk * 128;
     DeviceBuffer<double> H64(static_cast<size_t>(std::min(per, n) * k), s), q64(std::min(per, n), s);
-    const size_t smem = static_cast<size_t>(k * k) * sizeof(double);
-    auto kern = k <= 16 ? fit_mixed_kernel<16> : k <= 32 ? fit_mixed_kernel<32> : fit_mixed_kernel<64>;
     for (int64_t g0 = 0; g0 < n; g0 += per) {
         const int64_t m = std::min(per, n - g0);
-        const uint8_t* chunk_tiles = tiles + stored_tile_bytes(c, g0);
-        if (ao_tiles)
-            // AO values of these points already sit in HBM as split-BF16 tiles
-            gram_from_tiles(c, plan, chunk_tiles, m, G.get() + g0 * k, k, err.get(), s);
-        {
-            ISDF_PROFILE("fit_mixed", s);
-            kern<<<blocks_for(m), 256, smem, s>>>(G.get() + g0 * k, m, static_cast<int>(k), f.T.get(),
-                                                  f.wa.get(), theta + g0, ldt);
-            ISDF_LAUNCH_CHECK();
-        }
-        {
-            // one FP64 iterative-refinement step of these Theta columns
-            ISDF_PROFILE("fit_refine", s);
-            refine_theta(kmax, chunk_tiles, c.nchunks, m, static_cast<int>(k), img.get(), f, w,
-                         kp.index.get() + g0, theta + g0, ldt, H64.get(), q64.get(), rtw.get(), racc.get(), s);
-        }
-        if (on_chunk && ao_tiles) (*on_chunk)(g0, m);
+        ISDF_PROFILE("fit_refine", s);
+        refine_theta(kmax, tiles + stored_tile_bytes(c, g0), tiles_r + stored_remainder_bytes(c, g0), c.nchunks, m,
+                     static_cast<int>(k), img.get(), f, w, kp.index.get() + g0, theta + g0, ldt, H64.get(),
+                     q64.get(), rtw.get(), racc.get(), s);
     }
-    double h[3];
-    int herr = 0;
-    ISDF_CUDA(cudaMemcpyAsync(h, racc.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
-    ISDF_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    double r[4];
+    ISDF_CUDA(cudaMemcpyAsync(r, racc.get(), sizeof(r), cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaMemcpyAsync(out.theta_w.data(), rtw.get(), k * sizeof(double), cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaStreamSynchronize(s));
-    if (herr) fail(kRuntime, "tensor-core fit pipeline timed out (error flags " + std::to_string(herr) + ")");
     // relative pair-error excess of the refined Theta over the FP64 fit:
     // (err^2 + excess)^(1/2) / err - 1 <= excess / (2 err^2)
-    const double e = kTileValueEps;
-    out.mixed_bound = (h[0] > 0) ? (2.0 * e + e * e) * (2.0 * e + e * e) * h[1] / (2.0 * h[0])
-                                 : std::numeric_limits<double>::infinity();
-    out.max_abs_coeff = h[2];
-    out.n = n;
-    out.err2 = std::numeric_limits<double>::quiet_NaN();
-    out.exact2 = std::numeric_limits<double>::quiet_NaN();
+    out.mixed_bound = (r[0] > 0) ? r[3] / (2.0 * r[0]) : std::numeric_limits<double>::infinity();
+    out.max_abs_coeff = r[2];
+    out.path = 3;
     return out;
 }
 

@@ -25,7 +25,7 @@ struct FitOutput {
     double err2 = 0, exact2 = 0, max_abs_coeff = 0;
     std::vector<double> theta_w;          // sum_g Theta[a, g] w_g
     double mixed_bound = 0;               // bound on the refined mixed fit's relative pair-error excess over FP64
-    int path = 0;                         // 0 FP64, 1 mixed + FP64 refinement, 2 mixed bound too loose -> FP64
+    int path = 0;                         // 0 FP64, 1 mixed, 3 mixed + FP64 refinement, 2 bound too loose -> FP64
 };
 
 // Largest relative pair-error excess over the FP64 fit that the refined mixed
@@ -42,10 +42,12 @@ FitOutput fit_grid(const Context& c, const double* pts, const double* w, const K
                    cudaStream_t s);
 
 // Mixed precision: G from the fused FP32-AO / split-BF16 tensor-core projection,
-// then h, X0 = T h and Theta0 in FP64, followed by one FP64 iterative-refinement
-// step over the stored split-BF16 AO tiles (G in FP64 against FP64 anchor
-// values, X1 = X0 + T (h - M X0)); mixed_bound bounds the refined Theta's
-// relative pair-error excess over the FP64 fit.  The pair-space error is not
+// then h, X0 = T h and Theta0 in FP64 (path 1) with an a-posteriori bound on
+// its relative pair-error excess over the FP64 fit; when that bound exceeds
+// the tolerance, one FP64 iterative-refinement step over the stored AO tiles
+// follows (path 3), whose (hi, lo, remainder) BF16 terms add up to the FP32
+// values exactly: G in FP64 against FP64 anchor values, X1 = X0 + T (h - M X0),
+// and mixed_bound then bounds the refined Theta's excess.  The pair-space error is not
 // evaluated here (see fit_grid with have_theta).  With `ao_tiles` (the AO
 // value tiles a mixed sketch of the same kept points left in HBM) and their
 // per-point sums of squares `ao_psq`, G comes from a GEMM over the tiles
@@ -57,8 +59,8 @@ bool fit_mixed_supported(int64_t k);
 using FitChunkHook = std::function<void(int64_t g0, int64_t m)>;
 FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
                          const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s,
-                         const uint8_t* ao_tiles = nullptr, const float* ao_psq = nullptr,
-                         const FitChunkHook* on_chunk = nullptr);
+                         const uint8_t* ao_tiles = nullptr, const uint8_t* ao_tiles_r = nullptr,
+                         const float* ao_psq = nullptr, const FitChunkHook* on_chunk = nullptr);
 
 void gather_points(const double* pts, const double* w, const int64_t* idx, int64_t n,
                    int64_t npts_total, double* out_pts, double* out_w, cudaStream_t s);

@@ -30,6 +30,7 @@ struct ProjectArgs {
     double* sumsq;             // [4] or null
     int* error;                // bit flags of bounded waits that gave up
     uint8_t* a_store;          // null, or [tile][chunk] (hi, lo) A tiles of axis entry store_axis
+    uint8_t* a_store_r;        // null, or [tile][chunk] BF16 remainder tiles x - hi - lo of that entry
     int store_axis;
 };
 
@@ -56,7 +57,7 @@ void project_tc(const Context& c, const ProjectPlan& plan, const double* pts, co
                 int64_t n, const double* weights, float* out, int64_t ld_out, int64_t col_stride,
                 double* sumsq,
                 float* point_sq, int* error, cudaStream_t s, uint8_t* a_store = nullptr,
-                int store_axis = 0);
+                int store_axis = 0, uint8_t* a_store_r = nullptr);
 
 // G[g*ld_out + j] from A tiles stored by project_tc (a_store) over n points and
 // a one-axis value plan: the same split-BF16 products as project_tc.
@@ -67,5 +68,10 @@ void gram_from_tiles(const Context& c, const ProjectPlan& pl, const uint8_t* a_t
 inline size_t stored_tile_bytes(const Context& c, int64_t n) {
     return static_cast<size_t>((n + 127) / 128) * c.nchunks * 2 * 128 * 32 * 2;
 }
+
+// Bytes of the stored remainder tiles over n points: the third BF16 term
+// r = x - hi - lo of each FP32 value x, so that hi + lo + r == x exactly (one
+// 8 KB tile per 128 points and K-chunk, same layout as the A tiles).
+inline size_t stored_remainder_bytes(const Context& c, int64_t n) { return stored_tile_bytes(c, n) / 2; }
 
 }  // namespace isdf

@@ -133,6 +133,7 @@ constexpr int kMaxVerifiedNao = 6144;
 struct RetainedAo {
     KeptPoints kp;
     const uint8_t* tiles = nullptr;  // [tile][K-chunk] (hi, lo) A tiles of the AO values
+    const uint8_t* tiles_r = nullptr;  // [tile][K-chunk] remainder tiles (hi + lo + r = FP32 value)
     DeviceBuffer<float> psq;       // [n][4] per-point sums of squares (component 0 = values)
     bool valid = false;
 };

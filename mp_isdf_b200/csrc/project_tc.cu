@@ -77,6 +77,21 @@ __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
     lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// The remainder r = bf16(x - hi - lo) of that split: x - hi and (x - hi) - lo
+// are exact in FP32 and the remainder has at most 8 significant bits, so
+// hi + lo + r == x exactly.
+__device__ __forceinline__ uint4 remainder8(const float* x, const uint4& hi, const uint4& lo) {
+    const uint32_t h[4] = {hi.x, hi.y, hi.z, hi.w}, l[4] = {lo.x, lo.y, lo.z, lo.w};
+    uint32_t r[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float h0 = __uint_as_float(h[i] << 16), h1 = __uint_as_float(h[i] & 0xffff0000u);
+        const float l0 = __uint_as_float(l[i] << 16), l1 = __uint_as_float(l[i] & 0xffff0000u);
+        r[i] = bf162_bits(__floats2bfloat162_rn((x[2 * i] - h0) - l0, (x[2 * i + 1] - h1) - l1));
+    }
+    return make_uint4(r[0], r[1], r[2], r[3]);
+}
+
 __device__ __forceinline__ void named_bar_sync(int id, int count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
@@ -255,6 +270,9 @@ project_tc_kernel(ProjectArgs args) {
                     const uint32_t off = tc::interleaved_offset(row, kg * 8, kLboA, kSboA);
                     *reinterpret_cast<uint4*>(sA + (a * 2 + 0) * kTileA + off) = hi;
                     *reinterpret_cast<uint4*>(sA + (a * 2 + 1) * kTileA + off) = lo;
+                    if (args.a_store_r && a == args.store_axis)   // warp-uniform: a is fixed per 128 u
+                        *reinterpret_cast<uint4*>(args.a_store_r + (static_cast<size_t>(tile) * nchunks + c) * kTileA +
+                                                  off) = remainder8(x, hi, lo);
                 }
                 tc::fence_proxy_async_smem();
                 tc::mbar_arrive(a_full);
@@ -546,7 +564,8 @@ bool project_tc_supported(int nax, int nout) {
 void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, const int64_t* index,
                 int64_t n, const double* weights, float* out, int64_t ld_out, int64_t col_stride,
                 double* sumsq,
-                float* point_sq, int* error, cudaStream_t s, uint8_t* a_store, int store_axis) {
+                float* point_sq, int* error, cudaStream_t s, uint8_t* a_store, int store_axis,
+                uint8_t* a_store_r) {
     if (n == 0) return;
     ProjectArgs a{};
     a.shells = c.d_shells;
@@ -572,6 +591,7 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     a.ld_out = ld_out;
     a.col_stride = col_stride;
     a.a_store = a_store;
+    a.a_store_r = a_store_r;
     a.store_axis = store_axis;
     require(a_store == nullptr || (store_axis >= 0 && store_axis < pl.nax), "invalid stored axis entry");
     a.nout = pl.nout;

@@ -259,7 +259,10 @@ py::dict fit(const std::shared_ptr<Context>& ctx, const FloatArray& coords, cons
     d["pair_relative"] = info.pair_relative;
     std::vector<double> tw(info.theta_w, info.theta_w + std::min<int64_t>(k, 64));
     d["theta_w"] = tw;
-    d["fit_path"] = info.fit_path == 0 ? "fp64" : info.fit_path == 1 ? "mixed" : "fp64-fallback";
+    d["fit_path"] = info.fit_path == 0   ? "fp64"
+                    : info.fit_path == 1 ? "mixed"
+                    : info.fit_path == 3 ? "mixed-refined"
+                                         : "fp64-fallback";
     d["mixed_bound"] = info.mixed_bound;
     return d;
 }

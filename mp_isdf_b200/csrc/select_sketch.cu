@@ -767,9 +767,10 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
         if (comps[a] == 0) store_axis = a;
     const size_t p_bytes = (static_cast<size_t>(n) * naxes * nout * sizeof(float) + 255) / 256 * 256;
     uint8_t* tiles = nullptr;
+    uint8_t* tiles_r = nullptr;
     if (keep) {
         // tiles (when they fit in free memory) and projections in the workspace
-        size_t tile_bytes = store_axis >= 0 ? stored_tile_bytes(c, n) : 0;
+        size_t tile_bytes = store_axis >= 0 ? stored_tile_bytes(c, n) + stored_remainder_bytes(c, n) : 0;
         if (tile_bytes + p_bytes > c.ws_bytes && tile_bytes > 0) {
             size_t free_b = 0, total_b = 0;
             ISDF_CUDA(cudaMemGetInfo(&free_b, &total_b));
@@ -779,7 +780,10 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
             }
         }
         uint8_t* base = c.workspace(tile_bytes + p_bytes);
-        if (store_axis >= 0) tiles = base;
+        if (store_axis >= 0) {
+            tiles = base;
+            tiles_r = base + stored_tile_bytes(c, n);
+        }
         P = reinterpret_cast<float*>(base + tile_bytes);
     } else {
         P_own.reset(static_cast<size_t>(n) * naxes * nout, s);
@@ -787,7 +791,7 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     }
     // column-major projections P[a*nout + j][g] (coalesced for the combine pass)
     project_tc(c, plan, pts, kp.index.get(), n, w, P, 1, n, sumsq.get(), psq.get(),
-               err.get(), s, tiles, std::max(store_axis, 0));
+               err.get(), s, tiles, std::max(store_axis, 0), tiles_r);
     double h[4] = {0, 0, 0, 0};
     int herr = 0;
     ISDF_CUDA(cudaMemcpyAsync(h, sumsq.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -825,6 +829,7 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     ms.source.delta = ms.delta.get();
     if (keep && store_axis >= 0) {
         keep->tiles = tiles;
+        keep->tiles_r = tiles_r;
         keep->psq = std::move(psq);
         keep->valid = true;
     }

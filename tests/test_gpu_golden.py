@@ -13,9 +13,9 @@ Criteria, per configuration and form:
   1e-5 cond(C)^2 (the solve can amplify the stored tiles' ~5e-6 error of
   Phi_g by cond(M) = cond(C)^2);
 * pair-space error (python/isdf.py:154-191): FP64 within 1e-9 relative of the
-  oracle's, mixed within 1e-8 relative, reached by the tensor-core fit plus
-  its one FP64 refinement step (fit path 1, bound <= 1e-8) without an FP64
-  recomputation.
+  oracle's, mixed within 1e-8 relative, reached by the tensor-core fit (fit
+  path 1) or by it and one FP64 refinement step (path 3), with the bound
+  <= 1e-8 and without an FP64 recomputation.
 """
 from pathlib import Path
 
@@ -93,9 +93,10 @@ def test_select_fit_matches_oracle(case, precision):
         assert theta_err <= max(1e-10, 1e-14 * cond ** 2), (theta_err, msg)
         assert pair_err <= 1e-9, (pair_err, msg)
     else:
-        # the tensor-core Gram plus one FP64 refinement step is accepted at
-        # every benchmark configuration: no FP64 recomputation of the fit
-        assert finfo.fit_path == 1, msg
+        # the tensor-core Gram (path 1), or it followed by one FP64 refinement
+        # step (path 3), is accepted at every benchmark configuration: no FP64
+        # recomputation of the fit
+        assert finfo.fit_path in (1, 3), msg
         assert finfo.mixed_bound <= 1e-8, (finfo.mixed_bound, msg)
         assert theta_err <= 1e-5 * max(1.0, cond) ** 2, (theta_err, msg)
         assert pair_err <= 1e-8, (pair_err, msg)

@@ -126,7 +126,7 @@ def test_mixed_dense_device_api(small_water):
     info64 = ctx.fit(x, wt, pm, theta64, precision="fp64")
     torch.cuda.synchronize()
     print("small water mixed fit path", info.fit_path, "bound", info.mixed_bound)
-    assert info.fit_path == 1 and info.mixed_bound <= 1e-8
+    assert info.fit_path in (1, 3) and info.mixed_bound <= 1e-8
     assert abs(info.pair_relative - info64.pair_relative) <= 1e-8 * info64.pair_relative
 
 
@@ -161,7 +161,7 @@ def test_select_fit_matches_select_then_fit(small_water, axes):
         # FP64 fits differ only by the order of atomic reductions, amplified by
         # cond(C)^2 in the solve; mixed fits also by FP32 AO rounding
         scale = max(1.0, info.condition) ** 2
-        assert rel <= (1e-12 * scale if info.fit_path != 1 else 1e-5 * scale), rel
+        assert rel <= (1e-12 * scale if info.fit_path in (0, 2) else 1e-5 * scale), rel
         if precision == "mixed":
             assert abs(info2.mixed_bound - info.mixed_bound) <= 1e-3 * info.mixed_bound
         assert abs(info2.pair_relative - info.pair_relative) <= 1e-8 * info.pair_relative
