@@ -298,6 +298,126 @@ void launch_tile_l(const Context& c, const TileArgs& a, cudaStream_t s) {
     else launch_tile<T, GRAD, kMaxL, 2>(a, s);
 }
 
+// Tiled axis features F[p*ld + offset[a] + ao] = scale[a] * comp_a(p, ao): the
+// layout of ao_tile_kernel (64 points per block, piece lanes of the chunk
+// layout, a padded shared tile [comp][slot][point] per K-chunk), with the
+// points gathered through `index`, one contiguous row store per (axis entry,
+// point) and chunk, and the per-component sums of squares of the points with
+// nonzero weight accumulated by the evaluating threads (FP64).
+template <class T>
+struct TileSqSink {
+    T* st; int p, base; bool count; double sq[4];
+    template <int C> __device__ __forceinline__ void put(int ao, T v) {
+        st[(C * 32 + ao + base) * kTileStride + p] = v;
+        if (count) sq[C] += static_cast<double>(v) * static_cast<double>(v);
+    }
+};
+
+struct AxisTileArgs {
+    const ShellDesc* shells; const void* exps; const void* coefs;
+    const int4* pieces; const int* lane_begin; const int* fill; const int* chunk_ao0; int nchunks;
+    const double* pts; const int64_t* index; int64_t n; const double* weights;
+    void* out; int64_t ld; double* sumsq;
+    int nent; int comp[16]; int off[16]; double scale[16];   // the non-occupied axis entries
+};
+
+template <class T, bool GRAD>
+constexpr size_t axis_tile_smem_bytes() {
+    return (GRAD ? 4 : 1) * 32 * kTileStride * sizeof(T) + kTilePts * sizeof(T*);
+}
+
+template <class T, bool GRAD, int LMAX, int PPT>
+__global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) axis_tile_kernel(AxisTileArgs a) {
+    constexpr int kNComp = GRAD ? 4 : 1;
+    constexpr int kWarps = kTilePts / 32 * PPT;
+    extern __shared__ __align__(16) uint8_t tile_raw[];
+    T** rowp = reinterpret_cast<T**>(tile_raw);                       // [kTilePts]
+    T* st = reinterpret_cast<T*>(tile_raw + kTilePts * sizeof(T*));
+    __shared__ double red[kWarps][4];
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+    const int lanegrp = warp % PPT, p = (warp / PPT) * 32 + lane;
+    const int64_t b0 = static_cast<int64_t>(blockIdx.x) * kTilePts;
+    const int64_t g = b0 + p;
+    const bool valid = g < a.n;
+    const int64_t gi = valid ? (a.index ? a.index[g] : g) : 0;
+    const double px = valid ? a.pts[3 * gi] : 0.0, py = valid ? a.pts[3 * gi + 1] : 0.0,
+                 pz = valid ? a.pts[3 * gi + 2] : 0.0;
+    const bool count = valid && a.sumsq != nullptr && (a.weights == nullptr || a.weights[gi] != 0.0);
+    const T* exps = static_cast<const T*>(a.exps);
+    const T* coefs = static_cast<const T*>(a.coefs);
+    for (int i = threadIdx.x; i < kTilePts; i += blockDim.x) {
+        const int64_t gp = b0 + i;
+        rowp[i] = gp < a.n ? static_cast<T*>(a.out) + gp * a.ld : nullptr;
+    }
+    double sq[4] = {0.0, 0.0, 0.0, 0.0};
+    const double cut = kExpCut * 1.0001;
+    for (int c = 0; c < a.nchunks; ++c) {
+        const int pb = a.lane_begin[c * PPT + lanegrp], pe = a.lane_begin[c * PPT + lanegrp + 1];
+        for (int pi = pb; pi < pe; ++pi) {
+            const int4 pc = a.pieces[pi];
+            const ShellDesc b = a.shells[pc.x];
+            const int ns = 2 * b.l + 1;
+            const double dx = px - b.x, dy = py - b.y, dz = pz - b.z;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (__all_sync(0xffffffffu, !valid || static_cast<double>(b.amin) * r2 > cut)) {
+                for (int k = pc.w; k < pc.w + pc.z * ns; ++k)
+#pragma unroll
+                    for (int cc = 0; cc < kNComp; ++cc) st[(cc * 32 + k) * kTileStride + p] = T(0);
+                continue;
+            }
+            TileSqSink<T> sink{st, p, pc.w - (b.ao_off + pc.y * ns), count, {0.0, 0.0, 0.0, 0.0}};
+            eval_shell_rel<T, GRAD, LMAX>(b, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
+                                          static_cast<T>(r2), exps, coefs, sink, pc.y, pc.y + pc.z);
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) sq[cc] += sink.sq[cc];
+        }
+        __syncthreads();
+        const int fill = a.fill[c], ao0 = a.chunk_ao0[c];
+        for (int r = warp; r < a.nent * kTilePts; r += kWarps) {
+            const int e = r / kTilePts, pp = r % kTilePts;
+            T* row = rowp[pp];
+            if (row != nullptr && lane < fill)
+                row[a.off[e] + ao0 + lane] =
+                    static_cast<T>(a.scale[e] * static_cast<double>(st[(a.comp[e] * 32 + lane) * kTileStride + pp]));
+        }
+        __syncthreads();
+    }
+    if (a.sumsq) {
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+            double v = sq[cc];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) red[warp][cc] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < 4) {
+            double v = 0.0;
+            for (int w2 = 0; w2 < kWarps; ++w2) v += red[w2][threadIdx.x];
+            if (v != 0.0) atomicAdd(&a.sumsq[threadIdx.x], v);
+        }
+    }
+}
+
+template <class T, bool GRAD, int LMAX, int PPT>
+void launch_axis_tile(const AxisTileArgs& a, cudaStream_t s) {
+    const int64_t nb = (a.n + kTilePts - 1) / kTilePts;
+    require(nb < (1ll << 31), "too many grid points for one launch");
+    constexpr size_t smem = axis_tile_smem_bytes<T, GRAD>();
+    auto kern = axis_tile_kernel<T, GRAD, LMAX, PPT>;
+    if constexpr (smem > 48 * 1024)
+        ISDF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    kern<<<static_cast<unsigned>(nb), kTilePts / 32 * PPT * 32, smem, s>>>(a);
+    ISDF_LAUNCH_CHECK();
+}
+
+template <class T, bool GRAD>
+void launch_axis_tile_l(const Context& c, const AxisTileArgs& a, cudaStream_t s) {
+    if (c.lmax <= 2) launch_axis_tile<T, GRAD, 2, 6>(a, s);
+    else if (c.lmax <= 4) launch_axis_tile<T, GRAD, 4, 2>(a, s);
+    else launch_axis_tile<T, GRAD, kMaxL, 2>(a, s);
+}
+
 template <class T, bool GRAD>
 __global__ void __launch_bounds__(kPtsPerBlock * kShellLanes)
 ao_axis_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restrict__ exps,
@@ -408,15 +528,30 @@ void eval_axis_features(const Context& c, const double* pts, const int64_t* inde
     const int64_t nb = (n + kPtsPerBlock - 1) / kPtsPerBlock;
     require(nb < (1ll << 31), "too many grid points for one launch");
     const bool grad = (ax.need_mask & 0xE) != 0;
-    if (grad)
+    if (n > 2048) {
+        // tiled: contiguous row stores per (axis entry, point) and K-chunk
+        AxisTileArgs ta{c.d_shells, exps_of<T>(c), coefs_of<T>(c), c.d_pieces, c.d_piece_begin, c.d_fill,
+                        c.d_chunk_ao0, c.nchunks, pts, index, n, weights, out, ld, sumsq, 0, {}, {}, {}};
+        for (int e = 0; e < ax.naxes; ++e) {
+            if (ax.occ[e]) continue;
+            ta.comp[ta.nent] = ax.comp[e];
+            ta.off[ta.nent] = ax.offset[e];
+            ta.scale[ta.nent] = ax.scale[e];
+            ++ta.nent;
+        }
+        if (grad) launch_axis_tile_l<T, true>(c, ta, s);
+        else launch_axis_tile_l<T, false>(c, ta, s);
+    } else if (grad) {
         ao_axis_kernel<T, true><<<static_cast<unsigned>(nb), block, 0, s>>>(
             c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, index, n, ax,
             out, ld, sumsq, weights, c.nao);
-    else
+        ISDF_LAUNCH_CHECK();
+    } else {
         ao_axis_kernel<T, false><<<static_cast<unsigned>(nb), block, 0, s>>>(
             c.d_shells, c.nshell, exps_of<T>(c), coefs_of<T>(c), pts, index, n, ax,
             out, ld, sumsq, weights, c.nao);
-    ISDF_LAUNCH_CHECK();
+        ISDF_LAUNCH_CHECK();
+    }
     if (!ax.has_occ) return;
     // occupied-orbital entries: psi = Phi C_occ (anchor_select_impl.hpp:69-72),
     // from the AO values of the same points, then scaled (sumsq slot 4)

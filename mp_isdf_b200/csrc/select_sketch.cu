@@ -471,6 +471,42 @@ __global__ void combine_sketch_kernel(const double* __restrict__ P, int naxes, i
     if (!ok) atomicOr(bad, 1);
 }
 
+// The same combine for blocks of kCombinePts points: their projections (one
+// contiguous block of P) are staged in shared memory, so the loads are
+// coalesced and consecutive threads write consecutive columns of a sketch row.
+constexpr int kCombinePts = 16;
+
+__global__ void __launch_bounds__(256)
+combine_sketch_tiled_kernel(const double* __restrict__ P, int naxes, int64_t ell,
+                            const double* __restrict__ scales, const double* __restrict__ w,
+                            const int64_t* __restrict__ index, int64_t n, double* __restrict__ Yt,
+                            int64_t ldy, int* __restrict__ bad) {
+    extern __shared__ double sP[];
+    const int64_t width = naxes * 2 * ell;
+    const int64_t g0 = static_cast<int64_t>(blockIdx.x) * kCombinePts;
+    const int64_t np = min(static_cast<int64_t>(kCombinePts), n - g0);
+    for (int64_t i = threadIdx.x; i < np * width; i += blockDim.x) sP[i] = P[g0 * width + i];
+    __syncthreads();
+    bool ok = true;
+    const double inv_sqrt_ell = 1.0 / sqrt(static_cast<double>(ell));
+    for (int64_t i = threadIdx.x; i < kCombinePts * ell; i += blockDim.x) {
+        const int64_t sidx = i / kCombinePts, pp = i % kCombinePts;
+        if (pp >= np) continue;
+        const int64_t g = g0 + pp;
+        const double* pg = sP + pp * width;
+        double left = 0, right = 0;
+        for (int a = 0; a < naxes; ++a) {
+            const double sc = scales ? scales[a] : 1.0;
+            left += sc * pg[a * 2 * ell + sidx];
+            right += sc * pg[a * 2 * ell + ell + sidx];
+        }
+        const double y = sqrt(fabs(w[index[g]])) * inv_sqrt_ell * left * right;
+        ok = ok && isfinite(y);
+        Yt[sidx * ldy + g] = y;
+    }
+    if (!ok) atomicOr(bad, 1);
+}
+
 }  // namespace
 
 void sketch_fp64(const Context& c, const double* pts, const KeptPoints& kp, const double* w,
@@ -525,9 +561,15 @@ void sketch_fp64(const Context& c, const double* pts, const KeptPoints& kp, cons
     DeviceBuffer<int> bad(1, s);
     bad.zero(s);
     ISDF_PROFILE("sketch_combine", s);
-    combine_sketch_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(
-        P.get(), naxes, ell, naxes > 1 ? dscales.get() : nullptr, w, kp.index.get(), n, Yt, ldy,
-        bad.get());
+    const size_t csmem = static_cast<size_t>(kCombinePts) * naxes * 2 * ell * sizeof(double);
+    if (csmem <= 48 * 1024) {
+        combine_sketch_tiled_kernel<<<static_cast<unsigned>((n + kCombinePts - 1) / kCombinePts), 256, csmem, s>>>(
+            P.get(), naxes, ell, naxes > 1 ? dscales.get() : nullptr, w, kp.index.get(), n, Yt, ldy, bad.get());
+    } else {
+        combine_sketch_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(
+            P.get(), naxes, ell, naxes > 1 ? dscales.get() : nullptr, w, kp.index.get(), n, Yt, ldy,
+            bad.get());
+    }
     ISDF_LAUNCH_CHECK();
     int hbad = 0;
     ISDF_CUDA(cudaMemcpyAsync(&hbad, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
