@@ -146,6 +146,76 @@ __device__ __forceinline__ void eval_shell_rel(const ShellDesc& b, T x, T y, T z
     }
 }
 
+// ---- packed pieces (FP32, the fused projection) -----------------------------------
+// A piece's primitives come as one float4 (alpha, c_j, c_j+1, c_j+2) per
+// primitive and group of three contractions, so one 16-byte load feeds the
+// exponential and up to three radial sums.  `sink.put<C>(ao, v)` receives the
+// AO index relative to the piece's first AO.
+template <int L, bool GRAD, int NG, class Sink>
+__device__ __forceinline__ void eval_piece_group(const SphPoly<float, L, GRAD>& poly, float x, float y, float z,
+                                                 float r2, const float4* __restrict__ pr, int nprim, int ng,
+                                                 int ao_rel0, Sink& sink) {
+    constexpr int NS = 2 * L + 1;
+    float R[NG], Rp[NG];
+#pragma unroll
+    for (int j = 0; j < NG; ++j) { R[j] = 0.f; Rp[j] = 0.f; }
+#pragma unroll 2
+    for (int p = 0; p < nprim; ++p) {
+        const float4 q = __ldg(pr + p);
+        const float arg = q.x * r2;
+        if (arg > static_cast<float>(kExpCut)) continue;
+        const float e = __expf(-arg);
+        const float cc[3] = {q.y, q.z, q.w};
+#pragma unroll
+        for (int j = 0; j < NG; ++j) {
+            const float c = cc[j] * e;
+            R[j] += c;
+            if constexpr (GRAD) Rp[j] -= q.x * c;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NG; ++j)
+        if (NG == 1 || j < ng) {
+            const int ao0 = ao_rel0 + j * NS;
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                sink.template put<0>(ao0 + s, R[j] * poly.v[s]);
+                if constexpr (GRAD) {
+                    const float two_rp = 2.f * Rp[j] * poly.v[s];
+                    sink.template put<1>(ao0 + s, R[j] * poly.vx[s] + x * two_rp);
+                    sink.template put<2>(ao0 + s, R[j] * poly.vy[s] + y * two_rp);
+                    sink.template put<3>(ao0 + s, R[j] * poly.vz[s] + z * two_rp);
+                }
+            }
+        }
+}
+
+template <int L, bool GRAD, class Sink>
+__device__ __forceinline__ void eval_piece_core(float x, float y, float z, float r2, const float4* __restrict__ pr,
+                                                int nprim, int nc, Sink& sink) {
+    const SphPoly<float, L, GRAD> poly(x, y, z);
+    if (nc == 1) {
+        eval_piece_group<L, GRAD, 1>(poly, x, y, z, r2, pr, nprim, 1, 0, sink);
+        return;
+    }
+    for (int g0 = 0; g0 < nc; g0 += 3, pr += nprim)
+        eval_piece_group<L, GRAD, 3>(poly, x, y, z, r2, pr, nprim, min(3, nc - g0), g0 * (2 * L + 1), sink);
+}
+
+template <bool GRAD, int LMAX, class Sink>
+__device__ __forceinline__ void eval_piece(int l, float x, float y, float z, float r2, const float4* pr, int nprim,
+                                           int nc, Sink& sink) {
+    switch (l) {
+    case 0: eval_piece_core<0, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    case 1: if constexpr (LMAX >= 1) eval_piece_core<1, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    case 2: if constexpr (LMAX >= 2) eval_piece_core<2, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    case 3: if constexpr (LMAX >= 3) eval_piece_core<3, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    case 4: if constexpr (LMAX >= 4) eval_piece_core<4, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    case 5: if constexpr (LMAX >= 5) eval_piece_core<5, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    default: if constexpr (LMAX >= 6) eval_piece_core<6, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    }
+}
+
 // Same, from FP64 offsets: r2 is formed in FP64 and rounded once to T.
 template <class T, bool GRAD, int LMAX = kMaxL, class Sink>
 __device__ __forceinline__ void eval_shell_any(const ShellDesc& b, double dx, double dy, double dz,

@@ -33,6 +33,8 @@ Context::~Context() {
     cudaFree(d_fill);
     cudaFree(d_chunk_ao0);
     cudaFree(d_ao_slot);
+    cudaFree(d_piece_rec);
+    cudaFree(d_piece_prim);
     cudaFree(ws);
 }
 
@@ -47,6 +49,7 @@ void upload_shell_centres(Context& c) {
     }
     ISDF_CUDA(cudaMemcpy(c.d_shell_hi, hi.data(), hi.size() * sizeof(float4), cudaMemcpyHostToDevice));
     ISDF_CUDA(cudaMemcpy(c.d_shell_lo, lo.data(), lo.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    if (c.d_piece_rec) upload_piece_records(c);   // the piece records carry the centres too
 }
 
 uint8_t* Context::workspace(size_t bytes) const {
@@ -123,6 +126,8 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
         ISDF_CUDA(cudaMemcpy(dst, src.data(), src.size() * sizeof(V), cudaMemcpyHostToDevice));
     };
     std::vector<float> expf_(exps.begin(), exps.end()), coeff_(coefs.begin(), coefs.end());
+    c->h_expf = expf_;
+    c->h_coeff = coeff_;
     up(c->d_shells, c->shells);
     up(c->d_exp, exps);
     up(c->d_coef, coefs);

@@ -145,6 +145,15 @@ struct Context {
     int* d_fill = nullptr;                // used slots per chunk
     int* d_chunk_ao0 = nullptr;           // first AO of each chunk (a chunk is a contiguous AO range)
     int2* d_ao_slot = nullptr;            // (chunk, slot) of each AO
+    // Packed piece records of the fused kernel, in the order of d_pieces: per
+    // piece three float4 -- (x_hi, y_hi, z_hi, amin), (x_lo, y_lo, z_lo,
+    // prim_off as bits), (l, nprim, contractions, first slot as int bits) --
+    // and per piece, group of three contractions and primitive one float4
+    // (alpha, c_j, c_j+1, c_j+2) at prim_off (FP32, zero-padded contractions).
+    float4* d_piece_rec = nullptr;
+    float4* d_piece_prim = nullptr;
+    std::vector<int4> h_pieces;           // host copy of the pieces
+    std::vector<float> h_expf, h_coeff;   // host FP32 exponents / coefficients (shell order)
     // Grow-only device workspace of the fused selection + fit (the stored AO
     // tiles and the sketch projections), kept across calls so that repeated
     // calls allocate nothing large; a call holds ws_mu while it uses it.
@@ -157,8 +166,11 @@ struct Context {
     ~Context();
 };
 
-// Copies the shells' centres (FP32 hi + lo) and smallest exponents to the device.
+// Copies the shells' centres (FP32 hi + lo) and smallest exponents to the device
+// (and refreshes the packed piece records, which hold them too).
 void upload_shell_centres(Context& c);
+// (Re)writes the packed piece records and primitive table (d_piece_rec/prim).
+void upload_piece_records(Context& c);
 // Fills the context's K-chunk layout (defined with the projection kernel).
 void build_chunk_layout(Context& c);
 // Producer lanes per point of the projection kernel for a basis' largest l.

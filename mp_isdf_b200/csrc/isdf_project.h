@@ -9,6 +9,8 @@ struct ProjectArgs {
     const ShellDesc* shells;
     const float4* shell_hi;    // (x_hi, y_hi, z_hi, amin) per shell
     const float4* shell_lo;    // (x_lo, y_lo, z_lo, 0) per shell
+    const float4* piece_rec;   // packed piece records (Context::d_piece_rec)
+    const float4* piece_prim;  // packed primitives (Context::d_piece_prim)
     const float* expf_;
     const float* coeff_;
     float* point_sq;           // [n][4] per-point sums of squares per component, or null

@@ -38,6 +38,12 @@ namespace isdf {
 
 namespace {
 
+inline float __int_as_float_host(int v) {
+    float f;
+    std::memcpy(&f, &v, sizeof(f));
+    return f;
+}
+
 constexpr int kRows = 128;            // points per tile (UMMA M)
 constexpr int kChunk = 32;            // AO slots per K-chunk
 constexpr uint32_t kTileA = kRows * kChunk * 2;       // bytes of one BF16 A tile (8 KB)
@@ -217,10 +223,12 @@ project_tc_kernel(ProjectArgs args) {
                 float csq[4] = {0.f, 0.f, 0.f, 0.f};
                 if (valid) {
                     for (int pi = pb; pi < pe; ++pi) {
-                        const int4 pc = args.pieces[pi];
-                        const float4 ch = args.shell_hi[pc.x], cl = args.shell_lo[pc.x];
-                        const ShellDesc b = args.shells[pc.x];
-                        const int ns = 2 * b.l + 1;
+                        // one packed record per piece: centre (hi, lo), smallest exponent,
+                        // primitive offset, l, primitive and contraction counts, first slot
+                        const float4 ch = __ldg(args.piece_rec + 3 * pi), cl = __ldg(args.piece_rec + 3 * pi + 1);
+                        const int4 meta = __ldg(reinterpret_cast<const int4*>(args.piece_rec) + 3 * pi + 2);
+                        const int l = meta.x, nprim = meta.y, nc = meta.z, slot0 = meta.w;
+                        const int ns = 2 * l + 1;
                         const float dx = (pxh - ch.x) + (pxl - cl.x);
                         const float dy = (pyh - ch.y) + (pyl - cl.y);
                         const float dz = (pzh - ch.z) + (pzl - cl.z);
@@ -231,14 +239,14 @@ project_tc_kernel(ProjectArgs args) {
                         // only when it holds for the whole warp (no divergent paths)
                         if (__all_sync(__activemask(), ch.w * r2 > static_cast<float>(kExpCut))) {
                             // every primitive is cut off: the piece is exactly zero here
-                            for (int k = pc.w; k < pc.w + pc.z * ns; ++k)
+                            for (int k = slot0; k < slot0 + nc * ns; ++k)
 #pragma unroll
                                 for (int cc = 0; cc < kNComp; ++cc) sStage[(cc * kChunk + k) * kRows + p] = 0.f;
                             continue;
                         }
-                        StageSink sink{sStage, p, pc.w - (b.ao_off + pc.y * ns), {0.f, 0.f, 0.f, 0.f}};
-                        eval_shell_rel<float, GRAD, LMAX>(b, dx, dy, dz, r2, args.expf_, args.coeff_, sink,
-                                                          pc.y, pc.y + pc.z);
+                        StageSink sink{sStage, p, slot0, {0.f, 0.f, 0.f, 0.f}};
+                        eval_piece<GRAD, LMAX>(l, dx, dy, dz, r2, args.piece_prim + __float_as_int(cl.w), nprim, nc,
+                                               sink);
 #pragma unroll
                         for (int cc = 0; cc < 4; ++cc) csq[cc] += sink.sq[cc];
                     }
@@ -486,12 +494,44 @@ void build_chunk_layout(Context& c) {
         ISDF_CUDA(cudaMemcpy(dst, src.data(), src.size() * sizeof(V), cudaMemcpyHostToDevice));
     };
     up(c.d_pieces, pieces);
+    c.h_pieces = pieces;
+    upload_piece_records(c);
     up(c.d_piece_begin, lane_begin);
     up(c.d_fill, fill);
     std::vector<int> ao0(fill.size(), 0);
     for (size_t i = 1; i < fill.size(); ++i) ao0[i] = ao0[i - 1] + fill[i - 1];
     up(c.d_chunk_ao0, ao0);
     up(c.d_ao_slot, ao_slot);
+}
+
+void upload_piece_records(Context& c) {
+    std::vector<float4> rec, prim;
+    rec.reserve(c.h_pieces.size() * 3);
+    for (const int4& pc : c.h_pieces) {
+        const ShellDesc& sh = c.shells[pc.x];
+        const float xh = static_cast<float>(sh.x), yh = static_cast<float>(sh.y), zh = static_cast<float>(sh.z);
+        const int off = static_cast<int>(prim.size());
+        rec.push_back(make_float4(xh, yh, zh, sh.amin));
+        rec.push_back(make_float4(static_cast<float>(sh.x - xh), static_cast<float>(sh.y - yh),
+                                  static_cast<float>(sh.z - zh), __int_as_float_host(off)));
+        int4 meta = make_int4(sh.l, sh.nprim, pc.z, pc.w);
+        float4 mf;
+        std::memcpy(&mf, &meta, sizeof(mf));
+        rec.push_back(mf);
+        for (int g0 = 0; g0 < pc.z; g0 += 3)
+            for (int p = 0; p < sh.nprim; ++p) {
+                float cc[3] = {0.f, 0.f, 0.f};
+                for (int j = 0; j < 3 && g0 + j < pc.z; ++j)
+                    cc[j] = c.h_coeff[sh.coef_off + (pc.y + g0 + j) * sh.nprim + p];
+                prim.push_back(make_float4(c.h_expf[sh.prim_off + p], cc[0], cc[1], cc[2]));
+            }
+    }
+    if (rec.empty()) rec.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
+    if (prim.empty()) prim.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
+    if (!c.d_piece_rec) ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c.d_piece_rec), rec.size() * sizeof(float4)));
+    if (!c.d_piece_prim) ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c.d_piece_prim), prim.size() * sizeof(float4)));
+    ISDF_CUDA(cudaMemcpy(c.d_piece_rec, rec.data(), rec.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    ISDF_CUDA(cudaMemcpy(c.d_piece_prim, prim.data(), prim.size() * sizeof(float4), cudaMemcpyHostToDevice));
 }
 
 namespace {
@@ -571,6 +611,8 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     a.shells = c.d_shells;
     a.shell_hi = c.d_shell_hi;
     a.shell_lo = c.d_shell_lo;
+    a.piece_rec = c.d_piece_rec;
+    a.piece_prim = c.d_piece_prim;
     a.expf_ = c.d_expf;
     a.coeff_ = c.d_coeff;
     a.point_sq = point_sq;
