@@ -313,6 +313,20 @@ int isdf_grid_metric_host(isdf_ctx* ctx, const double* left_host, int64_t kl, co
                           int64_t kr, const double* xyz_host, const double* w_host, int64_t n,
                           int32_t symmetrize, double* metric_host);
 
+/* ---- ISDF Coulomb and exchange matrices --------------------------------------
+ * Replaces evaluate_isdf_jk (python/isdf.py:130-151):
+ *   (mu nu|lam sig) ~ sum_pq X[p,mu] X[p,nu] Z[p,q] X[q,lam] X[q,sig],
+ *   J = X^T diag(Z diag(X D X^T)) X,  K = X^T (Z o (X D X^T)) X,
+ * both symmetrised, (A + A^T)/2.  x: k x nao anchor AO values, z: k x k
+ * metric (already carrying both anchors' quadrature weights), dm: nao x nao
+ * (symmetric; validated by the caller), j / k_out: nao x nao, either may be
+ * NULL.  FP64 tensor-core GEMMs.  The device variant takes device pointers
+ * and a stream; the _host variant host buffers. */
+int isdf_jk(isdf_ctx* ctx, const double* x_dev, int64_t k, const double* z_dev, const double* dm_dev,
+            double* j_dev, double* k_out_dev, void* stream);
+int isdf_jk_host(isdf_ctx* ctx, const double* x_host, int64_t k, const double* z_host, const double* dm_host,
+                 double* j_host, double* k_out_host);
+
 /* ---- RBRP (robust blockwise random pivoting) ---------------------------------
  * Replaces rbrp_ao_cpu / rbrp_ao_device (cpp/src/anchor_select_rbrp.cpp:195-320,
  * cpp/src/anchor_select_rbrp_device.cpp, cpp/src/anchor_select_pybind.cpp:68-140):

@@ -26,7 +26,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
                      "--expt-relaxed-constexpr", "-I", str(ROOT / "include"), "-I", str(CSRC)]
 CU_SOURCES = ["context.cu", "linalg.cu", "select_sketch.cu", "select_pairqr.cu", "fit.cu",
               "capi.cu", "profile.cu", "qrcp_sketch.cu", "project_tc.cu",
-              "adjoint.cu", "noalloc.cu", "gram_tiles.cu", "metric.cu", "rbrp.cu"]
+              "adjoint.cu", "noalloc.cu", "gram_tiles.cu", "metric.cu", "rbrp.cu", "jk.cu"]
 LIB = PKG / "libisdf_b200.so"
 EXT_SUFFIX = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
 PYMOD = PKG / f"mp_isdf{EXT_SUFFIX}"

@@ -32,7 +32,7 @@ SYMBOLS = [
     "isdf_rbrp_args_default", "isdf_rbrp_ao", "isdf_rbrp_points", "isdf_rbrp_result_info",
     "isdf_rbrp_result_copy", "isdf_rbrp_result_free",
     "isdf_sketch_shard_project", "isdf_sketch_shard_combine", "isdf_sketch_shard_free",
-    "isdf_sketch_select_gathered", "isdf_fit_at",
+    "isdf_sketch_select_gathered", "isdf_fit_at", "isdf_jk", "isdf_jk_host",
 ]
 
 ALGORITHMS = {"qrcp_dense": 0, "qrcp_online": 1, "rand_sketch": 2, "rand_sketch_density": 4,
@@ -137,6 +137,8 @@ def lib():
         L.isdf_sketch_factors.argtypes = [I64, I64, ctypes.c_uint64, P, P]
         L.isdf_grid_metric.argtypes = [P, P, I64, I64, P, I64, I64, P, P, I64, I32, P, P]
         L.isdf_grid_metric_host.argtypes = [P, P, I64, P, I64, P, P, I64, I32, P]
+        L.isdf_jk.argtypes = [P, P, I64, P, P, P, P, P]
+        L.isdf_jk_host.argtypes = [P, P, I64, P, P, P, P]
         L.isdf_profile_read.argtypes = [I32, P, P, P, ctypes.POINTER(I32)]
         _lib = L
     return _lib

@@ -686,6 +686,39 @@ int isdf_grid_metric_host(isdf_ctx* ctx, const double* left, int64_t kl, const d
     });
 }
 
+int isdf_jk(isdf_ctx* ctx, const double* x, int64_t k, const double* z, const double* dm, double* j,
+            double* kout, void* stream) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        if (k < 0) isdf::fail(isdf::kInvalid, "invalid anchor count");
+        if ((k > 0 && (!x || !z)) || (c.nao > 0 && !dm)) isdf::fail(isdf::kInvalid, "null J/K input");
+        isdf::isdf_jk_device(c.nao, k, x, z, dm, j, kout, as_stream(stream));
+    });
+}
+
+int isdf_jk_host(isdf_ctx* ctx, const double* x, int64_t k, const double* z, const double* dm, double* j,
+                 double* kout) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        if (k < 0) isdf::fail(isdf::kInvalid, "invalid anchor count");
+        if ((k > 0 && (!x || !z)) || (c.nao > 0 && !dm)) isdf::fail(isdf::kInvalid, "null J/K input");
+        cudaStream_t s = ctx->stream;
+        const int64_t nao = c.nao;
+        isdf::DeviceBuffer<double> dx, dz, dd, dj(static_cast<size_t>(j ? nao * nao : 0), s),
+            dk(static_cast<size_t>(kout ? nao * nao : 0), s);
+        upload(dx, x, static_cast<size_t>(k * nao), s);
+        upload(dz, z, static_cast<size_t>(k * k), s);
+        upload(dd, dm, static_cast<size_t>(nao * nao), s);
+        isdf::isdf_jk_device(nao, k, dx.get(), dz.get(), dd.get(), j ? dj.get() : nullptr,
+                             kout ? dk.get() : nullptr, s);
+        if (j) ISDF_CUDA(cudaMemcpyAsync(j, dj.get(), nao * nao * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (kout) ISDF_CUDA(cudaMemcpyAsync(kout, dk.get(), nao * nao * sizeof(double), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 struct isdf_rbrp_result {
     isdf::RbrpResult r;
     int64_t n = 0, nao = 0;

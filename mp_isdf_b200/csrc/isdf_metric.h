@@ -14,4 +14,9 @@ void grid_metric(const double* left, int64_t ldl, int kl, const double* right, i
                  const double* xyz, const double* w, int64_t n, bool symmetrize, double* metric_host,
                  cudaStream_t s);
 
+// ISDF J and K of a density matrix on the device (X: k x nao anchor AO values,
+// Z: k x k metric, D: nao x nao; J, K: nao x nao, symmetrised; either may be null).
+void isdf_jk_device(int64_t nao, int64_t k, const double* X, const double* Z, const double* D, double* J,
+                    double* K, cudaStream_t s);
+
 }  // namespace isdf

@@ -213,11 +213,18 @@ project_tc_kernel(ProjectArgs args) {
                 count = args.sumsq && (args.weights == nullptr || args.weights[gi] != 0.0);
             }
             float psq[4] = {0.f, 0.f, 0.f, 0.f};
+            // the chunk's piece range and fill are read one chunk ahead
+            int pb_n = args.lane_begin[lanegrp], pe_n = args.lane_begin[lanegrp + 1], fill_n = args.chunk_fill[0];
             for (int c = 0; c < nchunks; ++c, ++q) {
                 float* sStage = sStage0 + (q & 1) * (SM::kStage / 4);
+                const int pb = pb_n, pe = pe_n, fill = fill_n;
+                if (c + 1 < nchunks) {
+                    pb_n = __ldg(args.lane_begin + (c + 1) * PPT + lanegrp);
+                    pe_n = __ldg(args.lane_begin + (c + 1) * PPT + lanegrp + 1);
+                    fill_n = __ldg(args.chunk_fill + c + 1);
+                }
                 // 1. evaluate this chunk's pieces into the FP32 staging buffer
-                const int pb = args.lane_begin[c * PPT + lanegrp], pe = args.lane_begin[c * PPT + lanegrp + 1];
-                for (int k = (valid ? args.chunk_fill[c] : 0) + lanegrp; k < kChunk; k += PPT)
+                for (int k = (valid ? fill : 0) + lanegrp; k < kChunk; k += PPT)
 #pragma unroll
                     for (int cc = 0; cc < kNComp; ++cc) sStage[(cc * kChunk + k) * kRows + p] = 0.f;
                 float csq[4] = {0.f, 0.f, 0.f, 0.f};

@@ -318,6 +318,24 @@ PYBIND11_MODULE(mp_isdf, m) {
                                         const FloatArray& weights) {
         return metric(left, right, coords, weights);
     }, py::arg("left"), py::arg("right"), py::arg("coords"), py::arg("weights"));
+    // ISDF J and K (python/isdf.py:130-151) on the device: x k x nao anchor AO
+    // values, z k x k metric, dm nao x nao (symmetric)
+    m.def("isdf_jk", [](Context& c, const FloatArray& x, const FloatArray& z, const FloatArray& dm) {
+        if (x.ndim() != 2 || x.shape(1) != c.nao) throw std::invalid_argument("X must have shape (k, nao)");
+        const int64_t k = x.shape(0);
+        if (z.ndim() != 2 || z.shape(0) != k || z.shape(1) != k)
+            throw std::invalid_argument("Coulomb metric has the wrong anchor dimensions");
+        if (dm.ndim() != 2 || dm.shape(0) != c.nao || dm.shape(1) != c.nao)
+            throw std::invalid_argument("dm must be a finite AO density matrix of shape (nao,nao)");
+        py::array_t<double> j({c.nao, c.nao}), kk({c.nao, c.nao});
+        int rc;
+        {
+            py::gil_scoped_release release;
+            rc = isdf_jk_host(c.h, x.data(), k, z.data(), dm.data(), j.mutable_data(), kk.mutable_data());
+        }
+        check(rc);
+        return py::make_tuple(j, kk);
+    }, py::arg("context"), py::arg("x"), py::arg("z"), py::arg("dm"));
     // RBRP (cpp/src/anchor_select_pybind.cpp:68-140): result dict in the reference's layout
     auto rbrp_dict = [](isdf_rbrp_result* h, bool compute_id) {
         struct Free { isdf_rbrp_result* h; ~Free() { isdf_rbrp_result_free(h); } } guard{h};

@@ -108,7 +108,8 @@ def evaluate_isdf_jk(result, dm):
     """Return (J, K) for a real symmetric AO density matrix
     (``python/isdf.py:130-151``).  The metric in `result` already includes both
     anchor quadrature weights; (mu nu|lam sig) is approximated by
-    sum_pq X[p,mu] X[p,nu] Z[p,q] X[q,lam] X[q,sig] with X[p,mu] = AO_mu(anchor_p)."""
+    sum_pq X[p,mu] X[p,nu] Z[p,q] X[q,lam] X[q,sig] with X[p,mu] = AO_mu(anchor_p); J and K
+    are built on the B200 (mp_isdf.isdf_jk: FP64 tensor-core GEMMs)."""
     x = np.asarray(result["X1"])
     z = result["coulomb_metric"]
     if z is None:
@@ -120,10 +121,11 @@ def evaluate_isdf_jk(result, dm):
         raise ValueError("dm must be symmetric")
     if np.shape(z) != (len(x), len(x)):
         raise ValueError("Coulomb metric has the wrong anchor dimensions")
-    anchor_density = x @ density @ x.T
-    coulomb = x.T @ ((z @ np.diag(anchor_density))[:, None] * x)
-    exchange = x.T @ (z * anchor_density) @ x
-    return 0.5 * (coulomb + coulomb.T), 0.5 * (exchange + exchange.T)
+    context = result.get("context")
+    if context is None:
+        raise ValueError("the ISDF result carries no AO context")
+    return mp_isdf.isdf_jk(context, np.ascontiguousarray(x), np.ascontiguousarray(z, dtype=np.float64),
+                           np.ascontiguousarray(density))
 
 
 def _validate_point_importance(importance, ngrid):
@@ -429,7 +431,7 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
             "coordinates": coords, "weights": weights, "interp_vecs": interp_vecs,
             "overlap_reconstruction": overlap_approx,
             "overlap_relative_error": overlap_relative_error,
-            "pair_space_errors": pair_space_errors, "X1": anchor_ao,
+            "pair_space_errors": pair_space_errors, "X1": anchor_ao, "context": context,
             "elapsed": last - started, "timings": timings}
 
 

@@ -172,3 +172,40 @@ def test_driver_metric_and_jk(grid):
         isdf.build_isdf(M, anchor_rank=8, grid=(pts, w), compute_metric=True, metric_algorithm="unblocked_greedy")
     with pytest.raises(ValueError, match="symmetric"):
         isdf.evaluate_isdf_jk(res, dm + np.triu(np.ones_like(dm), 1))
+
+
+@pytest.mark.gpu
+def test_isdf_jk_device_matches_oracle():
+    """mp_isdf.isdf_jk (FP64 tensor-core GEMMs on the device) against the
+    oracle's NumPy restatement of evaluate_isdf_jk (python/isdf.py:130-151),
+    for anchor counts 1, 8, 37 (ragged GEMM tiles) and the device C-ABI."""
+    import ctypes
+    import mp_isdf
+    import torch
+    from mp_isdf_b200 import capi, inputs
+    symbols, xyz = inputs.water_cluster((2, 1, 1), seed=2)
+    t = inputs.build_tables(symbols, xyz)
+    c = mp_isdf.LibcintContext(t.atm, t.bas, t.env)
+    rng = np.random.default_rng(9)
+    for k in (1, 8, 37):
+        x = rng.normal(size=(k, t.nao))
+        z = rng.normal(size=(k, k))
+        z = z + z.T
+        dm = rng.normal(size=(t.nao, t.nao))
+        dm = dm + dm.T
+        j, kk = mp_isdf.isdf_jk(c, x, z, dm)
+        jr, kr = O.isdf_jk(x, z, dm)
+        np.testing.assert_allclose(j, jr, rtol=1e-12, atol=1e-12 * np.abs(jr).max())
+        np.testing.assert_allclose(kk, kr, rtol=1e-12, atol=1e-12 * np.abs(kr).max())
+        assert np.array_equal(j, j.T) and np.array_equal(kk, kk.T)
+    # device pointers through the C-ABI, K only
+    ctx = capi.Context(t.atm, t.bas, t.env)
+    dx, dz, dd = (torch.tensor(a, device="cuda") for a in (x, z, dm))
+    kd = torch.empty(t.nao, t.nao, dtype=torch.float64, device="cuda")
+    P = ctypes.c_void_p
+    capi.check(capi.lib().isdf_jk(ctx.h, P(dx.data_ptr()), len(x), P(dz.data_ptr()), P(dd.data_ptr()), None,
+                                  P(kd.data_ptr()), P(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(kd.cpu().numpy(), kr, rtol=1e-12, atol=1e-12 * np.abs(kr).max())
+    with pytest.raises(ValueError):
+        mp_isdf.isdf_jk(c, x[:, :-1], z, dm)
