@@ -227,6 +227,46 @@ int isdf_sketch_shard_combine(isdf_sketch_shard* shard, const double* sumsq_glob
                               double* delta_dev, int64_t* kept_dev, double* kept_xyz_dev,
                               double* kept_w_dev, double* scales_host, void* stream);
 void isdf_sketch_shard_free(isdf_sketch_shard* shard);
+/* Distributed pivoted QR of the sketch: each rank keeps its own columns
+ * (yt_dev: ell x n_local from isdf_sketch_shard_combine) and the ranks
+ * exchange only per-step keys and the winning column (instead of gathering
+ * the whole sketch).  pos_offset: the number of kept points on lower ranks
+ * (global positions of this rank's columns start there); n_total: all
+ * ranks' kept points.  Per step j = 0 .. ell-1, on every rank:
+ *  a. isdf_qr_shard_update(j): applies reflector j-1; returns this rank's
+ *     share of row j-1's energy and either its best key (value = squared
+ *     trailing norm, global position, local column; value -1: none) or, in
+ *     the mixed form (verified = 1), its best lower bound;
+ *  b. mixed form only: the global maximum of the bounds, then
+ *     isdf_qr_shard_verify(j, bound) returns the key (candidates recomputed
+ *     exactly in FP64);
+ *  c. the global best key (largest value, ties to the smaller position); its
+ *     owner reads the column (isdf_qr_shard_column, ell rows) for all ranks;
+ *  d. isdf_qr_shard_pivot(j, rows, ...) with pivot_col / moved_col the local
+ *     pivot column and the local column at position j (-1 on other ranks);
+ *     returns R_jj.
+ * A final isdf_qr_shard_update(ell) returns the last row's energy shares.
+ * isdf_sketch_rank applies the tail / numerical-rank / exact-rank rules
+ * (cpp/src/anchor_select_randomized_id.cpp:320-374) to the per-step |R_jj|
+ * and row energies (summed over ranks, plus R_jj^2).  Same pivots as
+ * isdf_sketch_select_gathered. */
+typedef struct isdf_qr_shard isdf_qr_shard;
+int isdf_qr_shard_create(isdf_ctx* ctx, const isdf_select_args* args, double* yt_dev, int64_t n_local,
+                         int64_t n_total, int64_t pos_offset, const double* kept_xyz_dev, const double* kept_w_dev,
+                         double* delta_dev, const double* scales_host, isdf_qr_shard** out, int64_t* ell,
+                         int32_t* verified, void* stream);
+int isdf_qr_shard_update(isdf_qr_shard* h, int64_t j, double* key_value, int64_t* key_pos, int64_t* key_col,
+                         double* energy_part, double* lower_bound);
+int isdf_qr_shard_verify(isdf_qr_shard* h, int64_t j, double lower_bound, double* key_value, int64_t* key_pos,
+                         int64_t* key_col);
+int isdf_qr_shard_column(isdf_qr_shard* h, int64_t col, double* rows_host);
+int isdf_qr_shard_pivot(isdf_qr_shard* h, int64_t j, const double* rows_host, int64_t pivot_col, int64_t pivot_pos,
+                        int64_t moved_col, double* r_jj);
+int isdf_qr_shard_reverified(isdf_qr_shard* h, int64_t* count);
+void isdf_qr_shard_free(isdf_qr_shard* h);
+int isdf_sketch_rank(isdf_ctx* ctx, const isdf_select_args* args, int64_t n_total, const double* diag_host,
+                     const double* energy_host, int64_t steps, int64_t* rank, int64_t* numerical_rank,
+                     double* relative_tail);
 int isdf_sketch_select_gathered(isdf_ctx* ctx, const isdf_select_args* args, double* yt_dev, int64_t n,
                                 const double* kept_xyz_dev, const double* kept_w_dev, double* delta_dev,
                                 const double* scales_host, int64_t* pivots_host, int64_t capacity,

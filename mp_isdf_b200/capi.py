@@ -33,6 +33,8 @@ SYMBOLS = [
     "isdf_rbrp_result_copy", "isdf_rbrp_result_free",
     "isdf_sketch_shard_project", "isdf_sketch_shard_combine", "isdf_sketch_shard_free",
     "isdf_sketch_select_gathered", "isdf_fit_at", "isdf_jk", "isdf_jk_host",
+    "isdf_qr_shard_create", "isdf_qr_shard_update", "isdf_qr_shard_verify", "isdf_qr_shard_column",
+    "isdf_qr_shard_pivot", "isdf_qr_shard_reverified", "isdf_qr_shard_free", "isdf_sketch_rank",
 ]
 
 ALGORITHMS = {"qrcp_dense": 0, "qrcp_online": 1, "rand_sketch": 2, "rand_sketch_density": 4,
@@ -124,6 +126,19 @@ def lib():
         L.isdf_sketch_select_gathered.argtypes = [P, ctypes.POINTER(SelectArgs), P, I64, P, P, P, P, P,
                                                   I64, ctypes.POINTER(I64), ctypes.POINTER(SelectInfo), P]
         L.isdf_fit_at.argtypes = [P, P, P, I64, P, P, I64, I32, I32, P, ctypes.POINTER(FitInfo), P, P]
+        L.isdf_qr_shard_create.argtypes = [P, ctypes.POINTER(SelectArgs), P, I64, I64, I64, P, P, P, P,
+                                           ctypes.POINTER(P), ctypes.POINTER(I64), ctypes.POINTER(I32), P]
+        L.isdf_qr_shard_update.argtypes = [P, I64, ctypes.POINTER(F64), ctypes.POINTER(I64), ctypes.POINTER(I64),
+                                           ctypes.POINTER(F64), ctypes.POINTER(F64)]
+        L.isdf_qr_shard_verify.argtypes = [P, I64, F64, ctypes.POINTER(F64), ctypes.POINTER(I64),
+                                           ctypes.POINTER(I64)]
+        L.isdf_qr_shard_column.argtypes = [P, I64, P]
+        L.isdf_qr_shard_pivot.argtypes = [P, I64, P, I64, I64, I64, ctypes.POINTER(F64)]
+        L.isdf_qr_shard_reverified.argtypes = [P, ctypes.POINTER(I64)]
+        L.isdf_qr_shard_free.argtypes = [P]
+        L.isdf_qr_shard_free.restype = None
+        L.isdf_sketch_rank.argtypes = [P, ctypes.POINTER(SelectArgs), I64, P, P, I64, ctypes.POINTER(I64),
+                                       ctypes.POINTER(I64), ctypes.POINTER(F64)]
         L.isdf_pair_error.argtypes = [P, P, P, I64, P, I64, P, ctypes.POINTER(F64),
                                       ctypes.POINTER(F64), P]
         L.isdf_pair_error_terms.argtypes = [I64, I64, P, P, P, P, P, P, P]
@@ -295,6 +310,29 @@ class Context:
         del keep
         return piv[:npiv.value].copy(), info
 
+    def qr_shard(self, yt, n_total, pos_offset, kept_xyz, kept_w, delta, scales, **kw):
+        """This rank's share of the distributed sketch QR over its columns yt
+        ([ell, n_local] device tensor)."""
+        args, keep = make_select_args(**kw)
+        h, ell, ver = P(), I64(), I32()
+        sc = _np(scales, np.float64)
+        n_local = yt.shape[1] if yt.dim() == 2 else 0
+        check(lib().isdf_qr_shard_create(self.h, ctypes.byref(args), _ptr(yt), n_local, n_total, pos_offset,
+                                         _ptr(kept_xyz), _ptr(kept_w), _ptr(delta), _ptr(sc), ctypes.byref(h),
+                                         ctypes.byref(ell), ctypes.byref(ver), _stream(yt)))
+        del keep
+        return QrShard(h.value, ell.value, bool(ver.value), (yt, kept_xyz, kept_w, delta))
+
+    def sketch_rank(self, n_total, diag, energy, **kw):
+        """(rank, numerical rank, relative tail) of a sketch QR's |R_jj| and row energies."""
+        args, keep = make_select_args(**kw)
+        d, e = _np(diag, np.float64), _np(energy, np.float64)
+        r, nr, t = I64(), I64(), F64()
+        check(lib().isdf_sketch_rank(self.h, ctypes.byref(args), n_total, _ptr(d), _ptr(e), len(d),
+                                     ctypes.byref(r), ctypes.byref(nr), ctypes.byref(t)))
+        del keep
+        return r.value, nr.value, t.value
+
     def fit_at(self, xyz, w, anchor_xyz, anchor_w, theta, precision="fp64", want_error=True):
         """Fit on device points with anchors given by coordinates; returns
         (FitInfo, [err2, exact2] of these points)."""
@@ -435,6 +473,53 @@ class Context:
                                   1 if precision == "mixed" else 0, int(want_error), _ptr(theta),
                                   ctypes.byref(info)))
         return theta[:len(a) * info.n_kept].reshape(len(a), info.n_kept), info
+
+
+class QrShard:
+    """One rank's share of the distributed sketch QR (isdf_qr_shard_*)."""
+
+    def __init__(self, h, ell, verified, keep):
+        self.h, self.ell, self.verified = h, ell, verified
+        self._keep = keep   # the device arrays the handle points at
+
+    def update(self, j):
+        v, e, lb = F64(), F64(), F64()
+        p, c = I64(), I64()
+        check(lib().isdf_qr_shard_update(self.h, j, ctypes.byref(v), ctypes.byref(p), ctypes.byref(c),
+                                         ctypes.byref(e), ctypes.byref(lb)))
+        return v.value, p.value, c.value, e.value, lb.value
+
+    def verify(self, j, bound):
+        v, p, c = F64(), I64(), I64()
+        check(lib().isdf_qr_shard_verify(self.h, j, bound, ctypes.byref(v), ctypes.byref(p), ctypes.byref(c)))
+        return v.value, p.value, c.value
+
+    def column(self, col):
+        rows = np.empty(self.ell)
+        check(lib().isdf_qr_shard_column(self.h, col, _ptr(rows)))
+        return rows
+
+    def pivot(self, j, rows, pivot_col, pivot_pos, moved_col):
+        rows = _np(rows, np.float64)
+        r = F64()
+        check(lib().isdf_qr_shard_pivot(self.h, j, _ptr(rows), pivot_col, pivot_pos, moved_col, ctypes.byref(r)))
+        return r.value
+
+    def reverified(self):
+        n = I64()
+        check(lib().isdf_qr_shard_reverified(self.h, ctypes.byref(n)))
+        return n.value
+
+    def free(self):
+        if self.h:
+            lib().isdf_qr_shard_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 class SketchShard:

@@ -952,6 +952,110 @@ int isdf_sketch_shard_combine(isdf_sketch_shard* h, const double* sumsq_global, 
 
 void isdf_sketch_shard_free(isdf_sketch_shard* h) { delete h; }
 
+struct isdf_qr_shard {
+    isdf_ctx* ctx = nullptr;
+    std::unique_ptr<isdf::SketchQrShard> sh;
+    bool verified = false;
+};
+
+int isdf_qr_shard_create(isdf_ctx* ctx, const isdf_select_args* args, double* yt, int64_t n_local, int64_t n_total,
+                         int64_t pos_offset, const double* kept_xyz, const double* kept_w, double* delta,
+                         const double* scales_host, isdf_qr_shard** out, int64_t* ell, int32_t* verified,
+                         void* stream) {
+    return guarded([&] {
+        if (!out) isdf::fail(isdf::kInvalid, "null QR shard handle");
+        *out = nullptr;
+        if (!args || !scales_host) isdf::fail(isdf::kInvalid, "invalid distributed QR arguments");
+        if (n_local > 0 && (!yt || !kept_xyz || !kept_w)) isdf::fail(isdf::kInvalid, "null distributed QR input");
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        isdf::SelectOptions o = options_of(args);
+        if (o.algorithm != ISDF_RAND_SKETCH_QUADRATURE)
+            isdf::fail(isdf::kInvalid, "grid-sharded selection supports rand_sketch (quadrature)");
+        const std::vector<double> scales(scales_host, scales_host + o.axes.size());
+        auto h = std::make_unique<isdf_qr_shard>();
+        h->ctx = ctx;
+        h->sh = isdf::make_sketch_qr_shard(c, o, yt, n_local, n_total, kept_xyz, kept_w, delta, scales, pos_offset,
+                                           as_stream(stream));
+        h->verified = delta != nullptr && h->sh->su.mixed;
+        if (ell) *ell = h->sh->su.ell;
+        if (verified) *verified = h->verified ? 1 : 0;
+        *out = h.release();
+    });
+}
+
+int isdf_qr_shard_update(isdf_qr_shard* h, int64_t j, double* key_value, int64_t* key_pos, int64_t* key_col,
+                         double* energy_part, double* lower_bound) {
+    return guarded([&] {
+        if (!h || !key_value || !key_pos || !key_col || !energy_part || !lower_bound)
+            isdf::fail(isdf::kInvalid, "null distributed QR argument");
+        DeviceGuard dg(ctx_of(h->ctx).device);
+        const isdf::QrShardKey k = h->sh->qr->update(j, energy_part, lower_bound);
+        *key_value = k.v;
+        *key_pos = k.pos;
+        *key_col = k.col;
+    });
+}
+
+int isdf_qr_shard_verify(isdf_qr_shard* h, int64_t j, double lower_bound, double* key_value, int64_t* key_pos,
+                         int64_t* key_col) {
+    return guarded([&] {
+        if (!h || !key_value || !key_pos || !key_col) isdf::fail(isdf::kInvalid, "null distributed QR argument");
+        DeviceGuard dg(ctx_of(h->ctx).device);
+        const isdf::QrShardKey k = h->sh->qr->verify(j, lower_bound);
+        *key_value = k.v;
+        *key_pos = k.pos;
+        *key_col = k.col;
+    });
+}
+
+int isdf_qr_shard_column(isdf_qr_shard* h, int64_t col, double* rows_host) {
+    return guarded([&] {
+        if (!h || !rows_host) isdf::fail(isdf::kInvalid, "null distributed QR argument");
+        DeviceGuard dg(ctx_of(h->ctx).device);
+        h->sh->qr->column(col, rows_host);
+    });
+}
+
+int isdf_qr_shard_pivot(isdf_qr_shard* h, int64_t j, const double* rows_host, int64_t pivot_col, int64_t pivot_pos,
+                        int64_t moved_col, double* r_jj) {
+    return guarded([&] {
+        if (!h || !rows_host || !r_jj) isdf::fail(isdf::kInvalid, "null distributed QR argument");
+        DeviceGuard dg(ctx_of(h->ctx).device);
+        *r_jj = h->sh->qr->pivot(j, rows_host, pivot_col, pivot_pos, moved_col);
+    });
+}
+
+int isdf_qr_shard_reverified(isdf_qr_shard* h, int64_t* count) {
+    return guarded([&] {
+        if (!h || !count) isdf::fail(isdf::kInvalid, "null distributed QR argument");
+        DeviceGuard dg(ctx_of(h->ctx).device);
+        *count = h->sh->qr->reverified();
+    });
+}
+
+void isdf_qr_shard_free(isdf_qr_shard* h) { delete h; }
+
+int isdf_sketch_rank(isdf_ctx* ctx, const isdf_select_args* args, int64_t n_total, const double* diag,
+                     const double* energy, int64_t steps, int64_t* rank, int64_t* numerical_rank,
+                     double* relative_tail) {
+    return guarded([&] {
+        if (!args || !rank || steps < 0 || (steps > 0 && (!diag || !energy)))
+            isdf::fail(isdf::kInvalid, "invalid sketch rank arguments");
+        auto& c = ctx_of(ctx);
+        isdf::SelectOptions o = options_of(args);
+        const isdf::SketchSetup su = isdf::sketch_setup(c, o, std::max<int64_t>(n_total, 1));
+        isdf::SketchQR qr;
+        qr.diag.assign(diag, diag + steps);
+        qr.energy.assign(energy, energy + steps);
+        qr.jpvt.assign(steps, 0);   // the pivots themselves are the caller's
+        const isdf::SketchRank r = isdf::sketch_rank(qr, su.ell, n_total, o, su.physical_rank);
+        *rank = r.rank;
+        if (numerical_rank) *numerical_rank = r.numerical_rank;
+        if (relative_tail) *relative_tail = r.relative_tail;
+    });
+}
+
 int isdf_sketch_select_gathered(isdf_ctx* ctx, const isdf_select_args* args, double* yt, int64_t n,
                                 const double* kept_xyz, const double* kept_w, double* delta,
                                 const double* scales_host, int64_t* pivots, int64_t capacity,

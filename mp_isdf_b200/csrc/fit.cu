@@ -510,10 +510,6 @@ __global__ void anchor_slot_image_kernel(const double* __restrict__ phi_a, int k
     img[i] = (j < fill[c] && ao < nao) ? phi_a[static_cast<int64_t>(a) * nao + ao] : 0.0;
 }
 
-__device__ __forceinline__ double bf16_bits_to_double(uint32_t bits16) {
-    return static_cast<double>(__uint_as_float(bits16 << 16));
-}
-
 // H[g][a0 + a] = (sum_mu x[g][mu] phi_{a0+a}(mu))^2 for a < KMAX, a0 + a < k, with
 // x = hi + lo + r from the stored tiles (FP64 FMAs); q[g] = sum_mu x^2 when a0 == 0.
 // One 128-point tile per block of 64 threads: thread t takes rows t and t + 64,

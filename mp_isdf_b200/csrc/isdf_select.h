@@ -3,6 +3,8 @@
 
 #include "isdf_internal.h"
 
+#include <memory>
+
 namespace isdf {
 
 struct KeptPoints {
@@ -116,6 +118,41 @@ void sketch_factors(int64_t d, int64_t ell, uint64_t seed, HostFactors& u, HostF
 SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t s,
                      const ExactSketchSource* exact = nullptr);
 
+// One rank's share of the column-pivoted QR of a sketch whose columns are
+// split over ranks (the distributed form of qrcp_sketch, same kernels and
+// arithmetic).  Per step j the caller runs update(j) on every rank (exact
+// mode: returns the rank's best (squared trailing norm, global position,
+// local column) key; verified mode: the rank's best lower bound, then, after
+// the global maximum of the bounds, verify(j, bound) returns the key), picks
+// the global best key (ties to the smaller position), fetches the winner's
+// rows from its owner (column) and calls pivot(j, ...) on every rank with the
+// same rows.  energy_part is the rank's share of row j-1's energy.  Columns
+// carry global positions offset + local index (dgeqp3's swap order).
+struct QrShardKey {
+    double v;        // squared trailing norm (-1 when the rank has no candidate)
+    int64_t pos;     // global position
+    int64_t col;     // local column
+};
+class QrShard {
+public:
+    QrShard(double* Yt, int64_t ldy, int64_t m, int64_t n, int64_t pos_offset, const ExactSketchSource* exact,
+            cudaStream_t s);
+    ~QrShard();
+    QrShard(const QrShard&) = delete;
+    QrShard& operator=(const QrShard&) = delete;
+    QrShardKey update(int64_t j, double* energy_part, double* lower_bound);
+    QrShardKey verify(int64_t j, double lower_bound);
+    void column(int64_t col, double* rows_host);
+    // pivot_col / moved_col: this rank's pivot column and the column it holds
+    // at position j (-1 when another rank holds them); returns R_jj (signed)
+    double pivot(int64_t j, const double* rows_host, int64_t pivot_col, int64_t pivot_pos, int64_t moved_col);
+    int64_t reverified() const;
+
+private:
+    struct Impl;
+    std::unique_ptr<Impl> d_;
+};
+
 struct MixedSketch {
     DeviceBuffer<double> scales, WT, delta;
     ExactSketchSource source;
@@ -198,6 +235,23 @@ std::vector<int64_t> select_sketch_gathered(const Context& c, const SelectOption
                                             const double* kept_xyz, const double* kept_w, double* delta,
                                             const std::vector<double>& scales, SketchDiagnostics* diag,
                                             cudaStream_t s);
+
+// One rank's share of the distributed sketch QR over its own kept points
+// (Yt: ell x n_local, leading dimension n_local): the QR state and, in the
+// mixed form (delta non-null), the FP64 recomputation source of its columns.
+struct SketchQrShard {
+    SketchSetup su;
+    int64_t n_total = 0;
+    DeviceBuffer<double> WT, scales;
+    DeviceBuffer<int64_t> index;
+    ExactSketchSource src;
+    std::unique_ptr<QrShard> qr;
+};
+std::unique_ptr<SketchQrShard> make_sketch_qr_shard(const Context& c, const SelectOptions& o, double* Yt,
+                                                    int64_t n_local, int64_t n_total, const double* kept_xyz,
+                                                    const double* kept_w, double* delta,
+                                                    const std::vector<double>& scales, int64_t pos_offset,
+                                                    cudaStream_t s);
 
 // qrcp_dense / qrcp_online: greedy max-residual pivoting of the weighted
 // pair columns sqrt|w_g| f_g (x) f_g, computed without materialising them.

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cmath>
+#include <cstring>
 
 namespace isdf {
 namespace {
@@ -529,7 +530,255 @@ ExactKernel pick_exact_kernel(bool grad, int lmax) {
     return {exact_columns_kernel<false, kMaxL, 256>, 256};
 }
 
+// ---- one rank's share of a distributed pivoted QR ----------------------------------
+// pos[g] = offset + g (global positions of this rank's columns)
+__global__ void iota_offset_kernel(int64_t* pos, int64_t n, int64_t offset) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) pos[i] = offset + i;
+}
+
+// Best of the per-block keys (and re-verification keys) of this rank.
+__global__ void __launch_bounds__(1024) reduce_keys_kernel(const ArgKey* partial, int nblocks, const ArgKey* xpartial,
+                                                           int nx, ArgKey* out) {
+    __shared__ ArgKey ksh[32];
+    ArgKey k = key_none();
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+        if (key_better(partial[b], k)) k = partial[b];
+    for (int b = threadIdx.x; b < nx; b += blockDim.x)
+        if (key_better(xpartial[b], k)) k = xpartial[b];
+    k = block_best<1024>(k, ksh);
+    if (threadIdx.x == 0) *out = k;
+}
+
+// Pivot step j of a distributed QR, identical on every rank: the owner marks
+// its pivot column selected (position j); the rank holding the column at
+// position j moves it to the pivot's former position (dgeqp3's swap); every
+// rank builds reflector j from the pivot column's rows (the arithmetic of
+// qr_pivot_kernel) and clears the verified-mode step state.
+__global__ void shard_pivot_kernel(QrState st, int64_t j, const double* __restrict__ rows, int64_t pivot_col,
+                                   int64_t pivot_pos, int64_t moved_col, double* beta_out) {
+    __shared__ double sh_scale;
+    if (threadIdx.x == 0) {
+        if (pivot_col >= 0) {
+            st.selected[pivot_col] = 1;
+            st.pos[pivot_col] = j;
+        }
+        if (moved_col >= 0) st.pos[moved_col] = pivot_pos;
+        if (st.count) {
+            *st.count = 0;
+            *st.lb_bits = 0ull;
+        }
+        const double alpha = rows[j];
+        double xnorm = 0;
+        for (int64_t i = j + 1; i < st.m; ++i) xnorm = hypot(xnorm, rows[i]);
+        double beta, tau, scale;
+        if (xnorm == 0.0) {
+            beta = alpha; tau = 0.0; scale = 0.0;
+        } else {
+            beta = -copysign(hypot(alpha, xnorm), alpha);
+            tau = (beta - alpha) / beta;
+            scale = 1.0 / (alpha - beta);
+        }
+        st.tau[j] = tau;
+        st.diag[j] = fabs(beta);
+        *beta_out = beta;
+        sh_scale = scale;
+    }
+    __syncthreads();
+    double* v = st.vhist + j * st.m;
+    for (int64_t i = threadIdx.x; i < st.m; i += blockDim.x)
+        v[i] = i < j ? 0.0 : i == j ? 1.0 : rows[i] * sh_scale;
+}
+
+ExactArgs make_exact_args(const ExactSketchSource& ex) {
+    ExactArgs ea{};
+    const Context& c = *ex.ctx;
+    ea.shells = c.d_shells; ea.nshell = c.nshell; ea.exps = c.d_exp; ea.coefs = c.d_coef;
+    ea.nao = c.nao; ea.naxes = ex.naxes; ea.grad = 0;
+    for (int a = 0; a < ex.naxes; ++a) { ea.comp[a] = ex.comp[a]; ea.grad |= ex.comp[a] > 0; }
+    ea.scales = ex.scales; ea.WT = ex.WT; ea.pts = ex.pts; ea.index = ex.index;
+    ea.w = ex.w; ea.ell = ex.ell;
+    return ea;
+}
+
 }  // namespace
+
+struct QrShard::Impl {
+    cudaStream_t s;
+    int64_t m, n, steps, ldy;
+    int nblocks;
+    bool pairs;
+    QrState st;
+    DeviceBuffer<int64_t> pos, col_at, jpvt, cand, count;
+    DeviceBuffer<char> selected;
+    DeviceBuffer<double> vhist, tau, diag, energy, est, lr_split, rows, beta;
+    DeviceBuffer<ArgKey> partial, xpartial, key;
+    DeviceBuffer<unsigned long long> lb_bits, reverified;
+    DeviceBuffer<unsigned> done;
+    bool verified = false;
+    ExactArgs ea{};
+    size_t exact_smem = 0;
+    ExactKernel exact_kernel;
+};
+
+QrShard::QrShard(double* Yt, int64_t ldy, int64_t m, int64_t n, int64_t pos_offset, const ExactSketchSource* exact,
+                 cudaStream_t s)
+    : d_(new Impl) {
+    Impl& d = *d_;
+    d.s = s;
+    d.m = m;
+    d.n = n;
+    d.ldy = ldy;
+    d.steps = m;
+    require(m >= 1 && m <= kMaxSketchRows, "distributed sketch QR supports 1 to 128 sketch rows");
+    d.nblocks = static_cast<int>((n + kQrThreads - 1) / kQrThreads);
+    const size_t nn = static_cast<size_t>(std::max<int64_t>(n, 1));
+    d.pos.reset(nn, s);
+    d.col_at.reset(nn, s);
+    d.jpvt.reset(m, s);
+    d.selected.reset(nn, s);
+    d.vhist.reset(static_cast<size_t>(m * m), s);
+    d.tau.reset(m, s);
+    d.diag.reset(m, s);
+    d.energy.reset(m + 1, s);
+    d.partial.reset(std::max(d.nblocks, 1), s);
+    d.key.reset(1, s);
+    d.rows.reset(m, s);
+    d.beta.reset(1, s);
+    d.selected.zero(s);
+    d.energy.zero(s);
+    d.tau.zero(s);
+    if (n > 0) {
+        iota_offset_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(d.pos.get(), n, pos_offset);
+        ISDF_LAUNCH_CHECK();
+    }
+    d.st = QrState{Yt, ldy, m, n, d.pos.get(), d.col_at.get(), d.selected.get(), d.vhist.get(), d.tau.get(),
+                   d.diag.get(), d.energy.get(), d.jpvt.get(), d.partial.get(), nullptr, nullptr, nullptr,
+                   nullptr, nullptr};
+    d.reverified.reset(1, s);
+    d.reverified.zero(s);
+    if (exact) {
+        d.verified = true;
+        d.est.reset(nn, s);
+        d.lb_bits.reset(1, s);
+        d.cand.reset(nn, s);
+        d.count.reset(1, s);
+        d.xpartial.reset(kExactBlocks, s);
+        d.lr_split.reset(static_cast<size_t>(kSplitCands) * 2 * exact->ell, s);
+        d.done.reset(kSplitCands, s);
+        d.lb_bits.zero(s);
+        d.count.zero(s);
+        d.done.zero(s);
+        d.st.est = d.est.get();
+        d.st.delta = exact->delta;
+        d.st.lb_bits = d.lb_bits.get();
+        d.st.count = d.count.get();
+        d.st.xpartial = d.xpartial.get();
+        d.ea = make_exact_args(*exact);
+        d.exact_smem = (static_cast<size_t>(d.ea.grad ? 4 : 1) * exact->ctx->nao + 2 * exact->ell + m) * sizeof(double);
+        d.exact_kernel = pick_exact_kernel(d.ea.grad != 0, exact->ctx->lmax);
+        ISDF_CUDA(cudaFuncSetAttribute(d.exact_kernel.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(d.exact_smem)));
+    }
+    constexpr size_t kStagedBytes = static_cast<size_t>(kRegRows) * kQrThreads * sizeof(double);
+    ISDF_CUDA(cudaFuncSetAttribute(qr_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kStagedBytes)));
+    ISDF_CUDA(cudaFuncSetAttribute(qr_update_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kStagedBytes)));
+    d.pairs = ldy % 2 == 0 && reinterpret_cast<uintptr_t>(Yt) % 16 == 0;
+}
+
+QrShard::~QrShard() = default;
+
+QrShardKey QrShard::update(int64_t j, double* energy_part, double* lower_bound) {
+    Impl& d = *d_;
+    QrShardKey out{-1.0, INT64_MAX, -1};
+    *energy_part = 0.0;
+    *lower_bound = 0.0;
+    if (d.n == 0) return out;
+    {
+        ISDF_PROFILE("qrcp_sketch_update", d.s);
+        const int64_t touched = d.m - (j > 0 ? j - 1 : 0);
+        const size_t staged = static_cast<size_t>(touched) * kQrThreads * sizeof(double);
+        if (touched <= kRegRows && d.pairs)
+            qr_update_pairs_kernel<<<d.nblocks, kPairThreads, staged, d.s>>>(d.st, j);
+        else if (touched <= kRegRows)
+            qr_update_kernel<true><<<d.nblocks, kQrThreads, staged, d.s>>>(d.st, j);
+        else
+            qr_update_kernel<false><<<d.nblocks, kQrThreads, 0, d.s>>>(d.st, j);
+        ISDF_LAUNCH_CHECK();
+    }
+    if (j > 0)
+        ISDF_CUDA(cudaMemcpyAsync(energy_part, d.energy.get() + (j - 1), sizeof(double), cudaMemcpyDeviceToHost, d.s));
+    if (j < d.m) {
+        if (d.verified) {
+            unsigned long long bits = 0;
+            ISDF_CUDA(cudaMemcpyAsync(&bits, d.lb_bits.get(), sizeof(bits), cudaMemcpyDeviceToHost, d.s));
+            ISDF_CUDA(cudaStreamSynchronize(d.s));
+            std::memcpy(lower_bound, &bits, sizeof(double));
+            return out;
+        }
+        reduce_keys_kernel<<<1, 1024, 0, d.s>>>(d.partial.get(), d.nblocks, nullptr, 0, d.key.get());
+        ISDF_LAUNCH_CHECK();
+        ISDF_CUDA(cudaMemcpyAsync(&out, d.key.get(), sizeof(out), cudaMemcpyDeviceToHost, d.s));
+    }
+    ISDF_CUDA(cudaStreamSynchronize(d.s));
+    return out;
+}
+
+QrShardKey QrShard::verify(int64_t j, double lower_bound) {
+    Impl& d = *d_;
+    QrShardKey out{-1.0, INT64_MAX, -1};
+    if (d.n == 0) return out;
+    require(d.verified, "verify() needs error bounds");
+    unsigned long long bits = 0;
+    std::memcpy(&bits, &lower_bound, sizeof(bits));
+    ISDF_CUDA(cudaMemcpyAsync(d.lb_bits.get(), &bits, sizeof(bits), cudaMemcpyHostToDevice, d.s));
+    {
+        ISDF_PROFILE("qrcp_sketch_verify", d.s);
+        candidates_kernel<<<d.nblocks, kQrThreads, 0, d.s>>>(d.st, d.cand.get());
+        ISDF_LAUNCH_CHECK();
+        d.exact_kernel.fn<<<kExactBlocks, d.exact_kernel.threads, d.exact_smem, d.s>>>(
+            d.ea, d.st, d.cand.get(), j, d.reverified.get(), d.lr_split.get(), d.done.get());
+        ISDF_LAUNCH_CHECK();
+    }
+    reduce_keys_kernel<<<1, 1024, 0, d.s>>>(d.partial.get(), d.nblocks, d.xpartial.get(), kExactBlocks, d.key.get());
+    ISDF_LAUNCH_CHECK();
+    ISDF_CUDA(cudaMemcpyAsync(&out, d.key.get(), sizeof(out), cudaMemcpyDeviceToHost, d.s));
+    ISDF_CUDA(cudaStreamSynchronize(d.s));
+    return out;
+}
+
+void QrShard::column(int64_t col, double* rows_host) {
+    Impl& d = *d_;
+    require(col >= 0 && col < d.n, "pivot column outside this rank's columns");
+    ISDF_CUDA(cudaMemcpy2DAsync(rows_host, sizeof(double), d.st.Yt + col, d.ldy * sizeof(double), sizeof(double),
+                                d.m, cudaMemcpyDeviceToHost, d.s));
+    ISDF_CUDA(cudaStreamSynchronize(d.s));
+}
+
+double QrShard::pivot(int64_t j, const double* rows_host, int64_t pivot_col, int64_t pivot_pos, int64_t moved_col) {
+    Impl& d = *d_;
+    require(j >= 0 && j < d.m, "pivot step outside the sketch rows");
+    require(pivot_col < d.n && moved_col < d.n, "pivot or moved column outside this rank's columns");
+    ISDF_CUDA(cudaMemcpyAsync(d.rows.get(), rows_host, d.m * sizeof(double), cudaMemcpyHostToDevice, d.s));
+    {
+        ISDF_PROFILE("qrcp_sketch_pivot", d.s);
+        shard_pivot_kernel<<<1, 128, 0, d.s>>>(d.st, j, d.rows.get(), pivot_col, pivot_pos, moved_col, d.beta.get());
+        ISDF_LAUNCH_CHECK();
+    }
+    double beta = 0;
+    ISDF_CUDA(cudaMemcpyAsync(&beta, d.beta.get(), sizeof(beta), cudaMemcpyDeviceToHost, d.s));
+    ISDF_CUDA(cudaStreamSynchronize(d.s));
+    return beta;
+}
+
+int64_t QrShard::reverified() const {
+    unsigned long long r = 0;
+    ISDF_CUDA(cudaMemcpyAsync(&r, d_->reverified.get(), sizeof(r), cudaMemcpyDeviceToHost, d_->s));
+    ISDF_CUDA(cudaStreamSynchronize(d_->s));
+    return static_cast<int64_t>(r);
+}
 
 SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t s,
                      const ExactSketchSource* exact) {

@@ -1175,6 +1175,55 @@ void sketch_shard_combine(const Context& c, SketchShard& st, const double* sumsq
     if (hbad) fail(kOverflow, "non-finite randomized ID sketch");
 }
 
+std::unique_ptr<SketchQrShard> make_sketch_qr_shard(const Context& c, const SelectOptions& o, double* Yt,
+                                                    int64_t n_local, int64_t n_total, const double* kept_xyz,
+                                                    const double* kept_w, double* delta,
+                                                    const std::vector<double>& scales, int64_t pos_offset,
+                                                    cudaStream_t s) {
+    require(n_local >= 0 && n_total >= n_local && pos_offset >= 0 && pos_offset + n_local <= n_total,
+            "invalid distributed sketch QR shard sizes");
+    auto sh = std::make_unique<SketchQrShard>();
+    sh->n_total = n_total;
+    sh->su = sketch_setup(c, o, std::max<int64_t>(n_total, 1), s);
+    const SketchSetup& su = sh->su;
+    if (su.ax.has_occ) fail(kInvalid, "grid-sharded selection supports the ao, dx, dy, dz axes");
+    require(static_cast<int>(scales.size()) == su.ax.naxes, "one scale per axis entry is required");
+    const ExactSketchSource* ex = nullptr;
+    if (delta && su.mixed && n_local > 0) {
+        HostFactors u, v;
+        sketch_factors(su.d, su.ell, o.seed, u, v);
+        const int64_t d = su.d, nout = 2 * su.ell;
+        std::vector<double> hwt(static_cast<size_t>(d * nout));
+        for (int64_t jj = 0; jj < d; ++jj)
+            for (int64_t t = 0; t < su.ell; ++t) {
+                hwt[t * d + jj] = u[jj * su.ell + t];
+                hwt[(su.ell + t) * d + jj] = v[jj * su.ell + t];
+            }
+        sh->WT.reset(hwt.size(), s);
+        sh->scales.reset(scales.size(), s);
+        sh->index.reset(n_local, s);
+        ISDF_CUDA(cudaMemcpyAsync(sh->WT.get(), hwt.data(), hwt.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        ISDF_CUDA(cudaMemcpyAsync(sh->scales.get(), scales.data(), scales.size() * sizeof(double),
+                                  cudaMemcpyHostToDevice, s));
+        iota_i64(sh->index.get(), n_local, s);
+        ExactSketchSource& src = sh->src;
+        src.ctx = &c;
+        src.naxes = su.ax.naxes;
+        for (int a = 0; a < su.ax.naxes; ++a) src.comp[a] = su.ax.comp[a];
+        src.scales = sh->scales.get();
+        src.WT = sh->WT.get();
+        src.pts = kept_xyz;
+        src.index = sh->index.get();
+        src.w = kept_w;
+        src.ell = su.ell;
+        src.delta = delta;
+        ex = &src;
+        ISDF_CUDA(cudaStreamSynchronize(s));   // the host staging vector goes out of scope
+    }
+    sh->qr = std::make_unique<QrShard>(Yt, n_local, su.ell, n_local, pos_offset, ex, s);
+    return sh;
+}
+
 std::vector<int64_t> select_sketch_gathered(const Context& c, const SelectOptions& o, double* Yt, int64_t n,
                                             const double* kept_xyz, const double* kept_w, double* delta,
                                             const std::vector<double>& scales, SketchDiagnostics* diag_out,

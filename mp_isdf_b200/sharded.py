@@ -9,22 +9,37 @@ contiguous shard of the grid, in grid order, and runs::
     1. project its shard                  -> per-component sums of squares
        all-reduce(sum) of 4 doubles       -> global multi-axis scales
     2. its shard's sketch columns          (ell x n_r, + error bounds)
-       all-gather of the columns, bounds, kept coordinates and weights
-    3. the pivoted QR of the gathered sketch (identical inputs on every rank,
-       hence identical anchors; this is the single-GPU QR of the whole grid)
+    3. the pivoted QR of the whole sketch with the columns left where they
+       are (``distributed_sketch_qr``).  Per pivot step j:
+         - every rank applies reflector j-1 to its columns and forms its best
+           key (squared trailing norm, global position); in the mixed form its
+           best lower bound first, all-reduce(max), then the exact
+           re-verification of its candidates;
+         - all-gather of one key per rank (4 doubles): the global winner
+           (ties to the smaller position, dgeqp3's order) and row j-1's energy;
+         - the winner's ell rows and its grid index, coordinates and weight
+           from its owner (all-reduce(sum) of a vector that is zero elsewhere);
+         - every rank builds reflector j from those rows and moves the column
+           at position j to the winner's position (dgeqp3's swap);
+       then the tail / numerical-rank rules on the per-step |R_jj| and
+       energies (identical on every rank, hence identical anchors: those of
+       the single-GPU QR of the whole grid);
     4. the fit on its shard with the anchors' coordinates
        all-reduce(sum) of the pair-error sums
 
-The AO evaluation and projections (the dominant cost) are split over the
-ranks; the exchanged data is O(ell * n) doubles, which NVLink moves in well
-under a millisecond at (H2O)64.  Collectives go through ``torch.distributed``
-(NCCL for CUDA tensors; gloo works for CPU tensors), or ``LocalComm`` for one
-process.  The compute backend is pluggable; ``CudaBackend`` drives the
-library's C-ABI phases.
+The AO evaluation, the projections and the QR updates are split over the
+ranks; per pivot step the ranks exchange O(ell + ranks) doubles, so the
+exchange is latency-bound (2-3 small collectives per step, ell steps).
+``qr="gathered"`` keeps the earlier form: all-gather of the whole sketch and
+the same QR replicated on every rank.  Collectives go through
+``torch.distributed`` (NCCL for CUDA tensors; gloo works for CPU tensors), or
+``LocalComm`` for one process.  The compute backend is pluggable;
+``CudaBackend`` drives the library's C-ABI phases.
 """
 from __future__ import annotations
 
 from dataclasses import dataclass, field
+from types import SimpleNamespace
 
 import numpy as np
 
@@ -83,7 +98,71 @@ class ShardedResult:
     counts: list = field(default_factory=list)
 
 
-def select_fit_sharded(backend, comm, xyz, w, grid_offset, ng_total, want_error=True, **select_kw):
+def _allreduce_max(comm, backend, value):
+    return max(float(backend.to_numpy(t)[0]) for t in comm.allgather(backend.tensor(np.array([value], np.float64))))
+
+
+def distributed_sketch_qr(backend, comm, qr, steps, verified, offsets, counts, record):
+    """Column-pivoted QR of a sketch whose columns stay on their ranks.
+
+    ``qr``: this rank's QR state (``backend.qr_begin``); ``offsets``/``counts``:
+    every rank's first global position and column count; ``record(col)``:
+    this rank's (grid index, x, y, z, weight) of a local column.  Returns the
+    per-step pivots as (grid index, xyz, weight) records, |R_jj| and the row
+    energies of R, identical on every rank.
+    """
+    moved = {}   # global position -> (rank, local column), for positions a swap changed
+
+    def holder(pos):
+        if pos in moved:
+            return moved[pos]
+        for r in range(len(offsets)):
+            if offsets[r] <= pos < offsets[r] + counts[r]:
+                return r, pos - offsets[r]
+        raise RuntimeError("position outside the sketch")
+
+    diag, energy, pivots = [], np.zeros(steps), []
+    ell = qr.ell
+    for j in range(steps + 1):
+        val, pos, col, e_part, lb = backend.qr_update(qr, j)
+        if j == steps:
+            tot = backend.to_numpy(comm.allreduce_sum(backend.tensor(np.array([e_part], np.float64))))
+            if j > 0:
+                energy[j - 1] += float(tot[0])
+            break
+        if verified:
+            val, pos, col = backend.qr_verify(qr, j, _allreduce_max(comm, backend, lb))
+        keys = [backend.to_numpy(k) for k in
+                comm.allgather(backend.tensor(np.array([val, pos, col, e_part], np.float64)))]
+        if j > 0:
+            energy[j - 1] += float(sum(k[3] for k in keys))
+        best = None
+        for r, k in enumerate(keys):
+            if k[0] < 0:
+                continue
+            if best is None or k[0] > keys[best][0] or (k[0] == keys[best][0] and k[1] < keys[best][1]):
+                best = r
+        if best is None:
+            raise RuntimeError("no column left for the pivoted QR")
+        p, lc = int(keys[best][1]), int(keys[best][2])
+        buf = np.zeros(ell + 5)
+        if comm.rank == best:
+            buf[:ell] = backend.qr_column(qr, lc)
+            buf[ell:] = record(lc)
+        buf = backend.to_numpy(comm.allreduce_sum(backend.tensor(buf)))
+        hr, hc = holder(j)
+        moved[p] = (hr, hc)
+        moved[j] = (best, lc)
+        r_jj = backend.qr_pivot(qr, j, buf[:ell], lc if comm.rank == best else -1, p,
+                                hc if comm.rank == hr else -1)
+        diag.append(abs(r_jj))
+        energy[j] += r_jj * r_jj
+        pivots.append(buf[ell:].copy())
+    return pivots, np.array(diag), energy
+
+
+def select_fit_sharded(backend, comm, xyz, w, grid_offset, ng_total, want_error=True, qr="distributed",
+                       **select_kw):
     """Selection + fit of one cluster whose grid is split over the ranks.
 
     ``xyz``/``w``: this rank's contiguous shard (device tensors for the CUDA
@@ -100,10 +179,45 @@ def select_fit_sharded(backend, comm, xyz, w, grid_offset, ng_total, want_error=
     sums = comm.allreduce_sum(backend.tensor(np.asarray(sumsq, np.float64)))
     # 2. this shard's sketch columns with the global scales
     yt, delta, kept, kxyz, kw, scales = backend.combine(shard, backend.to_numpy(sums), ell, n_kept, naxes)
-    # 3. gather everything the pivoted QR needs, in grid order
     counts = [int(backend.to_numpy(c)[0]) for c in comm.allgather(backend.tensor(np.array([n_kept], np.int64)))]
     offsets = [int(backend.to_numpy(o)[0])
                for o in comm.allgather(backend.tensor(np.array([grid_offset], np.int64)))]
+    if qr == "distributed":
+        # 3. the pivoted QR with the columns left on their ranks
+        n_total = int(sum(counts))
+        pos_offset = int(sum(counts[:comm.rank]))
+        state = backend.qr_begin(yt, n_total, pos_offset, kxyz, kw, delta, scales, **select_kw)
+        kept_np = backend.to_numpy(kept) if n_kept else np.zeros(0, np.int64)
+        kxyz_np = backend.to_numpy(kxyz) if n_kept else np.zeros((0, 3))
+        kw_np = backend.to_numpy(kw) if n_kept else np.zeros(0)
+
+        def record(col):
+            return np.array([kept_np[col] + grid_offset, *kxyz_np[col], kw_np[col]], np.float64)
+
+        steps = min(state.ell, n_total)
+        pivots, diag, energy = distributed_sketch_qr(backend, comm, state, steps, state.verified,
+                                                     [int(sum(counts[:r])) for r in range(len(counts))],
+                                                     counts, record)
+        rank_k, numerical_rank, rel_tail = backend.sketch_rank(n_total, diag, energy, **select_kw)
+        sinfo = SimpleNamespace(n_kept=n_total, sketch_rows=state.ell, numerical_rank=numerical_rank,
+                                relative_residual=rel_tail, verifications=backend.qr_reverified(state),
+                                reselections=0, precision_used=int(state.verified))
+        backend.qr_end(state)
+        chosen = pivots[:rank_k]
+        anchors = np.array([int(round(r[0])) for r in chosen], np.int64)
+        a_xyz = np.array([r[1:4] for r in chosen], np.float64).reshape(-1, 3)
+        a_w = np.array([r[4] for r in chosen], np.float64)
+        theta, finfo, fsums = backend.fit_at(xyz, w, a_xyz, a_w, precision, want_error)
+        tot = backend.to_numpy(comm.allreduce_sum(backend.tensor(np.asarray(fsums, np.float64))))
+        err2, exact2 = max(float(tot[0]), 0.0), float(tot[1])
+        shard_free = getattr(shard, "free", None)
+        if shard_free:
+            shard_free()
+        return ShardedResult(anchors=anchors, theta=theta, n_kept_local=n_kept, kept_offset=pos_offset,
+                             pair_l2=float(np.sqrt(err2)),
+                             pair_relative=float(np.sqrt(err2 / exact2)) if exact2 else 0.0,
+                             select_info=sinfo, fit_info=finfo, counts=counts)
+    # 3. (gathered form) everything the pivoted QR needs, in grid order
     yt_all = _gather_ragged(comm, yt.t().contiguous(), n_kept, counts).t().contiguous()
     delta_all = _gather_ragged(comm, delta, n_kept, counts)
     kxyz_all = _gather_ragged(comm, kxyz, n_kept, counts)
@@ -159,6 +273,37 @@ class CudaBackend:
 
     def select_gathered(self, yt, kxyz, kw, delta, scales, **kw_sel):
         return self.ctx.sketch_select_gathered(yt, kxyz, kw, delta, scales, **kw_sel)
+
+    # distributed QR (isdf_qr_shard_*)
+    def qr_begin(self, yt, n_total, pos_offset, kxyz, kw, delta, scales, **kw_sel):
+        return self.ctx.qr_shard(yt.contiguous(), n_total, pos_offset, kxyz, kw, delta, scales, **kw_sel)
+
+    @staticmethod
+    def qr_update(qr, j):
+        return qr.update(j)
+
+    @staticmethod
+    def qr_verify(qr, j, bound):
+        return qr.verify(j, bound)
+
+    @staticmethod
+    def qr_column(qr, col):
+        return qr.column(col)
+
+    @staticmethod
+    def qr_pivot(qr, j, rows, pivot_col, pivot_pos, moved_col):
+        return qr.pivot(j, rows, pivot_col, pivot_pos, moved_col)
+
+    @staticmethod
+    def qr_reverified(qr):
+        return qr.reverified()
+
+    @staticmethod
+    def qr_end(qr):
+        qr.free()
+
+    def sketch_rank(self, n_total, diag, energy, **kw_sel):
+        return self.ctx.sketch_rank(n_total, diag, energy, **kw_sel)
 
     def fit_at(self, xyz, w, a_xyz, a_w, precision, want_error):
         import torch

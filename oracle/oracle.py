@@ -498,6 +498,19 @@ def sketch_qr_rank(y, ell, oversampling, tolerance, max_rank, physical_rank):
     steps = min(ell, n)
     energy = np.array([np.sum(qr_[i, i:] ** 2) for i in range(steps)])
     diag = np.abs(np.diag(qr_)[:steps])
+    rank, tails, numerical_rank = sketch_rank_rules(diag, energy, ell, n, oversampling, tolerance, max_rank,
+                                                    physical_rank)
+    pos = [int(jpvt[i] - 1) for i in range(rank)]
+    return pos, dict(jpvt=jpvt - 1, diag=diag, tails=tails, numerical_rank=numerical_rank)
+
+
+def sketch_rank_rules(diag, energy, ell, n, oversampling, tolerance, max_rank, physical_rank):
+    """Tails, numerical rank, cap and selected rank from the per-step |R_ii|
+    and row energies of the sketch QR (``anchor_select_randomized_id.cpp:320-374``):
+    (rank, tails, numerical_rank)."""
+    steps = min(ell, n)
+    diag = np.asarray(diag, float)[:steps]
+    energy = np.asarray(energy, float)[:steps]
     tails = np.zeros(steps + 1)
     for i in range(steps - 1, -1, -1):
         tails[i] = np.hypot(tails[i + 1], np.sqrt(energy[i]))
@@ -519,8 +532,7 @@ def sketch_qr_rank(y, ell, oversampling, tolerance, max_rank, physical_rank):
             if tails[i] <= tolerance * norm:
                 rank = i
                 break
-    pos = [int(jpvt[i] - 1) for i in range(rank)]
-    return pos, dict(jpvt=jpvt - 1, diag=diag, tails=tails, numerical_rank=numerical_rank)
+    return rank, tails, numerical_rank
 
 
 def select_rand_sketch(ctx, pts, w, axes, tolerance=1e-10, max_rank=0, sketch_size=128,

@@ -10,6 +10,11 @@ import torch
 from oracle import oracle as O
 
 
+class _State(dict):
+    """A dict whose entries also read as attributes (state.ell, state.verified)."""
+    __getattr__ = dict.__getitem__
+
+
 class OracleBackend:
     """The sharded phases restated on the CPU with the oracle (FP64)."""
 
@@ -27,10 +32,10 @@ class OracleBackend:
 
     def project(self, xyz, w, ng_total, axes=("ao",), axis_weights=None, max_rank=0, oversampling=16,
                 seed=7, **_):
-        xyz, w = self.to_numpy(xyz), self.to_numpy(w)
+        xyz, w = self.to_numpy(xyz).reshape(-1, 3), self.to_numpy(w)
         keep = np.flatnonzero(w != 0)
         codes = [O.AXIS_CODES[a] for a in axes]
-        f = self.oc.axis_features(xyz[keep], codes, None)
+        f = self.oc.axis_features(xyz[keep], codes, None) if len(keep) else np.zeros((0, len(codes) * self.nao))
         sumsq = np.zeros(4)
         for a, c in enumerate(codes):
             sumsq[c] = np.sum(f[:, a * self.nao:(a + 1) * self.nao] ** 2)
@@ -42,7 +47,8 @@ class OracleBackend:
         factors = np.ones(naxes) if not shard["aw"] else np.asarray(shard["aw"], float)
         scales = factors / np.sqrt(sumsq[codes]) if naxes > 1 else np.ones(1)
         u, v = O.sketch_factors(naxes * self.nao, ell, shard["seed"])
-        y = self.oc.sketch(shard["xyz"][keep], shard["w"][keep], codes, scales if naxes > 1 else None, u, v, ell)
+        y = (self.oc.sketch(shard["xyz"][keep], shard["w"][keep], codes, scales if naxes > 1 else None, u, v, ell)
+             if len(keep) else np.zeros((0, ell)))
         return (torch.as_tensor(np.ascontiguousarray(y.T)), torch.zeros(len(keep), dtype=torch.float64),
                 torch.as_tensor(keep.astype(np.int64)), torch.as_tensor(shard["xyz"][keep]),
                 torch.as_tensor(shard["w"][keep]), scales)
@@ -54,9 +60,84 @@ class OracleBackend:
         pos, _ = O.sketch_qr_rank(y, y.shape[1], oversampling, tolerance, max_rank, d * (d + 1) // 2)
         return pos, None
 
+    # the distributed QR of the sketch columns of this rank, restated in NumPy
+    # with the arithmetic of the library's per-rank steps (exact trailing
+    # norms, dgeqp3's pivot order through global positions)
+    def qr_begin(self, yt, n_total, pos_offset, kxyz, kw, delta, scales, **_):
+        a = self.to_numpy(yt).copy()
+        n = a.shape[1] if a.ndim == 2 else 0
+        ell = a.shape[0]
+        return _State(A=a.reshape(ell, n), ell=ell, pos=pos_offset + np.arange(n), sel=np.zeros(n, bool),
+                      v=np.zeros((ell, ell)), tau=np.zeros(ell), verified=False)
+
+    @staticmethod
+    def qr_update(st, j):
+        A, act = st["A"], ~st["sel"]
+        ell = st["ell"]
+        e = 0.0
+        if j > 0 and st["tau"][j - 1] != 0.0 and act.any():
+            v = st["v"][j - 1][j - 1:]
+            sub = A[j - 1:, act]
+            A[j - 1:, act] = sub - np.outer(v, st["tau"][j - 1] * (v @ sub))
+        if j > 0:
+            e = float(np.sum(A[j - 1, act] ** 2))
+        if j < ell and act.any():
+            cols = np.flatnonzero(act)
+            nrm = np.sum(A[j:, cols] ** 2, axis=0)
+            top = nrm.max()
+            tied = cols[nrm == top]
+            c = int(tied[np.argmin(st["pos"][tied])])
+            return float(top), int(st["pos"][c]), c, e, 0.0
+        return -1.0, 2 ** 62, -1, e, 0.0
+
+    @staticmethod
+    def qr_column(st, col):
+        return st["A"][:, col].copy()
+
+    @staticmethod
+    def qr_pivot(st, j, rows, pivot_col, pivot_pos, moved_col):
+        if pivot_col >= 0:
+            st["sel"][pivot_col] = True
+            st["pos"][pivot_col] = j
+        if moved_col >= 0:
+            st["pos"][moved_col] = pivot_pos
+        alpha = rows[j]
+        xnorm = 0.0
+        for x in rows[j + 1:]:
+            xnorm = float(np.hypot(xnorm, x))
+        if xnorm == 0.0:
+            beta, tau, scale = alpha, 0.0, 0.0
+        else:
+            beta = -np.copysign(np.hypot(alpha, xnorm), alpha)
+            tau = (beta - alpha) / beta
+            scale = 1.0 / (alpha - beta)
+        v = np.zeros(st["ell"])
+        v[j] = 1.0
+        v[j + 1:] = rows[j + 1:] * scale
+        st["v"][j], st["tau"][j] = v, tau
+        return float(beta)
+
+    @staticmethod
+    def qr_reverified(st):
+        return 0
+
+    @staticmethod
+    def qr_end(st):
+        pass
+
+    def sketch_rank(self, n_total, diag, energy, axes=("ao",), max_rank=0, oversampling=16, sketch_size=128,
+                    tolerance=1e-10, **_):
+        d = len(axes) * self.nao
+        ell = max_rank + oversampling if max_rank else sketch_size
+        rank, tails, nrank = O.sketch_rank_rules(diag, energy, ell, n_total, oversampling, tolerance, max_rank,
+                                                 d * (d + 1) // 2)
+        return rank, nrank, float(tails[rank] / tails[0]) if tails[0] else 0.0
+
     def fit_at(self, xyz, w, a_xyz, a_w, precision, want_error):
-        xyz, w = self.to_numpy(xyz), self.to_numpy(w)
+        xyz, w = self.to_numpy(xyz).reshape(-1, 3), self.to_numpy(w)
         keep = w != 0
+        if not keep.any():
+            return torch.zeros((len(a_w), 0), dtype=torch.float64), None, np.zeros(2)
         theta, err = O.gram_fit(self.oc, xyz[keep], w[keep], a_xyz, a_w)
         return torch.as_tensor(theta), None, np.array([err["err2"], err["exact2"]])
 

@@ -1,6 +1,8 @@
 """Grid-sharded selection + fit (mp_isdf_b200.sharded).
 
-CPU: two gloo ranks run the protocol with the oracle backend and must give
+CPU: two or three gloo ranks (one of them possibly without grid points) run the
+protocol -- the distributed pivoted QR or the gathered one -- with the oracle
+backend and must give
 the single-process oracle's anchors, Theta columns and pair error.  GPU: the
 library's sharded phases with two shards in one process (threads standing in
 for ranks, no collectives between kernels) against isdf_select_fit on the
@@ -37,17 +39,23 @@ def _split(ng, size):
     return [(edges[r], edges[r + 1]) for r in range(size)]
 
 
-def _gloo_rank(rank, size, port, out_dir):
+def _gloo_rank(rank, size, port, out_dir, qr="distributed", empty_rank=-1):
+    import datetime
     import torch
     import torch.distributed as dist
     from mp_isdf_b200.sharded import TorchComm, select_fit_sharded
     from sharded_helpers import OracleBackend
-    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=size)
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=size,
+                            timeout=datetime.timedelta(seconds=120))
     try:
         mol, pts, w = _system()
-        lo, hi = _split(len(pts), size)[rank]
+        bounds = _split(len(pts), size - (empty_rank >= 0))
+        if empty_rank >= 0:   # this rank's shard holds no grid point at all
+            bounds.insert(empty_rank, (bounds[empty_rank - 1][1], bounds[empty_rank - 1][1]) if empty_rank
+                          else (0, 0))
+        lo, hi = bounds[rank]
         res = select_fit_sharded(OracleBackend(mol), TorchComm(), torch.as_tensor(pts[lo:hi]),
-                                 torch.as_tensor(w[lo:hi]), lo, len(pts), **KW)
+                                 torch.as_tensor(w[lo:hi]), lo, len(pts), qr=qr, **KW)
         np.save(os.path.join(out_dir, f"theta{rank}.npy"), res.theta.numpy())
         with open(os.path.join(out_dir, f"res{rank}.json"), "w") as f:
             json.dump({"anchors": res.anchors.tolist(), "pair_relative": res.pair_relative,
@@ -62,16 +70,27 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def test_gloo_two_ranks_match_single_process():
+@pytest.mark.parametrize("size,qr,empty_rank", [
+    (2, "distributed", -1),   # pivoted QR with the columns left on their ranks
+    (2, "gathered", -1),      # the whole sketch gathered, the QR replicated
+    (3, "distributed", 1),    # the middle rank owns no kept point
+    (2, "distributed", 0),    # rank 0 owns no kept point
+])
+def test_gloo_ranks_match_single_process(size, qr, empty_rank):
+    """The sharded protocol on gloo CPU ranks with the oracle backend gives
+    the single-process oracle's anchors, Theta columns and pair error."""
     import torch.multiprocessing as mp
     from oracle import oracle as O
     mol, pts, w = _system()
     with tempfile.TemporaryDirectory() as d:
-        mp.start_processes(_gloo_rank, args=(2, _free_port(), d), nprocs=2, join=True, start_method="spawn")
-        res = [json.load(open(os.path.join(d, f"res{r}.json"))) for r in range(2)]
-        thetas = [np.load(os.path.join(d, f"theta{r}.npy")) for r in range(2)]
-    assert res[0]["anchors"] == res[1]["anchors"]
-    assert res[0]["counts"][0] > 0 and res[0]["counts"][1] > 0
+        mp.start_processes(_gloo_rank, args=(size, _free_port(), d, qr, empty_rank), nprocs=size, join=True,
+                           start_method="spawn")
+        res = [json.load(open(os.path.join(d, f"res{r}.json"))) for r in range(size)]
+        thetas = [np.load(os.path.join(d, f"theta{r}.npy")) for r in range(size)]
+    for r in range(1, size):
+        assert res[r]["anchors"] == res[0]["anchors"]
+    counts = res[0]["counts"]
+    assert all((c == 0) == (r == empty_rank) for r, c in enumerate(counts)), counts
     oc = O.OracleContext(mol.atm, mol.bas, mol.env)
     codes = [O.AXIS_CODES[a] for a in KW["axes"]]
     scales = O.axis_scales(oc, pts, w, codes, KW["axis_weights"])
@@ -82,13 +101,14 @@ def test_gloo_two_ranks_match_single_process():
     theta_ref, err = O.gram_fit(oc, pts[keep], w[keep], pts[ref], w[ref])
     theta = np.concatenate(thetas, axis=1)
     np.testing.assert_allclose(theta, theta_ref, rtol=1e-9, atol=1e-9 * np.abs(theta_ref).max())
-    np.testing.assert_allclose(res[0]["pair_relative"], err["relative"], rtol=1e-10)
-    np.testing.assert_allclose(res[1]["pair_relative"], err["relative"], rtol=1e-10)
+    for r in range(size):
+        np.testing.assert_allclose(res[r]["pair_relative"], err["relative"], rtol=1e-10)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_cuda_phases_two_shards_match_select_fit(precision):
+@pytest.mark.parametrize("precision,qr", [("mixed", "distributed"), ("fp64", "distributed"),
+                                          ("mixed", "gathered"), ("fp64", "gathered")])
+def test_cuda_phases_two_shards_match_select_fit(precision, qr):
     import threading
     import torch
     from mp_isdf_b200 import capi
@@ -112,7 +132,7 @@ def test_cuda_phases_two_shards_match_select_fit(precision):
             lo, hi = _split(len(pts), size)[rank]
             results[rank] = select_fit_sharded(CudaBackend(c), ThreadComm(rank, size, shared),
                                                x[lo:hi].contiguous(), wt[lo:hi].contiguous(), lo, len(pts),
-                                               precision=precision, **KW)
+                                               precision=precision, qr=qr, **KW)
             torch.cuda.synchronize()
         except Exception as e:  # surfaced below
             errors.append(e)
