@@ -146,31 +146,48 @@ __device__ __forceinline__ void eval_shell_rel(const ShellDesc& b, T x, T y, T z
     }
 }
 
-// ---- packed pieces (FP32, the fused projection) -----------------------------------
-// A piece's primitives come as one float4 (alpha, c_j, c_j+1, c_j+2) per
-// primitive and group of three contractions, so one 16-byte load feeds the
-// exponential and up to three radial sums.  `sink.put<C>(ao, v)` receives the
-// AO index relative to the piece's first AO.
-template <int L, bool GRAD, int NG, class Sink>
-__device__ __forceinline__ void eval_piece_group(const SphPoly<float, L, GRAD>& poly, float x, float y, float z,
-                                                 float r2, const float4* __restrict__ pr, int nprim, int ng,
-                                                 int ao_rel0, Sink& sink) {
+// ---- packed pieces -------------------------------------------------------------------
+// A piece's primitives come as one record (alpha, c_j, c_j+1, c_j+2) per
+// primitive and group of three contractions -- one float4 (FP32 table) or two
+// double2 (FP64 table) -- so one or two 16-byte loads feed the exponential
+// and up to three radial sums.  `sink.put<C>(ao, v)` receives the AO index
+// relative to the piece's first AO.
+template <class T> struct PackedPrim;
+template <> struct PackedPrim<float> {
+    using rec = float4;
+    static __device__ __forceinline__ void load(const float4* __restrict__ pr, int p, float& a, float (&c)[3]) {
+        const float4 q = __ldg(pr + p);
+        a = q.x; c[0] = q.y; c[1] = q.z; c[2] = q.w;
+    }
+};
+template <> struct PackedPrim<double> {
+    using rec = double2;   // two per primitive
+    static __device__ __forceinline__ void load(const double2* __restrict__ pr, int p, double& a, double (&c)[3]) {
+        const double2 u = __ldg(pr + 2 * p), v = __ldg(pr + 2 * p + 1);
+        a = u.x; c[0] = u.y; c[1] = v.x; c[2] = v.y;
+    }
+};
+
+template <class T, int L, bool GRAD, int NG, class Sink>
+__device__ __forceinline__ void eval_piece_group(const SphPoly<T, L, GRAD>& poly, T x, T y, T z, T r2,
+                                                 const typename PackedPrim<T>::rec* __restrict__ pr, int nprim,
+                                                 int ng, int ao_rel0, Sink& sink) {
     constexpr int NS = 2 * L + 1;
-    float R[NG], Rp[NG];
+    T R[NG], Rp[NG];
 #pragma unroll
-    for (int j = 0; j < NG; ++j) { R[j] = 0.f; Rp[j] = 0.f; }
+    for (int j = 0; j < NG; ++j) { R[j] = T(0); Rp[j] = T(0); }
 #pragma unroll 2
     for (int p = 0; p < nprim; ++p) {
-        const float4 q = __ldg(pr + p);
-        const float arg = q.x * r2;
-        if (arg > static_cast<float>(kExpCut)) continue;
-        const float e = __expf(-arg);
-        const float cc[3] = {q.y, q.z, q.w};
+        T a, cc[3];
+        PackedPrim<T>::load(pr, p, a, cc);
+        const T arg = a * r2;
+        if (arg > static_cast<T>(kExpCut)) continue;
+        const T e = ao_exp(-arg);
 #pragma unroll
         for (int j = 0; j < NG; ++j) {
-            const float c = cc[j] * e;
+            const T c = cc[j] * e;
             R[j] += c;
-            if constexpr (GRAD) Rp[j] -= q.x * c;
+            if constexpr (GRAD) Rp[j] -= a * c;
         }
     }
 #pragma unroll
@@ -181,7 +198,7 @@ __device__ __forceinline__ void eval_piece_group(const SphPoly<float, L, GRAD>& 
             for (int s = 0; s < NS; ++s) {
                 sink.template put<0>(ao0 + s, R[j] * poly.v[s]);
                 if constexpr (GRAD) {
-                    const float two_rp = 2.f * Rp[j] * poly.v[s];
+                    const T two_rp = T(2) * Rp[j] * poly.v[s];
                     sink.template put<1>(ao0 + s, R[j] * poly.vx[s] + x * two_rp);
                     sink.template put<2>(ao0 + s, R[j] * poly.vy[s] + y * two_rp);
                     sink.template put<3>(ao0 + s, R[j] * poly.vz[s] + z * two_rp);
@@ -190,29 +207,30 @@ __device__ __forceinline__ void eval_piece_group(const SphPoly<float, L, GRAD>& 
         }
 }
 
-template <int L, bool GRAD, class Sink>
-__device__ __forceinline__ void eval_piece_core(float x, float y, float z, float r2, const float4* __restrict__ pr,
+template <class T, int L, bool GRAD, class Sink>
+__device__ __forceinline__ void eval_piece_core(T x, T y, T z, T r2, const typename PackedPrim<T>::rec* __restrict__ pr,
                                                 int nprim, int nc, Sink& sink) {
-    const SphPoly<float, L, GRAD> poly(x, y, z);
+    const SphPoly<T, L, GRAD> poly(x, y, z);
     if (nc == 1) {
-        eval_piece_group<L, GRAD, 1>(poly, x, y, z, r2, pr, nprim, 1, 0, sink);
+        eval_piece_group<T, L, GRAD, 1>(poly, x, y, z, r2, pr, nprim, 1, 0, sink);
         return;
     }
-    for (int g0 = 0; g0 < nc; g0 += 3, pr += nprim)
-        eval_piece_group<L, GRAD, 3>(poly, x, y, z, r2, pr, nprim, min(3, nc - g0), g0 * (2 * L + 1), sink);
+    constexpr int kRecs = sizeof(T) == 8 ? 2 : 1;   // records per primitive
+    for (int g0 = 0; g0 < nc; g0 += 3, pr += kRecs * nprim)
+        eval_piece_group<T, L, GRAD, 3>(poly, x, y, z, r2, pr, nprim, min(3, nc - g0), g0 * (2 * L + 1), sink);
 }
 
-template <bool GRAD, int LMAX, class Sink>
-__device__ __forceinline__ void eval_piece(int l, float x, float y, float z, float r2, const float4* pr, int nprim,
-                                           int nc, Sink& sink) {
+template <class T, bool GRAD, int LMAX, class Sink>
+__device__ __forceinline__ void eval_piece(int l, T x, T y, T z, T r2, const typename PackedPrim<T>::rec* pr,
+                                           int nprim, int nc, Sink& sink) {
     switch (l) {
-    case 0: eval_piece_core<0, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
-    case 1: if constexpr (LMAX >= 1) eval_piece_core<1, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
-    case 2: if constexpr (LMAX >= 2) eval_piece_core<2, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
-    case 3: if constexpr (LMAX >= 3) eval_piece_core<3, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
-    case 4: if constexpr (LMAX >= 4) eval_piece_core<4, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
-    case 5: if constexpr (LMAX >= 5) eval_piece_core<5, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
-    default: if constexpr (LMAX >= 6) eval_piece_core<6, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    case 0: eval_piece_core<T, 0, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    case 1: if constexpr (LMAX >= 1) eval_piece_core<T, 1, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    case 2: if constexpr (LMAX >= 2) eval_piece_core<T, 2, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    case 3: if constexpr (LMAX >= 3) eval_piece_core<T, 3, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    case 4: if constexpr (LMAX >= 4) eval_piece_core<T, 4, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    case 5: if constexpr (LMAX >= 5) eval_piece_core<T, 5, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
+    default: if constexpr (LMAX >= 6) eval_piece_core<T, 6, GRAD>(x, y, z, r2, pr, nprim, nc, sink); break;
     }
 }
 

@@ -35,6 +35,8 @@ Context::~Context() {
     cudaFree(d_ao_slot);
     cudaFree(d_piece_rec);
     cudaFree(d_piece_prim);
+    cudaFree(d_piece_c64);
+    cudaFree(d_piece_prim64);
     cudaFree(ws);
 }
 
@@ -128,6 +130,8 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
     std::vector<float> expf_(exps.begin(), exps.end()), coeff_(coefs.begin(), coefs.end());
     c->h_expf = expf_;
     c->h_coeff = coeff_;
+    c->h_exp64 = exps;
+    c->h_coef64 = coefs;
     up(c->d_shells, c->shells);
     up(c->d_exp, exps);
     up(c->d_coef, coefs);
@@ -213,10 +217,16 @@ struct TileSink {
 };
 
 struct TileArgs {
-    const ShellDesc* shells; const void* exps; const void* coefs;
-    const int4* pieces; const int* lane_begin; const int* fill; const int* chunk_ao0; int nchunks;
+    const float4* piece_rec; const double2* piece_c64; const void* prims;   // packed piece records
+    const int* lane_begin; const int* fill; const int* chunk_ao0; int nchunks;
     const double* pts; int64_t n, ld; void* val; void* grad; bool want_val;
 };
+
+// The packed primitive table of T (float4 entries, or two double2 per entry).
+template <class T>
+__device__ __forceinline__ const typename PackedPrim<T>::rec* packed_prims(const void* p, int prim_off) {
+    return static_cast<const typename PackedPrim<T>::rec*>(p) + (sizeof(T) == 8 ? 2 : 1) * prim_off;
+}
 
 template <class T, bool GRAD>
 constexpr size_t tile_smem_bytes() {
@@ -237,8 +247,6 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) ao_tile_kernel(TileA
     const bool valid = g < a.n;
     const double px = valid ? a.pts[3 * g] : 0.0, py = valid ? a.pts[3 * g + 1] : 0.0,
                  pz = valid ? a.pts[3 * g + 2] : 0.0;
-    const T* exps = static_cast<const T*>(a.exps);
-    const T* coefs = static_cast<const T*>(a.coefs);
     // output row of (component, point), or null where nothing is written
     for (int i = threadIdx.x; i < kNComp * kTilePts; i += blockDim.x) {
         const int cc = i / kTilePts;
@@ -257,20 +265,24 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) ao_tile_kernel(TileA
     for (int c = 0; c < a.nchunks; ++c) {
         const int pb = a.lane_begin[c * PPT + lanegrp], pe = a.lane_begin[c * PPT + lanegrp + 1];
         for (int pi = pb; pi < pe; ++pi) {
-            const int4 pc = a.pieces[pi];
-            const ShellDesc b = a.shells[pc.x];
-            const int ns = 2 * b.l + 1;
-            const double dx = px - b.x, dy = py - b.y, dz = pz - b.z;
+            // packed record: (l, primitives, contractions, first slot), centre and
+            // smallest exponent, primitive-table offset
+            const int4 meta = __ldg(reinterpret_cast<const int4*>(a.piece_rec) + 3 * pi + 2);
+            const int poff = __float_as_int(__ldg(a.piece_rec + 3 * pi + 1).w);
+            const double2 cxy = __ldg(a.piece_c64 + 2 * pi), cza = __ldg(a.piece_c64 + 2 * pi + 1);
+            const int l = meta.x, nprim = meta.y, nc = meta.z, slot0 = meta.w;
+            const int ns = 2 * l + 1;
+            const double dx = px - cxy.x, dy = py - cxy.y, dz = pz - cza.x;
             const double r2 = dx * dx + dy * dy + dz * dz;
-            if (__all_sync(0xffffffffu, !valid || static_cast<double>(b.amin) * r2 > cut)) {
-                for (int k = pc.w; k < pc.w + pc.z * ns; ++k)
+            if (__all_sync(0xffffffffu, !valid || cza.y * r2 > cut)) {
+                for (int k = slot0; k < slot0 + nc * ns; ++k)
 #pragma unroll
                     for (int cc = 0; cc < kNComp; ++cc) st[(cc * 32 + k) * kTileStride + p] = T(0);
                 continue;
             }
-            TileSink<T> sink{st, p, pc.w - (b.ao_off + pc.y * ns)};
-            eval_shell_rel<T, GRAD, LMAX>(b, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
-                                          static_cast<T>(r2), exps, coefs, sink, pc.y, pc.y + pc.z);
+            TileSink<T> sink{st, p, slot0};
+            eval_piece<T, GRAD, LMAX>(l, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
+                                      static_cast<T>(r2), packed_prims<T>(a.prims, poff), nprim, nc, sink);
         }
         __syncthreads();
         const int fill = a.fill[c], ao0 = a.chunk_ao0[c];
@@ -319,8 +331,8 @@ struct TileSqSink {
 };
 
 struct AxisTileArgs {
-    const ShellDesc* shells; const void* exps; const void* coefs;
-    const int4* pieces; const int* lane_begin; const int* fill; const int* chunk_ao0; int nchunks;
+    const float4* piece_rec; const double2* piece_c64; const void* prims;   // packed piece records
+    const int* lane_begin; const int* fill; const int* chunk_ao0; int nchunks;
     const double* pts; const int64_t* index; int64_t n; const double* weights;
     void* out; int64_t ld; double* sumsq;
     int nent; int comp[16]; int off[16]; double scale[16];   // the non-occupied axis entries
@@ -348,8 +360,6 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) axis_tile_kernel(Axi
     const double px = valid ? a.pts[3 * gi] : 0.0, py = valid ? a.pts[3 * gi + 1] : 0.0,
                  pz = valid ? a.pts[3 * gi + 2] : 0.0;
     const bool count = valid && a.sumsq != nullptr && (a.weights == nullptr || a.weights[gi] != 0.0);
-    const T* exps = static_cast<const T*>(a.exps);
-    const T* coefs = static_cast<const T*>(a.coefs);
     for (int i = threadIdx.x; i < kTilePts; i += blockDim.x) {
         const int64_t gp = b0 + i;
         rowp[i] = gp < a.n ? static_cast<T*>(a.out) + gp * a.ld : nullptr;
@@ -359,20 +369,22 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) axis_tile_kernel(Axi
     for (int c = 0; c < a.nchunks; ++c) {
         const int pb = a.lane_begin[c * PPT + lanegrp], pe = a.lane_begin[c * PPT + lanegrp + 1];
         for (int pi = pb; pi < pe; ++pi) {
-            const int4 pc = a.pieces[pi];
-            const ShellDesc b = a.shells[pc.x];
-            const int ns = 2 * b.l + 1;
-            const double dx = px - b.x, dy = py - b.y, dz = pz - b.z;
+            const int4 meta = __ldg(reinterpret_cast<const int4*>(a.piece_rec) + 3 * pi + 2);
+            const int poff = __float_as_int(__ldg(a.piece_rec + 3 * pi + 1).w);
+            const double2 cxy = __ldg(a.piece_c64 + 2 * pi), cza = __ldg(a.piece_c64 + 2 * pi + 1);
+            const int l = meta.x, nprim = meta.y, nc = meta.z, slot0 = meta.w;
+            const int ns = 2 * l + 1;
+            const double dx = px - cxy.x, dy = py - cxy.y, dz = pz - cza.x;
             const double r2 = dx * dx + dy * dy + dz * dz;
-            if (__all_sync(0xffffffffu, !valid || static_cast<double>(b.amin) * r2 > cut)) {
-                for (int k = pc.w; k < pc.w + pc.z * ns; ++k)
+            if (__all_sync(0xffffffffu, !valid || cza.y * r2 > cut)) {
+                for (int k = slot0; k < slot0 + nc * ns; ++k)
 #pragma unroll
                     for (int cc = 0; cc < kNComp; ++cc) st[(cc * 32 + k) * kTileStride + p] = T(0);
                 continue;
             }
-            TileSqSink<T> sink{st, p, pc.w - (b.ao_off + pc.y * ns), count, {0.0, 0.0, 0.0, 0.0}};
-            eval_shell_rel<T, GRAD, LMAX>(b, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
-                                          static_cast<T>(r2), exps, coefs, sink, pc.y, pc.y + pc.z);
+            TileSqSink<T> sink{st, p, slot0, count, {0.0, 0.0, 0.0, 0.0}};
+            eval_piece<T, GRAD, LMAX>(l, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
+                                      static_cast<T>(r2), packed_prims<T>(a.prims, poff), nprim, nc, sink);
 #pragma unroll
             for (int cc = 0; cc < 4; ++cc) sq[cc] += sink.sq[cc];
         }
@@ -486,6 +498,9 @@ __global__ void occ_block_kernel(double* out, int64_t ld, int64_t n, int nocc, d
 template <class T> const T* exps_of(const Context& c);
 template <> const double* exps_of<double>(const Context& c) { return c.d_exp; }
 template <> const float* exps_of<float>(const Context& c) { return c.d_expf; }
+template <class T> const void* prims_of(const Context& c);
+template <> const void* prims_of<double>(const Context& c) { return c.d_piece_prim64; }
+template <> const void* prims_of<float>(const Context& c) { return c.d_piece_prim; }
 template <class T> const T* coefs_of(const Context& c);
 template <> const double* coefs_of<double>(const Context& c) { return c.d_coef; }
 template <> const float* coefs_of<float>(const Context& c) { return c.d_coeff; }
@@ -502,7 +517,7 @@ void eval_ao(const Context& c, const double* pts, int64_t n, T* out_val, T* out_
     // spread over the block; otherwise 32 points x 4 shell lanes
     const bool few = n <= 2048;
     if (!few) {
-        TileArgs a{c.d_shells, exps_of<T>(c), coefs_of<T>(c), c.d_pieces, c.d_piece_begin, c.d_fill,
+        TileArgs a{c.d_piece_rec, c.d_piece_c64, prims_of<T>(c), c.d_piece_begin, c.d_fill,
                    c.d_chunk_ao0, c.nchunks, pts, n, ld, out_val, out_grad, out_val != nullptr};
         if (out_grad) launch_tile_l<T, true>(c, a, s);
         else launch_tile_l<T, false>(c, a, s);
@@ -535,7 +550,7 @@ void eval_axis_features(const Context& c, const double* pts, const int64_t* inde
     const bool grad = (ax.need_mask & 0xE) != 0;
     if (n > 2048) {
         // tiled: contiguous row stores per (axis entry, point) and K-chunk
-        AxisTileArgs ta{c.d_shells, exps_of<T>(c), coefs_of<T>(c), c.d_pieces, c.d_piece_begin, c.d_fill,
+        AxisTileArgs ta{c.d_piece_rec, c.d_piece_c64, prims_of<T>(c), c.d_piece_begin, c.d_fill,
                         c.d_chunk_ao0, c.nchunks, pts, index, n, weights, out, ld, sumsq, 0, {}, {}, {}};
         for (int e = 0; e < ax.naxes; ++e) {
             if (ax.occ[e]) continue;

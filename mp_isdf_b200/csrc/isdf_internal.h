@@ -152,8 +152,14 @@ struct Context {
     // (alpha, c_j, c_j+1, c_j+2) at prim_off (FP32, zero-padded contractions).
     float4* d_piece_rec = nullptr;
     float4* d_piece_prim = nullptr;
+    // FP64 twins for the tiled evaluators: centre and smallest exponent as two
+    // double2 (x, y), (z, amin) per piece, and two double2 (alpha, c_j),
+    // (c_j+1, c_j+2) per entry of the primitive table (same entry index).
+    double2* d_piece_c64 = nullptr;
+    double2* d_piece_prim64 = nullptr;
     std::vector<int4> h_pieces;           // host copy of the pieces
     std::vector<float> h_expf, h_coeff;   // host FP32 exponents / coefficients (shell order)
+    std::vector<double> h_exp64, h_coef64;   // the same in FP64
     // Grow-only device workspace of the fused selection + fit (the stored AO
     // tiles and the sketch projections), kept across calls so that repeated
     // calls allocate nothing large; a call holds ws_mu while it uses it.

@@ -252,8 +252,8 @@ project_tc_kernel(ProjectArgs args) {
                             continue;
                         }
                         StageSink sink{sStage, p, slot0, {0.f, 0.f, 0.f, 0.f}};
-                        eval_piece<GRAD, LMAX>(l, dx, dy, dz, r2, args.piece_prim + __float_as_int(cl.w), nprim, nc,
-                                               sink);
+                        eval_piece<float, GRAD, LMAX>(l, dx, dy, dz, r2, args.piece_prim + __float_as_int(cl.w), nprim,
+                                                      nc, sink);
 #pragma unroll
                         for (int cc = 0; cc < 4; ++cc) csq[cc] += sink.sq[cc];
                     }
@@ -513,9 +513,12 @@ void build_chunk_layout(Context& c) {
 
 void upload_piece_records(Context& c) {
     std::vector<float4> rec, prim;
+    std::vector<double2> c64, prim64;
     rec.reserve(c.h_pieces.size() * 3);
     for (const int4& pc : c.h_pieces) {
         const ShellDesc& sh = c.shells[pc.x];
+        c64.push_back(make_double2(sh.x, sh.y));
+        c64.push_back(make_double2(sh.z, static_cast<double>(sh.amin)));
         const float xh = static_cast<float>(sh.x), yh = static_cast<float>(sh.y), zh = static_cast<float>(sh.z);
         const int off = static_cast<int>(prim.size());
         rec.push_back(make_float4(xh, yh, zh, sh.amin));
@@ -527,18 +530,29 @@ void upload_piece_records(Context& c) {
         rec.push_back(mf);
         for (int g0 = 0; g0 < pc.z; g0 += 3)
             for (int p = 0; p < sh.nprim; ++p) {
-                float cc[3] = {0.f, 0.f, 0.f};
+                double cc[3] = {0.0, 0.0, 0.0};
                 for (int j = 0; j < 3 && g0 + j < pc.z; ++j)
-                    cc[j] = c.h_coeff[sh.coef_off + (pc.y + g0 + j) * sh.nprim + p];
-                prim.push_back(make_float4(c.h_expf[sh.prim_off + p], cc[0], cc[1], cc[2]));
+                    cc[j] = c.h_coef64[sh.coef_off + (pc.y + g0 + j) * sh.nprim + p];
+                const double a = c.h_exp64[sh.prim_off + p];
+                prim.push_back(make_float4(static_cast<float>(a), static_cast<float>(cc[0]),
+                                           static_cast<float>(cc[1]), static_cast<float>(cc[2])));
+                prim64.push_back(make_double2(a, cc[0]));
+                prim64.push_back(make_double2(cc[1], cc[2]));
             }
     }
     if (rec.empty()) rec.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
     if (prim.empty()) prim.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
-    if (!c.d_piece_rec) ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c.d_piece_rec), rec.size() * sizeof(float4)));
-    if (!c.d_piece_prim) ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c.d_piece_prim), prim.size() * sizeof(float4)));
-    ISDF_CUDA(cudaMemcpy(c.d_piece_rec, rec.data(), rec.size() * sizeof(float4), cudaMemcpyHostToDevice));
-    ISDF_CUDA(cudaMemcpy(c.d_piece_prim, prim.data(), prim.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    if (c64.empty()) c64.push_back(make_double2(0.0, 0.0));
+    if (prim64.empty()) prim64.push_back(make_double2(0.0, 0.0));
+    auto put = [](auto*& dst, const auto& src) {
+        using V = std::remove_pointer_t<std::remove_reference_t<decltype(dst)>>;
+        if (!dst) ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&dst), src.size() * sizeof(V)));
+        ISDF_CUDA(cudaMemcpy(dst, src.data(), src.size() * sizeof(V), cudaMemcpyHostToDevice));
+    };
+    put(c.d_piece_rec, rec);
+    put(c.d_piece_prim, prim);
+    put(c.d_piece_c64, c64);
+    put(c.d_piece_prim64, prim64);
 }
 
 namespace {
