@@ -151,10 +151,19 @@ def peaks():
 
 
 # DRAM bytes per kept grid point of one launch, from an ncu capture of the
-# 454035-point (H2O)64 case (dram__bytes_read.sum + dram__bytes_write.sum);
-# the kernel streams per-point data, so the traffic scales with the points.
-MEASURED_TRAFFIC_PER_POINT = {"project_tc_grad": 7211.0}
-TRAFFIC_SOURCE = "ncu dram bytes of a 454035-point capture, scaled by kept points"
+# (H2O)64 case cut to 397312 grid points / 363237 kept points
+# (dram__bytes_read.sum + dram__bytes_write.sum = 54.9 MB + 3735.2 MB); the
+# kernel streams per-point data, so the traffic scales with the points.
+MEASURED_TRAFFIC_PER_POINT = {"project_tc_grad": 10434.0}
+TRAFFIC_SOURCE = "ncu dram bytes of a 363237-kept-point capture, scaled by kept points"
+
+# ncu figures of the adjoint's fused grid kernel (one launch, --set full)
+ADJOINT_PROFILE = {
+    "kernel": "adjoint_grid_kernel<2, 8, 1>",
+    "workload": "(H2O)8, 192 AOs, 46608 kept points, 8 anchors",
+    "issue_active_frac": 0.302, "fp64_pipe_frac": 0.173, "warps_active_frac": 0.125,
+    "registers_per_thread": 255, "summary": "profiles/adjoint_grid_kernel_c4_fp64.md",
+}
 
 
 def inputs_axis_comp(name):
@@ -244,7 +253,7 @@ def time_adjoint(ctx, mol, x, wt, anchors, cfg, steps=3):
         times.append(a.elapsed_time(b) / 1e3)
     return {"s": statistics.mean(times), "step_times_s": times, "energy": e,
             "grad_norm": float(np.linalg.norm(g)), "form": "FP64, fused grid pass: AO values and gradients recomputed per 128-point tile, never stored",
-            "electrons": cfg["electrons"]}
+            "electrons": cfg["electrons"], "ncu": ADJOINT_PROFILE}
 
 
 def _event_time(fn, reps=2):
