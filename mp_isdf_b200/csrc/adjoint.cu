@@ -149,6 +149,7 @@ __global__ void matvec_kernel(int k, const double* __restrict__ T, const double*
 constexpr int kAdjPts = 128;      // points per tile
 constexpr int kAdjLanes = 2;      // shell lanes per point
 constexpr int kAdjMaxAtoms = 1024;
+constexpr double kAdjCut = kExpCut * 1.0001;   // margin for the FP32 screening exponent
 
 struct AdjGridArgs {
     const ShellDesc* shells;
@@ -239,11 +240,15 @@ __global__ void __launch_bounds__(kAdjPts * kAdjLanes, 1) adjoint_grid_kernel(Ad
         GramSink<KMAX> gs{args.phia, args.nao, {}};
 #pragma unroll
         for (int a = 0; a < KMAX; ++a) gs.G[a] = 0.0;
-        if (valid)
-            for (int sh = sl; sh < args.nshell; sh += kAdjLanes) {
-                const ShellDesc b = args.shells[sh];
-                eval_shell_any<double, false, LMAX>(b, px - b.x, py - b.y, pz - b.z, args.exps, args.coefs, gs);
-            }
+        // a shell whose FP64 screening exponent puts all 32 points of the warp
+        // beyond kExpCut is skipped (no value or gradient above kScreenFp64);
+        // the shell loop is uniform over the warp (sl is)
+        for (int sh = sl; sh < args.nshell; sh += kAdjLanes) {
+            const ShellDesc b = args.shells[sh];
+            const double dx = px - b.x, dy = py - b.y, dz = pz - b.z;
+            if (__all_sync(0xffffffffu, !valid || b.scr64 * (dx * dx + dy * dy + dz * dz) > kAdjCut)) continue;
+            if (valid) eval_shell_any<double, false, LMAX>(b, dx, dy, dz, args.exps, args.coefs, gs);
+        }
 #pragma unroll
         for (int a = 0; a < KMAX; ++a) Gs[(sl * kAdjPts + p) * KMAX + a] = gs.G[a];
         __syncthreads();
@@ -275,9 +280,10 @@ __global__ void __launch_bounds__(kAdjPts * kAdjLanes, 1) adjoint_grid_kernel(Ad
         for (int a = 0; a < KMAX; ++a) gr.al[a] = As[p * KMAX + a];
         for (int sh = sl; sh < args.nshell; sh += kAdjLanes) {
             const ShellDesc b = args.shells[sh];
+            const double dx = px - b.x, dy = py - b.y, dz = pz - b.z;
+            if (__all_sync(0xffffffffu, !valid || b.scr64 * (dx * dx + dy * dy + dz * dz) > kAdjCut)) continue;
             gr.acc[0] = gr.acc[1] = gr.acc[2] = 0.0;
-            if (valid)
-                eval_shell_any<double, true, LMAX>(b, px - b.x, py - b.y, pz - b.z, args.exps, args.coefs, gr);
+            if (valid) eval_shell_any<double, true, LMAX>(b, dx, dy, dz, args.exps, args.coefs, gr);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 const double r = warp_allsum(gr.acc[c]);
@@ -361,7 +367,7 @@ AdjointResult energy_gradient(const Context& c, const double* pts, const double*
     ISDF_LAUNCH_CHECK();
     gemm_f64(k, k, nao, f.phi_a.get(), nao, 0, f.phi_aT.get(), k, 0, S.get(), k, 0, 1, false, s);
 
-    const int kmax = k <= 8 ? 8 : k <= 16 ? 16 : 32;
+    const int kmax = k <= 4 ? 4 : k <= 8 ? 8 : k <= 12 ? 12 : k <= 16 ? 16 : 32;
     const size_t fused_smem =
         (static_cast<size_t>(kAdjLanes + 1) * kAdjPts * kmax + 3 * c.natm + kmax + 1) * sizeof(double);
     const bool fused = k <= 32 && c.natm <= kAdjMaxAtoms && fused_smem <= 200 * 1024;
@@ -383,11 +389,15 @@ AdjointResult energy_gradient(const Context& c, const double* pts, const double*
                       kp.index.get(), n, phia_pad.get(), dphia_pad.get(), z_pad.get(), gacc.get(), v.get(),
                       energy.get()};
         if (c.lmax <= 2) {
-            if (kmax == 8) launch_adjoint_grid<2, 8>(a, want_grad, s);
+            if (kmax == 4) launch_adjoint_grid<2, 4>(a, want_grad, s);
+            else if (kmax == 8) launch_adjoint_grid<2, 8>(a, want_grad, s);
+            else if (kmax == 12) launch_adjoint_grid<2, 12>(a, want_grad, s);
             else if (kmax == 16) launch_adjoint_grid<2, 16>(a, want_grad, s);
             else launch_adjoint_grid<2, 32>(a, want_grad, s);
         } else {
-            if (kmax == 8) launch_adjoint_grid<kMaxL, 8>(a, want_grad, s);
+            if (kmax == 4) launch_adjoint_grid<kMaxL, 4>(a, want_grad, s);
+            else if (kmax == 8) launch_adjoint_grid<kMaxL, 8>(a, want_grad, s);
+            else if (kmax == 12) launch_adjoint_grid<kMaxL, 12>(a, want_grad, s);
             else if (kmax == 16) launch_adjoint_grid<kMaxL, 16>(a, want_grad, s);
             else launch_adjoint_grid<kMaxL, 32>(a, want_grad, s);
         }

@@ -65,6 +65,60 @@ uint8_t* Context::workspace(size_t bytes) const {
     return ws;
 }
 
+// Bound on |P_lm(x)| / |x|^l over the components m of the spherical
+// polynomials: the sum of the absolute cartesian coefficients, since every
+// monomial x^a y^b z^c of degree l is at most |x|^l in absolute value.
+static double c2s_abs_bound(int l) {
+    double best = 0.0;
+    const int ncart = (l + 1) * (l + 2) / 2;
+    for (int sidx = 0; sidx < 2 * l + 1; ++sidx) {
+        double sum = 0.0;
+        for (int cidx = 0; cidx < ncart; ++cidx) sum += std::fabs(c2s_coef(l, sidx, cidx));
+        best = std::max(best, sum);
+    }
+    return best;
+}
+
+// Largest value or d/dx, d/dy, d/dz component of any contraction of the
+// shell at a point with amin r^2 >= X.  A primitive term is
+// c exp(-a r^2) P(x) with |P| <= S r^l and |dP/dx| <= l S r^(l-1), so one
+// component is at most |c| S exp(-a r^2) max(r^l, l r^(l-1) + 2 a r^(l+1)).
+// Each of these falls with r where a r^2 >= (l+1)/2, which holds at every
+// r >= r0 = sqrt(X / amin) for X >= (l+1)/2 (a >= amin): the maximum is at r0.
+static double screened_term_bound(int l, int nprim, int nctr, const double* exps, const double* coefs,
+                                  double amin, double X, double S) {
+    const double r0 = std::sqrt(X / amin);
+    double total = 0.0;
+    for (int p = 0; p < nprim; ++p) {
+        double c = 0.0;
+        for (int j = 0; j < nctr; ++j) c = std::max(c, std::fabs(coefs[j * nprim + p]));
+        const double a = exps[p];
+        const double rl = std::pow(r0, l);
+        const double grad = (l > 0 ? l * std::pow(r0, l - 1) : 0.0) + 2.0 * a * r0 * rl;
+        total += c * S * std::exp(-a * r0 * r0) * std::max(rl, grad);
+    }
+    return total;
+}
+
+// Smallest screening argument X in [(l+1)/2 + 1, kExpCut] whose dropped terms
+// stay within eps / 2 (the half leaves room for the FP32 rounding of the
+// screening test); kExpCut (exact zeros only) when none does.
+double screening_argument(int l, int nprim, int nctr, const double* exps, const double* coefs, double eps) {
+    double amin = exps[0];
+    for (int p = 1; p < nprim; ++p) amin = std::min(amin, exps[p]);
+    if (!(amin > 0.0)) return kExpCut;
+    const double S = c2s_abs_bound(l);
+    double lo = 0.5 * (l + 1) + 1.0, hi = kExpCut;
+    if (screened_term_bound(l, nprim, nctr, exps, coefs, amin, hi, S) > 0.5 * eps) return kExpCut;
+    if (screened_term_bound(l, nprim, nctr, exps, coefs, amin, lo, S) <= 0.5 * eps) return lo;
+    for (int it = 0; it < 64; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (screened_term_bound(l, nprim, nctr, exps, coefs, amin, mid, S) <= 0.5 * eps) hi = mid;
+        else lo = mid;
+    }
+    return hi;
+}
+
 Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nbas,
                         const double* env, int64_t nenv) {
     require(natm >= 0 && nbas >= 0 && nenv >= 20, "invalid libcint ATM/BAS/ENV table sizes");
@@ -110,6 +164,13 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
         s.coef_off = static_cast<int>(coefs.size());
         s.atom = atom;
         s.amin = static_cast<float>(*std::min_element(env + b[5], env + b[5] + np));
+        {
+            const double amin = *std::min_element(env + b[5], env + b[5] + np);
+            const double x32 = screening_argument(l, np, nc, env + b[5], env + b[6], kScreenFp32);
+            const double x64 = screening_argument(l, np, nc, env + b[5], env + b[6], kScreenFp64);
+            s.scr32 = static_cast<float>(amin * (kExpCut / x32));
+            s.scr64 = static_cast<float>(amin * (kExpCut / x64));
+        }
         const double* xyz = &c->atom_xyz[3 * atom];
         s.x = xyz[0]; s.y = xyz[1]; s.z = xyz[2];
         exps.insert(exps.end(), env + b[5], env + b[5] + np);
@@ -258,9 +319,9 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) ao_tile_kernel(TileA
         }
         rowp[i] = r;
     }
-    // a piece is skipped where amin r^2 exceeds the cutoff with a margin that
-    // covers amin's rounding to FP32 and r^2's rounding to T, so that every
-    // primitive of the shell is also cut in the evaluation
+    // a piece is written as zeros where its FP64 screening exponent puts all
+    // 32 points of the warp beyond kExpCut (nothing dropped above kScreenFp64);
+    // the margin covers the exponent's rounding to FP32
     const double cut = kExpCut * 1.0001;
     for (int c = 0; c < a.nchunks; ++c) {
         const int pb = a.lane_begin[c * PPT + lanegrp], pe = a.lane_begin[c * PPT + lanegrp + 1];

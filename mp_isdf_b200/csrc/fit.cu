@@ -372,7 +372,8 @@ namespace {
 // FP64; also Theta.w, max |X|, and the terms of an a-posteriori bound on how far
 // the pair error of Theta0 can lie from the FP64 fit's:
 //   excess <= lambda_max(T) * sum_g |w_g| |dh_g|^2,
-//   |dG_ga| <= kFitGramBound |phi_g| |phi_a|  (dh = 2 G dG + dG^2).
+//   |dG_ga| <= (kFitGramBound |phi_g| + trunc) |phi_a|  (dh = 2 G dG + dG^2),
+// trunc = kScreenFp32 sqrt(nao) covering the pieces the fused kernel screened.
 // When the bound exceeds the tolerance (ill-conditioned anchors amplify the
 // split-BF16 error of the anchors' side of G by cond(C)^2), the FP64
 // refinement step below follows.
@@ -386,7 +387,7 @@ fit_mixed_kernel(const float* __restrict__ G, const float* __restrict__ psq, int
                  const double* __restrict__ anorm, const double* __restrict__ wa,
                  const double* __restrict__ w, const int64_t* __restrict__ index,
                  double* __restrict__ theta, int64_t ldt, double* __restrict__ tw,
-                 double* __restrict__ acc) {
+                 double* __restrict__ acc, double trunc) {
     extern __shared__ double sm[];
     double* Ts = sm;                // k*k
     double* Ms = sm + k * k;        // k*k
@@ -410,7 +411,7 @@ fit_mixed_kernel(const float* __restrict__ G, const float* __restrict__ psq, int
             if (a < k) {
                 const double gv = static_cast<double>(G[g * k + a]);
                 h[a] = gv * gv;
-                const double dG = kFitGramBound * fn * anorm[a];
+                const double dG = (kFitGramBound * fn + trunc) * anorm[a];
                 const double dh = 2.0 * fabs(gv) * dG + dG * dG;
                 dh2 += dh * dh;
             }
@@ -489,8 +490,9 @@ __global__ void row_norms_kernel(const double* __restrict__ a, int rows, int col
 // evaluation remains, and it is projected, not amplified: the pair-error
 // excess is
 //     sum_g |w_g| |P_C dp_g|^2 <= sum_g |w_g| |dp_g|^2,  |dp_g| <= 2 |x_g| d_g + d_g^2,
-// with d_g = 2^-19 |x_g| bounding |x_g - phi_g| (twice the largest 2-norm
-// error of the FP32 AO values measured against FP64 ones).
+// with d_g = 2^-19 |x_g| + trunc bounding |x_g - phi_g| (2^-19: twice the
+// largest 2-norm error of the FP32 AO values measured against FP64 ones;
+// trunc = kScreenFp32 sqrt(nao): the pieces the fused kernel screened).
 namespace {
 
 constexpr double kFp32EvalError = 1.0 / 524288.0;   // 2^-19
@@ -615,7 +617,7 @@ __global__ void __launch_bounds__(256)
 refine_update_kernel(const double* __restrict__ H, const double* __restrict__ qv, int64_t n, int k,
                      const double* __restrict__ T, const double* __restrict__ M, const double* __restrict__ wa,
                      const double* __restrict__ w, const int64_t* __restrict__ index, double* __restrict__ theta,
-                     int64_t ldt, double* __restrict__ tw, double* __restrict__ acc) {
+                     int64_t ldt, double* __restrict__ tw, double* __restrict__ acc, double trunc) {
     __shared__ double red[8];
     __shared__ double tws[64];
     for (int i = threadIdx.x; i < k; i += blockDim.x) tws[i] = 0.0;
@@ -654,7 +656,7 @@ refine_update_kernel(const double* __restrict__ H, const double* __restrict__ qv
         e2 = aw * (q * q - 2.0 * xh + xmx);
         q2 = aw * q * q;
         const double xn = sqrt(q);
-        const double d = kFp32EvalError * xn;
+        const double d = kFp32EvalError * xn + trunc;
         const double dp = 2.0 * xn * d + d * d;
         b2 = aw * dp * dp;
     }
@@ -699,7 +701,7 @@ void launch_refine_gram(const uint8_t* tiles, const uint8_t* tiles_r, int nchunk
 void refine_theta(int kmax, const uint8_t* tiles, const uint8_t* tiles_r, int nchunks, int64_t n, int k,
                   const double* img,
                   const AnchorFactor& f, const double* w, const int64_t* index, double* theta, int64_t ldt,
-                  double* H, double* q, double* tw, double* acc, cudaStream_t s) {
+                  double* H, double* q, double* tw, double* acc, double trunc, cudaStream_t s) {
     switch (kmax) {
     case 4: launch_refine_gram<4>(tiles, tiles_r, nchunks, n, k, img, H, q, s); break;
     case 8: launch_refine_gram<8>(tiles, tiles_r, nchunks, n, k, img, H, q, s); break;
@@ -709,7 +711,7 @@ void refine_theta(int kmax, const uint8_t* tiles, const uint8_t* tiles_r, int nc
     default: launch_refine_gram<32>(tiles, tiles_r, nchunks, n, k, img, H, q, s); break;
     }
     refine_update_kernel<<<blocks_for(n), 256, 0, s>>>(H, q, n, k, f.T.get(), f.M.get(), f.wa.get(), w, index,
-                                                     theta, ldt, tw, acc);
+                                                     theta, ldt, tw, acc, trunc);
     ISDF_LAUNCH_CHECK();
 }
 
@@ -763,6 +765,7 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
     const int64_t per = (ntiles + nchunk - 1) / nchunk * 128;
     const size_t smem = static_cast<size_t>(2 * k * k + k) * sizeof(double);
     auto kern = k <= 16 ? fit_mixed_kernel<16> : k <= 32 ? fit_mixed_kernel<32> : fit_mixed_kernel<64>;
+    const double trunc = kScreenFp32 * std::sqrt(static_cast<double>(c.nao));
     // 1. the tensor-core first iterate Theta0 and its a-posteriori bound
     for (int64_t g0 = 0; g0 < n; g0 += per) {
         const int64_t m = std::min(per, n - g0);
@@ -773,7 +776,8 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
             ISDF_PROFILE("fit_mixed", s);
             kern<<<blocks_for(m), 256, smem, s>>>(G.get() + g0 * k, point_sq + g0 * 4, m, static_cast<int>(k),
                                                   f.T.get(), f.M.get(), anorm.get(), f.wa.get(), w,
-                                                  kp.index.get() + g0, theta + g0, ldt, tw.get(), acc.get());
+                                                  kp.index.get() + g0, theta + g0, ldt, tw.get(), acc.get(),
+                                                  trunc);
             ISDF_LAUNCH_CHECK();
         }
         if (on_chunk && ao_tiles) (*on_chunk)(g0, m);
@@ -816,7 +820,7 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
         ISDF_PROFILE("fit_refine", s);
         refine_theta(kmax, tiles + stored_tile_bytes(c, g0), tiles_r + stored_remainder_bytes(c, g0), c.nchunks, m,
                      static_cast<int>(k), img.get(), f, w, kp.index.get() + g0, theta + g0, ldt, H64.get(),
-                     q64.get(), rtw.get(), racc.get(), s);
+                     q64.get(), rtw.get(), racc.get(), trunc, s);
     }
     double r[4];
     ISDF_CUDA(cudaMemcpyAsync(r, racc.get(), sizeof(r), cudaMemcpyDeviceToHost, s));

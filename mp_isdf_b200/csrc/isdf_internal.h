@@ -15,6 +15,17 @@ constexpr int kMaxL = 6;          // highest angular momentum the AO kernels han
 constexpr int kMaxCtrGroup = 4;   // contractions evaluated per exponential sweep
 constexpr double kExpCut = 100.0; // alpha*r^2 beyond which a primitive is skipped (<4e-44)
 
+// Piece screening of the tiled evaluators.  A piece (contraction group of one
+// shell) is written as zeros for a warp of points where amin r^2 >= X_sh at all
+// of them; X_sh <= kExpCut is chosen per shell (screening_argument) so that no
+// value or d/dx, d/dy, d/dz component dropped that way exceeds kScreenFp64 in
+// absolute value (FP64 tables: far below the reference's AO tolerance of
+// 1e-12) or kScreenFp32 (the FP32 tables of the fused projection, whose error
+// bounds carry it as an absolute term).  The one-point-per-block kernels and
+// the FP64 re-verification do not screen.
+constexpr double kScreenFp64 = 1e-15;
+constexpr double kScreenFp32 = 1e-11;
+
 // ---- errors -----------------------------------------------------------------
 struct Error : std::runtime_error {
     int code;
@@ -111,6 +122,9 @@ struct ShellDesc {
     int coef_off;   // coefficients [nctr][nprim] at coef_off
     int atom;
     float amin;     // smallest exponent: the shell is exactly zero where amin r^2 > kExpCut
+    // screening exponents amin * kExpCut / X_sh for the FP32 and FP64 bounds:
+    // the piece is dropped for a warp where scr r^2 > kExpCut at every point
+    float scr32, scr64;
     double x, y, z;
 };
 

@@ -12,8 +12,9 @@
 //   * the fit Gram G[g][k] = phi_g . phi_a(k) (AO values only).
 // K-chunks hold whole contraction groups ("pieces") padded to 32 slots, so a
 // producer thread evaluates each (point, piece) once, writes its values at
-// fixed slots and needs no range checks.  A piece whose every primitive is
-// beyond the exponent cutoff at a point is exactly zero there and skipped.
+// fixed slots and needs no range checks.  A piece is written as zeros for a
+// warp of points that all lie beyond its shell's FP32 screening radius (no
+// dropped value or gradient above kScreenFp32).
 // The per-component sums of squares of the FP32 values are accumulated (FP32
 // per piece, FP64 across pieces) for the multi-axis Frobenius scales and the
 // error bounds.
@@ -240,12 +241,12 @@ project_tc_kernel(ProjectArgs args) {
                         const float dy = (pyh - ch.y) + (pyl - cl.y);
                         const float dz = (pzh - ch.z) + (pzl - cl.z);
                         const float r2 = dx * dx + dy * dy + dz * dz;
-                        // the same r2 decides the screening and every primitive's cutoff:
-                        // a point beyond the cutoff of the shell's smallest exponent gets
-                        // exact zeros from the evaluation too, so the zero fill is taken
-                        // only when it holds for the whole warp (no divergent paths)
+                        // ch.w is the shell's FP32 screening exponent: where it puts
+                        // every point of the warp beyond kExpCut, no value or gradient
+                        // of the piece exceeds kScreenFp32 there (the mixed form's error
+                        // bounds carry that as an absolute term); taken only for the
+                        // whole warp, so the evaluation does not split
                         if (__all_sync(__activemask(), ch.w * r2 > static_cast<float>(kExpCut))) {
-                            // every primitive is cut off: the piece is exactly zero here
                             for (int k = slot0; k < slot0 + nc * ns; ++k)
 #pragma unroll
                                 for (int cc = 0; cc < kNComp; ++cc) sStage[(cc * kChunk + k) * kRows + p] = 0.f;
@@ -518,10 +519,11 @@ void upload_piece_records(Context& c) {
     for (const int4& pc : c.h_pieces) {
         const ShellDesc& sh = c.shells[pc.x];
         c64.push_back(make_double2(sh.x, sh.y));
-        c64.push_back(make_double2(sh.z, static_cast<double>(sh.amin)));
+        // the screening exponents (FP64 table: kScreenFp64, FP32: kScreenFp32)
+        c64.push_back(make_double2(sh.z, static_cast<double>(sh.scr64)));
         const float xh = static_cast<float>(sh.x), yh = static_cast<float>(sh.y), zh = static_cast<float>(sh.z);
         const int off = static_cast<int>(prim.size());
-        rec.push_back(make_float4(xh, yh, zh, sh.amin));
+        rec.push_back(make_float4(xh, yh, zh, sh.scr32));
         rec.push_back(make_float4(static_cast<float>(sh.x - xh), static_cast<float>(sh.y - yh),
                                   static_cast<float>(sh.z - zh), __int_as_float_host(off)));
         int4 meta = make_int4(sh.l, sh.nprim, pc.z, pc.w);

@@ -718,15 +718,47 @@ namespace {
 // representation error: |d(f.u)| <= kSplitBf16Bound * |f| * |u_scale|.
 constexpr double kSplitBf16Bound = 1.5e-4;
 
+// Per-axis absolute column sums A[a][t] = sum_mu |f[(a*nao + mu)*ell + t]| of
+// a sketch factor (rows j = a*nao + mu, ell columns).
+std::vector<double> factor_abs_sums(const HostFactors& f, int naxes, int64_t nao, int64_t ell) {
+    std::vector<double> out(static_cast<size_t>(naxes) * ell, 0.0);
+    for (int a = 0; a < naxes; ++a)
+        for (int64_t mu = 0; mu < nao; ++mu) {
+            const double* row = f.data() + (a * nao + mu) * ell;
+            double* o = out.data() + a * ell;
+            for (int64_t t = 0; t < ell; ++t) o[t] += std::fabs(row[t]);
+        }
+    return out;
+}
+
+// Bound on how far any projection f_g . u_s or f_g . v_s (axis entries scaled
+// by sc) moves when every feature entry is off by at most eps: the screening
+// of the fused kernel's FP32 evaluation (kScreenFp32 per value or gradient).
+double projection_abs_error(const std::vector<double>& au, const std::vector<double>& av,
+                            const std::vector<double>& sc, int64_t ell, double eps) {
+    double worst = 0.0;
+    for (int64_t t = 0; t < ell; ++t) {
+        double su = 0.0, sv = 0.0;
+        for (size_t a = 0; a < sc.size(); ++a) {
+            su += sc[a] * au[a * ell + t];
+            sv += sc[a] * av[a * ell + t];
+        }
+        worst = std::max(worst, std::max(su, sv));
+    }
+    return eps * worst;
+}
+
 // Yt[s][g] = sw/sqrt(ell) L_s R_s from the FP32 per-axis partials, and the
-// absolute error bound of the column's norm:
-//   delta_g = k * sw/sqrt(ell) * |f_g| * sqrt(sum_s (|L_s| + |R_s| + k|f_g|)^2)
+// absolute error bound of the column's norm: with e = k|f_g| + tabs bounding
+// the error of each partial (split-BF16 products, and tabs for the screened
+// pieces),
+//   delta_g = sw/sqrt(ell) * e * sqrt(sum_s (|L_s| + |R_s| + e)^2)
 __global__ void combine_mixed_kernel(const float* __restrict__ P, const float* __restrict__ psq,
                                      int naxes, const int* __restrict__ comp, int64_t ell,
                                      const double* __restrict__ scales, const double* __restrict__ w,
                                      const int64_t* __restrict__ index, int64_t n,
                                      double* __restrict__ Yt, int64_t ldy, double* __restrict__ delta,
-                                     int* __restrict__ bad) {
+                                     int* __restrict__ bad, double tabs) {
     const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (g >= n) return;
     const double sw = sqrt(fabs(w[index[g]])) / sqrt(static_cast<double>(ell));
@@ -737,7 +769,7 @@ __global__ void combine_mixed_kernel(const float* __restrict__ P, const float* _
         f2 += sc * sc * static_cast<double>(psq[g * 4 + comp[a]]);
     }
     const double fn = sqrt(f2);
-    const double k = kSplitBf16Bound;
+    const double e_abs = kSplitBf16Bound * fn + tabs;
     double bound2 = 0;
     bool ok = true;
     for (int64_t s = 0; s < ell; ++s) {
@@ -750,10 +782,10 @@ __global__ void combine_mixed_kernel(const float* __restrict__ P, const float* _
         const double y = sw * left * right;
         ok = ok && isfinite(y);
         Yt[s * ldy + g] = y;
-        const double e = fabs(left) + fabs(right) + k * fn;
+        const double e = fabs(left) + fabs(right) + e_abs;
         bound2 += e * e;
     }
-    delta[g] = k * sw * fn * sqrt(bound2);
+    delta[g] = sw * e_abs * sqrt(bound2);
     if (!ok) atomicOr(bad, 1);
 }
 
@@ -834,6 +866,9 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     // column-major projections P[a*nout + j][g] (coalesced for the combine pass)
     project_tc(c, plan, pts, kp.index.get(), n, w, P, 1, n, sumsq.get(), psq.get(),
                err.get(), s, tiles, std::max(store_axis, 0), tiles_r);
+    // host work under the kernel: the factors' absolute column sums for the
+    // screening term of the error bounds
+    const std::vector<double> au = factor_abs_sums(u, naxes, nao, ell), av = factor_abs_sums(v, naxes, nao, ell);
     double h[4] = {0, 0, 0, 0};
     int herr = 0;
     ISDF_CUDA(cudaMemcpyAsync(h, sumsq.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -852,7 +887,8 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
         ISDF_PROFILE("sketch_combine", s);
         combine_mixed_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(
             P, psq.get(), naxes, dcomp.get(), ell, naxes > 1 ? ms.scales.get() : nullptr, w,
-            kp.index.get(), n, Yt, ldy, ms.delta.get(), bad.get());
+            kp.index.get(), n, Yt, ldy, ms.delta.get(), bad.get(),
+            projection_abs_error(au, av, sc, ell, kScreenFp32));
         ISDF_LAUNCH_CHECK();
     }
     int hbad = 0;
@@ -1155,7 +1191,9 @@ void sketch_shard_combine(const Context& c, SketchShard& st, const double* sumsq
         ISDF_PROFILE("sketch_combine", s);
         combine_mixed_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(
             st.Pf.get(), st.psq.get(), naxes, dcomp.get(), ell, naxes > 1 ? dsc.get() : nullptr, st.w,
-            st.kp.index.get(), n, Yt, n, delta, bad.get());
+            st.kp.index.get(), n, Yt, n, delta, bad.get(),
+            projection_abs_error(factor_abs_sums(st.u, naxes, c.nao, ell), factor_abs_sums(st.v, naxes, c.nao, ell),
+                                 scales, ell, kScreenFp32));
         ISDF_LAUNCH_CHECK();
         ISDF_CUDA(cudaStreamSynchronize(s));
     } else {
