@@ -33,6 +33,7 @@ Context::~Context() {
     cudaFree(d_fill);
     cudaFree(d_chunk_ao0);
     cudaFree(d_ao_slot);
+    cudaFree(d_piece_chunk);
     cudaFree(d_piece_rec);
     cudaFree(d_piece_prim);
     cudaFree(d_piece_c64);

@@ -159,15 +159,17 @@ struct Context {
     int* d_fill = nullptr;                // used slots per chunk
     int* d_chunk_ao0 = nullptr;           // first AO of each chunk (a chunk is a contiguous AO range)
     int2* d_ao_slot = nullptr;            // (chunk, slot) of each AO
+    int* d_piece_chunk = nullptr;         // chunk of each piece (d_pieces order)
+    int npieces = 0;
     // Packed piece records of the fused kernel, in the order of d_pieces: per
-    // piece three float4 -- (x_hi, y_hi, z_hi, amin), (x_lo, y_lo, z_lo,
+    // piece three float4 -- (x_hi, y_hi, z_hi, FP32 screening exponent), (x_lo, y_lo, z_lo,
     // prim_off as bits), (l, nprim, contractions, first slot as int bits) --
     // and per piece, group of three contractions and primitive one float4
     // (alpha, c_j, c_j+1, c_j+2) at prim_off (FP32, zero-padded contractions).
     float4* d_piece_rec = nullptr;
     float4* d_piece_prim = nullptr;
-    // FP64 twins for the tiled evaluators: centre and smallest exponent as two
-    // double2 (x, y), (z, amin) per piece, and two double2 (alpha, c_j),
+    // FP64 twins for the tiled evaluators: centre and FP64 screening exponent
+    // as two double2 (x, y), (z, scr64) per piece, and two double2 (alpha, c_j),
     // (c_j+1, c_j+2) per entry of the primitive table (same entry index).
     double2* d_piece_c64 = nullptr;
     double2* d_piece_prim64 = nullptr;

@@ -23,6 +23,8 @@ struct ProjectArgs {
     const int4* pieces;        // (shell, first contraction, contractions, first slot in chunk)
     const int* lane_begin;     // pieces of lane j in chunk c: [lane_begin[c*PPT+j], lane_begin[c*PPT+j+1])
     const int* chunk_fill;     // slots of chunk c in use; the rest are zero
+    const int* piece_chunk;    // chunk of each piece
+    int npieces;
     const uint8_t* wimg;       // per chunk: nax x (hi, lo) BF16 tiles
     int comp_mask;
     int axis_comp[4];

@@ -50,6 +50,8 @@ constexpr int kChunk = 32;            // AO slots per K-chunk
 constexpr uint32_t kTileA = kRows * kChunk * 2;       // bytes of one BF16 A tile (8 KB)
 constexpr uint32_t kLboA = (kRows / 8) * 128;          // K-adjacent core matrices
 constexpr uint32_t kSboA = 128;                        // M-adjacent core matrices
+constexpr int kLiveWords = 8;          // chunk-liveness bits per tile (up to 256 chunks)
+constexpr float kBoxMargin = 1e-3f;    // bohr: covers FP32 rounding of points and centres
 
 // Writes the component values of one piece into the FP32 staging buffer
 // stage[comp][slot][point]; slot = ao + base.
@@ -151,6 +153,8 @@ project_tc_kernel(ProjectArgs args) {
     volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 8);
     volatile int* prod_abort = reinterpret_cast<volatile int*>(bars + 9);   // [2]
     __shared__ double red[kThreads / 32][4];
+    __shared__ uint32_t live_s[kLiveWords];   // chunks of the current tile that are not screened
+    __shared__ float tile_box[4][6];          // per point warp: coordinate minima, maxima
 
     const int tid = threadIdx.x;
     const int warp = tid / 32, lane = tid % 32;
@@ -199,6 +203,8 @@ project_tc_kernel(ProjectArgs args) {
         uint32_t q = 0;   // chunk sequence number of this CTA
         uint32_t t = 0;   // tile sequence number of this CTA
         bool stop = false;
+        bool a_zero = false;   // the A tiles hold zeros from a screened chunk
+        const bool use_live = args.piece_chunk != nullptr && nchunks <= 32 * kLiveWords;
         for (int64_t tile = blockIdx.x; tile < ntiles && !stop; tile += gridDim.x, ++t) {
             const int64_t g = tile * kRows + p;
             const bool valid = g < n;
@@ -213,6 +219,55 @@ project_tc_kernel(ProjectArgs args) {
                 pxl = static_cast<float>(px - pxh); pyl = static_cast<float>(py - pyh); pzl = static_cast<float>(pz - pzh);
                 count = args.sumsq && (args.weights == nullptr || args.weights[gi] != 0.0);
             }
+            // Chunks screened for the whole tile: a chunk every piece of which
+            // lies beyond its FP32 screening radius from the tile's bounding box
+            // is zero at every point of the tile (each warp's own test would drop
+            // every piece); it is neither evaluated nor converted, and its A
+            // tiles are written as zeros.
+            if (use_live) {
+                if (tid < kLiveWords) live_s[tid] = 0u;
+                if (tid < kRows) {   // warps 0-3 hold each of the tile's points once
+                    const float pc[3] = {pxh + pxl, pyh + pyl, pzh + pzl};
+                    float lo3[3], hi3[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        lo3[d] = valid ? pc[d] : INFINITY;
+                        hi3[d] = valid ? pc[d] : -INFINITY;
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) {
+                            lo3[d] = fminf(lo3[d], __shfl_xor_sync(0xffffffffu, lo3[d], o));
+                            hi3[d] = fmaxf(hi3[d], __shfl_xor_sync(0xffffffffu, hi3[d], o));
+                        }
+                    }
+                    if (lane == 0)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) { tile_box[warp][d] = lo3[d]; tile_box[warp][3 + d] = hi3[d]; }
+                }
+                named_bar_sync(1, kProducers);
+                float mid[3], half[3];
+                bool any = true;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    float lo = tile_box[0][d], hi = tile_box[0][3 + d];
+#pragma unroll
+                    for (int w = 1; w < 4; ++w) { lo = fminf(lo, tile_box[w][d]); hi = fmaxf(hi, tile_box[w][3 + d]); }
+                    any = any && lo <= hi;
+                    mid[d] = 0.5f * (lo + hi);
+                    half[d] = 0.5f * (hi - lo) + kBoxMargin;
+                }
+                if (any)
+                    for (int pi = tid; pi < args.npieces; pi += kProducers) {
+                        const float4 ch = __ldg(args.piece_rec + 3 * pi), cl = __ldg(args.piece_rec + 3 * pi + 1);
+                        const float ex = fmaxf(fabsf((ch.x + cl.x) - mid[0]) - half[0], 0.f);
+                        const float ey = fmaxf(fabsf((ch.y + cl.y) - mid[1]) - half[1], 0.f);
+                        const float ez = fmaxf(fabsf((ch.z + cl.z) - mid[2]) - half[2], 0.f);
+                        if (!(ch.w * (ex * ex + ey * ey + ez * ez) > static_cast<float>(kExpCut))) {
+                            const int pc = __ldg(args.piece_chunk + pi);
+                            atomicOr(&live_s[pc >> 5], 1u << (pc & 31));
+                        }
+                    }
+                named_bar_sync(1, kProducers);
+            }
             float psq[4] = {0.f, 0.f, 0.f, 0.f};
             // the chunk's piece range and fill are read one chunk ahead
             int pb_n = args.lane_begin[lanegrp], pe_n = args.lane_begin[lanegrp + 1], fill_n = args.chunk_fill[0];
@@ -224,12 +279,14 @@ project_tc_kernel(ProjectArgs args) {
                     pe_n = __ldg(args.lane_begin + (c + 1) * PPT + lanegrp + 1);
                     fill_n = __ldg(args.chunk_fill + c + 1);
                 }
+                const bool live = !use_live || ((live_s[c >> 5] >> (c & 31)) & 1u);
                 // 1. evaluate this chunk's pieces into the FP32 staging buffer
-                for (int k = (valid ? fill : 0) + lanegrp; k < kChunk; k += PPT)
+                if (live)
+                    for (int k = (valid ? fill : 0) + lanegrp; k < kChunk; k += PPT)
 #pragma unroll
-                    for (int cc = 0; cc < kNComp; ++cc) sStage[(cc * kChunk + k) * kRows + p] = 0.f;
+                        for (int cc = 0; cc < kNComp; ++cc) sStage[(cc * kChunk + k) * kRows + p] = 0.f;
                 float csq[4] = {0.f, 0.f, 0.f, 0.f};
-                if (valid) {
+                if (valid && live) {
                     for (int pi = pb; pi < pe; ++pi) {
                         // one packed record per piece: centre (hi, lo), smallest exponent,
                         // primitive offset, l, primitive and contraction counts, first slot
@@ -271,8 +328,21 @@ project_tc_kernel(ProjectArgs args) {
                 if (prod_abort[q & 1]) { stop = true; break; }
                 // 2. wait until the previous chunk's MMAs (and tile store) released A
                 if (q > 0 && !tc::mbar_wait(a_empty, (q - 1) & 1)) fail_wait(0);
-                // 3. convert staging -> BF16 hi/lo A tiles (UMMA interleaved K-major)
-                for (int u = tid; u < kRows * NAX * (kChunk / 8); u += kProducers) {
+                // 3. convert staging -> BF16 hi/lo A tiles (UMMA interleaved K-major);
+                // a screened chunk leaves zeros (A and, when kept, its remainder tile)
+                if (!live) {
+                    if (!a_zero)
+                        for (uint32_t u = tid; u < NAX * 2 * kTileA / 16; u += kProducers)
+                            *reinterpret_cast<uint4*>(sA + 16 * u) = make_uint4(0u, 0u, 0u, 0u);
+                    a_zero = true;
+                    if (args.a_store_r)
+                        for (uint32_t u = tid; u < kTileA / 16; u += kProducers)
+                            *reinterpret_cast<uint4*>(args.a_store_r + (static_cast<size_t>(tile) * nchunks + c) * kTileA +
+                                                      16 * u) = make_uint4(0u, 0u, 0u, 0u);
+                } else {
+                    a_zero = false;
+                }
+                for (int u = tid; live && u < kRows * NAX * (kChunk / 8); u += kProducers) {
                     const int row = u % kRows;
                     const int rest = u / kRows;
                     const int kg = rest % (kChunk / 8);
@@ -333,6 +403,13 @@ project_tc_kernel(ProjectArgs args) {
         if (lane == 0) {
             constexpr uint32_t idesc = tc::idesc_bf16_f32(kRows, NT);
             constexpr uint32_t kLboB = (NT / 8) * 128;
+            // The operand descriptors are affine in the tile offsets: a base
+            // descriptor plus (byte offset >> 4) in its start-address field
+            // (bits 0-13; shared addresses stay below 2^18, so nothing carries
+            // out of the field).
+            const uint64_t dA0 = tc::smem_desc_kmajor_noswizzle(tc::smem_addr(sA), kLboA, kSboA);
+            const uint64_t dB00 = tc::smem_desc_kmajor_noswizzle(tc::smem_addr(sB), kLboB, 128);
+            const uint64_t dB01 = tc::smem_desc_kmajor_noswizzle(tc::smem_addr(sB + (kBStages - 1) * kBStage), kLboB, 128);
             uint32_t q = 0;
             bool ok = true;
             for (int64_t tile = blockIdx.x; tile < ntiles && ok && !*abort_flag; tile += gridDim.x) {
@@ -341,19 +418,18 @@ project_tc_kernel(ProjectArgs args) {
                     if (!tc::mbar_wait(&b_full[s], (q / kBStages) & 1)) { fail_wait(2); ok = false; break; }
                     if (!tc::mbar_wait(a_full, q & 1)) { fail_wait(3); ok = false; break; }
                     tc::tc_fence_after();
+                    const uint64_t dB0 = s == 0 ? dB00 : dB01;
+                    const uint32_t acc0 = c == 0 ? 0u : 1u;
+#pragma unroll
                     for (int a = 0; a < NAX; ++a) {
                         const uint32_t d = tmem_base + static_cast<uint32_t>(a * NT);
-                        const uint32_t a_hi = tc::smem_addr(sA + (a * 2 + 0) * kTileA);
-                        const uint32_t a_lo = tc::smem_addr(sA + (a * 2 + 1) * kTileA);
-                        const uint32_t b_hi = tc::smem_addr(sB + s * kBStage + (a * 2 + 0) * kTileB);
-                        const uint32_t b_lo = tc::smem_addr(sB + s * kBStage + (a * 2 + 1) * kTileB);
+#pragma unroll
                         for (int kk = 0; kk < kChunk / 16; ++kk) {
-                            const uint64_t dah = tc::smem_desc_kmajor_noswizzle(a_hi + kk * 2 * kLboA, kLboA, kSboA);
-                            const uint64_t dal = tc::smem_desc_kmajor_noswizzle(a_lo + kk * 2 * kLboA, kLboA, kSboA);
-                            const uint64_t dbh = tc::smem_desc_kmajor_noswizzle(b_hi + kk * 2 * kLboB, kLboB, 128);
-                            const uint64_t dbl = tc::smem_desc_kmajor_noswizzle(b_lo + kk * 2 * kLboB, kLboB, 128);
-                            const uint32_t first = (c == 0 && kk == 0) ? 0u : 1u;
-                            tc::mma_bf16(d, dah, dbh, idesc, first);
+                            const uint64_t dah = dA0 + (((a * 2 + 0) * kTileA + kk * 2 * kLboA) >> 4);
+                            const uint64_t dal = dA0 + (((a * 2 + 1) * kTileA + kk * 2 * kLboA) >> 4);
+                            const uint64_t dbh = dB0 + (((a * 2 + 0) * kTileB + kk * 2 * kLboB) >> 4);
+                            const uint64_t dbl = dB0 + (((a * 2 + 1) * kTileB + kk * 2 * kLboB) >> 4);
+                            tc::mma_bf16(d, dah, dbh, idesc, kk == 0 ? acc0 : 1u);
                             tc::mma_bf16(d, dah, dbl, idesc, 1u);
                             tc::mma_bf16(d, dal, dbh, idesc, 1u);
                         }
@@ -493,6 +569,10 @@ void build_chunk_layout(Context& c) {
         }
     }
     lane_begin.push_back(static_cast<int>(pieces.size()));
+    std::vector<int> piece_chunk(std::max<size_t>(pieces.size(), 1), 0);
+    for (size_t ch = 0; ch < chunks.size(); ++ch)
+        for (int i = lane_begin[ch * lanes]; i < lane_begin[(ch + 1) * lanes]; ++i) piece_chunk[i] = static_cast<int>(ch);
+    c.npieces = static_cast<int>(pieces.size());
     if (pieces.empty()) pieces.push_back(make_int4(0, 0, 0, 0));
     c.nchunks = static_cast<int>(fill.size());
     c.piece_lanes = lanes;
@@ -510,6 +590,7 @@ void build_chunk_layout(Context& c) {
     for (size_t i = 1; i < fill.size(); ++i) ao0[i] = ao0[i - 1] + fill[i - 1];
     up(c.d_chunk_ao0, ao0);
     up(c.d_ao_slot, ao_slot);
+    up(c.d_piece_chunk, piece_chunk);
 }
 
 void upload_piece_records(Context& c) {
@@ -647,6 +728,8 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     a.nchunks = pl.nchunks;
     a.pieces = c.d_pieces;
     a.lane_begin = c.d_piece_begin;
+    a.piece_chunk = c.d_piece_chunk;
+    a.npieces = c.npieces;
     require(c.piece_lanes == piece_lanes_for_lmax(pl.lmax), "chunk layout built for other producer lanes");
     a.chunk_fill = c.d_fill;
     a.wimg = reinterpret_cast<const uint8_t*>(pl.wimg.get());
