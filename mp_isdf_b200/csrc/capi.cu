@@ -422,7 +422,7 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
     if (!have && precision == ISDF_MIXED && isdf::fit_mixed_supported(k)) {
         o = isdf::fit_grid_mixed(c, xyz, w, kp, f, theta, kp.n, s, reuse ? ra->tiles : nullptr,
                                  reuse ? ra->tiles_r : nullptr,
-                                 reuse ? ra->psq.get() : nullptr, on_chunk);
+                                 reuse ? ra->psq.get() : nullptr, on_chunk, reuse ? ra->chunk_zero : nullptr);
         if (!(o.mixed_bound <= isdf::kMixedFitTolerance)) {
             // a fit whose pair error is very small cannot absorb the stored
             // tiles' representation error: recompute Theta with FP64 AO values

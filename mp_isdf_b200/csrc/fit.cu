@@ -720,7 +720,7 @@ void refine_theta(int kmax, const uint8_t* tiles, const uint8_t* tiles_r, int nc
 FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
                          const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s,
                          const uint8_t* ao_tiles, const uint8_t* ao_tiles_r, const float* ao_psq,
-                         const FitChunkHook* on_chunk) {
+                         const FitChunkHook* on_chunk, const uint8_t* ao_chunk_zero) {
     FitOutput out;
     const int64_t n = kp.n, k = f.k, nao = c.nao;
     out.theta_w.assign(k, 0.0);
@@ -771,7 +771,8 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
         const int64_t m = std::min(per, n - g0);
         if (ao_tiles)
             // AO values of these points already sit in HBM as split-BF16 tiles
-            gram_from_tiles(c, plan, ao_tiles + stored_tile_bytes(c, g0), m, G.get() + g0 * k, k, err.get(), s);
+            gram_from_tiles(c, plan, ao_tiles + stored_tile_bytes(c, g0), m, G.get() + g0 * k, k, err.get(), s,
+                            ao_chunk_zero ? ao_chunk_zero + (g0 / 128) * c.nchunks : nullptr);
         {
             ISDF_PROFILE("fit_mixed", s);
             kern<<<blocks_for(m), 256, smem, s>>>(G.get() + g0 * k, point_sq + g0 * 4, m, static_cast<int>(k),

@@ -36,7 +36,15 @@ struct GramArgs {
     int64_t ld_out;
     int nout;
     int* error;
+    const uint8_t* chunk_zero;   // null, or [tile][chunk] nonzero where the tiles are zeros
 };
+
+// A chunk whose stored tiles are zeros is skipped by the loader and the MMA
+// thread alike, except the last chunk of a tile none of whose chunks was
+// taken (its zero tiles initialise the accumulator).
+__device__ __forceinline__ bool skip_chunk(const GramArgs& a, int64_t tile, int c, bool taken) {
+    return a.chunk_zero && a.chunk_zero[tile * a.nchunks + c] && (taken || c + 1 < a.nchunks);
+}
 
 template <int NT>
 __global__ void __launch_bounds__(kThreads, 1) gram_tiles_kernel(GramArgs args) {
@@ -82,9 +90,13 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tiles_kernel(GramArgs args) 
         if (lane == 0) {
             uint32_t q = 0;
             for (int64_t tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x) {
-                for (int c = 0; c < nchunks; ++c, ++q) {
+                bool taken = false;
+                for (int c = 0; c < nchunks; ++c) {
+                    if (skip_chunk(args, tile, c, taken)) continue;
+                    taken = true;
                     const uint32_t s = q % kStages;
-                    if (q >= kStages && !tc::mbar_wait(&empty[s], ((q / kStages) - 1) & 1)) {
+                    ++q;
+                    if (q > kStages && !tc::mbar_wait(&empty[s], ((q - 1) / kStages - 1) & 1)) {
                         fail_wait(8);
                         break;
                     }
@@ -115,9 +127,15 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tiles_kernel(GramArgs args) 
                 tc::tc_fence_after();
                 const uint32_t d = tmem_base + ab * NT;
                 bool ok = true;
-                for (int c = 0; c < nchunks; ++c, ++q) {
+                bool taken = false;
+                for (int c = 0; c < nchunks; ++c) {
+                    if (skip_chunk(args, tile, c, taken)) continue;
+                    const bool first = !taken;
+                    taken = true;
                     const uint32_t s = q % kStages;
-                    if (!tc::mbar_wait(&full[s], (q / kStages) & 1)) {
+                    const uint32_t ph = (q / kStages) & 1;
+                    ++q;
+                    if (!tc::mbar_wait(&full[s], ph)) {
                         fail_wait(10);
                         ok = false;
                         break;
@@ -131,7 +149,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tiles_kernel(GramArgs args) 
                             const uint32_t bb = tc::smem_addr(st + 2 * kTileA + pb[pr] * kTileB) + kk * 2 * kLboB;
                             tc::mma_bf16(d, tc::smem_desc_kmajor_noswizzle(aa, kLboA, kSboA),
                                          tc::smem_desc_kmajor_noswizzle(bb, kLboB, 128), idesc,
-                                         (c == 0 && kk == 0 && pr == 0) ? 0u : 1u);
+                                         (first && kk == 0 && pr == 0) ? 0u : 1u);
                         }
                     }
                     tc::mma_commit(&empty[s]);
@@ -191,12 +209,12 @@ void launch_gram(const GramArgs& a, int nsm, cudaStream_t s) {
 }  // namespace
 
 void gram_from_tiles(const Context& c, const ProjectPlan& pl, const uint8_t* a_tiles, int64_t n, float* out,
-                     int64_t ld_out, int* error, cudaStream_t s) {
+                     int64_t ld_out, int* error, cudaStream_t s, const uint8_t* chunk_zero) {
     if (n == 0) return;
     require(pl.nax == 1 && !pl.grad, "stored-tile GEMM takes a one-axis value plan");
     require(pl.nchunks == c.nchunks, "weight image and stored tiles disagree on the K-chunks");
     GramArgs a{a_tiles, reinterpret_cast<const uint8_t*>(pl.wimg.get()), n, pl.nchunks, out, ld_out,
-               pl.nout, error};
+               pl.nout, error, chunk_zero};
     int dev = 0, nsm = 148;
     ISDF_CUDA(cudaGetDevice(&dev));
     ISDF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));

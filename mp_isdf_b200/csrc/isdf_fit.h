@@ -60,7 +60,8 @@ using FitChunkHook = std::function<void(int64_t g0, int64_t m)>;
 FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
                          const AnchorFactor& f, double* theta, int64_t ldt, cudaStream_t s,
                          const uint8_t* ao_tiles = nullptr, const uint8_t* ao_tiles_r = nullptr,
-                         const float* ao_psq = nullptr, const FitChunkHook* on_chunk = nullptr);
+                         const float* ao_psq = nullptr, const FitChunkHook* on_chunk = nullptr,
+                         const uint8_t* ao_chunk_zero = nullptr);
 
 void gather_points(const double* pts, const double* w, const int64_t* idx, int64_t n,
                    int64_t npts_total, double* out_pts, double* out_w, cudaStream_t s);

@@ -35,6 +35,7 @@ struct ProjectArgs {
     int* error;                // bit flags of bounded waits that gave up
     uint8_t* a_store;          // null, or [tile][chunk] (hi, lo) A tiles of axis entry store_axis
     uint8_t* a_store_r;        // null, or [tile][chunk] BF16 remainder tiles x - hi - lo of that entry
+    uint8_t* chunk_zero;       // null, or [tile][chunk]: 1 where the chunk was screened for the tile
     int store_axis;
 };
 
@@ -61,12 +62,16 @@ void project_tc(const Context& c, const ProjectPlan& plan, const double* pts, co
                 int64_t n, const double* weights, float* out, int64_t ld_out, int64_t col_stride,
                 double* sumsq,
                 float* point_sq, int* error, cudaStream_t s, uint8_t* a_store = nullptr,
-                int store_axis = 0, uint8_t* a_store_r = nullptr);
+                int store_axis = 0, uint8_t* a_store_r = nullptr, uint8_t* chunk_zero = nullptr);
 
 // G[g*ld_out + j] from A tiles stored by project_tc (a_store) over n points and
 // a one-axis value plan: the same split-BF16 products as project_tc.
+// chunk_zero (optional): one byte per stored (tile, K-chunk), nonzero where the
+// fused projection screened the chunk for the whole tile (its tiles are zeros
+// and the GEMM skips them).
 void gram_from_tiles(const Context& c, const ProjectPlan& pl, const uint8_t* a_tiles, int64_t n,
-                     float* out, int64_t ld_out, int* error, cudaStream_t s);
+                     float* out, int64_t ld_out, int* error, cudaStream_t s,
+                     const uint8_t* chunk_zero = nullptr);
 
 // Bytes of the stored A tiles of one axis entry over n points.
 inline size_t stored_tile_bytes(const Context& c, int64_t n) {
@@ -77,5 +82,9 @@ inline size_t stored_tile_bytes(const Context& c, int64_t n) {
 // r = x - hi - lo of each FP32 value x, so that hi + lo + r == x exactly (one
 // 8 KB tile per 128 points and K-chunk, same layout as the A tiles).
 inline size_t stored_remainder_bytes(const Context& c, int64_t n) { return stored_tile_bytes(c, n) / 2; }
+// Bytes of the per-(tile, K-chunk) screening flags over n points (256-byte multiple).
+inline size_t stored_flag_bytes(const Context& c, int64_t n) {
+    return ((static_cast<size_t>((n + 127) / 128) * c.nchunks + 255) / 256) * 256;
+}
 
 }  // namespace isdf

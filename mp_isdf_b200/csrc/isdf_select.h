@@ -171,6 +171,7 @@ struct RetainedAo {
     KeptPoints kp;
     const uint8_t* tiles = nullptr;  // [tile][K-chunk] (hi, lo) A tiles of the AO values
     const uint8_t* tiles_r = nullptr;  // [tile][K-chunk] remainder tiles (hi + lo + r = FP32 value)
+    const uint8_t* chunk_zero = nullptr;  // [tile][K-chunk] 1 where the chunk's tiles are zeros (screened)
     DeviceBuffer<float> psq;       // [n][4] per-point sums of squares (component 0 = values)
     bool valid = false;
 };

@@ -280,6 +280,8 @@ project_tc_kernel(ProjectArgs args) {
                     fill_n = __ldg(args.chunk_fill + c + 1);
                 }
                 const bool live = !use_live || ((live_s[c >> 5] >> (c & 31)) & 1u);
+                if (args.chunk_zero && tid == 0)
+                    args.chunk_zero[static_cast<size_t>(tile) * nchunks + c] = live ? 0 : 1;
                 // 1. evaluate this chunk's pieces into the FP32 staging buffer
                 if (live)
                     for (int k = (valid ? fill : 0) + lanegrp; k < kChunk; k += PPT)
@@ -709,7 +711,7 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
                 int64_t n, const double* weights, float* out, int64_t ld_out, int64_t col_stride,
                 double* sumsq,
                 float* point_sq, int* error, cudaStream_t s, uint8_t* a_store, int store_axis,
-                uint8_t* a_store_r) {
+                uint8_t* a_store_r, uint8_t* chunk_zero) {
     if (n == 0) return;
     ProjectArgs a{};
     a.shells = c.d_shells;
@@ -740,6 +742,7 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     a.col_stride = col_stride;
     a.a_store = a_store;
     a.a_store_r = a_store_r;
+    a.chunk_zero = chunk_zero;
     a.store_axis = store_axis;
     require(a_store == nullptr || (store_axis >= 0 && store_axis < pl.nax), "invalid stored axis entry");
     a.nout = pl.nout;

@@ -842,9 +842,13 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     const size_t p_bytes = (static_cast<size_t>(n) * naxes * nout * sizeof(float) + 255) / 256 * 256;
     uint8_t* tiles = nullptr;
     uint8_t* tiles_r = nullptr;
+    uint8_t* chunk_zero = nullptr;
     if (keep) {
-        // tiles (when they fit in free memory) and projections in the workspace
-        size_t tile_bytes = store_axis >= 0 ? stored_tile_bytes(c, n) + stored_remainder_bytes(c, n) : 0;
+        // tiles (when they fit in free memory), their screening flags and the
+        // projections in the workspace
+        size_t tile_bytes = store_axis >= 0 ? stored_tile_bytes(c, n) + stored_remainder_bytes(c, n) +
+                                                  stored_flag_bytes(c, n)
+                                            : 0;
         if (tile_bytes + p_bytes > c.ws_bytes && tile_bytes > 0) {
             size_t free_b = 0, total_b = 0;
             ISDF_CUDA(cudaMemGetInfo(&free_b, &total_b));
@@ -857,6 +861,7 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
         if (store_axis >= 0) {
             tiles = base;
             tiles_r = base + stored_tile_bytes(c, n);
+            chunk_zero = tiles_r + stored_remainder_bytes(c, n);
         }
         P = reinterpret_cast<float*>(base + tile_bytes);
     } else {
@@ -865,7 +870,7 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     }
     // column-major projections P[a*nout + j][g] (coalesced for the combine pass)
     project_tc(c, plan, pts, kp.index.get(), n, w, P, 1, n, sumsq.get(), psq.get(),
-               err.get(), s, tiles, std::max(store_axis, 0), tiles_r);
+               err.get(), s, tiles, std::max(store_axis, 0), tiles_r, chunk_zero);
     // host work under the kernel: the factors' absolute column sums for the
     // screening term of the error bounds
     const std::vector<double> au = factor_abs_sums(u, naxes, nao, ell), av = factor_abs_sums(v, naxes, nao, ell);
@@ -908,6 +913,7 @@ MixedSketch sketch_mixed(const Context& c, const double* pts, const KeptPoints& 
     if (keep && store_axis >= 0) {
         keep->tiles = tiles;
         keep->tiles_r = tiles_r;
+        keep->chunk_zero = chunk_zero;
         keep->psq = std::move(psq);
         keep->valid = true;
     }
