@@ -188,7 +188,10 @@ int isdf_fit_host(isdf_ctx* ctx, const double* xyz_host, const double* w_host, i
  * args->precision; in the mixed rand_sketch form the split-BF16 AO value
  * tiles of the sketch pass stay in HBM and the fit contracts them instead of
  * evaluating the AOs again (the reference likewise evaluates Phi once and
- * hands it to the fit).  theta_dev needs capacity k * ng (k <= capacity). */
+ * hands it to the fit).  A mixed request whose selection kept no AO tiles
+ * (pair-QR algorithms, no plain AO value axis) fits in FP64 below 2^28 AO
+ * values (ng * nao), where that is the cheaper fit (fit_info->fit_path 0).
+ * theta_dev needs capacity k * ng (k <= capacity). */
 int isdf_select_fit(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz_dev,
                     const double* w_dev, int64_t ng, int64_t* pivots_host, int64_t capacity,
                     int64_t* npivots, isdf_select_info* select_info, int32_t want_error,

@@ -377,6 +377,17 @@ struct AnchorCoords {
     const double* w = nullptr;     // k
 };
 
+// Fit form of the fused selection + fit.  A mixed request whose selection left
+// no AO tiles (the FP64 selections, or no plain value axis) would have to run
+// its own fused AO pass plus the bound's host round trips; below 2^28 AO values
+// that costs more than the FP64 fit (about 0.5 ms at C1 and C4), so those fits
+// run in FP64 (fit_path 0).
+int32_t fused_fit_precision(isdf_ctx* ctx, int32_t precision, const isdf::RetainedAo& keep, int64_t ng) {
+    if (precision != ISDF_MIXED || keep.valid) return precision;
+    const double values = static_cast<double>(ng) * ctx_of(ctx).nao;
+    return values < 268435456.0 ? ISDF_FP64 : precision;
+}
+
 void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, const int64_t* anchors,
               int64_t k, int32_t precision, const double* theta_in, double* theta_out,
               isdf_fit_info* info, double* l2, double* rel, cudaStream_t s, bool want_error = true,
@@ -508,8 +519,9 @@ int isdf_select_fit(isdf_ctx* ctx, const isdf_select_args* args, const double* x
             isdf::fail(isdf::kInvalid, "pivot buffer is too small");
         if (!out.empty()) std::memcpy(pivots, out.data(), out.size() * sizeof(int64_t));
         if (npivots) *npivots = static_cast<int64_t>(out.size());
-        fit_impl(ctx, xyz, w, ng, out.data(), static_cast<int64_t>(out.size()), args->precision, nullptr,
-                 theta, fit_info, nullptr, nullptr, s, want_error != 0, &keep);
+        fit_impl(ctx, xyz, w, ng, out.data(), static_cast<int64_t>(out.size()),
+                 fused_fit_precision(ctx, args->precision, keep, ng), nullptr, theta, fit_info, nullptr, nullptr,
+                 s, want_error != 0, &keep);
     });
 }
 
@@ -589,7 +601,8 @@ int isdf_select_fit_host(isdf_ctx* ctx, const isdf_select_args* args, const doub
                                         m * sizeof(double), np, cudaMemcpyDeviceToHost, cp.stream));
         };
         const bool stream_out = theta_host && np > 0 && keep.valid;
-        fit_impl(ctx, dx.get(), dw.get(), ng, out.data(), np, args->precision, nullptr, dt.get(), &local,
+        fit_impl(ctx, dx.get(), dw.get(), ng, out.data(), np, fused_fit_precision(ctx, args->precision, keep, ng),
+                 nullptr, dt.get(), &local,
                  nullptr, nullptr, s, want_error != 0, &keep, nullptr, nullptr, stream_out ? &hook : nullptr);
         const bool copied = cp.used() && local.fit_path == 1;
         cp.finish();

@@ -136,7 +136,9 @@ def test_select_fit_matches_select_then_fit(small_water, axes):
     contracts the AO value tiles the sketch left in HBM) against isdf_select
     followed by isdf_fit on the same device points: identical anchors, the
     same fit path, Theta and the error bound to FP32-evaluation level, and the
-    pair-space error within 1e-8 relative of the FP64 fit's."""
+    pair-space error within 1e-8 relative of the FP64 fit's.  Without a plain
+    AO value axis the sketch keeps no AO tiles, and below 2^28 AO values the
+    fused call then fits in FP64 (fit path 0), as isdf_fit in FP64 does."""
     import torch
     from mp_isdf_b200 import capi
     mol, pts, w = small_water
@@ -147,7 +149,8 @@ def test_select_fit_matches_select_then_fit(small_water, axes):
     for precision in ("mixed", "fp64"):
         piv, _ = ctx.select(x, wt, precision=precision, **kw)
         theta = torch.zeros(len(piv) * len(pts), dtype=torch.float64, device="cuda")
-        info = ctx.fit(x, wt, piv, theta, precision=precision, want_error=True)
+        fit_precision = "fp64" if "ao" not in axes else precision
+        info = ctx.fit(x, wt, piv, theta, precision=fit_precision, want_error=True)
         theta2 = torch.zeros(8 * len(pts), dtype=torch.float64, device="cuda")
         piv2, sinfo, info2 = ctx.select_fit(x, wt, theta2, want_error=True, precision=precision, **kw)
         torch.cuda.synchronize()
@@ -162,7 +165,7 @@ def test_select_fit_matches_select_then_fit(small_water, axes):
         # cond(C)^2 in the solve; mixed fits also by FP32 AO rounding
         scale = max(1.0, info.condition) ** 2
         assert rel <= (1e-12 * scale if info.fit_path in (0, 2) else 1e-5 * scale), rel
-        if precision == "mixed":
+        if fit_precision == "mixed":
             assert abs(info2.mixed_bound - info.mixed_bound) <= 1e-3 * info.mixed_bound
         assert abs(info2.pair_relative - info.pair_relative) <= 1e-8 * info.pair_relative
 
