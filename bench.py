@@ -152,17 +152,18 @@ def peaks():
 
 # DRAM bytes per kept grid point of one launch, from an ncu capture of the
 # (H2O)64 case cut to 397312 grid points / 363237 kept points
-# (dram__bytes_read.sum + dram__bytes_write.sum = 54.9 MB + 3735.2 MB); the
+# (dram__bytes_read.sum + dram__bytes_write.sum = 28.1 MB + 3737.3 MB); the
 # kernel streams per-point data, so the traffic scales with the points.
-MEASURED_TRAFFIC_PER_POINT = {"project_tc_grad": 10434.0}
+MEASURED_TRAFFIC_PER_POINT = {"project_tc_grad": 10366.0}
 TRAFFIC_SOURCE = "ncu dram bytes of a 363237-kept-point capture, scaled by kept points"
 
-# ncu figures of the adjoint's fused grid kernel (one launch, --set full)
+# ncu figures of the adjoint's fused grid kernel (one launch, --set full) on
+# the (H2O)64 basis with the C5 anchors, grid cut to 60000 points
 ADJOINT_PROFILE = {
-    "kernel": "adjoint_grid_kernel<2, 8, 1>",
-    "workload": "(H2O)8, 192 AOs, 46608 kept points, 8 anchors",
-    "issue_active_frac": 0.302, "fp64_pipe_frac": 0.173, "warps_active_frac": 0.125,
-    "registers_per_thread": 255, "summary": "profiles/adjoint_grid_kernel_c4_fp64.md",
+    "kernel": "adjoint_grid_kernel<2, 12, 1>",
+    "workload": "(H2O)64, 1536 AOs, 10 anchors, 60000 grid points",
+    "issue_active_frac": 0.251, "fp64_pipe_frac": 0.132, "warps_active_frac": 0.125,
+    "registers_per_thread": 255, "summary": "profiles/adjoint_grid_kernel_c5_fp64.md",
 }
 
 
