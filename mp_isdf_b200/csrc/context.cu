@@ -290,9 +290,20 @@ __device__ __forceinline__ const typename PackedPrim<T>::rec* packed_prims(const
     return static_cast<const typename PackedPrim<T>::rec*>(p) + (sizeof(T) == 8 ? 2 : 1) * prim_off;
 }
 
+// Shared tiles per block: two for the value-only tiles (chunk c evaluated into
+// one while other warps still store chunk c - 1 from the other, one barrier
+// per chunk; FP64 values 12.5 -> 12.2 ms at C5), else one (two barriers per
+// chunk: doubling the 33 KB FP32 gradient tile left less L1 and was slower).
+template <class T, bool GRAD>
+constexpr int tile_bufs() {
+    return 2 * (GRAD ? 4 : 1) * 32 * kTileStride * sizeof(T) <= 40 * 1024 ? 2 : 1;
+}
+template <class T, bool GRAD>
+constexpr size_t tile_elems() { return static_cast<size_t>(GRAD ? 4 : 1) * 32 * kTileStride; }
+
 template <class T, bool GRAD>
 constexpr size_t tile_smem_bytes() {
-    return (GRAD ? 4 : 1) * 32 * kTileStride * sizeof(T) + (GRAD ? 4 : 1) * kTilePts * sizeof(T*);
+    return tile_bufs<T, GRAD>() * tile_elems<T, GRAD>() * sizeof(T) + (GRAD ? 4 : 1) * kTilePts * sizeof(T*);
 }
 
 template <class T, bool GRAD, int LMAX, int PPT>
@@ -301,7 +312,7 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) ao_tile_kernel(TileA
     constexpr int kWarps = kTilePts / 32 * PPT;
     extern __shared__ __align__(16) uint8_t tile_raw[];
     T** rowp = reinterpret_cast<T**>(tile_raw);                       // [kNComp][kTilePts]
-    T* st = reinterpret_cast<T*>(tile_raw + kNComp * kTilePts * sizeof(T*));
+    T* const st0 = reinterpret_cast<T*>(tile_raw + kNComp * kTilePts * sizeof(T*));
     const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
     const int lanegrp = warp % PPT, p = (warp / PPT) * 32 + lane;
     const int64_t b0 = static_cast<int64_t>(blockIdx.x) * kTilePts;
@@ -325,6 +336,7 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) ao_tile_kernel(TileA
     // the margin covers the exponent's rounding to FP32
     const double cut = kExpCut * 1.0001;
     for (int c = 0; c < a.nchunks; ++c) {
+        T* const st = st0 + (tile_bufs<T, GRAD>() == 2 ? (c & 1) * tile_elems<T, GRAD>() : 0);
         const int pb = a.lane_begin[c * PPT + lanegrp], pe = a.lane_begin[c * PPT + lanegrp + 1];
         for (int pi = pb; pi < pe; ++pi) {
             // packed record: (l, primitives, contractions, first slot), centre and
@@ -353,7 +365,7 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) ao_tile_kernel(TileA
             if (row != nullptr && lane < fill)
                 row[ao0 + lane] = st[((r / kTilePts) * 32 + lane) * kTileStride + r % kTilePts];
         }
-        __syncthreads();
+        if constexpr (tile_bufs<T, GRAD>() == 1) __syncthreads();   // the tile is refilled next
     }
 }
 
@@ -402,7 +414,7 @@ struct AxisTileArgs {
 
 template <class T, bool GRAD>
 constexpr size_t axis_tile_smem_bytes() {
-    return (GRAD ? 4 : 1) * 32 * kTileStride * sizeof(T) + kTilePts * sizeof(T*);
+    return tile_bufs<T, GRAD>() * tile_elems<T, GRAD>() * sizeof(T) + kTilePts * sizeof(T*);
 }
 
 template <class T, bool GRAD, int LMAX, int PPT>
@@ -411,7 +423,7 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) axis_tile_kernel(Axi
     constexpr int kWarps = kTilePts / 32 * PPT;
     extern __shared__ __align__(16) uint8_t tile_raw[];
     T** rowp = reinterpret_cast<T**>(tile_raw);                       // [kTilePts]
-    T* st = reinterpret_cast<T*>(tile_raw + kTilePts * sizeof(T*));
+    T* const st0 = reinterpret_cast<T*>(tile_raw + kTilePts * sizeof(T*));
     __shared__ double red[kWarps][4];
     const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
     const int lanegrp = warp % PPT, p = (warp / PPT) * 32 + lane;
@@ -429,6 +441,7 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) axis_tile_kernel(Axi
     double sq[4] = {0.0, 0.0, 0.0, 0.0};
     const double cut = kExpCut * 1.0001;
     for (int c = 0; c < a.nchunks; ++c) {
+        T* const st = st0 + (tile_bufs<T, GRAD>() == 2 ? (c & 1) * tile_elems<T, GRAD>() : 0);
         const int pb = a.lane_begin[c * PPT + lanegrp], pe = a.lane_begin[c * PPT + lanegrp + 1];
         for (int pi = pb; pi < pe; ++pi) {
             const int4 meta = __ldg(reinterpret_cast<const int4*>(a.piece_rec) + 3 * pi + 2);
@@ -459,7 +472,7 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) axis_tile_kernel(Axi
                 row[a.off[e] + ao0 + lane] =
                     static_cast<T>(a.scale[e] * static_cast<double>(st[(a.comp[e] * 32 + lane) * kTileStride + pp]));
         }
-        __syncthreads();
+        if constexpr (tile_bufs<T, GRAD>() == 1) __syncthreads();   // the tile is refilled next
     }
     if (a.sumsq) {
 #pragma unroll
