@@ -84,18 +84,66 @@ argmax_final_kernel(const ArgKey* __restrict__ partial, int nblocks, ArgKey* __r
 
 // L[g, j] = (sw_p sw_g D_g^2 - sum_{i<j} R_ij L_gi) / R_jj ; est_g -= L_gj^2
 __global__ void update_residual_kernel(const double* __restrict__ D, const double* __restrict__ sw,
-                                       double swp, int64_t n, double* __restrict__ L,
+                                       int64_t p, int64_t n, double* __restrict__ L,
                                        int64_t ldl, int j, const double* __restrict__ Rcol,
                                        double rjj, double* __restrict__ est,
                                        const char* __restrict__ selected) {
     const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (g >= n) return;
-    double v = swp * sw[g] * D[g] * D[g];
+    double v = sw[p] * sw[g] * D[g] * D[g];
     const double* lg = L + g * ldl;
     for (int i = 0; i < j; ++i) v -= Rcol[i] * lg[i];
     v /= rjj;
     L[g * ldl + j] = v;
     if (!selected[g]) est[g] = fmax(est[g] - v * v, 0.0);
+}
+
+// a[i*d + k] = sw[p] f[i] f[k]: the weighted pair vector of column p
+__global__ void pair_vector_sw_kernel(const double* __restrict__ f, int64_t d, const double* __restrict__ sw,
+                                      int64_t p, double* __restrict__ a) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= d * d) return;
+    a[i] = sw[p] * f[i / d] * f[i % d];
+}
+
+// est[p] = the exact squared residual just computed
+__global__ void set_est_kernel(double* __restrict__ est, int64_t p, const double* __restrict__ scal) {
+    est[p] = scal[0];
+}
+
+// column j of R: the two CGS passes' coefficients and R_jj = |r|
+__global__ void rcol_kernel(const double* __restrict__ t0, const double* __restrict__ t1, int j,
+                            const double* __restrict__ scal, double* __restrict__ Rcol) {
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) Rcol[i] = i < j ? t0[i] + t1[i] : sqrt(scal[0]);
+}
+
+// per-block sums of K_gg and a non-finite flag (fixed order: deterministic)
+__global__ void __launch_bounds__(256) kdiag_partial_kernel(const double* __restrict__ kd, int64_t n,
+                                                            double* __restrict__ part, int* __restrict__ bad) {
+    __shared__ double sh[256 / 32];
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * 256 + threadIdx.x;
+    double v = 0.0;
+    if (g < n) {
+        v = kd[g];
+        if (!isfinite(v)) atomicOr(bad, 1);
+    }
+    v = block_sum<256>(v, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+__global__ void __launch_bounds__(256) sum_partials_kernel(const double* __restrict__ part, int nb,
+                                                           double* __restrict__ out) {
+    __shared__ double sh[256 / 32];
+    double v = 0.0;
+    for (int b = threadIdx.x; b < nb; b += 256) v += part[b];
+    v = block_sum<256>(v, sh);
+    if (threadIdx.x == 0) out[0] = v;
+}
+
+__global__ void gather_index_kernel(const int64_t* __restrict__ index, const int64_t* __restrict__ pos, int k,
+                                    int64_t* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < k) out[i] = index[pos[i]];
 }
 
 }  // namespace
@@ -106,82 +154,88 @@ struct PairQr {
     const Context& c;
     cudaStream_t s;
     int64_t n = 0, d = 0, m = 0;
-    DeviceBuffer<double> F, sw, nf, est, kdiag, D, L, Q, a, r, tvec, scal, Rcol;
+    DeviceBuffer<double> F, sw, nf, est, kdiag, D, L, Q, a, r, t0, t1, scal, Rcol;
     DeviceBuffer<char> selected;
     DeviceBuffer<int64_t> pos;
     DeviceBuffer<ArgKey> partial, best;
     int64_t capL = 0;
     int nblocks = 0;
-    std::vector<double> R;   // column-major, capL x capL (host)
     PairQr(const Context& ctx, cudaStream_t st) : c(ctx), s(st) {}
 
-    ArgKey argmax(bool use_pos) {
+    void argmax_launch(bool use_pos) {
         argmax_kernel<<<nblocks, kNT, 0, s>>>(est.get(), selected.get(),
                                               use_pos ? pos.get() : nullptr, n, partial.get());
         ISDF_LAUNCH_CHECK();
         argmax_final_kernel<<<1, 1024, 0, s>>>(partial.get(), nblocks, best.get());
         ISDF_LAUNCH_CHECK();
+    }
+    ArgKey argmax(bool use_pos) {
+        argmax_launch(use_pos);
         ArgKey h;
         ISDF_CUDA(cudaMemcpyAsync(&h, best.get(), sizeof(ArgKey), cudaMemcpyDeviceToHost, s));
         ISDF_CUDA(cudaStreamSynchronize(s));
         return h;
     }
 
-    // Exact residual of column p against the j current basis vectors: leaves the
-    // residual in r, the CGS2 coefficients in coeff (host), returns |r|^2.
-    double exact_residual(int64_t p, int j, std::vector<double>& coeff) {
-        double swp = 0;
-        ISDF_CUDA(cudaMemcpyAsync(&swp, sw.get() + p, sizeof(double), cudaMemcpyDeviceToHost, s));
-        ISDF_CUDA(cudaStreamSynchronize(s));
-        pair_vector(F.get() + p * d, d, swp, a.get(), s);
-        coeff.assign(j, 0.0);
+    // Exact residual of column p against the j current basis vectors, on the
+    // device: the residual in r, the two CGS passes' coefficients in t0 and
+    // t1, |r|^2 in scal, and est[p] = |r|^2.
+    void exact_residual_launch(int64_t p, int j) {
+        pair_vector_sw_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, s>>>(F.get() + p * d, d,
+                                                                                    sw.get(), p, a.get());
+        ISDF_LAUNCH_CHECK();
         scal.zero(s);
         if (j == 0) {
-            rows_axpy(Q.get(), 0, m, tvec.get(), a.get(), r.get(), scal.get(), s);
+            rows_axpy(Q.get(), 0, m, t0.get(), a.get(), r.get(), scal.get(), s);
         } else {
-            const double* src = a.get();
-            for (int pass = 0; pass < 2; ++pass) {
-                tvec.zero(s);
-                rows_dot(Q.get(), j, m, src, tvec.get(), s);
-                if (pass == 1) scal.zero(s);
-                rows_axpy(Q.get(), j, m, tvec.get(), src, r.get(), pass == 1 ? scal.get() : nullptr, s);
-                std::vector<double> t(j);
-                ISDF_CUDA(cudaMemcpyAsync(t.data(), tvec.get(), j * sizeof(double),
-                                          cudaMemcpyDeviceToHost, s));
-                ISDF_CUDA(cudaStreamSynchronize(s));
-                for (int i = 0; i < j; ++i) coeff[i] += t[i];
-                src = r.get();
-            }
+            t0.zero(s);
+            rows_dot(Q.get(), j, m, a.get(), t0.get(), s);
+            rows_axpy(Q.get(), j, m, t0.get(), a.get(), r.get(), nullptr, s);
+            t1.zero(s);
+            rows_dot(Q.get(), j, m, r.get(), t1.get(), s);
+            rows_axpy(Q.get(), j, m, t1.get(), r.get(), r.get(), scal.get(), s);
         }
+        set_est_kernel<<<1, 1, 0, s>>>(est.get(), p, scal.get());
+        ISDF_LAUNCH_CHECK();
+    }
+    double exact_residual(int64_t p, int j) {
+        exact_residual_launch(p, j);
         double nr2 = 0;
         ISDF_CUDA(cudaMemcpyAsync(&nr2, scal.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
         ISDF_CUDA(cudaStreamSynchronize(s));
         return nr2;
     }
-
-    void set_est(int64_t g, double v) {
-        ISDF_CUDA(cudaMemcpyAsync(est.get() + g, &v, sizeof(double), cudaMemcpyHostToDevice, s));
+    // exact residual of p, then the argmax over the updated estimates: one
+    // host round trip for both
+    ArgKey verify(int64_t p, int j, bool use_pos, double& exact2) {
+        exact_residual_launch(p, j);
+        argmax_launch(use_pos);
+        ArgKey h;
+        ISDF_CUDA(cudaMemcpyAsync(&h, best.get(), sizeof(ArgKey), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaMemcpyAsync(&exact2, scal.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
         ISDF_CUDA(cudaStreamSynchronize(s));
+        return h;
     }
 
     void grow(int64_t need) {
         if (need <= capL) return;
         const int64_t cap2 = std::max<int64_t>(need, std::max<int64_t>(8, 2 * capL));
-        DeviceBuffer<double> L2(static_cast<size_t>(n * cap2), s), Q2(static_cast<size_t>(cap2 * m), s);
+        DeviceBuffer<double> L2(static_cast<size_t>(n * cap2), s), Q2(static_cast<size_t>(cap2 * m), s),
+            t02(cap2, s), t12(cap2, s);
         if (capL) {
             ISDF_CUDA(cudaMemcpy2DAsync(L2.get(), cap2 * sizeof(double), L.get(), capL * sizeof(double),
                                         capL * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
             ISDF_CUDA(cudaMemcpyAsync(Q2.get(), Q.get(), capL * m * sizeof(double),
                                       cudaMemcpyDeviceToDevice, s));
+            // the coefficients of the column being accepted
+            ISDF_CUDA(cudaMemcpyAsync(t02.get(), t0.get(), capL * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            ISDF_CUDA(cudaMemcpyAsync(t12.get(), t1.get(), capL * sizeof(double), cudaMemcpyDeviceToDevice, s));
         }
         L = std::move(L2);
         Q = std::move(Q2);
-        std::vector<double> R2(static_cast<size_t>(cap2 * cap2), 0.0);
-        for (int64_t jj = 0; jj < capL; ++jj)
-            for (int64_t ii = 0; ii < capL; ++ii) R2[jj * cap2 + ii] = R[jj * capL + ii];
-        R.swap(R2);
+        t0 = std::move(t02);
+        t1 = std::move(t12);
         capL = cap2;
-        tvec.reset(capL, s);
         Rcol.reset(capL, s);
     }
 };
@@ -260,32 +314,34 @@ std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const d
     q.partial.reset(q.nblocks, s);
     q.best.reset(1, s);
     q.a.reset(m, s); q.r.reset(m, s); q.scal.reset(1, s);
+    DeviceBuffer<double> kpart(q.nblocks, s), ksum(1, s);
+    DeviceBuffer<int> kbad(1, s);
+    kbad.zero(s);
     gather_weights_kernel<<<nb, 256, 0, s>>>(w, kp.index.get(), n, q.sw.get());
     ISDF_LAUNCH_CHECK();
     row_dot(q.F.get(), n, d, nullptr, q.nf.get(), s);
     init_est_kernel<<<nb, 256, 0, s>>>(q.sw.get(), q.nf.get(), n, q.est.get(), q.kdiag.get());
     ISDF_LAUNCH_CHECK();
     {
-        std::vector<double> kd(n);
-        ISDF_CUDA(cudaMemcpyAsync(kd.data(), q.kdiag.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
-        ISDF_CUDA(cudaStreamSynchronize(s));
+        // sum of K_gg (the squared Frobenius norm of the pair matrix) and its finiteness
+        kdiag_partial_kernel<<<q.nblocks, 256, 0, s>>>(q.kdiag.get(), n, kpart.get(), kbad.get());
+        ISDF_LAUNCH_CHECK();
+        sum_partials_kernel<<<1, 256, 0, s>>>(kpart.get(), q.nblocks, ksum.get());
+        ISDF_LAUNCH_CHECK();
         double frob2 = 0;
-        for (double x : kd) {
-            if (!std::isfinite(x)) fail(kOverflow, online ? "non-finite online AO pair column"
-                                                          : "non-finite weighted pair product");
-            frob2 += x;
-        }
+        int hbad = 0;
+        ISDF_CUDA(cudaMemcpyAsync(&frob2, ksum.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaMemcpyAsync(&hbad, kbad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        if (hbad || !std::isfinite(frob2))
+            fail(kOverflow, online ? "non-finite online AO pair column" : "non-finite weighted pair product");
         if (diag) diag->floor = 32 * std::numeric_limits<double>::epsilon() * std::sqrt(frob2);
         q.grow(8);
         const int64_t cap = std::min({m, n, o.max_rank ? o.max_rank : std::min(m, n)});
         const double eps = std::numeric_limits<double>::epsilon();
         const double floor = online ? 32 * eps * std::sqrt(frob2) : 0.0;
-        std::vector<int64_t> kept(n);
-        ISDF_CUDA(cudaMemcpyAsync(kept.data(), kp.index.get(), n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-        ISDF_CUDA(cudaStreamSynchronize(s));
         std::vector<int64_t> result;
         double first = -1;
-        std::vector<double> coeff;
         int64_t verifications = 0, reselections = 0, exact_scans = 0;
         DeviceBuffer<char> flags(n, s);
         std::vector<char> hflags;
@@ -295,13 +351,12 @@ std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const d
             if (j == cap) break;
             ArgKey k = q.argmax(!online);
             if (k.col < 0) break;
-            // verification loop
+            // verification loop: the leader's exact residual, then the argmax
+            // over the updated estimates (one host round trip per candidate)
             double exact2 = 0;
             while (true) {
-                exact2 = q.exact_residual(k.col, j, coeff);
+                const ArgKey k2 = q.verify(k.col, j, !online, exact2);
                 ++verifications;
-                q.set_est(k.col, exact2);
-                ArgKey k2 = q.argmax(!online);
                 if (k2.col == k.col) break;
                 ++reselections;
                 k = k2;
@@ -322,11 +377,11 @@ std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const d
                 ISDF_CUDA(cudaStreamSynchronize(s));
                 ++exact_scans;
                 for (int64_t g = 0; g < n; ++g)
-                    if (hflags[g]) q.set_est(g, q.exact_residual(g, j, coeff));
+                    if (hflags[g]) q.exact_residual_launch(g, j);   // also sets est[g]
                 exact_mode = true;
                 k = q.argmax(!online);
                 if (k.col < 0) break;
-                exact2 = q.exact_residual(k.col, j, coeff);
+                exact2 = q.exact_residual(k.col, j);
                 const double r2 = std::sqrt(exact2);
                 if (first == 0 || r2 <= thr) break;
             }
@@ -334,8 +389,8 @@ std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const d
             const int64_t p = k.col;
             const double rj = std::sqrt(exact2);
             q.grow(j + 1);
-            for (int i = 0; i < j; ++i) q.R[static_cast<size_t>(j) * q.capL + i] = coeff[i];
-            q.R[static_cast<size_t>(j) * q.capL + j] = rj;
+            rcol_kernel<<<1, 64, 0, s>>>(q.t0.get(), q.t1.get(), j, q.scal.get(), q.Rcol.get());
+            ISDF_LAUNCH_CHECK();
             scale_copy(q.r.get(), 1.0 / rj, m, q.Q.get() + static_cast<int64_t>(j) * m, s);
             mark_selected_kernel<<<1, 1, 0, s>>>(q.selected.get(), q.est.get(), p);
             ISDF_LAUNCH_CHECK();
@@ -345,21 +400,26 @@ std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const d
             }
             // new column of L and downdated estimates
             row_dot(q.F.get(), n, d, q.F.get() + p * d, q.D.get(), s);
-            ISDF_CUDA(cudaMemcpyAsync(q.Rcol.get(), q.R.data() + static_cast<size_t>(j) * q.capL,
-                                      j * sizeof(double) + sizeof(double), cudaMemcpyHostToDevice, s));
-            double swp = 0;
-            ISDF_CUDA(cudaMemcpyAsync(&swp, q.sw.get() + p, sizeof(double), cudaMemcpyDeviceToHost, s));
-            ISDF_CUDA(cudaStreamSynchronize(s));
-            update_residual_kernel<<<nb, 256, 0, s>>>(q.D.get(), q.sw.get(), swp, n, q.L.get(), q.capL,
+            update_residual_kernel<<<nb, 256, 0, s>>>(q.D.get(), q.sw.get(), p, n, q.L.get(), q.capL,
                                                       j, q.Rcol.get(), rj, q.est.get(), q.selected.get());
             ISDF_LAUNCH_CHECK();
             exact_mode = false;   // downdated estimates carry rounding again
             result.push_back(p);
             if (diag) diag->rdiag.push_back(rj);
         }
+        // grid indices of the pivots
+        std::vector<int64_t> out(result.size());
+        if (!result.empty()) {
+            DeviceBuffer<int64_t> dres(result.size(), s), dout(result.size(), s);
+            ISDF_CUDA(cudaMemcpyAsync(dres.get(), result.data(), result.size() * sizeof(int64_t),
+                                      cudaMemcpyHostToDevice, s));
+            gather_index_kernel<<<static_cast<unsigned>((result.size() + 255) / 256), 256, 0, s>>>(
+                kp.index.get(), dres.get(), static_cast<int>(result.size()), dout.get());
+            ISDF_LAUNCH_CHECK();
+            ISDF_CUDA(cudaMemcpyAsync(out.data(), dout.get(), out.size() * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                      s));
+        }
         ISDF_CUDA(cudaStreamSynchronize(s));
-        std::vector<int64_t> out;
-        for (auto p : result) out.push_back(kept[p]);
         if (diag) {
             diag->rank = static_cast<int64_t>(out.size());
             diag->verifications = verifications;
