@@ -201,8 +201,8 @@ def build_isdf(mol, *, level=0, anchor_rank=0, anchor_tol=None, axes=("ao",), ax
     AO axis only, FP64 form) weight pair columns by sqrt(point_importance) and
     screen points whose squared AO norm is <= `ao_screening_threshold`
     (``python/isdf.py:322-340``).  `point_importance` is the complete m on the
-    grid; generating it needs an RKS B3LYP density (PySCF), which this build
-    does not have, so it must be given.
+    grid; generating it needs an RKS B3LYP density (PySCF), which this
+    package does not provide, so it must be given.
 
     The occupied-orbital axis (`"occ"`) takes the row-major (nao, nao) RHF
     `mo_coeff` and `nocc` (the reference takes them from a PySCF RHF,

@@ -1,7 +1,7 @@
 """The drop-in driver python/isdf.py run as a program (its CLI,
 python/isdf.py:825-1004 of the reference): every anchor algorithm of this
-build, the axes parser, the pair-space error, the grid metric and the JSON
-record; refusals for what is outside this build."""
+package, the axes parser, the pair-space error, the grid metric and the JSON
+record; refusals for what is outside its scope."""
 import json
 import subprocess
 import sys
