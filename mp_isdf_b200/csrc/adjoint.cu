@@ -160,25 +160,29 @@ struct AdjGridArgs {
     const double* w;
     const int64_t* index;      // kept points
     int64_t n;
-    const double* phia;        // [KMAX][nao], rows >= k zero
-    const double* dphia;       // [3][KMAX][nao], rows >= k zero
+    const double* pk;          // [nao][4][KMAX]: Phi_a and its d/dx, d/dy, d/dz per AO, anchors >= k zero
     const double* z;           // [KMAX], zero padded
     double* gacc;              // [natm][3] += sum_g sum_{mu in atom} (beta grad phi + phi t)
     double* v;                 // [KMAX] += sum_g u_g G_gk^2
     double* energy;            // += sum_g w_g rho_g^2
 };
 
-// sweep 1: G[a] += phi_mu(g) Phi_a[a][mu]
+// sweep 1: G[a] += phi_mu(g) Phi_a[a][mu]; an AO's anchor values are
+// contiguous, read as 16-byte pairs
 template <int KMAX>
 struct GramSink {
-    const double* phia;
-    int nao;
+    const double* pk;
     double G[KMAX];
     template <int C>
     __device__ __forceinline__ void put(int ao, double v) {
         if constexpr (C == 0) {
+            const double2* q = reinterpret_cast<const double2*>(pk + static_cast<int64_t>(ao) * 4 * KMAX);
 #pragma unroll
-            for (int a = 0; a < KMAX; ++a) G[a] += v * __ldg(phia + a * nao + ao);
+            for (int a = 0; a < KMAX / 2; ++a) {
+                const double2 x = __ldg(q + a);
+                G[2 * a] += v * x.x;
+                G[2 * a + 1] += v * x.y;
+            }
         }
     }
 };
@@ -187,21 +191,26 @@ struct GramSink {
 // acc += beta grad phi_mu(g) + phi_mu(g) t
 template <int KMAX>
 struct GradSink {
-    const double* phia;
-    const double* dphia;
-    int nao;
+    const double* pk;
     double al[KMAX];
     double beta, acc[3];
     template <int C>
     __device__ __forceinline__ void put(int ao, double v) {
         if constexpr (C == 0) {
             double b = 0, t0 = 0, t1 = 0, t2 = 0;
+            const double2* q = reinterpret_cast<const double2*>(pk + static_cast<int64_t>(ao) * 4 * KMAX);
 #pragma unroll
-            for (int a = 0; a < KMAX; ++a) {
-                b += al[a] * __ldg(phia + a * nao + ao);
-                t0 += al[a] * __ldg(dphia + (0 * KMAX + a) * nao + ao);
-                t1 += al[a] * __ldg(dphia + (1 * KMAX + a) * nao + ao);
-                t2 += al[a] * __ldg(dphia + (2 * KMAX + a) * nao + ao);
+            for (int a = 0; a < KMAX / 2; ++a) {
+                const double2 x = __ldg(q + a), x0 = __ldg(q + KMAX / 2 + a), x1 = __ldg(q + KMAX + a),
+                              x2 = __ldg(q + 3 * KMAX / 2 + a);
+                b += al[2 * a] * x.x;
+                t0 += al[2 * a] * x0.x;
+                t1 += al[2 * a] * x1.x;
+                t2 += al[2 * a] * x2.x;
+                b += al[2 * a + 1] * x.y;
+                t0 += al[2 * a + 1] * x0.y;
+                t1 += al[2 * a + 1] * x1.y;
+                t2 += al[2 * a + 1] * x2.y;
             }
             beta = b;
             acc[0] += v * t0;
@@ -237,7 +246,7 @@ __global__ void __launch_bounds__(kAdjPts * kAdjLanes, 1) adjoint_grid_kernel(Ad
             wg = args.w[gi];
         }
         // sweep 1: G = Phi_a phi_g, partial over this lane's shells
-        GramSink<KMAX> gs{args.phia, args.nao, {}};
+        GramSink<KMAX> gs{args.pk, {}};
 #pragma unroll
         for (int a = 0; a < KMAX; ++a) gs.G[a] = 0.0;
         // a shell whose FP64 screening exponent puts all 32 points of the warp
@@ -275,7 +284,7 @@ __global__ void __launch_bounds__(kAdjPts * kAdjLanes, 1) adjoint_grid_kernel(Ad
         if constexpr (!GRAD) continue;
         // sweep 2: values and gradients; per shell, the warp's 32 points are
         // reduced before one shared-memory add per component
-        GradSink<KMAX> gr{args.phia, args.dphia, args.nao, {}, 0.0, {0.0, 0.0, 0.0}};
+        GradSink<KMAX> gr{args.pk, {}, 0.0, {0.0, 0.0, 0.0}};
 #pragma unroll
         for (int a = 0; a < KMAX; ++a) gr.al[a] = As[p * KMAX + a];
         for (int sh = sl; sh < args.nshell; sh += kAdjLanes) {
@@ -320,6 +329,20 @@ __global__ void pad_rows_kernel(const double* __restrict__ src, int ncomp, int k
     const int a = static_cast<int>((i / nao) % kmax);
     const int c = static_cast<int>(i / (static_cast<int64_t>(nao) * kmax));
     dst[i] = a < k ? src[(static_cast<int64_t>(c) * k + a) * nao + mu] : 0.0;
+}
+
+// out[mu][c][a] = (c == 0 ? phi_a : dphi_a[c - 1])[a][mu] for a < k, 0 for k <= a < kmax
+__global__ void pack_anchor_rows_kernel(const double* __restrict__ phia, const double* __restrict__ dphia, int k,
+                                        int kmax, int nao, double* __restrict__ out) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= static_cast<int64_t>(nao) * 4 * kmax) return;
+    const int a = static_cast<int>(i % kmax);
+    const int c = static_cast<int>((i / kmax) % 4);
+    const int64_t mu = i / (4 * kmax);
+    double v = 0.0;
+    if (a < k && (c == 0 || dphia))
+        v = c == 0 ? phia[static_cast<int64_t>(a) * nao + mu] : dphia[(static_cast<int64_t>(c - 1) * k + a) * nao + mu];
+    out[i] = v;
 }
 
 }  // namespace
@@ -375,19 +398,16 @@ AdjointResult energy_gradient(const Context& c, const double* pts, const double*
     gacc.zero(s);
     if (fused) {
         ISDF_PROFILE("adjoint_grid", s);
-        DeviceBuffer<double> phia_pad(static_cast<size_t>(kmax * nao), s),
-            dphia_pad(static_cast<size_t>(3 * kmax * nao), s), z_pad(kmax, s);
-        pad_rows_kernel<<<nblk(kmax * nao), 256, 0, s>>>(f.phi_a.get(), 1, static_cast<int>(k), kmax,
-                                                          static_cast<int>(nao), phia_pad.get());
-        ISDF_LAUNCH_CHECK();
-        pad_rows_kernel<<<nblk(3 * kmax * nao), 256, 0, s>>>(dphia.get(), 3, static_cast<int>(k), kmax,
-                                                              static_cast<int>(nao), dphia_pad.get());
+        // anchor values and gradients per AO, contiguous (16-byte pair loads)
+        DeviceBuffer<double> pk(static_cast<size_t>(4 * kmax * nao), s), z_pad(kmax, s);
+        pack_anchor_rows_kernel<<<nblk(4 * kmax * nao), 256, 0, s>>>(f.phi_a.get(), want_grad ? dphia.get() : nullptr,
+                                                                    static_cast<int>(k), kmax, static_cast<int>(nao),
+                                                                    pk.get());
         ISDF_LAUNCH_CHECK();
         pad_rows_kernel<<<1, 256, 0, s>>>(z.get(), 1, static_cast<int>(k), kmax, 1, z_pad.get());
         ISDF_LAUNCH_CHECK();
         AdjGridArgs a{c.d_shells, c.nshell, static_cast<int>(nao), c.natm, c.d_exp, c.d_coef, pts, w,
-                      kp.index.get(), n, phia_pad.get(), dphia_pad.get(), z_pad.get(), gacc.get(), v.get(),
-                      energy.get()};
+                      kp.index.get(), n, pk.get(), z_pad.get(), gacc.get(), v.get(), energy.get()};
         if (c.lmax <= 2) {
             if (kmax == 4) launch_adjoint_grid<2, 4>(a, want_grad, s);
             else if (kmax == 8) launch_adjoint_grid<2, 8>(a, want_grad, s);
