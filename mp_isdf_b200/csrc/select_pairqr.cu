@@ -37,17 +37,38 @@ __global__ void gather_weights_kernel(const double* __restrict__ w, const int64_
     if (g < n) sw[g] = sqrt(fabs(w[idx[g]]));
 }
 
-// F[:, a-block] *= scale[a]
-// Column j of F (the features of axis entry a, offset[a] <= j < offset[a] +
-// width[a]) times scales[a].
-__global__ void scale_columns_kernel(double* F, int64_t n, int64_t d, AxisSpec ax,
-                                     const double* __restrict__ scales) {
-    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= n * d) return;
-    const int j = static_cast<int>(i % d);
+// The multi-axis scales are applied where F is read instead of in F itself
+// (a pass over n x d values saved): cs[j] = scale of column j's axis entry.
+__global__ void column_scales_kernel(AxisSpec ax, const double* __restrict__ scales, int64_t d,
+                                     double* __restrict__ cs) {
+    const int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= d) return;
     int a = 0;
     while (a + 1 < ax.naxes && j >= ax.offset[a + 1]) ++a;
-    F[i] *= scales[a];
+    cs[j] = scales[a];
+}
+
+// warp per row: nf[g] = sum_k (cs[k] F[g,k])^2
+__global__ void scaled_row_norms_kernel(const double* __restrict__ F, int64_t n, int64_t d,
+                                        const double* __restrict__ cs, double* __restrict__ nf) {
+    const int64_t g = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (g >= n) return;
+    const double* row = F + g * d;
+    double acc = 0;
+    for (int64_t k = lane; k < d; k += 32) {
+        const double v = cs[k] * row[k];
+        acc += v * v;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) nf[g] = acc;
+}
+
+// x[k] = cs[k]^2 F[p,k]: with it, F x is the Gram row of the scaled features
+__global__ void scaled_pivot_row_kernel(const double* __restrict__ fp, const double* __restrict__ cs, int64_t d,
+                                        double* __restrict__ x) {
+    const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < d) x[k] = cs[k] * cs[k] * fp[k];
 }
 
 __global__ void init_est_kernel(const double* __restrict__ sw, const double* __restrict__ nf,
@@ -98,12 +119,14 @@ __global__ void update_residual_kernel(const double* __restrict__ D, const doubl
     if (!selected[g]) est[g] = fmax(est[g] - v * v, 0.0);
 }
 
-// a[i*d + k] = sw[p] f[i] f[k]: the weighted pair vector of column p
+// a[i*d + k] = sw[p] f[i] f[k]: the weighted pair vector of column p (f
+// scaled by cs where the axis entries carry scales)
 __global__ void pair_vector_sw_kernel(const double* __restrict__ f, int64_t d, const double* __restrict__ sw,
-                                      int64_t p, double* __restrict__ a) {
+                                      int64_t p, const double* __restrict__ cs, double* __restrict__ a) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= d * d) return;
-    a[i] = sw[p] * f[i / d] * f[i % d];
+    const int64_t r = i / d, c = i % d;
+    a[i] = cs ? sw[p] * (cs[r] * f[r]) * (cs[c] * f[c]) : sw[p] * f[r] * f[c];
 }
 
 // est[p] = the exact squared residual just computed
@@ -154,7 +177,7 @@ struct PairQr {
     const Context& c;
     cudaStream_t s;
     int64_t n = 0, d = 0, m = 0;
-    DeviceBuffer<double> F, sw, nf, est, kdiag, D, L, Q, a, r, t0, t1, scal, Rcol;
+    DeviceBuffer<double> F, sw, nf, est, kdiag, D, L, Q, a, r, t0, t1, scal, Rcol, cs, xp;
     DeviceBuffer<char> selected;
     DeviceBuffer<int64_t> pos;
     DeviceBuffer<ArgKey> partial, best;
@@ -181,8 +204,8 @@ struct PairQr {
     // device: the residual in r, the two CGS passes' coefficients in t0 and
     // t1, |r|^2 in scal, and est[p] = |r|^2.
     void exact_residual_launch(int64_t p, int j) {
-        pair_vector_sw_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, s>>>(F.get() + p * d, d,
-                                                                                    sw.get(), p, a.get());
+        pair_vector_sw_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, s>>>(
+            F.get() + p * d, d, sw.get(), p, cs.get(), a.get());
         ISDF_LAUNCH_CHECK();
         scal.zero(s);
         if (j == 0) {
@@ -299,10 +322,11 @@ std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const d
         auto sc = axis_scales_from_sumsq(ax, h, o.axis_weights.empty() ? nullptr : o.axis_weights.data(), true);
         DeviceBuffer<double> dsc(sc.size(), s);
         ISDF_CUDA(cudaMemcpyAsync(dsc.get(), sc.data(), sc.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        scale_columns_kernel<<<static_cast<unsigned>((n * d + 255) / 256), 256, 0, s>>>(
-            q.F.get(), n, d, ax, dsc.get());
+        q.cs.reset(d, s);
+        q.xp.reset(d, s);
+        column_scales_kernel<<<static_cast<unsigned>((d + 255) / 256), 256, 0, s>>>(ax, dsc.get(), d, q.cs.get());
         ISDF_LAUNCH_CHECK();
-        ISDF_CUDA(cudaStreamSynchronize(s));
+        ISDF_CUDA(cudaStreamSynchronize(s));   // host scales go out of scope
     }
     const unsigned nb = static_cast<unsigned>((n + 255) / 256);
     q.sw.reset(n, s); q.nf.reset(n, s); q.est.reset(n, s); q.kdiag.reset(n, s); q.D.reset(n, s);
@@ -319,7 +343,13 @@ std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const d
     kbad.zero(s);
     gather_weights_kernel<<<nb, 256, 0, s>>>(w, kp.index.get(), n, q.sw.get());
     ISDF_LAUNCH_CHECK();
-    row_dot(q.F.get(), n, d, nullptr, q.nf.get(), s);
+    if (q.cs.get()) {
+        scaled_row_norms_kernel<<<static_cast<unsigned>((n * 32 + 255) / 256), 256, 0, s>>>(q.F.get(), n, d,
+                                                                                          q.cs.get(), q.nf.get());
+        ISDF_LAUNCH_CHECK();
+    } else {
+        row_dot(q.F.get(), n, d, nullptr, q.nf.get(), s);
+    }
     init_est_kernel<<<nb, 256, 0, s>>>(q.sw.get(), q.nf.get(), n, q.est.get(), q.kdiag.get());
     ISDF_LAUNCH_CHECK();
     {
@@ -399,7 +429,14 @@ std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const d
                 ISDF_LAUNCH_CHECK();
             }
             // new column of L and downdated estimates
-            row_dot(q.F.get(), n, d, q.F.get() + p * d, q.D.get(), s);
+            const double* xrow = q.F.get() + p * d;
+            if (q.cs.get()) {
+                scaled_pivot_row_kernel<<<static_cast<unsigned>((d + 255) / 256), 256, 0, s>>>(xrow, q.cs.get(), d,
+                                                                                             q.xp.get());
+                ISDF_LAUNCH_CHECK();
+                xrow = q.xp.get();
+            }
+            row_dot(q.F.get(), n, d, xrow, q.D.get(), s);
             update_residual_kernel<<<nb, 256, 0, s>>>(q.D.get(), q.sw.get(), p, n, q.L.get(), q.capL,
                                                       j, q.Rcol.get(), rj, q.est.get(), q.selected.get());
             ISDF_LAUNCH_CHECK();
