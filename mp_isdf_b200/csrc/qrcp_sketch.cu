@@ -269,8 +269,10 @@ __global__ void __launch_bounds__(kPairThreads) qr_update_pairs_kernel(QrState s
 }
 
 // Verified mode: every unselected column whose interval reaches the best
-// lower bound (and is not exact yet) is listed for recomputation; the others
-// enter the per-block argmax keys directly.
+// lower bound (and is not exact yet) is listed for recomputation; the exact
+// columns enter the per-block argmax keys directly.  A column that is neither
+// cannot win: its estimate is below (sqrt(e) + delta)^2 < lb^2, and the column
+// that sets lb is a candidate or exact with a norm of at least lb.
 __global__ void __launch_bounds__(kQrThreads) candidates_kernel(QrState st, int64_t* cand) {
     __shared__ ArgKey ksh[kQrThreads / 32];
     const int64_t g = static_cast<int64_t>(blockIdx.x) * kQrThreads + threadIdx.x;
@@ -282,7 +284,7 @@ __global__ void __launch_bounds__(kQrThreads) candidates_kernel(QrState st, int6
             const int64_t i = static_cast<int64_t>(
                 atomicAdd(reinterpret_cast<unsigned long long*>(st.count), 1ull));
             cand[i] = g;
-        } else {
+        } else if (!(d > 0.0)) {
             key = ArgKey{e, st.pos[g], g};
         }
     }
