@@ -30,7 +30,10 @@
 #include <mutex>
 #include <new>
 #include <random>
+#include <condition_variable>
+#include <functional>
 #include <thread>
+#include <unistd.h>
 
 namespace isdf {
 
@@ -308,6 +311,71 @@ private:
     int idx_ = kN;
 };
 
+// Worker threads for the sketch-factor draw, created once per process (a
+// call used to start a dozen threads, 20-50 us each): start(n, job) has n pool
+// threads call job(0..n-1) while the caller works on; wait() returns when all
+// have finished.  One run at a time (start takes a lock that wait releases); a
+// process forked after the pool started gets a fresh pool.
+class DrawPool {
+public:
+    static DrawPool& get(int size) {
+        static std::mutex mu;
+        static DrawPool* pool = nullptr;
+        std::lock_guard<std::mutex> lk(mu);
+        if (!pool || pool->pid_ != getpid() || pool->size() < size) pool = new DrawPool(size);   // old one leaks
+        return *pool;
+    }
+    int size() const { return static_cast<int>(threads_.size()); }
+    void start(int n, const std::function<void(int)>& job) {
+        run_mu_.lock();
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            job_ = &job;
+            njobs_ = n;
+            pending_ = n;
+            ++gen_;
+        }
+        cv_.notify_all();
+    }
+    void wait() {
+        {
+            std::unique_lock<std::mutex> lk(m_);
+            done_.wait(lk, [this] { return pending_ == 0; });
+            job_ = nullptr;
+        }
+        run_mu_.unlock();
+    }
+
+private:
+    explicit DrawPool(int size) : pid_(getpid()) {
+        for (int i = 0; i < size; ++i) {
+            threads_.emplace_back([this, i] { loop(i); });
+            threads_.back().detach();
+        }
+    }
+    void loop(int id) {
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> lk(m_);
+        for (;;) {
+            cv_.wait(lk, [&] { return gen_ != seen; });
+            seen = gen_;
+            if (id >= njobs_) continue;
+            const std::function<void(int)>* job = job_;
+            lk.unlock();
+            (*job)(id);
+            lk.lock();
+            if (--pending_ == 0) done_.notify_all();
+        }
+    }
+    pid_t pid_;
+    std::vector<std::thread> threads_;
+    std::mutex m_, run_mu_;
+    std::condition_variable cv_, done_;
+    const std::function<void(int)>* job_ = nullptr;
+    int njobs_ = 0, pending_ = 0;
+    uint64_t gen_ = 0;
+};
+
 struct PolarDraws {
     std::vector<uint64_t> raw;        // two engine outputs per attempt
     std::vector<int64_t> block_out;   // deviates produced before each block
@@ -397,11 +465,29 @@ void sketch_factors(int64_t d, int64_t ell, uint64_t seed, double* u, double* v)
             }
     };
     {
-        std::vector<std::thread> threads;
-        threads.emplace_back([&] { tail_gen[1] = polar_draw(seeds[1], pairs, max_blocks, pd[1]); });
-        for (int w = 0; w < nw; ++w) threads.emplace_back(work, w);
-        tail_gen[0] = polar_draw(seeds[0], pairs, max_blocks, pd[0]);
-        for (auto& t : threads) t.join();
+        // pool job 0 draws stream 1, jobs 1..nw transform; this thread draws stream 0
+        DrawPool& pool = DrawPool::get(nw + 1);
+        std::exception_ptr err;
+        std::mutex err_mu;
+        const std::function<void(int)> job = [&](int i) {
+            try {
+                if (i == 0) tail_gen[1] = polar_draw(seeds[1], pairs, max_blocks, pd[1]);
+                else work(i - 1);
+            } catch (...) {
+                std::lock_guard<std::mutex> lk(err_mu);
+                if (!err) err = std::current_exception();
+            }
+        };
+        pool.start(nw + 1, job);
+        try {
+            tail_gen[0] = polar_draw(seeds[0], pairs, max_blocks, pd[0]);
+        } catch (...) {
+            pd[0].done.store(true, std::memory_order_release);   // release the transform workers
+            pool.wait();
+            throw;
+        }
+        pool.wait();
+        if (err) std::rethrow_exception(err);
     }
     for (int k = 0; k < 2; ++k) {
         // practically never: continue the engine where the blocks end
