@@ -103,6 +103,29 @@ def test_sketch_factors_match_standard_library_streams(d, ell, seed):
     assert np.array_equal(v, ov)
 
 
+def test_sketch_factors_concurrent_calls():
+    """The draw's process-wide worker pool serves one call at a time: calls
+    from several host threads at once (different seeds and sizes) each return
+    their own standard-library streams."""
+    import threading
+    from mp_isdf_b200 import capi
+    from oracle import oracle as O
+    cases = [(96, 12, 2), (384, 26, 5), (1536, 26, 9), (7, 3, 11)] * 2
+    got = [None] * len(cases)
+
+    def draw(i):
+        got[i] = capi.sketch_factors(*cases[i])
+
+    threads = [threading.Thread(target=draw, args=(i,)) for i in range(len(cases))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for (d, ell, seed), (u, v) in zip(cases, got):
+        ou, ov = O.sketch_factors(d, ell, seed)
+        assert np.array_equal(u, ou) and np.array_equal(v, ov)
+
+
 def test_pair_error_terms_reject_null_arrays_without_gpu():
     """Both pair-error reductions reject null device arrays with
     ISDF_ERR_INVALID before any CUDA call (so this runs without a GPU)."""
