@@ -320,6 +320,22 @@ int isdf_pair_error_terms_noalloc(int64_t n, int64_t k, const double* q_dev, con
 int isdf_energy_gradient(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t ng,
                          const int64_t* anchors_host, int64_t k, const double* dm_host,
                          double* energy, double* grad_host, void* stream);
+/* The adjoint over grid shards (one rank per GPU, the grid split into
+ * contiguous shards): isdf_energy_gradient_shard returns a rank's partial sums
+ * over its own points for anchors given by coordinates (k x 3, bohr) and
+ * weights (isdf_adjoint_partial_size doubles: [E, v (k), per-atom grid terms
+ * (natm x 3), alpha^T Phi_g (k x nao), per-AO grid terms (3 x nao)]); after the
+ * element-wise sum of the partials over ranks (one all-reduce),
+ * isdf_energy_gradient_finish gives E and dE/dR, the same on every rank and
+ * equal to isdf_energy_gradient over the whole grid.  want_grad = 0 / grad_host
+ * = NULL: the energy alone. */
+int isdf_adjoint_partial_size(isdf_ctx* ctx, int64_t k, int64_t* size);
+int isdf_energy_gradient_shard(isdf_ctx* ctx, const double* xyz_dev, const double* w_dev, int64_t ng,
+                               const double* anchor_xyz_host, const double* anchor_w_host, int64_t k,
+                               const double* dm_host, int32_t want_grad, double* partial_host, void* stream);
+int isdf_energy_gradient_finish(isdf_ctx* ctx, const double* anchor_xyz_host, const double* anchor_w_host,
+                                int64_t k, const double* dm_host, const double* sums_host, double* energy,
+                                double* grad_host, void* stream);
 /* Moves the atoms of a context (natm x 3, bohr; the basis functions follow). */
 int isdf_ctx_set_coords(isdf_ctx* ctx, const double* coords_host);
 

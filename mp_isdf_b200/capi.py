@@ -27,6 +27,7 @@ SYMBOLS = [
     "isdf_fit", "isdf_fit_host", "isdf_pair_error", "isdf_pair_error_terms",
     "isdf_profile_enable", "isdf_profile_read", "isdf_project_axes",
     "isdf_energy_gradient", "isdf_ctx_set_coords", "isdf_pair_error_terms_noalloc",
+    "isdf_adjoint_partial_size", "isdf_energy_gradient_shard", "isdf_energy_gradient_finish",
     "isdf_select_fit", "isdf_select_fit_host", "isdf_launch_count", "isdf_sketch_factors",
     "isdf_grid_metric", "isdf_grid_metric_host", "isdf_evaluate_axis_mo", "isdf_evaluate_axis_mo_host",
     "isdf_rbrp_args_default", "isdf_rbrp_ao", "isdf_rbrp_points", "isdf_rbrp_result_info",
@@ -145,6 +146,9 @@ def lib():
         L.isdf_pair_error_terms_noalloc.argtypes = [I64, I64, P, P, P, P, P, P, P]
         L.isdf_project_axes.argtypes = [P, P, I64, P, I32, P, I32, I32, P, P]
         L.isdf_energy_gradient.argtypes = [P, P, P, I64, P, I64, P, ctypes.POINTER(F64), P, P]
+        L.isdf_adjoint_partial_size.argtypes = [P, I64, ctypes.POINTER(I64)]
+        L.isdf_energy_gradient_shard.argtypes = [P, P, P, I64, P, P, I64, P, I32, P, P]
+        L.isdf_energy_gradient_finish.argtypes = [P, P, P, I64, P, P, ctypes.POINTER(F64), P, P]
         L.isdf_ctx_set_coords.argtypes = [P, P]
         L.isdf_profile_enable.argtypes = [I32]
         L.isdf_launch_count.argtypes = []
@@ -401,6 +405,32 @@ class Context:
         g = np.zeros((self.natm, 3))
         check(lib().isdf_energy_gradient(self.h, _ptr(xyz), _ptr(w), xyz.shape[0], _ptr(a), len(a),
                                          _ptr(d), ctypes.byref(e), _ptr(g), _stream(xyz)))
+        return e.value, g
+
+    def energy_gradient_shard(self, xyz, w, anchor_xyz, anchor_w, dm, want_grad=True):
+        """A grid shard's partial sums (numpy float64) of the adjoint for anchors
+        given by coordinates (k x 3) and weights; device tensors xyz, w."""
+        axyz = _np(anchor_xyz, np.float64).reshape(-1, 3)
+        aw = _np(anchor_w, np.float64)
+        d = _np(dm, np.float64)
+        n = I64()
+        check(lib().isdf_adjoint_partial_size(self.h, len(aw), ctypes.byref(n)))
+        out = np.zeros(n.value)
+        check(lib().isdf_energy_gradient_shard(self.h, _ptr(xyz), _ptr(w), xyz.shape[0], _ptr(axyz), _ptr(aw),
+                                               len(aw), _ptr(d), 1 if want_grad else 0, _ptr(out),
+                                               _stream(xyz)))
+        return out
+
+    def energy_gradient_finish(self, anchor_xyz, anchor_w, dm, sums, want_grad=True):
+        """(E, dE/dR[natm,3]) from the partial sums added over all shards."""
+        axyz = _np(anchor_xyz, np.float64).reshape(-1, 3)
+        aw = _np(anchor_w, np.float64)
+        d = _np(dm, np.float64)
+        sm = _np(sums, np.float64)
+        e = F64()
+        g = np.zeros((self.natm, 3))
+        check(lib().isdf_energy_gradient_finish(self.h, _ptr(axyz), _ptr(aw), len(aw), _ptr(d), _ptr(sm),
+                                                ctypes.byref(e), _ptr(g) if want_grad else None, None))
         return e.value, g
 
     def energy(self, xyz, w, anchors, dm):

@@ -364,31 +364,54 @@ void set_atom_coords(Context& c, const double* coords) {
     upload_shell_centres(c);
 }
 
-AdjointResult energy_gradient(const Context& c, const double* pts, const double* w,
-                              const KeptPoints& kp, const AnchorFactor& f, const double* dm,
-                              bool want_grad, cudaStream_t s) {
-    AdjointResult r;
-    const int64_t n = kp.n, k = f.k, nao = c.nao;
-    r.grad.assign(static_cast<size_t>(c.natm) * 3, 0.0);
-    if (k == 0 || n == 0) return r;
-    require(k <= 4096, "too many anchors for the adjoint");
-    // anchor-side quantities
-    DeviceBuffer<double> dphia(static_cast<size_t>(3 * k * nao), s), Dd(static_cast<size_t>(nao * nao), s),
-        PhiD(static_cast<size_t>(k * nao), s), S(static_cast<size_t>(k * k), s), rhoa(k, s), z(k, s),
-        v(k, s), y(k, s), W(static_cast<size_t>(k * k), s), B(static_cast<size_t>(k * nao), s),
-        WPhi(static_cast<size_t>(k * nao), s), coef(static_cast<size_t>(k * nao), s),
-        acc(static_cast<size_t>(3 * nao), s), energy(1, s);
-    ISDF_CUDA(cudaMemcpyAsync(Dd.get(), dm, nao * nao * sizeof(double), cudaMemcpyHostToDevice, s));
-    v.zero(s); B.zero(s); acc.zero(s); energy.zero(s);
+namespace {
+
+// Anchor-side quantities of both passes: Phi_a D, rho_a, z = T rho_a, S and
+// (with gradients) the anchors' AO gradients.
+struct AnchorSide {
+    DeviceBuffer<double> dphia, Dd, PhiD, S, rhoa, z;
+};
+AnchorSide anchor_side(const Context& c, const AnchorFactor& f, const double* dm, bool want_grad, cudaStream_t s) {
+    const int64_t k = f.k, nao = c.nao;
+    AnchorSide a;
+    a.dphia.reset(static_cast<size_t>(3 * k * nao), s);
+    a.Dd.reset(static_cast<size_t>(nao * nao), s);
+    a.PhiD.reset(static_cast<size_t>(k * nao), s);
+    a.S.reset(static_cast<size_t>(k * k), s);
+    a.rhoa.reset(k, s);
+    a.z.reset(k, s);
+    ISDF_CUDA(cudaMemcpyAsync(a.Dd.get(), dm, nao * nao * sizeof(double), cudaMemcpyHostToDevice, s));
     if (want_grad)   // anchor AO gradients (anchor coordinates gathered by the caller into f)
-        eval_ao<double>(c, f.anchor_pts.get(), k, nullptr, dphia.get(), nao, s);
-    gemm_f64(k, nao, nao, f.phi_a.get(), nao, 0, Dd.get(), nao, 0, PhiD.get(), nao, 0, 1, false, s);
+        eval_ao<double>(c, f.anchor_pts.get(), k, nullptr, a.dphia.get(), nao, s);
+    gemm_f64(k, nao, nao, f.phi_a.get(), nao, 0, a.Dd.get(), nao, 0, a.PhiD.get(), nao, 0, 1, false, s);
     rho_anchor_kernel<<<static_cast<unsigned>(k), 32, 0, s>>>(static_cast<int>(k), static_cast<int>(nao),
-                                                                PhiD.get(), f.phi_a.get(), rhoa.get());
+                                                                a.PhiD.get(), f.phi_a.get(), a.rhoa.get());
     ISDF_LAUNCH_CHECK();
-    matvec_kernel<<<nblk(k), 256, 0, s>>>(static_cast<int>(k), f.T.get(), rhoa.get(), z.get());
+    matvec_kernel<<<nblk(k), 256, 0, s>>>(static_cast<int>(k), f.T.get(), a.rhoa.get(), a.z.get());
     ISDF_LAUNCH_CHECK();
-    gemm_f64(k, k, nao, f.phi_a.get(), nao, 0, f.phi_aT.get(), k, 0, S.get(), k, 0, 1, false, s);
+    gemm_f64(k, k, nao, f.phi_a.get(), nao, 0, f.phi_aT.get(), k, 0, a.S.get(), k, 0, 1, false, s);
+    return a;
+}
+
+}  // namespace
+
+size_t adjoint_partial_size(const Context& c, int64_t k) {
+    return static_cast<size_t>(1 + k + 3 * c.natm + k * c.nao + 3 * c.nao);
+}
+
+std::vector<double> energy_gradient_partial(const Context& c, const double* pts, const double* w,
+                                            const KeptPoints& kp, const AnchorFactor& f, const double* dm,
+                                            bool want_grad, cudaStream_t s) {
+    const int64_t n = kp.n, k = f.k, nao = c.nao;
+    std::vector<double> out(adjoint_partial_size(c, k), 0.0);
+    if (k == 0 || n == 0) return out;
+    require(k <= 4096, "too many anchors for the adjoint");
+    AnchorSide as = anchor_side(c, f, dm, want_grad, s);
+    const DeviceBuffer<double>& dphia = as.dphia;
+    const DeviceBuffer<double>& z = as.z;
+    DeviceBuffer<double> v(k, s), B(static_cast<size_t>(k * nao), s), acc(static_cast<size_t>(3 * nao), s),
+        energy(1, s);
+    v.zero(s); B.zero(s); acc.zero(s); energy.zero(s);
 
     const int kmax = k <= 4 ? 4 : k <= 8 ? 8 : k <= 12 ? 12 : k <= 16 ? 16 : 32;
     const size_t fused_smem =
@@ -446,35 +469,62 @@ AdjointResult energy_gradient(const Context& c, const double* pts, const double*
         column_dot_kernel<<<cg, 256, 0, s>>>(beta.get(), dphi.get(), b, static_cast<int>(nao), acc.get());
         ISDF_LAUNCH_CHECK();
     }
-    if (!want_grad) {
-        ISDF_CUDA(cudaMemcpyAsync(&r.energy, energy.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
-        ISDF_CUDA(cudaStreamSynchronize(s));
-        return r;
-    }
+    // [E, v (k), per-atom grid terms (natm x 3), B (k x nao), acc (3 x nao)]
+    double* o = out.data();
+    ISDF_CUDA(cudaMemcpyAsync(o, energy.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(o + 1, v.get(), k * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(o + 1 + k, gacc.get(), 3 * c.natm * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(o + 1 + k + 3 * c.natm, B.get(), k * nao * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaMemcpyAsync(o + 1 + k + 3 * c.natm + k * nao, acc.get(), 3 * nao * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    return out;
+}
+
+AdjointResult energy_gradient_finish(const Context& c, const AnchorFactor& f, const double* dm,
+                                     const double* sums, bool want_grad, cudaStream_t s) {
+    AdjointResult r;
+    const int64_t k = f.k, nao = c.nao;
+    r.grad.assign(static_cast<size_t>(c.natm) * 3, 0.0);
+    r.energy = sums[0];
+    if (k == 0 || !want_grad) return r;
+    AnchorSide as = anchor_side(c, f, dm, true, s);
+    DeviceBuffer<double> v(k, s), y(k, s), W(static_cast<size_t>(k * k), s), B(static_cast<size_t>(k * nao), s),
+        WPhi(static_cast<size_t>(k * nao), s), coef(static_cast<size_t>(k * nao), s),
+        acc(static_cast<size_t>(3 * nao), s);
+    const double* hB = sums + 1 + k + 3 * c.natm;
+    ISDF_CUDA(cudaMemcpyAsync(v.get(), sums + 1, k * sizeof(double), cudaMemcpyHostToDevice, s));
+    ISDF_CUDA(cudaMemcpyAsync(B.get(), hB, k * nao * sizeof(double), cudaMemcpyHostToDevice, s));
+    ISDF_CUDA(cudaMemcpyAsync(acc.get(), hB + k * nao, 3 * nao * sizeof(double), cudaMemcpyHostToDevice, s));
     // anchor terms
-    anchor_terms_kernel<<<1, 256, 0, s>>>(static_cast<int>(k), static_cast<int>(nao), f.phi_a.get(), S.get(),
-                                          f.T.get(), PhiD.get(), z.get(), v.get(), y.get(), W.get());
+    anchor_terms_kernel<<<1, 256, 0, s>>>(static_cast<int>(k), static_cast<int>(nao), f.phi_a.get(), as.S.get(),
+                                          f.T.get(), as.PhiD.get(), as.z.get(), v.get(), y.get(), W.get());
     ISDF_LAUNCH_CHECK();
     gemm_f64(k, nao, k, W.get(), k, 0, f.phi_a.get(), nao, 0, WPhi.get(), nao, 0, 1, false, s);
     anchor_coef_kernel<<<nblk(k * nao), 256, 0, s>>>(static_cast<int>(k), static_cast<int>(nao), B.get(),
-                                                     PhiD.get(), WPhi.get(), y.get(), coef.get());
+                                                     as.PhiD.get(), WPhi.get(), y.get(), coef.get());
     ISDF_LAUNCH_CHECK();
     dim3 cg(static_cast<unsigned>((nao + 255) / 256), 3);
     anchor_contrib_kernel<<<cg, 256, 0, s>>>(static_cast<int>(k), static_cast<int>(nao), coef.get(),
-                                             dphia.get(), acc.get());
+                                             as.dphia.get(), acc.get());
     ISDF_LAUNCH_CHECK();
-    std::vector<double> hacc(3 * nao), hg(3 * c.natm);
+    std::vector<double> hacc(3 * nao);
     ISDF_CUDA(cudaMemcpyAsync(hacc.data(), acc.get(), hacc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-    ISDF_CUDA(cudaMemcpyAsync(hg.data(), gacc.get(), hg.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-    ISDF_CUDA(cudaMemcpyAsync(&r.energy, energy.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
     ISDF_CUDA(cudaStreamSynchronize(s));
     // d phi / d R_A = -grad_r phi for AOs on atom A
     for (int64_t mu = 0; mu < nao; ++mu) {
         const int a = c.ao_atom[mu];
         for (int cc = 0; cc < 3; ++cc) r.grad[a * 3 + cc] -= hacc[cc * nao + mu];
     }
+    const double* hg = sums + 1 + k;
     for (int i = 0; i < 3 * c.natm; ++i) r.grad[i] -= hg[i];   // fused grid pass (per atom)
     return r;
+}
+
+AdjointResult energy_gradient(const Context& c, const double* pts, const double* w, const KeptPoints& kp,
+                              const AnchorFactor& f, const double* dm, bool want_grad, cudaStream_t s) {
+    const std::vector<double> part = energy_gradient_partial(c, pts, w, kp, f, dm, want_grad, s);
+    return energy_gradient_finish(c, f, dm, part.data(), want_grad, s);
 }
 
 }  // namespace isdf

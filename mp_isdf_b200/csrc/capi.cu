@@ -649,6 +649,59 @@ int isdf_energy_gradient(isdf_ctx* ctx, const double* xyz, const double* w, int6
     });
 }
 
+namespace {
+// Anchors given by coordinates and weights (host), factored on the device.
+isdf::AnchorFactor factor_anchor_coords(isdf::Context& c, const double* axyz, const double* aw, int64_t k,
+                                        cudaStream_t s) {
+    if (k <= 0 || !axyz || !aw) isdf::fail(isdf::kInvalid, "anchor coordinates and weights are required");
+    for (int64_t i = 0; i < 3 * k; ++i)
+        if (!std::isfinite(axyz[i])) isdf::fail(isdf::kInvalid, "anchor coordinates must be finite");
+    isdf::DeviceBuffer<double> apts(static_cast<size_t>(3 * k), s), dw(k, s);
+    ISDF_CUDA(cudaMemcpyAsync(apts.get(), axyz, 3 * k * sizeof(double), cudaMemcpyHostToDevice, s));
+    ISDF_CUDA(cudaMemcpyAsync(dw.get(), aw, k * sizeof(double), cudaMemcpyHostToDevice, s));
+    ISDF_PROFILE("phase:factor_anchors", s);
+    isdf::AnchorFactor f = isdf::factor_anchors(c, apts.get(), dw.get(), k, s);
+    ISDF_CUDA(cudaStreamSynchronize(s));   // the host arrays may go out of scope
+    return f;
+}
+}  // namespace
+
+int isdf_adjoint_partial_size(isdf_ctx* ctx, int64_t k, int64_t* size) {
+    return guarded([&] {
+        if (k < 0 || !size) isdf::fail(isdf::kInvalid, "invalid adjoint partial size arguments");
+        *size = static_cast<int64_t>(isdf::adjoint_partial_size(ctx_of(ctx), k));
+    });
+}
+
+int isdf_energy_gradient_shard(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng,
+                               const double* anchor_xyz, const double* anchor_w, int64_t k, const double* dm,
+                               int32_t want_grad, double* partial, void* stream) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        cudaStream_t s = as_stream(stream);
+        if (ng < 0 || k <= 0 || !dm || !partial) isdf::fail(isdf::kInvalid, "invalid adjoint arguments");
+        isdf::AnchorFactor f = factor_anchor_coords(c, anchor_xyz, anchor_w, k, s);
+        isdf::KeptPoints kp = isdf::compact_points(xyz, w, ng, s);
+        const std::vector<double> part = isdf::energy_gradient_partial(c, xyz, w, kp, f, dm, want_grad != 0, s);
+        std::memcpy(partial, part.data(), part.size() * sizeof(double));
+    });
+}
+
+int isdf_energy_gradient_finish(isdf_ctx* ctx, const double* anchor_xyz, const double* anchor_w, int64_t k,
+                                const double* dm, const double* sums, double* energy, double* grad, void* stream) {
+    return guarded([&] {
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        cudaStream_t s = as_stream(stream);
+        if (k <= 0 || !dm || !sums) isdf::fail(isdf::kInvalid, "invalid adjoint arguments");
+        isdf::AnchorFactor f = factor_anchor_coords(c, anchor_xyz, anchor_w, k, s);
+        isdf::AdjointResult r = isdf::energy_gradient_finish(c, f, dm, sums, grad != nullptr, s);
+        if (energy) *energy = r.energy;
+        if (grad) std::memcpy(grad, r.grad.data(), r.grad.size() * sizeof(double));
+    });
+}
+
 int isdf_ctx_set_coords(isdf_ctx* ctx, const double* coords) {
     return guarded([&] {
         auto& c = ctx_of(ctx);

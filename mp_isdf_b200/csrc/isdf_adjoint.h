@@ -17,6 +17,18 @@ AdjointResult energy_gradient(const Context& c, const double* pts, const double*
                               const KeptPoints& kp, const AnchorFactor& f, const double* dm_host,
                               bool want_grad, cudaStream_t s);
 
+// The same in two steps, for grid shards: the sums over one set of kept
+// points, [E, v (k), per-atom grid terms (natm x 3), B = alpha^T Phi_g
+// (k x nao), per-AO grid terms (3 x nao)] (adjoint_partial_size doubles;
+// what the fused grid pass folds per atom leaves B and the per-AO terms
+// zero), and the energy and gradient from the sums over all shards.
+size_t adjoint_partial_size(const Context& c, int64_t k);
+std::vector<double> energy_gradient_partial(const Context& c, const double* pts, const double* w,
+                                            const KeptPoints& kp, const AnchorFactor& f, const double* dm_host,
+                                            bool want_grad, cudaStream_t s);
+AdjointResult energy_gradient_finish(const Context& c, const AnchorFactor& f, const double* dm_host,
+                                     const double* sums_host, bool want_grad, cudaStream_t s);
+
 // Moves the atoms (and their shells) to new coordinates (natm x 3, bohr).
 void set_atom_coords(Context& c, const double* coords_host);
 

@@ -27,6 +27,10 @@ contiguous shard of the grid, in grid order, and runs::
     4. the fit on its shard with the anchors' coordinates
        all-reduce(sum) of the pair-error sums
 
+``energy_gradient_sharded`` runs the nuclear-gradient adjoint the same way:
+per-rank partial sums, one all-reduce(sum), the anchor-side algebra on every
+rank.
+
 The AO evaluation, the projections and the QR updates are split over the
 ranks; per pivot step the ranks exchange O(ell + ranks) doubles, so the
 exchange is latency-bound (2-3 small collectives per step, ell steps).
@@ -243,6 +247,19 @@ def select_fit_sharded(backend, comm, xyz, w, grid_offset, ng_total, want_error=
                          select_info=sinfo, fit_info=finfo, counts=counts)
 
 
+def energy_gradient_sharded(backend, comm, xyz, w, anchor_xyz, anchor_w, dm, want_grad=True):
+    """The adjoint (E = sum_g w_g rho_ISDF(g)^2 and dE/dR) over grid shards:
+    every rank sums over its own points (``backend.adjoint_partial``: E, v,
+    the per-atom grid terms and the anchor-coefficient sums), one
+    all-reduce(sum) adds the partials, and every rank finishes the same
+    anchor-side algebra (``backend.adjoint_finish``).  Anchors are given by
+    coordinates (k x 3) and weights, as from select_fit_sharded.  Returns
+    (E, dE/dR[natm, 3]), the same on every rank."""
+    part = backend.adjoint_partial(xyz, w, anchor_xyz, anchor_w, dm, want_grad)
+    tot = backend.to_numpy(comm.allreduce_sum(backend.tensor(np.asarray(part, np.float64))))
+    return backend.adjoint_finish(anchor_xyz, anchor_w, dm, tot, want_grad)
+
+
 def _pad(t, n):
     out = t.new_zeros((n,) + tuple(t.shape[1:]))
     out[:t.shape[0]] = t
@@ -304,6 +321,12 @@ class CudaBackend:
 
     def sketch_rank(self, n_total, diag, energy, **kw_sel):
         return self.ctx.sketch_rank(n_total, diag, energy, **kw_sel)
+
+    def adjoint_partial(self, xyz, w, a_xyz, a_w, dm, want_grad):
+        return self.ctx.energy_gradient_shard(xyz, w, a_xyz, a_w, dm, want_grad)
+
+    def adjoint_finish(self, a_xyz, a_w, dm, sums, want_grad):
+        return self.ctx.energy_gradient_finish(a_xyz, a_w, dm, sums, want_grad)
 
     def fit_at(self, xyz, w, a_xyz, a_w, precision, want_error):
         import torch

@@ -133,6 +133,14 @@ class OracleBackend:
                                                  d * (d + 1) // 2)
         return rank, nrank, float(tails[rank] / tails[0]) if tails[0] else 0.0
 
+    def adjoint_partial(self, xyz, w, a_xyz, a_w, dm, want_grad):
+        return oracle_adjoint_partial(self.oc, self.to_numpy(xyz).reshape(-1, 3), self.to_numpy(w),
+                                      np.asarray(a_xyz).reshape(-1, 3), np.asarray(dm), want_grad)
+
+    def adjoint_finish(self, a_xyz, a_w, dm, sums, want_grad):
+        return oracle_adjoint_finish(self.oc, np.asarray(a_xyz).reshape(-1, 3), np.asarray(dm), np.asarray(sums),
+                                     want_grad)
+
     def fit_at(self, xyz, w, a_xyz, a_w, precision, want_error):
         xyz, w = self.to_numpy(xyz).reshape(-1, 3), self.to_numpy(w)
         keep = w != 0
@@ -140,6 +148,59 @@ class OracleBackend:
             return torch.zeros((len(a_w), 0), dtype=torch.float64), None, np.zeros(2)
         theta, err = O.gram_fit(self.oc, xyz[keep], w[keep], a_xyz, a_w)
         return torch.as_tensor(theta), None, np.array([err["err2"], err["exact2"]])
+
+
+def _anchor_side(oc, a_xyz, dm):
+    phi_a = oc.eval_ao(a_xyz)
+    S = phi_a @ phi_a.T
+    M = S * S
+    rho_a = np.einsum("ki,ij,kj->k", phi_a, dm, phi_a)
+    return phi_a, S, M, np.linalg.solve(M, rho_a)
+
+
+def oracle_adjoint_partial(oc, xyz, w, a_xyz, dm, want_grad):
+    """One shard's sums of the oracle adjoint (oracle.isdf_energy_gradient split
+    at its grid loop): [E, v, per-atom grid terms, alpha^T Phi_g, zeros(3 nao)]."""
+    keep = w != 0
+    xyz, w = xyz[keep], w[keep]
+    phi_a, S, M, z = _anchor_side(oc, a_xyz, dm)
+    k, nao = phi_a.shape
+    E, v, gacc, B = 0.0, np.zeros(k), np.zeros((oc.natm, 3)), np.zeros((k, nao))
+    if len(w):
+        phi = oc.eval_ao(xyz)
+        G = phi @ phi_a.T
+        h = G * G
+        rho = h @ z
+        E = float(np.sum(w * rho * rho))
+        u = 2 * w * rho
+        v = u @ h
+        if want_grad:
+            dphi = oc.eval_ao_gradient(xyz)
+            alpha = 2 * u[:, None] * z[None, :] * G
+            B = alpha.T @ phi
+            contrib = np.einsum("gm,cgm->cm", alpha @ phi_a, dphi)
+            for c in range(3):
+                np.add.at(gacc[:, c], oc.ao_atom, contrib[c])
+    return np.concatenate([[E], v, gacc.ravel(), B.ravel(), np.zeros(3 * nao)])
+
+
+def oracle_adjoint_finish(oc, a_xyz, dm, sums, want_grad):
+    phi_a, S, M, z = _anchor_side(oc, a_xyz, dm)
+    k, nao = phi_a.shape
+    grad = np.zeros((oc.natm, 3))
+    if not want_grad:
+        return float(sums[0]), grad
+    v = sums[1:1 + k]
+    gacc = sums[1 + k:1 + k + 3 * oc.natm].reshape(oc.natm, 3)
+    B = sums[1 + k + 3 * oc.natm:1 + k + 3 * oc.natm + k * nao].reshape(k, nao)
+    y = np.linalg.solve(M, v)
+    coef = B + 2 * y[:, None] * (phi_a @ dm)
+    W = 2 * S * (y[:, None] * z[None, :])
+    coef -= (W + W.T) @ phi_a
+    contrib = np.einsum("km,ckm->cm", coef, oc.eval_ao_gradient(a_xyz))
+    for c in range(3):
+        np.add.at(grad[:, c], oc.ao_atom, -contrib[c])
+    return float(sums[0]), grad - gacc
 
 
 class ThreadComm:

@@ -167,3 +167,107 @@ def test_cuda_single_rank_local_comm():
     res = select_fit_sharded(CudaBackend(ctx), LocalComm(), x, wt, 0, len(pts), precision="mixed", **KW)
     piv, _ = ctx.select(x, wt, precision="mixed", **KW)
     np.testing.assert_array_equal(res.anchors, piv)
+
+
+# ---- the adjoint over grid shards -------------------------------------------------
+ADJ_ANCHORS = [3, 40, 77, 120, 161, 205]   # kept-point positions used as anchors
+
+
+def _adjoint_inputs():
+    mol, pts, w = _system()
+    keep = np.flatnonzero(w != 0)
+    anchors = keep[ADJ_ANCHORS]
+    c = np.random.default_rng(8).normal(size=(mol.nao, 4))
+    dm = 0.05 * (c @ c.T)
+    return mol, pts, w, anchors, dm
+
+
+def _gloo_adjoint_rank(rank, size, port, out_dir, empty_rank):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from mp_isdf_b200.sharded import TorchComm, energy_gradient_sharded
+    from sharded_helpers import OracleBackend
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=size,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        mol, pts, w, anchors, dm = _adjoint_inputs()
+        bounds = _split(len(pts), size - (empty_rank >= 0))
+        if empty_rank >= 0:
+            bounds.insert(empty_rank, (0, 0))
+        lo, hi = bounds[rank]
+        e, g = energy_gradient_sharded(OracleBackend(mol), TorchComm(), torch.as_tensor(pts[lo:hi]),
+                                       torch.as_tensor(w[lo:hi]), pts[anchors], w[anchors], dm)
+        np.save(os.path.join(out_dir, f"grad{rank}.npy"), np.concatenate([[e], g.ravel()]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("size,empty_rank", [(2, -1), (3, 0)])
+def test_gloo_adjoint_matches_oracle(size, empty_rank):
+    """The sharded adjoint (per-rank partial sums, one all-reduce, the same
+    anchor-side finish on every rank) on gloo CPU ranks with the oracle backend
+    gives the single-process oracle's energy and nuclear gradient, also with a
+    rank that holds no grid point."""
+    import torch.multiprocessing as mp
+    from oracle import oracle as O
+    mol, pts, w, anchors, dm = _adjoint_inputs()
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_gloo_adjoint_rank, args=(size, _free_port(), d, empty_rank), nprocs=size, join=True,
+                           start_method="spawn")
+        out = [np.load(os.path.join(d, f"grad{r}.npy")) for r in range(size)]
+    for r in range(1, size):
+        np.testing.assert_array_equal(out[r], out[0])
+    oc = O.OracleContext(mol.atm, mol.bas, mol.env)
+    keep = w != 0
+    e_ref = O.isdf_energy(oc, pts[keep], w[keep], pts[anchors], w[anchors], dm)
+    g_ref = O.isdf_energy_gradient(oc, pts[keep], w[keep], pts[anchors], w[anchors], dm)
+    np.testing.assert_allclose(out[0][0], e_ref, rtol=1e-11)
+    np.testing.assert_allclose(out[0][1:].reshape(-1, 3), g_ref, rtol=0, atol=1e-10 * np.abs(g_ref).max())
+
+
+@pytest.mark.gpu
+def test_cuda_adjoint_two_shards_match_single_call():
+    """The library's sharded adjoint entry points with two shards in one
+    process (threads standing in for ranks) against isdf_energy_gradient on
+    the whole grid, gradient and energy-only."""
+    import threading
+    import torch
+    from mp_isdf_b200 import capi
+    from mp_isdf_b200.sharded import CudaBackend, energy_gradient_sharded
+    from sharded_helpers import ThreadComm
+    mol, pts, w, anchors, dm = _adjoint_inputs()
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    x = torch.tensor(pts, device="cuda")
+    wt = torch.tensor(w, device="cuda")
+    e_ref, g_ref = ctx.energy_gradient(x, wt, anchors, dm)
+    size = 2
+    for want_grad in (True, False):
+        shared = ThreadComm.Shared(size)
+        results, errors = [None] * size, []
+
+        def run(rank):
+            try:
+                torch.cuda.set_device(0)
+                c = capi.Context(mol.atm, mol.bas, mol.env)
+                lo, hi = _split(len(pts), size)[rank]
+                results[rank] = energy_gradient_sharded(CudaBackend(c), ThreadComm(rank, size, shared),
+                                                        x[lo:hi].contiguous(), wt[lo:hi].contiguous(),
+                                                        pts[anchors], w[anchors], dm, want_grad)
+                torch.cuda.synchronize()
+            except Exception as e:  # surfaced below
+                errors.append(e)
+                shared.barrier.abort()
+
+        threads = [threading.Thread(target=run, args=(r,)) for r in range(size)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        assert not errors, errors
+        for e, g in results:
+            np.testing.assert_allclose(e, e_ref, rtol=1e-12)
+            if want_grad:
+                np.testing.assert_allclose(g, g_ref, rtol=0, atol=1e-11 * np.abs(g_ref).max())
+            else:
+                assert not g.any()
