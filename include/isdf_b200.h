@@ -267,6 +267,33 @@ int isdf_qr_shard_pivot(isdf_qr_shard* h, int64_t j, const double* rows_host, in
                         int64_t moved_col, double* r_jj);
 int isdf_qr_shard_reverified(isdf_qr_shard* h, int64_t* count);
 void isdf_qr_shard_free(isdf_qr_shard* h);
+/* The pair-space QR of qrcp_dense / qrcp_online (cpp/src/anchor_select_qrcp.cpp:95-225,
+ * cpp/src/anchor_select_online_qr.cpp:176-375) over grid shards, one rank per
+ * GPU: a rank holds the features and residual estimates of its kept points,
+ * the explicit pair basis is replicated.  create: compaction and features of
+ * the shard (n_kept, d, the 5 per-component sums of squares for the
+ * multi-axis scales); init: global sums -> scales, estimates, positions from
+ * pos_offset (the global kept position of the shard's first kept point),
+ * out2 = (sum of K_gg, non-finite flag) to be summed over ranks.  Per pivot:
+ * argmax gives the shard's best (estimate, position, global kept index; -1
+ * when none); the owner exports the winner's row (d features, sqrt|w|, grid
+ * index, x, y, z, w: d + 6 doubles), every rank verifies it (exact CGS2 in a
+ * fixed reduction order: the same exact2 everywhere) and accepts it; scan
+ * recomputes the shard's uncertain columns exactly before a stop.  Driven by
+ * mp_isdf_b200.sharded.select_pair_qr_sharded; same anchors as isdf_select. */
+typedef struct isdf_pairqr_shard isdf_pairqr_shard;
+int isdf_pairqr_shard_create(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz_dev,
+                             const double* w_dev, int64_t ng, int64_t grid_offset, isdf_pairqr_shard** out,
+                             int64_t* n_kept, int64_t* features, double* sumsq_host, void* stream);
+int isdf_pairqr_shard_init(isdf_pairqr_shard* h, const double* sumsq_global, int64_t pos_offset, double* out2);
+int isdf_pairqr_shard_argmax(isdf_pairqr_shard* h, double* key3);
+int isdf_pairqr_shard_row(isdf_pairqr_shard* h, int64_t col, double* row_host);
+int isdf_pairqr_shard_verify(isdf_pairqr_shard* h, const double* row_host, int64_t j, int64_t col,
+                             double* exact2);
+int isdf_pairqr_shard_accept(isdf_pairqr_shard* h, const double* row_host, int64_t j, int64_t col, double exact2,
+                             int64_t winner_pos, int32_t dense);
+int isdf_pairqr_shard_scan(isdf_pairqr_shard* h, int64_t j, double thr2, int64_t* count);
+void isdf_pairqr_shard_free(isdf_pairqr_shard* h);
 int isdf_sketch_rank(isdf_ctx* ctx, const isdf_select_args* args, int64_t n_total, const double* diag_host,
                      const double* energy_host, int64_t steps, int64_t* rank, int64_t* numerical_rank,
                      double* relative_tail);

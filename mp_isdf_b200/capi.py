@@ -34,6 +34,8 @@ SYMBOLS = [
     "isdf_rbrp_result_copy", "isdf_rbrp_result_free",
     "isdf_sketch_shard_project", "isdf_sketch_shard_combine", "isdf_sketch_shard_free",
     "isdf_sketch_select_gathered", "isdf_fit_at", "isdf_jk", "isdf_jk_host",
+    "isdf_pairqr_shard_create", "isdf_pairqr_shard_init", "isdf_pairqr_shard_argmax", "isdf_pairqr_shard_row",
+    "isdf_pairqr_shard_verify", "isdf_pairqr_shard_accept", "isdf_pairqr_shard_scan", "isdf_pairqr_shard_free",
     "isdf_qr_shard_create", "isdf_qr_shard_update", "isdf_qr_shard_verify", "isdf_qr_shard_column",
     "isdf_qr_shard_pivot", "isdf_qr_shard_reverified", "isdf_qr_shard_free", "isdf_sketch_rank",
 ]
@@ -137,6 +139,16 @@ def lib():
         L.isdf_qr_shard_pivot.argtypes = [P, I64, P, I64, I64, I64, ctypes.POINTER(F64)]
         L.isdf_qr_shard_reverified.argtypes = [P, ctypes.POINTER(I64)]
         L.isdf_qr_shard_free.argtypes = [P]
+        L.isdf_pairqr_shard_create.argtypes = [P, ctypes.POINTER(SelectArgs), P, P, I64, I64, ctypes.POINTER(P),
+                                               ctypes.POINTER(I64), ctypes.POINTER(I64), P, P]
+        L.isdf_pairqr_shard_init.argtypes = [P, P, I64, P]
+        L.isdf_pairqr_shard_argmax.argtypes = [P, P]
+        L.isdf_pairqr_shard_row.argtypes = [P, I64, P]
+        L.isdf_pairqr_shard_verify.argtypes = [P, P, I64, I64, ctypes.POINTER(F64)]
+        L.isdf_pairqr_shard_accept.argtypes = [P, P, I64, I64, F64, I64, I32]
+        L.isdf_pairqr_shard_scan.argtypes = [P, I64, F64, ctypes.POINTER(I64)]
+        L.isdf_pairqr_shard_free.argtypes = [P]
+        L.isdf_pairqr_shard_free.restype = None
         L.isdf_qr_shard_free.restype = None
         L.isdf_sketch_rank.argtypes = [P, ctypes.POINTER(SelectArgs), I64, P, P, I64, ctypes.POINTER(I64),
                                        ctypes.POINTER(I64), ctypes.POINTER(F64)]
@@ -313,6 +325,18 @@ class Context:
                                                 ctypes.byref(npiv), ctypes.byref(info), _stream(yt)))
         del keep
         return piv[:npiv.value].copy(), info
+
+    def pairqr_shard(self, xyz, w, grid_offset, **kw):
+        """This rank's share of the sharded pair-space QR (qrcp_dense /
+        qrcp_online) over its grid shard (device tensors)."""
+        args, keep = make_select_args(**kw)
+        h, n, d = P(), I64(), I64()
+        sumsq = np.zeros(5)
+        check(lib().isdf_pairqr_shard_create(self.h, ctypes.byref(args), _ptr(xyz), _ptr(w), xyz.shape[0],
+                                             int(grid_offset), ctypes.byref(h), ctypes.byref(n), ctypes.byref(d),
+                                             _ptr(sumsq), _stream(xyz)))
+        del keep
+        return PairQrShard(h.value, n.value, d.value, sumsq, (xyz, w))
 
     def qr_shard(self, yt, n_total, pos_offset, kept_xyz, kept_w, delta, scales, **kw):
         """This rank's share of the distributed sketch QR over its columns yt
@@ -503,6 +527,54 @@ class Context:
                                   1 if precision == "mixed" else 0, int(want_error), _ptr(theta),
                                   ctypes.byref(info)))
         return theta[:len(a) * info.n_kept].reshape(len(a), info.n_kept), info
+
+
+class PairQrShard:
+    """One rank's share of the sharded pair-space QR (isdf_pairqr_shard_*)."""
+
+    def __init__(self, h, n_kept, d, sumsq, keep):
+        self.h, self.n_kept, self.d, self.sumsq = h, n_kept, d, sumsq
+        self._keep = keep   # the device arrays the handle points at
+
+    def init(self, sumsq_global, pos_offset):
+        out = np.zeros(2)
+        check(lib().isdf_pairqr_shard_init(self.h, _ptr(_np(sumsq_global, np.float64)), int(pos_offset), _ptr(out)))
+        return out
+
+    def argmax(self):
+        key = np.zeros(3)
+        check(lib().isdf_pairqr_shard_argmax(self.h, _ptr(key)))
+        return key
+
+    def row(self, col):
+        out = np.zeros(self.d + 6)
+        check(lib().isdf_pairqr_shard_row(self.h, int(col), _ptr(out)))
+        return out
+
+    def verify(self, row, j, col):
+        e = F64()
+        check(lib().isdf_pairqr_shard_verify(self.h, _ptr(_np(row, np.float64)), int(j), int(col), ctypes.byref(e)))
+        return e.value
+
+    def accept(self, row, j, col, exact2, winner_pos, dense):
+        check(lib().isdf_pairqr_shard_accept(self.h, _ptr(_np(row, np.float64)), int(j), int(col), float(exact2),
+                                             int(winner_pos), 1 if dense else 0))
+
+    def scan(self, j, thr2):
+        n = I64()
+        check(lib().isdf_pairqr_shard_scan(self.h, int(j), float(thr2), ctypes.byref(n)))
+        return n.value
+
+    def free(self):
+        if self.h:
+            lib().isdf_pairqr_shard_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 class QrShard:

@@ -1162,4 +1162,88 @@ int isdf_fit_at(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, c
     });
 }
 
+struct isdf_pairqr_shard {
+    isdf_ctx* ctx = nullptr;
+    std::unique_ptr<isdf::PairQrShard> sh;
+};
+
+int isdf_pairqr_shard_create(isdf_ctx* ctx, const isdf_select_args* args, const double* xyz, const double* w,
+                             int64_t ng, int64_t grid_offset, isdf_pairqr_shard** out, int64_t* n_kept,
+                             int64_t* features, double* sumsq_host, void* stream) {
+    return guarded([&] {
+        if (!out) isdf::fail(isdf::kInvalid, "null shard handle");
+        *out = nullptr;
+        if (!args) isdf::fail(isdf::kInvalid, "selection arguments are required");
+        auto& c = ctx_of(ctx);
+        DeviceGuard dg(c.device);
+        isdf::SelectOptions o = options_of(args);
+        if (o.algorithm != ISDF_QRCP_DENSE && o.algorithm != ISDF_QRCP_ONLINE)
+            isdf::fail(isdf::kInvalid, "the sharded pair QR takes qrcp_dense or qrcp_online");
+        if (ng < 0 || grid_offset < 0) isdf::fail(isdf::kInvalid, "invalid shard size or offset");
+        auto h = std::make_unique<isdf_pairqr_shard>();
+        h->ctx = ctx;
+        h->sh = std::make_unique<isdf::PairQrShard>(c, o, xyz, w, ng, grid_offset, as_stream(stream));
+        if (n_kept) *n_kept = h->sh->n_kept();
+        if (features) *features = h->sh->features();
+        if (sumsq_host) h->sh->local_sumsq(sumsq_host);
+        *out = h.release();
+    });
+}
+
+int isdf_pairqr_shard_init(isdf_pairqr_shard* h, const double* sumsq_global, int64_t pos_offset, double* out2) {
+    return guarded([&] {
+        if (!h || !sumsq_global || !out2 || pos_offset < 0) isdf::fail(isdf::kInvalid, "invalid shard init arguments");
+        DeviceGuard dg(ctx_of(h->ctx).device);
+        h->sh->init(sumsq_global, pos_offset, out2);
+    });
+}
+
+int isdf_pairqr_shard_argmax(isdf_pairqr_shard* h, double* key3) {
+    return guarded([&] {
+        if (!h || !key3) isdf::fail(isdf::kInvalid, "invalid shard argmax arguments");
+        DeviceGuard dg(ctx_of(h->ctx).device);
+        h->sh->argmax(key3);
+    });
+}
+
+int isdf_pairqr_shard_row(isdf_pairqr_shard* h, int64_t col, double* row_host) {
+    return guarded([&] {
+        if (!h || !row_host) isdf::fail(isdf::kInvalid, "invalid shard row arguments");
+        DeviceGuard dg(ctx_of(h->ctx).device);
+        h->sh->row(col, row_host);
+    });
+}
+
+int isdf_pairqr_shard_verify(isdf_pairqr_shard* h, const double* row_host, int64_t j, int64_t col, double* exact2) {
+    return guarded([&] {
+        if (!h || !row_host || !exact2 || j < 0) isdf::fail(isdf::kInvalid, "invalid shard verify arguments");
+        DeviceGuard dg(ctx_of(h->ctx).device);
+        *exact2 = h->sh->verify(row_host, static_cast<int>(j), col);
+    });
+}
+
+int isdf_pairqr_shard_accept(isdf_pairqr_shard* h, const double* row_host, int64_t j, int64_t col, double exact2,
+                             int64_t winner_pos, int32_t dense) {
+    return guarded([&] {
+        if (!h || !row_host || j < 0 || !(exact2 > 0)) isdf::fail(isdf::kInvalid, "invalid shard accept arguments");
+        DeviceGuard dg(ctx_of(h->ctx).device);
+        h->sh->accept(row_host, static_cast<int>(j), col, exact2, winner_pos, dense != 0);
+    });
+}
+
+int isdf_pairqr_shard_scan(isdf_pairqr_shard* h, int64_t j, double thr2, int64_t* count) {
+    return guarded([&] {
+        if (!h || j < 0) isdf::fail(isdf::kInvalid, "invalid shard scan arguments");
+        DeviceGuard dg(ctx_of(h->ctx).device);
+        const int64_t c = h->sh->scan(static_cast<int>(j), thr2);
+        if (count) *count = c;
+    });
+}
+
+void isdf_pairqr_shard_free(isdf_pairqr_shard* h) {
+    if (!h) return;
+    DeviceGuard dg(ctx_of(h->ctx).device);
+    delete h;
+}
+
 }  // extern "C"

@@ -256,6 +256,42 @@ std::unique_ptr<SketchQrShard> make_sketch_qr_shard(const Context& c, const Sele
 
 // qrcp_dense / qrcp_online: greedy max-residual pivoting of the weighted
 // pair columns sqrt|w_g| f_g (x) f_g, computed without materialising them.
+// One rank's share of the pair-space QR (qrcp_dense / qrcp_online) over a grid
+// shard: its kept points' features, residual estimates and L rows, with the
+// explicit pair basis Q replicated.  Every rank makes the same calls in the
+// same order; verify() and accept() give bit-identical results on every rank
+// (fixed-order reductions), so the ranks' bases stay equal.
+class PairQrShard {
+public:
+    // pos_offset: the global kept position of this shard's first kept point;
+    // grid_offset: the global grid index of its first grid point
+    PairQrShard(const Context& c, const SelectOptions& o, const double* pts, const double* w, int64_t ng,
+                int64_t grid_offset, cudaStream_t s);
+    ~PairQrShard();
+    int64_t n_kept() const;
+    int64_t features() const;   // d
+    void local_sumsq(double out[5]) const;
+    // the global multi-axis sums and position offset -> local (sum K_gg, non-finite flag)
+    void init(const double* sumsq_global, int64_t pos_offset, double out[2]);
+    // best unselected local column: (estimate, global position, global kept index; -1 when none)
+    void argmax(double key[3]);
+    // row of global kept column gcol (local), kRowExtra + d doubles: its d
+    // features, sqrt|w|, global grid index, x, y, z, w
+    static constexpr int kRowExtra = 6;
+    void row(int64_t gcol, double* out) const;
+    // exact squared residual of the row's pair vector against the j basis vectors
+    // (also the owner's estimate of it)
+    double verify(const double* row_host, int j, int64_t gcol);
+    // take the verified column as pivot j (the coefficients of its last verify)
+    void accept(const double* row_host, int j, int64_t gcol, double exact2, int64_t winner_pos, bool dense);
+    // exact recomputation of every local column whose estimate could exceed thr2
+    int64_t scan(int j, double thr2);
+
+private:
+    struct Impl;
+    Impl* p_;
+};
+
 std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const double* w,
                                     int64_t ng, const SelectOptions& o, cudaStream_t s,
                                     PairQrDiagnostics* diag = nullptr);

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <limits>
 
 namespace isdf {
@@ -167,6 +168,88 @@ __global__ void gather_index_kernel(const int64_t* __restrict__ index, const int
                                     int64_t* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < k) out[i] = index[pos[i]];
+}
+
+// ---- fixed-order reductions (the sharded QR needs bit-identical results on
+// every rank): per-block partials, then one block per output in block order
+constexpr int kDetBlocks = 256;
+
+// part[r * kDetBlocks + b] = sum over block b's slice of Q[r, :] . x
+__global__ void __launch_bounds__(256) rows_dot_part_kernel(const double* __restrict__ Q, int rows, int64_t m,
+                                                            const double* __restrict__ x, double* __restrict__ part) {
+    __shared__ double sh[256 / 32];
+    const int64_t chunk = (m + gridDim.x - 1) / gridDim.x;
+    const int64_t k0 = blockIdx.x * chunk, k1 = min(m, k0 + chunk);
+    for (int r = 0; r < rows; ++r) {
+        double acc = 0;
+        const double* q = Q + static_cast<int64_t>(r) * m;
+        for (int64_t k = k0 + threadIdx.x; k < k1; k += 256) acc += q[k] * x[k];
+        acc = block_sum<256>(acc, sh);
+        if (threadIdx.x == 0) part[r * kDetBlocks + blockIdx.x] = acc;
+    }
+}
+
+// y = x - Q^T t (elementwise); part[b] = block b's sum of y^2
+__global__ void __launch_bounds__(256) rows_axpy_part_kernel(const double* __restrict__ Q, int rows, int64_t m,
+                                                             const double* __restrict__ t, const double* x, double* y,
+                                                             double* __restrict__ part) {
+    __shared__ double sh[256 / 32];
+    double acc = 0;
+    const int64_t chunk = (m + gridDim.x - 1) / gridDim.x;
+    const int64_t k0 = blockIdx.x * chunk, k1 = min(m, k0 + chunk);
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += 256) {
+        double v = x[k];
+        for (int r = 0; r < rows; ++r) v -= Q[static_cast<int64_t>(r) * m + k] * t[r];
+        y[k] = v;
+        acc += v * v;
+    }
+    acc = block_sum<256>(acc, sh);
+    if (threadIdx.x == 0 && part) part[blockIdx.x] = acc;
+}
+
+// out[r] = sum_b part[r * kDetBlocks + b], in block order per thread, then a fixed tree
+__global__ void __launch_bounds__(256) reduce_parts_kernel(const double* __restrict__ part, double* __restrict__ out) {
+    __shared__ double sh[256 / 32];
+    double v = 0;
+    for (int b = threadIdx.x; b < kDetBlocks; b += 256) v += part[blockIdx.x * kDetBlocks + b];
+    v = block_sum<256>(v, sh);
+    if (threadIdx.x == 0) out[blockIdx.x] = v;
+}
+
+// L[g, j] and the downdate, with the pivot's weight from a device scalar
+__global__ void update_residual_swp_kernel(const double* __restrict__ D, const double* __restrict__ sw,
+                                           const double* __restrict__ swp, int64_t n, double* __restrict__ L,
+                                           int64_t ldl, int j, const double* __restrict__ Rcol, double rjj,
+                                           double* __restrict__ est, const char* __restrict__ selected) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    double v = swp[0] * sw[g] * D[g] * D[g];
+    const double* lg = L + g * ldl;
+    for (int i = 0; i < j; ++i) v -= Rcol[i] * lg[i];
+    v /= rjj;
+    L[g * ldl + j] = v;
+    if (!selected[g]) est[g] = fmax(est[g] - v * v, 0.0);
+}
+
+// dgeqp3's swap over shards: the local column at position j takes the winner's
+// old position, the winner (if local) takes j
+__global__ void shard_swap_pos_kernel(int64_t* __restrict__ pos, int64_t n, int64_t j, int64_t winner_pos,
+                                      int64_t winner_local) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    if (g == winner_local) pos[g] = j;
+    else if (pos[g] == j) pos[g] = winner_pos;
+}
+
+__global__ void pos_iota_kernel(int64_t* __restrict__ pos, int64_t n, int64_t offset) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g < n) pos[g] = offset + g;
+}
+
+// row buffer of column p: its d features and sqrt|w_p|
+__global__ void export_row_kernel(const double* __restrict__ F, int64_t d, const double* __restrict__ sw, int64_t p,
+                                  double* __restrict__ row) {
+    for (int64_t k = threadIdx.x; k <= d; k += blockDim.x) row[k] = k < d ? F[p * d + k] : sw[p];
 }
 
 }  // namespace
@@ -466,6 +549,275 @@ std::vector<int64_t> select_pair_qr(const Context& c, const double* pts, const d
         }
         return out;
     }
+}
+
+// ---- the pair QR over grid shards -------------------------------------------------
+struct PairQrShard::Impl {
+    const Context& c;
+    cudaStream_t s;
+    SelectOptions o;
+    AxisSetup axs;
+    KeptPoints kp;
+    PairQr q;
+    const double* pts = nullptr;
+    const double* w = nullptr;
+    int64_t grid_offset = 0, pos_offset = 0;
+    double sumsq[5] = {0, 0, 0, 0, 0};
+    DeviceBuffer<double> rowbuf, part;
+    Impl(const Context& ctx, const SelectOptions& opt, cudaStream_t st) : c(ctx), s(st), o(opt), q(ctx, st) {}
+
+    void ensure(int64_t rows) {
+        q.grow(rows);
+        if (part.size() < static_cast<size_t>(kDetBlocks) * q.capL) part.reset(static_cast<size_t>(kDetBlocks) * q.capL, s);
+    }
+    // CGS2 of the pair vector of the row in rowbuf against the j basis vectors,
+    // in fixed reduction order: r, t0, t1 and scal = |r|^2
+    void exact_residual(int j) {
+        const int64_t m = q.m, d = q.d;
+        pair_vector_sw_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, s>>>(rowbuf.get(), d,
+                                                                                    rowbuf.get() + d, 0,
+                                                                                    q.cs.get(), q.a.get());
+        ISDF_LAUNCH_CHECK();
+        if (j == 0) {
+            rows_axpy_part_kernel<<<kDetBlocks, 256, 0, s>>>(q.Q.get(), 0, m, q.t0.get(), q.a.get(), q.r.get(),
+                                                             part.get());
+            ISDF_LAUNCH_CHECK();
+        } else {
+            rows_dot_part_kernel<<<kDetBlocks, 256, 0, s>>>(q.Q.get(), j, m, q.a.get(), part.get());
+            ISDF_LAUNCH_CHECK();
+            reduce_parts_kernel<<<j, 256, 0, s>>>(part.get(), q.t0.get());
+            ISDF_LAUNCH_CHECK();
+            rows_axpy_part_kernel<<<kDetBlocks, 256, 0, s>>>(q.Q.get(), j, m, q.t0.get(), q.a.get(), q.r.get(),
+                                                             nullptr);
+            ISDF_LAUNCH_CHECK();
+            rows_dot_part_kernel<<<kDetBlocks, 256, 0, s>>>(q.Q.get(), j, m, q.r.get(), part.get());
+            ISDF_LAUNCH_CHECK();
+            reduce_parts_kernel<<<j, 256, 0, s>>>(part.get(), q.t1.get());
+            ISDF_LAUNCH_CHECK();
+            rows_axpy_part_kernel<<<kDetBlocks, 256, 0, s>>>(q.Q.get(), j, m, q.t1.get(), q.r.get(), q.r.get(),
+                                                             part.get());
+            ISDF_LAUNCH_CHECK();
+        }
+        reduce_parts_kernel<<<1, 256, 0, s>>>(part.get(), q.scal.get());
+        ISDF_LAUNCH_CHECK();
+    }
+    int64_t local(int64_t gcol) const {
+        const int64_t l = gcol - pos_offset;
+        return (gcol >= 0 && l >= 0 && l < q.n) ? l : -1;
+    }
+    void upload_row(const double* row_host) {
+        ISDF_CUDA(cudaMemcpyAsync(rowbuf.get(), row_host, (q.d + 1) * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+};
+
+PairQrShard::PairQrShard(const Context& c, const SelectOptions& o, const double* pts, const double* w, int64_t ng,
+                         int64_t grid_offset, cudaStream_t s)
+    : p_(new Impl(c, o, s)) {
+    Impl& I = *p_;
+    const bool online = o.algorithm == 1;
+    if (!std::isfinite(o.tolerance) || o.tolerance < 0 || (online && o.batch_size <= 0))
+        fail(kInvalid, online ? "invalid online QR weights, tolerance or batch size"
+                              : "invalid weights, axis list, or tolerance");
+    validate_axis_weights(o.axis_weights.empty() ? nullptr : o.axis_weights.data(), static_cast<int>(o.axes.size()));
+    I.axs = make_axis_setup(c, o, s);
+    const int64_t d = I.axs.ax.d;
+    if (d > 46340) fail(kOverflow, online ? "AO pair dimension is too large" : "pair-product matrix is too large");
+    I.pts = pts;
+    I.w = w;
+    I.grid_offset = grid_offset;
+    I.kp = compact_points(pts, w, ng, s);
+    PairQr& q = I.q;
+    q.n = I.kp.n; q.d = d; q.m = d * d;
+    q.nblocks = static_cast<int>(std::max<int64_t>(1, (q.n + kNT - 1) / kNT));
+    q.F.reset(static_cast<size_t>(std::max<int64_t>(q.n, 1) * d), s);
+    DeviceBuffer<double> sq(5, s);
+    sq.zero(s);
+    if (q.n > 0)
+        eval_axis_features<double>(c, pts, I.kp.index.get(), q.n, I.axs.ax, q.F.get(), d,
+                                   I.axs.ax.naxes > 1 ? sq.get() : nullptr, nullptr, s);
+    ISDF_CUDA(cudaMemcpyAsync(I.sumsq, sq.get(), sizeof(I.sumsq), cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+}
+
+PairQrShard::~PairQrShard() { delete p_; }
+int64_t PairQrShard::n_kept() const { return p_->q.n; }
+int64_t PairQrShard::features() const { return p_->q.d; }
+void PairQrShard::local_sumsq(double out[5]) const { std::memcpy(out, p_->sumsq, sizeof(p_->sumsq)); }
+
+void PairQrShard::init(const double* sumsq_global, int64_t pos_offset, double out[2]) {
+    Impl& I = *p_;
+    PairQr& q = I.q;
+    cudaStream_t s = I.s;
+    const int64_t n = q.n, d = q.d;
+    I.pos_offset = pos_offset;
+    const AxisSpec& ax = I.axs.ax;
+    if (ax.naxes > 1) {
+        // every rank derives the same scales from the same global sums
+        auto sc = axis_scales_from_sumsq(ax, sumsq_global,
+                                         I.o.axis_weights.empty() ? nullptr : I.o.axis_weights.data(), true);
+        DeviceBuffer<double> dsc(sc.size(), s);
+        ISDF_CUDA(cudaMemcpyAsync(dsc.get(), sc.data(), sc.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        q.cs.reset(d, s);
+        q.xp.reset(d, s);
+        column_scales_kernel<<<static_cast<unsigned>((d + 255) / 256), 256, 0, s>>>(ax, dsc.get(), d, q.cs.get());
+        ISDF_LAUNCH_CHECK();
+        ISDF_CUDA(cudaStreamSynchronize(s));
+    }
+    const int64_t nn = std::max<int64_t>(n, 1);
+    q.sw.reset(nn, s); q.nf.reset(nn, s); q.est.reset(nn, s); q.kdiag.reset(nn, s); q.D.reset(nn, s);
+    q.selected.reset(nn, s); q.selected.zero(s);
+    q.pos.reset(nn, s);
+    q.partial.reset(q.nblocks, s);
+    q.best.reset(1, s);
+    q.a.reset(q.m, s); q.r.reset(q.m, s); q.scal.reset(1, s);
+    I.rowbuf.reset(d + 1, s);
+    I.ensure(8);
+    out[0] = 0.0;
+    out[1] = 0.0;
+    if (n > 0) {
+        const unsigned nb = static_cast<unsigned>((n + 255) / 256);
+        pos_iota_kernel<<<nb, 256, 0, s>>>(q.pos.get(), n, pos_offset);
+        ISDF_LAUNCH_CHECK();
+        gather_weights_kernel<<<nb, 256, 0, s>>>(I.w, I.kp.index.get(), n, q.sw.get());
+        ISDF_LAUNCH_CHECK();
+        if (q.cs.get()) {
+            scaled_row_norms_kernel<<<static_cast<unsigned>((n * 32 + 255) / 256), 256, 0, s>>>(q.F.get(), n, d,
+                                                                                              q.cs.get(), q.nf.get());
+            ISDF_LAUNCH_CHECK();
+        } else {
+            row_dot(q.F.get(), n, d, nullptr, q.nf.get(), s);
+        }
+        init_est_kernel<<<nb, 256, 0, s>>>(q.sw.get(), q.nf.get(), n, q.est.get(), q.kdiag.get());
+        ISDF_LAUNCH_CHECK();
+        DeviceBuffer<double> kpart(q.nblocks, s), ksum(1, s);
+        DeviceBuffer<int> kbad(1, s);
+        kbad.zero(s);
+        kdiag_partial_kernel<<<q.nblocks, 256, 0, s>>>(q.kdiag.get(), n, kpart.get(), kbad.get());
+        ISDF_LAUNCH_CHECK();
+        sum_partials_kernel<<<1, 256, 0, s>>>(kpart.get(), q.nblocks, ksum.get());
+        ISDF_LAUNCH_CHECK();
+        int hbad = 0;
+        ISDF_CUDA(cudaMemcpyAsync(&out[0], ksum.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaMemcpyAsync(&hbad, kbad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        ISDF_CUDA(cudaStreamSynchronize(s));
+        out[1] = hbad ? 1.0 : 0.0;
+    }
+}
+
+void PairQrShard::argmax(double key[3]) {
+    Impl& I = *p_;
+    PairQr& q = I.q;
+    key[0] = -1.0; key[1] = -1.0; key[2] = -1.0;
+    if (q.n == 0) return;
+    const ArgKey k = q.argmax(true);
+    if (k.col < 0) return;
+    key[0] = k.v;
+    key[1] = static_cast<double>(k.pos);
+    key[2] = static_cast<double>(I.pos_offset + k.col);
+}
+
+void PairQrShard::row(int64_t gcol, double* out) const {
+    const Impl& I = *p_;
+    const PairQr& q = I.q;
+    const int64_t l = I.local(gcol);
+    require(l >= 0, "the column is not on this shard");
+    DeviceBuffer<double> buf(q.d + 1, I.s);
+    export_row_kernel<<<1, 256, 0, I.s>>>(q.F.get(), q.d, q.sw.get(), l, buf.get());
+    ISDF_LAUNCH_CHECK();
+    int64_t gi = 0;
+    ISDF_CUDA(cudaMemcpyAsync(out, buf.get(), (q.d + 1) * sizeof(double), cudaMemcpyDeviceToHost, I.s));
+    ISDF_CUDA(cudaMemcpyAsync(&gi, I.kp.index.get() + l, sizeof(int64_t), cudaMemcpyDeviceToHost, I.s));
+    ISDF_CUDA(cudaStreamSynchronize(I.s));
+    double xyzw[4];
+    ISDF_CUDA(cudaMemcpyAsync(xyzw, I.pts + 3 * gi, 3 * sizeof(double), cudaMemcpyDeviceToHost, I.s));
+    ISDF_CUDA(cudaMemcpyAsync(xyzw + 3, I.w + gi, sizeof(double), cudaMemcpyDeviceToHost, I.s));
+    ISDF_CUDA(cudaStreamSynchronize(I.s));
+    out[q.d + 1] = static_cast<double>(I.grid_offset + gi);
+    for (int i = 0; i < 4; ++i) out[q.d + 2 + i] = xyzw[i];
+}
+
+double PairQrShard::verify(const double* row_host, int j, int64_t gcol) {
+    Impl& I = *p_;
+    PairQr& q = I.q;
+    I.ensure(j + 1);
+    I.upload_row(row_host);
+    I.exact_residual(j);
+    const int64_t l = I.local(gcol);
+    if (l >= 0) {
+        set_est_kernel<<<1, 1, 0, I.s>>>(q.est.get(), l, q.scal.get());
+        ISDF_LAUNCH_CHECK();
+    }
+    double exact2 = 0;
+    ISDF_CUDA(cudaMemcpyAsync(&exact2, q.scal.get(), sizeof(double), cudaMemcpyDeviceToHost, I.s));
+    ISDF_CUDA(cudaStreamSynchronize(I.s));
+    return exact2;
+}
+
+void PairQrShard::accept(const double* row_host, int j, int64_t gcol, double exact2, int64_t winner_pos, bool dense) {
+    Impl& I = *p_;
+    PairQr& q = I.q;
+    cudaStream_t s = I.s;
+    const int64_t n = q.n, d = q.d, m = q.m;
+    I.ensure(j + 1);
+    I.upload_row(row_host);   // the same row as the last verify (r, t0, t1 are its)
+    const double rj = std::sqrt(exact2);
+    rcol_kernel<<<1, 64, 0, s>>>(q.t0.get(), q.t1.get(), j, q.scal.get(), q.Rcol.get());
+    ISDF_LAUNCH_CHECK();
+    scale_copy(q.r.get(), 1.0 / rj, m, q.Q.get() + static_cast<int64_t>(j) * m, s);
+    const int64_t l = I.local(gcol);
+    if (l >= 0) {
+        mark_selected_kernel<<<1, 1, 0, s>>>(q.selected.get(), q.est.get(), l);
+        ISDF_LAUNCH_CHECK();
+    }
+    if (n > 0) {
+        const unsigned nb = static_cast<unsigned>((n + 255) / 256);
+        if (dense) {
+            shard_swap_pos_kernel<<<nb, 256, 0, s>>>(q.pos.get(), n, j, winner_pos, l);
+            ISDF_LAUNCH_CHECK();
+        }
+        const double* xrow = I.rowbuf.get();
+        if (q.cs.get()) {
+            scaled_pivot_row_kernel<<<static_cast<unsigned>((d + 255) / 256), 256, 0, s>>>(I.rowbuf.get(), q.cs.get(),
+                                                                                         d, q.xp.get());
+            ISDF_LAUNCH_CHECK();
+            xrow = q.xp.get();
+        }
+        row_dot(q.F.get(), n, d, xrow, q.D.get(), s);
+        update_residual_swp_kernel<<<nb, 256, 0, s>>>(q.D.get(), q.sw.get(), I.rowbuf.get() + d, n, q.L.get(), q.capL,
+                                                      j, q.Rcol.get(), rj, q.est.get(), q.selected.get());
+        ISDF_LAUNCH_CHECK();
+    }
+    ISDF_CUDA(cudaStreamSynchronize(s));   // the host row may go out of scope
+}
+
+int64_t PairQrShard::scan(int j, double thr2) {
+    Impl& I = *p_;
+    PairQr& q = I.q;
+    cudaStream_t s = I.s;
+    const int64_t n = q.n;
+    if (n == 0) return 0;
+    I.ensure(j + 1);
+    const double rel = 64.0 * std::numeric_limits<double>::epsilon() * static_cast<double>(j + 1);
+    DeviceBuffer<char> flags(n, s);
+    flag_uncertain_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(q.est.get(), q.kdiag.get(),
+                                                                                q.selected.get(), n, rel, thr2,
+                                                                                flags.get());
+    ISDF_LAUNCH_CHECK();
+    std::vector<char> h(n);
+    ISDF_CUDA(cudaMemcpyAsync(h.data(), flags.get(), n, cudaMemcpyDeviceToHost, s));
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    int64_t cnt = 0;
+    for (int64_t g = 0; g < n; ++g)
+        if (h[g]) {
+            export_row_kernel<<<1, 256, 0, s>>>(q.F.get(), q.d, q.sw.get(), g, I.rowbuf.get());
+            ISDF_LAUNCH_CHECK();
+            I.exact_residual(j);
+            set_est_kernel<<<1, 1, 0, s>>>(q.est.get(), g, q.scal.get());
+            ISDF_LAUNCH_CHECK();
+            ++cnt;
+        }
+    ISDF_CUDA(cudaStreamSynchronize(s));
+    return cnt;
 }
 
 }  // namespace isdf

@@ -165,6 +165,108 @@ def distributed_sketch_qr(backend, comm, qr, steps, verified, offsets, counts, r
     return pivots, np.array(diag), energy
 
 
+_EPS = np.finfo(np.float64).eps
+
+
+def _better(a, b):
+    """Key order of the pivot choice: larger value, then smaller position."""
+    if b is None or b[2] < 0:
+        return a[2] >= 0
+    if a[2] < 0:
+        return False
+    return a[0] > b[0] or (a[0] == b[0] and a[1] < b[1])
+
+
+def select_pair_qr_sharded(backend, comm, xyz, w, grid_offset, algorithm="qrcp_dense", tolerance=1e-10,
+                           max_rank=0, **kw):
+    """The pair-space QR of qrcp_dense / qrcp_online over grid shards
+    (``cpp/src/anchor_select_qrcp.cpp:95-225``, ``anchor_select_online_qr.cpp:176-375``;
+    the single-GPU form is ``select_pairqr.cu``).  Every rank holds its kept
+    points' features and residual estimates; the explicit pair basis is
+    replicated.  Per pivot: all-gather of one key per rank (estimate, position,
+    global kept index), the owner's row of the leader (d + 6 doubles) by
+    all-reduce(sum), its exact residual on every rank (the same value
+    everywhere) and, while the leader changes, again; the same stop rules and
+    stop-confirming scan as the single-GPU selection.  Returns (anchor grid
+    indices, anchor coordinates [k, 3], anchor weights [k], kept count)."""
+    online = algorithm in ("qrcp_online", 1)
+    dense = not online
+    sel = dict(kw, algorithm=algorithm, tolerance=tolerance, max_rank=max_rank)
+    st = backend.pq_begin(xyz, w, grid_offset, **sel)
+    counts = [int(backend.to_numpy(c)[0]) for c in comm.allgather(backend.tensor(np.array([st.n_kept], np.int64)))]
+    n_total = int(sum(counts))
+    pos_offset = int(sum(counts[:comm.rank]))
+    sums = backend.to_numpy(comm.allreduce_sum(backend.tensor(np.asarray(st.sumsq, np.float64))))
+    kd = backend.to_numpy(comm.allreduce_sum(backend.tensor(backend.pq_init(st, sums, pos_offset))))
+    if kd[1] != 0 or not np.isfinite(kd[0]):
+        raise OverflowError("non-finite online AO pair column" if online else "non-finite weighted pair product")
+    frob2 = float(kd[0])
+    d = st.d
+    m = d * d
+    cap = min(m, n_total, max_rank if max_rank else min(m, n_total))
+    floor = 32 * _EPS * np.sqrt(frob2) if online else 0.0
+    rows_width = d + 6
+    starts = [int(sum(counts[:r])) for r in range(len(counts))]
+
+    def global_argmax():
+        keys = [backend.to_numpy(k) for k in comm.allgather(backend.tensor(np.asarray(backend.pq_argmax(st),
+                                                                                      np.float64)))]
+        best = None
+        for k in keys:
+            if _better(k, best):
+                best = k
+        return best if best is not None and best[2] >= 0 else None
+
+    def fetch_row(key):
+        col = int(key[2])
+        own = starts[comm.rank] <= col < starts[comm.rank] + counts[comm.rank]
+        row = backend.pq_row(st, col) if own else np.zeros(rows_width)
+        return backend.to_numpy(comm.allreduce_sum(backend.tensor(np.asarray(row, np.float64))))
+
+    result, first, exact_mode = [], -1.0, False
+    while True:
+        j = len(result)
+        if j == cap:
+            break
+        k = global_argmax()
+        if k is None:
+            break
+        # verification loop: the leader's exact residual, then the argmax again
+        while True:
+            row = fetch_row(k)
+            exact2 = backend.pq_verify(st, row, j, int(k[2]))
+            k2 = global_argmax()
+            if k2 is not None and int(k2[2]) == int(k[2]):
+                break
+            if k2 is None:
+                break
+            k = k2
+        rjj = float(np.sqrt(exact2))
+        if first < 0:
+            first = rjj
+        thr = max(tolerance * first, floor)
+        stop = first == 0 or rjj <= thr or (online and rjj <= floor)
+        if stop:
+            if exact_mode:
+                break
+            # confirm on exact values: every rank rescans its uncertain columns
+            backend.pq_scan(st, j, thr * thr)
+            exact_mode = True
+            k = global_argmax()
+            if k is None:
+                break
+            row = fetch_row(k)
+            exact2 = backend.pq_verify(st, row, j, int(k[2]))
+            if first == 0 or np.sqrt(exact2) <= thr:
+                break
+        backend.pq_accept(st, row, j, int(k[2]), exact2, int(k[1]), dense)
+        exact_mode = False
+        result.append(row[d + 1:d + 6].copy())
+    backend.pq_end(st)
+    rec = np.array(result).reshape(-1, 5)
+    return rec[:, 0].round().astype(np.int64), rec[:, 1:4], rec[:, 4], n_total
+
+
 def select_fit_sharded(backend, comm, xyz, w, grid_offset, ng_total, want_error=True, qr="distributed",
                        **select_kw):
     """Selection + fit of one cluster whose grid is split over the ranks.
@@ -178,6 +280,21 @@ def select_fit_sharded(backend, comm, xyz, w, grid_offset, ng_total, want_error=
     import torch
     precision = select_kw.get("precision", "fp64")
     naxes = len(select_kw.get("axes", ("ao",)))
+    if select_kw.get("algorithm", "rand_sketch") in ("qrcp_dense", "qrcp_online", 0, 1):
+        # pair-space QR over the shards, then the fit on each shard
+        sel = {kk: v for kk, v in select_kw.items() if kk != "precision"}
+        anchors, a_xyz, a_w, n_total = select_pair_qr_sharded(backend, comm, xyz, w, grid_offset, **sel)
+        theta, finfo, fsums = backend.fit_at(xyz, w, a_xyz, a_w, precision, want_error)
+        tot = backend.to_numpy(comm.allreduce_sum(backend.tensor(np.asarray(fsums, np.float64))))
+        err2, exact2 = max(float(tot[0]), 0.0), float(tot[1])
+        counts = [int(backend.to_numpy(c)[0]) for c in
+                  comm.allgather(backend.tensor(np.array([theta.shape[1]], np.int64)))]
+        sinfo = SimpleNamespace(n_kept=n_total, sketch_rows=0, numerical_rank=0, relative_residual=0.0,
+                                verifications=0, reselections=0, precision_used=0)
+        return ShardedResult(anchors=anchors, theta=theta, n_kept_local=int(theta.shape[1]),
+                             kept_offset=int(sum(counts[:comm.rank])), pair_l2=float(np.sqrt(err2)),
+                             pair_relative=float(np.sqrt(err2 / exact2)) if exact2 else 0.0,
+                             select_info=sinfo, fit_info=finfo, counts=counts)
     # 1. projection of the shard and the global per-component sums of squares
     shard, n_kept, ell, sumsq = backend.project(xyz, w, ng_total, **select_kw)
     sums = comm.allreduce_sum(backend.tensor(np.asarray(sumsq, np.float64)))
@@ -324,6 +441,38 @@ class CudaBackend:
 
     def adjoint_partial(self, xyz, w, a_xyz, a_w, dm, want_grad):
         return self.ctx.energy_gradient_shard(xyz, w, a_xyz, a_w, dm, want_grad)
+
+    # the sharded pair-space QR (isdf_pairqr_shard_*)
+    def pq_begin(self, xyz, w, grid_offset, **kw_sel):
+        return self.ctx.pairqr_shard(xyz, w, grid_offset, **kw_sel)
+
+    @staticmethod
+    def pq_init(st, sums, pos_offset):
+        return st.init(sums, pos_offset)
+
+    @staticmethod
+    def pq_argmax(st):
+        return st.argmax()
+
+    @staticmethod
+    def pq_row(st, col):
+        return st.row(col)
+
+    @staticmethod
+    def pq_verify(st, row, j, col):
+        return st.verify(row, j, col)
+
+    @staticmethod
+    def pq_accept(st, row, j, col, exact2, winner_pos, dense):
+        st.accept(row, j, col, exact2, winner_pos, dense)
+
+    @staticmethod
+    def pq_scan(st, j, thr2):
+        return st.scan(j, thr2)
+
+    @staticmethod
+    def pq_end(st):
+        st.free()
 
     def adjoint_finish(self, a_xyz, a_w, dm, sums, want_grad):
         return self.ctx.energy_gradient_finish(a_xyz, a_w, dm, sums, want_grad)

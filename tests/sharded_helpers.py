@@ -3,6 +3,7 @@ CPU backend built on the oracle (so that the protocol runs on gloo ranks
 without a GPU) and a thread-based communicator (so that several shards can
 run in one process on one GPU).  Test infrastructure only."""
 import threading
+from types import SimpleNamespace
 
 import numpy as np
 import torch
@@ -132,6 +133,91 @@ class OracleBackend:
         rank, tails, nrank = O.sketch_rank_rules(diag, energy, ell, n_total, oversampling, tolerance, max_rank,
                                                  d * (d + 1) // 2)
         return rank, nrank, float(tails[rank] / tails[0]) if tails[0] else 0.0
+
+    # ---- the sharded pair-space QR, restated with exact residuals (the
+    # arithmetic of oracle.pair_qrcp_exact: basis as symmetric d x d matrices)
+    def pq_begin(self, xyz, w, grid_offset, axes=("ao",), axis_weights=None, algorithm="qrcp_dense", **_):
+        xyz, w = self.to_numpy(xyz).reshape(-1, 3), self.to_numpy(w)
+        keep = np.flatnonzero(w != 0)
+        codes = [O.AXIS_CODES[a] for a in axes]
+        nao = self.nao
+        F = self.oc.axis_features(xyz[keep], codes) if len(keep) else np.zeros((0, len(codes) * nao))
+        sumsq = np.zeros(5)
+        for i in range(len(codes)):
+            sumsq[i] = np.sum(F[:, i * nao:(i + 1) * nao] ** 2)
+        return SimpleNamespace(n_kept=len(keep), d=F.shape[1], sumsq=sumsq, F=F, sw=np.sqrt(np.abs(w[keep])),
+                               keep=keep, xyz=xyz, w=w, grid_offset=grid_offset, codes=codes,
+                               aw=axis_weights, basis=[], coef=[], est={}, last=None)
+
+    def pq_init(self, st, sums, pos_offset):
+        ne = len(st.codes)
+        st.colscale = np.ones(st.d)
+        if ne > 1:   # every rank derives the same scales from the same global sums
+            factors = np.ones(ne) if not st.aw else np.asarray(st.aw, float)
+            st.colscale = np.repeat(factors / np.sqrt(sums[:ne]), self.nao)
+        st.Fs = st.F * st.colscale[None, :]
+        st.pos = pos_offset + np.arange(st.n_kept)
+        st.pos_offset = pos_offset
+        st.selected = np.zeros(st.n_kept, bool)
+        st.norm2 = (st.sw * np.einsum("gi,gi->g", st.Fs, st.Fs)) ** 2
+        return np.array([st.norm2.sum(), 0.0 if np.all(np.isfinite(st.norm2)) else 1.0])
+
+    @staticmethod
+    def pq_argmax(st):
+        if st.n_kept == 0 or st.selected.all():
+            return np.array([-1.0, -1.0, -1.0])
+        res = st.norm2 - sum((c ** 2 for c in st.coef), np.zeros(st.n_kept))
+        for g, v in st.est.items():
+            res[g] = v
+        res[st.selected] = -np.inf
+        best = max(np.flatnonzero(~st.selected), key=lambda g: (res[g], -st.pos[g]))
+        return np.array([res[best], st.pos[best], st.pos_offset + best])
+
+    @staticmethod
+    def pq_row(st, col):
+        g = col - st.pos_offset
+        gi = st.keep[g]
+        return np.concatenate([st.F[g], [st.sw[g], st.grid_offset + gi], st.xyz[gi], [st.w[gi]]])
+
+    def pq_verify(self, st, row, j, col):
+        d = st.d
+        f = row[:d] * st.colscale
+        v = row[d] * np.outer(f, f)
+        t0 = [np.sum(Q * v) for Q in st.basis]
+        for t, Q in zip(t0, st.basis):
+            v = v - t * Q
+        for Q in st.basis:                      # second Gram-Schmidt pass
+            v = v - np.sum(Q * v) * Q
+        exact2 = float(np.sum(v * v))
+        st.last = (col, v)
+        g = col - st.pos_offset
+        if 0 <= g < st.n_kept:
+            st.est[g] = exact2
+        return exact2
+
+    def pq_accept(self, st, row, j, col, exact2, winner_pos, dense):
+        v = st.last[1] / np.sqrt(exact2)
+        v = 0.5 * (v + v.T)
+        st.basis.append(v)
+        st.coef.append(st.sw * np.einsum("gi,gi->g", st.Fs @ v, st.Fs) if st.n_kept else np.zeros(0))
+        st.est = {}
+        g = col - st.pos_offset
+        if dense and st.n_kept:
+            at_j = np.flatnonzero(st.pos == j)
+            if len(at_j):
+                st.pos[at_j] = winner_pos
+        if 0 <= g < st.n_kept:
+            st.selected[g] = True
+            if dense:
+                st.pos[g] = j
+
+    @staticmethod
+    def pq_scan(st, j, thr2):
+        return 0
+
+    @staticmethod
+    def pq_end(st):
+        pass
 
     def adjoint_partial(self, xyz, w, a_xyz, a_w, dm, want_grad):
         return oracle_adjoint_partial(self.oc, self.to_numpy(xyz).reshape(-1, 3), self.to_numpy(w),

@@ -271,3 +271,116 @@ def test_cuda_adjoint_two_shards_match_single_call():
                 np.testing.assert_allclose(g, g_ref, rtol=0, atol=1e-11 * np.abs(g_ref).max())
             else:
                 assert not g.any()
+
+
+# ---- the pair-space QR over grid shards -------------------------------------------
+PQ_KW = dict(axes=("ao", "dx", "dy", "dz"), axis_weights=[1.0, 0.5, 0.5, 0.5], max_rank=6)
+
+
+def _gloo_pairqr_rank(rank, size, port, out_dir, algorithm, empty_rank):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from mp_isdf_b200.sharded import TorchComm, select_fit_sharded
+    from sharded_helpers import OracleBackend
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=size,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        mol, pts, w = _system()
+        bounds = _split(len(pts), size - (empty_rank >= 0))
+        if empty_rank >= 0:
+            bounds.insert(empty_rank, (bounds[empty_rank - 1][1], bounds[empty_rank - 1][1]) if empty_rank
+                          else (0, 0))
+        lo, hi = bounds[rank]
+        res = select_fit_sharded(OracleBackend(mol), TorchComm(), torch.as_tensor(pts[lo:hi]),
+                                 torch.as_tensor(w[lo:hi]), lo, len(pts), algorithm=algorithm, **PQ_KW)
+        np.save(os.path.join(out_dir, f"theta{rank}.npy"), res.theta.numpy())
+        with open(os.path.join(out_dir, f"res{rank}.json"), "w") as f:
+            json.dump({"anchors": res.anchors.tolist(), "pair_relative": res.pair_relative}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("size,algorithm,empty_rank", [(2, "qrcp_dense", -1), (3, "qrcp_online", 1)])
+def test_gloo_pair_qr_matches_oracle(size, algorithm, empty_rank):
+    """The pair-space QR over gloo CPU ranks (per-step key all-gather, the
+    leader's row by all-reduce, the same exact residual on every rank) with
+    the oracle backend gives the single-process oracle's exact-norm pivots,
+    Theta and pair error, also with a rank that owns no kept point."""
+    import torch.multiprocessing as mp
+    from oracle import oracle as O
+    mol, pts, w = _system()
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_gloo_pairqr_rank, args=(size, _free_port(), d, algorithm, empty_rank), nprocs=size,
+                           join=True, start_method="spawn")
+        res = [json.load(open(os.path.join(d, f"res{r}.json"))) for r in range(size)]
+        thetas = [np.load(os.path.join(d, f"theta{r}.npy")) for r in range(size)]
+    for r in range(1, size):
+        assert res[r]["anchors"] == res[0]["anchors"]
+    oc = O.OracleContext(mol.atm, mol.bas, mol.env)
+    codes = [O.AXIS_CODES[a] for a in PQ_KW["axes"]]
+    keep = np.flatnonzero(w != 0)
+    scales = O.axis_scales(oc, pts, w, codes, PQ_KW["axis_weights"])
+    pos, _, gaps = O.pair_qrcp_exact(oc.axis_features(pts[keep], codes, scales), w[keep], PQ_KW["max_rank"])
+    ref = [int(keep[p]) for p in pos]
+    for j, (a, b) in enumerate(zip(res[0]["anchors"], ref)):
+        if a != b:
+            assert gaps[j] <= 1e-10, (j, a, b, gaps[j])
+            return
+    assert res[0]["anchors"] == ref
+    theta_ref, err = O.gram_fit(oc, pts[keep], w[keep], pts[ref], w[ref])
+    theta = np.concatenate([t for t in thetas if t.size], axis=1)
+    np.testing.assert_allclose(theta, theta_ref, rtol=1e-9, atol=1e-9 * np.abs(theta_ref).max())
+    for r in range(size):
+        np.testing.assert_allclose(res[r]["pair_relative"], err["relative"], rtol=1e-10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("algorithm", ["qrcp_dense", "qrcp_online"])
+def test_cuda_pair_qr_two_shards_match_select_fit(algorithm):
+    """The library's sharded pair-space QR (isdf_pairqr_shard_*) with two
+    shards in one process (threads standing in for ranks) against
+    isdf_select_fit on the whole grid: the same anchors, Theta and pair error."""
+    import threading
+    import torch
+    from mp_isdf_b200 import capi
+    from mp_isdf_b200.sharded import CudaBackend, select_fit_sharded
+    from sharded_helpers import ThreadComm
+    mol, pts, w = _system()
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    x = torch.tensor(pts, device="cuda")
+    wt = torch.tensor(w, device="cuda")
+    theta = torch.zeros(PQ_KW["max_rank"] * len(pts), dtype=torch.float64, device="cuda")
+    piv, _, finfo = ctx.select_fit(x, wt, theta, want_error=True, precision="fp64", algorithm=algorithm, **PQ_KW)
+    torch.cuda.synchronize()
+    size = 2
+    shared = ThreadComm.Shared(size)
+    results, errors = [None] * size, []
+
+    def run(rank):
+        try:
+            torch.cuda.set_device(0)
+            c = capi.Context(mol.atm, mol.bas, mol.env)
+            lo, hi = _split(len(pts), size)[rank]
+            results[rank] = select_fit_sharded(CudaBackend(c), ThreadComm(rank, size, shared),
+                                               x[lo:hi].contiguous(), wt[lo:hi].contiguous(), lo, len(pts),
+                                               precision="fp64", algorithm=algorithm, **PQ_KW)
+            torch.cuda.synchronize()
+        except Exception as e:  # surfaced below
+            errors.append(e)
+            shared.barrier.abort()
+
+    threads = [threading.Thread(target=run, args=(r,)) for r in range(size)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    np.testing.assert_array_equal(results[0].anchors, piv)
+    np.testing.assert_array_equal(results[1].anchors, piv)
+    th_sharded = torch.cat([r.theta for r in results], dim=1).cpu().numpy()
+    k, n = len(piv), finfo.n_kept
+    th_ref = theta[:k * n].view(k, n).cpu().numpy()
+    rel = np.abs(th_sharded - th_ref).max() / np.abs(th_ref).max()
+    assert rel <= 1e-12 * max(1.0, finfo.condition) ** 2, rel
+    assert abs(results[0].pair_relative - finfo.pair_relative) <= 1e-10 * finfo.pair_relative
