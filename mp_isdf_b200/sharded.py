@@ -27,6 +27,11 @@ contiguous shard of the grid, in grid order, and runs::
     4. the fit on its shard with the anchors' coordinates
        all-reduce(sum) of the pair-error sums
 
+qrcp_dense and qrcp_online go through ``select_pair_qr_sharded``: the ranks keep
+their points' features and residual estimates, the pair basis is replicated,
+and per pivot one key per rank is all-gathered and the leader's row
+all-reduced; every rank verifies it exactly with the same result.
+
 ``energy_gradient_sharded`` runs the nuclear-gradient adjoint the same way:
 per-rank partial sums, one all-reduce(sum), the anchor-side algebra on every
 rank.
@@ -274,8 +279,9 @@ def select_fit_sharded(backend, comm, xyz, w, grid_offset, ng_total, want_error=
     ``xyz``/``w``: this rank's contiguous shard (device tensors for the CUDA
     backend), starting at global grid index ``grid_offset``; ``ng_total``: the
     whole grid's size.  ``select_kw``: the arguments of ``Context.select``
-    (rand_sketch).  Returns a ``ShardedResult`` with global anchor indices
-    (identical on every rank) and this rank's Theta columns.
+    (rand_sketch, qrcp_dense or qrcp_online).  Returns a ``ShardedResult`` with
+    global anchor indices (identical on every rank) and this rank's Theta
+    columns.
     """
     import torch
     precision = select_kw.get("precision", "fp64")
