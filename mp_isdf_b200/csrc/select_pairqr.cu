@@ -329,8 +329,9 @@ struct PairQr {
         DeviceBuffer<double> L2(static_cast<size_t>(n * cap2), s), Q2(static_cast<size_t>(cap2 * m), s),
             t02(cap2, s), t12(cap2, s);
         if (capL) {
-            ISDF_CUDA(cudaMemcpy2DAsync(L2.get(), cap2 * sizeof(double), L.get(), capL * sizeof(double),
-                                        capL * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
+            if (n > 0)   // a shard may hold no kept point
+                ISDF_CUDA(cudaMemcpy2DAsync(L2.get(), cap2 * sizeof(double), L.get(), capL * sizeof(double),
+                                            capL * sizeof(double), n, cudaMemcpyDeviceToDevice, s));
             ISDF_CUDA(cudaMemcpyAsync(Q2.get(), Q.get(), capL * m * sizeof(double),
                                       cudaMemcpyDeviceToDevice, s));
             // the coefficients of the column being accepted
