@@ -50,8 +50,8 @@ def parse():
                          "fitted Theta, the FP64 density (column-normalized) sketch and the FP64 "
                          "quadrature sketch with an occupied-orbital axis")
     ap.add_argument("--mode", choices=("auto", "sharded", "replicas"), default="auto",
-                    help="N > 1: shard one cluster's grid over the ranks (auto, for rand_sketch "
-                         "configs) or run one cluster per rank")
+                    help="N > 1: shard one cluster's grid over the ranks (auto) or run one cluster "
+                         "per rank")
     ap.add_argument("--max-points", type=int, default=0,
                     help="keep every k-th grid point so that at most this many remain "
                          "(small cases for profiling; 0 = full grid)")
@@ -531,8 +531,8 @@ def run_ours(args, rank, world, local_rank):
     def sel_kw(precision):
         return selection_kwargs(cfg, names, factors, precision)
 
-    sharded = cfg["algorithm"] == "rand_sketch" and (
-        args.mode == "sharded" or (args.mode == "auto" and world > 1))
+    # every selection algorithm shards (the sketch QR, the pair-space QR)
+    sharded = args.mode == "sharded" or (args.mode == "auto" and world > 1)
     if sharded:
         # one cluster per step, its grid split into contiguous per-rank shards
         from mp_isdf_b200.sharded import CudaBackend, LocalComm, TorchComm, select_fit_sharded
