@@ -79,8 +79,7 @@ def workload_desc(cfg_key, cfg, mol, pts, w, names, precision):
     return {
         "workload": f"{cfg_key} {cfg['name']}: synthetic cc-pVDZ-shaped basis ({mol.nao} AOs), "
                     f"level-{cfg['level']} stand-in grid ({len(pts)} points, "
-                    f"{int(np.count_nonzero(w))} nonzero-weight), axes {cfg['axes']}, {algo}, "
-                    f"{precision} form",
+                    f"{int(np.count_nonzero(w))} nonzero-weight), axes {cfg['axes']}, {algo}",
         "nao": mol.nao, "grid_points": int(len(pts)), "axes": cfg["axes"], "algorithm": cfg["algorithm"],
         "anchor_rank": cfg["rank"],
         "sketch_rows": cfg["rank"] + cfg["oversampling"] if cfg["algorithm"] == "rand_sketch" else None,
