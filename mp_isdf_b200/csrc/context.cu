@@ -34,6 +34,8 @@ Context::~Context() {
     cudaFree(d_chunk_ao0);
     cudaFree(d_ao_slot);
     cudaFree(d_piece_chunk);
+    cudaFree(d_win_entry);
+    cudaFree(d_win_begin);
     cudaFree(d_piece_rec);
     cudaFree(d_piece_prim);
     cudaFree(d_piece_c64);
@@ -125,6 +127,7 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
     require(natm >= 0 && nbas >= 0 && nenv >= 20, "invalid libcint ATM/BAS/ENV table sizes");
     auto c = std::make_unique<Context>();
     ISDF_CUDA(cudaGetDevice(&c->device));
+    ISDF_CUDA(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device));
     {
         // Scratch buffers come from this process's default stream-ordered pool;
         // keep freed blocks cached across calls instead of returning them to
@@ -206,6 +209,7 @@ Context* create_context(const int32_t* atm, int natm, const int32_t* bas, int nb
         upload_shell_centres(*c);
     }
     build_chunk_layout(*c);
+    build_window_layout(*c);
     return c.release();
 }
 
@@ -254,34 +258,51 @@ ao_raw_kernel(const ShellDesc* __restrict__ shells, int nshell, const T* __restr
 }
 
 // Tiled evaluation for the (Ng, nao) / (3, Ng, nao) layouts: a block takes 64
-// points (two warps per piece lane, lane = point) and walks the K-chunks of
-// the context's chunk layout (contiguous AO ranges of at most 32 slots holding
-// whole contraction groups); the two warps of lane j evaluate the pieces that
-// the layout balanced onto lane j, for points 0-31 and 32-63, so each piece's
-// metadata is read twice close together.  The chunk's values go to a padded
-// shared tile [comp][slot][point]; then every (component, point) row of the
-// chunk is written as one contiguous run of `fill` values from a row pointer
-// formed once per block, so a warp store covers up to 256 bytes instead of 32
-// scattered words.  The values are those of ao_raw_kernel up to the
-// contraction of products into FMAs (same offsets, same per-contraction
-// arithmetic), except that a piece whose every primitive is beyond the cutoff
-// at all 32 points of a warp is written as +0 without evaluation (the
-// evaluation gives zeros there as well, possibly signed).
+// points (two warps per piece lane, lane = point) and walks the AO windows
+// [32w, 32w + 32) of the context's window layout; the two warps of lane j
+// evaluate the window's pieces that the layout balanced onto lane j, for
+// points 0-31 and 32-63, into a padded shared tile [comp][slot][point].  Then
+// every (component, point) row segment of the window leaves as one aligned run
+// of up to 32 values -- a whole 128-byte line of FP32 (two of FP64) when the
+// row length is a multiple of 32 values -- and the store pass leaves zeros
+// behind in the tile, so a screened piece costs no shared-memory writes.  A
+// piece across a window boundary is evaluated in each window and writes the
+// slots inside it.  The values are those of ao_raw_kernel up to the contraction
+// of products into FMAs (same offsets, same per-contraction arithmetic), with
+// +0 where a piece is screened for a whole warp.  Written without any
+// evaluation, the C5 layout's rows took 26.7 ms as 28-32 value runs from the
+// arbitrary starts of contraction-group chunks (FP32, 4 components: 1.8 TB/s)
+// and 9.5 ms as aligned 32-value windows (5.1 TB/s).
+//
+// Screening, in two steps: the bounding box of the tile's points against each
+// piece's FP64 screening radius (a candidate bit per piece in shared memory:
+// the record of a piece that is not a candidate is never read), then each
+// warp's 32 points against the candidate's radius.  The FP64 screening
+// exponent drops nothing above kScreenFp64 (1e-15) for either table.
 constexpr int kTilePts = 64;
 constexpr int kTileStride = kTilePts + 1;   // padded point stride: conflict-free row reads
+constexpr double kScreenCut = kExpCut * 1.0001;   // margin for the exponent's rounding to FP32
 
 template <class T>
-struct TileSink {
+struct WinSink {
     T* st; int p, base;
     template <int C> __device__ __forceinline__ void put(int ao, T v) {
-        st[(C * 32 + ao + base) * kTileStride + p] = v;
+        const int s = ao + base;
+        if (static_cast<unsigned>(s) < static_cast<unsigned>(kWin)) st[(C * kWin + s) * kTileStride + p] = v;
     }
 };
 
-struct TileArgs {
-    const float4* piece_rec; const double2* piece_c64; const void* prims;   // packed piece records
-    const int* lane_begin; const int* fill; const int* chunk_ao0; int nchunks;
-    const double* pts; int64_t n, ld; void* val; void* grad; bool want_val;
+// the same, with the sums of squares of the slots it writes (each AO once)
+template <class T>
+struct WinSqSink {
+    T* st; int p, base; bool count; double sq[4];
+    template <int C> __device__ __forceinline__ void put(int ao, T v) {
+        const int s = ao + base;
+        if (static_cast<unsigned>(s) < static_cast<unsigned>(kWin)) {
+            st[(C * kWin + s) * kTileStride + p] = v;
+            if (count) sq[C] += static_cast<double>(v) * static_cast<double>(v);
+        }
+    }
 };
 
 // The packed primitive table of T (float4 entries, or two double2 per entry).
@@ -290,29 +311,101 @@ __device__ __forceinline__ const typename PackedPrim<T>::rec* packed_prims(const
     return static_cast<const typename PackedPrim<T>::rec*>(p) + (sizeof(T) == 8 ? 2 : 1) * prim_off;
 }
 
-// Shared tiles per block: two for the value-only tiles (chunk c evaluated into
-// one while other warps still store chunk c - 1 from the other, one barrier
-// per chunk; FP64 values 12.5 -> 12.2 ms at C5), else one (two barriers per
-// chunk: doubling the 33 KB FP32 gradient tile left less L1 and was slower).
+// Candidate pieces of a tile: bit pi of cand is set where piece pi's FP64
+// screening radius reaches the bounding box of the tile's valid points (its
+// half-widths widened by 1e-9 bohr, far above the rounding of the box
+// arithmetic, so that a piece left out is screened at every point by the
+// per-warp test as well).  The warps that hold each point once (box_warp)
+// reduce the box; called by every thread, ends with a block barrier.
+__device__ void tile_candidates(const double2* __restrict__ c64, int npieces, double px, double py, double pz,
+                                bool valid, bool box_warp, int half, double (*box)[6], uint32_t* cand) {
+    const int lane = threadIdx.x % 32;
+    if (box_warp) {
+        const double pc[3] = {px, py, pz};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double lo = valid ? pc[d] : INFINITY, hi = valid ? pc[d] : -INFINITY;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+            }
+            if (lane == 0) { box[half][d] = lo; box[half][3 + d] = hi; }
+        }
+    }
+    for (int i = threadIdx.x; i < (npieces + 31) / 32; i += blockDim.x) cand[i] = 0u;
+    __syncthreads();
+    double mid[3], hw[3];
+    bool any = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double lo = box[0][d], hi = box[0][3 + d];
+#pragma unroll
+        for (int h = 1; h < kTilePts / 32; ++h) { lo = fmin(lo, box[h][d]); hi = fmax(hi, box[h][3 + d]); }
+        any = any && lo <= hi;
+        mid[d] = 0.5 * (lo + hi);
+        hw[d] = 0.5 * (hi - lo) + 1e-9;
+    }
+    if (any)
+        for (int pi = threadIdx.x; pi < npieces; pi += blockDim.x) {
+            const double2 cxy = __ldg(c64 + 2 * pi), cza = __ldg(c64 + 2 * pi + 1);
+            const double ex = fmax(fabs(cxy.x - mid[0]) - hw[0], 0.0);
+            const double ey = fmax(fabs(cxy.y - mid[1]) - hw[1], 0.0);
+            const double ez = fmax(fabs(cza.x - mid[2]) - hw[2], 0.0);
+            if (!(cza.y * (ex * ex + ey * ey + ez * ez) > kScreenCut)) atomicOr(&cand[pi >> 5], 1u << (pi & 31));
+        }
+    __syncthreads();
+}
+
+struct TileArgs {
+    const float4* piece_rec; const double2* piece_c64; const void* prims;   // packed piece records
+    const int2* win_entry; const int* win_begin; int nwin, nao, npieces, lanes;   // window layout
+    const double* pts; int64_t n, ld; void* val; void* grad; bool want_val;
+};
+
+// Shared tiles per block: two for the value-only tiles (window w is evaluated
+// into one while other warps still store window w - 1 from the other, one
+// barrier per window), else one (two barriers per window).
 template <class T, bool GRAD>
 constexpr int tile_bufs() {
-    return 2 * (GRAD ? 4 : 1) * 32 * kTileStride * sizeof(T) <= 40 * 1024 ? 2 : 1;
+    return 2 * (GRAD ? 4 : 1) * kWin * kTileStride * sizeof(T) <= 40 * 1024 ? 2 : 1;
 }
 template <class T, bool GRAD>
-constexpr size_t tile_elems() { return static_cast<size_t>(GRAD ? 4 : 1) * 32 * kTileStride; }
+constexpr size_t tile_elems() { return static_cast<size_t>(GRAD ? 4 : 1) * kWin * kTileStride; }
 
+// dynamic shared memory: row pointers, tiles, candidate bits
 template <class T, bool GRAD>
-constexpr size_t tile_smem_bytes() {
-    return tile_bufs<T, GRAD>() * tile_elems<T, GRAD>() * sizeof(T) + (GRAD ? 4 : 1) * kTilePts * sizeof(T*);
+size_t tile_smem_bytes(int nrowp, int npieces) {
+    return nrowp * sizeof(T*) + tile_bufs<T, GRAD>() * tile_elems<T, GRAD>() * sizeof(T) +
+           4 * static_cast<size_t>((npieces + 31) / 32);
+}
+
+// One piece of a window for the warp's 32 points: nothing where the piece is
+// not a candidate of the tile or where every point of the warp lies beyond its
+// screening radius, else its values into the tile through the sink.
+__device__ __forceinline__ bool piece_live(const float4* __restrict__ rec, const double2* __restrict__ c64,
+                                           const uint32_t* cand, int pi, double px, double py, double pz,
+                                           bool valid, int4& meta, int& poff, double& dx, double& dy,
+                                           double& dz, double& r2) {
+    if (!((cand[pi >> 5] >> (pi & 31)) & 1u)) return false;
+    meta = __ldg(reinterpret_cast<const int4*>(rec) + 3 * pi + 2);
+    poff = __float_as_int(__ldg(rec + 3 * pi + 1).w);
+    const double2 cxy = __ldg(c64 + 2 * pi), cza = __ldg(c64 + 2 * pi + 1);
+    dx = px - cxy.x; dy = py - cxy.y; dz = pz - cza.x;
+    r2 = dx * dx + dy * dy + dz * dz;
+    return !__all_sync(0xffffffffu, !valid || cza.y * r2 > kScreenCut);
 }
 
 template <class T, bool GRAD, int LMAX, int PPT>
 __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) ao_tile_kernel(TileArgs a) {
     constexpr int kNComp = GRAD ? 4 : 1;
     constexpr int kWarps = kTilePts / 32 * PPT;
+    constexpr int kBufs = tile_bufs<T, GRAD>();
     extern __shared__ __align__(16) uint8_t tile_raw[];
+    __shared__ double box[kTilePts / 32][6];
     T** rowp = reinterpret_cast<T**>(tile_raw);                       // [kNComp][kTilePts]
     T* const st0 = reinterpret_cast<T*>(tile_raw + kNComp * kTilePts * sizeof(T*));
+    uint32_t* const cand = reinterpret_cast<uint32_t*>(st0 + kBufs * tile_elems<T, GRAD>());
     const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
     const int lanegrp = warp % PPT, p = (warp / PPT) * 32 + lane;
     const int64_t b0 = static_cast<int64_t>(blockIdx.x) * kTilePts;
@@ -331,41 +424,37 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) ao_tile_kernel(TileA
         }
         rowp[i] = r;
     }
-    // a piece is written as zeros where its FP64 screening exponent puts all
-    // 32 points of the warp beyond kExpCut (nothing dropped above kScreenFp64);
-    // the margin covers the exponent's rounding to FP32
-    const double cut = kExpCut * 1.0001;
-    for (int c = 0; c < a.nchunks; ++c) {
-        T* const st = st0 + (tile_bufs<T, GRAD>() == 2 ? (c & 1) * tile_elems<T, GRAD>() : 0);
-        const int pb = a.lane_begin[c * PPT + lanegrp], pe = a.lane_begin[c * PPT + lanegrp + 1];
-        for (int pi = pb; pi < pe; ++pi) {
-            // packed record: (l, primitives, contractions, first slot), centre and
-            // smallest exponent, primitive-table offset
-            const int4 meta = __ldg(reinterpret_cast<const int4*>(a.piece_rec) + 3 * pi + 2);
-            const int poff = __float_as_int(__ldg(a.piece_rec + 3 * pi + 1).w);
-            const double2 cxy = __ldg(a.piece_c64 + 2 * pi), cza = __ldg(a.piece_c64 + 2 * pi + 1);
-            const int l = meta.x, nprim = meta.y, nc = meta.z, slot0 = meta.w;
-            const int ns = 2 * l + 1;
-            const double dx = px - cxy.x, dy = py - cxy.y, dz = pz - cza.x;
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            if (__all_sync(0xffffffffu, !valid || cza.y * r2 > cut)) {
-                for (int k = slot0; k < slot0 + nc * ns; ++k)
-#pragma unroll
-                    for (int cc = 0; cc < kNComp; ++cc) st[(cc * 32 + k) * kTileStride + p] = T(0);
+    // the tiles start as zeros; the store pass zeroes every entry it reads
+    for (size_t i = threadIdx.x; i < kBufs * tile_elems<T, GRAD>() * sizeof(T) / 16; i += blockDim.x)
+        reinterpret_cast<uint4*>(st0)[i] = make_uint4(0u, 0u, 0u, 0u);
+    tile_candidates(a.piece_c64, a.npieces, px, py, pz, valid, lanegrp == 0, warp / PPT, box, cand);
+    for (int w = 0; w < a.nwin; ++w) {
+        T* const st = st0 + (kBufs == 2 ? (w & 1) * tile_elems<T, GRAD>() : 0);
+        const int eb = __ldg(a.win_begin + w * PPT + lanegrp), ee = __ldg(a.win_begin + w * PPT + lanegrp + 1);
+        for (int e = eb; e < ee; ++e) {
+            const int2 en = __ldg(a.win_entry + e);
+            int4 meta; int poff; double dx, dy, dz, r2;
+            if (!piece_live(a.piece_rec, a.piece_c64, cand, en.x, px, py, pz, valid, meta, poff, dx, dy, dz, r2))
                 continue;
-            }
-            TileSink<T> sink{st, p, slot0};
-            eval_piece<T, GRAD, LMAX>(l, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
-                                      static_cast<T>(r2), packed_prims<T>(a.prims, poff), nprim, nc, sink);
+            WinSink<T> sink{st, p, en.y};
+            eval_piece<T, GRAD, LMAX>(meta.x, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
+                                      static_cast<T>(r2), packed_prims<T>(a.prims, poff), meta.y, meta.z, sink);
         }
         __syncthreads();
-        const int fill = a.fill[c], ao0 = a.chunk_ao0[c];
-        for (int r = warp; r < kNComp * kTilePts; r += kWarps) {
-            T* row = rowp[r];
-            if (row != nullptr && lane < fill)
-                row[ao0 + lane] = st[((r / kTilePts) * 32 + lane) * kTileStride + r % kTilePts];
+        // a warp takes whole point columns: it stores each component's row
+        // segment and zeroes the column behind it
+        const int ao0 = w * kWin, fill = min(kWin, a.nao - ao0);
+        for (int pp = warp; pp < kTilePts; pp += kWarps) {
+#pragma unroll
+            for (int cc = 0; cc < kNComp; ++cc) {
+                T* const row = rowp[cc * kTilePts + pp];
+                T& slot = st[(cc * kWin + lane) * kTileStride + pp];
+                const T v = slot;
+                slot = T(0);
+                if (row != nullptr && lane < fill) row[ao0 + lane] = v;
+            }
         }
-        if constexpr (tile_bufs<T, GRAD>() == 1) __syncthreads();   // the tile is refilled next
+        if constexpr (kBufs == 1) __syncthreads();   // the tile is refilled next
     }
 }
 
@@ -373,58 +462,186 @@ template <class T, bool GRAD, int LMAX, int PPT>
 void launch_tile(const TileArgs& a, cudaStream_t s) {
     const int64_t nb = (a.n + kTilePts - 1) / kTilePts;
     require(nb < (1ll << 31), "too many grid points for one launch");
-    constexpr size_t smem = tile_smem_bytes<T, GRAD>();
+    constexpr int kNComp = GRAD ? 4 : 1;
+    const size_t smem = tile_smem_bytes<T, GRAD>(kNComp * kTilePts, a.npieces);
+    require(smem <= 227 * 1024, "basis too large for the tiled AO evaluator's shared memory");
     auto kern = ao_tile_kernel<T, GRAD, LMAX, PPT>;
-    if constexpr (smem > 48 * 1024)
+    if (smem > 48 * 1024)
         ISDF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     kern<<<static_cast<unsigned>(nb), kTilePts / 32 * PPT * 32, smem, s>>>(a);
     ISDF_LAUNCH_CHECK();
 }
 
-template <class T, bool GRAD>
-void launch_tile_l(const Context& c, const TileArgs& a, cudaStream_t s) {
-    // lane counts as in piece_lanes_for_lmax()
-    if (c.lmax <= 2) launch_tile<T, GRAD, 2, 6>(a, s);
-    else if (c.lmax <= 4) launch_tile<T, GRAD, 4, 2>(a, s);
-    else launch_tile<T, GRAD, kMaxL, 2>(a, s);
-}
+// Values only, one warp per 32 points and no block barriers: the warp keeps a
+// private padded tile [slot][point] of one AO window, takes as candidates the
+// pieces whose FP64 screening radius reaches the bounding box of its points
+// (lane = piece, a ballot per 32 pieces), and per window loads the window's
+// entries with one coalesced load (lane = entry), keeps the candidates in a
+// ballot mask and evaluates them one by one (lane = point, each warp-uniform
+// piece screened as in ao_tile_kernel); then it stores its 32 aligned row
+// segments (lane = slot) and zeroes the tile behind them.  Same values as
+// ao_tile_kernel.  At C5 (FP64, 1.99 M points) the block form spent most of its
+// stalls at the per-window barrier and on the per-entry record chains.
+constexpr int kValWarps = 4;                      // independent warps per block
+constexpr int kWarpTileStride = 33;               // padded point stride of the warp tile
 
-// Tiled axis features F[p*ld + offset[a] + ao] = scale[a] * comp_a(p, ao): the
-// layout of ao_tile_kernel (64 points per block, piece lanes of the chunk
-// layout, a padded shared tile [comp][slot][point] per K-chunk), with the
-// points gathered through `index`, one contiguous row store per (axis entry,
-// point) and chunk, and the per-component sums of squares of the points with
-// nonzero weight accumulated by the evaluating threads (FP64).
 template <class T>
-struct TileSqSink {
-    T* st; int p, base; bool count; double sq[4];
+struct WarpSink {
+    T* st; int p, base;
     template <int C> __device__ __forceinline__ void put(int ao, T v) {
-        st[(C * 32 + ao + base) * kTileStride + p] = v;
-        if (count) sq[C] += static_cast<double>(v) * static_cast<double>(v);
+        static_assert(C == 0, "value tiles only");
+        const int s = ao + base;
+        if (static_cast<unsigned>(s) < static_cast<unsigned>(kWin)) st[s * kWarpTileStride + p] = v;
     }
 };
 
+template <class T>
+size_t value_warp_bytes(int npieces) {
+    const size_t b = kWin * kWarpTileStride * sizeof(T) + 4 * static_cast<size_t>((npieces + 31) / 32);
+    return (b + 15) / 16 * 16;
+}
+
+template <class T, int LMAX>
+__global__ void __launch_bounds__(kValWarps * 32, 6) ao_value_warp_kernel(TileArgs a, int warp_bytes) {
+    extern __shared__ __align__(16) uint8_t warp_raw[];
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+    T* const st = reinterpret_cast<T*>(warp_raw + static_cast<size_t>(warp) * warp_bytes);
+    uint32_t* const cand = reinterpret_cast<uint32_t*>(warp_raw + static_cast<size_t>(warp) * warp_bytes +
+                                                       kWin * kWarpTileStride * sizeof(T));
+    const int64_t g0 = (static_cast<int64_t>(blockIdx.x) * kValWarps + warp) * 32;
+    if (g0 >= a.n) return;   // whole warps only; nothing below synchronises the block
+    const int64_t g = g0 + lane;
+    const bool valid = g < a.n;
+    const double px = valid ? a.pts[3 * g] : 0.0, py = valid ? a.pts[3 * g + 1] : 0.0,
+                 pz = valid ? a.pts[3 * g + 2] : 0.0;
+    for (int i = lane; i < kWin * kWarpTileStride * static_cast<int>(sizeof(T)) / 16; i += 32)
+        reinterpret_cast<uint4*>(st)[i] = make_uint4(0u, 0u, 0u, 0u);
+    // candidates: the bounding box of the warp's valid points (every lane
+    // holds it after the butterfly), widened by 1e-9 bohr
+    double mid[3], hw[3];
+    {
+        const double pc[3] = {px, py, pz};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double lo = valid ? pc[d] : INFINITY, hi = valid ? pc[d] : -INFINITY;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+            }
+            mid[d] = 0.5 * (lo + hi);
+            hw[d] = 0.5 * (hi - lo) + 1e-9;
+        }
+    }
+    for (int k = 0; k < (a.npieces + 31) / 32; ++k) {
+        const int pi = k * 32 + lane;
+        bool c = false;
+        if (pi < a.npieces) {
+            const double2 cxy = __ldg(a.piece_c64 + 2 * pi), cza = __ldg(a.piece_c64 + 2 * pi + 1);
+            const double ex = fmax(fabs(cxy.x - mid[0]) - hw[0], 0.0);
+            const double ey = fmax(fabs(cxy.y - mid[1]) - hw[1], 0.0);
+            const double ez = fmax(fabs(cza.x - mid[2]) - hw[2], 0.0);
+            c = !(cza.y * (ex * ex + ey * ey + ez * ez) > kScreenCut);
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, c);
+        if (lane == 0) cand[k] = m;
+    }
+    __syncwarp();
+    const int np = a.n - g0 < 32 ? static_cast<int>(a.n - g0) : 32;
+    for (int w = 0; w < a.nwin; ++w) {
+        const int eb = __ldg(a.win_begin + w * a.lanes), ee = __ldg(a.win_begin + (w + 1) * a.lanes);
+        for (int base = eb; base < ee; base += 32) {
+            const int e = base + lane;
+            const int2 en = e < ee ? __ldg(a.win_entry + e) : make_int2(0, 0);
+            const bool c = e < ee && ((cand[en.x >> 5] >> (en.x & 31)) & 1u);
+            for (uint32_t m = __ballot_sync(0xffffffffu, c); m != 0u; m &= m - 1u) {
+                const int k = __ffs(m) - 1;
+                const int pi = __shfl_sync(0xffffffffu, en.x, k), off = __shfl_sync(0xffffffffu, en.y, k);
+                int4 meta; int poff; double dx, dy, dz, r2;
+                if (!piece_live(a.piece_rec, a.piece_c64, cand, pi, px, py, pz, valid, meta, poff, dx, dy, dz, r2))
+                    continue;
+                WarpSink<T> sink{st, lane, off};
+                eval_piece<T, false, LMAX>(meta.x, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
+                                           static_cast<T>(r2), packed_prims<T>(a.prims, poff), meta.y, meta.z, sink);
+            }
+        }
+        __syncwarp();
+        const int ao0 = w * kWin, fill = min(kWin, a.nao - ao0);
+        T* const out = static_cast<T*>(a.val) + g0 * a.ld + ao0 + lane;
+#pragma unroll 4
+        for (int pp = 0; pp < 32; ++pp) {
+            T& slot = st[lane * kWarpTileStride + pp];
+            const T v = slot;
+            slot = T(0);
+            if (pp < np && lane < fill) out[pp * a.ld] = v;
+        }
+        __syncwarp();
+    }
+}
+
+template <class T, int LMAX>
+void launch_value_warp(const TileArgs& a, cudaStream_t s) {
+    const int64_t nb = (a.n + kValWarps * 32 - 1) / (kValWarps * 32);
+    require(nb < (1ll << 31), "too many grid points for one launch");
+    const size_t wb = value_warp_bytes<T>(a.npieces);
+    const size_t smem = kValWarps * wb;
+    require(smem <= 227 * 1024, "basis too large for the tiled AO evaluator's shared memory");
+    auto kern = ao_value_warp_kernel<T, LMAX>;
+    if (smem > 48 * 1024)
+        ISDF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    kern<<<static_cast<unsigned>(nb), kValWarps * 32, smem, s>>>(a, static_cast<int>(wb));
+    ISDF_LAUNCH_CHECK();
+}
+
+template <class T, bool GRAD>
+void launch_tile_l(const Context& c, const TileArgs& a, cudaStream_t s) {
+    // the warp form has one warp per 32 points, a sixth of the block form's
+    // warps: it takes launches of at least two waves of its resident blocks
+    // (the FP64 fit's 43 690-point chunks at C5 ran 16 ms longer per step on it)
+    const bool warp_form = a.n >= static_cast<int64_t>(c.nsm) * 2 * 6 * kValWarps * 32;
+    if constexpr (!GRAD) {
+        if (!warp_form) {
+            if (c.lmax <= 2) launch_tile<T, false, 2, 6>(a, s);
+            else if (c.lmax <= 4) launch_tile<T, false, 4, 2>(a, s);
+            else launch_tile<T, false, kMaxL, 2>(a, s);
+            return;
+        }
+        if (c.lmax <= 2) launch_value_warp<T, 2>(a, s);
+        else if (c.lmax <= 4) launch_value_warp<T, 4>(a, s);
+        else launch_value_warp<T, kMaxL>(a, s);
+    } else {
+        // lane counts as in piece_lanes_for_lmax()
+        if (c.lmax <= 2) launch_tile<T, GRAD, 2, 6>(a, s);
+        else if (c.lmax <= 4) launch_tile<T, GRAD, 4, 2>(a, s);
+        else launch_tile<T, GRAD, kMaxL, 2>(a, s);
+    }
+}
+
+// Tiled axis features F[p*ld + offset[a] + ao] = scale[a] * comp_a(p, ao): the
+// layout of ao_tile_kernel (64 points per block, piece lanes of the window
+// layout, a padded shared tile [comp][slot][point] per AO window), with the
+// points gathered through `index`, one aligned row segment per (axis entry,
+// point) and window, and the per-component sums of squares of the points with
+// nonzero weight accumulated by the evaluating threads (FP64).
 struct AxisTileArgs {
     const float4* piece_rec; const double2* piece_c64; const void* prims;   // packed piece records
-    const int* lane_begin; const int* fill; const int* chunk_ao0; int nchunks;
+    const int2* win_entry; const int* win_begin; int nwin, nao, npieces;     // window layout
     const double* pts; const int64_t* index; int64_t n; const double* weights;
     void* out; int64_t ld; double* sumsq;
     int nent; int comp[16]; int off[16]; double scale[16];   // the non-occupied axis entries
 };
 
-template <class T, bool GRAD>
-constexpr size_t axis_tile_smem_bytes() {
-    return tile_bufs<T, GRAD>() * tile_elems<T, GRAD>() * sizeof(T) + kTilePts * sizeof(T*);
-}
-
 template <class T, bool GRAD, int LMAX, int PPT>
 __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) axis_tile_kernel(AxisTileArgs a) {
     constexpr int kNComp = GRAD ? 4 : 1;
     constexpr int kWarps = kTilePts / 32 * PPT;
+    constexpr int kBufs = tile_bufs<T, GRAD>();
     extern __shared__ __align__(16) uint8_t tile_raw[];
+    __shared__ double box[kTilePts / 32][6];
+    __shared__ double red[kWarps][4];
     T** rowp = reinterpret_cast<T**>(tile_raw);                       // [kTilePts]
     T* const st0 = reinterpret_cast<T*>(tile_raw + kTilePts * sizeof(T*));
-    __shared__ double red[kWarps][4];
+    uint32_t* const cand = reinterpret_cast<uint32_t*>(st0 + kBufs * tile_elems<T, GRAD>());
     const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
     const int lanegrp = warp % PPT, p = (warp / PPT) * 32 + lane;
     const int64_t b0 = static_cast<int64_t>(blockIdx.x) * kTilePts;
@@ -438,41 +655,38 @@ __global__ void __launch_bounds__(kTilePts / 32 * PPT * 32) axis_tile_kernel(Axi
         const int64_t gp = b0 + i;
         rowp[i] = gp < a.n ? static_cast<T*>(a.out) + gp * a.ld : nullptr;
     }
+    for (size_t i = threadIdx.x; i < kBufs * tile_elems<T, GRAD>() * sizeof(T) / 16; i += blockDim.x)
+        reinterpret_cast<uint4*>(st0)[i] = make_uint4(0u, 0u, 0u, 0u);
+    tile_candidates(a.piece_c64, a.npieces, px, py, pz, valid, lanegrp == 0, warp / PPT, box, cand);
     double sq[4] = {0.0, 0.0, 0.0, 0.0};
-    const double cut = kExpCut * 1.0001;
-    for (int c = 0; c < a.nchunks; ++c) {
-        T* const st = st0 + (tile_bufs<T, GRAD>() == 2 ? (c & 1) * tile_elems<T, GRAD>() : 0);
-        const int pb = a.lane_begin[c * PPT + lanegrp], pe = a.lane_begin[c * PPT + lanegrp + 1];
-        for (int pi = pb; pi < pe; ++pi) {
-            const int4 meta = __ldg(reinterpret_cast<const int4*>(a.piece_rec) + 3 * pi + 2);
-            const int poff = __float_as_int(__ldg(a.piece_rec + 3 * pi + 1).w);
-            const double2 cxy = __ldg(a.piece_c64 + 2 * pi), cza = __ldg(a.piece_c64 + 2 * pi + 1);
-            const int l = meta.x, nprim = meta.y, nc = meta.z, slot0 = meta.w;
-            const int ns = 2 * l + 1;
-            const double dx = px - cxy.x, dy = py - cxy.y, dz = pz - cza.x;
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            if (__all_sync(0xffffffffu, !valid || cza.y * r2 > cut)) {
-                for (int k = slot0; k < slot0 + nc * ns; ++k)
-#pragma unroll
-                    for (int cc = 0; cc < kNComp; ++cc) st[(cc * 32 + k) * kTileStride + p] = T(0);
+    for (int w = 0; w < a.nwin; ++w) {
+        T* const st = st0 + (kBufs == 2 ? (w & 1) * tile_elems<T, GRAD>() : 0);
+        const int eb = __ldg(a.win_begin + w * PPT + lanegrp), ee = __ldg(a.win_begin + w * PPT + lanegrp + 1);
+        for (int e = eb; e < ee; ++e) {
+            const int2 en = __ldg(a.win_entry + e);
+            int4 meta; int poff; double dx, dy, dz, r2;
+            if (!piece_live(a.piece_rec, a.piece_c64, cand, en.x, px, py, pz, valid, meta, poff, dx, dy, dz, r2))
                 continue;
-            }
-            TileSqSink<T> sink{st, p, slot0, count, {0.0, 0.0, 0.0, 0.0}};
-            eval_piece<T, GRAD, LMAX>(l, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
-                                      static_cast<T>(r2), packed_prims<T>(a.prims, poff), nprim, nc, sink);
+            WinSqSink<T> sink{st, p, en.y, count, {0.0, 0.0, 0.0, 0.0}};
+            eval_piece<T, GRAD, LMAX>(meta.x, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
+                                      static_cast<T>(r2), packed_prims<T>(a.prims, poff), meta.y, meta.z, sink);
 #pragma unroll
             for (int cc = 0; cc < 4; ++cc) sq[cc] += sink.sq[cc];
         }
         __syncthreads();
-        const int fill = a.fill[c], ao0 = a.chunk_ao0[c];
-        for (int r = warp; r < a.nent * kTilePts; r += kWarps) {
-            const int e = r / kTilePts, pp = r % kTilePts;
-            T* row = rowp[pp];
+        // a warp takes whole point columns: every axis entry's row segment,
+        // then the column's components zeroed
+        const int ao0 = w * kWin, fill = min(kWin, a.nao - ao0);
+        for (int pp = warp; pp < kTilePts; pp += kWarps) {
+            T* const row = rowp[pp];
             if (row != nullptr && lane < fill)
-                row[a.off[e] + ao0 + lane] =
-                    static_cast<T>(a.scale[e] * static_cast<double>(st[(a.comp[e] * 32 + lane) * kTileStride + pp]));
+                for (int e = 0; e < a.nent; ++e)
+                    row[a.off[e] + ao0 + lane] =
+                        static_cast<T>(a.scale[e] * static_cast<double>(st[(a.comp[e] * kWin + lane) * kTileStride + pp]));
+#pragma unroll
+            for (int cc = 0; cc < kNComp; ++cc) st[(cc * kWin + lane) * kTileStride + pp] = T(0);
         }
-        if constexpr (tile_bufs<T, GRAD>() == 1) __syncthreads();   // the tile is refilled next
+        if constexpr (kBufs == 1) __syncthreads();   // the tile is refilled next
     }
     if (a.sumsq) {
 #pragma unroll
@@ -495,9 +709,10 @@ template <class T, bool GRAD, int LMAX, int PPT>
 void launch_axis_tile(const AxisTileArgs& a, cudaStream_t s) {
     const int64_t nb = (a.n + kTilePts - 1) / kTilePts;
     require(nb < (1ll << 31), "too many grid points for one launch");
-    constexpr size_t smem = axis_tile_smem_bytes<T, GRAD>();
+    const size_t smem = tile_smem_bytes<T, GRAD>(kTilePts, a.npieces);
+    require(smem <= 227 * 1024, "basis too large for the tiled AO evaluator's shared memory");
     auto kern = axis_tile_kernel<T, GRAD, LMAX, PPT>;
-    if constexpr (smem > 48 * 1024)
+    if (smem > 48 * 1024)
         ISDF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     kern<<<static_cast<unsigned>(nb), kTilePts / 32 * PPT * 32, smem, s>>>(a);
     ISDF_LAUNCH_CHECK();
@@ -582,6 +797,51 @@ template <> const float* coefs_of<float>(const Context& c) { return c.d_coeff; }
 
 }  // namespace
 
+void build_window_layout(Context& c) {
+    const int lanes = c.piece_lanes;
+    const int nwin = (c.nao + kWin - 1) / kWin;
+    std::vector<std::vector<int2>> per_win(nwin);
+    for (int i = 0; i < c.npieces; ++i) {
+        const int4 pc = c.h_pieces[i];
+        const ShellDesc& sh = c.shells[pc.x];
+        const int ns = 2 * sh.l + 1;
+        const int a0 = sh.ao_off + pc.y * ns, a1 = a0 + pc.z * ns;
+        for (int w = a0 / kWin; w * kWin < a1; ++w) per_win[w].push_back(make_int2(i, a0 - w * kWin));
+    }
+    // balance each window's pieces over the lanes (longest first onto the
+    // least-loaded lane) with the chunk layout's estimate of their cost
+    auto cost = [&](const int2& e) {
+        const int4 pc = c.h_pieces[e.x];
+        const ShellDesc& sh = c.shells[pc.x];
+        return 6 + sh.nprim * (2 + pc.z) + pc.z * (2 * sh.l + 1) * 3;
+    };
+    std::vector<int2> entries;
+    std::vector<int> begin;
+    for (const auto& win : per_win) {
+        std::vector<int> order(win.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = static_cast<int>(i);
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(win[x]) > cost(win[y]); });
+        std::vector<std::vector<int2>> per_lane(lanes);
+        std::vector<int> load(lanes, 0);
+        for (int i : order) {
+            const int l = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+            per_lane[l].push_back(win[i]);
+            load[l] += cost(win[i]);
+        }
+        for (int l = 0; l < lanes; ++l) {
+            begin.push_back(static_cast<int>(entries.size()));
+            entries.insert(entries.end(), per_lane[l].begin(), per_lane[l].end());
+        }
+    }
+    begin.push_back(static_cast<int>(entries.size()));
+    if (entries.empty()) entries.push_back(make_int2(0, 0));
+    c.nwin = nwin;
+    ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c.d_win_entry), entries.size() * sizeof(int2)));
+    ISDF_CUDA(cudaMemcpy(c.d_win_entry, entries.data(), entries.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    ISDF_CUDA(cudaMalloc(reinterpret_cast<void**>(&c.d_win_begin), begin.size() * sizeof(int)));
+    ISDF_CUDA(cudaMemcpy(c.d_win_begin, begin.data(), begin.size() * sizeof(int), cudaMemcpyHostToDevice));
+}
+
 template <class T>
 void eval_ao(const Context& c, const double* pts, int64_t n, T* out_val, T* out_grad,
              int64_t ld, cudaStream_t s) {
@@ -592,8 +852,8 @@ void eval_ao(const Context& c, const double* pts, int64_t n, T* out_val, T* out_
     // spread over the block; otherwise 32 points x 4 shell lanes
     const bool few = n <= 2048;
     if (!few) {
-        TileArgs a{c.d_piece_rec, c.d_piece_c64, prims_of<T>(c), c.d_piece_begin, c.d_fill,
-                   c.d_chunk_ao0, c.nchunks, pts, n, ld, out_val, out_grad, out_val != nullptr};
+        TileArgs a{c.d_piece_rec, c.d_piece_c64, prims_of<T>(c), c.d_win_entry, c.d_win_begin, c.nwin, c.nao,
+                   c.npieces, c.piece_lanes, pts, n, ld, out_val, out_grad, out_val != nullptr};
         if (out_grad) launch_tile_l<T, true>(c, a, s);
         else launch_tile_l<T, false>(c, a, s);
         return;
@@ -624,9 +884,9 @@ void eval_axis_features(const Context& c, const double* pts, const int64_t* inde
     require(nb < (1ll << 31), "too many grid points for one launch");
     const bool grad = (ax.need_mask & 0xE) != 0;
     if (n > 2048) {
-        // tiled: contiguous row stores per (axis entry, point) and K-chunk
-        AxisTileArgs ta{c.d_piece_rec, c.d_piece_c64, prims_of<T>(c), c.d_piece_begin, c.d_fill,
-                        c.d_chunk_ao0, c.nchunks, pts, index, n, weights, out, ld, sumsq, 0, {}, {}, {}};
+        // tiled: one aligned row segment per (axis entry, point) and AO window
+        AxisTileArgs ta{c.d_piece_rec, c.d_piece_c64, prims_of<T>(c), c.d_win_entry, c.d_win_begin, c.nwin, c.nao,
+                        c.npieces, pts, index, n, weights, out, ld, sumsq, 0, {}, {}, {}};
         for (int e = 0; e < ax.naxes; ++e) {
             if (ax.occ[e]) continue;
             ta.comp[ta.nent] = ax.comp[e];

@@ -131,6 +131,7 @@ struct ShellDesc {
 // Angular momentum group: a run of shells with equal l (kernels specialise on l).
 struct Context {
     int device = 0;
+    int nsm = 148;       // streaming multiprocessors of the device
     int natm = 0;
     int nao = 0;
     int nshell = 0;
@@ -161,6 +162,15 @@ struct Context {
     int2* d_ao_slot = nullptr;            // (chunk, slot) of each AO
     int* d_piece_chunk = nullptr;         // chunk of each piece (d_pieces order)
     int npieces = 0;
+    // AO-window layout of the tiled evaluators: window w covers the AOs
+    // [32w, 32w + 32), so each stored row segment is a whole, aligned run of
+    // the output row; its entries are the pieces that overlap it (a piece
+    // across a window boundary appears in both), each as (piece, offset of the
+    // piece's first AO from 32w), balanced over the producer lanes:
+    // lane j of window w owns [win_begin[w*lanes + j], win_begin[w*lanes + j + 1]).
+    int nwin = 0;
+    int2* d_win_entry = nullptr;
+    int* d_win_begin = nullptr;
     // Packed piece records of the fused kernel, in the order of d_pieces: per
     // piece three float4 -- (x_hi, y_hi, z_hi, FP32 screening exponent), (x_lo, y_lo, z_lo,
     // prim_off as bits), (l, nprim, contractions, first slot as int bits) --
@@ -195,6 +205,9 @@ void upload_shell_centres(Context& c);
 void upload_piece_records(Context& c);
 // Fills the context's K-chunk layout (defined with the projection kernel).
 void build_chunk_layout(Context& c);
+// Fills the AO-window layout from the pieces of the K-chunk layout.
+void build_window_layout(Context& c);
+constexpr int kWin = 32;   // AOs per window of the tiled evaluators
 // Producer lanes per point of the projection kernel for a basis' largest l.
 inline int piece_lanes_for_lmax(int lmax) { return lmax <= 2 ? 6 : 2; }
 

@@ -90,8 +90,8 @@ def test_ao_float32_and_device_tensor_path(small_water):
 
 @pytest.mark.parametrize("extra_l", [None, 4, 6])
 def test_ao_tiled_path_matches_point_path_and_oracle(small_water, extra_l):
-    """Grids above 2048 points take the tiled evaluator (32 points per block,
-    chunk rows stored contiguously); fewer take one point per block.  Both
+    """Grids above 2048 points take the tiled evaluator (64 points per block,
+    aligned 32-AO window rows); fewer take one point per block.  Both
     give the same values (up to the contraction of a product into an FMA,
     which may differ between kernels, and the tiled kernel's screening, which
     writes zeros for a piece whose values and gradients stay below 1e-15 at
@@ -148,6 +148,58 @@ def test_ao_tiled_path_matches_point_path_and_oracle(small_water, extra_l):
         if dt == torch.float64:
             np.testing.assert_allclose(v.cpu().numpy(), oc.eval_ao(p), rtol=1e-11, atol=1e-12)
             np.testing.assert_allclose(g.cpu().numpy(), oc.eval_ao_gradient(p), rtol=1e-11, atol=1e-12)
+
+
+@pytest.mark.parametrize("extra_l", [None, 4, 6])
+def test_ao_value_warp_form_matches_block_form_and_oracle(small_water, extra_l):
+    """Value-only launches of at least two waves (SMs x 1536 points) take the
+    warp form of the tiled evaluator (one warp per 32 points, its own bounding
+    box, no block barriers); smaller ones the block form.  Over a ragged count
+    just above that size, with a block of points far from every atom, the
+    values equal the block form's (the same points in slices below the
+    threshold: the same per-piece arithmetic, up to FMA contraction) and, in
+    FP64, the oracle's on a sample."""
+    import torch
+    from mp_isdf_b200 import capi, inputs
+    mol, pts, w = small_water
+    if extra_l is None:
+        tables = mol
+    else:
+        def shells_of(sym):
+            sh = inputs.element_shells(sym)
+            if sym == "O":
+                sh = sh + [inputs.Shell(extra_l, np.array([2.1, 0.6]), np.array([[0.7, 0.4], [0.0, 1.0]]))]
+            return sh
+        tables = inputs.build_tables(mol.symbols, mol.coords, shells_of)
+    ctx = capi.Context(tables.atm, tables.bas, tables.env)
+    oc = O.OracleContext(tables.atm, tables.bas, tables.env)
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    threshold = nsm * 1536
+    rng = np.random.default_rng(11)
+    n = threshold + 1000 + 13
+    reps = -(-n // len(pts))
+    p = (np.tile(pts, (reps, 1)) + rng.normal(scale=0.05, size=(reps * len(pts), 3)))[:n]
+    far0 = 4096
+    p[far0:far0 + 64] = mol.coords[0] + np.array([40.0, 0.0, 0.0]) + rng.normal(size=(64, 3))
+    nao = tables.nao
+    xyz = torch.tensor(p, device="cuda")
+    slab = threshold // 2   # block form
+    for dt, tol in ((torch.float64, 1e-14), (torch.float32, 1e-6)):
+        v = torch.empty(n, nao, dtype=dt, device="cuda")
+        ctx.eval_ao(xyz, v)
+        vb = torch.empty(n, nao, dtype=dt, device="cuda")
+        for s0 in range(0, n, slab):
+            part = torch.empty(min(slab, n - s0), nao, dtype=dt, device="cuda")
+            ctx.eval_ao(xyz[s0:s0 + slab].contiguous(), part)
+            vb[s0:s0 + len(part)] = part
+        torch.cuda.synchronize()
+        a, b = v.double().cpu().numpy(), vb.double().cpu().numpy()
+        scale = np.abs(b).max(axis=1, keepdims=True) + 1e-300
+        assert np.all(np.abs(a - b) <= tol * scale + 1e-15)
+        assert not v[far0:far0 + 64].any()   # far block: exact zeros
+        if dt == torch.float64:
+            sample = np.sort(rng.choice(n, 600, replace=False))
+            np.testing.assert_allclose(a[sample], oc.eval_ao(p[sample]), rtol=1e-11, atol=1e-12)
 
 
 def test_evaluate_axis_matches_oracle(water, mpi):
