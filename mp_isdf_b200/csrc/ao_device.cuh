@@ -176,7 +176,9 @@ __device__ __forceinline__ void eval_piece_group(const SphPoly<T, L, GRAD>& poly
     T R[NG], Rp[NG];
 #pragma unroll
     for (int j = 0; j < NG; ++j) { R[j] = T(0); Rp[j] = T(0); }
-#pragma unroll 2
+    // several primitives' loads and exponentials in flight (FP64 exp is a
+    // long dependent chain)
+#pragma unroll(sizeof(T) == 8 ? 4 : 2)
     for (int p = 0; p < nprim; ++p) {
         T a, cc[3];
         PackedPrim<T>::load(pr, p, a, cc);

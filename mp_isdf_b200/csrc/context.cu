@@ -554,12 +554,29 @@ __global__ void __launch_bounds__(kValWarps * 32, 6) ao_value_warp_kernel(TileAr
             const int e = base + lane;
             const int2 en = e < ee ? __ldg(a.win_entry + e) : make_int2(0, 0);
             const bool c = e < ee && ((cand[en.x >> 5] >> (en.x & 31)) & 1u);
-            for (uint32_t m = __ballot_sync(0xffffffffu, c); m != 0u; m &= m - 1u) {
-                const int k = __ffs(m) - 1;
-                const int pi = __shfl_sync(0xffffffffu, en.x, k), off = __shfl_sync(0xffffffffu, en.y, k);
-                int4 meta; int poff; double dx, dy, dz, r2;
-                if (!piece_live(a.piece_rec, a.piece_c64, cand, pi, px, py, pz, valid, meta, poff, dx, dy, dz, r2))
-                    continue;
+            // candidates one by one, the next one's record loaded while the
+            // current one is evaluated
+            uint32_t m = __ballot_sync(0xffffffffu, c);
+            int4 meta_n{}; int poff_n = 0, off_n = 0; double2 cxy_n{}, cza_n{};
+            auto fetch = [&](uint32_t mm) {
+                const int k = __ffs(mm) - 1;
+                const int pi = __shfl_sync(0xffffffffu, en.x, k);
+                off_n = __shfl_sync(0xffffffffu, en.y, k);
+                meta_n = __ldg(reinterpret_cast<const int4*>(a.piece_rec) + 3 * pi + 2);
+                poff_n = __float_as_int(__ldg(a.piece_rec + 3 * pi + 1).w);
+                cxy_n = __ldg(a.piece_c64 + 2 * pi);
+                cza_n = __ldg(a.piece_c64 + 2 * pi + 1);
+            };
+            if (m != 0u) fetch(m);
+            while (m != 0u) {
+                const int4 meta = meta_n;
+                const int poff = poff_n, off = off_n;
+                const double2 cxy = cxy_n, cza = cza_n;
+                m &= m - 1u;
+                if (m != 0u) fetch(m);
+                const double dx = px - cxy.x, dy = py - cxy.y, dz = pz - cza.x;
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                if (__all_sync(0xffffffffu, !valid || cza.y * r2 > kScreenCut)) continue;
                 WarpSink<T> sink{st, lane, off};
                 eval_piece<T, false, LMAX>(meta.x, static_cast<T>(dx), static_cast<T>(dy), static_cast<T>(dz),
                                            static_cast<T>(r2), packed_prims<T>(a.prims, poff), meta.y, meta.z, sink);
