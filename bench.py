@@ -52,6 +52,11 @@ def parse():
     ap.add_argument("--mode", choices=("auto", "sharded", "replicas"), default="auto",
                     help="N > 1: shard one cluster's grid over the ranks (auto) or run one cluster "
                          "per rank")
+    ap.add_argument("--ao-eval-points", type=int, default=0,
+                    help="time eval_ao on a contiguous slice of this many points from the middle of "
+                         "the grid instead of the whole grid (small cases for profiling; 0 = whole grid)")
+    ap.add_argument("--ao-eval-only", action="store_true",
+                    help="print only the eval_ao timings (profiling the standalone evaluator)")
     ap.add_argument("--max-points", type=int, default=0,
                     help="keep every k-th grid point so that at most this many remain "
                          "(small cases for profiling; 0 = full grid)")
@@ -272,13 +277,17 @@ def _event_time(fn, reps=2):
     return out, t
 
 
-def time_ao_eval(ctx, mol, x, hbm):
+def time_ao_eval(ctx, mol, x, hbm, points=0):
     """Standalone AO evaluation (the eval_ao / eval_ao_gradient boundary) over
-    every grid point of the workload: FP64 values (Ng, nao) and FP32 values
-    plus gradients (Ng, nao) + (3, Ng, nao), CUDA events around the last of
-    three calls.  Algorithmic bytes: the output written plus 24 B of
-    coordinates read per point; the roofline is HBM."""
+    every grid point of the workload (or a contiguous slice of `points` from
+    the middle of the grid): FP64 values (Ng, nao) and FP32 values plus
+    gradients (Ng, nao) + (3, Ng, nao), CUDA events around the last of three
+    calls.  Algorithmic bytes: the output written plus 24 B of coordinates
+    read per point; the roofline is HBM."""
     import torch
+    if 0 < points < x.shape[0]:
+        lo = (x.shape[0] - points) // 2
+        x = x[lo:lo + points].contiguous()
     n, nao = x.shape[0], mol.nao
     out = {}
     for name, dt, grad in (("fp64_values", torch.float64, False), ("fp32_values_gradients", torch.float32, True)):
@@ -519,6 +528,11 @@ def run_ours(args, rank, world, local_rank):
     forms = [args.precision] if args.precision else ["mixed", "fp64"]
     ctx = capi.Context(mol.atm, mol.bas, mol.env)
     x = torch.tensor(pts, device=dev)
+    if args.ao_eval_only:
+        if rank == 0:
+            print(json.dumps({"config": args.config,
+                              "ao_eval": time_ao_eval(ctx, mol, x, peaks()[0], args.ao_eval_points)}), flush=True)
+        return
     wt = torch.tensor(w, device=dev)
     n = len(pts)
     n_kept = int(np.count_nonzero(w))
@@ -667,7 +681,7 @@ def run_ours(args, rank, world, local_rank):
 
     ao_eval = None
     if world == 1 and not args.no_ao_eval:
-        ao_eval = time_ao_eval(ctx, mol, x, peaks()[0])
+        ao_eval = time_ao_eval(ctx, mol, x, peaks()[0], args.ao_eval_points)
 
     widened = None
     if args.widened and world == 1:

@@ -37,6 +37,10 @@ struct ProjectArgs {
     uint8_t* a_store_r;        // null, or [tile][chunk] BF16 remainder tiles x - hi - lo of that entry
     uint8_t* chunk_zero;       // null, or [tile][chunk]: 1 where the chunk was screened for the tile
     int store_axis;
+    // 1 where the axis entries read distinct components: the conversion then
+    // writes zeros back behind every staged value it reads, so a piece that is
+    // not evaluated needs no zero fill (else screened pieces are zero-filled)
+    int zero_behind;
 };
 
 struct ProjectPlan {

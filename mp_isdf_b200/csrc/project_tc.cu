@@ -51,6 +51,8 @@ constexpr uint32_t kTileA = kRows * kChunk * 2;       // bytes of one BF16 A til
 constexpr uint32_t kLboA = (kRows / 8) * 128;          // K-adjacent core matrices
 constexpr uint32_t kSboA = 128;                        // M-adjacent core matrices
 constexpr int kLiveWords = 8;          // chunk-liveness bits per tile (up to 256 chunks)
+constexpr int kCandWords = 32;         // piece-candidate bits per tile (up to 1024 pieces)
+static_assert(128 + 4 * kCandWords <= 256, "candidate bits exceed the barrier area");
 constexpr float kBoxMargin = 1e-3f;    // bohr: covers FP32 rounding of points and centres
 
 // Writes the component values of one piece into the FP32 staging buffer
@@ -152,6 +154,10 @@ project_tc_kernel(ProjectArgs args) {
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 7);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 8);
     volatile int* prod_abort = reinterpret_cast<volatile int*>(bars + 9);   // [2]
+    // pieces of the current tile that are not screened (bytes 128-255 of the
+    // barrier area: static shared memory stays within its 1 KB, so the
+    // 1 KB-aligned dynamic plan still fits)
+    uint32_t* cand_s = reinterpret_cast<uint32_t*>(bars + 16);   // [kCandWords]
     __shared__ double red[kThreads / 32][4];
     __shared__ uint32_t live_s[kLiveWords];   // chunks of the current tile that are not screened
     __shared__ float tile_box[4][6];          // per point warp: coordinate minima, maxima
@@ -178,6 +184,11 @@ project_tc_kernel(ProjectArgs args) {
         tc::mbar_init_fence();
     }
     if (warp == 0) tc::tmem_alloc(tmem_slot, kTmemCols);
+    // with zero-behind conversion the staging buffers start as zeros and stay
+    // zero wherever nothing is evaluated
+    if (args.zero_behind && warp < kMmaWarp)
+        for (uint32_t u = tid; u < 2 * SM::kStage / 16; u += kProducers)
+            reinterpret_cast<uint4*>(sStage0)[u] = make_uint4(0u, 0u, 0u, 0u);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
@@ -205,6 +216,11 @@ project_tc_kernel(ProjectArgs args) {
         bool stop = false;
         bool a_zero = false;   // the A tiles hold zeros from a screened chunk
         const bool use_live = args.piece_chunk != nullptr && nchunks <= 32 * kLiveWords;
+        const bool zb = args.zero_behind != 0;
+        // per-piece candidate bits of the tile: a piece outside them is skipped
+        // without reading its record (only with zero-behind conversion, which
+        // needs no zero fill for it)
+        const bool use_cand = use_live && zb && args.npieces <= 32 * kCandWords;
         for (int64_t tile = blockIdx.x; tile < ntiles && !stop; tile += gridDim.x, ++t) {
             const int64_t g = tile * kRows + p;
             const bool valid = g < n;
@@ -226,6 +242,7 @@ project_tc_kernel(ProjectArgs args) {
             // tiles are written as zeros.
             if (use_live) {
                 if (tid < kLiveWords) live_s[tid] = 0u;
+                if (tid < kCandWords) cand_s[tid] = 0u;
                 if (tid < kRows) {   // warps 0-3 hold each of the tile's points once
                     const float pc[3] = {pxh + pxl, pyh + pyl, pzh + pzl};
                     float lo3[3], hi3[3];
@@ -264,6 +281,7 @@ project_tc_kernel(ProjectArgs args) {
                         if (!(ch.w * (ex * ex + ey * ey + ez * ez) > static_cast<float>(kExpCut))) {
                             const int pc = __ldg(args.piece_chunk + pi);
                             atomicOr(&live_s[pc >> 5], 1u << (pc & 31));
+                            if (pi < 32 * kCandWords) atomicOr(&cand_s[pi >> 5], 1u << (pi & 31));
                         }
                     }
                 named_bar_sync(1, kProducers);
@@ -283,13 +301,14 @@ project_tc_kernel(ProjectArgs args) {
                 if (args.chunk_zero && tid == 0)
                     args.chunk_zero[static_cast<size_t>(tile) * nchunks + c] = live ? 0 : 1;
                 // 1. evaluate this chunk's pieces into the FP32 staging buffer
-                if (live)
+                if (live && !zb)
                     for (int k = (valid ? fill : 0) + lanegrp; k < kChunk; k += PPT)
 #pragma unroll
                         for (int cc = 0; cc < kNComp; ++cc) sStage[(cc * kChunk + k) * kRows + p] = 0.f;
                 float csq[4] = {0.f, 0.f, 0.f, 0.f};
                 if (valid && live) {
                     for (int pi = pb; pi < pe; ++pi) {
+                        if (use_cand && !((cand_s[pi >> 5] >> (pi & 31)) & 1u)) continue;   // warp-uniform
                         // one packed record per piece: centre (hi, lo), smallest exponent,
                         // primitive offset, l, primitive and contraction counts, first slot
                         const float4 ch = __ldg(args.piece_rec + 3 * pi), cl = __ldg(args.piece_rec + 3 * pi + 1);
@@ -306,7 +325,8 @@ project_tc_kernel(ProjectArgs args) {
                         // bounds carry that as an absolute term); taken only for the
                         // whole warp, so the evaluation does not split
                         if (__all_sync(__activemask(), ch.w * r2 > static_cast<float>(kExpCut))) {
-                            for (int k = slot0; k < slot0 + nc * ns; ++k)
+                            if (!zb)
+                                for (int k = slot0; k < slot0 + nc * ns; ++k)
 #pragma unroll
                                 for (int cc = 0; cc < kNComp; ++cc) sStage[(cc * kChunk + k) * kRows + p] = 0.f;
                             continue;
@@ -353,6 +373,9 @@ project_tc_kernel(ProjectArgs args) {
                     float x[8];
 #pragma unroll
                     for (int i = 0; i < 8; ++i) x[i] = sStage[(slot * kChunk + kg * 8 + i) * kRows + row];
+                    if (zb)
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) sStage[(slot * kChunk + kg * 8 + i) * kRows + row] = 0.f;
                     uint4 hi, lo;
                     split8(x, hi, lo);
                     const uint32_t off = tc::interleaved_offset(row, kg * 8, kLboA, kSboA);
@@ -737,6 +760,10 @@ void project_tc(const Context& c, const ProjectPlan& pl, const double* pts, cons
     a.wimg = reinterpret_cast<const uint8_t*>(pl.wimg.get());
     a.comp_mask = pl.comp_mask;
     for (int i = 0; i < pl.nax; ++i) a.axis_comp[i] = pl.axis_comp[i];
+    a.zero_behind = 1;
+    for (int i = 0; i < pl.nax; ++i)
+        for (int j = 0; j < i; ++j)
+            if (pl.axis_comp[i] == pl.axis_comp[j]) a.zero_behind = 0;
     a.out = out;
     a.ld_out = ld_out;
     a.col_stride = col_stride;
