@@ -450,6 +450,14 @@ void fit_impl(isdf_ctx* ctx, const double* xyz, const double* w, int64_t ng, con
     } else {
         o = isdf::fit_grid(c, xyz, w, kp, f, theta, kp.n, have, s);
     }
+    if (!have && theta && k > 0 && kp.n > 0 && kp.spatial()) {
+        // the selection's spatial point order: Theta's columns back to the
+        // ascending kept order of the interface
+        isdf::DeviceBuffer<double> tmp(static_cast<size_t>(k * kp.n), s);
+        isdf::unpermute_columns(theta, tmp.get(), kp.n, k, kp.rank.get(), 0, kp.n, s);
+        ISDF_CUDA(cudaMemcpyAsync(theta, tmp.get(), static_cast<size_t>(k * kp.n) * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, s));
+    }
     const double el2 = std::sqrt(o.err2);
     const double erel = o.exact2 ? el2 / std::sqrt(o.exact2) : (el2 == 0 ? 0.0 : INFINITY);
     if (info) {
@@ -591,13 +599,23 @@ int isdf_select_fit_host(isdf_ctx* ctx, const isdf_select_args* args, const doub
         // are copied out on a second stream while the next chunk is fitted; if
         // the mixed Theta is then rejected (FP64 recompute), it is copied again.
         ChunkCopies cp;
+        // a spatial kept order (whole windows per chunk): each chunk's columns
+        // go back to ascending order in a staging copy before they leave
+        isdf::DeviceBuffer<double> dt_asc;
+        if (keep.valid && keep.kp.spatial() && np > 0)
+            dt_asc.reset(static_cast<size_t>(np * keep.kp.n), s);
         isdf::FitChunkHook hook = [&](int64_t g0, int64_t m) {
             const int64_t n = keep.kp.n;
+            const double* src = dt.get();
+            if (dt_asc.get()) {
+                isdf::unpermute_columns(dt.get(), dt_asc.get(), n, np, keep.kp.rank.get(), g0, m, s);
+                src = dt_asc.get();
+            }
             cp.begin();
             cudaEvent_t ev = cp.event();
             ISDF_CUDA(cudaEventRecord(ev, s));
             ISDF_CUDA(cudaStreamWaitEvent(cp.stream, ev, 0));
-            ISDF_CUDA(cudaMemcpy2DAsync(theta_host + g0, n * sizeof(double), dt.get() + g0, n * sizeof(double),
+            ISDF_CUDA(cudaMemcpy2DAsync(theta_host + g0, n * sizeof(double), src + g0, n * sizeof(double),
                                         m * sizeof(double), np, cudaMemcpyDeviceToHost, cp.stream));
         };
         const bool stream_out = theta_host && np > 0 && keep.valid;

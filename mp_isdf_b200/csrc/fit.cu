@@ -762,7 +762,10 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
     // 128-point tiles, each at least two waves of the stored-tile GEMM.
     const int64_t ntiles = (n + 127) / 128;
     const int64_t nchunk = (ao_tiles && on_chunk) ? std::max<int64_t>(1, std::min<int64_t>(4, ntiles / 296)) : 1;
-    const int64_t per = (ntiles + nchunk - 1) / nchunk * 128;
+    int64_t per = (ntiles + nchunk - 1) / nchunk * 128;
+    // chunks of whole windows of a spatial order, so that each chunk's Theta
+    // columns can be put back in ascending order on their own
+    if (kp.spatial()) per = (per + kSpatialWindow - 1) / kSpatialWindow * kSpatialWindow;
     const size_t smem = static_cast<size_t>(2 * k * k + k) * sizeof(double);
     auto kern = k <= 16 ? fit_mixed_kernel<16> : k <= 32 ? fit_mixed_kernel<32> : fit_mixed_kernel<64>;
     const double trunc = kScreenFp32 * std::sqrt(static_cast<double>(c.nao));

@@ -8,16 +8,35 @@
 namespace isdf {
 
 struct KeptPoints {
-    DeviceBuffer<int64_t> index;  // original indices of nonzero-weight points, ascending
+    // original indices of the nonzero-weight points: ascending, or, when
+    // `rank` is set, ascending between windows of kSpatialWindow positions
+    // and in spatial (Morton) order inside each window
+    DeviceBuffer<int64_t> index;
+    DeviceBuffer<int64_t> rank;   // empty, or the ascending position of each position
     int64_t n = 0;
+    bool spatial() const { return rank.get() != nullptr; }
 };
+
+// Positions per window of the spatial order (whole 128-point tiles).  A
+// window holds the same points in both orders, so position ranges made of
+// whole windows can be mapped back to ascending order on their own.
+constexpr int64_t kSpatialWindow = 32768;
 
 // Flags non-finite weights (always) and non-finite coordinates of kept points,
 // and compacts the nonzero-weight points in their original order.  With an
 // importance vector (density sketches) every entry must be finite and
-// nonnegative, and points of zero importance are dropped too.
+// nonnegative, and points of zero importance are dropped too.  With `spatial`
+// the points inside each window of kSpatialWindow positions are then ordered
+// by the Morton code of their 1-bohr cell, so that consecutive points (the
+// 32-point warps and 128-point tiles of the evaluators) lie close together
+// and screen more pieces; `rank` maps positions back to ascending order.
 KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStream_t s,
-                          const double* importance = nullptr);
+                          const double* importance = nullptr, bool spatial = false);
+
+// dst[a*ld + rank[p]] = src[a*ld + p] for the k rows and positions
+// [p0, p0 + m), a range of whole windows (dst and src distinct).
+void unpermute_columns(const double* src, double* dst, int64_t ld, int64_t k, const int64_t* rank, int64_t p0,
+                       int64_t m, cudaStream_t s);
 
 struct SelectOptions {
     int algorithm = 0;               // LocalAnchorSelectionAlgorithm code

@@ -61,10 +61,59 @@ __global__ void flag_points_kernel(const double* __restrict__ pts, const double*
         atomicOr(bad, 2);
 }
 
+// 16 bits of v spread to every third bit
+__device__ __forceinline__ uint64_t spread3(uint64_t v) {
+    v &= 0xffffull;
+    v = (v | v << 16) & 0x0000ff0000ffull;
+    v = (v | v << 8) & 0x00f00f00f00full;
+    v = (v | v << 4) & 0x0c30c30c30c3ull;
+    v = (v | v << 2) & 0x249249249249ull;
+    return v;
+}
+
+// key of position i: window (i / kSpatialWindow) above the Morton code of the
+// point's 1-bohr cell (16 bits per axis, cells offset by 2^15); the value is i
+__global__ void spatial_key_kernel(const double* __restrict__ pts, const int64_t* __restrict__ index, int64_t n,
+                                   uint64_t* __restrict__ key, int64_t* __restrict__ val) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t g = index[i];
+    uint64_t m = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double c = floor(pts[3 * g + d]) + 32768.0;
+        const uint64_t q = c < 0.0 ? 0ull : c > 65535.0 ? 65535ull : static_cast<uint64_t>(c);
+        m |= spread3(q) << d;
+    }
+    key[i] = (static_cast<uint64_t>(i / kSpatialWindow) << 48) | m;
+    val[i] = i;
+}
+
+__global__ void gather_index_kernel(const int64_t* __restrict__ asc, const int64_t* __restrict__ perm, int64_t n,
+                                    int64_t* __restrict__ out) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = asc[perm[i]];
+}
+
+__global__ void unpermute_columns_kernel(const double* __restrict__ src, double* __restrict__ dst, int64_t ld,
+                                         int64_t k, const int64_t* __restrict__ rank, int64_t p0, int64_t m) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const int64_t p = p0 + i, r = rank[p];
+    for (int64_t a = 0; a < k; ++a) dst[a * ld + r] = src[a * ld + p];
+}
+
 }  // namespace
 
+void unpermute_columns(const double* src, double* dst, int64_t ld, int64_t k, const int64_t* rank, int64_t p0,
+                       int64_t m, cudaStream_t s) {
+    if (m <= 0 || k <= 0) return;
+    unpermute_columns_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, s>>>(src, dst, ld, k, rank, p0, m);
+    ISDF_LAUNCH_CHECK();
+}
+
 KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStream_t s,
-                          const double* importance) {
+                          const double* importance, bool spatial) {
     KeptPoints kp;
     kp.index.reset(std::max<int64_t>(n, 1), s);
     if (n == 0) return kp;
@@ -92,6 +141,26 @@ KeptPoints compact_points(const double* pts, const double* w, int64_t n, cudaStr
     if (hbad & 1) fail(kInvalid, "grid weights must be finite");
     if (hbad & 2) fail(kInvalid, "grid coordinates must be finite");
     kp.n = hcount;
+    if (spatial && hcount > 128 && hcount < (int64_t(1) << 31)) {
+        // Morton order inside each window: (key, position) pairs sorted by key
+        const int64_t m = hcount;
+        DeviceBuffer<uint64_t> key(m, s), key2(m, s);
+        DeviceBuffer<int64_t> val(m, s), perm(m, s), index(m, s);
+        const unsigned nb = static_cast<unsigned>((m + 255) / 256);
+        spatial_key_kernel<<<nb, 256, 0, s>>>(pts, kp.index.get(), m, key.get(), val.get());
+        ISDF_LAUNCH_CHECK();
+        size_t sort_bytes = 0;
+        ISDF_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, key.get(), key2.get(), val.get(), perm.get(),
+                                                  static_cast<int>(m), 0, 64, s));
+        DeviceBuffer<char> sort_tmp(sort_bytes, s);
+        ISDF_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp.get(), sort_bytes, key.get(), key2.get(), val.get(),
+                                                  perm.get(), static_cast<int>(m), 0, 64, s));
+        count_launches(8);   // the sort's passes (upper bound)
+        gather_index_kernel<<<nb, 256, 0, s>>>(kp.index.get(), perm.get(), m, index.get());
+        ISDF_LAUNCH_CHECK();
+        kp.index = std::move(index);
+        kp.rank = std::move(perm);
+    }
     return kp;
 }
 
@@ -1128,7 +1197,10 @@ std::vector<int64_t> select_rand_sketch(const Context& c, const double* pts, con
     KeptPoints kp;
     {
         ISDF_PROFILE("phase:compact", s);
-        kp = compact_points(pts, w, ng, s, density ? o.importance : nullptr);
+        // the sketch evaluates the kept points in spatial order (the pivots
+        // are mapped back through the index; a kept mixed fit restores Theta's
+        // ascending column order)
+        kp = compact_points(pts, w, ng, s, density ? o.importance : nullptr, !density);
     }
     int64_t n = kp.n;
     if (n == 0) {

@@ -268,7 +268,10 @@ def test_cuda_adjoint_two_shards_match_single_call():
         for e, g in results:
             np.testing.assert_allclose(e, e_ref, rtol=1e-12)
             if want_grad:
-                np.testing.assert_allclose(g, g_ref, rtol=0, atol=1e-11 * np.abs(g_ref).max())
+                # the per-atom terms are FP64 atomic sums in an order that
+                # varies between runs, and the gradient is a small difference
+                # of large terms: 1e-10 of the largest component, as above
+                np.testing.assert_allclose(g, g_ref, rtol=0, atol=1e-10 * np.abs(g_ref).max())
             else:
                 assert not g.any()
 
