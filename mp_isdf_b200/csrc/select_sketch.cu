@@ -662,6 +662,59 @@ combine_sketch_tiled_kernel(const double* __restrict__ P, int naxes, int64_t ell
     if (!ok) atomicOr(bad, 1);
 }
 
+// Two-buffer pipeline between the stream s and a side stream: work item i
+// runs its producer on side(i), which first waits until s has consumed item
+// i - 2 (same buffer); hand_back(i) makes s wait for that producer, and
+// consumed(i) marks the point on s after which buffer i % 2 is free again.
+// Without `on` everything stays on s.  join() makes s wait for the side
+// stream, so stream-ordered frees on s come after its last use.
+class StreamPair {
+public:
+    StreamPair(cudaStream_t s, bool on) : s_(s), on_(on) {
+        if (!on_) return;
+        ISDF_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+        for (auto& e : ev_) ISDF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ISDF_CUDA(cudaEventRecord(ev_[4], s_));          // everything enqueued on s so far
+        ISDF_CUDA(cudaStreamWaitEvent(side_, ev_[4], 0));
+    }
+    cudaStream_t side(int64_t i) {
+        if (!on_) return s_;
+        if (i >= 2) ISDF_CUDA(cudaStreamWaitEvent(side_, ev_[2 + (i & 1)], 0));
+        return side_;
+    }
+    void hand_back(int64_t i) {
+        if (!on_) return;
+        ISDF_CUDA(cudaEventRecord(ev_[i & 1], side_));
+        ISDF_CUDA(cudaStreamWaitEvent(s_, ev_[i & 1], 0));
+    }
+    void consumed(int64_t i) {
+        if (on_) ISDF_CUDA(cudaEventRecord(ev_[2 + (i & 1)], s_));
+    }
+    void join() {
+        if (!on_ || joined_) return;
+        ISDF_CUDA(cudaEventRecord(ev_[4], side_));
+        ISDF_CUDA(cudaStreamWaitEvent(s_, ev_[4], 0));
+        joined_ = true;
+    }
+    ~StreamPair() {
+        if (!on_) return;
+        if (!joined_) {   // an error path: let the side stream drain first
+            cudaEventRecord(ev_[4], side_);
+            cudaStreamWaitEvent(s_, ev_[4], 0);
+        }
+        cudaStreamSynchronize(side_);
+        for (auto e : ev_) cudaEventDestroy(e);
+        cudaStreamDestroy(side_);
+    }
+    StreamPair(const StreamPair&) = delete;
+    StreamPair& operator=(const StreamPair&) = delete;
+
+private:
+    cudaStream_t s_, side_ = nullptr;
+    bool on_, joined_ = false;
+    cudaEvent_t ev_[5] = {};
+};
+
 }  // namespace
 
 void sketch_fp64(const Context& c, const double* pts, const KeptPoints& kp, const double* w,
@@ -685,24 +738,37 @@ void sketch_fp64(const Context& c, const double* pts, const KeptPoints& kp, cons
     DeviceBuffer<double> sumsq(5, s);
     sumsq.zero(s);
     chunk = std::max<int64_t>(1, std::min(chunk, n));
-    DeviceBuffer<double> F(static_cast<size_t>(chunk * d), s);
     bool uniform = true;   // every entry nao wide: one batched GEMM
     for (int a = 0; a < naxes; ++a) uniform = uniform && ax.width[a] == c.nao && ax.offset[a] == a * c.nao;
-    for (int64_t g0 = 0; g0 < n; g0 += chunk) {
+    // The feature evaluation of chunk i + 1 runs on a second stream while the
+    // DMMA GEMM of chunk i runs on s, from two feature buffers: both kernels
+    // leave most of an SM idle (the evaluator is latency-bound at 24 warps per
+    // SM, the GEMM has 4 warps per block), and one block of each fits an SM.
+    const int nbuf = n > chunk ? 2 : 1;
+    DeviceBuffer<double> F[2];
+    for (int i = 0; i < nbuf; ++i) F[i].reset(static_cast<size_t>(chunk * d), s);
+    StreamPair sp(s, nbuf == 2);
+    int64_t i = 0;
+    for (int64_t g0 = 0; g0 < n; g0 += chunk, ++i) {
         const int64_t b = std::min(chunk, n - g0);
-        eval_axis_features<double>(c, pts, kp.index.get() + g0, b, ax, F.get(), d,
-                                   naxes > 1 ? sumsq.get() : nullptr, nullptr, s);
+        double* Fi = F[i % nbuf].get();
+        cudaStream_t se = sp.side(i);   // waits for the GEMM that last read this buffer
+        eval_axis_features<double>(c, pts, kp.index.get() + g0, b, ax, Fi, d,
+                                   naxes > 1 ? sumsq.get() : nullptr, nullptr, se);
+        sp.hand_back(i);                // s waits for these features
         // per-axis partial projections P[g][a][0..2ell)
         if (uniform) {
-            gemm_f64(b, 2 * ell, c.nao, F.get(), d, c.nao, W.get(), 2 * ell, c.nao * 2 * ell,
+            gemm_f64(b, 2 * ell, c.nao, Fi, d, c.nao, W.get(), 2 * ell, c.nao * 2 * ell,
                      P.get() + g0 * naxes * 2 * ell, naxes * 2 * ell, 2 * ell, naxes, false, s);
         } else {
             for (int a = 0; a < naxes; ++a)
-                gemm_f64(b, 2 * ell, ax.width[a], F.get() + ax.offset[a], d, 0,
+                gemm_f64(b, 2 * ell, ax.width[a], Fi + ax.offset[a], d, 0,
                          W.get() + static_cast<int64_t>(ax.offset[a]) * 2 * ell, 2 * ell, 0,
                          P.get() + g0 * naxes * 2 * ell + a * 2 * ell, naxes * 2 * ell, 0, 1, false, s);
         }
+        sp.consumed(i);                 // the buffer may be refilled after this GEMM
     }
+    sp.join();
     DeviceBuffer<double> dscales;
     if (naxes > 1) {
         double h[5];
