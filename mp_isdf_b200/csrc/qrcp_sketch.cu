@@ -50,7 +50,16 @@ struct QrState {
     unsigned long long* lb_bits;  // best lower bound max(sqrt(est) - delta, 0), as its bits
     int64_t* count;               // candidates of this step
     ArgKey* xpartial;             // per re-verification block
+    // per update block (kQrThreads columns), verified mode: the largest upper
+    // bound sqrt(est) + delta of its inexact columns (-1 if none) and the best
+    // argmax key of its exact columns, so the candidate scan can pass over a
+    // block that holds no candidate without reading its columns
+    double* seg_ub;
+    ArgKey* seg_key;
 };
+
+// Update blocks that one block of the candidate scan covers.
+constexpr int kCandSegs = 16;
 
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
@@ -72,6 +81,7 @@ __global__ void __launch_bounds__(kQrThreads) qr_update_kernel(QrState st, int64
     __shared__ ArgKey ksh[kQrThreads / 32];
     __shared__ double esh[kQrThreads / 32];
     __shared__ double lsh[kQrThreads / 32];
+    __shared__ double ush[kQrThreads / 32];
     __shared__ double vsh[kRegRows];
     extern __shared__ double xs[];   // STAGED: [kRegRows][kQrThreads]
     const int tid = threadIdx.x;
@@ -97,7 +107,7 @@ __global__ void __launch_bounds__(kQrThreads) qr_update_kernel(QrState st, int64
         __syncthreads();
     }
     ArgKey key = key_none();
-    double e = 0.0, lb = 0.0;
+    double e = 0.0, lb = 0.0, ub = -1.0;
     if (active) {
         const double t = j > 0 ? st.tau[j - 1] : 0.0;
         double nrm = 0;
@@ -145,7 +155,10 @@ __global__ void __launch_bounds__(kQrThreads) qr_update_kernel(QrState st, int64
         if (j < m) {
             if (verified) {
                 st.est[g] = nrm;
-                lb = fmax(sqrt(nrm) - st.delta[g], 0.0);
+                const double d = st.delta[g], r = sqrt(nrm);
+                lb = fmax(r - d, 0.0);
+                if (d > 0.0) ub = r + d;
+                else key = ArgKey{nrm, st.pos[g], g};   // exact column
             } else {
                 key = ArgKey{nrm, st.pos[g], g};
             }
@@ -153,16 +166,22 @@ __global__ void __launch_bounds__(kQrThreads) qr_update_kernel(QrState st, int64
     }
     e = warp_sum(e);
     lb = warp_max(lb);
-    if (tid % 32 == 0) { esh[tid / 32] = e; lsh[tid / 32] = lb; }
+    ub = warp_max(ub);
+    if (tid % 32 == 0) { esh[tid / 32] = e; lsh[tid / 32] = lb; ush[tid / 32] = ub; }
+    // verified: a block key only where the block holds an exact column (rare)
     ArgKey best = key_none();
-    if (!verified) best = block_best<kQrThreads>(key, ksh);
-    else __syncthreads();
+    if (!verified || __syncthreads_or(key.col >= 0)) best = block_best<kQrThreads>(key, ksh);
     if (tid == 0) {
-        double et = 0, lt = 0.0;
-        for (int i = 0; i < kQrThreads / 32; ++i) { et += esh[i]; lt = fmax(lt, lsh[i]); }
+        double et = 0, lt = 0.0, ut = -1.0;
+        for (int i = 0; i < kQrThreads / 32; ++i) { et += esh[i]; lt = fmax(lt, lsh[i]); ut = fmax(ut, ush[i]); }
         if (j > 0 && et != 0.0) atomicAdd(&st.energy[j - 1], et);
-        if (!verified) st.partial[blockIdx.x] = best;
-        else if (lt > 0.0) atomicMax(st.lb_bits, static_cast<unsigned long long>(__double_as_longlong(lt)));
+        if (!verified) {
+            st.partial[blockIdx.x] = best;
+        } else {
+            st.seg_ub[blockIdx.x] = ut;
+            st.seg_key[blockIdx.x] = best;
+            if (lt > 0.0) atomicMax(st.lb_bits, static_cast<unsigned long long>(__double_as_longlong(lt)));
+        }
     }
 }
 
@@ -177,6 +196,7 @@ __global__ void __launch_bounds__(kPairThreads) qr_update_pairs_kernel(QrState s
     __shared__ ArgKey ksh[kPairThreads / 32];
     __shared__ double esh[kPairThreads / 32];
     __shared__ double lsh[kPairThreads / 32];
+    __shared__ double ush[kPairThreads / 32];
     __shared__ double vsh[kRegRows];
     extern __shared__ __align__(16) double xs[];   // [rows][kQrThreads], columns 2 tid and 2 tid + 1
     const int tid = threadIdx.x;
@@ -202,7 +222,7 @@ __global__ void __launch_bounds__(kPairThreads) qr_update_pairs_kernel(QrState s
     asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
     ArgKey key = key_none();
-    double e = 0.0, lb = 0.0;
+    double e = 0.0, lb = 0.0, ub = -1.0;
     if (act[0] || act[1]) {
         const double t = j > 0 ? st.tau[j - 1] : 0.0;
         const double* x = xs + 2 * tid;
@@ -245,7 +265,14 @@ __global__ void __launch_bounds__(kPairThreads) qr_update_pairs_kernel(QrState s
                 const int64_t g = g0 + c;
                 if (verified) {
                     st.est[g] = nrm[c];
-                    lb = fmax(lb, fmax(sqrt(nrm[c]) - st.delta[g], 0.0));
+                    const double d = st.delta[g], r = sqrt(nrm[c]);
+                    lb = fmax(lb, fmax(r - d, 0.0));
+                    if (d > 0.0) {
+                        ub = fmax(ub, r + d);
+                    } else {   // exact column
+                        const ArgKey k{nrm[c], st.pos[g], g};
+                        if (key_better(k, key)) key = k;
+                    }
                 } else {
                     const ArgKey k{nrm[c], st.pos[g], g};
                     if (key_better(k, key)) key = k;
@@ -255,16 +282,22 @@ __global__ void __launch_bounds__(kPairThreads) qr_update_pairs_kernel(QrState s
     }
     e = warp_sum(e);
     lb = warp_max(lb);
-    if (tid % 32 == 0) { esh[tid / 32] = e; lsh[tid / 32] = lb; }
+    ub = warp_max(ub);
+    if (tid % 32 == 0) { esh[tid / 32] = e; lsh[tid / 32] = lb; ush[tid / 32] = ub; }
+    // verified: a block key only where the block holds an exact column (rare)
     ArgKey best = key_none();
-    if (!verified) best = block_best<kPairThreads>(key, ksh);
-    else __syncthreads();
+    if (!verified || __syncthreads_or(key.col >= 0)) best = block_best<kPairThreads>(key, ksh);
     if (tid == 0) {
-        double et = 0, lt = 0.0;
-        for (int i = 0; i < kPairThreads / 32; ++i) { et += esh[i]; lt = fmax(lt, lsh[i]); }
+        double et = 0, lt = 0.0, ut = -1.0;
+        for (int i = 0; i < kPairThreads / 32; ++i) { et += esh[i]; lt = fmax(lt, lsh[i]); ut = fmax(ut, ush[i]); }
         if (j > 0 && et != 0.0) atomicAdd(&st.energy[j - 1], et);
-        if (!verified) st.partial[blockIdx.x] = best;
-        else if (lt > 0.0) atomicMax(st.lb_bits, static_cast<unsigned long long>(__double_as_longlong(lt)));
+        if (!verified) {
+            st.partial[blockIdx.x] = best;
+        } else {
+            st.seg_ub[blockIdx.x] = ut;
+            st.seg_key[blockIdx.x] = best;
+            if (lt > 0.0) atomicMax(st.lb_bits, static_cast<unsigned long long>(__double_as_longlong(lt)));
+        }
     }
 }
 
@@ -273,24 +306,37 @@ __global__ void __launch_bounds__(kPairThreads) qr_update_pairs_kernel(QrState s
 // columns enter the per-block argmax keys directly.  A column that is neither
 // cannot win: its estimate is below (sqrt(e) + delta)^2 < lb^2, and the column
 // that sets lb is a candidate or exact with a norm of at least lb.
-__global__ void __launch_bounds__(kQrThreads) candidates_kernel(QrState st, int64_t* cand) {
+// A block covers kCandSegs update blocks; one whose largest upper bound is
+// below lb holds no candidate, and its exact columns' best key is the one the
+// update left, so its columns are not read.
+__global__ void __launch_bounds__(kQrThreads) candidates_kernel(QrState st, int64_t* cand, int nseg) {
     __shared__ ArgKey ksh[kQrThreads / 32];
-    const int64_t g = static_cast<int64_t>(blockIdx.x) * kQrThreads + threadIdx.x;
     const double lb = __longlong_as_double(static_cast<long long>(*st.lb_bits));
     ArgKey key = key_none();
-    if (g < st.n && !st.selected[g]) {
-        const double d = st.delta[g], e = st.est[g];
-        if (d > 0.0 && sqrt(e) + d >= lb) {
-            const int64_t i = static_cast<int64_t>(
-                atomicAdd(reinterpret_cast<unsigned long long*>(st.count), 1ull));
-            cand[i] = g;
-        } else if (!(d > 0.0)) {
-            key = ArgKey{e, st.pos[g], g};
+    const int s0 = blockIdx.x * kCandSegs, s1 = min(nseg, s0 + kCandSegs);
+    for (int sg = s0; sg < s1; ++sg) {
+        if (st.seg_ub[sg] < lb) {
+            if (threadIdx.x == 0 && key_better(st.seg_key[sg], key)) key = st.seg_key[sg];
+            continue;
+        }
+        const int64_t g = static_cast<int64_t>(sg) * kQrThreads + threadIdx.x;
+        if (g < st.n && !st.selected[g]) {
+            const double d = st.delta[g], e = st.est[g];
+            if (d > 0.0 && sqrt(e) + d >= lb) {
+                const int64_t i = static_cast<int64_t>(
+                    atomicAdd(reinterpret_cast<unsigned long long*>(st.count), 1ull));
+                cand[i] = g;
+            } else if (!(d > 0.0)) {
+                const ArgKey k{e, st.pos[g], g};
+                if (key_better(k, key)) key = k;
+            }
         }
     }
     const ArgKey best = block_best<kQrThreads>(key, ksh);
     if (threadIdx.x == 0) st.partial[blockIdx.x] = best;
 }
+
+inline int cand_blocks(int nblocks) { return (nblocks + kCandSegs - 1) / kCandSegs; }
 
 // Reduce the block keys (and, verified, the re-verification blocks' keys),
 // record the pivot, swap positions, build reflector j; then clear the
@@ -427,7 +473,7 @@ __device__ void exact_projections(const ExactArgs& ea, const double* feat, doubl
 // the j previous reflectors, rows stored, squared trailing norm into est[g]
 // with a zero bound.  Returns the column's argmax key (lane 0).
 __device__ ArgKey exact_finish(const ExactArgs& ea, const QrState& st, int64_t g, int64_t j, const double* lr,
-                               double* y) {
+                               double* y, const double* vhist, const double* tau) {
     const int lane = threadIdx.x % 32;
     const int64_t m = st.m;
     const int64_t gi = ea.index[g];
@@ -435,9 +481,9 @@ __device__ ArgKey exact_finish(const ExactArgs& ea, const QrState& st, int64_t g
     for (int64_t s = lane; s < m; s += 32) y[s] = sw * lr[s] * lr[ea.ell + s];
     __syncwarp();
     for (int64_t i = 0; i < j; ++i) {
-        const double t = st.tau[i];
+        const double t = tau[i];
         if (t == 0.0) continue;
-        const double* v = st.vhist + i * m;
+        const double* v = vhist + i * m;
         double dot = 0;
         for (int64_t r = i + lane; r < m; r += 32) dot += v[r] * y[r];
         dot = warp_allsum(dot) * t;
@@ -502,8 +548,20 @@ exact_columns_kernel(ExactArgs ea, QrState st, const int64_t* cand, int64_t j, u
             if (threadIdx.x == 0) done[ci] = 0u;   // ready for the next step
             __syncthreads();
         }
+        // the j reflectors and their tau, staged by the whole block into the
+        // feature area (no longer read) when they fit, so the one warp that
+        // applies them in sequence reads shared memory
+        const double* vh = st.vhist;
+        const double* tau = st.tau;
+        if ((j + 1) * st.m <= static_cast<int64_t>(kNComp) * ea.nao) {
+            for (int64_t i = threadIdx.x; i < j * st.m; i += blockDim.x) feat[i] = st.vhist[i];
+            for (int64_t i = threadIdx.x; i < j; i += blockDim.x) feat[j * st.m + i] = st.tau[i];
+            __syncthreads();
+            vh = feat;
+            tau = feat + j * st.m;
+        }
         if (threadIdx.x < 32) {
-            const ArgKey k = exact_finish(ea, st, g, j, lr, y);
+            const ArgKey k = exact_finish(ea, st, g, j, lr, y, vh, tau);
             if (threadIdx.x == 0 && key_better(k, best)) best = k;
         }
         __syncthreads();   // feat is reused by the next item
@@ -613,8 +671,8 @@ struct QrShard::Impl {
     QrState st;
     DeviceBuffer<int64_t> pos, col_at, jpvt, cand, count;
     DeviceBuffer<char> selected;
-    DeviceBuffer<double> vhist, tau, diag, energy, est, lr_split, rows, beta;
-    DeviceBuffer<ArgKey> partial, xpartial, key;
+    DeviceBuffer<double> vhist, tau, diag, energy, est, lr_split, rows, beta, seg_ub;
+    DeviceBuffer<ArgKey> partial, xpartial, key, seg_key;
     DeviceBuffer<unsigned long long> lb_bits, reverified;
     DeviceBuffer<unsigned> done;
     bool verified = false;
@@ -666,12 +724,16 @@ QrShard::QrShard(double* Yt, int64_t ldy, int64_t m, int64_t n, int64_t pos_offs
         d.cand.reset(nn, s);
         d.count.reset(1, s);
         d.xpartial.reset(kExactBlocks, s);
+        d.seg_ub.reset(std::max(d.nblocks, 1), s);
+        d.seg_key.reset(std::max(d.nblocks, 1), s);
         d.lr_split.reset(static_cast<size_t>(kSplitCands) * 2 * exact->ell, s);
         d.done.reset(kSplitCands, s);
         d.lb_bits.zero(s);
         d.count.zero(s);
         d.done.zero(s);
         d.st.est = d.est.get();
+        d.st.seg_ub = d.seg_ub.get();
+        d.st.seg_key = d.seg_key.get();
         d.st.delta = exact->delta;
         d.st.lb_bits = d.lb_bits.get();
         d.st.count = d.count.get();
@@ -738,13 +800,14 @@ QrShardKey QrShard::verify(int64_t j, double lower_bound) {
     ISDF_CUDA(cudaMemcpyAsync(d.lb_bits.get(), &bits, sizeof(bits), cudaMemcpyHostToDevice, d.s));
     {
         ISDF_PROFILE("qrcp_sketch_verify", d.s);
-        candidates_kernel<<<d.nblocks, kQrThreads, 0, d.s>>>(d.st, d.cand.get());
+        candidates_kernel<<<cand_blocks(d.nblocks), kQrThreads, 0, d.s>>>(d.st, d.cand.get(), d.nblocks);
         ISDF_LAUNCH_CHECK();
         d.exact_kernel.fn<<<kExactBlocks, d.exact_kernel.threads, d.exact_smem, d.s>>>(
             d.ea, d.st, d.cand.get(), j, d.reverified.get(), d.lr_split.get(), d.done.get());
         ISDF_LAUNCH_CHECK();
     }
-    reduce_keys_kernel<<<1, 1024, 0, d.s>>>(d.partial.get(), d.nblocks, d.xpartial.get(), kExactBlocks, d.key.get());
+    reduce_keys_kernel<<<1, 1024, 0, d.s>>>(d.partial.get(), cand_blocks(d.nblocks), d.xpartial.get(), kExactBlocks,
+                                            d.key.get());
     ISDF_LAUNCH_CHECK();
     ISDF_CUDA(cudaMemcpyAsync(&out, d.key.get(), sizeof(out), cudaMemcpyDeviceToHost, d.s));
     ISDF_CUDA(cudaStreamSynchronize(d.s));
@@ -793,8 +856,8 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
     DeviceBuffer<char> selected(n, s);
     DeviceBuffer<double> vhist(static_cast<size_t>(m * steps), s), tau(steps, s), diag(steps, s),
         energy(steps, s);
-    DeviceBuffer<ArgKey> partial(nblocks, s), xpartial;
-    DeviceBuffer<double> est, lr_split;
+    DeviceBuffer<ArgKey> partial(nblocks, s), xpartial, seg_key;
+    DeviceBuffer<double> est, lr_split, seg_ub;
     DeviceBuffer<unsigned long long> lb_bits;
     DeviceBuffer<unsigned> done;
     DeviceBuffer<int64_t> cand, count;
@@ -814,12 +877,16 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
         cand.reset(n, s);
         count.reset(1, s);
         xpartial.reset(kExactBlocks, s);
+        seg_ub.reset(nblocks, s);
+        seg_key.reset(nblocks, s);
         lr_split.reset(static_cast<size_t>(kSplitCands) * 2 * exact->ell, s);
         done.reset(kSplitCands, s);
         lb_bits.zero(s);
         count.zero(s);
         done.zero(s);
         st.est = est.get();
+        st.seg_ub = seg_ub.get();
+        st.seg_key = seg_key.get();
         st.delta = exact->delta;
         st.lb_bits = lb_bits.get();
         st.count = count.get();
@@ -862,7 +929,7 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
         if (j == steps) break;
         if (exact) {
             ISDF_PROFILE("qrcp_sketch_verify", s);
-            candidates_kernel<<<nblocks, kQrThreads, 0, s>>>(st, cand.get());
+            candidates_kernel<<<cand_blocks(nblocks), kQrThreads, 0, s>>>(st, cand.get(), nblocks);
             ISDF_LAUNCH_CHECK();
             exact_kernel.fn<<<kExactBlocks, exact_kernel.threads, exact_smem, s>>>(
                 ea, st, cand.get(), j, reverified_d.get(), lr_split.get(), done.get());
@@ -870,7 +937,9 @@ SketchQR qrcp_sketch(double* Yt, int64_t ldy, int64_t m, int64_t n, cudaStream_t
         }
         {
             ISDF_PROFILE("qrcp_sketch_pivot", s);
-            qr_pivot_kernel<<<1, 1024, 0, s>>>(st, j, nblocks, exact ? kExactBlocks : 0);
+            // verified: one key per candidate-scan block, else one per update block
+            qr_pivot_kernel<<<1, 1024, 0, s>>>(st, j, exact ? cand_blocks(nblocks) : nblocks,
+                                               exact ? kExactBlocks : 0);
             ISDF_LAUNCH_CHECK();
         }
     }
