@@ -34,6 +34,7 @@
 #include <functional>
 #include <thread>
 #include <unistd.h>
+#include <immintrin.h>
 
 namespace isdf {
 
@@ -361,12 +362,12 @@ private:
         const uint64_t y = (cur & kUpper) | (next & kLower);
         return far ^ (y >> 1) ^ ((uint64_t(0) - (y & 1)) & 0xb5026f5aa96619e9ULL);
     }
-    __attribute__((optimize("O3"))) void transition() {
+    __attribute__((optimize("O3"), target_clones("avx2", "default"))) void transition() {
         for (int i = 0; i < kN - kM; ++i) x_[i] = twist(x_[i], x_[i + 1], x_[i + kM]);
         for (int i = kN - kM; i < kN - 1; ++i) x_[i] = twist(x_[i], x_[i + 1], x_[i + kM - kN]);
         x_[kN - 1] = twist(x_[kN - 1], x_[0], x_[kM - 1]);
     }
-    __attribute__((optimize("O3"))) void temper(uint64_t* out) const {
+    __attribute__((optimize("O3"), target_clones("avx2", "default"))) void temper(uint64_t* out) const {
         for (int i = 0; i < kN; ++i) {
             uint64_t z = x_[i];
             z ^= (z >> 29) & 0x5555555555555555ULL;
@@ -445,6 +446,52 @@ private:
     uint64_t gen_ = 0;
 };
 
+// Accepted attempts among the 2 * attempts engine outputs at raw.
+int64_t polar_accepted(const uint64_t* raw, int64_t attempts) {
+    int64_t n_ok = 0;
+    for (int64_t a = 0; a < attempts; ++a) {
+        const double x = 2.0 * canonical53(raw[2 * a]) - 1.0;
+        const double y = 2.0 * canonical53(raw[2 * a + 1]) - 1.0;
+        const double r2 = x * x + y * y;
+        n_ok += (r2 <= 1.0) & (r2 != 0.0);
+    }
+    return n_ok;
+}
+
+// The same count, four attempts per step.  Each operation is the scalar
+// one's: the 64-bit output becomes a double through its two exactly converted
+// 32-bit halves (each placed in the mantissa of 2^84 or 2^52 and that power
+// subtracted) added with one rounding, then 2u - 1 and x^2 + y^2 by separate
+// multiplies and adds (the target has no FMA), so the count is identical.
+// 2 canonical53(r) - 1 for four outputs.
+__attribute__((target("avx2"))) inline __m256d centred_avx2(__m256i r) {
+    const __m256d hi = _mm256_sub_pd(
+        _mm256_castsi256_pd(_mm256_or_si256(_mm256_srli_epi64(r, 32), _mm256_set1_epi64x(0x4530000000000000LL))),
+        _mm256_set1_pd(0x1p84));
+    const __m256d lo = _mm256_sub_pd(
+        _mm256_castsi256_pd(_mm256_or_si256(_mm256_and_si256(r, _mm256_set1_epi64x(0xffffffffLL)),
+                                            _mm256_set1_epi64x(0x4330000000000000LL))),
+        _mm256_set1_pd(0x1p52));
+    // the largest double below 1 where the rounded value is 1
+    const __m256d u = _mm256_min_pd(_mm256_mul_pd(_mm256_add_pd(hi, lo), _mm256_set1_pd(0x1p-64)),
+                                    _mm256_set1_pd(0x1.fffffffffffffp-1));
+    return _mm256_sub_pd(_mm256_mul_pd(_mm256_set1_pd(2.0), u), _mm256_set1_pd(1.0));
+}
+
+__attribute__((target("avx2"))) int64_t polar_accepted_avx2(const uint64_t* raw, int64_t attempts) {
+    const __m256d one = _mm256_set1_pd(1.0), zero = _mm256_setzero_pd();
+    int64_t n_ok = 0, a = 0;
+    for (; a + 4 <= attempts; a += 4) {
+        // (x0 y0 x1 y1), (x2 y2 x3 y3) -> x_i^2 + y_i^2 for i = 0, 2, 1, 3
+        const __m256d t0 = centred_avx2(_mm256_loadu_si256(reinterpret_cast<const __m256i*>(raw + 2 * a)));
+        const __m256d t1 = centred_avx2(_mm256_loadu_si256(reinterpret_cast<const __m256i*>(raw + 2 * a + 4)));
+        const __m256d r2 = _mm256_hadd_pd(_mm256_mul_pd(t0, t0), _mm256_mul_pd(t1, t1));
+        const __m256d ok = _mm256_and_pd(_mm256_cmp_pd(r2, one, _CMP_LE_OQ), _mm256_cmp_pd(r2, zero, _CMP_NEQ_UQ));
+        n_ok += __builtin_popcount(static_cast<unsigned>(_mm256_movemask_pd(ok)));
+    }
+    return n_ok + polar_accepted(raw + 2 * a, attempts - a);
+}
+
 struct PolarDraws {
     std::vector<uint64_t> raw;        // two engine outputs per attempt
     std::vector<int64_t> block_out;   // deviates produced before each block
@@ -460,19 +507,13 @@ struct PolarDraws {
 // which are then all consumed.
 Mt64Blocks polar_draw(uint64_t seed, int64_t pairs, int64_t max_blocks, PolarDraws& pd) {
     Mt64Blocks gen(seed);
+    static const bool avx2 = __builtin_cpu_supports("avx2");
     int64_t acc = 0, b = 0;
     pd.block_out[0] = 0;
     while (acc < pairs && b < max_blocks) {
         const uint64_t* raw = pd.raw.data() + 2 * b * kPolarBlock;
         gen.fill(pd.raw.data() + 2 * b * kPolarBlock, 2 * kPolarBlock);
-        int64_t n_ok = 0;
-        for (int64_t a = 0; a < kPolarBlock; ++a) {
-            const double x = 2.0 * canonical53(raw[2 * a]) - 1.0;
-            const double y = 2.0 * canonical53(raw[2 * a + 1]) - 1.0;
-            const double r2 = x * x + y * y;
-            n_ok += (r2 <= 1.0) & (r2 != 0.0);
-        }
-        acc += n_ok;
+        acc += avx2 ? polar_accepted_avx2(raw, kPolarBlock) : polar_accepted(raw, kPolarBlock);
         pd.block_out[b + 1] = 2 * acc;
         pd.published.store(++b, std::memory_order_release);
     }

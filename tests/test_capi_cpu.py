@@ -91,7 +91,7 @@ def test_inputs_generator_shapes():
     assert tables.nao == 1536
 
 
-@pytest.mark.parametrize("d,ell,seed", [(1, 1, 0), (7, 3, 11), (96, 12, 2), (6144, 26, 7)])
+@pytest.mark.parametrize("d,ell,seed", [(1, 1, 0), (7, 3, 11), (96, 12, 2), (6144, 26, 7), (12288, 41, 13)])
 def test_sketch_factors_match_standard_library_streams(d, ell, seed):
     """U/V of rand_sketch (threaded polar-method draws) equal the oracle's
     std::normal_distribution streams bit for bit, odd counts included."""
