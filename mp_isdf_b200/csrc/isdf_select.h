@@ -20,7 +20,7 @@ struct KeptPoints {
 // Positions per window of the spatial order (whole 128-point tiles).  A
 // window holds the same points in both orders, so position ranges made of
 // whole windows can be mapped back to ascending order on their own.
-constexpr int64_t kSpatialWindow = 32768;
+constexpr int64_t kSpatialWindow = 131072;
 
 // Flags non-finite weights (always) and non-finite coordinates of kept points,
 // and compacts the nonzero-weight points in their original order.  With an
