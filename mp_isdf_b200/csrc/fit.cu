@@ -761,7 +761,7 @@ FitOutput fit_grid_mixed(const Context& c, const double* pts, const double* w, c
     // With stored tiles and a hook, the points go in a few chunks of whole
     // 128-point tiles, each at least two waves of the stored-tile GEMM.
     const int64_t ntiles = (n + 127) / 128;
-    const int64_t nchunk = (ao_tiles && on_chunk) ? std::max<int64_t>(1, std::min<int64_t>(4, ntiles / 296)) : 1;
+    const int64_t nchunk = (ao_tiles && on_chunk) ? std::max<int64_t>(1, std::min<int64_t>(8, ntiles / 296)) : 1;
     int64_t per = (ntiles + nchunk - 1) / nchunk * 128;
     // chunks of whole windows of a spatial order, so that each chunk's Theta
     // columns can be put back in ascending order on their own
