@@ -391,3 +391,28 @@ def test_cuda_pair_qr_two_shards_match_select_fit(algorithm, empty):
     rel = np.abs(th_sharded - th_ref).max() / np.abs(th_ref).max()
     assert rel <= 1e-12 * max(1.0, finfo.condition) ** 2, rel
     assert abs(results[0].pair_relative - finfo.pair_relative) <= 1e-10 * finfo.pair_relative
+
+
+@pytest.mark.gpu
+def test_verified_sketch_qr_every_column_a_candidate():
+    """Error bounds inflated to 1e30 make every column of the mixed sketch a
+    re-verification candidate at the first step (one block per column, several
+    columns per block, a candidate scan that reads every block) and exact from
+    then on (the scan takes every block's key from the update).  The pivots
+    equal those of the sketch's own bounds: a pivot is always an exact column."""
+    import torch
+    from mp_isdf_b200 import capi
+    mol, pts, w = _system()
+    ctx = capi.Context(mol.atm, mol.bas, mol.env)
+    x = torch.tensor(pts, device="cuda")
+    wt = torch.tensor(w, device="cuda")
+    shard, n_kept, ell, sumsq = ctx.sketch_shard_project(x, wt, len(pts), precision="mixed", **KW)
+    yt, delta, _, kxyz, kw_, scales = ctx.sketch_shard_combine(shard, sumsq, ell, n_kept, len(KW["axes"]))
+    assert n_kept > 16 * 148
+    piv, info = ctx.sketch_select_gathered(yt.clone(), kxyz, kw_, delta.clone(), scales, precision="mixed", **KW)
+    big = torch.full_like(delta, 1e30)
+    piv_all, info_all = ctx.sketch_select_gathered(yt.clone(), kxyz, kw_, big, scales, precision="mixed", **KW)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(piv_all, piv)
+    assert info_all.verifications >= n_kept > info.verifications
+    assert info_all.numerical_rank == info.numerical_rank
