@@ -496,7 +496,7 @@ def run_reference(args, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": "the reference's qrcp on this config "
                           "materialises a d^2 x n pair matrix that exceeds host memory"}), flush=True)
         return
-    # the timed steps cycle through the point samples of the repo arm's CPU leg
+    # the timed steps cycle through the point samples that the default run's cpu_baseline
     # (seeds 0..2), so both legs time the same work
     for i in range(args.warmup + args.steps):
         seed = (i - args.warmup) % 3 if i >= args.warmup else i % 3
