@@ -497,7 +497,7 @@ def run_reference(args, rank, world):
                           "materialises a d^2 x n pair matrix that exceeds host memory"}), flush=True)
         return
     # the timed steps cycle through the point samples that the default run's cpu_baseline
-    # (seeds 0..2), so both legs time the same work
+    # leg times (seeds 0..2), so both legs time the same work
     for i in range(args.warmup + args.steps):
         seed = (i - args.warmup) % 3 if i >= args.warmup else i % 3
         v, cores, sample = cpu_sample(mol, pts, w, names, factors, cfg, n_sample=n_sample, seed=seed)
