@@ -450,7 +450,29 @@ __device__ void exact_projections(const ExactArgs& ea, const double* feat, doubl
         const int si = item / nseg, seg = item % nseg;
         const double* wt = ea.WT + (s2a + si) * d;
         double acc = 0;
-        for (int a = 0; a < ea.naxes; ++a) {
+        int a = 0;
+        // four axis entries per pass, so their weight loads are in flight
+        // together; each entry's sum and the order of acc are unchanged
+        for (; a + 4 <= ea.naxes; a += 4) {
+            const double* f0 = feat + (GRAD ? ea.comp[a] : 0) * nao;
+            const double* f1 = feat + (GRAD ? ea.comp[a + 1] : 0) * nao;
+            const double* f2 = feat + (GRAD ? ea.comp[a + 2] : 0) * nao;
+            const double* f3 = feat + (GRAD ? ea.comp[a + 3] : 0) * nao;
+            const double* w0 = wt + static_cast<int64_t>(a) * nao;
+            double p0 = 0, p1 = 0, p2 = 0, p3 = 0;
+            for (int i = seg * 32 + lane; i < nao; i += 32 * nseg) {
+                const double x0 = w0[i], x1 = w0[nao + i], x2 = w0[2 * nao + i], x3 = w0[3 * nao + i];
+                p0 += f0[i] * x0;
+                p1 += f1[i] * x1;
+                p2 += f2[i] * x2;
+                p3 += f3[i] * x3;
+            }
+            acc += ea.scales[a] * p0;
+            acc += ea.scales[a + 1] * p1;
+            acc += ea.scales[a + 2] * p2;
+            acc += ea.scales[a + 3] * p3;
+        }
+        for (; a < ea.naxes; ++a) {
             const double* f = feat + (GRAD ? ea.comp[a] : 0) * nao;
             const double* wa = wt + static_cast<int64_t>(a) * nao;
             double pa = 0;
